@@ -1,0 +1,485 @@
+// Driver over STORMM's own CPU library (built from the reference sources by the Makefile beside
+// this file).  It is test infrastructure only: it reads Amber prmtop / inpcrd files through
+// STORMM's AtomGraph and PhaseSpace, runs STORMM's FP64 CPU evaluators, and writes what it
+// computed to a small binary record file that tests/golden/make_golden.py turns into fixtures.
+// It also times the evaluators for the CPU baseline.
+//
+// Modes:
+//   eval <prmtop> <inpcrd> <out.bin> [options]
+//       Parameters as STORMM parsed them, FP64 energies per term (double sums and the ScoreCard's
+//       fixed-point sums), per-term forces, GB intermediates (psi, effective radii, sumdeijda)
+//       and the StaticExclusionMask tables.
+//   minimize <prmtop> <inpcrd> <out.bin> --maxcyc N --ncyc N [options]
+//       STORMM's CPU line minimizer (MolecularMechanics/minimization.h:157); writes the energy
+//       history and the final coordinates.
+//   time <list-file> <seconds> [options]
+//       Evaluates energy + forces (evalRestrainedMMGB) over the systems named in <list-file>
+//       (one "prmtop inpcrd" pair per line) round-robin until <seconds> of wall time pass, and
+//       prints "evals=<n> seconds=<t>".  With --minimize N it instead runs N-cycle minimizations
+//       and prints "minimizations=<n> seconds=<t>".
+//
+// Options: --igb {0,1,2,5,7,8} (default 5 = OBC-II), --diel X (80), --salt X (0),
+//          --qtol X --qdisc X (charge smoothing, STORMM defaults), --scee X --scnb X,
+//          --quantize (round coordinates to the 2^-32 Angstrom fixed-point grid first).
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <string>
+#include <vector>
+#include "copyright.h"
+#include "Constants/generalized_born.h"
+#include "Constants/symbol_values.h"
+#include "MolecularMechanics/minimization.h"
+#include "MolecularMechanics/mm_evaluation.h"
+#include "Namelists/nml_minimize.h"
+#include "Potential/nonbonded_potential.h"
+#include "Potential/scorecard.h"
+#include "Potential/static_exclusionmask.h"
+#include "Potential/valence_potential.h"
+#include "Restraints/restraint_apparatus.h"
+#include "Topology/atomgraph.h"
+#include "Trajectory/phasespace.h"
+
+using namespace stormm;
+using namespace stormm::energy;
+using namespace stormm::topology;
+using namespace stormm::trajectory;
+using namespace stormm::restraints;
+using namespace stormm::namelist;
+using namespace stormm::mm;
+using stormm::generalized_born_defaults::NeckGeneralizedBornTable;
+using stormm::generalized_born_defaults::NeckGeneralizedBornKit;
+
+namespace {
+
+struct Options {
+  int igb = 5;
+  double diel = 80.0;
+  double salt = 0.0;
+  double qtol = -1.0;
+  double qdisc = -1.0;
+  double scee = 1.2;
+  double scnb = 2.0;
+  bool quantize = false;
+  int maxcyc = 0;
+  int ncyc = 0;
+  int minimize_cycles = 0;
+  double dx0 = 0.01;
+};
+
+// Record file: for each record, int32 name length, name bytes, one dtype char ('d' double,
+// 'i' int32, 'q' int64, 'u' uint32), int64 element count, raw little-endian data.
+class RecordWriter {
+public:
+  explicit RecordWriter(const std::string &path) : out_(path, std::ios::binary) {
+    if (!out_) {
+      std::fprintf(stderr, "cannot open %s\n", path.c_str());
+      std::exit(2);
+    }
+  }
+  template <typename T> void put(const std::string &name, char dtype, const T* data, size_t n) {
+    const int32_t len = name.size();
+    out_.write(reinterpret_cast<const char*>(&len), 4);
+    out_.write(name.data(), len);
+    out_.write(&dtype, 1);
+    const int64_t cnt = n;
+    out_.write(reinterpret_cast<const char*>(&cnt), 8);
+    if (n > 0) {
+      out_.write(reinterpret_cast<const char*>(data), n * sizeof(T));
+    }
+  }
+  void d(const std::string &name, const std::vector<double> &v) { put(name, 'd', v.data(), v.size()); }
+  void d(const std::string &name, const double* p, size_t n) { put(name, 'd', p, n); }
+  void i(const std::string &name, const std::vector<int> &v) { put(name, 'i', v.data(), v.size()); }
+  void i(const std::string &name, const int* p, size_t n) { put(name, 'i', p, n); }
+  void u(const std::string &name, const uint* p, size_t n) { put(name, 'u', p, n); }
+  void scalar(const std::string &name, double v) { put(name, 'd', &v, 1); }
+  void iscalar(const std::string &name, int v) { put(name, 'i', &v, 1); }
+private:
+  std::ofstream out_;
+};
+
+ImplicitSolventModel igbModel(int igb) {
+  switch (igb) {
+  case 0: return ImplicitSolventModel::NONE;
+  case 1: return ImplicitSolventModel::HCT_GB;
+  case 2: return ImplicitSolventModel::OBC_GB;
+  case 5: return ImplicitSolventModel::OBC_GB_II;
+  case 7: return ImplicitSolventModel::NECK_GB;
+  case 8: return ImplicitSolventModel::NECK_GB_II;
+  default:
+    std::fprintf(stderr, "unsupported igb %d\n", igb);
+    std::exit(2);
+  }
+}
+
+AtomGraph loadTopology(const std::string &prmtop, const Options &opt) {
+  AtomGraph ag;
+  const double qtol = (opt.qtol >= 0.0) ? opt.qtol : default_charge_rounding_tol;
+  const double qdisc = (opt.qdisc >= 0.0) ? opt.qdisc : default_charge_precision_inc;
+  ag.buildFromPrmtop(prmtop, ExceptionResponse::SILENT, symbols::amber_ancient_bioq, opt.scee,
+                     opt.scnb, qtol, qdisc);
+  ag.setImplicitSolventModel(igbModel(opt.igb), opt.diel, opt.salt, AtomicRadiusSet::NONE,
+                             ExceptionResponse::SILENT);
+  return ag;
+}
+
+void quantizeCoordinates(PhaseSpace *ps) {
+  PhaseSpaceWriter psw = ps->data();
+  const double scale = 4294967296.0;
+  for (int i = 0; i < psw.natom; i++) {
+    psw.xcrd[i] = static_cast<double>(std::llround(psw.xcrd[i] * scale)) / scale;
+    psw.ycrd[i] = static_cast<double>(std::llround(psw.ycrd[i] * scale)) / scale;
+    psw.zcrd[i] = static_cast<double>(std::llround(psw.zcrd[i] * scale)) / scale;
+  }
+}
+
+void zeroForces(PhaseSpaceWriter psw) {
+  for (int i = 0; i < psw.natom; i++) {
+    psw.xfrc[i] = 0.0;
+    psw.yfrc[i] = 0.0;
+    psw.zfrc[i] = 0.0;
+  }
+}
+
+void putForces(RecordWriter *rw, const std::string &name, const PhaseSpaceWriter &psw) {
+  std::vector<double> f(3 * psw.natom);
+  for (int i = 0; i < psw.natom; i++) {
+    f[3 * i] = psw.xfrc[i];
+    f[3 * i + 1] = psw.yfrc[i];
+    f[3 * i + 2] = psw.zfrc[i];
+  }
+  rw->d(name, f);
+}
+
+void putTopology(RecordWriter *rw, const AtomGraph &ag) {
+  const NonbondedKit<double> nbk = ag.getDoublePrecisionNonbondedKit();
+  const ValenceKit<double> vk = ag.getDoublePrecisionValenceKit();
+  const ImplicitSolventKit<double> isk = ag.getDoublePrecisionImplicitSolventKit();
+  const ChemicalDetailsKit cdk = ag.getChemicalDetailsKit();
+  const int n = nbk.natom;
+  rw->iscalar("natom", n);
+  rw->scalar("coulomb_constant", nbk.coulomb_constant);
+  rw->d("charge", nbk.charge, n);
+  rw->i("lj_idx", nbk.lj_idx, n);
+  rw->iscalar("n_lj_types", nbk.n_lj_types);
+  const size_t nt2 = static_cast<size_t>(nbk.n_lj_types) * nbk.n_lj_types;
+  rw->d("lja", nbk.lja_coeff, nt2);
+  rw->d("ljb", nbk.ljb_coeff, nt2);
+  rw->d("lja14", nbk.lja_14_coeff, nt2);
+  rw->d("ljb14", nbk.ljb_14_coeff, nt2);
+  rw->i("z_numbers", cdk.z_numbers, n);
+  rw->i("nb11_bounds", nbk.nb11_bounds, n + 1);
+  rw->i("nb11x", nbk.nb11x, nbk.nb11_bounds[n]);
+  rw->i("nb12_bounds", nbk.nb12_bounds, n + 1);
+  rw->i("nb12x", nbk.nb12x, nbk.nb12_bounds[n]);
+  rw->i("nb13_bounds", nbk.nb13_bounds, n + 1);
+  rw->i("nb13x", nbk.nb13x, nbk.nb13_bounds[n]);
+  rw->i("nb14_bounds", nbk.nb14_bounds, n + 1);
+  rw->i("nb14x", nbk.nb14x, nbk.nb14_bounds[n]);
+
+  // Valence terms, expanded per term
+  std::vector<int> bi(vk.nbond), bj(vk.nbond);
+  std::vector<double> bk(vk.nbond), bl(vk.nbond);
+  for (int t = 0; t < vk.nbond; t++) {
+    bi[t] = vk.bond_i_atoms[t];
+    bj[t] = vk.bond_j_atoms[t];
+    bk[t] = vk.bond_keq[vk.bond_param_idx[t]];
+    bl[t] = std::fabs(vk.bond_leq[vk.bond_param_idx[t]]);
+  }
+  rw->i("bond_i", bi);
+  rw->i("bond_j", bj);
+  rw->d("bond_k", bk);
+  rw->d("bond_r0", bl);
+  std::vector<int> ai(vk.nangl), aj(vk.nangl), ak(vk.nangl);
+  std::vector<double> akq(vk.nangl), ath(vk.nangl);
+  for (int t = 0; t < vk.nangl; t++) {
+    ai[t] = vk.angl_i_atoms[t];
+    aj[t] = vk.angl_j_atoms[t];
+    ak[t] = vk.angl_k_atoms[t];
+    akq[t] = vk.angl_keq[vk.angl_param_idx[t]];
+    ath[t] = vk.angl_theta[vk.angl_param_idx[t]];
+  }
+  rw->i("angl_i", ai);
+  rw->i("angl_j", aj);
+  rw->i("angl_k", ak);
+  rw->d("angl_k_eq", akq);
+  rw->d("angl_theta0", ath);
+  std::vector<int> di(vk.ndihe), dj(vk.ndihe), dk(vk.ndihe), dl(vk.ndihe), dkind(vk.ndihe);
+  std::vector<double> damp(vk.ndihe), dfreq(vk.ndihe), dphi(vk.ndihe), de14(vk.ndihe),
+                      dv14(vk.ndihe);
+  for (int t = 0; t < vk.ndihe; t++) {
+    di[t] = vk.dihe_i_atoms[t];
+    dj[t] = vk.dihe_j_atoms[t];
+    dk[t] = vk.dihe_k_atoms[t];
+    dl[t] = vk.dihe_l_atoms[t];
+    const int p = vk.dihe_param_idx[t];
+    damp[t] = vk.dihe_amp[p];
+    dfreq[t] = vk.dihe_freq[p];
+    dphi[t] = vk.dihe_phi[p];
+    const int a14 = vk.dihe14_param_idx[t];
+    de14[t] = (a14 == 0) ? 0.0 : vk.attn14_elec[a14];
+    dv14[t] = (a14 == 0) ? 0.0 : vk.attn14_vdw[a14];
+    dkind[t] = static_cast<int>(vk.dihe_modifiers[t].w);
+  }
+  rw->i("dihe_i", di);
+  rw->i("dihe_j", dj);
+  rw->i("dihe_k", dk);
+  rw->i("dihe_l", dl);
+  rw->d("dihe_amp", damp);
+  rw->d("dihe_freq", dfreq);
+  rw->d("dihe_phase", dphi);
+  rw->d("dihe_scee", de14);
+  rw->d("dihe_scnb", dv14);
+  rw->i("dihe_kind", dkind);
+  rw->iscalar("ninfr14", vk.ninfr14);
+
+  // Implicit solvent parameters
+  rw->iscalar("igb", static_cast<int>(isk.igb));
+  rw->scalar("dielectric", isk.dielectric);
+  rw->scalar("saltcon", isk.saltcon);
+  rw->d("pb_radii", isk.pb_radii, n);
+  rw->d("gb_screen", isk.gb_screen, n);
+  rw->d("gb_alpha", isk.gb_alpha, n);
+  rw->d("gb_beta", isk.gb_beta, n);
+  rw->d("gb_gamma", isk.gb_gamma, n);
+  rw->i("neck_gb_idx", isk.neck_gb_idx, n);
+}
+
+void putExclusionMask(RecordWriter *rw, const StaticExclusionMask &se) {
+  const StaticExclusionMaskReader ser = se.data();
+  const int nst = ser.supertile_stride_count;
+  rw->iscalar("se_supertile_stride_count", nst);
+  rw->i("se_supertile_map_idx", ser.supertile_map_idx, static_cast<size_t>(nst) * nst);
+  const size_t n_uni_st = se.getUniqueSuperTileCount();
+  const size_t n_uni_t = se.getUniqueTileCount();
+  rw->i("se_tile_map_idx", ser.tile_map_idx, n_uni_st * tiles_per_supertile);
+  rw->u("se_mask_data", ser.mask_data, n_uni_t * 2 * tile_length);
+}
+
+void putCoordinates(RecordWriter *rw, const std::string &name, const PhaseSpaceWriter &psw) {
+  std::vector<double> c(3 * psw.natom);
+  for (int i = 0; i < psw.natom; i++) {
+    c[3 * i] = psw.xcrd[i];
+    c[3 * i + 1] = psw.ycrd[i];
+    c[3 * i + 2] = psw.zcrd[i];
+  }
+  rw->d(name, c);
+}
+
+const std::vector<StateVariable> kTerms = {
+  StateVariable::BOND, StateVariable::ANGLE, StateVariable::PROPER_DIHEDRAL,
+  StateVariable::IMPROPER_DIHEDRAL, StateVariable::VDW, StateVariable::VDW_ONE_FOUR,
+  StateVariable::ELECTROSTATIC, StateVariable::ELEC_ONE_FOUR, StateVariable::GENERALIZED_BORN
+};
+
+void putScoreCard(RecordWriter *rw, const std::string &name, const ScoreCard &sc) {
+  std::vector<double> e;
+  for (StateVariable sv : kTerms) {
+    e.push_back(sc.reportInstantaneousStates(sv, 0));
+  }
+  rw->d(name, e);
+}
+
+int runEval(const std::string &prmtop, const std::string &inpcrd, const std::string &out,
+            const Options &opt) {
+  AtomGraph ag = loadTopology(prmtop, opt);
+  PhaseSpace ps(inpcrd, CoordinateFileKind::AMBER_INPCRD);
+  if (opt.quantize) {
+    quantizeCoordinates(&ps);
+  }
+  const StaticExclusionMask se(&ag);
+  const NeckGeneralizedBornTable ngb_tab;
+  RecordWriter rw(out);
+  putTopology(&rw, ag);
+  putExclusionMask(&rw, se);
+  PhaseSpaceWriter psw = ps.data();
+  putCoordinates(&rw, "coords", psw);
+  const ValenceKit<double> vk = ag.getDoublePrecisionValenceKit();
+  const NonbondedKit<double> nbk = ag.getDoublePrecisionNonbondedKit();
+  const ImplicitSolventKit<double> isk = ag.getDoublePrecisionImplicitSolventKit();
+  const NeckGeneralizedBornKit<double> ngbk = ngb_tab.dpData();
+  ScoreCard sc(1, 1, 32);
+
+  // Per-term FP64 energies (double sums) and forces
+  std::vector<double> esum;
+  zeroForces(psw);
+  esum.push_back(evaluateBondTerms(vk, psw, &sc, EvaluateForce::YES, 0));
+  putForces(&rw, "frc_bond", psw);
+  zeroForces(psw);
+  esum.push_back(evaluateAngleTerms(vk, psw, &sc, EvaluateForce::YES, 0));
+  putForces(&rw, "frc_angle", psw);
+  zeroForces(psw);
+  const double2 dihe = evaluateDihedralTerms(vk, psw, &sc, EvaluateForce::YES, 0);
+  esum.push_back(dihe.x);
+  esum.push_back(dihe.y);
+  putForces(&rw, "frc_dihedral", psw);
+  zeroForces(psw);
+  const double2 a14 = evaluateAttenuated14Terms(vk, nbk, psw, &sc, EvaluateForce::YES,
+                                                EvaluateForce::YES, 0);
+  putForces(&rw, "frc_14", psw);
+  zeroForces(psw);
+  const double2 nb = evaluateNonbondedEnergy(nbk, se.data(), psw, &sc, EvaluateForce::YES,
+                                             EvaluateForce::YES, 0);
+  putForces(&rw, "frc_nonbonded", psw);
+  esum.push_back(nb.y);
+  esum.push_back(a14.y);
+  esum.push_back(nb.x);
+  esum.push_back(a14.x);
+  zeroForces(psw);
+  std::vector<double> egb(psw.natom), psi(psw.natom), sdeijda(psw.natom);
+  const double gb = evaluateGeneralizedBornEnergy<double, double, double>(
+                      nbk, se.data(), isk, ngbk, psw.xcrd, psw.ycrd, psw.zcrd, psw.xfrc,
+                      psw.yfrc, psw.zfrc, egb.data(), psi.data(), sdeijda.data(), &sc,
+                      EvaluateForce::YES, 0);
+  esum.push_back(gb);
+  putForces(&rw, "frc_gb", psw);
+  rw.d("gb_psi", psi);
+  rw.d("gb_radii", egb);
+  rw.d("gb_sumdeijda", sdeijda);
+  rw.d("energy_terms", esum);
+  putScoreCard(&rw, "energy_terms_fixed", sc);
+
+  // The complete evaluation through the MM driver STORMM uses for single points
+  zeroForces(psw);
+  ScoreCard sc_all(1, 1, 26);
+  const RestraintApparatus ra(&ag);
+  evalRestrainedMMGB(&ps, &sc_all, ag, ngb_tab, se, ra, EvaluateForce::YES, 0);
+  putForces(&rw, "frc_total", psw);
+  putScoreCard(&rw, "energy_terms_mm", sc_all);
+  return 0;
+}
+
+MinimizeControls minimizeControls(const Options &opt) {
+  MinimizeControls mincon;
+  mincon.setTotalCycles(opt.maxcyc);
+  mincon.setSteepestDescentCycles(opt.ncyc);
+  mincon.setClashDampingCycles(0);
+  mincon.setInitialStep(opt.dx0);
+  mincon.setDiagnosticPrintFrequency(1);
+  return mincon;
+}
+
+int runMinimize(const std::string &prmtop, const std::string &inpcrd, const std::string &out,
+                const Options &opt) {
+  AtomGraph ag = loadTopology(prmtop, opt);
+  PhaseSpace ps(inpcrd, CoordinateFileKind::AMBER_INPCRD);
+  if (opt.quantize) {
+    quantizeCoordinates(&ps);
+  }
+  const StaticExclusionMask se(&ag);
+  const NeckGeneralizedBornTable ngb_tab;
+  const RestraintApparatus ra(&ag);
+  const MinimizeControls mincon = minimizeControls(opt);
+  ScoreCard sc = minimize(&ps, ag, ngb_tab, ra, se, mincon);
+  RecordWriter rw(out);
+  const std::vector<double> etot = sc.reportHistory(StateVariable::POTENTIAL_ENERGY, 0);
+  rw.d("min_potential_history", etot);
+  putCoordinates(&rw, "min_final_coords", ps.data());
+  std::vector<double> efinal;
+  for (StateVariable sv : kTerms) {
+    efinal.push_back(sc.reportInstantaneousStates(sv, 0));
+  }
+  rw.d("min_final_terms", efinal);
+  return 0;
+}
+
+int runTime(const std::string &list_file, double seconds, const Options &opt) {
+  std::ifstream lst(list_file);
+  std::vector<AtomGraph> ags;
+  std::vector<PhaseSpace> pss;
+  std::string top, crd;
+  while (lst >> top >> crd) {
+    ags.push_back(loadTopology(top, opt));
+    pss.emplace_back(crd, CoordinateFileKind::AMBER_INPCRD);
+  }
+  if (ags.empty()) {
+    std::fprintf(stderr, "no systems listed in %s\n", list_file.c_str());
+    return 2;
+  }
+  std::vector<StaticExclusionMask> ses;
+  std::vector<RestraintApparatus> ras;
+  for (size_t i = 0; i < ags.size(); i++) {
+    ses.emplace_back(&ags[i]);
+    ras.emplace_back(&ags[i]);
+  }
+  const NeckGeneralizedBornTable ngb_tab;
+  const auto t0 = std::chrono::steady_clock::now();
+  double elapsed = 0.0;
+  long long count = 0;
+  size_t idx = 0;
+  double checksum = 0.0;
+  while (elapsed < seconds) {
+    if (opt.minimize_cycles > 0) {
+      Options o2 = opt;
+      o2.maxcyc = opt.minimize_cycles;
+      PhaseSpace ps_copy = pss[idx];
+      const MinimizeControls mincon = minimizeControls(o2);
+      ScoreCard sc = minimize(&ps_copy, ags[idx], ngb_tab, ras[idx], ses[idx], mincon);
+      checksum += sc.reportInstantaneousStates(StateVariable::POTENTIAL_ENERGY, 0);
+    }
+    else {
+      ScoreCard sc(1, 1, 26);
+      pss[idx].initializeForces();
+      evalRestrainedMMGB(&pss[idx], &sc, ags[idx], ngb_tab, ses[idx], ras[idx],
+                         EvaluateForce::YES, 0);
+      checksum += sc.reportInstantaneousStates(StateVariable::POTENTIAL_ENERGY, 0);
+    }
+    count++;
+    idx = (idx + 1) % ags.size();
+    elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+  std::printf("%s=%lld seconds=%.6f systems=%zu checksum=%.6f\n",
+              (opt.minimize_cycles > 0) ? "minimizations" : "evals", count, elapsed, ags.size(),
+              checksum);
+  return 0;
+}
+
+} // namespace
+
+int main(int argc, char* argv[]) {
+  if (argc < 3) {
+    std::fprintf(stderr, "usage: %s eval|minimize|time ...\n", argv[0]);
+    return 2;
+  }
+  const std::string mode(argv[1]);
+  std::vector<std::string> pos;
+  Options opt;
+  for (int i = 2; i < argc; i++) {
+    const std::string a(argv[i]);
+    auto next = [&]() -> double {
+      if (i + 1 >= argc) {
+        std::fprintf(stderr, "missing value for %s\n", a.c_str());
+        std::exit(2);
+      }
+      return std::atof(argv[++i]);
+    };
+    if (a == "--igb") opt.igb = static_cast<int>(next());
+    else if (a == "--diel") opt.diel = next();
+    else if (a == "--salt") opt.salt = next();
+    else if (a == "--qtol") opt.qtol = next();
+    else if (a == "--qdisc") opt.qdisc = next();
+    else if (a == "--scee") opt.scee = next();
+    else if (a == "--scnb") opt.scnb = next();
+    else if (a == "--maxcyc") opt.maxcyc = static_cast<int>(next());
+    else if (a == "--ncyc") opt.ncyc = static_cast<int>(next());
+    else if (a == "--dx0") opt.dx0 = next();
+    else if (a == "--minimize") opt.minimize_cycles = static_cast<int>(next());
+    else if (a == "--quantize") opt.quantize = true;
+    else pos.push_back(a);
+  }
+  if (mode == "eval" && pos.size() == 3) {
+    return runEval(pos[0], pos[1], pos[2], opt);
+  }
+  if (mode == "minimize" && pos.size() == 3) {
+    return runMinimize(pos[0], pos[1], pos[2], opt);
+  }
+  if (mode == "time" && pos.size() == 2) {
+    return runTime(pos[0], std::atof(pos[1].c_str()), opt);
+  }
+  std::fprintf(stderr, "bad arguments for mode %s\n", mode.c_str());
+  return 2;
+}
