@@ -1,0 +1,131 @@
+"""Generate the golden fixtures in this directory by running STORMM's own CPU code.
+
+Requires the reference sources and the reference CPU build (oracle/ref/Makefile, which puts
+libstormm_ref.so and stormm_ref_driver under oracle/_ref/).  Run from the repository root:
+
+    python tests/golden/make_golden.py [--reference-root /root/reference]
+
+Fixtures written (numpy .npz, one per case):
+
+* ``synthetic_<name>.npz``: synthetic molecules (the 64-atom single-point molecule and edge-case
+  sizes) written as Amber prmtop/inpcrd, read back through STORMM's AtomGraph, and evaluated by
+  STORMM's FP64 CPU evaluators (Potential/valence_potential.tpp, nonbonded_potential.tpp).  Each
+  holds the parameters as STORMM parsed them, per-term energies and forces, GB intermediates and
+  the StaticExclusionMask tables.
+* ``reference_<system>_igb<k>.npz``: the reference's own test systems (Trp-cage, alanine
+  dipeptide) under the settings of test/Potential/test_generalized_born.cpp:236-301, with the
+  known-answer GB energies that test file asserts.
+* ``minimize_m0.npz``: STORMM's CPU line minimizer (MolecularMechanics/minimization.tpp) on the
+  64-atom molecule, energy history and final coordinates.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import re
+import struct
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from stormm_b200 import prmtop, synthetic  # noqa: E402
+
+DRIVER = os.path.join(ROOT, "oracle", "_ref", "stormm_ref_driver")
+
+
+def read_records(path):
+    out = {}
+    with open(path, "rb") as f:
+        while True:
+            h = f.read(4)
+            if not h:
+                break
+            n = struct.unpack("<i", h)[0]
+            name = f.read(n).decode()
+            dt = f.read(1).decode()
+            cnt = struct.unpack("<q", f.read(8))[0]
+            t = {"d": "<f8", "i": "<i4", "q": "<i8", "u": "<u4"}[dt]
+            out[name] = np.frombuffer(f.read(cnt * np.dtype(t).itemsize), dtype=t).copy()
+    return out
+
+
+def run_driver(args):
+    r = subprocess.run([DRIVER] + args, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"driver failed: {args}\n{r.stderr}")
+    return r.stdout
+
+
+def eval_molecule(mol, tmp, extra=()):
+    top = os.path.join(tmp, mol.name + ".top")
+    crd = os.path.join(tmp, mol.name + ".crd")
+    out = os.path.join(tmp, mol.name + ".bin")
+    prmtop.write_prmtop(mol, top)
+    prmtop.write_inpcrd(mol, crd)
+    run_driver(["eval", top, crd, out, "--quantize"] + list(extra))
+    return read_records(out), top, crd
+
+
+def gb_known_answers(ref_root):
+    """Known-answer GB energies asserted by the reference's GB test (Trp-cage, DHFR, alanine
+    dipeptide in that order; test/Potential/test_generalized_born.cpp:296-300)."""
+    text = open(os.path.join(ref_root, "test", "Potential", "test_generalized_born.cpp")).read()
+    answers = {}
+    for name in ("hct", "obc", "obc2", "neck", "neck2"):
+        m = re.search(r"std::vector<double> " + name + r"_gb_answer\s*=\s*\{([^}]*)\}", text)
+        answers[name] = np.array([float(v) for v in m.group(1).split(",")])
+    return answers
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference-root", default="/root/reference")
+    args = ap.parse_args()
+    if not os.path.exists(DRIVER):
+        raise SystemExit("build the reference driver first: make -C oracle/ref -j8")
+    with tempfile.TemporaryDirectory() as tmp:
+        # 1. the single-point molecule and edge-case sizes
+        mols = synthetic.workload_single()
+        for n in (2, 12, 16, 17, 31, 32, 33, 48, 100, 255, 256, 257, 300):
+            mols.append(synthetic.make_molecule(7700 + n, n, noise=0.1, name=f"E{n}"))
+        mols.append(synthetic.make_chain(7000, 600, name="C600"))
+        for mol in mols:
+            rec, top, crd = eval_molecule(mol, tmp)
+            np.savez_compressed(os.path.join(HERE, f"synthetic_{mol.name}.npz"), **rec)
+            print("wrote", mol.name, mol.natom, rec["energy_terms"])
+            if mol.name == "M0":
+                out = os.path.join(tmp, "m0_min.bin")
+                run_driver(["minimize", top, crd, out, "--quantize", "--maxcyc", "100",
+                            "--ncyc", "50"])
+                mrec = read_records(out)
+                np.savez_compressed(os.path.join(HERE, "minimize_m0.npz"), maxcyc=100, ncyc=50,
+                                    **mrec)
+                print("wrote minimize_m0", mrec["min_potential_history"][[0, -1]])
+
+        # 2. the reference's own GB test systems with its known answers
+        answers = gb_known_answers(args.reference_root)
+        tdir = os.path.join(args.reference_root, "test")
+        systems = {"trpcage": ("trpcage.top", "trpcage.inpcrd", 1.2, 2.0, 0),
+                   "ala_dipeptide": ("ala_dipeptide.top", "ala_dipeptide.inpcrd", 1.2, 2.0, 2)}
+        for sname, (tf, cf, scee, scnb, ans_idx) in systems.items():
+            for igb, key in ((1, "hct"), (2, "obc"), (5, "obc2")):
+                out = os.path.join(tmp, f"{sname}_{igb}.bin")
+                run_driver(["eval", os.path.join(tdir, "Topology", tf),
+                            os.path.join(tdir, "Trajectory", cf), out, "--igb", str(igb),
+                            "--diel", "78.5", "--qtol", "1e-10",
+                            "--qdisc", "9.31322574615478515625E-10",
+                            "--scee", str(scee), "--scnb", str(scnb)])
+                rec = read_records(out)
+                rec["known_answer_gb"] = np.array([answers[key][ans_idx]])
+                np.savez_compressed(os.path.join(HERE, f"reference_{sname}_igb{igb}.npz"), **rec)
+                print("wrote", sname, igb, rec["energy_terms"][-1], answers[key][ans_idx])
+
+
+if __name__ == "__main__":
+    main()
