@@ -376,8 +376,18 @@ int runMinimize(const std::string &prmtop, const std::string &inpcrd, const std:
   const MinimizeControls mincon = minimizeControls(opt);
   ScoreCard sc = minimize(&ps, ag, ngb_tab, ra, se, mincon);
   RecordWriter rw(out);
-  const std::vector<double> etot = sc.reportHistory(StateVariable::POTENTIAL_ENERGY, 0);
+  std::vector<double> etot;
+  for (StateVariable sv : kTerms) {
+    const std::vector<double> h = sc.reportHistory(sv, 0);
+    if (etot.empty()) {
+      etot.assign(h.size(), 0.0);
+    }
+    for (size_t k = 0; k < h.size() && k < etot.size(); k++) {
+      etot[k] += h[k];
+    }
+  }
   rw.d("min_potential_history", etot);
+  rw.scalar("min_final_potential", sc.reportPotentialEnergy(0));
   putCoordinates(&rw, "min_final_coords", ps.data());
   std::vector<double> efinal;
   for (StateVariable sv : kTerms) {
