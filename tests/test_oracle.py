@@ -86,7 +86,7 @@ def test_split_fixed_point_conversions():
     assert oracle.float_to_int63(1234.5) == (1234, 0) or oracle.float_to_int63(1234.5) == (1235, 0)
     x, y = oracle.float_to_int63(3.0 * 2.0 ** 31 + 4096.0)
     assert y == 3 and x == 4096
-    x, y = oracle.float_to_int63(-5.0 * 2.0 ** 31 - 256.0)
-    assert y == -5 and x == -256
+    x, y = oracle.float_to_int63(-5.0 * 2.0 ** 31 - 2048.0)
+    assert y == -5 and x == -2048
     x, y = oracle.double_to_int95(2.0 ** 64 + 2.0 ** 20)
     assert y == 2 and x == 2 ** 20
