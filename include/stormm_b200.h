@@ -1,0 +1,199 @@
+/*
+ * stormm_b200: C ABI of the B200-native batched implicit-solvent molecular-mechanics path.
+ *
+ * This is the drop-in boundary beneath STORMM's C++ API for one hot path: batched, non-periodic
+ * Coulomb + Lennard-Jones with exclusions and scaled 1-4 terms, the Generalized Born passes
+ * (Born radii, GB energy and dE/dR, radii chain-rule force), valence terms (bonds, angles,
+ * dihedrals), and the line-minimization driver built on them.  Every entry point takes plain
+ * pointers, sizes and a CUDA stream; none takes a C++ or torch type.  Entry points return
+ * SB_OK (0) or a negative SB_ERR_* code; sb_last_error() describes the last failure on the
+ * calling thread.
+ *
+ * Reference interfaces replaced (paths inside the STORMM source tree):
+ *   sb_synthesis_create      AtomGraphSynthesis + PhaseSpaceSynthesis + StaticExclusionMaskSynthesis
+ *                            + ImplicitSolventWorkspace + ScoreCard construction
+ *                            (Synthesis/atomgraph_synthesis.h:84-110, phasespace_synthesis.h:348-376,
+ *                            static_mask_synthesis.h:54, implicit_solvent_workspace.h:83,
+ *                            Potential/scorecard.h:110; setImplicitSolventModel
+ *                            atomgraph_synthesis.h:455-473)
+ *   sb_initialize            PhaseSpaceSynthesis::initializeForces, ImplicitSolventWorkspace::initialize,
+ *                            ScoreCard::initialize (phasespace_synthesis.h, kPsyInitializeForces
+ *                            hpc_phasespace_synthesis.cu:243; hpc_implicit_solvent_workspace.cu:21;
+ *                            hpc_scorecard.cu:17)
+ *   sb_launch_nonbonded      launchNonbonded (Potential/hpc_nonbonded_potential.h:142-157)
+ *   sb_launch_valence        launchValence (Potential/hpc_valence_potential.h:167-230)
+ *   sb_evaluate              launchNonbonded followed by launchValence, fused into one pass
+ *   sb_minimize              launchMinimization (MolecularMechanics/hpc_minimization.h:122-152)
+ */
+#ifndef STORMM_B200_H
+#define STORMM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------------------------ */
+/* Status codes                                                                                */
+/* ------------------------------------------------------------------------------------------ */
+#define SB_OK 0
+#define SB_ERR_ARGUMENT -1     /* an argument is out of range or inconsistent */
+#define SB_ERR_CUDA -2         /* a CUDA runtime call failed */
+#define SB_ERR_DEVICE -3       /* no usable sm_100 device */
+#define SB_ERR_UNSUPPORTED -4  /* a feature outside this path (e.g. neck GB) was requested */
+#define SB_ERR_KERNEL -5       /* a kernel reported an error through its status word */
+
+/* ------------------------------------------------------------------------------------------ */
+/* Enumerations (values follow STORMM's)                                                       */
+/* ------------------------------------------------------------------------------------------ */
+/* Generalized Born model, as Amber's igb keyword: 0 none, 1 HCT, 2 OBC-I, 5 OBC-II */
+#define SB_GB_NONE 0
+#define SB_GB_HCT 1
+#define SB_GB_OBC 2
+#define SB_GB_OBC2 5
+
+/* Energy slots per system, STORMM's StateVariable order (Potential/energy_enumerators.h:36-50) */
+#define SB_BOND 0
+#define SB_ANGLE 1
+#define SB_PROPER_DIHEDRAL 2
+#define SB_IMPROPER_DIHEDRAL 3
+#define SB_UREY_BRADLEY 4
+#define SB_CHARMM_IMPROPER 5
+#define SB_CMAP 6
+#define SB_VDW 7
+#define SB_VDW_ONE_FOUR 8
+#define SB_ELECTROSTATIC 9
+#define SB_ELEC_ONE_FOUR 10
+#define SB_GENERALIZED_BORN 11
+#define SB_RESTRAINT 12
+#define SB_NRG_STRIDE 16        /* energy slots per system in sb_get_energies output */
+
+/* Terms to evaluate (bit mask) */
+#define SB_TERM_VALENCE 1
+#define SB_TERM_NONBONDED 2     /* Coulomb + Lennard-Jones */
+#define SB_TERM_GB 4
+#define SB_TERM_ALL 7
+
+/* What sb_initialize clears (bit mask) */
+#define SB_INIT_FORCES 1
+#define SB_INIT_ENERGIES 2
+#define SB_INIT_GB_WORKSPACE 4
+
+/* ------------------------------------------------------------------------------------------ */
+/* Inputs                                                                                      */
+/* ------------------------------------------------------------------------------------------ */
+/* One molecule's topology (host memory, 0-based atom indices).  The fields are what STORMM's
+ * AtomGraph provides through its NonbondedKit, ValenceKit and ImplicitSolventKit
+ * (Topology/atomgraph_abstracts.h:88-377). */
+typedef struct {
+  int natom;
+  const double* charge;        /* natom, elementary charges */
+  const int* lj_idx;           /* natom, Lennard-Jones type of each atom */
+  int n_lj_types;
+  const double* lja;           /* n_lj_types^2, A coefficients (kcal/mol A^12) */
+  const double* ljb;           /* n_lj_types^2, B coefficients (kcal/mol A^6) */
+  const double* lja14;         /* n_lj_types^2, 1-4 A coefficients (NULL: same as lja) */
+  const double* ljb14;         /* n_lj_types^2, 1-4 B coefficients (NULL: same as ljb) */
+  const int* excl_bounds;      /* natom + 1, CSR bounds of each atom's excluded partners */
+  const int* excl_list;        /* 1-2, 1-3 and 1-4 partners of each atom (either order) */
+  const double* pb_radii;      /* natom, intrinsic GB radii (A) */
+  const double* gb_screen;     /* natom, GB screening factors */
+  const double* gb_alpha;      /* natom, OBC alpha (NULL: model defaults) */
+  const double* gb_beta;       /* natom */
+  const double* gb_gamma;      /* natom */
+  int nbond;
+  const int* bond_atoms;       /* 2 * nbond */
+  const double* bond_keq;      /* kcal/mol A^2 */
+  const double* bond_leq;      /* A */
+  int nangl;
+  const int* angl_atoms;       /* 3 * nangl */
+  const double* angl_keq;      /* kcal/mol rad^2 */
+  const double* angl_theta0;   /* rad */
+  int ndihe;
+  const int* dihe_atoms;       /* 4 * ndihe */
+  const double* dihe_amp;      /* kcal/mol */
+  const double* dihe_freq;     /* periodicity */
+  const double* dihe_phase;    /* rad */
+  const double* dihe_scee;     /* 1-4 electrostatic attenuation, 0 when the term carries no 1-4 */
+  const double* dihe_scnb;     /* 1-4 Lennard-Jones attenuation */
+  const int* dihe_improper;    /* nonzero: energy is reported as improper (NULL: all proper) */
+} sb_topology;
+
+typedef struct {
+  int igb;                     /* SB_GB_* */
+  double dielectric;           /* solvent dielectric (STORMM default 80) */
+  double saltcon;              /* salt concentration, mol/L */
+  double coulomb_constant;     /* kcal A / mol e^2 (STORMM/Amber 332.05221729) */
+  int gpos_bits;               /* fixed-point bits of coordinates (32) */
+  int frc_bits;                /* fixed-point bits of forces (23) */
+  int nrg_bits;                /* fixed-point bits of energies (26) */
+  int max_atoms_per_unit;      /* work-unit packing limit, 0: tuned default */
+  int max_tiles_per_unit;      /* work-unit packing limit, 0: tuned default */
+  int threads_per_block;       /* 0: tuned default */
+  int device;                  /* CUDA device ordinal */
+} sb_options;
+
+/* Fill *opt with STORMM's defaults (OBC-II, dielectric 80, no salt, 32/23/26 fixed-point bits) */
+void sb_default_options(sb_options* opt);
+
+typedef struct sb_synthesis sb_synthesis;
+
+/* Build a synthesis of nsys systems.  System k uses topology tops[topology_index[k]].  All device
+ * memory is allocated here and released by sb_synthesis_destroy. */
+int sb_synthesis_create(const sb_topology* tops, int ntop, const int* topology_index, int nsys,
+                        const sb_options* opt, sb_synthesis** out);
+int sb_synthesis_destroy(sb_synthesis* syn);
+
+int sb_system_count(const sb_synthesis* syn);
+/* Atom count of one system and the offset of its first atom in the padded device arrays */
+int sb_system_atoms(const sb_synthesis* syn, int system, int* natom, int* offset);
+/* Total padded atom count (every system starts on a multiple of 32) */
+int sb_padded_atom_count(const sb_synthesis* syn);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Host <-> device transfers (asynchronous on the stream; host buffers should be pinned for     */
+/* overlap).  xyz arrays hold all systems back to back without padding, 3 doubles per atom.    */
+/* ------------------------------------------------------------------------------------------ */
+int sb_set_coordinates(sb_synthesis* syn, const double* xyz, void* stream);
+int sb_get_coordinates(sb_synthesis* syn, double* xyz, void* stream);
+int sb_get_forces(sb_synthesis* syn, double* xyz, void* stream);
+/* energies: nsys * SB_NRG_STRIDE doubles, kcal/mol, STORMM's slot order */
+int sb_get_energies(sb_synthesis* syn, double* energies, void* stream);
+/* GB intermediates per atom (unpadded): psi (A^-1), effective radii (A), sum of dE/dR
+ * after the chain-rule prefactor, as STORMM's ImplicitSolventWorkspace holds them */
+int sb_get_gb_workspace(sb_synthesis* syn, double* psi, double* radii, double* sumdeijda,
+                        void* stream);
+/* Raw fixed-point arrays (padded layout) for bit-exact inspection: int64 x, y, z + int32 overflow */
+int sb_get_forces_fixed(sb_synthesis* syn, int64_t* xyz_primary, int32_t* xyz_overflow,
+                        void* stream);
+int sb_get_energies_fixed(sb_synthesis* syn, int64_t* energies, void* stream);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Evaluation                                                                                  */
+/* ------------------------------------------------------------------------------------------ */
+int sb_initialize(sb_synthesis* syn, int what, void* stream);
+/* All requested terms for every system in one fused pass.  Forces and energies accumulate
+ * into the synthesis' arrays (clear them with sb_initialize first). */
+int sb_evaluate(sb_synthesis* syn, int terms, int eval_force, int eval_energy, void* stream);
+/* Systems [first, first + count) only: the per-system drop-in launch sequence */
+int sb_evaluate_range(sb_synthesis* syn, int first, int count, int terms, int eval_force,
+                      int eval_energy, void* stream);
+/* STORMM's two launchers, each alone */
+int sb_launch_nonbonded(sb_synthesis* syn, int eval_force, int eval_energy, void* stream);
+int sb_launch_valence(sb_synthesis* syn, int eval_force, int eval_energy, void* stream);
+
+/* Number of work units the batched launches use, and the launch shape chosen */
+int sb_launch_info(const sb_synthesis* syn, int* work_units, int* blocks, int* threads);
+
+/* Read and clear the device status word that bounded device-side waits and checks set */
+int sb_check_status(sb_synthesis* syn, int* status);
+
+const char* sb_last_error(void);
+const char* sb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,306 @@
+"""stormm_b200: B200-native batched implicit-solvent molecular mechanics.
+
+Python access to the C ABI of include/stormm_b200.h (libstormm_b200.so, built in-tree by
+stormm_b200/build.py).  The library is the product; this module only marshals arguments.  There
+is no CPU fallback: if the CUDA library is missing or no device is usable, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libstormm_b200.so")
+
+SB_OK = 0
+SB_GB_NONE, SB_GB_HCT, SB_GB_OBC, SB_GB_OBC2 = 0, 1, 2, 5
+TERM_VALENCE, TERM_NONBONDED, TERM_GB, TERM_ALL = 1, 2, 4, 7
+INIT_FORCES, INIT_ENERGIES, INIT_GB_WORKSPACE = 1, 2, 4
+NRG_STRIDE = 16
+# StateVariable slots (STORMM Potential/energy_enumerators.h:36-50)
+NRG_SLOTS = {"bond": 0, "angle": 1, "proper_dihedral": 2, "improper_dihedral": 3, "vdw": 7,
+             "vdw_14": 8, "elec": 9, "elec_14": 10, "gb": 11}
+# order of the oracle's / reference driver's nine energy terms
+TERM_ORDER = ["bond", "angle", "proper_dihedral", "improper_dihedral", "vdw", "vdw_14", "elec",
+              "elec_14", "gb"]
+
+_P = ctypes.c_void_p
+
+
+class Topology(ctypes.Structure):
+    _fields_ = [
+        ("natom", ctypes.c_int), ("charge", _P), ("lj_idx", _P), ("n_lj_types", ctypes.c_int),
+        ("lja", _P), ("ljb", _P), ("lja14", _P), ("ljb14", _P), ("excl_bounds", _P),
+        ("excl_list", _P), ("pb_radii", _P), ("gb_screen", _P), ("gb_alpha", _P),
+        ("gb_beta", _P), ("gb_gamma", _P), ("nbond", ctypes.c_int), ("bond_atoms", _P),
+        ("bond_keq", _P), ("bond_leq", _P), ("nangl", ctypes.c_int), ("angl_atoms", _P),
+        ("angl_keq", _P), ("angl_theta0", _P), ("ndihe", ctypes.c_int), ("dihe_atoms", _P),
+        ("dihe_amp", _P), ("dihe_freq", _P), ("dihe_phase", _P), ("dihe_scee", _P),
+        ("dihe_scnb", _P), ("dihe_improper", _P),
+    ]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [
+        ("igb", ctypes.c_int), ("dielectric", ctypes.c_double), ("saltcon", ctypes.c_double),
+        ("coulomb_constant", ctypes.c_double), ("gpos_bits", ctypes.c_int),
+        ("frc_bits", ctypes.c_int), ("nrg_bits", ctypes.c_int),
+        ("max_atoms_per_unit", ctypes.c_int), ("max_tiles_per_unit", ctypes.c_int),
+        ("threads_per_block", ctypes.c_int), ("device", ctypes.c_int),
+    ]
+
+
+class StormmB200Error(RuntimeError):
+    pass
+
+
+_LIB = None
+
+
+def library() -> ctypes.CDLL:
+    """Load libstormm_b200.so; raise if it has not been built."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise StormmB200Error(f"CUDA library not built: {LIB_PATH} "
+                                  "(run python -m stormm_b200.build)")
+        lib = ctypes.CDLL(LIB_PATH)
+        vp = ctypes.c_void_p
+        sig = {
+            "sb_default_options": (None, [ctypes.POINTER(Options)]),
+            "sb_synthesis_create": (ctypes.c_int, [ctypes.POINTER(Topology), ctypes.c_int, vp,
+                                                   ctypes.c_int, ctypes.POINTER(Options),
+                                                   ctypes.POINTER(vp)]),
+            "sb_synthesis_destroy": (ctypes.c_int, [vp]),
+            "sb_system_count": (ctypes.c_int, [vp]),
+            "sb_system_atoms": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                               ctypes.POINTER(ctypes.c_int)]),
+            "sb_padded_atom_count": (ctypes.c_int, [vp]),
+            "sb_set_coordinates": (ctypes.c_int, [vp, vp, vp]),
+            "sb_get_coordinates": (ctypes.c_int, [vp, vp, vp]),
+            "sb_get_forces": (ctypes.c_int, [vp, vp, vp]),
+            "sb_get_energies": (ctypes.c_int, [vp, vp, vp]),
+            "sb_get_gb_workspace": (ctypes.c_int, [vp, vp, vp, vp, vp]),
+            "sb_get_forces_fixed": (ctypes.c_int, [vp, vp, vp, vp]),
+            "sb_get_energies_fixed": (ctypes.c_int, [vp, vp, vp]),
+            "sb_initialize": (ctypes.c_int, [vp, ctypes.c_int, vp]),
+            "sb_evaluate": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]),
+            "sb_evaluate_range": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.c_int, ctypes.c_int, vp]),
+            "sb_launch_nonbonded": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, vp]),
+            "sb_launch_valence": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, vp]),
+            "sb_launch_info": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int),
+                                              ctypes.POINTER(ctypes.c_int),
+                                              ctypes.POINTER(ctypes.c_int)]),
+            "sb_check_status": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int)]),
+            "sb_last_error": (ctypes.c_char_p, []),
+            "sb_version": (ctypes.c_char_p, []),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = lib
+    return _LIB
+
+
+def _check(rc: int, what: str) -> None:
+    if rc != SB_OK:
+        msg = library().sb_last_error().decode(errors="replace")
+        raise StormmB200Error(f"{what} failed ({rc}): {msg}")
+
+
+def default_options(**overrides) -> Options:
+    o = Options()
+    library().sb_default_options(ctypes.byref(o))
+    for k, v in overrides.items():
+        setattr(o, k, v)
+    return o
+
+
+class _TopologyArrays:
+    """Keeps the numpy arrays behind one sb_topology alive."""
+
+    def __init__(self, mol):
+        self.keep = []
+        t = Topology()
+
+        def ptr(a, dt):
+            a = np.ascontiguousarray(np.asarray(a).reshape(-1), dtype=dt)
+            self.keep.append(a)
+            return a.ctypes.data
+
+        n = mol.natom
+        t.natom = n
+        t.charge = ptr(mol.charge, np.float64)
+        t.lj_idx = ptr(mol.lj_idx, np.int32)
+        t.n_lj_types = mol.n_lj_types
+        t.lja = ptr(mol.lja, np.float64)
+        t.ljb = ptr(mol.ljb, np.float64)
+        lja14 = getattr(mol, "lja14", None)
+        ljb14 = getattr(mol, "ljb14", None)
+        t.lja14 = ptr(lja14, np.float64) if lja14 is not None else None
+        t.ljb14 = ptr(ljb14, np.float64) if ljb14 is not None else None
+        bounds = np.zeros(n + 1, dtype=np.int32)
+        items = []
+        for i in range(n):
+            part = sorted(set(mol.excl12[i]) | set(mol.excl13[i]) | set(mol.excl14[i]))
+            items.extend(part)
+            bounds[i + 1] = len(items)
+        t.excl_bounds = ptr(bounds, np.int32)
+        t.excl_list = ptr(np.array(items if items else [0], dtype=np.int32), np.int32)
+        t.pb_radii = ptr(mol.pb_radii, np.float64)
+        t.gb_screen = ptr(mol.gb_screen, np.float64)
+        for name in ("gb_alpha", "gb_beta", "gb_gamma"):
+            v = getattr(mol, name, None)
+            setattr(t, name, ptr(v, np.float64) if v is not None else None)
+        t.nbond = mol.bonds.shape[0]
+        t.bond_atoms = ptr(mol.bonds, np.int32)
+        t.bond_keq = ptr(mol.bond_k, np.float64)
+        t.bond_leq = ptr(mol.bond_r0, np.float64)
+        t.nangl = mol.angles.shape[0]
+        t.angl_atoms = ptr(mol.angles, np.int32)
+        t.angl_keq = ptr(mol.angl_k, np.float64)
+        t.angl_theta0 = ptr(mol.angl_theta0, np.float64)
+        t.ndihe = mol.dihedrals.shape[0]
+        t.dihe_atoms = ptr(mol.dihedrals, np.int32)
+        t.dihe_amp = ptr(mol.dihe_amp, np.float64)
+        t.dihe_freq = ptr(mol.dihe_freq, np.float64)
+        t.dihe_phase = ptr(mol.dihe_phase, np.float64)
+        scee = getattr(mol, "dihe_scee_array", None)
+        scnb = getattr(mol, "dihe_scnb_array", None)
+        has14 = np.asarray(mol.dihe_has14, dtype=bool)
+        if scee is None:
+            scee = np.where(has14, mol.scee, 0.0)
+        if scnb is None:
+            scnb = np.where(has14, mol.scnb, 0.0)
+        t.dihe_scee = ptr(scee, np.float64)
+        t.dihe_scnb = ptr(scnb, np.float64)
+        impr = getattr(mol, "dihe_improper", None)
+        t.dihe_improper = ptr(impr, np.int32) if impr is not None else None
+        self.struct = t
+
+
+class Synthesis:
+    """A batch of molecules resident on the GPU (STORMM's AtomGraphSynthesis +
+    PhaseSpaceSynthesis + ImplicitSolventWorkspace + ScoreCard for this path)."""
+
+    def __init__(self, molecules, topology_index=None, options: Options | None = None, **opts):
+        lib = library()
+        mols = list(molecules)
+        if topology_index is None:
+            topology_index = np.arange(len(mols), dtype=np.int32)
+        self.topology_index = np.ascontiguousarray(topology_index, dtype=np.int32)
+        self._tops = [_TopologyArrays(m) for m in mols]
+        arr = (Topology * len(mols))(*[t.struct for t in self._tops])
+        o = options if options is not None else default_options(**opts)
+        handle = ctypes.c_void_p()
+        _check(lib.sb_synthesis_create(arr, len(mols), self.topology_index.ctypes.data,
+                                       len(self.topology_index), ctypes.byref(o),
+                                       ctypes.byref(handle)), "sb_synthesis_create")
+        self.handle = handle
+        self.nsys = len(self.topology_index)
+        self.natoms = np.array([mols[t].natom for t in self.topology_index], dtype=np.int64)
+        self.total_atoms = int(self.natoms.sum())
+        self.offsets = np.concatenate([[0], np.cumsum(self.natoms)])
+
+    def close(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            library().sb_synthesis_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # transfers -----------------------------------------------------------------------------
+    def set_coordinates(self, xyz, stream=None):
+        a = np.ascontiguousarray(np.asarray(xyz, dtype=np.float64).reshape(-1))
+        if a.size != 3 * self.total_atoms:
+            raise ValueError("coordinate array does not match the synthesis atom count")
+        _check(library().sb_set_coordinates(self.handle, a.ctypes.data, stream),
+               "sb_set_coordinates")
+
+    def coordinates(self, stream=None):
+        out = np.zeros(3 * self.total_atoms)
+        _check(library().sb_get_coordinates(self.handle, out.ctypes.data, stream),
+               "sb_get_coordinates")
+        return out.reshape(-1, 3)
+
+    def forces(self, stream=None):
+        out = np.zeros(3 * self.total_atoms)
+        _check(library().sb_get_forces(self.handle, out.ctypes.data, stream), "sb_get_forces")
+        return out.reshape(-1, 3)
+
+    def energies(self, stream=None):
+        out = np.zeros(self.nsys * NRG_STRIDE)
+        _check(library().sb_get_energies(self.handle, out.ctypes.data, stream),
+               "sb_get_energies")
+        return out.reshape(self.nsys, NRG_STRIDE)
+
+    def energy_terms(self, stream=None):
+        """Per system, the nine terms in TERM_ORDER."""
+        e = self.energies(stream)
+        return e[:, [NRG_SLOTS[n] for n in TERM_ORDER]]
+
+    def gb_workspace(self, stream=None):
+        psi = np.zeros(self.total_atoms)
+        rad = np.zeros(self.total_atoms)
+        sde = np.zeros(self.total_atoms)
+        _check(library().sb_get_gb_workspace(self.handle, psi.ctypes.data, rad.ctypes.data,
+                                             sde.ctypes.data, stream), "sb_get_gb_workspace")
+        return psi, rad, sde
+
+    def forces_fixed(self, stream=None):
+        n = library().sb_padded_atom_count(self.handle)
+        prim = np.zeros(3 * n, dtype=np.int64)
+        ovrf = np.zeros(3 * n, dtype=np.int32)
+        _check(library().sb_get_forces_fixed(self.handle, prim.ctypes.data, ovrf.ctypes.data,
+                                             stream), "sb_get_forces_fixed")
+        return prim.reshape(3, n), ovrf.reshape(3, n)
+
+    def energies_fixed(self, stream=None):
+        out = np.zeros(self.nsys * NRG_STRIDE, dtype=np.int64)
+        _check(library().sb_get_energies_fixed(self.handle, out.ctypes.data, stream),
+               "sb_get_energies_fixed")
+        return out.reshape(self.nsys, NRG_STRIDE)
+
+    # evaluation ----------------------------------------------------------------------------
+    def initialize(self, what=INIT_FORCES | INIT_ENERGIES | INIT_GB_WORKSPACE, stream=None):
+        _check(library().sb_initialize(self.handle, what, stream), "sb_initialize")
+
+    def evaluate(self, terms=TERM_ALL, force=True, energy=True, stream=None):
+        _check(library().sb_evaluate(self.handle, terms, int(force), int(energy), stream),
+               "sb_evaluate")
+
+    def evaluate_range(self, first, count, terms=TERM_ALL, force=True, energy=True,
+                       stream=None):
+        _check(library().sb_evaluate_range(self.handle, first, count, terms, int(force),
+                                           int(energy), stream), "sb_evaluate_range")
+
+    def launch_nonbonded(self, force=True, energy=True, stream=None):
+        _check(library().sb_launch_nonbonded(self.handle, int(force), int(energy), stream),
+               "sb_launch_nonbonded")
+
+    def launch_valence(self, force=True, energy=True, stream=None):
+        _check(library().sb_launch_valence(self.handle, int(force), int(energy), stream),
+               "sb_launch_valence")
+
+    def launch_info(self):
+        u, b, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(library().sb_launch_info(self.handle, ctypes.byref(u), ctypes.byref(b),
+                                        ctypes.byref(t)), "sb_launch_info")
+        return {"work_units": u.value, "blocks": b.value, "threads": t.value}
+
+    def status(self):
+        st = ctypes.c_int()
+        _check(library().sb_check_status(self.handle, ctypes.byref(st)), "sb_check_status")
+        return st.value
+
+    def split(self, per_atom):
+        """Split a per-atom array of the whole synthesis into per-system arrays."""
+        return [per_atom[self.offsets[k]:self.offsets[k + 1]] for k in range(self.nsys)]

@@ -1,0 +1,61 @@
+"""In-tree build of the native libraries.
+
+* libstormm_b200.so        the CUDA path (csrc/*.cu) for sm_100a, C ABI in include/stormm_b200.h
+* libstormm_b200_synth.so  the seeded synthetic-molecule builder (csrc/synthetic.cpp)
+
+Run ``python -m stormm_b200.build`` (or __graft_entry__.build()).  nvcc cross-compiles without
+a GPU.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+INCLUDE = os.path.join(ROOT, "include")
+LIB = os.path.join(PKG, "libstormm_b200.so")
+SYNTH_LIB = os.path.join(PKG, "libstormm_b200_synth.so")
+
+CUDA_SOURCES = ["eval_fused.cu", "synthesis.cu"]
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+    "-Xcompiler", "-fPIC", "-shared", "-Xptxas", "-v",
+]
+
+
+def _nvcc():
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if cand and (os.path.exists(cand) or cand == "nvcc"):
+            return cand
+    return "nvcc"
+
+
+def _stale(target, sources):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(s) > t for s in sources)
+
+
+def build(force: bool = False, verbose: bool = False) -> None:
+    srcs = [os.path.join(CSRC, s) for s in CUDA_SOURCES]
+    deps = srcs + [os.path.join(CSRC, h) for h in os.listdir(CSRC)
+                   if h.endswith((".h", ".cuh"))] + [os.path.join(INCLUDE, "stormm_b200.h")]
+    if force or _stale(LIB, deps):
+        cmd = [_nvcc()] + NVCC_FLAGS + ["-I", INCLUDE, "-I", CSRC, "-o", LIB] + srcs
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if verbose or r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+        if r.returncode != 0:
+            raise RuntimeError("nvcc build of libstormm_b200.so failed")
+    synth_src = os.path.join(CSRC, "synthetic.cpp")
+    if force or _stale(SYNTH_LIB, [synth_src]):
+        cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-o", SYNTH_LIB, synth_src]
+        subprocess.run(cmd, check=True)
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)

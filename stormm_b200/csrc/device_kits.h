@@ -1,0 +1,110 @@
+// Device-side views of a synthesis, passed by value to the kernels.  These are internal to the
+// library: the C ABI (include/stormm_b200.h) exposes handles, not these layouts.
+//
+// Layout in HBM (structure of arrays, every system's first atom on a multiple of 32):
+//   coordinates  int64 x/y/z, fixed point with gpos_bits fraction bits (STORMM's
+//                PhaseSpaceSynthesis, Synthesis/phasespace_synthesis.h:87-197), int32 overflow
+//   forces       int64 x/y/z with frc_bits fraction bits + int32 overflow (int95 format,
+//                Numerics/split_fixed_precision.h:30-34)
+//   energies     int64 per system per StateVariable slot, nrg_bits fraction bits
+//   per-atom     charge * sqrt(Coulomb constant), LJ type, offset GB radius rho = r_pb - 0.09,
+//   parameters   screened radius s*rho, OBC alpha/beta/gamma, intrinsic radius r_pb
+//   valence      16-byte records (uint4) with 16-bit system-local atom indices
+//   exclusions   one 32 x 32 bit mask per tile of a system that holds an exclusion
+#ifndef STORMM_B200_DEVICE_KITS_H
+#define STORMM_B200_DEVICE_KITS_H
+
+#include <cstdint>
+#include <vector_types.h>
+
+namespace sb {
+
+constexpr int kTile = 32;                 // atoms per tile edge (one warp lane per atom)
+constexpr int kMaxUnitSystems = 32;       // systems per fused work unit
+constexpr int kNrgStride = 16;            // energy slots per system (STORMM StateVariable order)
+constexpr float kGbRadiiOffset = 0.09f;   // Constants/generalized_born.h:114
+constexpr float kGbKscale = 0.73f;        // Constants/generalized_born.h:123
+constexpr int kPsiBits = 29;              // fixed-point bits of the in-block psi accumulators
+constexpr int kDeijdaBits = 23;           // fixed-point bits of the in-block dE/dR accumulators
+
+// Energy slots (Potential/energy_enumerators.h:36-50)
+enum NrgSlot : int {
+  kBond = 0, kAngle = 1, kProperDihedral = 2, kImproperDihedral = 3, kVdw = 7, kVdw14 = 8,
+  kElec = 9, kElec14 = 10, kGb = 11
+};
+
+// Bond record:     x = i | j << 16, y = keq (float bits), z = leq (float bits), w = 0
+// Angle record:    x = i | j << 16, y = k, z = keq, w = theta0
+// Dihedral record: a.x = i | j << 16, a.y = k | l << 16, a.z = amp, a.w = phase
+//                  b.x = freq, b.y = 1/scee (0: no 1-4), b.z = 1/scnb, b.w = flags (1: improper)
+struct DevSynthesis {
+  int nsys;
+  int natom_padded;
+  int igb;                       // 0 none, 1 HCT, 2 OBC, 5 OBC-II
+  float kappa;                   // Debye-Hueckel kappa from the salt concentration
+  float inv_dielectric;
+  float frc_scale;               // 2^frc_bits
+  float nrg_scale;               // 2^nrg_bits
+  double inv_gpos_scale;         // 2^-gpos_bits
+  double psi_out_scale;          // 2^24, ImplicitSolventWorkspace's single-precision fp_bits
+
+  // per system
+  const int* atom_start;
+  const int* atom_count;
+  const int* bond_start;         // CSR over systems (nsys + 1)
+  const int* angl_start;
+  const int* dihe_start;
+  const int* lj_start;           // offset of the system's LJ table in ljab
+  const int* lj_ntypes;
+  const int* tile_start;         // offset of the system's tile-mask index list
+
+  // per atom
+  const long long* xcrd;
+  const long long* ycrd;
+  const long long* zcrd;
+  long long* xfrc;
+  long long* yfrc;
+  long long* zfrc;
+  int* xfrc_ovrf;
+  int* yfrc_ovrf;
+  int* zfrc_ovrf;
+  const float* charge;           // q * sqrt(Coulomb constant)
+  const int* lj_idx;
+  const float* rho;              // r_pb - 0.09
+  const float* srho;             // screen * rho
+  const float* pb_radii;
+  const float* gb_alpha;
+  const float* gb_beta;
+  const float* gb_gamma;
+
+  // tables
+  const float2* ljab;            // (A, B) per type pair
+  const float2* ljab14;
+  const uint4* bonds;
+  const uint4* angles;
+  const uint4* dihe_a;
+  const uint4* dihe_b;
+  const int* tile_mask_idx;      // per system tile, 0: no exclusions, else index into mask_pool
+  const unsigned int* mask_pool; // 32 rows per mask: row = i lane, bit = j lane
+
+  // outputs
+  unsigned long long* energies;  // nsys * kNrgStride, int64 two's complement
+  long long* psi;                // ImplicitSolventWorkspace psi (fixed, 2^24)
+  int* psi_ovrf;
+  long long* sumdeijda;
+  int* sumdeijda_ovrf;
+  float* born_radii;             // effective radii of the last evaluation
+
+  // work units: consecutive entries of unit_systems, described by unit_desc
+  int nunit;
+  const int4* unit_desc;         // x = first index in unit_systems, y = system count,
+                                 // z = atom slots (sum of padded sizes), w = tile count
+  const int* unit_systems;
+  int max_unit_slots;
+
+  int* status;                   // device status word (0 = fine)
+};
+
+}  // namespace sb
+
+#endif

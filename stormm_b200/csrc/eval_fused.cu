@@ -1,0 +1,981 @@
+// Fused batched evaluation of valence, Coulomb + Lennard-Jones and Generalized Born terms.
+//
+// One thread block evaluates one work unit at a time: a group of whole molecules whose atoms
+// fit in shared memory.  Everything a molecule needs stays on chip for the whole evaluation:
+//
+//   stage       int64 fixed-point coordinates -> (hi, lo) float pairs, per-atom parameters,
+//               per-molecule Lennard-Jones tables
+//   valence     bonds, angles, dihedrals and their attached 1-4 pairs
+//               (Potential/valence_potential.tpp:9-1420 restated for FP32)
+//   GB pass 1   Born-radius descreening sums psi_i over all pairs, both directions
+//               (Potential/nonbonded_potential.tpp:511-728)
+//   radii       effective radii, GB self energy and its dE/dR (nonbonded_potential.tpp:730-805)
+//   pass 2      Coulomb + Lennard-Jones on non-excluded pairs, GB pair energy and force, dE/dR
+//               sums (nonbonded_potential.tpp:8-425, 808-975)
+//   chain rule  OBC prefactor on dE/dR (nonbonded_potential.tpp:982-1021)
+//   pass 3      radius chain-rule forces (nonbonded_potential.tpp:1022-1290)
+//   commit      forces into the int64 + int32-overflow arrays, energies into per-system slots
+//
+// Pair passes walk 32 x 32 tiles of a molecule's lower triangle, one tile per warp.  Lane l
+// holds atom i = I*32 + l in registers; j atoms rotate through the lanes (lane l meets atom
+// (l + k) mod 32 of block J at step k) and j-side accumulators travel with a shuffle per step.
+// Diagonal tiles take 16 steps, the last one on half the lanes, so every pair is visited once.
+// Forces, psi and dE/dR leave registers once per tile through integer shared-memory atomics,
+// so every sum is independent of scheduling and the results are bit-identical run to run.
+#include <cuda_runtime.h>
+
+#include "device_kits.h"
+#include "fixed_point.cuh"
+
+namespace sb {
+
+namespace {
+
+// Constants/generalized_born.h:21-44 (Taylor series of the HCT integral at long range)
+__device__ __constant__ float kTaylorA = 0.33333333333333333333f;
+__device__ __constant__ float kTaylorB = 0.4f;
+__device__ __constant__ float kTaylorC = 0.42857142857142857143f;
+__device__ __constant__ float kTaylorD = 0.44444444444444444444f;
+__device__ __constant__ float kTaylorDD = 0.45454545454545454545f;
+__device__ __constant__ float kTaylorE = 1.33333333333333333333f;
+__device__ __constant__ float kTaylorF = 2.4f;
+__device__ __constant__ float kTaylorG = 3.42857142857142857143f;
+__device__ __constant__ float kTaylorH = 4.44444444444444444444f;
+__device__ __constant__ float kTaylorHH = 5.45454545454545454545f;
+
+constexpr unsigned kFullMask = 0xffffffffu;
+
+// HCT descreening of an atom of offset radius rho by a neighbour of screened radius sj at
+// distance r; returns the amount psi decreases by.
+__device__ __forceinline__ float hctIntegral(float r, float r2, float invr, float rho, float sj) {
+  const float sj2 = sj * sj;
+  if (r > 4.0f * sj) {
+    const float invr2 = invr * invr;
+    const float t = sj2 * invr2;
+    const float dumbo = kTaylorA + t * (kTaylorB + t * (kTaylorC + t * (kTaylorD + t * kTaylorDD)));
+    return sj * t * invr2 * dumbo;
+  }
+  if (r > rho + sj) {
+    return 0.5f * (sj / (r2 - sj2) + 0.5f * invr * logf((r - sj) / (r + sj)));
+  }
+  if (r > fabsf(rho - sj)) {
+    const float inv_rho = 1.0f / rho;
+    const float theta = 0.5f * inv_rho * invr * (r2 + rho * rho - sj2);
+    const float uij = 1.0f / (r + sj);
+    return 0.25f * (inv_rho * (2.0f - theta) - uij + invr * logf(rho * uij));
+  }
+  if (rho < sj) {
+    return 0.5f * (sj / (r2 - sj2) + 2.0f / rho + 0.5f * invr * logf((sj - r) / (sj + r)));
+  }
+  return 0.0f;
+}
+
+// Radial derivative of hctIntegral divided by r
+__device__ __forceinline__ float hctDerivative(float r, float r2, float invr, float rho,
+                                               float sj) {
+  const float invr2 = invr * invr;
+  const float sj2 = sj * sj;
+  if (r > 4.0f * sj) {
+    const float t = sj2 * invr2;
+    const float dumbo = kTaylorE + t * (kTaylorF + t * (kTaylorG + t * (kTaylorH + t * kTaylorHH)));
+    return t * sj * invr2 * invr2 * dumbo;
+  }
+  if (r > rho + sj) {
+    const float temp1 = 1.0f / (r2 - sj2);
+    return temp1 * sj * (-0.5f * invr2 + temp1) + 0.25f * invr * invr2 * logf((r - sj) / (r + sj));
+  }
+  if (r > fabsf(rho - sj)) {
+    const float temp1 = 1.0f / (r + sj);
+    const float invr3 = invr2 * invr;
+    const float inv_rho = 1.0f / rho;
+    return -0.25f * (-0.5f * (r2 - rho * rho + sj2) * invr3 * inv_rho * inv_rho +
+                     invr * temp1 * (temp1 - invr) - invr3 * logf(rho * temp1));
+  }
+  if (rho < sj) {
+    const float temp1 = 1.0f / (r2 - sj2);
+    return -0.5f * (sj * invr2 * temp1 - 2.0f * sj * temp1 * temp1 -
+                    0.5f * invr2 * invr * logf((sj - r) / (sj + r)));
+  }
+  return 0.0f;
+}
+
+// Shared-memory layout of one work unit
+struct UnitSmem {
+  float4* hi;       // x, y, z (high parts), charge
+  float4* lo;       // x, y, z (low parts), Lennard-Jones code (int bits)
+  float4* gb;       // rho, s*rho, effective radius, dE/dR after the chain rule
+  int* fx;          // int63 force accumulators: primary
+  int* fy;
+  int* fz;
+  int* fxo;         // overflow
+  int* fyo;
+  int* fzo;
+  int* psi;         // int63 psi accumulator, 2^kPsiBits
+  int* psio;
+  int* de;          // int63 dE/dR accumulator, 2^kDeijdaBits
+  int* deo;
+  float2* lj;       // Lennard-Jones tables of the unit's molecules
+  unsigned long long* nrg;   // per unit molecule energies
+  int* sys;         // molecule index
+  int* slot0;       // first slot of the molecule
+  int* natom;
+  int* tile0;       // prefix sum of tile counts (kMaxUnitSystems + 1)
+  int* ljbase;
+  int* bond0;       // prefix sums of valence term counts (kMaxUnitSystems + 1)
+  int* angl0;
+  int* dihe0;
+};
+
+__host__ __device__ inline size_t alignUp(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+}  // namespace
+
+// Dynamic shared memory needed for a work unit of max_slots atom slots and max_lj table entries
+size_t fusedSmemBytes(int max_slots, int max_lj) {
+  size_t b = 0;
+  b += 3 * sizeof(float4) * max_slots;
+  b += 10 * sizeof(int) * max_slots;
+  b = alignUp(b, 16);
+  b += sizeof(float2) * max_lj;
+  b = alignUp(b, 16);
+  b += sizeof(unsigned long long) * kMaxUnitSystems * kNrgStride;
+  b += sizeof(int) * (9 * kMaxUnitSystems + 8);
+  return b;
+}
+
+namespace {
+
+__device__ UnitSmem carveSmem(char* base, int max_slots, int max_lj) {
+  UnitSmem s;
+  size_t off = 0;
+  s.hi = reinterpret_cast<float4*>(base + off); off += sizeof(float4) * max_slots;
+  s.lo = reinterpret_cast<float4*>(base + off); off += sizeof(float4) * max_slots;
+  s.gb = reinterpret_cast<float4*>(base + off); off += sizeof(float4) * max_slots;
+  int* ip = reinterpret_cast<int*>(base + off);
+  s.fx = ip; ip += max_slots;
+  s.fy = ip; ip += max_slots;
+  s.fz = ip; ip += max_slots;
+  s.fxo = ip; ip += max_slots;
+  s.fyo = ip; ip += max_slots;
+  s.fzo = ip; ip += max_slots;
+  s.psi = ip; ip += max_slots;
+  s.psio = ip; ip += max_slots;
+  s.de = ip; ip += max_slots;
+  s.deo = ip; ip += max_slots;
+  off = alignUp(off + 10 * sizeof(int) * max_slots, 16);
+  s.lj = reinterpret_cast<float2*>(base + off); off += sizeof(float2) * max_lj;
+  off = alignUp(off, 16);
+  s.nrg = reinterpret_cast<unsigned long long*>(base + off);
+  off += sizeof(unsigned long long) * kMaxUnitSystems * kNrgStride;
+  int* q = reinterpret_cast<int*>(base + off);
+  s.sys = q; q += kMaxUnitSystems;
+  s.slot0 = q; q += kMaxUnitSystems;
+  s.natom = q; q += kMaxUnitSystems;
+  s.ljbase = q; q += kMaxUnitSystems;
+  s.tile0 = q; q += kMaxUnitSystems + 1;
+  s.bond0 = q; q += kMaxUnitSystems + 1;
+  s.angl0 = q; q += kMaxUnitSystems + 1;
+  s.dihe0 = q; q += kMaxUnitSystems + 1;
+  return s;
+}
+
+// Index of the unit molecule that owns position pos of a prefix-sum array of n + 1 entries
+__device__ __forceinline__ int findOwner(const int* prefix, int n, int pos) {
+  int k = 0;
+  while (k + 1 < n && prefix[k + 1] <= pos) {
+    k++;
+  }
+  return k;
+}
+
+// Tile (I, J), I >= J, of the lower triangle from its index within the molecule
+__device__ __forceinline__ void tileCoordinates(int local, int* ti, int* tj) {
+  int i = static_cast<int>((sqrtf(8.0f * local + 1.0f) - 1.0f) * 0.5f);
+  while (i * (i + 1) / 2 > local) i--;
+  while ((i + 1) * (i + 2) / 2 <= local) i++;
+  *ti = i;
+  *tj = local - i * (i + 1) / 2;
+}
+
+__device__ __forceinline__ float3 pairDelta(const float4 hi_i, const float4 lo_i, const float4 hi_j,
+                                            const float4 lo_j) {
+  return make_float3((hi_j.x - hi_i.x) + (lo_j.x - lo_i.x), (hi_j.y - hi_i.y) + (lo_j.y - lo_i.y),
+                     (hi_j.z - hi_i.z) + (lo_j.z - lo_i.z));
+}
+
+__device__ __forceinline__ void addForce(const UnitSmem &s, int slot, float fx, float fy, float fz,
+                                         float scale) {
+  atomicAddInt63(fx * scale, &s.fx[slot], &s.fxo[slot]);
+  atomicAddInt63(fy * scale, &s.fy[slot], &s.fyo[slot]);
+  atomicAddInt63(fz * scale, &s.fz[slot], &s.fzo[slot]);
+}
+
+__device__ __forceinline__ void addEnergy(const UnitSmem &s, int k, int slot, float e,
+                                          float scale) {
+  atomicAdd(&s.nrg[k * kNrgStride + slot],
+            static_cast<unsigned long long>(__float2ll_rn(e * scale)));
+}
+
+// Warp-wide int64 sum, result in every lane
+__device__ __forceinline__ long long warpSum(long long v) {
+  for (int o = 16; o > 0; o >>= 1) {
+    v += __shfl_xor_sync(kFullMask, v, o);
+  }
+  return v;
+}
+
+// Coordinate difference from the hi / lo representation of two atoms held in shared memory
+__device__ __forceinline__ float3 slotDelta(const UnitSmem &s, int a, int b) {
+  return pairDelta(s.hi[a], s.lo[a], s.hi[b], s.lo[b]);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Valence terms (Potential/valence_potential.tpp)
+// ------------------------------------------------------------------------------------------------
+template <bool FORCE, bool ENERGY>
+__device__ void valenceTerms(const DevSynthesis &d, const UnitSmem &s, int nsys_u) {
+  const float fs = d.frc_scale;
+  const float es = d.nrg_scale;
+  // bonds, valence_potential.tpp:9-97
+  const int nbond = s.bond0[nsys_u];
+  for (int f = threadIdx.x; f < nbond; f += blockDim.x) {
+    const int k = findOwner(s.bond0, nsys_u, f);
+    const uint4 rec = d.bonds[d.bond_start[s.sys[k]] + (f - s.bond0[k])];
+    const int ia = s.slot0[k] + static_cast<int>(rec.x & 0xffffu);
+    const int ja = s.slot0[k] + static_cast<int>(rec.x >> 16);
+    const float keq = __uint_as_float(rec.y);
+    const float leq = __uint_as_float(rec.z);
+    const float3 dv = slotDelta(s, ia, ja);
+    const float r = sqrtf(dv.x * dv.x + dv.y * dv.y + dv.z * dv.z);
+    const float dl = r - leq;
+    if (FORCE) {
+      const float fmag = 2.0f * keq * dl / r;
+      addForce(s, ia, fmag * dv.x, fmag * dv.y, fmag * dv.z, fs);
+      addForce(s, ja, -fmag * dv.x, -fmag * dv.y, -fmag * dv.z, fs);
+    }
+    if (ENERGY) {
+      addEnergy(s, k, kBond, keq * dl * dl, es);
+    }
+  }
+  // angles, valence_potential.tpp:170-288
+  const int nangl = s.angl0[nsys_u];
+  for (int f = threadIdx.x; f < nangl; f += blockDim.x) {
+    const int k = findOwner(s.angl0, nsys_u, f);
+    const uint4 rec = d.angles[d.angl_start[s.sys[k]] + (f - s.angl0[k])];
+    const int ia = s.slot0[k] + static_cast<int>(rec.x & 0xffffu);
+    const int ja = s.slot0[k] + static_cast<int>(rec.x >> 16);
+    const int ka = s.slot0[k] + static_cast<int>(rec.y);
+    const float keq = __uint_as_float(rec.z);
+    const float th0 = __uint_as_float(rec.w);
+    const float3 ba = slotDelta(s, ja, ia);
+    const float3 bc = slotDelta(s, ja, ka);
+    const float mgba = ba.x * ba.x + ba.y * ba.y + ba.z * ba.z;
+    const float mgbc = bc.x * bc.x + bc.y * bc.y + bc.z * bc.z;
+    const float invbabc = 1.0f / sqrtf(mgba * mgbc);
+    float costheta = (ba.x * bc.x + ba.y * bc.y + ba.z * bc.z) * invbabc;
+    costheta = fminf(fmaxf(costheta, -1.0f), 1.0f);
+    const float dtheta = acosf(costheta) - th0;
+    if (FORCE) {
+      const float dA = -2.0f * keq * dtheta / sqrtf(1.0f - costheta * costheta);
+      const float sqba = dA / mgba;
+      const float sqbc = dA / mgbc;
+      const float mbabc = dA * invbabc;
+      const float adx = bc.x * mbabc - costheta * ba.x * sqba;
+      const float ady = bc.y * mbabc - costheta * ba.y * sqba;
+      const float adz = bc.z * mbabc - costheta * ba.z * sqba;
+      const float cdx = ba.x * mbabc - costheta * bc.x * sqbc;
+      const float cdy = ba.y * mbabc - costheta * bc.y * sqbc;
+      const float cdz = ba.z * mbabc - costheta * bc.z * sqbc;
+      addForce(s, ia, -adx, -ady, -adz, fs);
+      addForce(s, ja, adx + cdx, ady + cdy, adz + cdz, fs);
+      addForce(s, ka, -cdx, -cdy, -cdz, fs);
+    }
+    if (ENERGY) {
+      addEnergy(s, k, kAngle, keq * dtheta * dtheta, es);
+    }
+  }
+  // dihedrals with attached 1-4 pairs, valence_potential.tpp:359-578, 1288-1420
+  const int ndihe = s.dihe0[nsys_u];
+  for (int f = threadIdx.x; f < ndihe; f += blockDim.x) {
+    const int k = findOwner(s.dihe0, nsys_u, f);
+    const int pos = d.dihe_start[s.sys[k]] + (f - s.dihe0[k]);
+    const uint4 ra = d.dihe_a[pos];
+    const uint4 rb = d.dihe_b[pos];
+    const int ia = s.slot0[k] + static_cast<int>(ra.x & 0xffffu);
+    const int ja = s.slot0[k] + static_cast<int>(ra.x >> 16);
+    const int ka = s.slot0[k] + static_cast<int>(ra.y & 0xffffu);
+    const int la = s.slot0[k] + static_cast<int>(ra.y >> 16);
+    const float amp = __uint_as_float(ra.z);
+    const float phase = __uint_as_float(ra.w);
+    const float freq = __uint_as_float(rb.x);
+    const float3 ab = slotDelta(s, ia, ja);
+    const float3 bc = slotDelta(s, ja, ka);
+    const float3 cd = slotDelta(s, ka, la);
+    float3 crabbc = make_float3(ab.y * bc.z - ab.z * bc.y, ab.z * bc.x - ab.x * bc.z,
+                                ab.x * bc.y - ab.y * bc.x);
+    float3 crbccd = make_float3(bc.y * cd.z - bc.z * cd.y, bc.z * cd.x - bc.x * cd.z,
+                                bc.x * cd.y - bc.y * cd.x);
+    const float m1 = crabbc.x * crabbc.x + crabbc.y * crabbc.y + crabbc.z * crabbc.z;
+    const float m2 = crbccd.x * crbccd.x + crbccd.y * crbccd.y + crbccd.z * crbccd.z;
+    float costheta = (crabbc.x * crbccd.x + crabbc.y * crbccd.y + crabbc.z * crbccd.z) /
+                     sqrtf(m1 * m2);
+    const float3 scr = make_float3(crabbc.y * crbccd.z - crabbc.z * crbccd.y,
+                                   crabbc.z * crbccd.x - crabbc.x * crbccd.z,
+                                   crabbc.x * crbccd.y - crabbc.y * crbccd.x);
+    costheta = fminf(fmaxf(costheta, -1.0f), 1.0f);
+    // signed angle; near 0 or pi take the arcsine route (Math/rounding.tpp:25-80)
+    const float sgn = (scr.x * bc.x + scr.y * bc.y + scr.z * bc.z > 0.0f) ? 1.0f : -1.0f;
+    float theta;
+    if (fabsf(costheta) >= 0.99993896484375f) {
+      const float ia1 = rsqrtf(m1);
+      const float ib1 = rsqrtf(m2);
+      float rx = crbccd.x * ib1 - crabbc.x * ia1;
+      float ry = crbccd.y * ib1 - crabbc.y * ia1;
+      float rz = crbccd.z * ib1 - crabbc.z * ia1;
+      float rs = sqrtf(rx * rx + ry * ry + rz * rz);
+      if (rs > 1.0f) {
+        rx = crbccd.x * ib1 + crabbc.x * ia1;
+        ry = crbccd.y * ib1 + crabbc.y * ia1;
+        rz = crbccd.z * ib1 + crabbc.z * ia1;
+        rs = 3.14159265358979323846f - sqrtf(rx * rx + ry * ry + rz * rz);
+      }
+      theta = sgn * rs;
+    }
+    else {
+      theta = sgn * acosf(costheta);
+    }
+    const float sangle = freq * theta - phase;
+    if (FORCE) {
+      const float fr = amp * freq * sinf(sangle);
+      const float mgab = sqrtf(ab.x * ab.x + ab.y * ab.y + ab.z * ab.z);
+      const float mgbc = sqrtf(bc.x * bc.x + bc.y * bc.y + bc.z * bc.z);
+      const float mgcd = sqrtf(cd.x * cd.x + cd.y * cd.y + cd.z * cd.z);
+      const float invab = 1.0f / mgab;
+      const float invbc = 1.0f / mgbc;
+      const float invcd = 1.0f / mgcd;
+      const float cosb = -(ab.x * bc.x + ab.y * bc.y + ab.z * bc.z) * invab * invbc;
+      const float cosc = -(bc.x * cd.x + bc.y * cd.y + bc.z * cd.z) * invbc * invcd;
+      const float isinb2 = (cosb * cosb < 0.99999904632568359375f) ? fr / (1.0f - cosb * cosb) :
+                                                                      fr * 1048576.0f;
+      const float isinc2 = (cosc * cosc < 0.99999904632568359375f) ? fr / (1.0f - cosc * cosc) :
+                                                                      fr * 1048576.0f;
+      const float invabc = invab * invbc;
+      const float invbcd = invbc * invcd;
+      crabbc.x *= invabc;
+      crabbc.y *= invabc;
+      crabbc.z *= invabc;
+      crbccd.x *= invbcd;
+      crbccd.y *= invbcd;
+      crbccd.z *= invbcd;
+      const float fa = -invab * isinb2;
+      const float fb1 = (mgbc - mgab * cosb) * invabc * isinb2;
+      const float fb2 = cosc * invbc * isinc2;
+      const float fd = -invcd * isinc2;
+      const float fix = crabbc.x * fa, fiy = crabbc.y * fa, fiz = crabbc.z * fa;
+      const float fjx = fb1 * crabbc.x - fb2 * crbccd.x;
+      const float fjy = fb1 * crabbc.y - fb2 * crbccd.y;
+      const float fjz = fb1 * crabbc.z - fb2 * crbccd.z;
+      const float flx = -fd * crbccd.x, fly = -fd * crbccd.y, flz = -fd * crbccd.z;
+      addForce(s, ia, fix, fiy, fiz, fs);
+      addForce(s, ja, fjx, fjy, fjz, fs);
+      addForce(s, ka, -(fix + fjx + flx), -(fiy + fjy + fly), -(fiz + fjz + flz), fs);
+      addForce(s, la, flx, fly, flz, fs);
+    }
+    if (ENERGY) {
+      addEnergy(s, k, (rb.w & 1u) ? kImproperDihedral : kProperDihedral,
+                amp * (1.0f + cosf(sangle)), es);
+    }
+    // attached 1-4 pair between atoms i and l
+    const float inv_scee = __uint_as_float(rb.y);
+    if (inv_scee > 0.0f) {
+      const float inv_scnb = __uint_as_float(rb.z);
+      const float3 dv = slotDelta(s, ia, la);
+      const float4 hi_i = s.hi[ia];
+      const float4 hi_l = s.hi[la];
+      const int code_i = __float_as_int(s.lo[ia].w);
+      const int code_l = __float_as_int(s.lo[la].w);
+      // the 1-4 table of the molecule follows its standard table in shared memory
+      const int nt = d.lj_ntypes[s.sys[k]];
+      const float2 ab14 = s.lj[(code_i & 0xffff) + (code_l >> 16) + nt * nt];
+      const float lja = ab14.x * inv_scnb;
+      const float ljb = ab14.y * inv_scnb;
+      const float qiqj = hi_i.w * hi_l.w * inv_scee;
+      const float invr2 = 1.0f / (dv.x * dv.x + dv.y * dv.y + dv.z * dv.z);
+      const float invr = sqrtf(invr2);
+      const float invr4 = invr2 * invr2;
+      if (FORCE) {
+        const float fmag = -(qiqj * invr * invr2) +
+                           (6.0f * ljb - 12.0f * lja * invr4 * invr2) * invr4 * invr4;
+        addForce(s, ia, fmag * dv.x, fmag * dv.y, fmag * dv.z, fs);
+        addForce(s, la, -fmag * dv.x, -fmag * dv.y, -fmag * dv.z, fs);
+      }
+      if (ENERGY) {
+        addEnergy(s, k, kElec14, qiqj * invr, es);
+        addEnergy(s, k, kVdw14, lja * invr4 * invr4 * invr4 - ljb * invr4 * invr2, es);
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Tile walks
+// ------------------------------------------------------------------------------------------------
+struct TileInfo {
+  int k;        // unit molecule
+  int ibase;    // first slot of block I
+  int jbase;    // first slot of block J
+  int ni;       // valid atoms in block I
+  int nj;       // valid atoms in block J
+  bool diag;
+  int I, J;
+};
+
+__device__ __forceinline__ TileInfo tileInfo(const UnitSmem &s, int nsys_u, int t) {
+  TileInfo ti;
+  ti.k = findOwner(s.tile0, nsys_u, t);
+  tileCoordinates(t - s.tile0[ti.k], &ti.I, &ti.J);
+  const int n = s.natom[ti.k];
+  ti.ibase = s.slot0[ti.k] + ti.I * kTile;
+  ti.jbase = s.slot0[ti.k] + ti.J * kTile;
+  ti.ni = min(kTile, n - ti.I * kTile);
+  ti.nj = min(kTile, n - ti.J * kTile);
+  ti.diag = (ti.I == ti.J);
+  return ti;
+}
+
+// GB pass 1: psi_i -= H(r, rho_i, s_j rho_j) and psi_j -= H(r, rho_j, s_i rho_i) for every pair
+__device__ void gbRadiiTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u, int ntiles) {
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwarp = blockDim.x >> 5;
+  const float ps = static_cast<float>(1 << kPsiBits);
+  for (int t = warp; t < ntiles; t += nwarp) {
+    const TileInfo ti = tileInfo(s, nsys_u, t);
+    const bool ivalid = lane < ti.ni;
+    const int islot = ti.ibase + lane;
+    const float4 hi_i = s.hi[islot];
+    const float4 lo_i = s.lo[islot];
+    const float4 gb_i = s.gb[islot];
+    float psi_i = 0.0f;
+    float psi_j = 0.0f;
+    const int kbeg = ti.diag ? 1 : 0;
+    const int kend = ti.diag ? 16 : 31;
+    for (int k = kbeg; k <= kend; k++) {
+      const int jl = (lane + k) & 31;
+      const int jslot = ti.jbase + jl;
+      const bool active = ivalid && (jl < ti.nj) && (!ti.diag || k < 16 || lane < 16);
+      if (active) {
+        const float4 hi_j = s.hi[jslot];
+        const float4 lo_j = s.lo[jslot];
+        const float4 gb_j = s.gb[jslot];
+        const float3 dv = pairDelta(hi_i, lo_i, hi_j, lo_j);
+        const float r2 = dv.x * dv.x + dv.y * dv.y + dv.z * dv.z;
+        const float r = sqrtf(r2);
+        const float invr = 1.0f / r;
+        psi_i -= hctIntegral(r, r2, invr, gb_i.x, gb_j.y);
+        psi_j -= hctIntegral(r, r2, invr, gb_j.x, gb_i.y);
+      }
+      psi_j = __shfl_sync(kFullMask, psi_j, (lane + 1) & 31);
+    }
+    if (ivalid) {
+      atomicAddInt63(psi_i * ps, &s.psi[islot], &s.psio[islot]);
+    }
+    const int jl_end = (lane + kend + 1) & 31;
+    if (jl_end < ti.nj) {
+      atomicAddInt63(psi_j * ps, &s.psi[ti.jbase + jl_end], &s.psio[ti.jbase + jl_end]);
+    }
+  }
+}
+
+// Pass 2: Coulomb + Lennard-Jones (non-excluded pairs) and GB pair terms
+template <bool FORCE, bool ENERGY, bool NB, bool GB>
+__device__ void pairTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u, int ntiles) {
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwarp = blockDim.x >> 5;
+  const float fs = d.frc_scale;
+  const float es = d.nrg_scale;
+  const float ds = static_cast<float>(1 << kDeijdaBits);
+  const float kappa = d.kappa;
+  const float inv_diel = d.inv_dielectric;
+  const float kk = -kappa * kGbKscale;
+  long long acc_elec = 0, acc_vdw = 0, acc_gb = 0;
+  int acc_k = -1;
+  for (int t = warp; t < ntiles; t += nwarp) {
+    const TileInfo ti = tileInfo(s, nsys_u, t);
+    if (ENERGY && ti.k != acc_k) {
+      if (acc_k >= 0) {
+        const long long se = warpSum(acc_elec), sv = warpSum(acc_vdw), sg = warpSum(acc_gb);
+        if (lane == 0) {
+          if (NB) {
+            atomicAdd(&s.nrg[acc_k * kNrgStride + kElec], static_cast<unsigned long long>(se));
+            atomicAdd(&s.nrg[acc_k * kNrgStride + kVdw], static_cast<unsigned long long>(sv));
+          }
+          if (GB) {
+            atomicAdd(&s.nrg[acc_k * kNrgStride + kGb], static_cast<unsigned long long>(sg));
+          }
+        }
+      }
+      acc_elec = acc_vdw = acc_gb = 0;
+      acc_k = ti.k;
+    }
+    const bool ivalid = lane < ti.ni;
+    const int islot = ti.ibase + lane;
+    const float4 hi_i = s.hi[islot];
+    const float4 lo_i = s.lo[islot];
+    const float4 gb_i = s.gb[islot];
+    const int code_i = __float_as_int(lo_i.w) & 0xffff;
+    unsigned int mask = 0u;
+    if (NB) {
+      const int midx = d.tile_mask_idx[d.tile_start[s.sys[ti.k]] + (t - s.tile0[ti.k])];
+      if (midx != 0) {
+        mask = __ldg(&d.mask_pool[static_cast<size_t>(midx) * 32 + lane]);
+      }
+    }
+    float fxi = 0.0f, fyi = 0.0f, fzi = 0.0f, dei = 0.0f;
+    float fxj = 0.0f, fyj = 0.0f, fzj = 0.0f, dej = 0.0f;
+    float e_elec = 0.0f, e_vdw = 0.0f, e_gb = 0.0f;
+    const int kbeg = ti.diag ? 1 : 0;
+    const int kend = ti.diag ? 16 : 31;
+    for (int k = kbeg; k <= kend; k++) {
+      const int jl = (lane + k) & 31;
+      const int jslot = ti.jbase + jl;
+      const bool active = ivalid && (jl < ti.nj) && (!ti.diag || k < 16 || lane < 16);
+      if (active) {
+        const float4 hi_j = s.hi[jslot];
+        const float4 lo_j = s.lo[jslot];
+        const float3 dv = pairDelta(hi_i, lo_i, hi_j, lo_j);
+        const float r2 = dv.x * dv.x + dv.y * dv.y + dv.z * dv.z;
+        const float qiqj = hi_i.w * hi_j.w;
+        float fmag = 0.0f;
+        if (NB && ((mask >> jl) & 1u) == 0u) {
+          const float invr2 = 1.0f / r2;
+          const float invr = sqrtf(invr2);
+          const float invr4 = invr2 * invr2;
+          const float2 ab = s.lj[code_i + (__float_as_int(lo_j.w) >> 16)];
+          if (ENERGY) {
+            e_elec += qiqj * invr;
+            e_vdw += (ab.x * invr4 * invr4 - ab.y * invr2) * invr4;
+          }
+          if (FORCE) {
+            fmag = -(qiqj * invr * invr2) +
+                   (6.0f * ab.y - 12.0f * ab.x * invr4 * invr2) * invr4 * invr4;
+          }
+        }
+        if (GB) {
+          const float4 gb_j = s.gb[jslot];
+          const float ijb = gb_i.z * gb_j.z;
+          const float efac = expf(-r2 / (4.0f * ijb));
+          const float fgbi = 1.0f / sqrtf(r2 + ijb * efac);
+          float expmkf, fgbk;
+          if (kappa > 0.0f) {
+            fgbk = kk / fgbi;
+            expmkf = expf(fgbk) * inv_diel;
+          }
+          else {
+            fgbk = 0.0f;
+            expmkf = inv_diel;
+          }
+          const float dielfac = 1.0f - expmkf;
+          if (ENERGY) {
+            e_gb -= qiqj * dielfac * fgbi;
+          }
+          if (FORCE) {
+            const float temp4 = fgbi * fgbi * fgbi;
+            const float temp6 = qiqj * temp4 * (dielfac + fgbk * expmkf);
+            fmag += temp6 * (1.0f - 0.25f * efac);
+            const float temp5 = 0.5f * efac * temp6 * (ijb + 0.25f * r2);
+            dei += gb_i.z * temp5;
+            dej += gb_j.z * temp5;
+          }
+        }
+        if (FORCE) {
+          fxi += fmag * dv.x;
+          fyi += fmag * dv.y;
+          fzi += fmag * dv.z;
+          fxj -= fmag * dv.x;
+          fyj -= fmag * dv.y;
+          fzj -= fmag * dv.z;
+        }
+      }
+      if (FORCE) {
+        const int src = (lane + 1) & 31;
+        fxj = __shfl_sync(kFullMask, fxj, src);
+        fyj = __shfl_sync(kFullMask, fyj, src);
+        fzj = __shfl_sync(kFullMask, fzj, src);
+        if (GB) {
+          dej = __shfl_sync(kFullMask, dej, src);
+        }
+      }
+    }
+    if (FORCE) {
+      if (ivalid) {
+        addForce(s, islot, fxi, fyi, fzi, fs);
+        if (GB) {
+          atomicAddInt63(dei * ds, &s.de[islot], &s.deo[islot]);
+        }
+      }
+      const int jl_end = (lane + kend + 1) & 31;
+      if (jl_end < ti.nj) {
+        const int js = ti.jbase + jl_end;
+        addForce(s, js, fxj, fyj, fzj, fs);
+        if (GB) {
+          atomicAddInt63(dej * ds, &s.de[js], &s.deo[js]);
+        }
+      }
+    }
+    if (ENERGY) {
+      acc_elec += __float2ll_rn(e_elec * es);
+      acc_vdw += __float2ll_rn(e_vdw * es);
+      acc_gb += __float2ll_rn(e_gb * es);
+    }
+  }
+  if (ENERGY) {
+    // every warp flushes (lanes agree on acc_k); warps without tiles flush zeros harmlessly
+    const long long se = warpSum(acc_elec), sv = warpSum(acc_vdw), sg = warpSum(acc_gb);
+    if (lane == 0 && acc_k >= 0) {
+      if (NB) {
+        atomicAdd(&s.nrg[acc_k * kNrgStride + kElec], static_cast<unsigned long long>(se));
+        atomicAdd(&s.nrg[acc_k * kNrgStride + kVdw], static_cast<unsigned long long>(sv));
+      }
+      if (GB) {
+        atomicAdd(&s.nrg[acc_k * kNrgStride + kGb], static_cast<unsigned long long>(sg));
+      }
+    }
+  }
+}
+
+// Pass 3: radius chain-rule forces
+__device__ void gbDerivativeTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u,
+                                  int ntiles) {
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwarp = blockDim.x >> 5;
+  const float fs = d.frc_scale;
+  for (int t = warp; t < ntiles; t += nwarp) {
+    const TileInfo ti = tileInfo(s, nsys_u, t);
+    const bool ivalid = lane < ti.ni;
+    const int islot = ti.ibase + lane;
+    const float4 hi_i = s.hi[islot];
+    const float4 lo_i = s.lo[islot];
+    const float4 gb_i = s.gb[islot];
+    float fxi = 0.0f, fyi = 0.0f, fzi = 0.0f;
+    float fxj = 0.0f, fyj = 0.0f, fzj = 0.0f;
+    const int kbeg = ti.diag ? 1 : 0;
+    const int kend = ti.diag ? 16 : 31;
+    for (int k = kbeg; k <= kend; k++) {
+      const int jl = (lane + k) & 31;
+      const int jslot = ti.jbase + jl;
+      const bool active = ivalid && (jl < ti.nj) && (!ti.diag || k < 16 || lane < 16);
+      if (active) {
+        const float4 hi_j = s.hi[jslot];
+        const float4 lo_j = s.lo[jslot];
+        const float4 gb_j = s.gb[jslot];
+        const float3 dv = pairDelta(hi_i, lo_i, hi_j, lo_j);
+        const float r2 = dv.x * dv.x + dv.y * dv.y + dv.z * dv.z;
+        const float r = sqrtf(r2);
+        const float invr = 1.0f / r;
+        const float fmag = hctDerivative(r, r2, invr, gb_i.x, gb_j.y) * gb_i.w +
+                           hctDerivative(r, r2, invr, gb_j.x, gb_i.y) * gb_j.w;
+        fxi -= fmag * dv.x;
+        fyi -= fmag * dv.y;
+        fzi -= fmag * dv.z;
+        fxj += fmag * dv.x;
+        fyj += fmag * dv.y;
+        fzj += fmag * dv.z;
+      }
+      const int src = (lane + 1) & 31;
+      fxj = __shfl_sync(kFullMask, fxj, src);
+      fyj = __shfl_sync(kFullMask, fyj, src);
+      fzj = __shfl_sync(kFullMask, fzj, src);
+    }
+    if (ivalid) {
+      addForce(s, islot, fxi, fyi, fzi, fs);
+    }
+    const int jl_end = (lane + kend + 1) & 31;
+    if (jl_end < ti.nj) {
+      addForce(s, ti.jbase + jl_end, fxj, fyj, fzj, fs);
+    }
+  }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------------
+// The fused kernel
+// ------------------------------------------------------------------------------------------------
+template <bool FORCE, bool ENERGY, int TERMS>
+__global__ void __launch_bounds__(256)
+kEvalFused(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
+  extern __shared__ __align__(16) char smem_raw[];
+  const UnitSmem s = carveSmem(smem_raw, d.max_unit_slots, max_lj);
+  constexpr bool VALE = (TERMS & 1) != 0;
+  constexpr bool NB = (TERMS & 2) != 0;
+  const bool gb = ((TERMS & 4) != 0) && (d.igb != 0);
+  for (int u = unit_begin + blockIdx.x; u < unit_end; u += gridDim.x) {
+    const int4 desc = d.unit_desc[u];
+    const int nsys_u = desc.y;
+    const int nslots = desc.z;
+    const int ntiles = desc.w;
+
+    // unit molecule table and prefix sums
+    if (threadIdx.x < nsys_u) {
+      const int sysid = d.unit_systems[desc.x + threadIdx.x];
+      s.sys[threadIdx.x] = sysid;
+      s.natom[threadIdx.x] = d.atom_count[sysid];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int slot = 0, tile = 0, lj = 0, nb = 0, na = 0, nd = 0;
+      for (int k = 0; k < nsys_u; k++) {
+        const int sysid = s.sys[k];
+        const int n = s.natom[k];
+        const int nblk = (n + kTile - 1) / kTile;
+        s.slot0[k] = slot;
+        s.tile0[k] = tile;
+        s.ljbase[k] = lj;
+        s.bond0[k] = nb;
+        s.angl0[k] = na;
+        s.dihe0[k] = nd;
+        slot += nblk * kTile;
+        tile += nblk * (nblk + 1) / 2;
+        const int nt = d.lj_ntypes[sysid];
+        lj += 2 * nt * nt;
+        nb += d.bond_start[sysid + 1] - d.bond_start[sysid];
+        na += d.angl_start[sysid + 1] - d.angl_start[sysid];
+        nd += d.dihe_start[sysid + 1] - d.dihe_start[sysid];
+      }
+      s.tile0[nsys_u] = tile;
+      s.bond0[nsys_u] = nb;
+      s.angl0[nsys_u] = na;
+      s.dihe0[nsys_u] = nd;
+      if (slot != nslots || tile != ntiles || lj > max_lj || slot > d.max_unit_slots) {
+        atomicOr(d.status, 1);
+      }
+    }
+    for (int e = threadIdx.x; e < nsys_u * kNrgStride; e += blockDim.x) {
+      s.nrg[e] = 0ull;
+    }
+    __syncthreads();
+    if (nslots > d.max_unit_slots) {
+      continue;   // reported through the status word; nothing in the unit is touched
+    }
+
+    // stage Lennard-Jones tables (standard then 1-4) of every molecule
+    for (int k = 0; k < nsys_u; k++) {
+      const int sysid = s.sys[k];
+      const int nt = d.lj_ntypes[sysid];
+      const int src = d.lj_start[sysid];
+      for (int e = threadIdx.x; e < nt * nt; e += blockDim.x) {
+        s.lj[s.ljbase[k] + e] = d.ljab[src + e];
+        s.lj[s.ljbase[k] + nt * nt + e] = d.ljab14[src + e];
+      }
+    }
+
+    // stage atoms
+    for (int slot = threadIdx.x; slot < nslots; slot += blockDim.x) {
+      const int k = findOwner(s.slot0, nsys_u, slot);
+      const int sysid = s.sys[k];
+      const int a = slot - s.slot0[k];
+      float4 hi, lo, g;
+      if (a < s.natom[k]) {
+        const int gi = d.atom_start[sysid] + a;
+        const double x = static_cast<double>(d.xcrd[gi]) * d.inv_gpos_scale;
+        const double y = static_cast<double>(d.ycrd[gi]) * d.inv_gpos_scale;
+        const double z = static_cast<double>(d.zcrd[gi]) * d.inv_gpos_scale;
+        hi.x = static_cast<float>(x);
+        hi.y = static_cast<float>(y);
+        hi.z = static_cast<float>(z);
+        hi.w = d.charge[gi];
+        lo.x = static_cast<float>(x - static_cast<double>(hi.x));
+        lo.y = static_cast<float>(y - static_cast<double>(hi.y));
+        lo.z = static_cast<float>(z - static_cast<double>(hi.z));
+        const int nt = d.lj_ntypes[sysid];
+        const int ty = d.lj_idx[gi];
+        lo.w = __int_as_float((s.ljbase[k] + ty * nt) | (ty << 16));
+        g.x = d.rho[gi];
+        g.y = d.srho[gi];
+        g.z = 1.0f;
+        g.w = 0.0f;
+      }
+      else {
+        // padding slot: never paired (validity checks), kept finite
+        hi = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        lo = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(s.ljbase[k]));
+        g = make_float4(1.0f, 0.0f, 1.0f, 0.0f);
+      }
+      s.hi[slot] = hi;
+      s.lo[slot] = lo;
+      s.gb[slot] = g;
+      s.fx[slot] = 0;
+      s.fy[slot] = 0;
+      s.fz[slot] = 0;
+      s.fxo[slot] = 0;
+      s.fyo[slot] = 0;
+      s.fzo[slot] = 0;
+      s.psi[slot] = 0;
+      s.psio[slot] = 0;
+      s.de[slot] = 0;
+      s.deo[slot] = 0;
+    }
+    __syncthreads();
+
+    if (VALE) {
+      valenceTerms<FORCE, ENERGY>(d, s, nsys_u);
+    }
+    if (gb) {
+      gbRadiiTiles(d, s, nsys_u, ntiles);
+      __syncthreads();
+      // effective radii, self terms (nonbonded_potential.tpp:730-805)
+      const float inv_ps = 1.0f / static_cast<float>(1 << kPsiBits);
+      const float ds = static_cast<float>(1 << kDeijdaBits);
+      for (int slot = threadIdx.x; slot < nslots; slot += blockDim.x) {
+        const int k = findOwner(s.slot0, nsys_u, slot);
+        const int a = slot - s.slot0[k];
+        if (a >= s.natom[k]) continue;
+        const int gi = d.atom_start[s.sys[k]] + a;
+        const float psi = static_cast<float>(int63ToLong(s.psi[slot], s.psio[slot])) * inv_ps;
+        float4 g = s.gb[slot];
+        const float rho = g.x;
+        float egbi;
+        if (d.igb == 1) {
+          egbi = 1.0f / (1.0f / rho + psi);
+          if (egbi < 0.0f) egbi = 30.0f;
+        }
+        else {
+          const float fipsi = psi * (-rho);
+          egbi = 1.0f / (1.0f / rho - tanhf((d.gb_alpha[gi] - d.gb_beta[gi] * fipsi +
+                                             d.gb_gamma[gi] * fipsi * fipsi) * fipsi) /
+                                      d.pb_radii[gi]);
+        }
+        g.z = egbi;
+        s.gb[slot] = g;
+        const float q = s.hi[slot].w;   // already scaled by sqrt(Coulomb constant)
+        const float expmkf = ((d.kappa > 0.0f) ? expf(-kGbKscale * d.kappa * egbi) : 1.0f) *
+                             d.inv_dielectric;
+        const float dielfac = 1.0f - expmkf;
+        const float atmq2h = 0.5f * q * q;
+        const float atmqd2h = atmq2h * dielfac;
+        if (ENERGY) {
+          addEnergy(s, k, kGb, -atmqd2h / egbi, d.nrg_scale);
+        }
+        if (FORCE) {
+          const float self_de = atmqd2h - kGbKscale * d.kappa * atmq2h * expmkf * egbi;
+          atomicAddInt63(self_de * ds, &s.de[slot], &s.deo[slot]);
+        }
+        d.born_radii[gi] = egbi;
+        d.psi[gi] = __double2ll_rn(static_cast<double>(psi) * d.psi_out_scale);
+        d.psi_ovrf[gi] = 0;
+      }
+      __syncthreads();
+    }
+    if (NB || gb) {
+      if (NB && gb) {
+        pairTiles<FORCE, ENERGY, true, true>(d, s, nsys_u, ntiles);
+      }
+      else if (NB) {
+        pairTiles<FORCE, ENERGY, true, false>(d, s, nsys_u, ntiles);
+      }
+      else {
+        pairTiles<FORCE, ENERGY, false, true>(d, s, nsys_u, ntiles);
+      }
+      __syncthreads();
+    }
+    if (gb && FORCE) {
+      // chain-rule prefactor of the OBC radii (nonbonded_potential.tpp:982-1021)
+      const float inv_ds = 1.0f / static_cast<float>(1 << kDeijdaBits);
+      const float inv_ps = 1.0f / static_cast<float>(1 << kPsiBits);
+      for (int slot = threadIdx.x; slot < nslots; slot += blockDim.x) {
+        const int k = findOwner(s.slot0, nsys_u, slot);
+        const int a = slot - s.slot0[k];
+        float4 g = s.gb[slot];
+        if (a >= s.natom[k]) {
+          g.w = 0.0f;
+          s.gb[slot] = g;
+          continue;
+        }
+        const int gi = d.atom_start[s.sys[k]] + a;
+        float sde = static_cast<float>(int63ToLong(s.de[slot], s.deo[slot])) * inv_ds;
+        if (d.igb != 1) {
+          const float psi = static_cast<float>(int63ToLong(s.psi[slot], s.psio[slot])) * inv_ps;
+          const float rho = g.x;
+          const float fipsi = psi * (-rho);
+          const float al = d.gb_alpha[gi], be = d.gb_beta[gi], ga = d.gb_gamma[gi];
+          const float thi = tanhf((al - (be - ga * fipsi) * fipsi) * fipsi);
+          sde *= (al - (2.0f * be - 3.0f * ga * fipsi) * fipsi) * (1.0f - thi * thi) * rho /
+                 d.pb_radii[gi];
+        }
+        g.w = sde;
+        s.gb[slot] = g;
+        d.sumdeijda[gi] = __double2ll_rn(static_cast<double>(sde) * d.psi_out_scale);
+        d.sumdeijda_ovrf[gi] = 0;
+      }
+      __syncthreads();
+      gbDerivativeTiles(d, s, nsys_u, ntiles);
+      __syncthreads();
+    }
+
+    // commit forces (each atom belongs to exactly one unit) and energies
+    if (FORCE) {
+      for (int slot = threadIdx.x; slot < nslots; slot += blockDim.x) {
+        const int k = findOwner(s.slot0, nsys_u, slot);
+        const int a = slot - s.slot0[k];
+        if (a >= s.natom[k]) continue;
+        const int gi = d.atom_start[s.sys[k]] + a;
+        addInt95(int63ToLong(s.fx[slot], s.fxo[slot]), &d.xfrc[gi], &d.xfrc_ovrf[gi]);
+        addInt95(int63ToLong(s.fy[slot], s.fyo[slot]), &d.yfrc[gi], &d.yfrc_ovrf[gi]);
+        addInt95(int63ToLong(s.fz[slot], s.fzo[slot]), &d.zfrc[gi], &d.zfrc_ovrf[gi]);
+      }
+    }
+    if (ENERGY) {
+      for (int e = threadIdx.x; e < nsys_u * kNrgStride; e += blockDim.x) {
+        const unsigned long long v = s.nrg[e];
+        if (v != 0ull) {
+          atomicAdd(&d.energies[s.sys[e / kNrgStride] * kNrgStride + (e % kNrgStride)], v);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Host-side launcher (called from the C++ layer)
+cudaError_t launchEvalFused(const DevSynthesis &d, int unit_begin, int unit_end, int max_lj,
+                            int terms, bool force, bool energy, int blocks, int threads,
+                            cudaStream_t stream) {
+  const size_t smem = fusedSmemBytes(d.max_unit_slots, max_lj);
+#define SB_LAUNCH(F, E, T)                                                                      \
+  {                                                                                             \
+    auto kern = kEvalFused<F, E, T>;                                                            \
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                                           static_cast<int>(smem));                             \
+    if (err != cudaSuccess) return err;                                                         \
+    kern<<<blocks, threads, smem, stream>>>(d, unit_begin, unit_end, max_lj);                   \
+    return cudaGetLastError();                                                                  \
+  }
+#define SB_TERMS(F, E)                                  \
+  switch (terms) {                                      \
+  case 1: SB_LAUNCH(F, E, 1)                            \
+  case 2: SB_LAUNCH(F, E, 2)                            \
+  case 3: SB_LAUNCH(F, E, 3)                            \
+  case 4: SB_LAUNCH(F, E, 4)                            \
+  case 5: SB_LAUNCH(F, E, 5)                            \
+  case 6: SB_LAUNCH(F, E, 6)                            \
+  case 7: SB_LAUNCH(F, E, 7)                            \
+  default: return cudaErrorInvalidValue;                \
+  }
+  if (force && energy) {
+    SB_TERMS(true, true)
+  }
+  else if (force) {
+    SB_TERMS(true, false)
+  }
+  else if (energy) {
+    SB_TERMS(false, true)
+  }
+  return cudaErrorInvalidValue;
+#undef SB_TERMS
+#undef SB_LAUNCH
+}
+
+}  // namespace sb

@@ -1,0 +1,814 @@
+// Host side of the batched implicit-solvent path: builds the device layout of a synthesis of
+// molecules (what STORMM's AtomGraphSynthesis, PhaseSpaceSynthesis, ImplicitSolventWorkspace and
+// ScoreCard hold for this path), packs molecules into work units, and implements the C ABI of
+// include/stormm_b200.h on top of the fused kernel.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <set>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "stormm_b200.h"
+#include "device_kits.h"
+#include "synthesis.h"
+
+namespace sb {
+
+size_t fusedSmemBytes(int max_slots, int max_lj);
+cudaError_t launchEvalFused(const DevSynthesis &d, int unit_begin, int unit_end, int max_lj,
+                            int terms, bool force, bool energy, int blocks, int threads,
+                            cudaStream_t stream);
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void setLastError(const std::string &msg) { g_last_error = msg; }
+const char* lastError() { return g_last_error.c_str(); }
+
+void cudaCheck(cudaError_t err, const char* what) {
+  if (err != cudaSuccess) {
+    throw Error(SB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(err));
+  }
+}
+
+namespace {
+
+double gbDefault(int igb, int which) {
+  // Constants/generalized_born.h:52-66 (OBC-I, OBC-II); HCT uses none of them
+  if (igb == SB_GB_OBC) {
+    return (which == 0) ? 0.8 : (which == 1) ? 0.0 : 2.909125;
+  }
+  if (igb == SB_GB_OBC2) {
+    return (which == 0) ? 1.0 : (which == 1) ? 0.8 : 4.85;
+  }
+  return 0.0;
+}
+
+uint32_t fbits(double v) {
+  const float f = static_cast<float>(v);
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  return u;
+}
+
+}  // namespace
+
+Synthesis::Synthesis(const sb_topology* tops, int ntop, const int* topology_index, int nsys_in,
+                     const sb_options &options) :
+    opt(options), nsys(nsys_in) {
+  if (nsys <= 0 || ntop <= 0 || tops == nullptr || topology_index == nullptr) {
+    throw Error(SB_ERR_ARGUMENT, "a synthesis needs at least one system and one topology");
+  }
+  if (opt.igb != SB_GB_NONE && opt.igb != SB_GB_HCT && opt.igb != SB_GB_OBC &&
+      opt.igb != SB_GB_OBC2) {
+    throw Error(SB_ERR_UNSUPPORTED, "implicit solvent model igb=" + std::to_string(opt.igb) +
+                " is not available on this path (supported: 0, 1, 2, 5)");
+  }
+  if (opt.gpos_bits < 24 || opt.gpos_bits > 40 || opt.frc_bits < 18 || opt.frc_bits > 40 ||
+      opt.nrg_bits < 22 || opt.nrg_bits > 40) {
+    throw Error(SB_ERR_ARGUMENT, "fixed-point bit counts out of range");
+  }
+  int dev_count = 0;
+  cudaCheck(cudaGetDeviceCount(&dev_count), "cudaGetDeviceCount");
+  if (opt.device < 0 || opt.device >= dev_count) {
+    throw Error(SB_ERR_DEVICE, "CUDA device " + std::to_string(opt.device) + " not present");
+  }
+  cudaCheck(cudaSetDevice(opt.device), "cudaSetDevice");
+  cudaDeviceProp prop;
+  cudaCheck(cudaGetDeviceProperties(&prop, opt.device), "cudaGetDeviceProperties");
+  if (prop.major < 10) {
+    throw Error(SB_ERR_DEVICE, std::string("device ") + prop.name + " is not sm_100 class");
+  }
+  sm_count = prop.multiProcessorCount;
+  max_smem_optin = static_cast<int>(prop.sharedMemPerBlockOptin);
+
+  topo.assign(topology_index, topology_index + nsys);
+  for (int s = 0; s < nsys; s++) {
+    if (topo[s] < 0 || topo[s] >= ntop) {
+      throw Error(SB_ERR_ARGUMENT, "topology index out of range for system " + std::to_string(s));
+    }
+  }
+  for (int t = 0; t < ntop; t++) {
+    const sb_topology &tp = tops[t];
+    if (tp.natom <= 0 || tp.natom > 65535 || tp.charge == nullptr || tp.lj_idx == nullptr ||
+        tp.lja == nullptr || tp.ljb == nullptr || tp.n_lj_types <= 0 ||
+        tp.n_lj_types > 64) {
+      throw Error(SB_ERR_ARGUMENT, "topology " + std::to_string(t) + " is incomplete or too large");
+    }
+    if (opt.igb != SB_GB_NONE && (tp.pb_radii == nullptr || tp.gb_screen == nullptr)) {
+      throw Error(SB_ERR_ARGUMENT, "topology " + std::to_string(t) + " lacks GB radii");
+    }
+  }
+  buildLayout(tops, ntop);
+  buildUnits();
+  upload();
+}
+
+void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
+  const double sqrt_kc = std::sqrt(opt.coulomb_constant);
+  atom_start.resize(nsys);
+  atom_count.resize(nsys);
+  int off = 0;
+  for (int s = 0; s < nsys; s++) {
+    atom_start[s] = off;
+    atom_count[s] = tops[topo[s]].natom;
+    off += (atom_count[s] + kTile - 1) / kTile * kTile;
+  }
+  natom_padded = off;
+  const size_t np = natom_padded;
+  h_charge.assign(np, 0.0f);
+  h_ljidx.assign(np, 0);
+  h_rho.assign(np, 1.0f);
+  h_srho.assign(np, 0.0f);
+  h_pb.assign(np, 1.09f);
+  h_alpha.assign(np, 0.0f);
+  h_beta.assign(np, 0.0f);
+  h_gamma.assign(np, 0.0f);
+
+  // per-topology Lennard-Jones tables and tile exclusion masks
+  std::vector<int> topo_lj_start(ntop), topo_tile_start(ntop);
+  h_mask_pool.assign(32, 0u);   // mask 0: no exclusions
+  for (int t = 0; t < ntop; t++) {
+    const sb_topology &tp = tops[t];
+    topo_lj_start[t] = h_ljab.size();
+    const int nt = tp.n_lj_types;
+    for (int e = 0; e < nt * nt; e++) {
+      h_ljab.push_back(make_float2(static_cast<float>(tp.lja[e]), static_cast<float>(tp.ljb[e])));
+      const double a14 = (tp.lja14 != nullptr) ? tp.lja14[e] : tp.lja[e];
+      const double b14 = (tp.ljb14 != nullptr) ? tp.ljb14[e] : tp.ljb[e];
+      h_ljab14.push_back(make_float2(static_cast<float>(a14), static_cast<float>(b14)));
+    }
+    // exclusions as a symmetric set of pairs
+    const int n = tp.natom;
+    std::vector<std::vector<int>> partners(n);
+    if (tp.excl_bounds != nullptr && tp.excl_list != nullptr) {
+      for (int i = 0; i < n; i++) {
+        for (int e = tp.excl_bounds[i]; e < tp.excl_bounds[i + 1]; e++) {
+          const int j = tp.excl_list[e];
+          if (j < 0 || j >= n) {
+            throw Error(SB_ERR_ARGUMENT, "exclusion partner out of range in topology " +
+                        std::to_string(t));
+          }
+          if (j == i) continue;
+          partners[i].push_back(j);
+          partners[j].push_back(i);
+        }
+      }
+    }
+    const int nblk = (n + kTile - 1) / kTile;
+    topo_tile_start[t] = h_tile_mask_idx.size();
+    for (int I = 0; I < nblk; I++) {
+      for (int J = 0; J <= I; J++) {
+        unsigned rows[32] = {0u};
+        bool any = false;
+        for (int l = 0; l < kTile; l++) {
+          const int a = I * kTile + l;
+          if (a >= n) break;
+          for (int b : partners[a]) {
+            if (b >= J * kTile && b < (J + 1) * kTile) {
+              rows[l] |= (1u << (b - J * kTile));
+              any = true;
+            }
+          }
+        }
+        if (any) {
+          h_tile_mask_idx.push_back(static_cast<int>(h_mask_pool.size() / 32));
+          h_mask_pool.insert(h_mask_pool.end(), rows, rows + 32);
+        }
+        else {
+          h_tile_mask_idx.push_back(0);
+        }
+      }
+    }
+  }
+
+  // per-system parameters and valence records
+  h_lj_start.resize(nsys);
+  h_lj_ntypes.resize(nsys);
+  h_tile_start.resize(nsys);
+  h_bond_start.assign(nsys + 1, 0);
+  h_angl_start.assign(nsys + 1, 0);
+  h_dihe_start.assign(nsys + 1, 0);
+  for (int s = 0; s < nsys; s++) {
+    const int t = topo[s];
+    const sb_topology &tp = tops[t];
+    h_lj_start[s] = topo_lj_start[t];
+    h_lj_ntypes[s] = tp.n_lj_types;
+    h_tile_start[s] = topo_tile_start[t];
+    const int base = atom_start[s];
+    for (int i = 0; i < tp.natom; i++) {
+      h_charge[base + i] = static_cast<float>(tp.charge[i] * sqrt_kc);
+      if (tp.lj_idx[i] < 0 || tp.lj_idx[i] >= tp.n_lj_types) {
+        throw Error(SB_ERR_ARGUMENT, "Lennard-Jones type out of range");
+      }
+      h_ljidx[base + i] = tp.lj_idx[i];
+      if (opt.igb != SB_GB_NONE) {
+        const double rho = tp.pb_radii[i] - 0.09;
+        h_rho[base + i] = static_cast<float>(rho);
+        h_srho[base + i] = static_cast<float>(tp.gb_screen[i] * rho);
+        h_pb[base + i] = static_cast<float>(tp.pb_radii[i]);
+        h_alpha[base + i] = static_cast<float>(tp.gb_alpha ? tp.gb_alpha[i] : gbDefault(opt.igb, 0));
+        h_beta[base + i] = static_cast<float>(tp.gb_beta ? tp.gb_beta[i] : gbDefault(opt.igb, 1));
+        h_gamma[base + i] = static_cast<float>(tp.gb_gamma ? tp.gb_gamma[i] : gbDefault(opt.igb, 2));
+      }
+    }
+    auto check_atom = [&](int a) {
+      if (a < 0 || a >= tp.natom) {
+        throw Error(SB_ERR_ARGUMENT, "valence term atom index out of range in topology " +
+                    std::to_string(t));
+      }
+      return static_cast<uint32_t>(a);
+    };
+    for (int b = 0; b < tp.nbond; b++) {
+      const uint32_t i = check_atom(tp.bond_atoms[2 * b]);
+      const uint32_t j = check_atom(tp.bond_atoms[2 * b + 1]);
+      h_bonds.push_back(make_uint4(i | (j << 16), fbits(tp.bond_keq[b]), fbits(tp.bond_leq[b]), 0u));
+    }
+    h_bond_start[s + 1] = h_bonds.size();
+    for (int a = 0; a < tp.nangl; a++) {
+      const uint32_t i = check_atom(tp.angl_atoms[3 * a]);
+      const uint32_t j = check_atom(tp.angl_atoms[3 * a + 1]);
+      const uint32_t k = check_atom(tp.angl_atoms[3 * a + 2]);
+      h_angles.push_back(make_uint4(i | (j << 16), k, fbits(tp.angl_keq[a]),
+                                    fbits(tp.angl_theta0[a])));
+    }
+    h_angl_start[s + 1] = h_angles.size();
+    for (int d = 0; d < tp.ndihe; d++) {
+      const uint32_t i = check_atom(tp.dihe_atoms[4 * d]);
+      const uint32_t j = check_atom(tp.dihe_atoms[4 * d + 1]);
+      const uint32_t k = check_atom(tp.dihe_atoms[4 * d + 2]);
+      const uint32_t l = check_atom(tp.dihe_atoms[4 * d + 3]);
+      const double scee = (tp.dihe_scee != nullptr) ? tp.dihe_scee[d] : 0.0;
+      const double scnb = (tp.dihe_scnb != nullptr) ? tp.dihe_scnb[d] : 0.0;
+      const uint32_t flags = (tp.dihe_improper != nullptr && tp.dihe_improper[d] != 0) ? 1u : 0u;
+      h_dihe_a.push_back(make_uint4(i | (j << 16), k | (l << 16), fbits(tp.dihe_amp[d]),
+                                    fbits(tp.dihe_phase[d])));
+      h_dihe_b.push_back(make_uint4(fbits(tp.dihe_freq[d]), fbits(scee > 0.0 ? 1.0 / scee : 0.0),
+                                    fbits((scee > 0.0 && scnb > 0.0) ? 1.0 / scnb : 0.0), flags));
+    }
+    h_dihe_start[s + 1] = h_dihe_a.size();
+  }
+}
+
+void Synthesis::buildUnits() {
+  const int max_slots_cap = (opt.max_atoms_per_unit > 0) ? opt.max_atoms_per_unit : 512;
+  const int max_tiles_cap = (opt.max_tiles_per_unit > 0) ? opt.max_tiles_per_unit : 64;
+  threads = (opt.threads_per_block > 0) ? opt.threads_per_block : 256;
+  if (threads % 32 != 0 || threads < 64 || threads > 256) {
+    throw Error(SB_ERR_ARGUMENT, "threads per block must be a multiple of 32 in [64, 256]");
+  }
+  std::vector<int> order(nsys);
+  for (int s = 0; s < nsys; s++) order[s] = s;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return atom_count[a] > atom_count[b]; });
+  auto slots_of = [&](int s) { return (atom_count[s] + kTile - 1) / kTile * kTile; };
+  auto tiles_of = [&](int s) {
+    const int nb = (atom_count[s] + kTile - 1) / kTile;
+    return nb * (nb + 1) / 2;
+  };
+  auto lj_of = [&](int s) { return 2 * h_lj_ntypes[s] * h_lj_ntypes[s]; };
+  const int max_lj_cap = 4096;
+  h_units.clear();
+  h_unit_systems.clear();
+  int4 cur = make_int4(0, 0, 0, 0);
+  int cur_lj = 0;
+  max_lj = 0;
+  max_unit_slots = 0;
+  for (int s : order) {
+    if (slots_of(s) > max_slots_cap) {
+      throw Error(SB_ERR_UNSUPPORTED, "system " + std::to_string(s) + " has " +
+                  std::to_string(atom_count[s]) + " atoms; the fused path holds up to " +
+                  std::to_string(max_slots_cap) + " atoms per work unit");
+    }
+    const bool fits = cur.y > 0 && cur.y < kMaxUnitSystems &&
+                      cur.z + slots_of(s) <= max_slots_cap &&
+                      cur.w + tiles_of(s) <= max_tiles_cap && cur_lj + lj_of(s) <= max_lj_cap;
+    if (!fits && cur.y > 0) {
+      h_units.push_back(cur);
+      max_lj = std::max(max_lj, cur_lj);
+      max_unit_slots = std::max(max_unit_slots, cur.z);
+      cur = make_int4(static_cast<int>(h_unit_systems.size()), 0, 0, 0);
+      cur_lj = 0;
+    }
+    if (cur.y == 0) {
+      cur.x = h_unit_systems.size();
+    }
+    h_unit_systems.push_back(s);
+    cur.y++;
+    cur.z += slots_of(s);
+    cur.w += tiles_of(s);
+    cur_lj += lj_of(s);
+  }
+  if (cur.y > 0) {
+    h_units.push_back(cur);
+    max_lj = std::max(max_lj, cur_lj);
+    max_unit_slots = std::max(max_unit_slots, cur.z);
+  }
+  // one unit per system, in system order, for the per-system launches
+  h_single_units.resize(nsys);
+  h_single_systems.resize(nsys);
+  for (int s = 0; s < nsys; s++) {
+    h_single_units[s] = make_int4(s, 1, slots_of(s), tiles_of(s));
+    h_single_systems[s] = s;
+    max_unit_slots = std::max(max_unit_slots, slots_of(s));
+    max_lj = std::max(max_lj, lj_of(s));
+  }
+  const size_t smem = fusedSmemBytes(max_unit_slots, max_lj);
+  if (static_cast<int>(smem) > max_smem_optin) {
+    throw Error(SB_ERR_ARGUMENT, "work units need " + std::to_string(smem) +
+                " bytes of shared memory, above the device limit");
+  }
+}
+
+void Synthesis::upload() {
+  d_atom_start.upload(atom_start);
+  d_atom_count.upload(atom_count);
+  d_bond_start.upload(h_bond_start);
+  d_angl_start.upload(h_angl_start);
+  d_dihe_start.upload(h_dihe_start);
+  d_lj_start.upload(h_lj_start);
+  d_lj_ntypes.upload(h_lj_ntypes);
+  d_tile_start.upload(h_tile_start);
+  d_charge.upload(h_charge);
+  d_ljidx.upload(h_ljidx);
+  d_rho.upload(h_rho);
+  d_srho.upload(h_srho);
+  d_pb.upload(h_pb);
+  d_alpha.upload(h_alpha);
+  d_beta.upload(h_beta);
+  d_gamma.upload(h_gamma);
+  d_ljab.upload(h_ljab);
+  d_ljab14.upload(h_ljab14);
+  d_bonds.upload(h_bonds);
+  d_angles.upload(h_angles);
+  d_dihe_a.upload(h_dihe_a);
+  d_dihe_b.upload(h_dihe_b);
+  d_tile_mask_idx.upload(h_tile_mask_idx);
+  d_mask_pool.upload(h_mask_pool);
+  d_units.upload(h_units);
+  d_unit_systems.upload(h_unit_systems);
+  d_single_units.upload(h_single_units);
+  d_single_systems.upload(h_single_systems);
+  const size_t np = natom_padded;
+  d_xcrd.zeros(np);
+  d_ycrd.zeros(np);
+  d_zcrd.zeros(np);
+  d_xcrd_ovrf.zeros(np);
+  d_ycrd_ovrf.zeros(np);
+  d_zcrd_ovrf.zeros(np);
+  d_xfrc.zeros(np);
+  d_yfrc.zeros(np);
+  d_zfrc.zeros(np);
+  d_xfrc_ovrf.zeros(np);
+  d_yfrc_ovrf.zeros(np);
+  d_zfrc_ovrf.zeros(np);
+  d_energies.zeros(static_cast<size_t>(nsys) * kNrgStride);
+  d_psi.zeros(np);
+  d_psi_ovrf.zeros(np);
+  d_sumdeijda.zeros(np);
+  d_sumdeijda_ovrf.zeros(np);
+  d_born_radii.zeros(np);
+  d_status.zeros(1);
+
+  DevSynthesis &d = dev;
+  std::memset(&d, 0, sizeof(DevSynthesis));
+  d.nsys = nsys;
+  d.natom_padded = natom_padded;
+  d.igb = opt.igb;
+  d.kappa = (opt.saltcon > 1.0e-8) ? static_cast<float>(std::sqrt(0.10806 * opt.saltcon)) : 0.0f;
+  d.inv_dielectric = static_cast<float>(1.0 / opt.dielectric);
+  d.frc_scale = static_cast<float>(std::ldexp(1.0, opt.frc_bits));
+  d.nrg_scale = static_cast<float>(std::ldexp(1.0, opt.nrg_bits));
+  d.inv_gpos_scale = std::ldexp(1.0, -opt.gpos_bits);
+  d.psi_out_scale = std::ldexp(1.0, 24);
+  d.atom_start = d_atom_start.p;
+  d.atom_count = d_atom_count.p;
+  d.bond_start = d_bond_start.p;
+  d.angl_start = d_angl_start.p;
+  d.dihe_start = d_dihe_start.p;
+  d.lj_start = d_lj_start.p;
+  d.lj_ntypes = d_lj_ntypes.p;
+  d.tile_start = d_tile_start.p;
+  d.xcrd = d_xcrd.p;
+  d.ycrd = d_ycrd.p;
+  d.zcrd = d_zcrd.p;
+  d.xfrc = d_xfrc.p;
+  d.yfrc = d_yfrc.p;
+  d.zfrc = d_zfrc.p;
+  d.xfrc_ovrf = d_xfrc_ovrf.p;
+  d.yfrc_ovrf = d_yfrc_ovrf.p;
+  d.zfrc_ovrf = d_zfrc_ovrf.p;
+  d.charge = d_charge.p;
+  d.lj_idx = d_ljidx.p;
+  d.rho = d_rho.p;
+  d.srho = d_srho.p;
+  d.pb_radii = d_pb.p;
+  d.gb_alpha = d_alpha.p;
+  d.gb_beta = d_beta.p;
+  d.gb_gamma = d_gamma.p;
+  d.ljab = d_ljab.p;
+  d.ljab14 = d_ljab14.p;
+  d.bonds = d_bonds.p;
+  d.angles = d_angles.p;
+  d.dihe_a = d_dihe_a.p;
+  d.dihe_b = d_dihe_b.p;
+  d.tile_mask_idx = d_tile_mask_idx.p;
+  d.mask_pool = d_mask_pool.p;
+  d.energies = d_energies.p;
+  d.psi = d_psi.p;
+  d.psi_ovrf = d_psi_ovrf.p;
+  d.sumdeijda = d_sumdeijda.p;
+  d.sumdeijda_ovrf = d_sumdeijda_ovrf.p;
+  d.born_radii = d_born_radii.p;
+  d.nunit = h_units.size();
+  d.unit_desc = d_units.p;
+  d.unit_systems = d_unit_systems.p;
+  d.max_unit_slots = max_unit_slots;
+  d.status = d_status.p;
+}
+
+void Synthesis::evaluate(int terms, bool force, bool energy, cudaStream_t stream) {
+  if (terms <= 0 || terms > SB_TERM_ALL) {
+    throw Error(SB_ERR_ARGUMENT, "terms must be a nonzero mask of SB_TERM_*");
+  }
+  if (!force && !energy) {
+    return;
+  }
+  const int nunit = h_units.size();
+  cudaCheck(launchEvalFused(dev, 0, nunit, max_lj, terms, force, energy, nunit, threads, stream),
+            "fused evaluation launch");
+}
+
+void Synthesis::evaluateRange(int first, int count, int terms, bool force, bool energy,
+                              cudaStream_t stream) {
+  if (first < 0 || count < 0 || first + count > nsys) {
+    throw Error(SB_ERR_ARGUMENT, "system range out of bounds");
+  }
+  if (terms <= 0 || terms > SB_TERM_ALL) {
+    throw Error(SB_ERR_ARGUMENT, "terms must be a nonzero mask of SB_TERM_*");
+  }
+  if (!force && !energy) {
+    return;
+  }
+  DevSynthesis d = dev;
+  d.unit_desc = d_single_units.p;
+  d.unit_systems = d_single_systems.p;
+  d.nunit = nsys;
+  for (int s = first; s < first + count; s++) {
+    cudaCheck(launchEvalFused(d, s, s + 1, max_lj, terms, force, energy, 1, threads, stream),
+              "per-system evaluation launch");
+  }
+}
+
+void Synthesis::initialize(int what, cudaStream_t stream) {
+  const size_t np = natom_padded;
+  if (what & SB_INIT_FORCES) {
+    cudaCheck(cudaMemsetAsync(d_xfrc.p, 0, np * sizeof(long long), stream), "memset");
+    cudaCheck(cudaMemsetAsync(d_yfrc.p, 0, np * sizeof(long long), stream), "memset");
+    cudaCheck(cudaMemsetAsync(d_zfrc.p, 0, np * sizeof(long long), stream), "memset");
+    cudaCheck(cudaMemsetAsync(d_xfrc_ovrf.p, 0, np * sizeof(int), stream), "memset");
+    cudaCheck(cudaMemsetAsync(d_yfrc_ovrf.p, 0, np * sizeof(int), stream), "memset");
+    cudaCheck(cudaMemsetAsync(d_zfrc_ovrf.p, 0, np * sizeof(int), stream), "memset");
+  }
+  if (what & SB_INIT_ENERGIES) {
+    cudaCheck(cudaMemsetAsync(d_energies.p, 0, d_energies.n * sizeof(unsigned long long), stream),
+              "memset");
+  }
+  if (what & SB_INIT_GB_WORKSPACE) {
+    cudaCheck(cudaMemsetAsync(d_psi.p, 0, np * sizeof(long long), stream), "memset");
+    cudaCheck(cudaMemsetAsync(d_psi_ovrf.p, 0, np * sizeof(int), stream), "memset");
+    cudaCheck(cudaMemsetAsync(d_sumdeijda.p, 0, np * sizeof(long long), stream), "memset");
+    cudaCheck(cudaMemsetAsync(d_sumdeijda_ovrf.p, 0, np * sizeof(int), stream), "memset");
+  }
+}
+
+void Synthesis::setCoordinates(const double* xyz, cudaStream_t stream) {
+  const size_t np = natom_padded;
+  h_stage_ll.assign(3 * np, 0);
+  const double scale = std::ldexp(1.0, opt.gpos_bits);
+  size_t src = 0;
+  for (int s = 0; s < nsys; s++) {
+    for (int i = 0; i < atom_count[s]; i++) {
+      const size_t a = atom_start[s] + i;
+      for (int c = 0; c < 3; c++) {
+        const double v = xyz[3 * src + c];
+        if (!std::isfinite(v) || std::fabs(v) * scale > 9.0e18) {
+          throw Error(SB_ERR_ARGUMENT, "coordinate of system " + std::to_string(s) + " atom " +
+                      std::to_string(i) + " is not finite or out of the fixed-point range");
+        }
+        h_stage_ll[c * np + a] = std::llround(v * scale);
+      }
+      src++;
+    }
+  }
+  cudaCheck(cudaMemcpyAsync(d_xcrd.p, h_stage_ll.data(), np * sizeof(long long),
+                            cudaMemcpyHostToDevice, stream), "coordinate upload");
+  cudaCheck(cudaMemcpyAsync(d_ycrd.p, h_stage_ll.data() + np, np * sizeof(long long),
+                            cudaMemcpyHostToDevice, stream), "coordinate upload");
+  cudaCheck(cudaMemcpyAsync(d_zcrd.p, h_stage_ll.data() + 2 * np, np * sizeof(long long),
+                            cudaMemcpyHostToDevice, stream), "coordinate upload");
+  cudaCheck(cudaStreamSynchronize(stream), "coordinate upload");
+}
+
+void Synthesis::getCoordinates(double* xyz, cudaStream_t stream) {
+  const size_t np = natom_padded;
+  h_stage_ll.resize(3 * np);
+  cudaCheck(cudaMemcpyAsync(h_stage_ll.data(), d_xcrd.p, np * sizeof(long long),
+                            cudaMemcpyDeviceToHost, stream), "coordinate download");
+  cudaCheck(cudaMemcpyAsync(h_stage_ll.data() + np, d_ycrd.p, np * sizeof(long long),
+                            cudaMemcpyDeviceToHost, stream), "coordinate download");
+  cudaCheck(cudaMemcpyAsync(h_stage_ll.data() + 2 * np, d_zcrd.p, np * sizeof(long long),
+                            cudaMemcpyDeviceToHost, stream), "coordinate download");
+  cudaCheck(cudaStreamSynchronize(stream), "coordinate download");
+  const double inv = std::ldexp(1.0, -opt.gpos_bits);
+  size_t dst = 0;
+  for (int s = 0; s < nsys; s++) {
+    for (int i = 0; i < atom_count[s]; i++) {
+      const size_t a = atom_start[s] + i;
+      for (int c = 0; c < 3; c++) {
+        xyz[3 * dst + c] = static_cast<double>(h_stage_ll[c * np + a]) * inv;
+      }
+      dst++;
+    }
+  }
+}
+
+void Synthesis::getForcesFixed(long long* prim, int* ovrf, cudaStream_t stream) {
+  const size_t np = natom_padded;
+  cudaCheck(cudaMemcpyAsync(prim, d_xfrc.p, np * sizeof(long long), cudaMemcpyDeviceToHost,
+                            stream), "force download");
+  cudaCheck(cudaMemcpyAsync(prim + np, d_yfrc.p, np * sizeof(long long), cudaMemcpyDeviceToHost,
+                            stream), "force download");
+  cudaCheck(cudaMemcpyAsync(prim + 2 * np, d_zfrc.p, np * sizeof(long long),
+                            cudaMemcpyDeviceToHost, stream), "force download");
+  cudaCheck(cudaMemcpyAsync(ovrf, d_xfrc_ovrf.p, np * sizeof(int), cudaMemcpyDeviceToHost,
+                            stream), "force download");
+  cudaCheck(cudaMemcpyAsync(ovrf + np, d_yfrc_ovrf.p, np * sizeof(int), cudaMemcpyDeviceToHost,
+                            stream), "force download");
+  cudaCheck(cudaMemcpyAsync(ovrf + 2 * np, d_zfrc_ovrf.p, np * sizeof(int),
+                            cudaMemcpyDeviceToHost, stream), "force download");
+  cudaCheck(cudaStreamSynchronize(stream), "force download");
+}
+
+void Synthesis::getForces(double* xyz, cudaStream_t stream) {
+  const size_t np = natom_padded;
+  std::vector<long long> prim(3 * np);
+  std::vector<int> ovrf(3 * np);
+  getForcesFixed(prim.data(), ovrf.data(), stream);
+  const double inv = std::ldexp(1.0, -opt.frc_bits);
+  size_t dst = 0;
+  for (int s = 0; s < nsys; s++) {
+    for (int i = 0; i < atom_count[s]; i++) {
+      const size_t a = atom_start[s] + i;
+      for (int c = 0; c < 3; c++) {
+        const double v = static_cast<double>(ovrf[c * np + a]) * 9223372036854775808.0 +
+                         static_cast<double>(prim[c * np + a]);
+        xyz[3 * dst + c] = v * inv;
+      }
+      dst++;
+    }
+  }
+}
+
+void Synthesis::getEnergiesFixed(long long* out, cudaStream_t stream) {
+  cudaCheck(cudaMemcpyAsync(out, d_energies.p, d_energies.n * sizeof(long long),
+                            cudaMemcpyDeviceToHost, stream), "energy download");
+  cudaCheck(cudaStreamSynchronize(stream), "energy download");
+}
+
+void Synthesis::getEnergies(double* out, cudaStream_t stream) {
+  std::vector<long long> raw(d_energies.n);
+  getEnergiesFixed(raw.data(), stream);
+  const double inv = std::ldexp(1.0, -opt.nrg_bits);
+  for (size_t e = 0; e < raw.size(); e++) {
+    out[e] = static_cast<double>(raw[e]) * inv;
+  }
+}
+
+void Synthesis::getGbWorkspace(double* psi, double* radii, double* sde, cudaStream_t stream) {
+  const size_t np = natom_padded;
+  std::vector<long long> p(np), q(np);
+  std::vector<float> r(np);
+  cudaCheck(cudaMemcpyAsync(p.data(), d_psi.p, np * sizeof(long long), cudaMemcpyDeviceToHost,
+                            stream), "workspace download");
+  cudaCheck(cudaMemcpyAsync(q.data(), d_sumdeijda.p, np * sizeof(long long),
+                            cudaMemcpyDeviceToHost, stream), "workspace download");
+  cudaCheck(cudaMemcpyAsync(r.data(), d_born_radii.p, np * sizeof(float), cudaMemcpyDeviceToHost,
+                            stream), "workspace download");
+  cudaCheck(cudaStreamSynchronize(stream), "workspace download");
+  const double inv = std::ldexp(1.0, -24);
+  size_t dst = 0;
+  for (int s = 0; s < nsys; s++) {
+    for (int i = 0; i < atom_count[s]; i++) {
+      const size_t a = atom_start[s] + i;
+      if (psi) psi[dst] = static_cast<double>(p[a]) * inv;
+      if (sde) sde[dst] = static_cast<double>(q[a]) * inv;
+      if (radii) radii[dst] = r[a];
+      dst++;
+    }
+  }
+}
+
+int Synthesis::checkStatus(cudaStream_t stream) {
+  int st = 0;
+  cudaCheck(cudaMemcpyAsync(&st, d_status.p, sizeof(int), cudaMemcpyDeviceToHost, stream),
+            "status download");
+  cudaCheck(cudaMemsetAsync(d_status.p, 0, sizeof(int), stream), "status reset");
+  cudaCheck(cudaStreamSynchronize(stream), "status download");
+  return st;
+}
+
+}  // namespace sb
+
+// ------------------------------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------------------------------
+struct sb_synthesis {
+  std::unique_ptr<sb::Synthesis> impl;
+};
+
+namespace {
+
+template <typename F> int guarded(F &&f) {
+  try {
+    f();
+    return SB_OK;
+  }
+  catch (const sb::Error &e) {
+    sb::setLastError(e.what());
+    return e.code;
+  }
+  catch (const std::exception &e) {
+    sb::setLastError(e.what());
+    return SB_ERR_ARGUMENT;
+  }
+}
+
+cudaStream_t asStream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+sb::Synthesis* need(sb_synthesis* syn) {
+  if (syn == nullptr || !syn->impl) {
+    throw sb::Error(SB_ERR_ARGUMENT, "null synthesis handle");
+  }
+  return syn->impl.get();
+}
+
+const sb::Synthesis* need(const sb_synthesis* syn) {
+  if (syn == nullptr || !syn->impl) {
+    throw sb::Error(SB_ERR_ARGUMENT, "null synthesis handle");
+  }
+  return syn->impl.get();
+}
+
+}  // namespace
+
+extern "C" {
+
+void sb_default_options(sb_options* opt) {
+  std::memset(opt, 0, sizeof(sb_options));
+  opt->igb = SB_GB_OBC2;
+  opt->dielectric = 80.0;
+  opt->saltcon = 0.0;
+  opt->coulomb_constant = 332.0522172900000;
+  opt->gpos_bits = 32;
+  opt->frc_bits = 23;
+  opt->nrg_bits = 26;
+  opt->device = 0;
+}
+
+int sb_synthesis_create(const sb_topology* tops, int ntop, const int* topology_index, int nsys,
+                        const sb_options* opt, sb_synthesis** out) {
+  return guarded([&]() {
+    if (out == nullptr) throw sb::Error(SB_ERR_ARGUMENT, "null output handle");
+    *out = nullptr;
+    sb_options o;
+    if (opt != nullptr) {
+      o = *opt;
+    }
+    else {
+      sb_default_options(&o);
+    }
+    auto h = std::make_unique<sb_synthesis>();
+    h->impl = std::make_unique<sb::Synthesis>(tops, ntop, topology_index, nsys, o);
+    *out = h.release();
+  });
+}
+
+int sb_synthesis_destroy(sb_synthesis* syn) {
+  return guarded([&]() { delete syn; });
+}
+
+int sb_system_count(const sb_synthesis* syn) {
+  if (syn == nullptr || !syn->impl) return SB_ERR_ARGUMENT;
+  return syn->impl->nsys;
+}
+
+int sb_system_atoms(const sb_synthesis* syn, int system, int* natom, int* offset) {
+  return guarded([&]() {
+    const sb::Synthesis* s = need(syn);
+    if (system < 0 || system >= s->nsys) throw sb::Error(SB_ERR_ARGUMENT, "system out of range");
+    if (natom) *natom = s->atom_count[system];
+    if (offset) *offset = s->atom_start[system];
+  });
+}
+
+int sb_padded_atom_count(const sb_synthesis* syn) {
+  if (syn == nullptr || !syn->impl) return SB_ERR_ARGUMENT;
+  return syn->impl->natom_padded;
+}
+
+int sb_set_coordinates(sb_synthesis* syn, const double* xyz, void* stream) {
+  return guarded([&]() { need(syn)->setCoordinates(xyz, asStream(stream)); });
+}
+
+int sb_get_coordinates(sb_synthesis* syn, double* xyz, void* stream) {
+  return guarded([&]() { need(syn)->getCoordinates(xyz, asStream(stream)); });
+}
+
+int sb_get_forces(sb_synthesis* syn, double* xyz, void* stream) {
+  return guarded([&]() { need(syn)->getForces(xyz, asStream(stream)); });
+}
+
+int sb_get_energies(sb_synthesis* syn, double* energies, void* stream) {
+  return guarded([&]() { need(syn)->getEnergies(energies, asStream(stream)); });
+}
+
+int sb_get_gb_workspace(sb_synthesis* syn, double* psi, double* radii, double* sumdeijda,
+                        void* stream) {
+  return guarded([&]() { need(syn)->getGbWorkspace(psi, radii, sumdeijda, asStream(stream)); });
+}
+
+int sb_get_forces_fixed(sb_synthesis* syn, int64_t* xyz_primary, int32_t* xyz_overflow,
+                        void* stream) {
+  return guarded([&]() {
+    need(syn)->getForcesFixed(reinterpret_cast<long long*>(xyz_primary),
+                              reinterpret_cast<int*>(xyz_overflow), asStream(stream));
+  });
+}
+
+int sb_get_energies_fixed(sb_synthesis* syn, int64_t* energies, void* stream) {
+  return guarded([&]() {
+    need(syn)->getEnergiesFixed(reinterpret_cast<long long*>(energies), asStream(stream));
+  });
+}
+
+int sb_initialize(sb_synthesis* syn, int what, void* stream) {
+  return guarded([&]() { need(syn)->initialize(what, asStream(stream)); });
+}
+
+int sb_evaluate(sb_synthesis* syn, int terms, int eval_force, int eval_energy, void* stream) {
+  return guarded([&]() {
+    need(syn)->evaluate(terms, eval_force != 0, eval_energy != 0, asStream(stream));
+  });
+}
+
+int sb_evaluate_range(sb_synthesis* syn, int first, int count, int terms, int eval_force,
+                      int eval_energy, void* stream) {
+  return guarded([&]() {
+    need(syn)->evaluateRange(first, count, terms, eval_force != 0, eval_energy != 0,
+                             asStream(stream));
+  });
+}
+
+int sb_launch_nonbonded(sb_synthesis* syn, int eval_force, int eval_energy, void* stream) {
+  return guarded([&]() {
+    need(syn)->evaluate(SB_TERM_NONBONDED | SB_TERM_GB, eval_force != 0, eval_energy != 0,
+                        asStream(stream));
+  });
+}
+
+int sb_launch_valence(sb_synthesis* syn, int eval_force, int eval_energy, void* stream) {
+  return guarded([&]() {
+    need(syn)->evaluate(SB_TERM_VALENCE, eval_force != 0, eval_energy != 0, asStream(stream));
+  });
+}
+
+int sb_launch_info(const sb_synthesis* syn, int* work_units, int* blocks, int* threads) {
+  return guarded([&]() {
+    const sb::Synthesis* s = need(syn);
+    if (work_units) *work_units = s->h_units.size();
+    if (blocks) *blocks = s->h_units.size();
+    if (threads) *threads = s->threads;
+  });
+}
+
+int sb_check_status(sb_synthesis* syn, int* status) {
+  return guarded([&]() {
+    const int st = need(syn)->checkStatus(nullptr);
+    if (status) *status = st;
+  });
+}
+
+const char* sb_last_error(void) { return sb::lastError(); }
+
+const char* sb_version(void) { return "stormm_b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

@@ -1,0 +1,134 @@
+// Host-side synthesis of many molecules for the batched implicit-solvent path.
+//
+// One object holds what STORMM spreads over AtomGraphSynthesis (parameters, valence terms,
+// Lennard-Jones tables: Synthesis/atomgraph_synthesis.h:55), StaticExclusionMaskSynthesis
+// (exclusions, Synthesis/static_mask_synthesis.h:54), PhaseSpaceSynthesis (fixed-point
+// coordinates and forces, Synthesis/phasespace_synthesis.h:325), ImplicitSolventWorkspace
+// (Synthesis/implicit_solvent_workspace.h:65) and ScoreCard (Potential/scorecard.h:101) for this
+// path, as device arrays in the layout described in device_kits.h.
+#ifndef STORMM_B200_SYNTHESIS_H
+#define STORMM_B200_SYNTHESIS_H
+
+#include <cuda_runtime.h>
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "stormm_b200.h"
+#include "device_kits.h"
+
+namespace sb {
+
+class Error : public std::runtime_error {
+public:
+  Error(int code_in, const std::string &msg) : std::runtime_error(msg), code(code_in) {}
+  int code;
+};
+
+void cudaCheck(cudaError_t err, const char* what);
+void setLastError(const std::string &msg);
+const char* lastError();
+
+// Device array owned by the synthesis (cudaMalloc / cudaFree)
+template <typename T> struct DeviceArray {
+  T* p = nullptr;
+  size_t n = 0;
+  DeviceArray() = default;
+  DeviceArray(const DeviceArray &) = delete;
+  DeviceArray& operator=(const DeviceArray &) = delete;
+  ~DeviceArray() {
+    if (p != nullptr) {
+      cudaFree(p);
+    }
+  }
+  void allocate(size_t count) {
+    if (p != nullptr) {
+      cudaFree(p);
+      p = nullptr;
+    }
+    n = count;
+    cudaCheck(cudaMalloc(reinterpret_cast<void**>(&p), sizeof(T) * (count > 0 ? count : 1)),
+              "cudaMalloc");
+  }
+  void zeros(size_t count) {
+    allocate(count);
+    cudaCheck(cudaMemset(p, 0, sizeof(T) * (count > 0 ? count : 1)), "cudaMemset");
+  }
+  void upload(const std::vector<T> &v) {
+    allocate(v.size());
+    if (!v.empty()) {
+      cudaCheck(cudaMemcpy(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice),
+                "cudaMemcpy");
+    }
+  }
+};
+
+class Synthesis {
+public:
+  Synthesis(const sb_topology* tops, int ntop, const int* topology_index, int nsys,
+            const sb_options &options);
+
+  void evaluate(int terms, bool force, bool energy, cudaStream_t stream);
+  void evaluateRange(int first, int count, int terms, bool force, bool energy,
+                     cudaStream_t stream);
+  void initialize(int what, cudaStream_t stream);
+  void setCoordinates(const double* xyz, cudaStream_t stream);
+  void getCoordinates(double* xyz, cudaStream_t stream);
+  void getForces(double* xyz, cudaStream_t stream);
+  void getForcesFixed(long long* prim, int* ovrf, cudaStream_t stream);
+  void getEnergies(double* out, cudaStream_t stream);
+  void getEnergiesFixed(long long* out, cudaStream_t stream);
+  void getGbWorkspace(double* psi, double* radii, double* sde, cudaStream_t stream);
+  int checkStatus(cudaStream_t stream);
+
+  sb_options opt;
+  int nsys = 0;
+  int natom_padded = 0;
+  int sm_count = 0;
+  int max_smem_optin = 0;
+  int threads = 256;
+  int max_lj = 0;
+  int max_unit_slots = 0;
+  std::vector<int> topo;
+  std::vector<int> atom_start;
+  std::vector<int> atom_count;
+
+  // host staging of the packed layout
+  std::vector<float> h_charge, h_rho, h_srho, h_pb, h_alpha, h_beta, h_gamma;
+  std::vector<int> h_ljidx, h_lj_start, h_lj_ntypes, h_tile_start, h_tile_mask_idx;
+  std::vector<int> h_bond_start, h_angl_start, h_dihe_start;
+  std::vector<float2> h_ljab, h_ljab14;
+  std::vector<uint4> h_bonds, h_angles, h_dihe_a, h_dihe_b;
+  std::vector<unsigned int> h_mask_pool;
+  std::vector<int4> h_units, h_single_units;
+  std::vector<int> h_unit_systems, h_single_systems;
+  std::vector<long long> h_stage_ll;
+
+  // device arrays
+  DeviceArray<int> d_atom_start, d_atom_count, d_bond_start, d_angl_start, d_dihe_start;
+  DeviceArray<int> d_lj_start, d_lj_ntypes, d_tile_start, d_ljidx, d_tile_mask_idx;
+  DeviceArray<float> d_charge, d_rho, d_srho, d_pb, d_alpha, d_beta, d_gamma;
+  DeviceArray<float2> d_ljab, d_ljab14;
+  DeviceArray<uint4> d_bonds, d_angles, d_dihe_a, d_dihe_b;
+  DeviceArray<unsigned int> d_mask_pool;
+  DeviceArray<int4> d_units, d_single_units;
+  DeviceArray<int> d_unit_systems, d_single_systems;
+  DeviceArray<long long> d_xcrd, d_ycrd, d_zcrd, d_xfrc, d_yfrc, d_zfrc;
+  DeviceArray<int> d_xcrd_ovrf, d_ycrd_ovrf, d_zcrd_ovrf, d_xfrc_ovrf, d_yfrc_ovrf, d_zfrc_ovrf;
+  DeviceArray<unsigned long long> d_energies;
+  DeviceArray<long long> d_psi, d_sumdeijda;
+  DeviceArray<int> d_psi_ovrf, d_sumdeijda_ovrf, d_status;
+  DeviceArray<float> d_born_radii;
+
+  DevSynthesis dev;
+
+private:
+  void buildLayout(const sb_topology* tops, int ntop);
+  void buildUnits();
+  void upload();
+};
+
+}  // namespace sb
+
+#endif

@@ -1,0 +1,68 @@
+"""Helpers that turn golden fixtures into molecule objects for the library and the oracle."""
+import glob
+import os
+from types import SimpleNamespace
+
+import numpy as np
+
+from conftest import GOLDEN
+
+
+def load(name):
+    return dict(np.load(os.path.join(GOLDEN, name)))
+
+
+def synthetic_paths():
+    return sorted(glob.glob(os.path.join(GOLDEN, "synthetic_*.npz")))
+
+
+def reference_paths():
+    return sorted(glob.glob(os.path.join(GOLDEN, "reference_*.npz")))
+
+
+def molecule_from_fixture(g):
+    """Topology exactly as STORMM parsed it (charges after smoothing, LJ tables, GB parameters,
+    valence terms with their 1-4 attenuation), as the attributes the library expects."""
+    n = int(g["natom"][0])
+    nt = int(g["n_lj_types"][0])
+
+    def sets(key):
+        b, x = g[key + "_bounds"], g[key + "x"]
+        return [set(int(v) for v in x[b[i]:b[i + 1]]) for i in range(n)]
+
+    e11 = sets("nb11")
+    e12 = sets("nb12")
+    e13 = sets("nb13")
+    e14 = sets("nb14")
+    for i in range(n):
+        e12[i] |= e11[i]
+    scee = np.asarray(g["dihe_scee"], dtype=np.float64)
+    return SimpleNamespace(
+        natom=n, coords=g["coords"].reshape(n, 3), charge=g["charge"], lj_idx=g["lj_idx"],
+        n_lj_types=nt, lja=g["lja"].reshape(nt, nt), ljb=g["ljb"].reshape(nt, nt),
+        lja14=g["lja14"].reshape(nt, nt), ljb14=g["ljb14"].reshape(nt, nt),
+        excl12=e12, excl13=e13, excl14=e14, pb_radii=g["pb_radii"], gb_screen=g["gb_screen"],
+        gb_alpha=g["gb_alpha"], gb_beta=g["gb_beta"], gb_gamma=g["gb_gamma"],
+        bonds=np.stack([g["bond_i"], g["bond_j"]], axis=1), bond_k=g["bond_k"],
+        bond_r0=g["bond_r0"],
+        angles=np.stack([g["angl_i"], g["angl_j"], g["angl_k"]], axis=1), angl_k=g["angl_k_eq"],
+        angl_theta0=g["angl_theta0"],
+        dihedrals=np.stack([g["dihe_i"], g["dihe_j"], g["dihe_k"], g["dihe_l"]], axis=1),
+        dihe_amp=g["dihe_amp"], dihe_freq=g["dihe_freq"], dihe_phase=g["dihe_phase"],
+        dihe_has14=scee > 0.0, dihe_scee_array=scee, dihe_scnb_array=g["dihe_scnb"],
+        dihe_improper=(np.asarray(g["dihe_kind"]) >= 2).astype(np.int32), scee=1.2, scnb=2.0,
+        name="fixture")
+
+
+def igb_of_fixture(g):
+    """Amber igb number of the fixture's implicit solvent model (STORMM enum order)."""
+    return {0: 0, 1: 1, 2: 2, 3: 5}[int(g["igb"][0])]
+
+
+def reference_forces(g):
+    return (g["frc_bond"] + g["frc_angle"] + g["frc_dihedral"] + g["frc_14"] +
+            g["frc_nonbonded"] + g["frc_gb"]).reshape(-1, 3)
+
+
+def rms_rel(a, b):
+    return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))

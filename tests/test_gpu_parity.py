@@ -1,0 +1,172 @@
+"""CUDA path against the FP64 oracle and STORMM's own CPU results, through the C ABI.
+
+Tolerances (FP32 arithmetic with fixed-point accumulation against FP64):
+* energies: each term within 1e-6 of the system's summed absolute energy, and the total within
+  1e-6 relative;
+* forces: RMS relative error at most 5e-6 against FP64;
+* fixed-point sums: bit-identical across runs, across batch compositions and between the batched
+  and the per-system launches.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+import stormm_b200 as sb
+from fixtures import (igb_of_fixture, load, molecule_from_fixture, reference_forces,
+                      reference_paths, rms_rel, synthetic_paths)
+
+pytestmark = pytest.mark.gpu
+
+ENERGY_TOL = 1.0e-6
+FORCE_TOL = 5.0e-6
+
+
+def _run(mols, igb=5, dielectric=80.0, terms=sb.TERM_ALL, coords=None, **opts):
+    syn = sb.Synthesis(mols, igb=igb, dielectric=dielectric, **opts)
+    xyz = np.concatenate([m.coords for m in mols]) if coords is None else coords
+    syn.set_coordinates(xyz)
+    syn.initialize()
+    syn.evaluate(terms=terms)
+    out = {"energies": syn.energy_terms(), "forces": syn.forces(), "syn": syn}
+    assert syn.status() == 0
+    return out
+
+
+def _check_energy(e_gpu, e_ref):
+    scale = max(np.abs(e_ref).sum(), 1.0)
+    assert np.all(np.abs(e_gpu - e_ref) <= ENERGY_TOL * scale), (e_gpu, e_ref)
+    assert abs(e_gpu.sum() - e_ref.sum()) <= ENERGY_TOL * max(abs(e_ref.sum()), scale * 1e-2)
+
+
+@pytest.mark.parametrize("path", synthetic_paths(), ids=os.path.basename)
+def test_single_system_matches_stormm(path):
+    g = load(os.path.basename(path))
+    mol = molecule_from_fixture(g)
+    r = _run([mol], igb=igb_of_fixture(g), dielectric=float(g["dielectric"][0]))
+    _check_energy(r["energies"][0], g["energy_terms"])
+    err = rms_rel(r["forces"], reference_forces(g))
+    assert err <= FORCE_TOL, err
+
+
+@pytest.mark.parametrize("path", reference_paths(), ids=os.path.basename)
+def test_reference_systems_known_answers(path):
+    """Trp-cage and alanine dipeptide under HCT, OBC and OBC-II, against STORMM's CPU results
+    and the known GB energies of test/Potential/test_generalized_born.cpp:296-300."""
+    g = load(os.path.basename(path))
+    mol = molecule_from_fixture(g)
+    r = _run([mol], igb=igb_of_fixture(g), dielectric=float(g["dielectric"][0]))
+    _check_energy(r["energies"][0], g["energy_terms"])
+    assert abs(r["energies"][0][8] - g["known_answer_gb"][0]) < 1e-3
+    assert rms_rel(r["forces"], reference_forces(g)) <= FORCE_TOL
+
+
+def test_gb_workspace_matches_stormm():
+    g = load("synthetic_E100.npz")
+    r = _run([molecule_from_fixture(g)])
+    psi, rad, sde = r["syn"].gb_workspace()
+    np.testing.assert_allclose(psi, g["gb_psi"], rtol=1e-5, atol=1e-6)
+    np.testing.assert_allclose(rad, g["gb_radii"], rtol=1e-5)
+    np.testing.assert_allclose(sde, g["gb_sumdeijda"], rtol=1e-4, atol=1e-4)
+
+
+def test_batch_of_mixed_sizes_is_bit_identical_to_single_runs():
+    paths = synthetic_paths()
+    mols = [molecule_from_fixture(load(os.path.basename(p))) for p in paths]
+    batch = _run(mols)
+    prim_b, ovrf_b = batch["syn"].forces_fixed()
+    ef_b = batch["syn"].energies_fixed()
+    offs = []
+    for k, m in enumerate(mols):
+        single = _run([m])
+        prim_s, ovrf_s = single["syn"].forces_fixed()
+        _, off = _system_layout(batch["syn"], k)
+        n = m.natom
+        assert np.array_equal(prim_b[:, off:off + n], prim_s[:, :n])
+        assert np.array_equal(ovrf_b[:, off:off + n], ovrf_s[:, :n])
+        assert np.array_equal(ef_b[k], single["syn"].energies_fixed()[0])
+        offs.append(off)
+    # and each system still matches STORMM
+    for k, p in enumerate(paths):
+        g = load(os.path.basename(p))
+        _check_energy(batch["energies"][k], g["energy_terms"])
+
+
+def _system_layout(syn, k):
+    import ctypes
+    n, off = ctypes.c_int(), ctypes.c_int()
+    sb.library().sb_system_atoms(syn.handle, k, ctypes.byref(n), ctypes.byref(off))
+    return n.value, off.value
+
+
+def test_run_to_run_bit_identical():
+    mols = [molecule_from_fixture(load("synthetic_E300.npz")),
+            molecule_from_fixture(load("synthetic_M0.npz"))]
+    a = _run(mols)["syn"]
+    first = a.forces_fixed()
+    first_e = a.energies_fixed()
+    for _ in range(3):
+        a.initialize()
+        a.evaluate()
+        again = a.forces_fixed()
+        assert np.array_equal(first[0], again[0]) and np.array_equal(first[1], again[1])
+        assert np.array_equal(first_e, a.energies_fixed())
+
+
+def test_per_system_launches_match_batched():
+    mols = [molecule_from_fixture(load(os.path.basename(p))) for p in synthetic_paths()[:6]]
+    batch = _run(mols)["syn"]
+    ref_prim, ref_ovrf = batch.forces_fixed()
+    ref_e = batch.energies_fixed()
+    batch.initialize()
+    batch.evaluate_range(0, len(mols))
+    prim, ovrf = batch.forces_fixed()
+    assert np.array_equal(prim, ref_prim) and np.array_equal(ovrf, ref_ovrf)
+    assert np.array_equal(batch.energies_fixed(), ref_e)
+
+
+def test_separate_launchers_sum_to_fused():
+    mols = [molecule_from_fixture(load("synthetic_M0.npz")),
+            molecule_from_fixture(load("synthetic_E48.npz"))]
+    syn = _run(mols)["syn"]
+    fused_e = syn.energies_fixed()
+    fused_f = syn.forces_fixed()
+    syn.initialize()
+    syn.launch_nonbonded()
+    syn.launch_valence()
+    assert np.array_equal(syn.energies_fixed(), fused_e)
+    f = syn.forces_fixed()
+    assert np.array_equal(f[0], fused_f[0]) and np.array_equal(f[1], fused_f[1])
+
+
+def test_energy_only_matches_force_energy():
+    mols = [molecule_from_fixture(load("synthetic_E257.npz"))]
+    syn = _run(mols)["syn"]
+    e_fe = syn.energies_fixed()
+    syn.initialize()
+    syn.evaluate(force=False, energy=True)
+    assert np.array_equal(syn.energies_fixed(), e_fe)
+    assert not syn.forces().any()
+
+
+def test_synthetic_batch_against_oracle():
+    """A batch of fresh synthetic molecules (sizes 16-256) against the FP64 oracle."""
+    from stormm_b200 import synthetic
+    mols = [synthetic.make_molecule(500 + k, n) for k, n in enumerate(
+        [16, 23, 31, 32, 33, 47, 64, 65, 96, 127, 128, 129, 200, 255, 256])]
+    r = _run(mols)
+    f_all = r["forces"]
+    off = 0
+    for k, m in enumerate(mols):
+        o = oracle.from_molecule(m).evaluate(m.coords)
+        _check_energy(r["energies"][k], o["energies"])
+        err = rms_rel(f_all[off:off + m.natom], o["forces"])
+        assert err <= FORCE_TOL, (m.natom, err)
+        off += m.natom
+
+
+def test_unsupported_model_is_rejected():
+    mol = molecule_from_fixture(load("synthetic_E12.npz"))
+    with pytest.raises(sb.StormmB200Error):
+        sb.Synthesis([mol], igb=7)

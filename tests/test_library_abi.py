@@ -1,0 +1,42 @@
+"""The C-ABI library loads and exports every entry point include/stormm_b200.h declares.  These
+checks make no compute call, so they run without a GPU."""
+import ctypes
+import os
+import re
+
+import pytest
+
+import stormm_b200
+from conftest import ROOT
+
+
+def declared_functions():
+    text = open(os.path.join(ROOT, "include", "stormm_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(sb_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert "sb_synthesis_create" in names and "sb_evaluate" in names
+    assert len(names) >= 20
+
+
+def test_library_exports_every_declared_symbol():
+    lib = stormm_b200.library()
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, f"symbols declared but not exported: {missing}"
+
+
+def test_version_and_defaults_without_gpu():
+    lib = stormm_b200.library()
+    assert b"sm_100a" in lib.sb_version()
+    o = stormm_b200.default_options()
+    assert o.igb == 5 and o.dielectric == 80.0 and o.frc_bits == 23 and o.gpos_bits == 32
+
+
+def test_null_handle_is_an_error():
+    lib = stormm_b200.library()
+    rc = lib.sb_evaluate(None, 7, 1, 1, None)
+    assert rc == -1
+    assert b"null" in lib.sb_last_error()
