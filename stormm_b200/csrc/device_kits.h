@@ -21,6 +21,7 @@ namespace sb {
 
 constexpr int kTile = 32;                 // atoms per tile edge (one warp lane per atom)
 constexpr int kMaxUnitSystems = 32;       // systems per fused work unit
+constexpr int kMaxFusedAtoms = 2048;      // largest molecule the fused path holds on chip
 constexpr int kNrgStride = 16;            // energy slots per system (STORMM StateVariable order)
 constexpr float kGbRadiiOffset = 0.09f;   // Constants/generalized_born.h:114
 constexpr float kGbKscale = 0.73f;        // Constants/generalized_born.h:123
@@ -33,10 +34,11 @@ enum NrgSlot : int {
   kElec = 9, kElec14 = 10, kGb = 11
 };
 
-// Bond record:     x = i | j << 16, y = keq (float bits), z = leq (float bits), w = 0
+// Bond record:     x = i | j << 16, y = keq, z = leq (high float), w = leq - z (low float)
 // Angle record:    x = i | j << 16, y = k, z = keq, w = theta0
-// Dihedral record: a.x = i | j << 16, a.y = k | l << 16, a.z = amp, a.w = phase
-//                  b.x = freq, b.y = 1/scee (0: no 1-4), b.z = 1/scnb, b.w = flags (1: improper)
+// Dihedral record: a.x = i | j << 16, a.y = k | l << 16 | improper << 31, a.z = amp, a.w = freq
+//                  b.x = cos(phase), b.y = sin(phase), b.z = 1/scee (0: no 1-4), b.w = 1/scnb
+// (floats stored as their bit patterns; indices are molecule-local)
 struct DevSynthesis {
   int nsys;
   int natom_padded;

@@ -236,7 +236,8 @@ template <bool FORCE, bool ENERGY>
 __device__ void valenceTerms(const DevSynthesis &d, const UnitSmem &s, int nsys_u) {
   const float fs = d.frc_scale;
   const float es = d.nrg_scale;
-  // bonds, valence_potential.tpp:9-97
+  // bonds, valence_potential.tpp:9-97; the equilibrium length is held as a float pair so that
+  // r - r0 loses nothing to the rounding of r0
   const int nbond = s.bond0[nsys_u];
   for (int f = threadIdx.x; f < nbond; f += blockDim.x) {
     const int k = findOwner(s.bond0, nsys_u, f);
@@ -244,20 +245,54 @@ __device__ void valenceTerms(const DevSynthesis &d, const UnitSmem &s, int nsys_
     const int ia = s.slot0[k] + static_cast<int>(rec.x & 0xffffu);
     const int ja = s.slot0[k] + static_cast<int>(rec.x >> 16);
     const float keq = __uint_as_float(rec.y);
-    const float leq = __uint_as_float(rec.z);
-    const float3 dv = slotDelta(s, ia, ja);
-    const float r = sqrtf(dv.x * dv.x + dv.y * dv.y + dv.z * dv.z);
-    const float dl = r - leq;
+    const float leq_hi = __uint_as_float(rec.z);
+    const float leq_lo = __uint_as_float(rec.w);
+    // bond length as an unevaluated float pair: each coordinate difference is the exact sum of
+    // the high-part difference (TwoSum) and the low parts, the squared length keeps the FMA
+    // residues, and the square root gets one Newton correction
+    float dh[3], dlo[3];
+    {
+      const float4 hi_i = s.hi[ia], hi_j = s.hi[ja], lo_i = s.lo[ia], lo_j = s.lo[ja];
+      const float a[3] = {hi_j.x, hi_j.y, hi_j.z};
+      const float b[3] = {hi_i.x, hi_i.y, hi_i.z};
+      const float la[3] = {lo_j.x, lo_j.y, lo_j.z};
+      const float lb[3] = {lo_i.x, lo_i.y, lo_i.z};
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const float sdiff = a[c] - b[c];
+        const float bb = sdiff - a[c];
+        const float err = (a[c] - (sdiff - bb)) + (-b[c] - bb);
+        const float lo = err + (la[c] - lb[c]);
+        dh[c] = sdiff + lo;
+        dlo[c] = lo - (dh[c] - sdiff);
+      }
+    }
+    const float3 dv = make_float3(dh[0], dh[1], dh[2]);
+    float r2h = dh[0] * dh[0];
+    float r2l = fmaf(dh[0], dh[0], -r2h) + 2.0f * dh[0] * dlo[0];
+#pragma unroll
+    for (int c = 1; c < 3; c++) {
+      const float p = dh[c] * dh[c];
+      const float pe = fmaf(dh[c], dh[c], -p) + 2.0f * dh[c] * dlo[c];
+      const float sum = r2h + p;
+      const float bv = sum - r2h;
+      r2l += ((r2h - (sum - bv)) + (p - bv)) + pe;
+      r2h = sum;
+    }
+    const float r = sqrtf(r2h);
+    const float r_lo = (fmaf(-r, r, r2h) + r2l) / (2.0f * r);
+    const float dl = ((r - leq_hi) + r_lo) - leq_lo;
     if (FORCE) {
       const float fmag = 2.0f * keq * dl / r;
       addForce(s, ia, fmag * dv.x, fmag * dv.y, fmag * dv.z, fs);
       addForce(s, ja, -fmag * dv.x, -fmag * dv.y, -fmag * dv.z, fs);
     }
     if (ENERGY) {
-      addEnergy(s, k, kBond, keq * dl * dl, es);
+      addEnergy(s, k, kBond, __fmul_rn(__fmul_rn(keq, dl), dl), es);
     }
   }
-  // angles, valence_potential.tpp:170-288
+  // angles, valence_potential.tpp:170-288.  The angle comes from atan2(|ba x bc|, ba . bc),
+  // which stays well conditioned where acos of the cosine does not.
   const int nangl = s.angl0[nsys_u];
   for (int f = threadIdx.x; f < nangl; f += blockDim.x) {
     const int k = findOwner(s.angl0, nsys_u, f);
@@ -266,17 +301,26 @@ __device__ void valenceTerms(const DevSynthesis &d, const UnitSmem &s, int nsys_
     const int ja = s.slot0[k] + static_cast<int>(rec.x >> 16);
     const int ka = s.slot0[k] + static_cast<int>(rec.y);
     const float keq = __uint_as_float(rec.z);
-    const float th0 = __uint_as_float(rec.w);
+    float sth0, cth0;
+    sincosf(__uint_as_float(rec.w), &sth0, &cth0);
     const float3 ba = slotDelta(s, ja, ia);
     const float3 bc = slotDelta(s, ja, ka);
     const float mgba = ba.x * ba.x + ba.y * ba.y + ba.z * ba.z;
     const float mgbc = bc.x * bc.x + bc.y * bc.y + bc.z * bc.z;
     const float invbabc = 1.0f / sqrtf(mgba * mgbc);
-    float costheta = (ba.x * bc.x + ba.y * bc.y + ba.z * bc.z) * invbabc;
-    costheta = fminf(fmaxf(costheta, -1.0f), 1.0f);
-    const float dtheta = acosf(costheta) - th0;
+    const float dotp = ba.x * bc.x + ba.y * bc.y + ba.z * bc.z;
+    const float cx = ba.y * bc.z - ba.z * bc.y;
+    const float cy = ba.z * bc.x - ba.x * bc.z;
+    const float cz = ba.x * bc.y - ba.y * bc.x;
+    const float crs = sqrtf(cx * cx + cy * cy + cz * cz);
+    // theta - theta0 = atan2(sin(theta - theta0), cos(theta - theta0)), with the sine and cosine
+    // of theta from the cross and dot products and those of theta0 from the record
+    const float sth = crs * invbabc;
+    const float cth = dotp * invbabc;
+    const float dtheta = atan2f(fmaf(sth, cth0, -cth * sth0), fmaf(cth, cth0, sth * sth0));
     if (FORCE) {
-      const float dA = -2.0f * keq * dtheta / sqrtf(1.0f - costheta * costheta);
+      const float costheta = dotp * invbabc;
+      const float dA = -2.0f * keq * dtheta / (crs * invbabc);
       const float sqba = dA / mgba;
       const float sqbc = dA / mgbc;
       const float mbabc = dA * invbabc;
@@ -291,10 +335,14 @@ __device__ void valenceTerms(const DevSynthesis &d, const UnitSmem &s, int nsys_
       addForce(s, ka, -cdx, -cdy, -cdz, fs);
     }
     if (ENERGY) {
-      addEnergy(s, k, kAngle, keq * dtheta * dtheta, es);
+      addEnergy(s, k, kAngle, __fmul_rn(__fmul_rn(keq, dtheta), dtheta), es);
     }
   }
-  // dihedrals with attached 1-4 pairs, valence_potential.tpp:359-578, 1288-1420
+  // dihedrals with attached 1-4 pairs, valence_potential.tpp:359-578, 1288-1420.  The signed
+  // angle is carried as (cos, sin) from x = (ab x bc) . (bc x cd) and y = |bc| ab . (bc x cd),
+  // the same angle STORMM's acos / arcsine route gives (Math/rounding.tpp:25-80) without its
+  // ill conditioning near 0 and pi; cos(n theta - phase) and sin(n theta - phase) follow from
+  // the multiple-angle recurrence for integer periodicities.
   const int ndihe = s.dihe0[nsys_u];
   for (int f = threadIdx.x; f < ndihe; f += blockDim.x) {
     const int k = findOwner(s.dihe0, nsys_u, f);
@@ -304,10 +352,12 @@ __device__ void valenceTerms(const DevSynthesis &d, const UnitSmem &s, int nsys_
     const int ia = s.slot0[k] + static_cast<int>(ra.x & 0xffffu);
     const int ja = s.slot0[k] + static_cast<int>(ra.x >> 16);
     const int ka = s.slot0[k] + static_cast<int>(ra.y & 0xffffu);
-    const int la = s.slot0[k] + static_cast<int>(ra.y >> 16);
+    const int la = s.slot0[k] + static_cast<int>((ra.y >> 16) & 0x7fffu);
+    const bool improper = (ra.y & 0x80000000u) != 0u;
     const float amp = __uint_as_float(ra.z);
-    const float phase = __uint_as_float(ra.w);
-    const float freq = __uint_as_float(rb.x);
+    const float freq = __uint_as_float(ra.w);
+    const float cphase = __uint_as_float(rb.x);
+    const float sphase = __uint_as_float(rb.y);
     const float3 ab = slotDelta(s, ia, ja);
     const float3 bc = slotDelta(s, ja, ka);
     const float3 cd = slotDelta(s, ka, la);
@@ -315,40 +365,33 @@ __device__ void valenceTerms(const DevSynthesis &d, const UnitSmem &s, int nsys_
                                 ab.x * bc.y - ab.y * bc.x);
     float3 crbccd = make_float3(bc.y * cd.z - bc.z * cd.y, bc.z * cd.x - bc.x * cd.z,
                                 bc.x * cd.y - bc.y * cd.x);
-    const float m1 = crabbc.x * crabbc.x + crabbc.y * crabbc.y + crabbc.z * crabbc.z;
-    const float m2 = crbccd.x * crbccd.x + crbccd.y * crbccd.y + crbccd.z * crbccd.z;
-    float costheta = (crabbc.x * crbccd.x + crabbc.y * crbccd.y + crabbc.z * crbccd.z) /
-                     sqrtf(m1 * m2);
-    const float3 scr = make_float3(crabbc.y * crbccd.z - crabbc.z * crbccd.y,
-                                   crabbc.z * crbccd.x - crabbc.x * crbccd.z,
-                                   crabbc.x * crbccd.y - crabbc.y * crbccd.x);
-    costheta = fminf(fmaxf(costheta, -1.0f), 1.0f);
-    // signed angle; near 0 or pi take the arcsine route (Math/rounding.tpp:25-80)
-    const float sgn = (scr.x * bc.x + scr.y * bc.y + scr.z * bc.z > 0.0f) ? 1.0f : -1.0f;
-    float theta;
-    if (fabsf(costheta) >= 0.99993896484375f) {
-      const float ia1 = rsqrtf(m1);
-      const float ib1 = rsqrtf(m2);
-      float rx = crbccd.x * ib1 - crabbc.x * ia1;
-      float ry = crbccd.y * ib1 - crabbc.y * ia1;
-      float rz = crbccd.z * ib1 - crabbc.z * ia1;
-      float rs = sqrtf(rx * rx + ry * ry + rz * rz);
-      if (rs > 1.0f) {
-        rx = crbccd.x * ib1 + crabbc.x * ia1;
-        ry = crbccd.y * ib1 + crabbc.y * ia1;
-        rz = crbccd.z * ib1 + crabbc.z * ia1;
-        rs = 3.14159265358979323846f - sqrtf(rx * rx + ry * ry + rz * rz);
+    const float mgbc = sqrtf(bc.x * bc.x + bc.y * bc.y + bc.z * bc.z);
+    const float xx = crabbc.x * crbccd.x + crabbc.y * crbccd.y + crabbc.z * crbccd.z;
+    const float yy = mgbc * (ab.x * crbccd.x + ab.y * crbccd.y + ab.z * crbccd.z);
+    const float inv_rr = rsqrtf(fmaf(xx, xx, yy * yy));
+    const float c1 = xx * inv_rr;
+    const float s1 = yy * inv_rr;
+    float cn, sn;
+    const int nint = static_cast<int>(freq);
+    if (static_cast<float>(nint) == freq && nint >= 1 && nint <= 6) {
+      cn = c1;
+      sn = s1;
+      for (int m = 1; m < nint; m++) {
+        const float cnew = cn * c1 - sn * s1;
+        sn = sn * c1 + cn * s1;
+        cn = cnew;
       }
-      theta = sgn * rs;
     }
     else {
-      theta = sgn * acosf(costheta);
+      const float th = atan2f(yy, xx);
+      sincosf(freq * th, &sn, &cn);
     }
-    const float sangle = freq * theta - phase;
+    // sangle = n theta - phase
+    const float cos_sangle = cn * cphase + sn * sphase;
+    const float sin_sangle = sn * cphase - cn * sphase;
     if (FORCE) {
-      const float fr = amp * freq * sinf(sangle);
+      const float fr = amp * freq * sin_sangle;
       const float mgab = sqrtf(ab.x * ab.x + ab.y * ab.y + ab.z * ab.z);
-      const float mgbc = sqrtf(bc.x * bc.x + bc.y * bc.y + bc.z * bc.z);
       const float mgcd = sqrtf(cd.x * cd.x + cd.y * cd.y + cd.z * cd.z);
       const float invab = 1.0f / mgab;
       const float invbc = 1.0f / mgbc;
@@ -382,13 +425,13 @@ __device__ void valenceTerms(const DevSynthesis &d, const UnitSmem &s, int nsys_
       addForce(s, la, flx, fly, flz, fs);
     }
     if (ENERGY) {
-      addEnergy(s, k, (rb.w & 1u) ? kImproperDihedral : kProperDihedral,
-                amp * (1.0f + cosf(sangle)), es);
+      addEnergy(s, k, improper ? kImproperDihedral : kProperDihedral,
+                __fmul_rn(amp, __fadd_rn(1.0f, cos_sangle)), es);
     }
     // attached 1-4 pair between atoms i and l
-    const float inv_scee = __uint_as_float(rb.y);
+    const float inv_scee = __uint_as_float(rb.z);
     if (inv_scee > 0.0f) {
-      const float inv_scnb = __uint_as_float(rb.z);
+      const float inv_scnb = __uint_as_float(rb.w);
       const float3 dv = slotDelta(s, ia, la);
       const float4 hi_i = s.hi[ia];
       const float4 hi_l = s.hi[la];
@@ -410,8 +453,9 @@ __device__ void valenceTerms(const DevSynthesis &d, const UnitSmem &s, int nsys_
         addForce(s, la, -fmag * dv.x, -fmag * dv.y, -fmag * dv.z, fs);
       }
       if (ENERGY) {
-        addEnergy(s, k, kElec14, qiqj * invr, es);
-        addEnergy(s, k, kVdw14, lja * invr4 * invr4 * invr4 - ljb * invr4 * invr2, es);
+        addEnergy(s, k, kElec14, __fmul_rn(qiqj, invr), es);
+        addEnergy(s, k, kVdw14, __fsub_rn(__fmul_rn(__fmul_rn(__fmul_rn(lja, invr4), invr4), invr4),
+                                          __fmul_rn(__fmul_rn(ljb, invr4), invr2)), es);
       }
     }
   }
@@ -554,8 +598,9 @@ __device__ void pairTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u, 
           const float invr4 = invr2 * invr2;
           const float2 ab = s.lj[code_i + (__float_as_int(lo_j.w) >> 16)];
           if (ENERGY) {
-            e_elec += qiqj * invr;
-            e_vdw += (ab.x * invr4 * invr4 - ab.y * invr2) * invr4;
+            e_elec = __fadd_rn(e_elec, __fmul_rn(qiqj, invr));
+            e_vdw = __fadd_rn(e_vdw, __fmul_rn(__fsub_rn(__fmul_rn(__fmul_rn(ab.x, invr4), invr4),
+                                                         __fmul_rn(ab.y, invr2)), invr4));
           }
           if (FORCE) {
             fmag = -(qiqj * invr * invr2) +
@@ -578,7 +623,7 @@ __device__ void pairTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u, 
           }
           const float dielfac = 1.0f - expmkf;
           if (ENERGY) {
-            e_gb -= qiqj * dielfac * fgbi;
+            e_gb = __fsub_rn(e_gb, __fmul_rn(__fmul_rn(qiqj, dielfac), fgbi));
           }
           if (FORCE) {
             const float temp4 = fgbi * fgbi * fgbi;
@@ -822,6 +867,7 @@ kEvalFused(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
 
     if (VALE) {
       valenceTerms<FORCE, ENERGY>(d, s, nsys_u);
+      __syncthreads();
     }
     if (gb) {
       gbRadiiTiles(d, s, nsys_u, ntiles);
@@ -857,7 +903,7 @@ kEvalFused(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
         const float atmq2h = 0.5f * q * q;
         const float atmqd2h = atmq2h * dielfac;
         if (ENERGY) {
-          addEnergy(s, k, kGb, -atmqd2h / egbi, d.nrg_scale);
+          addEnergy(s, k, kGb, -__fdiv_rn(atmqd2h, egbi), d.nrg_scale);
         }
         if (FORCE) {
           const float self_de = atmqd2h - kGbKscale * d.kappa * atmq2h * expmkf * egbi;

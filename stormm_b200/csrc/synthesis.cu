@@ -230,7 +230,9 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
     for (int b = 0; b < tp.nbond; b++) {
       const uint32_t i = check_atom(tp.bond_atoms[2 * b]);
       const uint32_t j = check_atom(tp.bond_atoms[2 * b + 1]);
-      h_bonds.push_back(make_uint4(i | (j << 16), fbits(tp.bond_keq[b]), fbits(tp.bond_leq[b]), 0u));
+      const float leq_hi = static_cast<float>(tp.bond_leq[b]);
+      h_bonds.push_back(make_uint4(i | (j << 16), fbits(tp.bond_keq[b]), fbits(leq_hi),
+                                   fbits(tp.bond_leq[b] - static_cast<double>(leq_hi))));
     }
     h_bond_start[s + 1] = h_bonds.size();
     for (int a = 0; a < tp.nangl; a++) {
@@ -248,11 +250,17 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
       const uint32_t l = check_atom(tp.dihe_atoms[4 * d + 3]);
       const double scee = (tp.dihe_scee != nullptr) ? tp.dihe_scee[d] : 0.0;
       const double scnb = (tp.dihe_scnb != nullptr) ? tp.dihe_scnb[d] : 0.0;
-      const uint32_t flags = (tp.dihe_improper != nullptr && tp.dihe_improper[d] != 0) ? 1u : 0u;
-      h_dihe_a.push_back(make_uint4(i | (j << 16), k | (l << 16), fbits(tp.dihe_amp[d]),
-                                    fbits(tp.dihe_phase[d])));
-      h_dihe_b.push_back(make_uint4(fbits(tp.dihe_freq[d]), fbits(scee > 0.0 ? 1.0 / scee : 0.0),
-                                    fbits((scee > 0.0 && scnb > 0.0) ? 1.0 / scnb : 0.0), flags));
+      const uint32_t improper =
+        (tp.dihe_improper != nullptr && tp.dihe_improper[d] != 0) ? 0x80000000u : 0u;
+      if (l > 0x7fffu) {
+        throw Error(SB_ERR_UNSUPPORTED, "dihedral atom index above 32767");
+      }
+      h_dihe_a.push_back(make_uint4(i | (j << 16), k | (l << 16) | improper, fbits(tp.dihe_amp[d]),
+                                    fbits(tp.dihe_freq[d])));
+      h_dihe_b.push_back(make_uint4(fbits(std::cos(tp.dihe_phase[d])),
+                                    fbits(std::sin(tp.dihe_phase[d])),
+                                    fbits(scee > 0.0 ? 1.0 / scee : 0.0),
+                                    fbits((scee > 0.0 && scnb > 0.0) ? 1.0 / scnb : 0.0)));
     }
     h_dihe_start[s + 1] = h_dihe_a.size();
   }
@@ -278,28 +286,41 @@ void Synthesis::buildUnits() {
   const int max_lj_cap = 4096;
   h_units.clear();
   h_unit_systems.clear();
-  int4 cur = make_int4(0, 0, 0, 0);
-  int cur_lj = 0;
-  max_lj = 0;
-  max_unit_slots = 0;
-  for (int s : order) {
-    if (slots_of(s) > max_slots_cap) {
+  // molecules above the packing cap: one unit each, at the front (largest first)
+  n_big_units = 0;
+  big_slots = 0;
+  big_lj = 0;
+  size_t first_small = 0;
+  while (first_small < order.size() && slots_of(order[first_small]) > max_slots_cap) {
+    const int s = order[first_small];
+    if (atom_count[s] > kMaxFusedAtoms) {
       throw Error(SB_ERR_UNSUPPORTED, "system " + std::to_string(s) + " has " +
                   std::to_string(atom_count[s]) + " atoms; the fused path holds up to " +
-                  std::to_string(max_slots_cap) + " atoms per work unit");
+                  std::to_string(kMaxFusedAtoms) + " atoms per molecule");
     }
+    h_units.push_back(make_int4(static_cast<int>(h_unit_systems.size()), 1, slots_of(s),
+                                tiles_of(s)));
+    h_unit_systems.push_back(s);
+    big_slots = std::max(big_slots, slots_of(s));
+    big_lj = std::max(big_lj, lj_of(s));
+    n_big_units++;
+    first_small++;
+  }
+  int4 cur = make_int4(static_cast<int>(h_unit_systems.size()), 0, 0, 0);
+  int cur_lj = 0;
+  small_slots = 0;
+  small_lj = 0;
+  for (size_t oi = first_small; oi < order.size(); oi++) {
+    const int s = order[oi];
     const bool fits = cur.y > 0 && cur.y < kMaxUnitSystems &&
                       cur.z + slots_of(s) <= max_slots_cap &&
                       cur.w + tiles_of(s) <= max_tiles_cap && cur_lj + lj_of(s) <= max_lj_cap;
     if (!fits && cur.y > 0) {
       h_units.push_back(cur);
-      max_lj = std::max(max_lj, cur_lj);
-      max_unit_slots = std::max(max_unit_slots, cur.z);
+      small_lj = std::max(small_lj, cur_lj);
+      small_slots = std::max(small_slots, cur.z);
       cur = make_int4(static_cast<int>(h_unit_systems.size()), 0, 0, 0);
       cur_lj = 0;
-    }
-    if (cur.y == 0) {
-      cur.x = h_unit_systems.size();
     }
     h_unit_systems.push_back(s);
     cur.y++;
@@ -309,18 +330,22 @@ void Synthesis::buildUnits() {
   }
   if (cur.y > 0) {
     h_units.push_back(cur);
-    max_lj = std::max(max_lj, cur_lj);
-    max_unit_slots = std::max(max_unit_slots, cur.z);
+    small_lj = std::max(small_lj, cur_lj);
+    small_slots = std::max(small_slots, cur.z);
   }
   // one unit per system, in system order, for the per-system launches
   h_single_units.resize(nsys);
   h_single_systems.resize(nsys);
+  single_slots = 0;
+  single_lj = 0;
   for (int s = 0; s < nsys; s++) {
     h_single_units[s] = make_int4(s, 1, slots_of(s), tiles_of(s));
     h_single_systems[s] = s;
-    max_unit_slots = std::max(max_unit_slots, slots_of(s));
-    max_lj = std::max(max_lj, lj_of(s));
+    single_slots = std::max(single_slots, slots_of(s));
+    single_lj = std::max(single_lj, lj_of(s));
   }
+  max_unit_slots = std::max(std::max(big_slots, small_slots), single_slots);
+  max_lj = std::max(std::max(big_lj, small_lj), single_lj);
   const size_t smem = fusedSmemBytes(max_unit_slots, max_lj);
   if (static_cast<int>(smem) > max_smem_optin) {
     throw Error(SB_ERR_ARGUMENT, "work units need " + std::to_string(smem) +
@@ -443,8 +468,18 @@ void Synthesis::evaluate(int terms, bool force, bool energy, cudaStream_t stream
     return;
   }
   const int nunit = h_units.size();
-  cudaCheck(launchEvalFused(dev, 0, nunit, max_lj, terms, force, energy, nunit, threads, stream),
-            "fused evaluation launch");
+  if (n_big_units > 0) {
+    DevSynthesis d = dev;
+    d.max_unit_slots = big_slots;
+    cudaCheck(launchEvalFused(d, 0, n_big_units, big_lj, terms, force, energy, n_big_units,
+                              threads, stream), "fused evaluation launch (large molecules)");
+  }
+  if (nunit > n_big_units) {
+    DevSynthesis d = dev;
+    d.max_unit_slots = small_slots;
+    cudaCheck(launchEvalFused(d, n_big_units, nunit, small_lj, terms, force, energy,
+                              nunit - n_big_units, threads, stream), "fused evaluation launch");
+  }
 }
 
 void Synthesis::evaluateRange(int first, int count, int terms, bool force, bool energy,
@@ -462,8 +497,9 @@ void Synthesis::evaluateRange(int first, int count, int terms, bool force, bool 
   d.unit_desc = d_single_units.p;
   d.unit_systems = d_single_systems.p;
   d.nunit = nsys;
+  d.max_unit_slots = single_slots;
   for (int s = first; s < first + count; s++) {
-    cudaCheck(launchEvalFused(d, s, s + 1, max_lj, terms, force, energy, 1, threads, stream),
+    cudaCheck(launchEvalFused(d, s, s + 1, single_lj, terms, force, energy, 1, threads, stream),
               "per-system evaluation launch");
   }
 }

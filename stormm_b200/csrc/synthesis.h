@@ -90,6 +90,10 @@ public:
   int threads = 256;
   int max_lj = 0;
   int max_unit_slots = 0;
+  int n_big_units = 0;       // units [0, n_big_units) hold one molecule above the packing cap
+  int big_slots = 0, big_lj = 0;
+  int small_slots = 0, small_lj = 0;
+  int single_slots = 0, single_lj = 0;
   std::vector<int> topo;
   std::vector<int> atom_start;
   std::vector<int> atom_count;

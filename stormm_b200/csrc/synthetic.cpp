@@ -133,7 +133,30 @@ std::vector<V3> candidates(Rng &rng, const std::vector<V3> &dirs, int count) {
   for (V3 &d : out) {
     d = unit(d + V3{0.05 * rng.normal(), 0.05 * rng.normal(), 0.05 * rng.normal()});
   }
-  return out;
+  // Keep only directions whose angle to every existing bond lies in [85, 130] degrees, topping
+  // up with random directions in that window: near-linear bond angles make the dihedrals through
+  // them singular.
+  auto in_window = [&](const V3 &d) {
+    for (const V3 &b : dirs) {
+      const double c = dot(d, b);
+      if (c > std::cos(85.0 * kPi / 180.0) || c < std::cos(130.0 * kPi / 180.0)) {
+        return false;
+      }
+    }
+    return true;
+  };
+  std::vector<V3> kept;
+  for (const V3 &d : out) {
+    if (in_window(d)) kept.push_back(d);
+  }
+  for (int t = 0; t < 200 && static_cast<int>(kept.size()) < std::max(count / 2, 2); t++) {
+    const V3 d = randomUnit(rng);
+    if (in_window(d)) kept.push_back(d);
+  }
+  if (kept.empty()) {
+    kept = out;
+  }
+  return kept;
 }
 
 // Uniform cell grid for clash checks
@@ -513,8 +536,19 @@ int makeTree(uint64_t seed, int natom, double noise, sbsyn_molecule* out) {
       V3 best_p = {0.0, 0.0, 0.0};
       const double r = rng.uniform(1.00, 1.10);
       for (int par : heavy_ids) {
-        for (int t = 0; t < 6; t++) {
-          const V3 p = bld.pos[par] + r * randomUnit(rng);
+        for (int t = 0; t < 24; t++) {
+          const V3 dir = randomUnit(rng);
+          // keep every bond angle at the parent between 85 and 130 degrees
+          bool ok = true;
+          for (const V3 &b : bld.dirs[par]) {
+            const double c = dot(dir, b);
+            if (c > std::cos(85.0 * kPi / 180.0) || c < std::cos(130.0 * kPi / 180.0)) {
+              ok = false;
+              break;
+            }
+          }
+          if (!ok) continue;
+          const V3 p = bld.pos[par] + r * dir;
           std::vector<int> skip = bld.nbrs[par];
           skip.push_back(par);
           const double d = bld.grid.minDistance(p, bld.pos, skip, 3.0);
@@ -524,6 +558,9 @@ int makeTree(uint64_t seed, int natom, double noise, sbsyn_molecule* out) {
             best_p = p;
           }
         }
+      }
+      if (best_d < 0.0) {
+        best_p = bld.pos[best_par] + r * randomUnit(rng);
       }
       bld.capv[best_par]++;
       bld.commit(best_par, best_p, r, 1, 1);
