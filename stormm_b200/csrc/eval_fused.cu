@@ -22,6 +22,11 @@
 // Diagonal tiles take 16 steps, the last one on half the lanes, so every pair is visited once.
 // Forces, psi and dE/dR leave registers once per tile through integer shared-memory atomics,
 // so every sum is independent of scheduling and the results are bit-identical run to run.
+//
+// Shared memory per atom slot: pos_a = (x_hi, y_hi, z_hi, w1) and pos_b = (x_lo, y_lo, z_lo, w2)
+// feed the pair passes with two 16-byte loads per partner; w1 / w2 carry what the pass needs
+// (pass 1 and 3: s*rho and rho; pass 2: charge and effective radius).  prm holds the static
+// per-atom values, gbv the effective radius and the chain-rule dE/dR of the evaluation.
 #include <cuda_runtime.h>
 
 #include "device_kits.h"
@@ -32,21 +37,21 @@ namespace sb {
 namespace {
 
 // Constants/generalized_born.h:21-44 (Taylor series of the HCT integral at long range)
-__device__ __constant__ float kTaylorA = 0.33333333333333333333f;
-__device__ __constant__ float kTaylorB = 0.4f;
-__device__ __constant__ float kTaylorC = 0.42857142857142857143f;
-__device__ __constant__ float kTaylorD = 0.44444444444444444444f;
-__device__ __constant__ float kTaylorDD = 0.45454545454545454545f;
-__device__ __constant__ float kTaylorE = 1.33333333333333333333f;
-__device__ __constant__ float kTaylorF = 2.4f;
-__device__ __constant__ float kTaylorG = 3.42857142857142857143f;
-__device__ __constant__ float kTaylorH = 4.44444444444444444444f;
-__device__ __constant__ float kTaylorHH = 5.45454545454545454545f;
+constexpr float kTaylorA = 0.33333333333333333333f;
+constexpr float kTaylorB = 0.4f;
+constexpr float kTaylorC = 0.42857142857142857143f;
+constexpr float kTaylorD = 0.44444444444444444444f;
+constexpr float kTaylorDD = 0.45454545454545454545f;
+constexpr float kTaylorE = 1.33333333333333333333f;
+constexpr float kTaylorF = 2.4f;
+constexpr float kTaylorG = 3.42857142857142857143f;
+constexpr float kTaylorH = 4.44444444444444444444f;
+constexpr float kTaylorHH = 5.45454545454545454545f;
 
 constexpr unsigned kFullMask = 0xffffffffu;
 
 // HCT descreening of an atom of offset radius rho by a neighbour of screened radius sj at
-// distance r; returns the amount psi decreases by.
+// distance r (invr = 1/r); returns the amount psi decreases by.
 __device__ __forceinline__ float hctIntegral(float r, float r2, float invr, float rho, float sj) {
   const float sj2 = sj * sj;
   if (r > 4.0f * sj) {
@@ -56,16 +61,17 @@ __device__ __forceinline__ float hctIntegral(float r, float r2, float invr, floa
     return sj * t * invr2 * dumbo;
   }
   if (r > rho + sj) {
-    return 0.5f * (sj / (r2 - sj2) + 0.5f * invr * logf((r - sj) / (r + sj)));
+    return 0.5f * (__fdividef(sj, r2 - sj2) + 0.5f * invr * __logf(__fdividef(r - sj, r + sj)));
   }
   if (r > fabsf(rho - sj)) {
-    const float inv_rho = 1.0f / rho;
+    const float inv_rho = __fdividef(1.0f, rho);
     const float theta = 0.5f * inv_rho * invr * (r2 + rho * rho - sj2);
-    const float uij = 1.0f / (r + sj);
-    return 0.25f * (inv_rho * (2.0f - theta) - uij + invr * logf(rho * uij));
+    const float uij = __fdividef(1.0f, r + sj);
+    return 0.25f * (inv_rho * (2.0f - theta) - uij + invr * __logf(rho * uij));
   }
   if (rho < sj) {
-    return 0.5f * (sj / (r2 - sj2) + 2.0f / rho + 0.5f * invr * logf((sj - r) / (sj + r)));
+    return 0.5f * (__fdividef(sj, r2 - sj2) + __fdividef(2.0f, rho) +
+                   0.5f * invr * __logf(__fdividef(sj - r, sj + r)));
   }
   return 0.0f;
 }
@@ -81,29 +87,31 @@ __device__ __forceinline__ float hctDerivative(float r, float r2, float invr, fl
     return t * sj * invr2 * invr2 * dumbo;
   }
   if (r > rho + sj) {
-    const float temp1 = 1.0f / (r2 - sj2);
-    return temp1 * sj * (-0.5f * invr2 + temp1) + 0.25f * invr * invr2 * logf((r - sj) / (r + sj));
+    const float temp1 = __fdividef(1.0f, r2 - sj2);
+    return temp1 * sj * (-0.5f * invr2 + temp1) +
+           0.25f * invr * invr2 * __logf(__fdividef(r - sj, r + sj));
   }
   if (r > fabsf(rho - sj)) {
-    const float temp1 = 1.0f / (r + sj);
+    const float temp1 = __fdividef(1.0f, r + sj);
     const float invr3 = invr2 * invr;
-    const float inv_rho = 1.0f / rho;
+    const float inv_rho = __fdividef(1.0f, rho);
     return -0.25f * (-0.5f * (r2 - rho * rho + sj2) * invr3 * inv_rho * inv_rho +
-                     invr * temp1 * (temp1 - invr) - invr3 * logf(rho * temp1));
+                     invr * temp1 * (temp1 - invr) - invr3 * __logf(rho * temp1));
   }
   if (rho < sj) {
-    const float temp1 = 1.0f / (r2 - sj2);
+    const float temp1 = __fdividef(1.0f, r2 - sj2);
     return -0.5f * (sj * invr2 * temp1 - 2.0f * sj * temp1 * temp1 -
-                    0.5f * invr2 * invr * logf((sj - r) / (sj + r)));
+                    0.5f * invr2 * invr * __logf(__fdividef(sj - r, sj + r)));
   }
   return 0.0f;
 }
 
 // Shared-memory layout of one work unit
 struct UnitSmem {
-  float4* hi;       // x, y, z (high parts), charge
-  float4* lo;       // x, y, z (low parts), Lennard-Jones code (int bits)
-  float4* gb;       // rho, s*rho, effective radius, dE/dR after the chain rule
+  float4* pa;       // x_hi, y_hi, z_hi, pass payload w1
+  float4* pb;       // x_lo, y_lo, z_lo, pass payload w2
+  float4* prm;      // charge * sqrt(k_Coulomb), Lennard-Jones code (int bits), rho, s * rho
+  float2* gbv;      // effective radius, dE/dR after the chain rule
   int* fx;          // int63 force accumulators: primary
   int* fy;
   int* fz;
@@ -114,32 +122,32 @@ struct UnitSmem {
   int* psio;
   int* de;          // int63 dE/dR accumulator, 2^kDeijdaBits
   int* deo;
-  float2* lj;       // Lennard-Jones tables of the unit's molecules
+  float2* lj;       // Lennard-Jones tables of the unit's molecules (standard, then 1-4)
   unsigned long long* nrg;   // per unit molecule energies
   int* sys;         // molecule index
   int* slot0;       // first slot of the molecule
   int* natom;
-  int* tile0;       // prefix sum of tile counts (kMaxUnitSystems + 1)
   int* ljbase;
-  int* bond0;       // prefix sums of valence term counts (kMaxUnitSystems + 1)
-  int* angl0;
-  int* dihe0;
+  int* tile0;       // prefix sums (kMaxUnitSystems + 1 entries each)
+  int* bchunk0;     // valence work in chunks of 32 terms that never straddle two molecules
+  int* achunk0;
+  int* dchunk0;
 };
 
 __host__ __device__ inline size_t alignUp(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+constexpr int kSlotBytes = 3 * 16 + 8 + 10 * 4;
 
 }  // namespace
 
 // Dynamic shared memory needed for a work unit of max_slots atom slots and max_lj table entries
 size_t fusedSmemBytes(int max_slots, int max_lj) {
-  size_t b = 0;
-  b += 3 * sizeof(float4) * max_slots;
-  b += 10 * sizeof(int) * max_slots;
+  size_t b = static_cast<size_t>(kSlotBytes) * max_slots;
   b = alignUp(b, 16);
   b += sizeof(float2) * max_lj;
   b = alignUp(b, 16);
   b += sizeof(unsigned long long) * kMaxUnitSystems * kNrgStride;
-  b += sizeof(int) * (9 * kMaxUnitSystems + 8);
+  b += sizeof(int) * (4 * kMaxUnitSystems + 4 * (kMaxUnitSystems + 1));
   return b;
 }
 
@@ -148,9 +156,10 @@ namespace {
 __device__ UnitSmem carveSmem(char* base, int max_slots, int max_lj) {
   UnitSmem s;
   size_t off = 0;
-  s.hi = reinterpret_cast<float4*>(base + off); off += sizeof(float4) * max_slots;
-  s.lo = reinterpret_cast<float4*>(base + off); off += sizeof(float4) * max_slots;
-  s.gb = reinterpret_cast<float4*>(base + off); off += sizeof(float4) * max_slots;
+  s.pa = reinterpret_cast<float4*>(base + off); off += sizeof(float4) * max_slots;
+  s.pb = reinterpret_cast<float4*>(base + off); off += sizeof(float4) * max_slots;
+  s.prm = reinterpret_cast<float4*>(base + off); off += sizeof(float4) * max_slots;
+  s.gbv = reinterpret_cast<float2*>(base + off); off += sizeof(float2) * max_slots;
   int* ip = reinterpret_cast<int*>(base + off);
   s.fx = ip; ip += max_slots;
   s.fy = ip; ip += max_slots;
@@ -173,9 +182,9 @@ __device__ UnitSmem carveSmem(char* base, int max_slots, int max_lj) {
   s.natom = q; q += kMaxUnitSystems;
   s.ljbase = q; q += kMaxUnitSystems;
   s.tile0 = q; q += kMaxUnitSystems + 1;
-  s.bond0 = q; q += kMaxUnitSystems + 1;
-  s.angl0 = q; q += kMaxUnitSystems + 1;
-  s.dihe0 = q; q += kMaxUnitSystems + 1;
+  s.bchunk0 = q; q += kMaxUnitSystems + 1;
+  s.achunk0 = q; q += kMaxUnitSystems + 1;
+  s.dchunk0 = q; q += kMaxUnitSystems + 1;
   return s;
 }
 
@@ -197,10 +206,10 @@ __device__ __forceinline__ void tileCoordinates(int local, int* ti, int* tj) {
   *tj = local - i * (i + 1) / 2;
 }
 
-__device__ __forceinline__ float3 pairDelta(const float4 hi_i, const float4 lo_i, const float4 hi_j,
-                                            const float4 lo_j) {
-  return make_float3((hi_j.x - hi_i.x) + (lo_j.x - lo_i.x), (hi_j.y - hi_i.y) + (lo_j.y - lo_i.y),
-                     (hi_j.z - hi_i.z) + (lo_j.z - lo_i.z));
+__device__ __forceinline__ float3 pairDelta(const float4 a_i, const float4 b_i, const float4 a_j,
+                                            const float4 b_j) {
+  return make_float3((a_j.x - a_i.x) + (b_j.x - b_i.x), (a_j.y - a_i.y) + (b_j.y - b_i.y),
+                     (a_j.z - a_i.z) + (b_j.z - b_i.z));
 }
 
 __device__ __forceinline__ void addForce(const UnitSmem &s, int slot, float fx, float fy, float fz,
@@ -208,12 +217,6 @@ __device__ __forceinline__ void addForce(const UnitSmem &s, int slot, float fx, 
   atomicAddInt63(fx * scale, &s.fx[slot], &s.fxo[slot]);
   atomicAddInt63(fy * scale, &s.fy[slot], &s.fyo[slot]);
   atomicAddInt63(fz * scale, &s.fz[slot], &s.fzo[slot]);
-}
-
-__device__ __forceinline__ void addEnergy(const UnitSmem &s, int k, int slot, float e,
-                                          float scale) {
-  atomicAdd(&s.nrg[k * kNrgStride + slot],
-            static_cast<unsigned long long>(__float2ll_rn(e * scale)));
 }
 
 // Warp-wide int64 sum, result in every lane
@@ -224,239 +227,268 @@ __device__ __forceinline__ long long warpSum(long long v) {
   return v;
 }
 
-// Coordinate difference from the hi / lo representation of two atoms held in shared memory
+// Warp-reduce one scaled energy per lane (all lanes in one molecule) into its slot
+__device__ __forceinline__ void warpEnergy(const UnitSmem &s, int k, int slot, float e,
+                                           float scale) {
+  const long long v = warpSum(__float2ll_rn(e * scale));
+  if ((threadIdx.x & 31) == 0 && v != 0) {
+    atomicAdd(&s.nrg[k * kNrgStride + slot], static_cast<unsigned long long>(v));
+  }
+}
+
+// Coordinate difference b - a from the hi / lo representation of two slots
 __device__ __forceinline__ float3 slotDelta(const UnitSmem &s, int a, int b) {
-  return pairDelta(s.hi[a], s.lo[a], s.hi[b], s.lo[b]);
+  return pairDelta(s.pa[a], s.pb[a], s.pa[b], s.pb[b]);
 }
 
 // ------------------------------------------------------------------------------------------------
-// Valence terms (Potential/valence_potential.tpp)
+// Valence terms (Potential/valence_potential.tpp).  Warps take chunks of 32 terms of one molecule,
+// so each chunk's energies reduce across the warp into a single shared-memory update.
 // ------------------------------------------------------------------------------------------------
 template <bool FORCE, bool ENERGY>
 __device__ void valenceTerms(const DevSynthesis &d, const UnitSmem &s, int nsys_u) {
   const float fs = d.frc_scale;
   const float es = d.nrg_scale;
-  // bonds, valence_potential.tpp:9-97; the equilibrium length is held as a float pair so that
-  // r - r0 loses nothing to the rounding of r0
-  const int nbond = s.bond0[nsys_u];
-  for (int f = threadIdx.x; f < nbond; f += blockDim.x) {
-    const int k = findOwner(s.bond0, nsys_u, f);
-    const uint4 rec = d.bonds[d.bond_start[s.sys[k]] + (f - s.bond0[k])];
-    const int ia = s.slot0[k] + static_cast<int>(rec.x & 0xffffu);
-    const int ja = s.slot0[k] + static_cast<int>(rec.x >> 16);
-    const float keq = __uint_as_float(rec.y);
-    const float leq_hi = __uint_as_float(rec.z);
-    const float leq_lo = __uint_as_float(rec.w);
-    // bond length as an unevaluated float pair: each coordinate difference is the exact sum of
-    // the high-part difference (TwoSum) and the low parts, the squared length keeps the FMA
-    // residues, and the square root gets one Newton correction
-    float dh[3], dlo[3];
-    {
-      const float4 hi_i = s.hi[ia], hi_j = s.hi[ja], lo_i = s.lo[ia], lo_j = s.lo[ja];
-      const float a[3] = {hi_j.x, hi_j.y, hi_j.z};
-      const float b[3] = {hi_i.x, hi_i.y, hi_i.z};
-      const float la[3] = {lo_j.x, lo_j.y, lo_j.z};
-      const float lb[3] = {lo_i.x, lo_i.y, lo_i.z};
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwarp = blockDim.x >> 5;
+
+  // bonds, valence_potential.tpp:9-97; the equilibrium length is a float pair so that r - r0
+  // loses nothing to the rounding of r0, and the bond length itself is an unevaluated pair
+  for (int c = warp; c < s.bchunk0[nsys_u]; c += nwarp) {
+    const int k = findOwner(s.bchunk0, nsys_u, c);
+    const int sysid = s.sys[k];
+    const int t = (c - s.bchunk0[k]) * 32 + lane;
+    const int nterm = d.bond_start[sysid + 1] - d.bond_start[sysid];
+    float e = 0.0f;
+    if (t < nterm) {
+      const uint4 rec = d.bonds[d.bond_start[sysid] + t];
+      const int ia = s.slot0[k] + static_cast<int>(rec.x & 0xffffu);
+      const int ja = s.slot0[k] + static_cast<int>(rec.x >> 16);
+      const float keq = __uint_as_float(rec.y);
+      const float leq_hi = __uint_as_float(rec.z);
+      const float leq_lo = __uint_as_float(rec.w);
+      const float4 ai = s.pa[ia], aj = s.pa[ja], bi = s.pb[ia], bj = s.pb[ja];
+      const float av[3] = {aj.x, aj.y, aj.z};
+      const float bv[3] = {ai.x, ai.y, ai.z};
+      const float lav[3] = {bj.x, bj.y, bj.z};
+      const float lbv[3] = {bi.x, bi.y, bi.z};
+      float dh[3], dlo[3];
 #pragma unroll
-      for (int c = 0; c < 3; c++) {
-        const float sdiff = a[c] - b[c];
-        const float bb = sdiff - a[c];
-        const float err = (a[c] - (sdiff - bb)) + (-b[c] - bb);
-        const float lo = err + (la[c] - lb[c]);
-        dh[c] = sdiff + lo;
-        dlo[c] = lo - (dh[c] - sdiff);
+      for (int q = 0; q < 3; q++) {
+        const float sdiff = av[q] - bv[q];
+        const float bb = sdiff - av[q];
+        const float err = (av[q] - (sdiff - bb)) + (-bv[q] - bb);
+        const float lo = err + (lav[q] - lbv[q]);
+        dh[q] = sdiff + lo;
+        dlo[q] = lo - (dh[q] - sdiff);
       }
-    }
-    const float3 dv = make_float3(dh[0], dh[1], dh[2]);
-    float r2h = dh[0] * dh[0];
-    float r2l = fmaf(dh[0], dh[0], -r2h) + 2.0f * dh[0] * dlo[0];
+      float r2h = dh[0] * dh[0];
+      float r2l = fmaf(dh[0], dh[0], -r2h) + 2.0f * dh[0] * dlo[0];
 #pragma unroll
-    for (int c = 1; c < 3; c++) {
-      const float p = dh[c] * dh[c];
-      const float pe = fmaf(dh[c], dh[c], -p) + 2.0f * dh[c] * dlo[c];
-      const float sum = r2h + p;
-      const float bv = sum - r2h;
-      r2l += ((r2h - (sum - bv)) + (p - bv)) + pe;
-      r2h = sum;
-    }
-    const float r = sqrtf(r2h);
-    const float r_lo = (fmaf(-r, r, r2h) + r2l) / (2.0f * r);
-    const float dl = ((r - leq_hi) + r_lo) - leq_lo;
-    if (FORCE) {
-      const float fmag = 2.0f * keq * dl / r;
-      addForce(s, ia, fmag * dv.x, fmag * dv.y, fmag * dv.z, fs);
-      addForce(s, ja, -fmag * dv.x, -fmag * dv.y, -fmag * dv.z, fs);
-    }
-    if (ENERGY) {
-      addEnergy(s, k, kBond, __fmul_rn(__fmul_rn(keq, dl), dl), es);
-    }
-  }
-  // angles, valence_potential.tpp:170-288.  The angle comes from atan2(|ba x bc|, ba . bc),
-  // which stays well conditioned where acos of the cosine does not.
-  const int nangl = s.angl0[nsys_u];
-  for (int f = threadIdx.x; f < nangl; f += blockDim.x) {
-    const int k = findOwner(s.angl0, nsys_u, f);
-    const uint4 rec = d.angles[d.angl_start[s.sys[k]] + (f - s.angl0[k])];
-    const int ia = s.slot0[k] + static_cast<int>(rec.x & 0xffffu);
-    const int ja = s.slot0[k] + static_cast<int>(rec.x >> 16);
-    const int ka = s.slot0[k] + static_cast<int>(rec.y);
-    const float keq = __uint_as_float(rec.z);
-    float sth0, cth0;
-    sincosf(__uint_as_float(rec.w), &sth0, &cth0);
-    const float3 ba = slotDelta(s, ja, ia);
-    const float3 bc = slotDelta(s, ja, ka);
-    const float mgba = ba.x * ba.x + ba.y * ba.y + ba.z * ba.z;
-    const float mgbc = bc.x * bc.x + bc.y * bc.y + bc.z * bc.z;
-    const float invbabc = 1.0f / sqrtf(mgba * mgbc);
-    const float dotp = ba.x * bc.x + ba.y * bc.y + ba.z * bc.z;
-    const float cx = ba.y * bc.z - ba.z * bc.y;
-    const float cy = ba.z * bc.x - ba.x * bc.z;
-    const float cz = ba.x * bc.y - ba.y * bc.x;
-    const float crs = sqrtf(cx * cx + cy * cy + cz * cz);
-    // theta - theta0 = atan2(sin(theta - theta0), cos(theta - theta0)), with the sine and cosine
-    // of theta from the cross and dot products and those of theta0 from the record
-    const float sth = crs * invbabc;
-    const float cth = dotp * invbabc;
-    const float dtheta = atan2f(fmaf(sth, cth0, -cth * sth0), fmaf(cth, cth0, sth * sth0));
-    if (FORCE) {
-      const float costheta = dotp * invbabc;
-      const float dA = -2.0f * keq * dtheta / (crs * invbabc);
-      const float sqba = dA / mgba;
-      const float sqbc = dA / mgbc;
-      const float mbabc = dA * invbabc;
-      const float adx = bc.x * mbabc - costheta * ba.x * sqba;
-      const float ady = bc.y * mbabc - costheta * ba.y * sqba;
-      const float adz = bc.z * mbabc - costheta * ba.z * sqba;
-      const float cdx = ba.x * mbabc - costheta * bc.x * sqbc;
-      const float cdy = ba.y * mbabc - costheta * bc.y * sqbc;
-      const float cdz = ba.z * mbabc - costheta * bc.z * sqbc;
-      addForce(s, ia, -adx, -ady, -adz, fs);
-      addForce(s, ja, adx + cdx, ady + cdy, adz + cdz, fs);
-      addForce(s, ka, -cdx, -cdy, -cdz, fs);
+      for (int q = 1; q < 3; q++) {
+        const float p = dh[q] * dh[q];
+        const float pe = fmaf(dh[q], dh[q], -p) + 2.0f * dh[q] * dlo[q];
+        const float sum = r2h + p;
+        const float bvv = sum - r2h;
+        r2l += ((r2h - (sum - bvv)) + (p - bvv)) + pe;
+        r2h = sum;
+      }
+      const float r = sqrtf(r2h);
+      const float r_lo = (fmaf(-r, r, r2h) + r2l) / (2.0f * r);
+      const float dl = ((r - leq_hi) + r_lo) - leq_lo;
+      if (FORCE) {
+        const float fmag = 2.0f * keq * dl / r;
+        addForce(s, ia, fmag * dh[0], fmag * dh[1], fmag * dh[2], fs);
+        addForce(s, ja, -fmag * dh[0], -fmag * dh[1], -fmag * dh[2], fs);
+      }
+      e = __fmul_rn(__fmul_rn(keq, dl), dl);
     }
     if (ENERGY) {
-      addEnergy(s, k, kAngle, __fmul_rn(__fmul_rn(keq, dtheta), dtheta), es);
+      warpEnergy(s, k, kBond, e, es);
     }
   }
+
+  // angles, valence_potential.tpp:170-288.  theta - theta0 comes from rotating (cos, sin) of
+  // theta, taken from the dot and cross products, by theta0: well conditioned everywhere.
+  for (int c = warp; c < s.achunk0[nsys_u]; c += nwarp) {
+    const int k = findOwner(s.achunk0, nsys_u, c);
+    const int sysid = s.sys[k];
+    const int t = (c - s.achunk0[k]) * 32 + lane;
+    const int nterm = d.angl_start[sysid + 1] - d.angl_start[sysid];
+    float e = 0.0f;
+    if (t < nterm) {
+      const uint4 rec = d.angles[d.angl_start[sysid] + t];
+      const int ia = s.slot0[k] + static_cast<int>(rec.x & 0xffffu);
+      const int ja = s.slot0[k] + static_cast<int>(rec.x >> 16);
+      const int ka = s.slot0[k] + static_cast<int>(rec.y);
+      const float keq = __uint_as_float(rec.z);
+      float sth0, cth0;
+      sincosf(__uint_as_float(rec.w), &sth0, &cth0);
+      const float3 ba = slotDelta(s, ja, ia);
+      const float3 bc = slotDelta(s, ja, ka);
+      const float mgba = ba.x * ba.x + ba.y * ba.y + ba.z * ba.z;
+      const float mgbc = bc.x * bc.x + bc.y * bc.y + bc.z * bc.z;
+      const float invbabc = rsqrtf(mgba * mgbc);
+      const float dotp = ba.x * bc.x + ba.y * bc.y + ba.z * bc.z;
+      const float cx = ba.y * bc.z - ba.z * bc.y;
+      const float cy = ba.z * bc.x - ba.x * bc.z;
+      const float cz = ba.x * bc.y - ba.y * bc.x;
+      const float crs = sqrtf(cx * cx + cy * cy + cz * cz);
+      const float sth = crs * invbabc;
+      const float cth = dotp * invbabc;
+      const float dtheta = atan2f(fmaf(sth, cth0, -cth * sth0), fmaf(cth, cth0, sth * sth0));
+      if (FORCE) {
+        const float dA = -2.0f * keq * dtheta / sth;
+        const float sqba = dA / mgba;
+        const float sqbc = dA / mgbc;
+        const float mbabc = dA * invbabc;
+        const float adx = bc.x * mbabc - cth * ba.x * sqba;
+        const float ady = bc.y * mbabc - cth * ba.y * sqba;
+        const float adz = bc.z * mbabc - cth * ba.z * sqba;
+        const float cdx = ba.x * mbabc - cth * bc.x * sqbc;
+        const float cdy = ba.y * mbabc - cth * bc.y * sqbc;
+        const float cdz = ba.z * mbabc - cth * bc.z * sqbc;
+        addForce(s, ia, -adx, -ady, -adz, fs);
+        addForce(s, ja, adx + cdx, ady + cdy, adz + cdz, fs);
+        addForce(s, ka, -cdx, -cdy, -cdz, fs);
+      }
+      e = __fmul_rn(__fmul_rn(keq, dtheta), dtheta);
+    }
+    if (ENERGY) {
+      warpEnergy(s, k, kAngle, e, es);
+    }
+  }
+
   // dihedrals with attached 1-4 pairs, valence_potential.tpp:359-578, 1288-1420.  The signed
   // angle is carried as (cos, sin) from x = (ab x bc) . (bc x cd) and y = |bc| ab . (bc x cd),
-  // the same angle STORMM's acos / arcsine route gives (Math/rounding.tpp:25-80) without its
-  // ill conditioning near 0 and pi; cos(n theta - phase) and sin(n theta - phase) follow from
-  // the multiple-angle recurrence for integer periodicities.
-  const int ndihe = s.dihe0[nsys_u];
-  for (int f = threadIdx.x; f < ndihe; f += blockDim.x) {
-    const int k = findOwner(s.dihe0, nsys_u, f);
-    const int pos = d.dihe_start[s.sys[k]] + (f - s.dihe0[k]);
-    const uint4 ra = d.dihe_a[pos];
-    const uint4 rb = d.dihe_b[pos];
-    const int ia = s.slot0[k] + static_cast<int>(ra.x & 0xffffu);
-    const int ja = s.slot0[k] + static_cast<int>(ra.x >> 16);
-    const int ka = s.slot0[k] + static_cast<int>(ra.y & 0xffffu);
-    const int la = s.slot0[k] + static_cast<int>((ra.y >> 16) & 0x7fffu);
-    const bool improper = (ra.y & 0x80000000u) != 0u;
-    const float amp = __uint_as_float(ra.z);
-    const float freq = __uint_as_float(ra.w);
-    const float cphase = __uint_as_float(rb.x);
-    const float sphase = __uint_as_float(rb.y);
-    const float3 ab = slotDelta(s, ia, ja);
-    const float3 bc = slotDelta(s, ja, ka);
-    const float3 cd = slotDelta(s, ka, la);
-    float3 crabbc = make_float3(ab.y * bc.z - ab.z * bc.y, ab.z * bc.x - ab.x * bc.z,
-                                ab.x * bc.y - ab.y * bc.x);
-    float3 crbccd = make_float3(bc.y * cd.z - bc.z * cd.y, bc.z * cd.x - bc.x * cd.z,
-                                bc.x * cd.y - bc.y * cd.x);
-    const float mgbc = sqrtf(bc.x * bc.x + bc.y * bc.y + bc.z * bc.z);
-    const float xx = crabbc.x * crbccd.x + crabbc.y * crbccd.y + crabbc.z * crbccd.z;
-    const float yy = mgbc * (ab.x * crbccd.x + ab.y * crbccd.y + ab.z * crbccd.z);
-    const float inv_rr = rsqrtf(fmaf(xx, xx, yy * yy));
-    const float c1 = xx * inv_rr;
-    const float s1 = yy * inv_rr;
-    float cn, sn;
-    const int nint = static_cast<int>(freq);
-    if (static_cast<float>(nint) == freq && nint >= 1 && nint <= 6) {
-      cn = c1;
-      sn = s1;
-      for (int m = 1; m < nint; m++) {
-        const float cnew = cn * c1 - sn * s1;
-        sn = sn * c1 + cn * s1;
-        cn = cnew;
+  // the angle STORMM's acos / arcsine route gives (Math/rounding.tpp:25-80) without its ill
+  // conditioning near 0 and pi; cos(n theta - phase) and sin(n theta - phase) follow from the
+  // multiple-angle recurrence for integer periodicities.
+  for (int c = warp; c < s.dchunk0[nsys_u]; c += nwarp) {
+    const int k = findOwner(s.dchunk0, nsys_u, c);
+    const int sysid = s.sys[k];
+    const int t = (c - s.dchunk0[k]) * 32 + lane;
+    const int nterm = d.dihe_start[sysid + 1] - d.dihe_start[sysid];
+    float e_prop = 0.0f, e_impr = 0.0f, e_el14 = 0.0f, e_lj14 = 0.0f;
+    if (t < nterm) {
+      const int pos = d.dihe_start[sysid] + t;
+      const uint4 ra = d.dihe_a[pos];
+      const uint4 rb = d.dihe_b[pos];
+      const int ia = s.slot0[k] + static_cast<int>(ra.x & 0xffffu);
+      const int ja = s.slot0[k] + static_cast<int>(ra.x >> 16);
+      const int ka = s.slot0[k] + static_cast<int>(ra.y & 0xffffu);
+      const int la = s.slot0[k] + static_cast<int>((ra.y >> 16) & 0x7fffu);
+      const bool improper = (ra.y & 0x80000000u) != 0u;
+      const float amp = __uint_as_float(ra.z);
+      const float freq = __uint_as_float(ra.w);
+      const float cphase = __uint_as_float(rb.x);
+      const float sphase = __uint_as_float(rb.y);
+      const float3 ab = slotDelta(s, ia, ja);
+      const float3 bc = slotDelta(s, ja, ka);
+      const float3 cd = slotDelta(s, ka, la);
+      float3 crabbc = make_float3(ab.y * bc.z - ab.z * bc.y, ab.z * bc.x - ab.x * bc.z,
+                                  ab.x * bc.y - ab.y * bc.x);
+      float3 crbccd = make_float3(bc.y * cd.z - bc.z * cd.y, bc.z * cd.x - bc.x * cd.z,
+                                  bc.x * cd.y - bc.y * cd.x);
+      const float mgbc = sqrtf(bc.x * bc.x + bc.y * bc.y + bc.z * bc.z);
+      const float xx = crabbc.x * crbccd.x + crabbc.y * crbccd.y + crabbc.z * crbccd.z;
+      const float yy = mgbc * (ab.x * crbccd.x + ab.y * crbccd.y + ab.z * crbccd.z);
+      const float inv_rr = rsqrtf(fmaf(xx, xx, yy * yy));
+      const float c1 = xx * inv_rr;
+      const float s1 = yy * inv_rr;
+      float cn, sn;
+      const int nint = static_cast<int>(freq);
+      if (static_cast<float>(nint) == freq && nint >= 1 && nint <= 6) {
+        cn = c1;
+        sn = s1;
+        for (int m = 1; m < nint; m++) {
+          const float cnew = cn * c1 - sn * s1;
+          sn = sn * c1 + cn * s1;
+          cn = cnew;
+        }
       }
-    }
-    else {
-      const float th = atan2f(yy, xx);
-      sincosf(freq * th, &sn, &cn);
-    }
-    // sangle = n theta - phase
-    const float cos_sangle = cn * cphase + sn * sphase;
-    const float sin_sangle = sn * cphase - cn * sphase;
-    if (FORCE) {
-      const float fr = amp * freq * sin_sangle;
-      const float mgab = sqrtf(ab.x * ab.x + ab.y * ab.y + ab.z * ab.z);
-      const float mgcd = sqrtf(cd.x * cd.x + cd.y * cd.y + cd.z * cd.z);
-      const float invab = 1.0f / mgab;
-      const float invbc = 1.0f / mgbc;
-      const float invcd = 1.0f / mgcd;
-      const float cosb = -(ab.x * bc.x + ab.y * bc.y + ab.z * bc.z) * invab * invbc;
-      const float cosc = -(bc.x * cd.x + bc.y * cd.y + bc.z * cd.z) * invbc * invcd;
-      const float isinb2 = (cosb * cosb < 0.99999904632568359375f) ? fr / (1.0f - cosb * cosb) :
-                                                                      fr * 1048576.0f;
-      const float isinc2 = (cosc * cosc < 0.99999904632568359375f) ? fr / (1.0f - cosc * cosc) :
-                                                                      fr * 1048576.0f;
-      const float invabc = invab * invbc;
-      const float invbcd = invbc * invcd;
-      crabbc.x *= invabc;
-      crabbc.y *= invabc;
-      crabbc.z *= invabc;
-      crbccd.x *= invbcd;
-      crbccd.y *= invbcd;
-      crbccd.z *= invbcd;
-      const float fa = -invab * isinb2;
-      const float fb1 = (mgbc - mgab * cosb) * invabc * isinb2;
-      const float fb2 = cosc * invbc * isinc2;
-      const float fd = -invcd * isinc2;
-      const float fix = crabbc.x * fa, fiy = crabbc.y * fa, fiz = crabbc.z * fa;
-      const float fjx = fb1 * crabbc.x - fb2 * crbccd.x;
-      const float fjy = fb1 * crabbc.y - fb2 * crbccd.y;
-      const float fjz = fb1 * crabbc.z - fb2 * crbccd.z;
-      const float flx = -fd * crbccd.x, fly = -fd * crbccd.y, flz = -fd * crbccd.z;
-      addForce(s, ia, fix, fiy, fiz, fs);
-      addForce(s, ja, fjx, fjy, fjz, fs);
-      addForce(s, ka, -(fix + fjx + flx), -(fiy + fjy + fly), -(fiz + fjz + flz), fs);
-      addForce(s, la, flx, fly, flz, fs);
+      else {
+        sincosf(freq * atan2f(yy, xx), &sn, &cn);
+      }
+      const float cos_sangle = cn * cphase + sn * sphase;
+      const float sin_sangle = sn * cphase - cn * sphase;
+      if (FORCE) {
+        const float fr = amp * freq * sin_sangle;
+        const float mgab = sqrtf(ab.x * ab.x + ab.y * ab.y + ab.z * ab.z);
+        const float mgcd = sqrtf(cd.x * cd.x + cd.y * cd.y + cd.z * cd.z);
+        const float invab = 1.0f / mgab;
+        const float invbc = 1.0f / mgbc;
+        const float invcd = 1.0f / mgcd;
+        const float cosb = -(ab.x * bc.x + ab.y * bc.y + ab.z * bc.z) * invab * invbc;
+        const float cosc = -(bc.x * cd.x + bc.y * cd.y + bc.z * cd.z) * invbc * invcd;
+        const float isinb2 = (cosb * cosb < 0.99999904632568359375f) ? fr / (1.0f - cosb * cosb) :
+                                                                        fr * 1048576.0f;
+        const float isinc2 = (cosc * cosc < 0.99999904632568359375f) ? fr / (1.0f - cosc * cosc) :
+                                                                        fr * 1048576.0f;
+        const float invabc = invab * invbc;
+        const float invbcd = invbc * invcd;
+        crabbc.x *= invabc;
+        crabbc.y *= invabc;
+        crabbc.z *= invabc;
+        crbccd.x *= invbcd;
+        crbccd.y *= invbcd;
+        crbccd.z *= invbcd;
+        const float fa = -invab * isinb2;
+        const float fb1 = (mgbc - mgab * cosb) * invabc * isinb2;
+        const float fb2 = cosc * invbc * isinc2;
+        const float fd = -invcd * isinc2;
+        const float fix = crabbc.x * fa, fiy = crabbc.y * fa, fiz = crabbc.z * fa;
+        const float fjx = fb1 * crabbc.x - fb2 * crbccd.x;
+        const float fjy = fb1 * crabbc.y - fb2 * crbccd.y;
+        const float fjz = fb1 * crabbc.z - fb2 * crbccd.z;
+        const float flx = -fd * crbccd.x, fly = -fd * crbccd.y, flz = -fd * crbccd.z;
+        addForce(s, ia, fix, fiy, fiz, fs);
+        addForce(s, ja, fjx, fjy, fjz, fs);
+        addForce(s, ka, -(fix + fjx + flx), -(fiy + fjy + fly), -(fiz + fjz + flz), fs);
+        addForce(s, la, flx, fly, flz, fs);
+      }
+      const float edih = __fmul_rn(amp, __fadd_rn(1.0f, cos_sangle));
+      if (improper) {
+        e_impr = edih;
+      }
+      else {
+        e_prop = edih;
+      }
+      // attached 1-4 pair between atoms i and l
+      const float inv_scee = __uint_as_float(rb.z);
+      if (inv_scee > 0.0f) {
+        const float inv_scnb = __uint_as_float(rb.w);
+        const float3 dv = slotDelta(s, ia, la);
+        const float4 pi = s.prm[ia];
+        const float4 pl = s.prm[la];
+        const int code_i = __float_as_int(pi.y);
+        const int code_l = __float_as_int(pl.y);
+        // the molecule's 1-4 table follows its standard table in shared memory
+        const int nt = d.lj_ntypes[sysid];
+        const float2 ab14 = s.lj[(code_i & 0xffff) + (code_l >> 16) + nt * nt];
+        const float lja = ab14.x * inv_scnb;
+        const float ljb = ab14.y * inv_scnb;
+        const float qiqj = pi.x * pl.x * inv_scee;
+        const float invr2 = 1.0f / (dv.x * dv.x + dv.y * dv.y + dv.z * dv.z);
+        const float invr = sqrtf(invr2);
+        const float invr4 = invr2 * invr2;
+        if (FORCE) {
+          const float fmag = -(qiqj * invr * invr2) +
+                             (6.0f * ljb - 12.0f * lja * invr4 * invr2) * invr4 * invr4;
+          addForce(s, ia, fmag * dv.x, fmag * dv.y, fmag * dv.z, fs);
+          addForce(s, la, -fmag * dv.x, -fmag * dv.y, -fmag * dv.z, fs);
+        }
+        e_el14 = __fmul_rn(qiqj, invr);
+        e_lj14 = __fsub_rn(__fmul_rn(__fmul_rn(__fmul_rn(lja, invr4), invr4), invr4),
+                           __fmul_rn(__fmul_rn(ljb, invr4), invr2));
+      }
     }
     if (ENERGY) {
-      addEnergy(s, k, improper ? kImproperDihedral : kProperDihedral,
-                __fmul_rn(amp, __fadd_rn(1.0f, cos_sangle)), es);
-    }
-    // attached 1-4 pair between atoms i and l
-    const float inv_scee = __uint_as_float(rb.z);
-    if (inv_scee > 0.0f) {
-      const float inv_scnb = __uint_as_float(rb.w);
-      const float3 dv = slotDelta(s, ia, la);
-      const float4 hi_i = s.hi[ia];
-      const float4 hi_l = s.hi[la];
-      const int code_i = __float_as_int(s.lo[ia].w);
-      const int code_l = __float_as_int(s.lo[la].w);
-      // the 1-4 table of the molecule follows its standard table in shared memory
-      const int nt = d.lj_ntypes[s.sys[k]];
-      const float2 ab14 = s.lj[(code_i & 0xffff) + (code_l >> 16) + nt * nt];
-      const float lja = ab14.x * inv_scnb;
-      const float ljb = ab14.y * inv_scnb;
-      const float qiqj = hi_i.w * hi_l.w * inv_scee;
-      const float invr2 = 1.0f / (dv.x * dv.x + dv.y * dv.y + dv.z * dv.z);
-      const float invr = sqrtf(invr2);
-      const float invr4 = invr2 * invr2;
-      if (FORCE) {
-        const float fmag = -(qiqj * invr * invr2) +
-                           (6.0f * ljb - 12.0f * lja * invr4 * invr2) * invr4 * invr4;
-        addForce(s, ia, fmag * dv.x, fmag * dv.y, fmag * dv.z, fs);
-        addForce(s, la, -fmag * dv.x, -fmag * dv.y, -fmag * dv.z, fs);
-      }
-      if (ENERGY) {
-        addEnergy(s, k, kElec14, __fmul_rn(qiqj, invr), es);
-        addEnergy(s, k, kVdw14, __fsub_rn(__fmul_rn(__fmul_rn(__fmul_rn(lja, invr4), invr4), invr4),
-                                          __fmul_rn(__fmul_rn(ljb, invr4), invr2)), es);
-      }
+      warpEnergy(s, k, kProperDihedral, e_prop, es);
+      warpEnergy(s, k, kImproperDihedral, e_impr, es);
+      warpEnergy(s, k, kElec14, e_el14, es);
+      warpEnergy(s, k, kVdw14, e_lj14, es);
     }
   }
 }
@@ -471,81 +503,243 @@ struct TileInfo {
   int ni;       // valid atoms in block I
   int nj;       // valid atoms in block J
   bool diag;
-  int I, J;
+  int local;    // tile index within the molecule
 };
 
 __device__ __forceinline__ TileInfo tileInfo(const UnitSmem &s, int nsys_u, int t) {
   TileInfo ti;
   ti.k = findOwner(s.tile0, nsys_u, t);
-  tileCoordinates(t - s.tile0[ti.k], &ti.I, &ti.J);
+  ti.local = t - s.tile0[ti.k];
+  int I, J;
+  tileCoordinates(ti.local, &I, &J);
   const int n = s.natom[ti.k];
-  ti.ibase = s.slot0[ti.k] + ti.I * kTile;
-  ti.jbase = s.slot0[ti.k] + ti.J * kTile;
-  ti.ni = min(kTile, n - ti.I * kTile);
-  ti.nj = min(kTile, n - ti.J * kTile);
-  ti.diag = (ti.I == ti.J);
+  ti.ibase = s.slot0[ti.k] + I * kTile;
+  ti.jbase = s.slot0[ti.k] + J * kTile;
+  ti.ni = min(kTile, n - I * kTile);
+  ti.nj = min(kTile, n - J * kTile);
+  ti.diag = (I == J);
   return ti;
 }
 
-// GB pass 1: psi_i -= H(r, rho_i, s_j rho_j) and psi_j -= H(r, rho_j, s_i rho_i) for every pair
-__device__ void gbRadiiTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u, int ntiles) {
-  const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const int nwarp = blockDim.x >> 5;
-  const float ps = static_cast<float>(1 << kPsiBits);
-  for (int t = warp; t < ntiles; t += nwarp) {
-    const TileInfo ti = tileInfo(s, nsys_u, t);
+// Run one tile: p.pair(jslot, jl) for every pair of the tile (once each) and p.rotate() after
+// every step; full off-diagonal tiles take a branch-free loop.
+template <class P>
+__device__ __forceinline__ void walkTile(P &p, const TileInfo &ti, int lane) {
+  if (!ti.diag && ti.ni == kTile && ti.nj == kTile) {
+#pragma unroll 4
+    for (int k = 0; k < kTile; k++) {
+      const int jl = (lane + k) & 31;
+      p.pair(ti.jbase + jl, jl);
+      p.rotate(lane);
+    }
+  }
+  else {
     const bool ivalid = lane < ti.ni;
-    const int islot = ti.ibase + lane;
-    const float4 hi_i = s.hi[islot];
-    const float4 lo_i = s.lo[islot];
-    const float4 gb_i = s.gb[islot];
-    float psi_i = 0.0f;
-    float psi_j = 0.0f;
     const int kbeg = ti.diag ? 1 : 0;
     const int kend = ti.diag ? 16 : 31;
     for (int k = kbeg; k <= kend; k++) {
       const int jl = (lane + k) & 31;
-      const int jslot = ti.jbase + jl;
       const bool active = ivalid && (jl < ti.nj) && (!ti.diag || k < 16 || lane < 16);
       if (active) {
-        const float4 hi_j = s.hi[jslot];
-        const float4 lo_j = s.lo[jslot];
-        const float4 gb_j = s.gb[jslot];
-        const float3 dv = pairDelta(hi_i, lo_i, hi_j, lo_j);
-        const float r2 = dv.x * dv.x + dv.y * dv.y + dv.z * dv.z;
-        const float r = sqrtf(r2);
-        const float invr = 1.0f / r;
-        psi_i -= hctIntegral(r, r2, invr, gb_i.x, gb_j.y);
-        psi_j -= hctIntegral(r, r2, invr, gb_j.x, gb_i.y);
+        p.pair(ti.jbase + jl, jl);
       }
-      psi_j = __shfl_sync(kFullMask, psi_j, (lane + 1) & 31);
-    }
-    if (ivalid) {
-      atomicAddInt63(psi_i * ps, &s.psi[islot], &s.psio[islot]);
-    }
-    const int jl_end = (lane + kend + 1) & 31;
-    if (jl_end < ti.nj) {
-      atomicAddInt63(psi_j * ps, &s.psi[ti.jbase + jl_end], &s.psio[ti.jbase + jl_end]);
+      p.rotate(lane);
     }
   }
 }
 
-// Pass 2: Coulomb + Lennard-Jones (non-excluded pairs) and GB pair terms
+// Lane that holds block J's atom jl's traveling accumulator once the walk is over
+__device__ __forceinline__ int traveledAtom(const TileInfo &ti, int lane) {
+  return (lane + (ti.diag ? 17 : 32)) & 31;
+}
+
+// GB pass 1: psi_i -= H(r, rho_i, s_j rho_j) and psi_j -= H(r, rho_j, s_i rho_i)
+struct RadiiPass {
+  const UnitSmem &s;
+  float4 ai, bi;
+  float psi_i, psi_j;
+  __device__ RadiiPass(const UnitSmem &s_in) : s(s_in) {}
+  __device__ __forceinline__ void begin(int islot) {
+    ai = s.pa[islot];
+    bi = s.pb[islot];
+    psi_i = 0.0f;
+    psi_j = 0.0f;
+  }
+  __device__ __forceinline__ void pair(int jslot, int) {
+    const float4 aj = s.pa[jslot];
+    const float4 bj = s.pb[jslot];
+    const float3 dv = pairDelta(ai, bi, aj, bj);
+    const float r2 = fmaf(dv.x, dv.x, fmaf(dv.y, dv.y, dv.z * dv.z));
+    const float invr = rsqrtf(r2);
+    const float r = r2 * invr;
+    psi_i -= hctIntegral(r, r2, invr, bi.w, aj.w);
+    psi_j -= hctIntegral(r, r2, invr, bj.w, ai.w);
+  }
+  __device__ __forceinline__ void rotate(int lane) {
+    psi_j = __shfl_sync(kFullMask, psi_j, (lane + 1) & 31);
+  }
+};
+
+// Pass 2: Coulomb + Lennard-Jones on non-excluded pairs and the GB pair terms
+template <bool FORCE, bool ENERGY, bool NB, bool GB>
+struct PairPass {
+  const UnitSmem &s;
+  float kk, inv_diel;
+  bool salt;
+  float4 ai, bi;
+  int code_i;
+  unsigned mask;
+  float fxi, fyi, fzi, dei, fxj, fyj, fzj, dej;
+  float e_elec, e_vdw, e_gb;
+  __device__ PairPass(const UnitSmem &s_in, float kappa, float inv_dielectric) :
+      s(s_in), kk(-kappa * kGbKscale), inv_diel(inv_dielectric), salt(kappa > 0.0f) {}
+  __device__ __forceinline__ void begin(int islot, unsigned mask_in) {
+    ai = s.pa[islot];
+    bi = s.pb[islot];
+    code_i = __float_as_int(s.prm[islot].y) & 0xffff;
+    mask = mask_in;
+    fxi = fyi = fzi = dei = 0.0f;
+    fxj = fyj = fzj = dej = 0.0f;
+    e_elec = e_vdw = e_gb = 0.0f;
+  }
+  __device__ __forceinline__ void pair(int jslot, int jl) {
+    const float4 aj = s.pa[jslot];
+    const float4 bj = s.pb[jslot];
+    const float3 dv = pairDelta(ai, bi, aj, bj);
+    const float r2 = fmaf(dv.x, dv.x, fmaf(dv.y, dv.y, dv.z * dv.z));
+    const float qiqj = ai.w * aj.w;
+    float fmag = 0.0f;
+    if (NB && ((mask >> jl) & 1u) == 0u) {
+      // one Newton step on rsqrt keeps r^-12 within a few ulp
+      float invr = rsqrtf(r2);
+      invr = invr * fmaf(-0.5f * r2 * invr, invr, 1.5f);
+      const float invr2 = invr * invr;
+      const float invr4 = invr2 * invr2;
+      const float2 ab = s.lj[code_i + (__float_as_int(s.prm[jslot].y) >> 16)];
+      if (ENERGY) {
+        e_elec = __fadd_rn(e_elec, __fmul_rn(qiqj, invr));
+        e_vdw = __fadd_rn(e_vdw, __fmul_rn(__fsub_rn(__fmul_rn(__fmul_rn(ab.x, invr4), invr4),
+                                                     __fmul_rn(ab.y, invr2)), invr4));
+      }
+      if (FORCE) {
+        fmag = -(qiqj * invr * invr2) + (6.0f * ab.y - 12.0f * ab.x * invr4 * invr2) * invr4 * invr4;
+      }
+    }
+    if (GB) {
+      const float ijb = bi.w * bj.w;
+      const float efac = __expf(__fdividef(-r2, 4.0f * ijb));
+      const float fgbi = rsqrtf(fmaf(ijb, efac, r2));
+      float expmkf, fgbk;
+      if (salt) {
+        fgbk = __fdividef(kk, fgbi);
+        expmkf = __expf(fgbk) * inv_diel;
+      }
+      else {
+        fgbk = 0.0f;
+        expmkf = inv_diel;
+      }
+      const float dielfac = 1.0f - expmkf;
+      if (ENERGY) {
+        e_gb = __fsub_rn(e_gb, __fmul_rn(__fmul_rn(qiqj, dielfac), fgbi));
+      }
+      if (FORCE) {
+        const float temp4 = fgbi * fgbi * fgbi;
+        const float temp6 = qiqj * temp4 * fmaf(fgbk, expmkf, dielfac);
+        fmag += temp6 * fmaf(-0.25f, efac, 1.0f);
+        const float temp5 = 0.5f * efac * temp6 * fmaf(0.25f, r2, ijb);
+        dei = fmaf(bi.w, temp5, dei);
+        dej = fmaf(bj.w, temp5, dej);
+      }
+    }
+    if (FORCE) {
+      fxi = fmaf(fmag, dv.x, fxi);
+      fyi = fmaf(fmag, dv.y, fyi);
+      fzi = fmaf(fmag, dv.z, fzi);
+      fxj = fmaf(-fmag, dv.x, fxj);
+      fyj = fmaf(-fmag, dv.y, fyj);
+      fzj = fmaf(-fmag, dv.z, fzj);
+    }
+  }
+  __device__ __forceinline__ void rotate(int lane) {
+    if (FORCE) {
+      const int src = (lane + 1) & 31;
+      fxj = __shfl_sync(kFullMask, fxj, src);
+      fyj = __shfl_sync(kFullMask, fyj, src);
+      fzj = __shfl_sync(kFullMask, fzj, src);
+      if (GB) {
+        dej = __shfl_sync(kFullMask, dej, src);
+      }
+    }
+  }
+};
+
+// Pass 3: radius chain-rule forces
+struct DerivPass {
+  const UnitSmem &s;
+  float4 ai, bi;
+  float de_i;
+  float fxi, fyi, fzi, fxj, fyj, fzj;
+  __device__ DerivPass(const UnitSmem &s_in) : s(s_in) {}
+  __device__ __forceinline__ void begin(int islot) {
+    ai = s.pa[islot];
+    bi = s.pb[islot];
+    de_i = s.gbv[islot].y;
+    fxi = fyi = fzi = 0.0f;
+    fxj = fyj = fzj = 0.0f;
+  }
+  __device__ __forceinline__ void pair(int jslot, int) {
+    const float4 aj = s.pa[jslot];
+    const float4 bj = s.pb[jslot];
+    const float de_j = s.gbv[jslot].y;
+    const float3 dv = pairDelta(ai, bi, aj, bj);
+    const float r2 = fmaf(dv.x, dv.x, fmaf(dv.y, dv.y, dv.z * dv.z));
+    const float invr = rsqrtf(r2);
+    const float r = r2 * invr;
+    const float fmag = hctDerivative(r, r2, invr, bi.w, aj.w) * de_i +
+                       hctDerivative(r, r2, invr, bj.w, ai.w) * de_j;
+    fxi = fmaf(-fmag, dv.x, fxi);
+    fyi = fmaf(-fmag, dv.y, fyi);
+    fzi = fmaf(-fmag, dv.z, fzi);
+    fxj = fmaf(fmag, dv.x, fxj);
+    fyj = fmaf(fmag, dv.y, fyj);
+    fzj = fmaf(fmag, dv.z, fzj);
+  }
+  __device__ __forceinline__ void rotate(int lane) {
+    const int src = (lane + 1) & 31;
+    fxj = __shfl_sync(kFullMask, fxj, src);
+    fyj = __shfl_sync(kFullMask, fyj, src);
+    fzj = __shfl_sync(kFullMask, fzj, src);
+  }
+};
+
+__device__ void gbRadiiTiles(const UnitSmem &s, int nsys_u, int ntiles) {
+  const int lane = threadIdx.x & 31;
+  const float ps = static_cast<float>(1 << kPsiBits);
+  RadiiPass p(s);
+  for (int t = threadIdx.x >> 5; t < ntiles; t += blockDim.x >> 5) {
+    const TileInfo ti = tileInfo(s, nsys_u, t);
+    p.begin(ti.ibase + lane);
+    walkTile(p, ti, lane);
+    if (lane < ti.ni) {
+      atomicAddInt63(p.psi_i * ps, &s.psi[ti.ibase + lane], &s.psio[ti.ibase + lane]);
+    }
+    const int jl = traveledAtom(ti, lane);
+    if (jl < ti.nj) {
+      atomicAddInt63(p.psi_j * ps, &s.psi[ti.jbase + jl], &s.psio[ti.jbase + jl]);
+    }
+  }
+}
+
 template <bool FORCE, bool ENERGY, bool NB, bool GB>
 __device__ void pairTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u, int ntiles) {
   const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const int nwarp = blockDim.x >> 5;
   const float fs = d.frc_scale;
   const float es = d.nrg_scale;
   const float ds = static_cast<float>(1 << kDeijdaBits);
-  const float kappa = d.kappa;
-  const float inv_diel = d.inv_dielectric;
-  const float kk = -kappa * kGbKscale;
+  PairPass<FORCE, ENERGY, NB, GB> p(s, d.kappa, d.inv_dielectric);
   long long acc_elec = 0, acc_vdw = 0, acc_gb = 0;
   int acc_k = -1;
-  for (int t = warp; t < ntiles; t += nwarp) {
+  for (int t = threadIdx.x >> 5; t < ntiles; t += blockDim.x >> 5) {
     const TileInfo ti = tileInfo(s, nsys_u, t);
     if (ENERGY && ti.k != acc_k) {
       if (acc_k >= 0) {
@@ -563,120 +757,39 @@ __device__ void pairTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u, 
       acc_elec = acc_vdw = acc_gb = 0;
       acc_k = ti.k;
     }
-    const bool ivalid = lane < ti.ni;
-    const int islot = ti.ibase + lane;
-    const float4 hi_i = s.hi[islot];
-    const float4 lo_i = s.lo[islot];
-    const float4 gb_i = s.gb[islot];
-    const int code_i = __float_as_int(lo_i.w) & 0xffff;
-    unsigned int mask = 0u;
+    unsigned mask = 0u;
     if (NB) {
-      const int midx = d.tile_mask_idx[d.tile_start[s.sys[ti.k]] + (t - s.tile0[ti.k])];
+      const int midx = d.tile_mask_idx[d.tile_start[s.sys[ti.k]] + ti.local];
       if (midx != 0) {
         mask = __ldg(&d.mask_pool[static_cast<size_t>(midx) * 32 + lane]);
       }
     }
-    float fxi = 0.0f, fyi = 0.0f, fzi = 0.0f, dei = 0.0f;
-    float fxj = 0.0f, fyj = 0.0f, fzj = 0.0f, dej = 0.0f;
-    float e_elec = 0.0f, e_vdw = 0.0f, e_gb = 0.0f;
-    const int kbeg = ti.diag ? 1 : 0;
-    const int kend = ti.diag ? 16 : 31;
-    for (int k = kbeg; k <= kend; k++) {
-      const int jl = (lane + k) & 31;
-      const int jslot = ti.jbase + jl;
-      const bool active = ivalid && (jl < ti.nj) && (!ti.diag || k < 16 || lane < 16);
-      if (active) {
-        const float4 hi_j = s.hi[jslot];
-        const float4 lo_j = s.lo[jslot];
-        const float3 dv = pairDelta(hi_i, lo_i, hi_j, lo_j);
-        const float r2 = dv.x * dv.x + dv.y * dv.y + dv.z * dv.z;
-        const float qiqj = hi_i.w * hi_j.w;
-        float fmag = 0.0f;
-        if (NB && ((mask >> jl) & 1u) == 0u) {
-          const float invr2 = 1.0f / r2;
-          const float invr = sqrtf(invr2);
-          const float invr4 = invr2 * invr2;
-          const float2 ab = s.lj[code_i + (__float_as_int(lo_j.w) >> 16)];
-          if (ENERGY) {
-            e_elec = __fadd_rn(e_elec, __fmul_rn(qiqj, invr));
-            e_vdw = __fadd_rn(e_vdw, __fmul_rn(__fsub_rn(__fmul_rn(__fmul_rn(ab.x, invr4), invr4),
-                                                         __fmul_rn(ab.y, invr2)), invr4));
-          }
-          if (FORCE) {
-            fmag = -(qiqj * invr * invr2) +
-                   (6.0f * ab.y - 12.0f * ab.x * invr4 * invr2) * invr4 * invr4;
-          }
-        }
-        if (GB) {
-          const float4 gb_j = s.gb[jslot];
-          const float ijb = gb_i.z * gb_j.z;
-          const float efac = expf(-r2 / (4.0f * ijb));
-          const float fgbi = 1.0f / sqrtf(r2 + ijb * efac);
-          float expmkf, fgbk;
-          if (kappa > 0.0f) {
-            fgbk = kk / fgbi;
-            expmkf = expf(fgbk) * inv_diel;
-          }
-          else {
-            fgbk = 0.0f;
-            expmkf = inv_diel;
-          }
-          const float dielfac = 1.0f - expmkf;
-          if (ENERGY) {
-            e_gb = __fsub_rn(e_gb, __fmul_rn(__fmul_rn(qiqj, dielfac), fgbi));
-          }
-          if (FORCE) {
-            const float temp4 = fgbi * fgbi * fgbi;
-            const float temp6 = qiqj * temp4 * (dielfac + fgbk * expmkf);
-            fmag += temp6 * (1.0f - 0.25f * efac);
-            const float temp5 = 0.5f * efac * temp6 * (ijb + 0.25f * r2);
-            dei += gb_i.z * temp5;
-            dej += gb_j.z * temp5;
-          }
-        }
-        if (FORCE) {
-          fxi += fmag * dv.x;
-          fyi += fmag * dv.y;
-          fzi += fmag * dv.z;
-          fxj -= fmag * dv.x;
-          fyj -= fmag * dv.y;
-          fzj -= fmag * dv.z;
-        }
-      }
-      if (FORCE) {
-        const int src = (lane + 1) & 31;
-        fxj = __shfl_sync(kFullMask, fxj, src);
-        fyj = __shfl_sync(kFullMask, fyj, src);
-        fzj = __shfl_sync(kFullMask, fzj, src);
-        if (GB) {
-          dej = __shfl_sync(kFullMask, dej, src);
-        }
-      }
-    }
+    p.begin(ti.ibase + lane, mask);
+    walkTile(p, ti, lane);
     if (FORCE) {
-      if (ivalid) {
-        addForce(s, islot, fxi, fyi, fzi, fs);
+      if (lane < ti.ni) {
+        const int is = ti.ibase + lane;
+        addForce(s, is, p.fxi, p.fyi, p.fzi, fs);
         if (GB) {
-          atomicAddInt63(dei * ds, &s.de[islot], &s.deo[islot]);
+          atomicAddInt63(p.dei * ds, &s.de[is], &s.deo[is]);
         }
       }
-      const int jl_end = (lane + kend + 1) & 31;
-      if (jl_end < ti.nj) {
-        const int js = ti.jbase + jl_end;
-        addForce(s, js, fxj, fyj, fzj, fs);
+      const int jl = traveledAtom(ti, lane);
+      if (jl < ti.nj) {
+        const int js = ti.jbase + jl;
+        addForce(s, js, p.fxj, p.fyj, p.fzj, fs);
         if (GB) {
-          atomicAddInt63(dej * ds, &s.de[js], &s.deo[js]);
+          atomicAddInt63(p.dej * ds, &s.de[js], &s.deo[js]);
         }
       }
     }
     if (ENERGY) {
-      acc_elec += __float2ll_rn(e_elec * es);
-      acc_vdw += __float2ll_rn(e_vdw * es);
-      acc_gb += __float2ll_rn(e_gb * es);
+      acc_elec += __float2ll_rn(p.e_elec * es);
+      acc_vdw += __float2ll_rn(p.e_vdw * es);
+      acc_gb += __float2ll_rn(p.e_gb * es);
     }
   }
   if (ENERGY) {
-    // every warp flushes (lanes agree on acc_k); warps without tiles flush zeros harmlessly
     const long long se = warpSum(acc_elec), sv = warpSum(acc_vdw), sg = warpSum(acc_gb);
     if (lane == 0 && acc_k >= 0) {
       if (NB) {
@@ -690,56 +803,21 @@ __device__ void pairTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u, 
   }
 }
 
-// Pass 3: radius chain-rule forces
 __device__ void gbDerivativeTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u,
                                   int ntiles) {
   const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const int nwarp = blockDim.x >> 5;
   const float fs = d.frc_scale;
-  for (int t = warp; t < ntiles; t += nwarp) {
+  DerivPass p(s);
+  for (int t = threadIdx.x >> 5; t < ntiles; t += blockDim.x >> 5) {
     const TileInfo ti = tileInfo(s, nsys_u, t);
-    const bool ivalid = lane < ti.ni;
-    const int islot = ti.ibase + lane;
-    const float4 hi_i = s.hi[islot];
-    const float4 lo_i = s.lo[islot];
-    const float4 gb_i = s.gb[islot];
-    float fxi = 0.0f, fyi = 0.0f, fzi = 0.0f;
-    float fxj = 0.0f, fyj = 0.0f, fzj = 0.0f;
-    const int kbeg = ti.diag ? 1 : 0;
-    const int kend = ti.diag ? 16 : 31;
-    for (int k = kbeg; k <= kend; k++) {
-      const int jl = (lane + k) & 31;
-      const int jslot = ti.jbase + jl;
-      const bool active = ivalid && (jl < ti.nj) && (!ti.diag || k < 16 || lane < 16);
-      if (active) {
-        const float4 hi_j = s.hi[jslot];
-        const float4 lo_j = s.lo[jslot];
-        const float4 gb_j = s.gb[jslot];
-        const float3 dv = pairDelta(hi_i, lo_i, hi_j, lo_j);
-        const float r2 = dv.x * dv.x + dv.y * dv.y + dv.z * dv.z;
-        const float r = sqrtf(r2);
-        const float invr = 1.0f / r;
-        const float fmag = hctDerivative(r, r2, invr, gb_i.x, gb_j.y) * gb_i.w +
-                           hctDerivative(r, r2, invr, gb_j.x, gb_i.y) * gb_j.w;
-        fxi -= fmag * dv.x;
-        fyi -= fmag * dv.y;
-        fzi -= fmag * dv.z;
-        fxj += fmag * dv.x;
-        fyj += fmag * dv.y;
-        fzj += fmag * dv.z;
-      }
-      const int src = (lane + 1) & 31;
-      fxj = __shfl_sync(kFullMask, fxj, src);
-      fyj = __shfl_sync(kFullMask, fyj, src);
-      fzj = __shfl_sync(kFullMask, fzj, src);
+    p.begin(ti.ibase + lane);
+    walkTile(p, ti, lane);
+    if (lane < ti.ni) {
+      addForce(s, ti.ibase + lane, p.fxi, p.fyi, p.fzi, fs);
     }
-    if (ivalid) {
-      addForce(s, islot, fxi, fyi, fzi, fs);
-    }
-    const int jl_end = (lane + kend + 1) & 31;
-    if (jl_end < ti.nj) {
-      addForce(s, ti.jbase + jl_end, fxj, fyj, fzj, fs);
+    const int jl = traveledAtom(ti, lane);
+    if (jl < ti.nj) {
+      addForce(s, ti.jbase + jl, p.fxj, p.fyj, p.fzj, fs);
     }
   }
 }
@@ -750,7 +828,7 @@ __device__ void gbDerivativeTiles(const DevSynthesis &d, const UnitSmem &s, int 
 // The fused kernel
 // ------------------------------------------------------------------------------------------------
 template <bool FORCE, bool ENERGY, int TERMS>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
 kEvalFused(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
   extern __shared__ __align__(16) char smem_raw[];
   const UnitSmem s = carveSmem(smem_raw, d.max_unit_slots, max_lj);
@@ -779,21 +857,21 @@ kEvalFused(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
         s.slot0[k] = slot;
         s.tile0[k] = tile;
         s.ljbase[k] = lj;
-        s.bond0[k] = nb;
-        s.angl0[k] = na;
-        s.dihe0[k] = nd;
+        s.bchunk0[k] = nb;
+        s.achunk0[k] = na;
+        s.dchunk0[k] = nd;
         slot += nblk * kTile;
         tile += nblk * (nblk + 1) / 2;
         const int nt = d.lj_ntypes[sysid];
         lj += 2 * nt * nt;
-        nb += d.bond_start[sysid + 1] - d.bond_start[sysid];
-        na += d.angl_start[sysid + 1] - d.angl_start[sysid];
-        nd += d.dihe_start[sysid + 1] - d.dihe_start[sysid];
+        nb += (d.bond_start[sysid + 1] - d.bond_start[sysid] + 31) / 32;
+        na += (d.angl_start[sysid + 1] - d.angl_start[sysid] + 31) / 32;
+        nd += (d.dihe_start[sysid + 1] - d.dihe_start[sysid] + 31) / 32;
       }
       s.tile0[nsys_u] = tile;
-      s.bond0[nsys_u] = nb;
-      s.angl0[nsys_u] = na;
-      s.dihe0[nsys_u] = nd;
+      s.bchunk0[nsys_u] = nb;
+      s.achunk0[nsys_u] = na;
+      s.dchunk0[nsys_u] = nd;
       if (slot != nslots || tile != ntiles || lj > max_lj || slot > d.max_unit_slots) {
         atomicOr(d.status, 1);
       }
@@ -817,41 +895,42 @@ kEvalFused(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
       }
     }
 
-    // stage atoms
+    // stage atoms (a warp's 32 consecutive slots always belong to one molecule)
     for (int slot = threadIdx.x; slot < nslots; slot += blockDim.x) {
       const int k = findOwner(s.slot0, nsys_u, slot);
       const int sysid = s.sys[k];
       const int a = slot - s.slot0[k];
-      float4 hi, lo, g;
+      float4 pa, pb, prm;
       if (a < s.natom[k]) {
         const int gi = d.atom_start[sysid] + a;
         const double x = static_cast<double>(d.xcrd[gi]) * d.inv_gpos_scale;
         const double y = static_cast<double>(d.ycrd[gi]) * d.inv_gpos_scale;
         const double z = static_cast<double>(d.zcrd[gi]) * d.inv_gpos_scale;
-        hi.x = static_cast<float>(x);
-        hi.y = static_cast<float>(y);
-        hi.z = static_cast<float>(z);
-        hi.w = d.charge[gi];
-        lo.x = static_cast<float>(x - static_cast<double>(hi.x));
-        lo.y = static_cast<float>(y - static_cast<double>(hi.y));
-        lo.z = static_cast<float>(z - static_cast<double>(hi.z));
+        pa.x = static_cast<float>(x);
+        pa.y = static_cast<float>(y);
+        pa.z = static_cast<float>(z);
+        pb.x = static_cast<float>(x - static_cast<double>(pa.x));
+        pb.y = static_cast<float>(y - static_cast<double>(pa.y));
+        pb.z = static_cast<float>(z - static_cast<double>(pa.z));
         const int nt = d.lj_ntypes[sysid];
         const int ty = d.lj_idx[gi];
-        lo.w = __int_as_float((s.ljbase[k] + ty * nt) | (ty << 16));
-        g.x = d.rho[gi];
-        g.y = d.srho[gi];
-        g.z = 1.0f;
-        g.w = 0.0f;
+        prm.x = d.charge[gi];
+        prm.y = __int_as_float((s.ljbase[k] + ty * nt) | (ty << 16));
+        prm.z = d.rho[gi];
+        prm.w = d.srho[gi];
       }
       else {
         // padding slot: never paired (validity checks), kept finite
-        hi = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        lo = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(s.ljbase[k]));
-        g = make_float4(1.0f, 0.0f, 1.0f, 0.0f);
+        pa = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        pb = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+        prm = make_float4(0.0f, __int_as_float(s.ljbase[k]), 1.0f, 0.0f);
       }
-      s.hi[slot] = hi;
-      s.lo[slot] = lo;
-      s.gb[slot] = g;
+      pa.w = prm.w;   // pass 1 payload: s * rho
+      pb.w = prm.z;   //                 rho
+      s.pa[slot] = pa;
+      s.pb[slot] = pb;
+      s.prm[slot] = prm;
+      s.gbv[slot] = make_float2(1.0f, 0.0f);
       s.fx[slot] = 0;
       s.fy[slot] = 0;
       s.fz[slot] = 0;
@@ -870,48 +949,70 @@ kEvalFused(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
       __syncthreads();
     }
     if (gb) {
-      gbRadiiTiles(d, s, nsys_u, ntiles);
+      gbRadiiTiles(s, nsys_u, ntiles);
       __syncthreads();
-      // effective radii, self terms (nonbonded_potential.tpp:730-805)
+      // effective radii, self terms (nonbonded_potential.tpp:730-805); a warp's 32 slots
+      // belong to one molecule, so the self energies reduce across the warp
       const float inv_ps = 1.0f / static_cast<float>(1 << kPsiBits);
       const float ds = static_cast<float>(1 << kDeijdaBits);
       for (int slot = threadIdx.x; slot < nslots; slot += blockDim.x) {
         const int k = findOwner(s.slot0, nsys_u, slot);
         const int a = slot - s.slot0[k];
-        if (a >= s.natom[k]) continue;
-        const int gi = d.atom_start[s.sys[k]] + a;
-        const float psi = static_cast<float>(int63ToLong(s.psi[slot], s.psio[slot])) * inv_ps;
-        float4 g = s.gb[slot];
-        const float rho = g.x;
-        float egbi;
-        if (d.igb == 1) {
-          egbi = 1.0f / (1.0f / rho + psi);
-          if (egbi < 0.0f) egbi = 30.0f;
+        float e_self = 0.0f;
+        float4 pa = s.pa[slot];
+        float4 pb = s.pb[slot];
+        const float4 prm = s.prm[slot];
+        float egbi = 1.0f;
+        if (a < s.natom[k]) {
+          const int gi = d.atom_start[s.sys[k]] + a;
+          const float psi = static_cast<float>(int63ToLong(s.psi[slot], s.psio[slot])) * inv_ps;
+          const float rho = prm.z;
+          if (d.igb == 1) {
+            egbi = 1.0f / (1.0f / rho + psi);
+            if (egbi < 0.0f) egbi = 30.0f;
+          }
+          else {
+            const float fipsi = psi * (-rho);
+            egbi = 1.0f / (1.0f / rho - tanhf((d.gb_alpha[gi] - d.gb_beta[gi] * fipsi +
+                                               d.gb_gamma[gi] * fipsi * fipsi) * fipsi) /
+                                        d.pb_radii[gi]);
+          }
+          const float q = prm.x;   // already scaled by sqrt(Coulomb constant)
+          const float expmkf = ((d.kappa > 0.0f) ? expf(-kGbKscale * d.kappa * egbi) : 1.0f) *
+                               d.inv_dielectric;
+          const float dielfac = 1.0f - expmkf;
+          const float atmq2h = 0.5f * q * q;
+          const float atmqd2h = atmq2h * dielfac;
+          e_self = -__fdiv_rn(atmqd2h, egbi);
+          if (FORCE) {
+            const float self_de = atmqd2h - kGbKscale * d.kappa * atmq2h * expmkf * egbi;
+            atomicAddInt63(self_de * ds, &s.de[slot], &s.deo[slot]);
+          }
+          d.born_radii[gi] = egbi;
+          d.psi[gi] = __double2ll_rn(static_cast<double>(psi) * d.psi_out_scale);
+          d.psi_ovrf[gi] = 0;
+          pa.w = prm.x;   // pass 2 payload: charge
+          pb.w = egbi;    //                 effective radius
         }
         else {
-          const float fipsi = psi * (-rho);
-          egbi = 1.0f / (1.0f / rho - tanhf((d.gb_alpha[gi] - d.gb_beta[gi] * fipsi +
-                                             d.gb_gamma[gi] * fipsi * fipsi) * fipsi) /
-                                      d.pb_radii[gi]);
+          pa.w = 0.0f;
+          pb.w = 1.0f;
         }
-        g.z = egbi;
-        s.gb[slot] = g;
-        const float q = s.hi[slot].w;   // already scaled by sqrt(Coulomb constant)
-        const float expmkf = ((d.kappa > 0.0f) ? expf(-kGbKscale * d.kappa * egbi) : 1.0f) *
-                             d.inv_dielectric;
-        const float dielfac = 1.0f - expmkf;
-        const float atmq2h = 0.5f * q * q;
-        const float atmqd2h = atmq2h * dielfac;
+        s.pa[slot] = pa;
+        s.pb[slot] = pb;
+        s.gbv[slot].x = egbi;
         if (ENERGY) {
-          addEnergy(s, k, kGb, -__fdiv_rn(atmqd2h, egbi), d.nrg_scale);
+          warpEnergy(s, k, kGb, e_self, d.nrg_scale);
         }
-        if (FORCE) {
-          const float self_de = atmqd2h - kGbKscale * d.kappa * atmq2h * expmkf * egbi;
-          atomicAddInt63(self_de * ds, &s.de[slot], &s.deo[slot]);
-        }
-        d.born_radii[gi] = egbi;
-        d.psi[gi] = __double2ll_rn(static_cast<double>(psi) * d.psi_out_scale);
-        d.psi_ovrf[gi] = 0;
+      }
+      __syncthreads();
+    }
+    else if (NB) {
+      // pass 2 payload for Coulomb / Lennard-Jones alone: charge in w1
+      for (int slot = threadIdx.x; slot < nslots; slot += blockDim.x) {
+        float4 pa = s.pa[slot];
+        pa.w = s.prm[slot].x;
+        s.pa[slot] = pa;
       }
       __syncthreads();
     }
@@ -928,33 +1029,37 @@ kEvalFused(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
       __syncthreads();
     }
     if (gb && FORCE) {
-      // chain-rule prefactor of the OBC radii (nonbonded_potential.tpp:982-1021)
+      // chain-rule prefactor of the OBC radii (nonbonded_potential.tpp:982-1021), and the
+      // pass 3 payloads
       const float inv_ds = 1.0f / static_cast<float>(1 << kDeijdaBits);
       const float inv_ps = 1.0f / static_cast<float>(1 << kPsiBits);
       for (int slot = threadIdx.x; slot < nslots; slot += blockDim.x) {
         const int k = findOwner(s.slot0, nsys_u, slot);
         const int a = slot - s.slot0[k];
-        float4 g = s.gb[slot];
-        if (a >= s.natom[k]) {
-          g.w = 0.0f;
-          s.gb[slot] = g;
-          continue;
+        const float4 prm = s.prm[slot];
+        float4 pa = s.pa[slot];
+        float4 pb = s.pb[slot];
+        pa.w = prm.w;   // s * rho
+        pb.w = prm.z;   // rho
+        float sde = 0.0f;
+        if (a < s.natom[k]) {
+          const int gi = d.atom_start[s.sys[k]] + a;
+          sde = static_cast<float>(int63ToLong(s.de[slot], s.deo[slot])) * inv_ds;
+          if (d.igb != 1) {
+            const float psi = static_cast<float>(int63ToLong(s.psi[slot], s.psio[slot])) * inv_ps;
+            const float rho = prm.z;
+            const float fipsi = psi * (-rho);
+            const float al = d.gb_alpha[gi], be = d.gb_beta[gi], ga = d.gb_gamma[gi];
+            const float thi = tanhf((al - (be - ga * fipsi) * fipsi) * fipsi);
+            sde *= (al - (2.0f * be - 3.0f * ga * fipsi) * fipsi) * (1.0f - thi * thi) * rho /
+                   d.pb_radii[gi];
+          }
+          d.sumdeijda[gi] = __double2ll_rn(static_cast<double>(sde) * d.psi_out_scale);
+          d.sumdeijda_ovrf[gi] = 0;
         }
-        const int gi = d.atom_start[s.sys[k]] + a;
-        float sde = static_cast<float>(int63ToLong(s.de[slot], s.deo[slot])) * inv_ds;
-        if (d.igb != 1) {
-          const float psi = static_cast<float>(int63ToLong(s.psi[slot], s.psio[slot])) * inv_ps;
-          const float rho = g.x;
-          const float fipsi = psi * (-rho);
-          const float al = d.gb_alpha[gi], be = d.gb_beta[gi], ga = d.gb_gamma[gi];
-          const float thi = tanhf((al - (be - ga * fipsi) * fipsi) * fipsi);
-          sde *= (al - (2.0f * be - 3.0f * ga * fipsi) * fipsi) * (1.0f - thi * thi) * rho /
-                 d.pb_radii[gi];
-        }
-        g.w = sde;
-        s.gb[slot] = g;
-        d.sumdeijda[gi] = __double2ll_rn(static_cast<double>(sde) * d.psi_out_scale);
-        d.sumdeijda_ovrf[gi] = 0;
+        s.pa[slot] = pa;
+        s.pb[slot] = pb;
+        s.gbv[slot].y = sde;
       }
       __syncthreads();
       gbDerivativeTiles(d, s, nsys_u, ntiles);

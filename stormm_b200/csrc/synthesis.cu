@@ -267,8 +267,8 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
 }
 
 void Synthesis::buildUnits() {
-  const int max_slots_cap = (opt.max_atoms_per_unit > 0) ? opt.max_atoms_per_unit : 512;
-  const int max_tiles_cap = (opt.max_tiles_per_unit > 0) ? opt.max_tiles_per_unit : 64;
+  const int max_slots_cap = (opt.max_atoms_per_unit > 0) ? opt.max_atoms_per_unit : 256;
+  const int max_tiles_cap = (opt.max_tiles_per_unit > 0) ? opt.max_tiles_per_unit : 36;
   threads = (opt.threads_per_block > 0) ? opt.threads_per_block : 256;
   if (threads % 32 != 0 || threads < 64 || threads > 256) {
     throw Error(SB_ERR_ARGUMENT, "threads per block must be a multiple of 32 in [64, 256]");
@@ -283,7 +283,7 @@ void Synthesis::buildUnits() {
     return nb * (nb + 1) / 2;
   };
   auto lj_of = [&](int s) { return 2 * h_lj_ntypes[s] * h_lj_ntypes[s]; };
-  const int max_lj_cap = 4096;
+  const int max_lj_cap = 2048;
   h_units.clear();
   h_unit_systems.clear();
   // molecules above the packing cap: one unit each, at the front (largest first)
