@@ -152,10 +152,14 @@ int sb_system_atoms(const sb_synthesis* syn, int system, int* natom, int* offset
 int sb_padded_atom_count(const sb_synthesis* syn);
 
 /* ------------------------------------------------------------------------------------------ */
-/* Host <-> device transfers (asynchronous on the stream; host buffers should be pinned for     */
-/* overlap).  xyz arrays hold all systems back to back without padding, 3 doubles per atom.    */
+/* Host <-> device transfers.  xyz arrays hold all systems back to back without padding,       */
+/* 3 doubles per atom.  Each call is one copy plus a conversion kernel on the stream.          */
 /* ------------------------------------------------------------------------------------------ */
+/* Asynchronous: with a pinned host buffer the caller must keep it unchanged until the stream
+ * reaches this point.  Non-finite or out-of-range coordinates leave those atoms unchanged and
+ * set bit 2 of the status word (sb_check_status). */
 int sb_set_coordinates(sb_synthesis* syn, const double* xyz, void* stream);
+/* The getters synchronize the stream before returning. */
 int sb_get_coordinates(sb_synthesis* syn, double* xyz, void* stream);
 int sb_get_forces(sb_synthesis* syn, double* xyz, void* stream);
 /* energies: nsys * SB_NRG_STRIDE doubles, kcal/mol, STORMM's slot order */

@@ -52,58 +52,70 @@ constexpr unsigned kFullMask = 0xffffffffu;
 
 // HCT descreening of an atom of offset radius rho by a neighbour of screened radius sj at
 // distance r (invr = 1/r); returns the amount psi decreases by.
+//
+// Beyond r = 4 sj the reference's Taylor series applies (nonbonded_potential.tpp:590-596).
+// Closer in, the three closed forms the reference selects by overlap case (no overlap, partial
+// overlap, atom inside the neighbour's sphere: nonbonded_potential.tpp:597-628) are one
+// expression in U = r + sj and L = max(rho, |r - sj|):
+//   I = 1/2 [1/L - 1/U + (sj^2 - r^2)/(4r) (1/L^2 - 1/U^2) + ln(L/U) / (2r)]
+//       + (1/rho - 1/L) when rho < sj - r,
+// and I = 0 when rho >= U.  One formula instead of four keeps a warp on at most two paths.
 __device__ __forceinline__ float hctIntegral(float r, float r2, float invr, float rho, float sj) {
-  const float sj2 = sj * sj;
   if (r > 4.0f * sj) {
+    const float sj2 = sj * sj;
     const float invr2 = invr * invr;
     const float t = sj2 * invr2;
     const float dumbo = kTaylorA + t * (kTaylorB + t * (kTaylorC + t * (kTaylorD + t * kTaylorDD)));
     return sj * t * invr2 * dumbo;
   }
-  if (r > rho + sj) {
-    return 0.5f * (__fdividef(sj, r2 - sj2) + 0.5f * invr * __logf(__fdividef(r - sj, r + sj)));
+  const float u = r + sj;
+  if (rho >= u) {
+    return 0.0f;
   }
-  if (r > fabsf(rho - sj)) {
-    const float inv_rho = __fdividef(1.0f, rho);
-    const float theta = 0.5f * inv_rho * invr * (r2 + rho * rho - sj2);
-    const float uij = __fdividef(1.0f, r + sj);
-    return 0.25f * (inv_rho * (2.0f - theta) - uij + invr * __logf(rho * uij));
+  const float l = fmaxf(rho, fabsf(r - sj));
+  const float inv_lu = __fdividef(1.0f, l * u);
+  const float il = u * inv_lu;
+  const float iu = l * inv_lu;
+  const float dlu = il - iu;
+  float v = dlu + 0.25f * (sj * sj - r2) * invr * dlu * (il + iu) + 0.5f * invr * __logf(l * iu);
+  if (rho < sj - r) {
+    v += 2.0f * (__fdividef(1.0f, rho) - il);
   }
-  if (rho < sj) {
-    return 0.5f * (__fdividef(sj, r2 - sj2) + __fdividef(2.0f, rho) +
-                   0.5f * invr * __logf(__fdividef(sj - r, sj + r)));
-  }
-  return 0.0f;
+  return 0.5f * v;
 }
 
-// Radial derivative of hctIntegral divided by r
+// Radial derivative of hctIntegral, -(1/r) dI/dr, the factor the reference multiplies by the
+// chain-rule dE/dR (nonbonded_potential.tpp:1116-1165), from the same unified expression
+// (lambda = dL/dr: 1 without overlap, 0 on partial overlap, -1 inside the neighbour).
 __device__ __forceinline__ float hctDerivative(float r, float r2, float invr, float rho,
                                                float sj) {
   const float invr2 = invr * invr;
-  const float sj2 = sj * sj;
   if (r > 4.0f * sj) {
-    const float t = sj2 * invr2;
+    const float t = sj * sj * invr2;
     const float dumbo = kTaylorE + t * (kTaylorF + t * (kTaylorG + t * (kTaylorH + t * kTaylorHH)));
     return t * sj * invr2 * invr2 * dumbo;
   }
-  if (r > rho + sj) {
-    const float temp1 = __fdividef(1.0f, r2 - sj2);
-    return temp1 * sj * (-0.5f * invr2 + temp1) +
-           0.25f * invr * invr2 * __logf(__fdividef(r - sj, r + sj));
+  const float u = r + sj;
+  if (rho >= u) {
+    return 0.0f;
   }
-  if (r > fabsf(rho - sj)) {
-    const float temp1 = __fdividef(1.0f, r + sj);
-    const float invr3 = invr2 * invr;
-    const float inv_rho = __fdividef(1.0f, rho);
-    return -0.25f * (-0.5f * (r2 - rho * rho + sj2) * invr3 * inv_rho * inv_rho +
-                     invr * temp1 * (temp1 - invr) - invr3 * __logf(rho * temp1));
+  const float rms = r - sj;
+  const float l = fmaxf(rho, fabsf(rms));
+  const float lam = (rms >= rho) ? 1.0f : ((-rms > rho) ? -1.0f : 0.0f);
+  const float inv_lu = __fdividef(1.0f, l * u);
+  const float il = u * inv_lu;
+  const float iu = l * inv_lu;
+  const float il2 = il * il;
+  const float iu2 = iu * iu;
+  const float q = 0.25f * (sj * sj - r2) * invr;
+  const float dq = -0.25f * fmaf(sj * sj, invr2, 1.0f);
+  float di = -lam * il2 + iu2 + dq * (il2 - iu2) + 2.0f * q * (iu2 * iu - lam * il2 * il) +
+             0.5f * invr * (lam * il - iu - invr * __logf(l * iu));
+  di *= 0.5f;
+  if (-rms > rho) {
+    di -= il2;
   }
-  if (rho < sj) {
-    const float temp1 = __fdividef(1.0f, r2 - sj2);
-    return -0.5f * (sj * invr2 * temp1 - 2.0f * sj * temp1 * temp1 -
-                    0.5f * invr2 * invr * __logf(__fdividef(sj - r, sj + r)));
-  }
-  return 0.0f;
+  return -di * invr;
 }
 
 // Shared-memory layout of one work unit
@@ -526,7 +538,7 @@ __device__ __forceinline__ TileInfo tileInfo(const UnitSmem &s, int nsys_u, int 
 template <class P>
 __device__ __forceinline__ void walkTile(P &p, const TileInfo &ti, int lane) {
   if (!ti.diag && ti.ni == kTile && ti.nj == kTile) {
-#pragma unroll 4
+#pragma unroll 2
     for (int k = 0; k < kTile; k++) {
       const int jl = (lane + k) & 31;
       p.pair(ti.jbase + jl, jl);
@@ -944,9 +956,12 @@ kEvalFused(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
     }
     __syncthreads();
 
+    // valence terms and GB pass 1 touch disjoint accumulators: no barrier between them
     if (VALE) {
       valenceTerms<FORCE, ENERGY>(d, s, nsys_u);
-      __syncthreads();
+      if (!gb) {
+        __syncthreads();
+      }
     }
     if (gb) {
       gbRadiiTiles(s, nsys_u, ntiles);

@@ -25,6 +25,18 @@ size_t fusedSmemBytes(int max_slots, int max_lj);
 cudaError_t launchEvalFused(const DevSynthesis &d, int unit_begin, int unit_end, int max_lj,
                             int terms, bool force, bool energy, int blocks, int threads,
                             cudaStream_t stream);
+cudaError_t launchImportCoordinates(const double* d_xyz, const int* d_map, int natom,
+                                    double scale, long long* xcrd, long long* ycrd,
+                                    long long* zcrd, int* xo, int* yo, int* zo, int* status,
+                                    cudaStream_t stream);
+cudaError_t launchExportCoordinates(const long long* xcrd, const long long* ycrd,
+                                    const long long* zcrd, const int* d_map, int natom,
+                                    double inv_scale, double* d_xyz, cudaStream_t stream);
+cudaError_t launchExportForces(const long long* xf, const long long* yf, const long long* zf,
+                               const int* xo, const int* yo, const int* zo, const int* d_map,
+                               int natom, double inv_scale, double* d_xyz, cudaStream_t stream);
+cudaError_t launchExportEnergies(const unsigned long long* nrg, int n, double inv_scale,
+                                 double* d_out, cudaStream_t stream);
 
 namespace {
 thread_local std::string g_last_error;
@@ -123,6 +135,14 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
     off += (atom_count[s] + kTile - 1) / kTile * kTile;
   }
   natom_padded = off;
+  natom_total = 0;
+  h_unpadded_map.clear();
+  for (int sy = 0; sy < nsys; sy++) {
+    for (int i = 0; i < atom_count[sy]; i++) {
+      h_unpadded_map.push_back(atom_start[sy] + i);
+    }
+    natom_total += atom_count[sy];
+  }
   const size_t np = natom_padded;
   h_charge.assign(np, 0.0f);
   h_ljidx.assign(np, 0);
@@ -382,6 +402,9 @@ void Synthesis::upload() {
   d_unit_systems.upload(h_unit_systems);
   d_single_units.upload(h_single_units);
   d_single_systems.upload(h_single_systems);
+  d_unpadded_map.upload(h_unpadded_map);
+  d_stage_xyz.zeros(static_cast<size_t>(3) * natom_total);
+  d_stage_nrg.zeros(static_cast<size_t>(nsys) * kNrgStride);
   const size_t np = natom_padded;
   d_xcrd.zeros(np);
   d_ycrd.zeros(np);
@@ -527,54 +550,24 @@ void Synthesis::initialize(int what, cudaStream_t stream) {
 }
 
 void Synthesis::setCoordinates(const double* xyz, cudaStream_t stream) {
-  const size_t np = natom_padded;
-  h_stage_ll.assign(3 * np, 0);
-  const double scale = std::ldexp(1.0, opt.gpos_bits);
-  size_t src = 0;
-  for (int s = 0; s < nsys; s++) {
-    for (int i = 0; i < atom_count[s]; i++) {
-      const size_t a = atom_start[s] + i;
-      for (int c = 0; c < 3; c++) {
-        const double v = xyz[3 * src + c];
-        if (!std::isfinite(v) || std::fabs(v) * scale > 9.0e18) {
-          throw Error(SB_ERR_ARGUMENT, "coordinate of system " + std::to_string(s) + " atom " +
-                      std::to_string(i) + " is not finite or out of the fixed-point range");
-        }
-        h_stage_ll[c * np + a] = std::llround(v * scale);
-      }
-      src++;
-    }
-  }
-  cudaCheck(cudaMemcpyAsync(d_xcrd.p, h_stage_ll.data(), np * sizeof(long long),
+  // one copy of the caller's array (pinned memory makes it asynchronous and fast), then the
+  // conversion to fixed point on the device; non-finite or out-of-range input sets bit 2 of
+  // the status word and leaves those atoms unchanged
+  cudaCheck(cudaMemcpyAsync(d_stage_xyz.p, xyz, sizeof(double) * 3 * natom_total,
                             cudaMemcpyHostToDevice, stream), "coordinate upload");
-  cudaCheck(cudaMemcpyAsync(d_ycrd.p, h_stage_ll.data() + np, np * sizeof(long long),
-                            cudaMemcpyHostToDevice, stream), "coordinate upload");
-  cudaCheck(cudaMemcpyAsync(d_zcrd.p, h_stage_ll.data() + 2 * np, np * sizeof(long long),
-                            cudaMemcpyHostToDevice, stream), "coordinate upload");
-  cudaCheck(cudaStreamSynchronize(stream), "coordinate upload");
+  cudaCheck(launchImportCoordinates(d_stage_xyz.p, d_unpadded_map.p, natom_total,
+                                    std::ldexp(1.0, opt.gpos_bits), d_xcrd.p, d_ycrd.p,
+                                    d_zcrd.p, d_xcrd_ovrf.p, d_ycrd_ovrf.p, d_zcrd_ovrf.p,
+                                    d_status.p, stream), "coordinate import");
 }
 
 void Synthesis::getCoordinates(double* xyz, cudaStream_t stream) {
-  const size_t np = natom_padded;
-  h_stage_ll.resize(3 * np);
-  cudaCheck(cudaMemcpyAsync(h_stage_ll.data(), d_xcrd.p, np * sizeof(long long),
-                            cudaMemcpyDeviceToHost, stream), "coordinate download");
-  cudaCheck(cudaMemcpyAsync(h_stage_ll.data() + np, d_ycrd.p, np * sizeof(long long),
-                            cudaMemcpyDeviceToHost, stream), "coordinate download");
-  cudaCheck(cudaMemcpyAsync(h_stage_ll.data() + 2 * np, d_zcrd.p, np * sizeof(long long),
+  cudaCheck(launchExportCoordinates(d_xcrd.p, d_ycrd.p, d_zcrd.p, d_unpadded_map.p, natom_total,
+                                    std::ldexp(1.0, -opt.gpos_bits), d_stage_xyz.p, stream),
+            "coordinate export");
+  cudaCheck(cudaMemcpyAsync(xyz, d_stage_xyz.p, sizeof(double) * 3 * natom_total,
                             cudaMemcpyDeviceToHost, stream), "coordinate download");
   cudaCheck(cudaStreamSynchronize(stream), "coordinate download");
-  const double inv = std::ldexp(1.0, -opt.gpos_bits);
-  size_t dst = 0;
-  for (int s = 0; s < nsys; s++) {
-    for (int i = 0; i < atom_count[s]; i++) {
-      const size_t a = atom_start[s] + i;
-      for (int c = 0; c < 3; c++) {
-        xyz[3 * dst + c] = static_cast<double>(h_stage_ll[c * np + a]) * inv;
-      }
-      dst++;
-    }
-  }
 }
 
 void Synthesis::getForcesFixed(long long* prim, int* ovrf, cudaStream_t stream) {
@@ -595,23 +588,13 @@ void Synthesis::getForcesFixed(long long* prim, int* ovrf, cudaStream_t stream) 
 }
 
 void Synthesis::getForces(double* xyz, cudaStream_t stream) {
-  const size_t np = natom_padded;
-  std::vector<long long> prim(3 * np);
-  std::vector<int> ovrf(3 * np);
-  getForcesFixed(prim.data(), ovrf.data(), stream);
-  const double inv = std::ldexp(1.0, -opt.frc_bits);
-  size_t dst = 0;
-  for (int s = 0; s < nsys; s++) {
-    for (int i = 0; i < atom_count[s]; i++) {
-      const size_t a = atom_start[s] + i;
-      for (int c = 0; c < 3; c++) {
-        const double v = static_cast<double>(ovrf[c * np + a]) * 9223372036854775808.0 +
-                         static_cast<double>(prim[c * np + a]);
-        xyz[3 * dst + c] = v * inv;
-      }
-      dst++;
-    }
-  }
+  cudaCheck(launchExportForces(d_xfrc.p, d_yfrc.p, d_zfrc.p, d_xfrc_ovrf.p, d_yfrc_ovrf.p,
+                               d_zfrc_ovrf.p, d_unpadded_map.p, natom_total,
+                               std::ldexp(1.0, -opt.frc_bits), d_stage_xyz.p, stream),
+            "force export");
+  cudaCheck(cudaMemcpyAsync(xyz, d_stage_xyz.p, sizeof(double) * 3 * natom_total,
+                            cudaMemcpyDeviceToHost, stream), "force download");
+  cudaCheck(cudaStreamSynchronize(stream), "force download");
 }
 
 void Synthesis::getEnergiesFixed(long long* out, cudaStream_t stream) {
@@ -621,12 +604,12 @@ void Synthesis::getEnergiesFixed(long long* out, cudaStream_t stream) {
 }
 
 void Synthesis::getEnergies(double* out, cudaStream_t stream) {
-  std::vector<long long> raw(d_energies.n);
-  getEnergiesFixed(raw.data(), stream);
-  const double inv = std::ldexp(1.0, -opt.nrg_bits);
-  for (size_t e = 0; e < raw.size(); e++) {
-    out[e] = static_cast<double>(raw[e]) * inv;
-  }
+  const int n = nsys * kNrgStride;
+  cudaCheck(launchExportEnergies(d_energies.p, n, std::ldexp(1.0, -opt.nrg_bits), d_stage_nrg.p,
+                                 stream), "energy export");
+  cudaCheck(cudaMemcpyAsync(out, d_stage_nrg.p, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                            stream), "energy download");
+  cudaCheck(cudaStreamSynchronize(stream), "energy download");
 }
 
 void Synthesis::getGbWorkspace(double* psi, double* radii, double* sde, cudaStream_t stream) {

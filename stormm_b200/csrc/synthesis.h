@@ -85,6 +85,7 @@ public:
   sb_options opt;
   int nsys = 0;
   int natom_padded = 0;
+  int natom_total = 0;       // atoms without padding
   int sm_count = 0;
   int max_smem_optin = 0;
   int threads = 256;
@@ -108,6 +109,7 @@ public:
   std::vector<int4> h_units, h_single_units;
   std::vector<int> h_unit_systems, h_single_systems;
   std::vector<long long> h_stage_ll;
+  std::vector<int> h_unpadded_map;   // padded index of each unpadded atom
 
   // device arrays
   DeviceArray<int> d_atom_start, d_atom_count, d_bond_start, d_angl_start, d_dihe_start;
@@ -124,6 +126,8 @@ public:
   DeviceArray<long long> d_psi, d_sumdeijda;
   DeviceArray<int> d_psi_ovrf, d_sumdeijda_ovrf, d_status;
   DeviceArray<float> d_born_radii;
+  DeviceArray<int> d_unpadded_map;
+  DeviceArray<double> d_stage_xyz, d_stage_nrg;
 
   DevSynthesis dev;
 
