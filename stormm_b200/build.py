@@ -22,7 +22,7 @@ SYNTH_LIB = os.path.join(PKG, "libstormm_b200_synth.so")
 CUDA_SOURCES = ["eval_fused.cu", "synthesis.cu", "transfers.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared", "-Xptxas", "-v",
+    "-Xcompiler", "-fPIC", "-shared", "-Xptxas", "-v", "-ftz=true",
 ]
 
 

@@ -35,7 +35,7 @@ enum NrgSlot : int {
 };
 
 // Bond record:     x = i | j << 16, y = keq, z = leq (high float), w = leq - z (low float)
-// Angle record:    x = i | j << 16, y = k, z = keq, w = theta0
+// Angle record:    x = i | j << 16, y = k, z = keq, w = cos(theta0)
 // Dihedral record: a.x = i | j << 16, a.y = k | l << 16 | improper << 31, a.z = amp, a.w = freq
 //                  b.x = cos(phase), b.y = sin(phase), b.z = 1/scee (0: no 1-4), b.w = 1/scnb
 // (floats stored as their bit patterns; indices are molecule-local)

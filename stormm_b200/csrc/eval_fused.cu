@@ -26,7 +26,7 @@
 // Shared memory per atom slot: pos_a = (x_hi, y_hi, z_hi, w1) and pos_b = (x_lo, y_lo, z_lo, w2)
 // feed the pair passes with two 16-byte loads per partner; w1 / w2 carry what the pass needs
 // (pass 1 and 3: s*rho and rho; pass 2: charge and effective radius).  prm holds the static
-// per-atom values, gbv the effective radius and the chain-rule dE/dR of the evaluation.
+// per-atom values, gbv the reciprocal effective radius and the chain-rule dE/dR.
 #include <cuda_runtime.h>
 
 #include "device_kits.h"
@@ -69,9 +69,6 @@ __device__ __forceinline__ float hctIntegral(float r, float r2, float invr, floa
     return sj * t * invr2 * dumbo;
   }
   const float u = r + sj;
-  if (rho >= u) {
-    return 0.0f;
-  }
   const float l = fmaxf(rho, fabsf(r - sj));
   const float inv_lu = __fdividef(1.0f, l * u);
   const float il = u * inv_lu;
@@ -79,9 +76,10 @@ __device__ __forceinline__ float hctIntegral(float r, float r2, float invr, floa
   const float dlu = il - iu;
   float v = dlu + 0.25f * (sj * sj - r2) * invr * dlu * (il + iu) + 0.5f * invr * __logf(l * iu);
   if (rho < sj - r) {
+    // the atom sits inside the neighbour's sphere: rare, so a branch beats a reciprocal per pair
     v += 2.0f * (__fdividef(1.0f, rho) - il);
   }
-  return 0.5f * v;
+  return (rho < u) ? 0.5f * v : 0.0f;
 }
 
 // Radial derivative of hctIntegral, -(1/r) dI/dr, the factor the reference multiplies by the
@@ -96,9 +94,6 @@ __device__ __forceinline__ float hctDerivative(float r, float r2, float invr, fl
     return t * sj * invr2 * invr2 * dumbo;
   }
   const float u = r + sj;
-  if (rho >= u) {
-    return 0.0f;
-  }
   const float rms = r - sj;
   const float l = fmaxf(rho, fabsf(rms));
   const float lam = (rms >= rho) ? 1.0f : ((-rms > rho) ? -1.0f : 0.0f);
@@ -111,11 +106,8 @@ __device__ __forceinline__ float hctDerivative(float r, float r2, float invr, fl
   const float dq = -0.25f * fmaf(sj * sj, invr2, 1.0f);
   float di = -lam * il2 + iu2 + dq * (il2 - iu2) + 2.0f * q * (iu2 * iu - lam * il2 * il) +
              0.5f * invr * (lam * il - iu - invr * __logf(l * iu));
-  di *= 0.5f;
-  if (-rms > rho) {
-    di -= il2;
-  }
-  return -di * invr;
+  di = 0.5f * di - ((-rms > rho) ? il2 : 0.0f);
+  return (rho < u) ? -di * invr : 0.0f;
 }
 
 // Shared-memory layout of one work unit
@@ -123,7 +115,7 @@ struct UnitSmem {
   float4* pa;       // x_hi, y_hi, z_hi, pass payload w1
   float4* pb;       // x_lo, y_lo, z_lo, pass payload w2
   float4* prm;      // charge * sqrt(k_Coulomb), Lennard-Jones code (int bits), rho, s * rho
-  float2* gbv;      // effective radius, dE/dR after the chain rule
+  float2* gbv;      // 1 / effective radius, dE/dR after the chain rule
   int* fx;          // int63 force accumulators: primary
   int* fy;
   int* fz;
@@ -335,8 +327,8 @@ __device__ void valenceTerms(const DevSynthesis &d, const UnitSmem &s, int nsys_
       const int ja = s.slot0[k] + static_cast<int>(rec.x >> 16);
       const int ka = s.slot0[k] + static_cast<int>(rec.y);
       const float keq = __uint_as_float(rec.z);
-      float sth0, cth0;
-      sincosf(__uint_as_float(rec.w), &sth0, &cth0);
+      const float cth0 = __uint_as_float(rec.w);
+      const float sth0 = sqrtf(fmaxf(0.0f, fmaf(-cth0, cth0, 1.0f)));
       const float3 ba = slotDelta(s, ja, ia);
       const float3 bc = slotDelta(s, ja, ka);
       const float mgba = ba.x * ba.x + ba.y * ba.y + ba.z * ba.z;
@@ -534,10 +526,13 @@ __device__ __forceinline__ TileInfo tileInfo(const UnitSmem &s, int nsys_u, int 
 }
 
 // Run one tile: p.pair(jslot, jl) for every pair of the tile (once each) and p.rotate() after
-// every step; full off-diagonal tiles take a branch-free loop.
+// every step.  Padding slots hold parameters that make every contribution to a real atom exactly
+// zero (no charge, zero screened radius and dE/dR, masked Lennard-Jones, far-away coordinates),
+// so partial tiles run the same branch-free loop; only the last step of a diagonal tile, where
+// lanes l and l + 16 would meet the same pair, runs on half the lanes.
 template <class P>
 __device__ __forceinline__ void walkTile(P &p, const TileInfo &ti, int lane) {
-  if (!ti.diag && ti.ni == kTile && ti.nj == kTile) {
+  if (!ti.diag) {
 #pragma unroll 2
     for (int k = 0; k < kTile; k++) {
       const int jl = (lane + k) & 31;
@@ -546,17 +541,16 @@ __device__ __forceinline__ void walkTile(P &p, const TileInfo &ti, int lane) {
     }
   }
   else {
-    const bool ivalid = lane < ti.ni;
-    const int kbeg = ti.diag ? 1 : 0;
-    const int kend = ti.diag ? 16 : 31;
-    for (int k = kbeg; k <= kend; k++) {
+#pragma unroll 1
+    for (int k = 1; k < 16; k++) {
       const int jl = (lane + k) & 31;
-      const bool active = ivalid && (jl < ti.nj) && (!ti.diag || k < 16 || lane < 16);
-      if (active) {
-        p.pair(ti.jbase + jl, jl);
-      }
+      p.pair(ti.jbase + jl, jl);
       p.rotate(lane);
     }
+    if (lane < 16) {
+      p.pair(ti.jbase + lane + 16, lane + 16);
+    }
+    p.rotate(lane);
   }
 }
 
@@ -599,6 +593,7 @@ struct PairPass {
   float kk, inv_diel;
   bool salt;
   float4 ai, bi;
+  float inv4ri;     // 1 / (4 R_i)
   int code_i;
   unsigned mask;
   float fxi, fyi, fzi, dei, fxj, fyj, fzj, dej;
@@ -608,6 +603,7 @@ struct PairPass {
   __device__ __forceinline__ void begin(int islot, unsigned mask_in) {
     ai = s.pa[islot];
     bi = s.pb[islot];
+    inv4ri = 0.25f * s.gbv[islot].x;
     code_i = __float_as_int(s.prm[islot].y) & 0xffff;
     mask = mask_in;
     fxi = fyi = fzi = dei = 0.0f;
@@ -619,15 +615,20 @@ struct PairPass {
     const float4 bj = s.pb[jslot];
     const float3 dv = pairDelta(ai, bi, aj, bj);
     const float r2 = fmaf(dv.x, dv.x, fmaf(dv.y, dv.y, dv.z * dv.z));
-    const float qiqj = ai.w * aj.w;
+    const float qiqj_all = ai.w * aj.w;
     float fmag = 0.0f;
-    if (NB && ((mask >> jl) & 1u) == 0u) {
+    if (NB) {
+      // excluded and padding pairs take the same path with zero parameters
+      const float incl = ((mask >> jl) & 1u) ? 0.0f : 1.0f;
       // one Newton step on rsqrt keeps r^-12 within a few ulp
       float invr = rsqrtf(r2);
       invr = invr * fmaf(-0.5f * r2 * invr, invr, 1.5f);
       const float invr2 = invr * invr;
       const float invr4 = invr2 * invr2;
-      const float2 ab = s.lj[code_i + (__float_as_int(s.prm[jslot].y) >> 16)];
+      float2 ab = s.lj[code_i + (__float_as_int(s.prm[jslot].y) >> 16)];
+      ab.x *= incl;
+      ab.y *= incl;
+      const float qiqj = qiqj_all * incl;
       if (ENERGY) {
         e_elec = __fadd_rn(e_elec, __fmul_rn(qiqj, invr));
         e_vdw = __fadd_rn(e_vdw, __fmul_rn(__fsub_rn(__fmul_rn(__fmul_rn(ab.x, invr4), invr4),
@@ -638,8 +639,9 @@ struct PairPass {
       }
     }
     if (GB) {
+      const float qiqj = qiqj_all;
       const float ijb = bi.w * bj.w;
-      const float efac = __expf(__fdividef(-r2, 4.0f * ijb));
+      const float efac = __expf(-r2 * inv4ri * s.gbv[jslot].x);
       const float fgbi = rsqrtf(fmaf(ijb, efac, r2));
       float expmkf, fgbk;
       if (salt) {
@@ -932,8 +934,10 @@ kEvalFused(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
         prm.w = d.srho[gi];
       }
       else {
-        // padding slot: never paired (validity checks), kept finite
-        pa = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        // padding slot: far from everything (16 A apart along x beyond 5000 A), no charge,
+        // zero screened radius, masked from Coulomb / Lennard-Jones: every pair term it enters
+        // is exactly zero for the real atom
+        pa = make_float4(5000.0f + 16.0f * static_cast<float>(slot), 0.0f, 0.0f, 0.0f);
         pb = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
         prm = make_float4(0.0f, __int_as_float(s.ljbase[k]), 1.0f, 0.0f);
       }
@@ -1015,7 +1019,7 @@ kEvalFused(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
         }
         s.pa[slot] = pa;
         s.pb[slot] = pb;
-        s.gbv[slot].x = egbi;
+        s.gbv[slot].x = 1.0f / egbi;
         if (ENERGY) {
           warpEnergy(s, k, kGb, e_self, d.nrg_scale);
         }

@@ -187,11 +187,25 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
     topo_tile_start[t] = h_tile_mask_idx.size();
     for (int I = 0; I < nblk; I++) {
       for (int J = 0; J <= I; J++) {
+        // row l bit m: the pair (I*32 + l, J*32 + m) takes no Coulomb / Lennard-Jones term,
+        // either because it is a 1-1..1-4 exclusion or because one of the slots is padding
+        // beyond the molecule's last atom (as STORMM's tile masks mark them,
+        // Potential/static_exclusionmask.cpp:120-150)
         unsigned rows[32] = {0u};
         bool any = false;
         for (int l = 0; l < kTile; l++) {
           const int a = I * kTile + l;
-          if (a >= n) break;
+          if (a >= n) {
+            rows[l] = 0xffffffffu;
+            any = true;
+            continue;
+          }
+          for (int m = 0; m < kTile; m++) {
+            if (J * kTile + m >= n) {
+              rows[l] |= (1u << m);
+              any = true;
+            }
+          }
           for (int b : partners[a]) {
             if (b >= J * kTile && b < (J + 1) * kTile) {
               rows[l] |= (1u << (b - J * kTile));
@@ -260,7 +274,7 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
       const uint32_t j = check_atom(tp.angl_atoms[3 * a + 1]);
       const uint32_t k = check_atom(tp.angl_atoms[3 * a + 2]);
       h_angles.push_back(make_uint4(i | (j << 16), k, fbits(tp.angl_keq[a]),
-                                    fbits(tp.angl_theta0[a])));
+                                    fbits(std::cos(tp.angl_theta0[a]))));
     }
     h_angl_start[s + 1] = h_angles.size();
     for (int d = 0; d < tp.ndihe; d++) {
