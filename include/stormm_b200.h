@@ -190,6 +190,43 @@ int sb_launch_valence(sb_synthesis* syn, int eval_force, int eval_energy, void* 
 /* Number of work units the batched launches use, and the launch shape chosen */
 int sb_launch_info(const sb_synthesis* syn, int* work_units, int* blocks, int* threads);
 
+/* ------------------------------------------------------------------------------------------ */
+/* Line minimization                                                                           */
+/* ------------------------------------------------------------------------------------------ */
+/* STORMM's MinimizeControls for the GPU minimizer (Namelists/nml_minimize.h:21-30,
+ * MolecularMechanics/hpc_minimization.h:122-152) */
+typedef struct {
+  int total_cycles;            /* maxcyc: line-minimization cycles (STORMM default 200) */
+  int sd_cycles;               /* ncyc: steepest-descent cycles before conjugate gradient (50) */
+  int clash_cycles;            /* cdcyc: must be 0 (softened-core cycles are not provided) */
+  double initial_step;         /* dx0: first move length, A (0.01) */
+  double convergence_rms;      /* a system stops once its RMS force (kcal/mol/A, over 3N
+                                  components) is at or below this; 0: run every cycle, as
+                                  STORMM's GPU minimizer does */
+  int record_history;          /* nonzero: keep each system's energy at the start of every cycle
+                                  and the final energy (total_cycles + 1 values per system) */
+} sb_minimize_controls;
+
+void sb_default_minimize_controls(sb_minimize_controls* ctl);
+
+/* Minimize every system from its current coordinates: steepest descent for sd_cycles, then
+ * conjugate gradient, each cycle a force evaluation and a four-point line search with a cubic
+ * fit, as launchMinimization (hpc_minimization.h:122-152).  Coordinates move in place; on return
+ * (stream order) the energies hold each system's final energy terms.  The whole minimization is
+ * one kernel launch per molecule size class. */
+int sb_minimize(sb_synthesis* syn, const sb_minimize_controls* ctl, void* stream);
+/* Systems [first, first + count) with one launch per system: the per-system drop-in sequence */
+int sb_minimize_range(sb_synthesis* syn, int first, int count, const sb_minimize_controls* ctl,
+                      void* stream);
+/* Energy history of the last minimization that recorded one: nsys * (total_cycles + 1) doubles,
+ * system-major.  Entry c is the energy at the start of cycle c; the entry after a system's last
+ * cycle is its final energy (later entries stay 0 for a system that converged early). */
+int sb_get_minimize_history(sb_synthesis* syn, double* history, void* stream);
+/* Per system: cycles completed, whether the RMS force target was met, latest RMS force.  Any
+ * output may be NULL. */
+int sb_get_minimize_progress(sb_synthesis* syn, int* cycles_done, int* converged,
+                             double* rms_force, void* stream);
+
 /* Read and clear the device status word that bounded device-side waits and checks set */
 int sb_check_status(sb_synthesis* syn, int* status);
 

@@ -61,6 +61,9 @@ def _lib():
             ctypes.c_int]
         _LIB.orc_minimize.argtypes = [ctypes.POINTER(_System), ctypes.c_void_p, ctypes.c_int,
                                       ctypes.c_int, ctypes.c_double, ctypes.c_void_p]
+        _LIB.orc_minimize_ex.argtypes = [ctypes.POINTER(_System), ctypes.c_void_p, ctypes.c_int,
+                                         ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
         _LIB.orc_float_to_int63.argtypes = [ctypes.c_float, ctypes.POINTER(ctypes.c_int32),
                                             ctypes.POINTER(ctypes.c_int32)]
         _LIB.orc_double_to_int95.argtypes = [ctypes.c_double, ctypes.POINTER(ctypes.c_int64),
@@ -105,12 +108,15 @@ class OracleSystem:
         return {"energies": e, "forces": None if f is None else f.reshape(-1, 3), "psi": psi,
                 "radii": rad, "sumdeijda": sde}
 
-    def minimize(self, coords, maxcyc, sd_cycles, dx0=0.01):
+    def minimize(self, coords, maxcyc, sd_cycles, dx0=0.01, drms=0.0, with_cycles=False):
         lib = _lib()
         c = np.ascontiguousarray(np.asarray(coords, dtype=np.float64).reshape(-1)).copy()
         hist = np.zeros(maxcyc + 1)
-        lib.orc_minimize(ctypes.byref(self.struct), c.ctypes.data, maxcyc, sd_cycles, dx0,
-                         hist.ctypes.data)
+        ran = ctypes.c_int(0)
+        lib.orc_minimize_ex(ctypes.byref(self.struct), c.ctypes.data, maxcyc, sd_cycles, dx0,
+                            drms, hist.ctypes.data, ctypes.byref(ran))
+        if with_cycles:
+            return c.reshape(-1, 3), hist, ran.value
         return c.reshape(-1, 3), hist
 
 

@@ -497,6 +497,11 @@ static void cubic_fit(const double* x, const double* e, double* abcd) {
 
 void orc_minimize(const orc_system* s, double* coords, int maxcyc, int sd_cycles, double dx0,
                   double* history) {
+  orc_minimize_ex(s, coords, maxcyc, sd_cycles, dx0, 0.0, history, NULL);
+}
+
+void orc_minimize_ex(const orc_system* s, double* coords, int maxcyc, int sd_cycles, double dx0,
+                     double drms, double* history, int* cycles_run) {
   const int n = s->natom;
   const size_t nb = (size_t)n * 3 * sizeof(double);
   double* frc = (double*)malloc(nb);
@@ -505,11 +510,20 @@ void orc_minimize(const orc_system* s, double* coords, int maxcyc, int sd_cycles
   double* dir = (double*)malloc(nb);
   double e[ORC_NTERMS];
   double l_move = dx0;
+  int done_at = maxcyc;
   for (int cyc = 0; cyc < maxcyc; cyc++) {
     /* force + energy evaluation at the start of the cycle */
     orc_evaluate(s, coords, frc, e, NULL, NULL, NULL, 7);
     const double e0 = total_energy(e);
     if (history) history[cyc] = e0;
+    if (drms > 0.0) {
+      double ff = 0.0;
+      for (int k = 0; k < 3 * n; k++) ff += frc[k] * frc[k];
+      if (sqrt(ff / (3.0 * n)) <= drms) {
+        done_at = cyc;
+        break;
+      }
+    }
 
     /* conjugate gradient direction, Math/conjugate_gradient.cui:8-140 and
      * hpc_reduction.cu:154-300; the step counter has been advanced once before this call
@@ -619,7 +633,8 @@ void orc_minimize(const orc_system* s, double* coords, int maxcyc, int sd_cycles
     }
   }
   orc_evaluate(s, coords, NULL, e, NULL, NULL, NULL, 7);
-  if (history) history[maxcyc] = total_energy(e);
+  if (history) history[done_at] = total_energy(e);
+  if (cycles_run) *cycles_run = done_at;
   free(frc);
   free(prv);
   free(cgt);

@@ -52,6 +52,14 @@ class Options(ctypes.Structure):
     ]
 
 
+class MinimizeControls(ctypes.Structure):
+    _fields_ = [
+        ("total_cycles", ctypes.c_int), ("sd_cycles", ctypes.c_int),
+        ("clash_cycles", ctypes.c_int), ("initial_step", ctypes.c_double),
+        ("convergence_rms", ctypes.c_double), ("record_history", ctypes.c_int),
+    ]
+
+
 class StormmB200Error(RuntimeError):
     pass
 
@@ -95,6 +103,12 @@ def library() -> ctypes.CDLL:
                                               ctypes.POINTER(ctypes.c_int),
                                               ctypes.POINTER(ctypes.c_int)]),
             "sb_check_status": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int)]),
+            "sb_default_minimize_controls": (None, [ctypes.POINTER(MinimizeControls)]),
+            "sb_minimize": (ctypes.c_int, [vp, ctypes.POINTER(MinimizeControls), vp]),
+            "sb_minimize_range": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.POINTER(MinimizeControls), vp]),
+            "sb_get_minimize_history": (ctypes.c_int, [vp, vp, vp]),
+            "sb_get_minimize_progress": (ctypes.c_int, [vp, vp, vp, vp, vp]),
             "sb_last_error": (ctypes.c_char_p, []),
             "sb_version": (ctypes.c_char_p, []),
         }
@@ -181,6 +195,16 @@ class _TopologyArrays:
         impr = getattr(mol, "dihe_improper", None)
         t.dihe_improper = ptr(impr, np.int32) if impr is not None else None
         self.struct = t
+
+
+def minimize_controls(**overrides) -> MinimizeControls:
+    """STORMM's minimizer defaults (maxcyc 200, ncyc 50, dx0 0.01, no clash damping) with
+    overrides by field name."""
+    c = MinimizeControls()
+    library().sb_default_minimize_controls(ctypes.byref(c))
+    for k, v in overrides.items():
+        setattr(c, k, v)
+    return c
 
 
 class Synthesis:
@@ -289,6 +313,40 @@ class Synthesis:
     def launch_valence(self, force=True, energy=True, stream=None):
         _check(library().sb_launch_valence(self.handle, int(force), int(energy), stream),
                "sb_launch_valence")
+
+    # minimization ------------------------------------------------------------------------
+    def minimize(self, stream=None, **controls):
+        """Line-minimize every system in place (fields of MinimizeControls as keywords)."""
+        c = minimize_controls(**controls)
+        self._history_stride = c.total_cycles + 1 if c.record_history else 0
+        _check(library().sb_minimize(self.handle, ctypes.byref(c), stream), "sb_minimize")
+
+    def minimize_range(self, first, count, stream=None, **controls):
+        """The same with one launch per system, systems [first, first + count)."""
+        c = minimize_controls(**controls)
+        self._history_stride = c.total_cycles + 1 if c.record_history else 0
+        _check(library().sb_minimize_range(self.handle, first, count, ctypes.byref(c), stream),
+               "sb_minimize_range")
+
+    def minimize_history(self, stream=None):
+        """(nsys, total_cycles + 1) energies of the last minimization run with history."""
+        stride = getattr(self, "_history_stride", 0)
+        if stride == 0:
+            raise StormmB200Error("the last minimization kept no history")
+        out = np.zeros(self.nsys * stride)
+        _check(library().sb_get_minimize_history(self.handle, out.ctypes.data, stream),
+               "sb_get_minimize_history")
+        return out.reshape(self.nsys, stride)
+
+    def minimize_progress(self, stream=None):
+        """(cycles completed, converged flags, latest RMS force) per system."""
+        cyc = np.zeros(self.nsys, dtype=np.int32)
+        conv = np.zeros(self.nsys, dtype=np.int32)
+        rms = np.zeros(self.nsys)
+        _check(library().sb_get_minimize_progress(self.handle, cyc.ctypes.data, conv.ctypes.data,
+                                                  rms.ctypes.data, stream),
+               "sb_get_minimize_progress")
+        return cyc, conv.astype(bool), rms
 
     def launch_info(self):
         u, b, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

@@ -107,6 +107,30 @@ struct DevSynthesis {
   int* status;                   // device status word (0 = fine)
 };
 
+// Line-minimization state (MolecularMechanics/line_minimization.h:15-221 and the conjugate
+// gradient substrate, Math/hpc_reduction.h:55-63), per system and per padded atom.  It persists
+// between launches, so a minimization can run in several launches of a few cycles each.
+struct DevMinimizer {
+  long long* xcrd;               // the synthesis' coordinates, moved in place
+  long long* ycrd;
+  long long* zcrd;
+  long long* xprv;               // force of the previous cycle, fixed point with frc_bits
+  long long* yprv;
+  long long* zprv;
+  float* xcg;                    // conjugate-gradient direction (kcal/mol/A, not normalized)
+  float* ycg;
+  float* zcg;
+  double* l_move;                // per system: baseline move length (A)
+  int* cycle;                    // per system: completed line-minimization cycles
+  int* done;                     // per system: nonzero once the RMS force met the target
+  double* rms_force;             // per system: RMS force at the start of the latest cycle
+  double* history;               // per system: energy at the start of each cycle (may be null)
+  int hist_stride;               // history entries per system
+  int sd_cycles;                 // steepest-descent cycles before conjugate gradient
+  double drms;                   // RMS force target (kcal/mol/A), 0: none
+  int* queue;                    // work-unit counter, zero before each launch
+};
+
 }  // namespace sb
 
 #endif

@@ -27,1068 +27,46 @@
 // feed the pair passes with two 16-byte loads per partner; w1 / w2 carry what the pass needs
 // (pass 1 and 3: s*rho and rho; pass 2: charge and effective radius).  prm holds the static
 // per-atom values, gbv the reciprocal effective radius and the chain-rule dE/dR.
-#include <cuda_runtime.h>
-
-#include "device_kits.h"
-#include "fixed_point.cuh"
+#include "unit_eval.cuh"
 
 namespace sb {
 
-namespace {
-
-// Constants/generalized_born.h:21-44 (Taylor series of the HCT integral at long range)
-constexpr float kTaylorA = 0.33333333333333333333f;
-constexpr float kTaylorB = 0.4f;
-constexpr float kTaylorC = 0.42857142857142857143f;
-constexpr float kTaylorD = 0.44444444444444444444f;
-constexpr float kTaylorDD = 0.45454545454545454545f;
-constexpr float kTaylorE = 1.33333333333333333333f;
-constexpr float kTaylorF = 2.4f;
-constexpr float kTaylorG = 3.42857142857142857143f;
-constexpr float kTaylorH = 4.44444444444444444444f;
-constexpr float kTaylorHH = 5.45454545454545454545f;
-
-constexpr unsigned kFullMask = 0xffffffffu;
-
-// HCT descreening of an atom of offset radius rho by a neighbour of screened radius sj at
-// distance r (invr = 1/r); returns the amount psi decreases by.
-//
-// Beyond r = 4 sj the reference's Taylor series applies (nonbonded_potential.tpp:590-596).
-// Closer in, the three closed forms the reference selects by overlap case (no overlap, partial
-// overlap, atom inside the neighbour's sphere: nonbonded_potential.tpp:597-628) are one
-// expression in U = r + sj and L = max(rho, |r - sj|):
-//   I = 1/2 [1/L - 1/U + (sj^2 - r^2)/(4r) (1/L^2 - 1/U^2) + ln(L/U) / (2r)]
-//       + (1/rho - 1/L) when rho < sj - r,
-// and I = 0 when rho >= U.  One formula instead of four keeps a warp on at most two paths.
-__device__ __forceinline__ float hctIntegral(float r, float r2, float invr, float rho, float sj) {
-  if (r > 4.0f * sj) {
-    const float sj2 = sj * sj;
-    const float invr2 = invr * invr;
-    const float t = sj2 * invr2;
-    const float dumbo = kTaylorA + t * (kTaylorB + t * (kTaylorC + t * (kTaylorD + t * kTaylorDD)));
-    return sj * t * invr2 * dumbo;
-  }
-  const float u = r + sj;
-  const float l = fmaxf(rho, fabsf(r - sj));
-  const float inv_lu = __fdividef(1.0f, l * u);
-  const float il = u * inv_lu;
-  const float iu = l * inv_lu;
-  const float dlu = il - iu;
-  float v = dlu + 0.25f * (sj * sj - r2) * invr * dlu * (il + iu) + 0.5f * invr * __logf(l * iu);
-  if (rho < sj - r) {
-    // the atom sits inside the neighbour's sphere: rare, so a branch beats a reciprocal per pair
-    v += 2.0f * (__fdividef(1.0f, rho) - il);
-  }
-  return (rho < u) ? 0.5f * v : 0.0f;
-}
-
-// Radial derivative of hctIntegral, -(1/r) dI/dr, the factor the reference multiplies by the
-// chain-rule dE/dR (nonbonded_potential.tpp:1116-1165), from the same unified expression
-// (lambda = dL/dr: 1 without overlap, 0 on partial overlap, -1 inside the neighbour).
-__device__ __forceinline__ float hctDerivative(float r, float r2, float invr, float rho,
-                                               float sj) {
-  const float invr2 = invr * invr;
-  if (r > 4.0f * sj) {
-    const float t = sj * sj * invr2;
-    const float dumbo = kTaylorE + t * (kTaylorF + t * (kTaylorG + t * (kTaylorH + t * kTaylorHH)));
-    return t * sj * invr2 * invr2 * dumbo;
-  }
-  const float u = r + sj;
-  const float rms = r - sj;
-  const float l = fmaxf(rho, fabsf(rms));
-  const float lam = (rms >= rho) ? 1.0f : ((-rms > rho) ? -1.0f : 0.0f);
-  const float inv_lu = __fdividef(1.0f, l * u);
-  const float il = u * inv_lu;
-  const float iu = l * inv_lu;
-  const float il2 = il * il;
-  const float iu2 = iu * iu;
-  const float q = 0.25f * (sj * sj - r2) * invr;
-  const float dq = -0.25f * fmaf(sj * sj, invr2, 1.0f);
-  float di = -lam * il2 + iu2 + dq * (il2 - iu2) + 2.0f * q * (iu2 * iu - lam * il2 * il) +
-             0.5f * invr * (lam * il - iu - invr * __logf(l * iu));
-  di = 0.5f * di - ((-rms > rho) ? il2 : 0.0f);
-  return (rho < u) ? -di * invr : 0.0f;
-}
-
-// Shared-memory layout of one work unit
-struct UnitSmem {
-  float4* pa;       // x_hi, y_hi, z_hi, pass payload w1
-  float4* pb;       // x_lo, y_lo, z_lo, pass payload w2
-  float4* prm;      // charge * sqrt(k_Coulomb), Lennard-Jones code (int bits), rho, s * rho
-  float2* gbv;      // 1 / effective radius, dE/dR after the chain rule
-  int* fx;          // int63 force accumulators: primary
-  int* fy;
-  int* fz;
-  int* fxo;         // overflow
-  int* fyo;
-  int* fzo;
-  int* psi;         // int63 psi accumulator, 2^kPsiBits
-  int* psio;
-  int* de;          // int63 dE/dR accumulator, 2^kDeijdaBits
-  int* deo;
-  float2* lj;       // Lennard-Jones tables of the unit's molecules (standard, then 1-4)
-  unsigned long long* nrg;   // per unit molecule energies
-  int* sys;         // molecule index
-  int* slot0;       // first slot of the molecule
-  int* natom;
-  int* ljbase;
-  int* tile0;       // prefix sums (kMaxUnitSystems + 1 entries each)
-  int* bchunk0;     // valence work in chunks of 32 terms that never straddle two molecules
-  int* achunk0;
-  int* dchunk0;
-};
-
-__host__ __device__ inline size_t alignUp(size_t x, size_t a) { return (x + a - 1) / a * a; }
-
-constexpr int kSlotBytes = 3 * 16 + 8 + 10 * 4;
-
-}  // namespace
-
 // Dynamic shared memory needed for a work unit of max_slots atom slots and max_lj table entries
-size_t fusedSmemBytes(int max_slots, int max_lj) {
-  size_t b = static_cast<size_t>(kSlotBytes) * max_slots;
-  b = alignUp(b, 16);
-  b += sizeof(float2) * max_lj;
-  b = alignUp(b, 16);
-  b += sizeof(unsigned long long) * kMaxUnitSystems * kNrgStride;
-  b += sizeof(int) * (4 * kMaxUnitSystems + 4 * (kMaxUnitSystems + 1));
-  return b;
-}
-
-namespace {
-
-__device__ UnitSmem carveSmem(char* base, int max_slots, int max_lj) {
-  UnitSmem s;
-  size_t off = 0;
-  s.pa = reinterpret_cast<float4*>(base + off); off += sizeof(float4) * max_slots;
-  s.pb = reinterpret_cast<float4*>(base + off); off += sizeof(float4) * max_slots;
-  s.prm = reinterpret_cast<float4*>(base + off); off += sizeof(float4) * max_slots;
-  s.gbv = reinterpret_cast<float2*>(base + off); off += sizeof(float2) * max_slots;
-  int* ip = reinterpret_cast<int*>(base + off);
-  s.fx = ip; ip += max_slots;
-  s.fy = ip; ip += max_slots;
-  s.fz = ip; ip += max_slots;
-  s.fxo = ip; ip += max_slots;
-  s.fyo = ip; ip += max_slots;
-  s.fzo = ip; ip += max_slots;
-  s.psi = ip; ip += max_slots;
-  s.psio = ip; ip += max_slots;
-  s.de = ip; ip += max_slots;
-  s.deo = ip; ip += max_slots;
-  off = alignUp(off + 10 * sizeof(int) * max_slots, 16);
-  s.lj = reinterpret_cast<float2*>(base + off); off += sizeof(float2) * max_lj;
-  off = alignUp(off, 16);
-  s.nrg = reinterpret_cast<unsigned long long*>(base + off);
-  off += sizeof(unsigned long long) * kMaxUnitSystems * kNrgStride;
-  int* q = reinterpret_cast<int*>(base + off);
-  s.sys = q; q += kMaxUnitSystems;
-  s.slot0 = q; q += kMaxUnitSystems;
-  s.natom = q; q += kMaxUnitSystems;
-  s.ljbase = q; q += kMaxUnitSystems;
-  s.tile0 = q; q += kMaxUnitSystems + 1;
-  s.bchunk0 = q; q += kMaxUnitSystems + 1;
-  s.achunk0 = q; q += kMaxUnitSystems + 1;
-  s.dchunk0 = q; q += kMaxUnitSystems + 1;
-  return s;
-}
-
-// Index of the unit molecule that owns position pos of a prefix-sum array of n + 1 entries
-__device__ __forceinline__ int findOwner(const int* prefix, int n, int pos) {
-  int k = 0;
-  while (k + 1 < n && prefix[k + 1] <= pos) {
-    k++;
-  }
-  return k;
-}
-
-// Tile (I, J), I >= J, of the lower triangle from its index within the molecule
-__device__ __forceinline__ void tileCoordinates(int local, int* ti, int* tj) {
-  int i = static_cast<int>((sqrtf(8.0f * local + 1.0f) - 1.0f) * 0.5f);
-  while (i * (i + 1) / 2 > local) i--;
-  while ((i + 1) * (i + 2) / 2 <= local) i++;
-  *ti = i;
-  *tj = local - i * (i + 1) / 2;
-}
-
-__device__ __forceinline__ float3 pairDelta(const float4 a_i, const float4 b_i, const float4 a_j,
-                                            const float4 b_j) {
-  return make_float3((a_j.x - a_i.x) + (b_j.x - b_i.x), (a_j.y - a_i.y) + (b_j.y - b_i.y),
-                     (a_j.z - a_i.z) + (b_j.z - b_i.z));
-}
-
-__device__ __forceinline__ void addForce(const UnitSmem &s, int slot, float fx, float fy, float fz,
-                                         float scale) {
-  atomicAddInt63(fx * scale, &s.fx[slot], &s.fxo[slot]);
-  atomicAddInt63(fy * scale, &s.fy[slot], &s.fyo[slot]);
-  atomicAddInt63(fz * scale, &s.fz[slot], &s.fzo[slot]);
-}
-
-// Warp-wide int64 sum, result in every lane
-__device__ __forceinline__ long long warpSum(long long v) {
-  for (int o = 16; o > 0; o >>= 1) {
-    v += __shfl_xor_sync(kFullMask, v, o);
-  }
-  return v;
-}
-
-// Warp-reduce one scaled energy per lane (all lanes in one molecule) into its slot
-__device__ __forceinline__ void warpEnergy(const UnitSmem &s, int k, int slot, float e,
-                                           float scale) {
-  const long long v = warpSum(__float2ll_rn(e * scale));
-  if ((threadIdx.x & 31) == 0 && v != 0) {
-    atomicAdd(&s.nrg[k * kNrgStride + slot], static_cast<unsigned long long>(v));
-  }
-}
-
-// Coordinate difference b - a from the hi / lo representation of two slots
-__device__ __forceinline__ float3 slotDelta(const UnitSmem &s, int a, int b) {
-  return pairDelta(s.pa[a], s.pb[a], s.pa[b], s.pb[b]);
-}
+size_t fusedSmemBytes(int max_slots, int max_lj) { return unitSmemBytes(max_slots, max_lj); }
 
 // ------------------------------------------------------------------------------------------------
-// Valence terms (Potential/valence_potential.tpp).  Warps take chunks of 32 terms of one molecule,
-// so each chunk's energies reduce across the warp into a single shared-memory update.
-// ------------------------------------------------------------------------------------------------
-template <bool FORCE, bool ENERGY>
-__device__ void valenceTerms(const DevSynthesis &d, const UnitSmem &s, int nsys_u) {
-  const float fs = d.frc_scale;
-  const float es = d.nrg_scale;
-  const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const int nwarp = blockDim.x >> 5;
-
-  // bonds, valence_potential.tpp:9-97; the equilibrium length is a float pair so that r - r0
-  // loses nothing to the rounding of r0, and the bond length itself is an unevaluated pair
-  for (int c = warp; c < s.bchunk0[nsys_u]; c += nwarp) {
-    const int k = findOwner(s.bchunk0, nsys_u, c);
-    const int sysid = s.sys[k];
-    const int t = (c - s.bchunk0[k]) * 32 + lane;
-    const int nterm = d.bond_start[sysid + 1] - d.bond_start[sysid];
-    float e = 0.0f;
-    if (t < nterm) {
-      const uint4 rec = d.bonds[d.bond_start[sysid] + t];
-      const int ia = s.slot0[k] + static_cast<int>(rec.x & 0xffffu);
-      const int ja = s.slot0[k] + static_cast<int>(rec.x >> 16);
-      const float keq = __uint_as_float(rec.y);
-      const float leq_hi = __uint_as_float(rec.z);
-      const float leq_lo = __uint_as_float(rec.w);
-      const float4 ai = s.pa[ia], aj = s.pa[ja], bi = s.pb[ia], bj = s.pb[ja];
-      const float av[3] = {aj.x, aj.y, aj.z};
-      const float bv[3] = {ai.x, ai.y, ai.z};
-      const float lav[3] = {bj.x, bj.y, bj.z};
-      const float lbv[3] = {bi.x, bi.y, bi.z};
-      float dh[3], dlo[3];
-#pragma unroll
-      for (int q = 0; q < 3; q++) {
-        const float sdiff = av[q] - bv[q];
-        const float bb = sdiff - av[q];
-        const float err = (av[q] - (sdiff - bb)) + (-bv[q] - bb);
-        const float lo = err + (lav[q] - lbv[q]);
-        dh[q] = sdiff + lo;
-        dlo[q] = lo - (dh[q] - sdiff);
-      }
-      float r2h = dh[0] * dh[0];
-      float r2l = fmaf(dh[0], dh[0], -r2h) + 2.0f * dh[0] * dlo[0];
-#pragma unroll
-      for (int q = 1; q < 3; q++) {
-        const float p = dh[q] * dh[q];
-        const float pe = fmaf(dh[q], dh[q], -p) + 2.0f * dh[q] * dlo[q];
-        const float sum = r2h + p;
-        const float bvv = sum - r2h;
-        r2l += ((r2h - (sum - bvv)) + (p - bvv)) + pe;
-        r2h = sum;
-      }
-      const float r = sqrtf(r2h);
-      const float r_lo = (fmaf(-r, r, r2h) + r2l) / (2.0f * r);
-      const float dl = ((r - leq_hi) + r_lo) - leq_lo;
-      if (FORCE) {
-        const float fmag = 2.0f * keq * dl / r;
-        addForce(s, ia, fmag * dh[0], fmag * dh[1], fmag * dh[2], fs);
-        addForce(s, ja, -fmag * dh[0], -fmag * dh[1], -fmag * dh[2], fs);
-      }
-      e = __fmul_rn(__fmul_rn(keq, dl), dl);
-    }
-    if (ENERGY) {
-      warpEnergy(s, k, kBond, e, es);
-    }
-  }
-
-  // angles, valence_potential.tpp:170-288.  theta - theta0 comes from rotating (cos, sin) of
-  // theta, taken from the dot and cross products, by theta0: well conditioned everywhere.
-  for (int c = warp; c < s.achunk0[nsys_u]; c += nwarp) {
-    const int k = findOwner(s.achunk0, nsys_u, c);
-    const int sysid = s.sys[k];
-    const int t = (c - s.achunk0[k]) * 32 + lane;
-    const int nterm = d.angl_start[sysid + 1] - d.angl_start[sysid];
-    float e = 0.0f;
-    if (t < nterm) {
-      const uint4 rec = d.angles[d.angl_start[sysid] + t];
-      const int ia = s.slot0[k] + static_cast<int>(rec.x & 0xffffu);
-      const int ja = s.slot0[k] + static_cast<int>(rec.x >> 16);
-      const int ka = s.slot0[k] + static_cast<int>(rec.y);
-      const float keq = __uint_as_float(rec.z);
-      const float cth0 = __uint_as_float(rec.w);
-      const float sth0 = sqrtf(fmaxf(0.0f, fmaf(-cth0, cth0, 1.0f)));
-      const float3 ba = slotDelta(s, ja, ia);
-      const float3 bc = slotDelta(s, ja, ka);
-      const float mgba = ba.x * ba.x + ba.y * ba.y + ba.z * ba.z;
-      const float mgbc = bc.x * bc.x + bc.y * bc.y + bc.z * bc.z;
-      const float invbabc = rsqrtf(mgba * mgbc);
-      const float dotp = ba.x * bc.x + ba.y * bc.y + ba.z * bc.z;
-      const float cx = ba.y * bc.z - ba.z * bc.y;
-      const float cy = ba.z * bc.x - ba.x * bc.z;
-      const float cz = ba.x * bc.y - ba.y * bc.x;
-      const float crs = sqrtf(cx * cx + cy * cy + cz * cz);
-      const float sth = crs * invbabc;
-      const float cth = dotp * invbabc;
-      const float dtheta = atan2f(fmaf(sth, cth0, -cth * sth0), fmaf(cth, cth0, sth * sth0));
-      if (FORCE) {
-        const float dA = -2.0f * keq * dtheta / sth;
-        const float sqba = dA / mgba;
-        const float sqbc = dA / mgbc;
-        const float mbabc = dA * invbabc;
-        const float adx = bc.x * mbabc - cth * ba.x * sqba;
-        const float ady = bc.y * mbabc - cth * ba.y * sqba;
-        const float adz = bc.z * mbabc - cth * ba.z * sqba;
-        const float cdx = ba.x * mbabc - cth * bc.x * sqbc;
-        const float cdy = ba.y * mbabc - cth * bc.y * sqbc;
-        const float cdz = ba.z * mbabc - cth * bc.z * sqbc;
-        addForce(s, ia, -adx, -ady, -adz, fs);
-        addForce(s, ja, adx + cdx, ady + cdy, adz + cdz, fs);
-        addForce(s, ka, -cdx, -cdy, -cdz, fs);
-      }
-      e = __fmul_rn(__fmul_rn(keq, dtheta), dtheta);
-    }
-    if (ENERGY) {
-      warpEnergy(s, k, kAngle, e, es);
-    }
-  }
-
-  // dihedrals with attached 1-4 pairs, valence_potential.tpp:359-578, 1288-1420.  The signed
-  // angle is carried as (cos, sin) from x = (ab x bc) . (bc x cd) and y = |bc| ab . (bc x cd),
-  // the angle STORMM's acos / arcsine route gives (Math/rounding.tpp:25-80) without its ill
-  // conditioning near 0 and pi; cos(n theta - phase) and sin(n theta - phase) follow from the
-  // multiple-angle recurrence for integer periodicities.
-  for (int c = warp; c < s.dchunk0[nsys_u]; c += nwarp) {
-    const int k = findOwner(s.dchunk0, nsys_u, c);
-    const int sysid = s.sys[k];
-    const int t = (c - s.dchunk0[k]) * 32 + lane;
-    const int nterm = d.dihe_start[sysid + 1] - d.dihe_start[sysid];
-    float e_prop = 0.0f, e_impr = 0.0f, e_el14 = 0.0f, e_lj14 = 0.0f;
-    if (t < nterm) {
-      const int pos = d.dihe_start[sysid] + t;
-      const uint4 ra = d.dihe_a[pos];
-      const uint4 rb = d.dihe_b[pos];
-      const int ia = s.slot0[k] + static_cast<int>(ra.x & 0xffffu);
-      const int ja = s.slot0[k] + static_cast<int>(ra.x >> 16);
-      const int ka = s.slot0[k] + static_cast<int>(ra.y & 0xffffu);
-      const int la = s.slot0[k] + static_cast<int>((ra.y >> 16) & 0x7fffu);
-      const bool improper = (ra.y & 0x80000000u) != 0u;
-      const float amp = __uint_as_float(ra.z);
-      const float freq = __uint_as_float(ra.w);
-      const float cphase = __uint_as_float(rb.x);
-      const float sphase = __uint_as_float(rb.y);
-      const float3 ab = slotDelta(s, ia, ja);
-      const float3 bc = slotDelta(s, ja, ka);
-      const float3 cd = slotDelta(s, ka, la);
-      float3 crabbc = make_float3(ab.y * bc.z - ab.z * bc.y, ab.z * bc.x - ab.x * bc.z,
-                                  ab.x * bc.y - ab.y * bc.x);
-      float3 crbccd = make_float3(bc.y * cd.z - bc.z * cd.y, bc.z * cd.x - bc.x * cd.z,
-                                  bc.x * cd.y - bc.y * cd.x);
-      const float mgbc = sqrtf(bc.x * bc.x + bc.y * bc.y + bc.z * bc.z);
-      const float xx = crabbc.x * crbccd.x + crabbc.y * crbccd.y + crabbc.z * crbccd.z;
-      const float yy = mgbc * (ab.x * crbccd.x + ab.y * crbccd.y + ab.z * crbccd.z);
-      const float inv_rr = rsqrtf(fmaf(xx, xx, yy * yy));
-      const float c1 = xx * inv_rr;
-      const float s1 = yy * inv_rr;
-      float cn, sn;
-      const int nint = static_cast<int>(freq);
-      if (static_cast<float>(nint) == freq && nint >= 1 && nint <= 6) {
-        cn = c1;
-        sn = s1;
-        for (int m = 1; m < nint; m++) {
-          const float cnew = cn * c1 - sn * s1;
-          sn = sn * c1 + cn * s1;
-          cn = cnew;
-        }
-      }
-      else {
-        sincosf(freq * atan2f(yy, xx), &sn, &cn);
-      }
-      const float cos_sangle = cn * cphase + sn * sphase;
-      const float sin_sangle = sn * cphase - cn * sphase;
-      if (FORCE) {
-        const float fr = amp * freq * sin_sangle;
-        const float mgab = sqrtf(ab.x * ab.x + ab.y * ab.y + ab.z * ab.z);
-        const float mgcd = sqrtf(cd.x * cd.x + cd.y * cd.y + cd.z * cd.z);
-        const float invab = 1.0f / mgab;
-        const float invbc = 1.0f / mgbc;
-        const float invcd = 1.0f / mgcd;
-        const float cosb = -(ab.x * bc.x + ab.y * bc.y + ab.z * bc.z) * invab * invbc;
-        const float cosc = -(bc.x * cd.x + bc.y * cd.y + bc.z * cd.z) * invbc * invcd;
-        const float isinb2 = (cosb * cosb < 0.99999904632568359375f) ? fr / (1.0f - cosb * cosb) :
-                                                                        fr * 1048576.0f;
-        const float isinc2 = (cosc * cosc < 0.99999904632568359375f) ? fr / (1.0f - cosc * cosc) :
-                                                                        fr * 1048576.0f;
-        const float invabc = invab * invbc;
-        const float invbcd = invbc * invcd;
-        crabbc.x *= invabc;
-        crabbc.y *= invabc;
-        crabbc.z *= invabc;
-        crbccd.x *= invbcd;
-        crbccd.y *= invbcd;
-        crbccd.z *= invbcd;
-        const float fa = -invab * isinb2;
-        const float fb1 = (mgbc - mgab * cosb) * invabc * isinb2;
-        const float fb2 = cosc * invbc * isinc2;
-        const float fd = -invcd * isinc2;
-        const float fix = crabbc.x * fa, fiy = crabbc.y * fa, fiz = crabbc.z * fa;
-        const float fjx = fb1 * crabbc.x - fb2 * crbccd.x;
-        const float fjy = fb1 * crabbc.y - fb2 * crbccd.y;
-        const float fjz = fb1 * crabbc.z - fb2 * crbccd.z;
-        const float flx = -fd * crbccd.x, fly = -fd * crbccd.y, flz = -fd * crbccd.z;
-        addForce(s, ia, fix, fiy, fiz, fs);
-        addForce(s, ja, fjx, fjy, fjz, fs);
-        addForce(s, ka, -(fix + fjx + flx), -(fiy + fjy + fly), -(fiz + fjz + flz), fs);
-        addForce(s, la, flx, fly, flz, fs);
-      }
-      const float edih = __fmul_rn(amp, __fadd_rn(1.0f, cos_sangle));
-      if (improper) {
-        e_impr = edih;
-      }
-      else {
-        e_prop = edih;
-      }
-      // attached 1-4 pair between atoms i and l
-      const float inv_scee = __uint_as_float(rb.z);
-      if (inv_scee > 0.0f) {
-        const float inv_scnb = __uint_as_float(rb.w);
-        const float3 dv = slotDelta(s, ia, la);
-        const float4 pi = s.prm[ia];
-        const float4 pl = s.prm[la];
-        const int code_i = __float_as_int(pi.y);
-        const int code_l = __float_as_int(pl.y);
-        // the molecule's 1-4 table follows its standard table in shared memory
-        const int nt = d.lj_ntypes[sysid];
-        const float2 ab14 = s.lj[(code_i & 0xffff) + (code_l >> 16) + nt * nt];
-        const float lja = ab14.x * inv_scnb;
-        const float ljb = ab14.y * inv_scnb;
-        const float qiqj = pi.x * pl.x * inv_scee;
-        const float invr2 = 1.0f / (dv.x * dv.x + dv.y * dv.y + dv.z * dv.z);
-        const float invr = sqrtf(invr2);
-        const float invr4 = invr2 * invr2;
-        if (FORCE) {
-          const float fmag = -(qiqj * invr * invr2) +
-                             (6.0f * ljb - 12.0f * lja * invr4 * invr2) * invr4 * invr4;
-          addForce(s, ia, fmag * dv.x, fmag * dv.y, fmag * dv.z, fs);
-          addForce(s, la, -fmag * dv.x, -fmag * dv.y, -fmag * dv.z, fs);
-        }
-        e_el14 = __fmul_rn(qiqj, invr);
-        e_lj14 = __fsub_rn(__fmul_rn(__fmul_rn(__fmul_rn(lja, invr4), invr4), invr4),
-                           __fmul_rn(__fmul_rn(ljb, invr4), invr2));
-      }
-    }
-    if (ENERGY) {
-      warpEnergy(s, k, kProperDihedral, e_prop, es);
-      warpEnergy(s, k, kImproperDihedral, e_impr, es);
-      warpEnergy(s, k, kElec14, e_el14, es);
-      warpEnergy(s, k, kVdw14, e_lj14, es);
-    }
-  }
-}
-
-// ------------------------------------------------------------------------------------------------
-// Tile walks
-// ------------------------------------------------------------------------------------------------
-struct TileInfo {
-  int k;        // unit molecule
-  int ibase;    // first slot of block I
-  int jbase;    // first slot of block J
-  int ni;       // valid atoms in block I
-  int nj;       // valid atoms in block J
-  bool diag;
-  int local;    // tile index within the molecule
-};
-
-__device__ __forceinline__ TileInfo tileInfo(const UnitSmem &s, int nsys_u, int t) {
-  TileInfo ti;
-  ti.k = findOwner(s.tile0, nsys_u, t);
-  ti.local = t - s.tile0[ti.k];
-  int I, J;
-  tileCoordinates(ti.local, &I, &J);
-  const int n = s.natom[ti.k];
-  ti.ibase = s.slot0[ti.k] + I * kTile;
-  ti.jbase = s.slot0[ti.k] + J * kTile;
-  ti.ni = min(kTile, n - I * kTile);
-  ti.nj = min(kTile, n - J * kTile);
-  ti.diag = (I == J);
-  return ti;
-}
-
-// Run one tile: p.pair(jslot, jl) for every pair of the tile (once each) and p.rotate() after
-// every step.  Padding slots hold parameters that make every contribution to a real atom exactly
-// zero (no charge, zero screened radius and dE/dR, masked Lennard-Jones, far-away coordinates),
-// so partial tiles run the same branch-free loop; only the last step of a diagonal tile, where
-// lanes l and l + 16 would meet the same pair, runs on half the lanes.
-template <class P>
-__device__ __forceinline__ void walkTile(P &p, const TileInfo &ti, int lane) {
-  if (!ti.diag) {
-#pragma unroll 2
-    for (int k = 0; k < kTile; k++) {
-      const int jl = (lane + k) & 31;
-      p.pair(ti.jbase + jl, jl);
-      p.rotate(lane);
-    }
-  }
-  else {
-#pragma unroll 1
-    for (int k = 1; k < 16; k++) {
-      const int jl = (lane + k) & 31;
-      p.pair(ti.jbase + jl, jl);
-      p.rotate(lane);
-    }
-    if (lane < 16) {
-      p.pair(ti.jbase + lane + 16, lane + 16);
-    }
-    p.rotate(lane);
-  }
-}
-
-// Lane that holds block J's atom jl's traveling accumulator once the walk is over
-__device__ __forceinline__ int traveledAtom(const TileInfo &ti, int lane) {
-  return (lane + (ti.diag ? 17 : 32)) & 31;
-}
-
-// GB pass 1: psi_i -= H(r, rho_i, s_j rho_j) and psi_j -= H(r, rho_j, s_i rho_i)
-struct RadiiPass {
-  const UnitSmem &s;
-  float4 ai, bi;
-  float psi_i, psi_j;
-  __device__ RadiiPass(const UnitSmem &s_in) : s(s_in) {}
-  __device__ __forceinline__ void begin(int islot) {
-    ai = s.pa[islot];
-    bi = s.pb[islot];
-    psi_i = 0.0f;
-    psi_j = 0.0f;
-  }
-  __device__ __forceinline__ void pair(int jslot, int) {
-    const float4 aj = s.pa[jslot];
-    const float4 bj = s.pb[jslot];
-    const float3 dv = pairDelta(ai, bi, aj, bj);
-    const float r2 = fmaf(dv.x, dv.x, fmaf(dv.y, dv.y, dv.z * dv.z));
-    const float invr = rsqrtf(r2);
-    const float r = r2 * invr;
-    psi_i -= hctIntegral(r, r2, invr, bi.w, aj.w);
-    psi_j -= hctIntegral(r, r2, invr, bj.w, ai.w);
-  }
-  __device__ __forceinline__ void rotate(int lane) {
-    psi_j = __shfl_sync(kFullMask, psi_j, (lane + 1) & 31);
-  }
-};
-
-// Pass 2: Coulomb + Lennard-Jones on non-excluded pairs and the GB pair terms
-template <bool FORCE, bool ENERGY, bool NB, bool GB>
-struct PairPass {
-  const UnitSmem &s;
-  float kk, inv_diel;
-  bool salt;
-  float4 ai, bi;
-  float inv4ri;     // 1 / (4 R_i)
-  int code_i;
-  unsigned mask;
-  float fxi, fyi, fzi, dei, fxj, fyj, fzj, dej;
-  float e_elec, e_vdw, e_gb;
-  __device__ PairPass(const UnitSmem &s_in, float kappa, float inv_dielectric) :
-      s(s_in), kk(-kappa * kGbKscale), inv_diel(inv_dielectric), salt(kappa > 0.0f) {}
-  __device__ __forceinline__ void begin(int islot, unsigned mask_in) {
-    ai = s.pa[islot];
-    bi = s.pb[islot];
-    inv4ri = 0.25f * s.gbv[islot].x;
-    code_i = __float_as_int(s.prm[islot].y) & 0xffff;
-    mask = mask_in;
-    fxi = fyi = fzi = dei = 0.0f;
-    fxj = fyj = fzj = dej = 0.0f;
-    e_elec = e_vdw = e_gb = 0.0f;
-  }
-  __device__ __forceinline__ void pair(int jslot, int jl) {
-    const float4 aj = s.pa[jslot];
-    const float4 bj = s.pb[jslot];
-    const float3 dv = pairDelta(ai, bi, aj, bj);
-    const float r2 = fmaf(dv.x, dv.x, fmaf(dv.y, dv.y, dv.z * dv.z));
-    const float qiqj_all = ai.w * aj.w;
-    float fmag = 0.0f;
-    if (NB) {
-      // excluded and padding pairs take the same path with zero parameters
-      const float incl = ((mask >> jl) & 1u) ? 0.0f : 1.0f;
-      // one Newton step on rsqrt keeps r^-12 within a few ulp
-      float invr = rsqrtf(r2);
-      invr = invr * fmaf(-0.5f * r2 * invr, invr, 1.5f);
-      const float invr2 = invr * invr;
-      const float invr4 = invr2 * invr2;
-      float2 ab = s.lj[code_i + (__float_as_int(s.prm[jslot].y) >> 16)];
-      ab.x *= incl;
-      ab.y *= incl;
-      const float qiqj = qiqj_all * incl;
-      if (ENERGY) {
-        e_elec = __fadd_rn(e_elec, __fmul_rn(qiqj, invr));
-        e_vdw = __fadd_rn(e_vdw, __fmul_rn(__fsub_rn(__fmul_rn(__fmul_rn(ab.x, invr4), invr4),
-                                                     __fmul_rn(ab.y, invr2)), invr4));
-      }
-      if (FORCE) {
-        fmag = -(qiqj * invr * invr2) + (6.0f * ab.y - 12.0f * ab.x * invr4 * invr2) * invr4 * invr4;
-      }
-    }
-    if (GB) {
-      const float qiqj = qiqj_all;
-      const float ijb = bi.w * bj.w;
-      const float efac = __expf(-r2 * inv4ri * s.gbv[jslot].x);
-      const float fgbi = rsqrtf(fmaf(ijb, efac, r2));
-      float expmkf, fgbk;
-      if (salt) {
-        fgbk = __fdividef(kk, fgbi);
-        expmkf = __expf(fgbk) * inv_diel;
-      }
-      else {
-        fgbk = 0.0f;
-        expmkf = inv_diel;
-      }
-      const float dielfac = 1.0f - expmkf;
-      if (ENERGY) {
-        e_gb = __fsub_rn(e_gb, __fmul_rn(__fmul_rn(qiqj, dielfac), fgbi));
-      }
-      if (FORCE) {
-        const float temp4 = fgbi * fgbi * fgbi;
-        const float temp6 = qiqj * temp4 * fmaf(fgbk, expmkf, dielfac);
-        fmag += temp6 * fmaf(-0.25f, efac, 1.0f);
-        const float temp5 = 0.5f * efac * temp6 * fmaf(0.25f, r2, ijb);
-        dei = fmaf(bi.w, temp5, dei);
-        dej = fmaf(bj.w, temp5, dej);
-      }
-    }
-    if (FORCE) {
-      fxi = fmaf(fmag, dv.x, fxi);
-      fyi = fmaf(fmag, dv.y, fyi);
-      fzi = fmaf(fmag, dv.z, fzi);
-      fxj = fmaf(-fmag, dv.x, fxj);
-      fyj = fmaf(-fmag, dv.y, fyj);
-      fzj = fmaf(-fmag, dv.z, fzj);
-    }
-  }
-  __device__ __forceinline__ void rotate(int lane) {
-    if (FORCE) {
-      const int src = (lane + 1) & 31;
-      fxj = __shfl_sync(kFullMask, fxj, src);
-      fyj = __shfl_sync(kFullMask, fyj, src);
-      fzj = __shfl_sync(kFullMask, fzj, src);
-      if (GB) {
-        dej = __shfl_sync(kFullMask, dej, src);
-      }
-    }
-  }
-};
-
-// Pass 3: radius chain-rule forces
-struct DerivPass {
-  const UnitSmem &s;
-  float4 ai, bi;
-  float de_i;
-  float fxi, fyi, fzi, fxj, fyj, fzj;
-  __device__ DerivPass(const UnitSmem &s_in) : s(s_in) {}
-  __device__ __forceinline__ void begin(int islot) {
-    ai = s.pa[islot];
-    bi = s.pb[islot];
-    de_i = s.gbv[islot].y;
-    fxi = fyi = fzi = 0.0f;
-    fxj = fyj = fzj = 0.0f;
-  }
-  __device__ __forceinline__ void pair(int jslot, int) {
-    const float4 aj = s.pa[jslot];
-    const float4 bj = s.pb[jslot];
-    const float de_j = s.gbv[jslot].y;
-    const float3 dv = pairDelta(ai, bi, aj, bj);
-    const float r2 = fmaf(dv.x, dv.x, fmaf(dv.y, dv.y, dv.z * dv.z));
-    const float invr = rsqrtf(r2);
-    const float r = r2 * invr;
-    const float fmag = hctDerivative(r, r2, invr, bi.w, aj.w) * de_i +
-                       hctDerivative(r, r2, invr, bj.w, ai.w) * de_j;
-    fxi = fmaf(-fmag, dv.x, fxi);
-    fyi = fmaf(-fmag, dv.y, fyi);
-    fzi = fmaf(-fmag, dv.z, fzi);
-    fxj = fmaf(fmag, dv.x, fxj);
-    fyj = fmaf(fmag, dv.y, fyj);
-    fzj = fmaf(fmag, dv.z, fzj);
-  }
-  __device__ __forceinline__ void rotate(int lane) {
-    const int src = (lane + 1) & 31;
-    fxj = __shfl_sync(kFullMask, fxj, src);
-    fyj = __shfl_sync(kFullMask, fyj, src);
-    fzj = __shfl_sync(kFullMask, fzj, src);
-  }
-};
-
-__device__ void gbRadiiTiles(const UnitSmem &s, int nsys_u, int ntiles) {
-  const int lane = threadIdx.x & 31;
-  const float ps = static_cast<float>(1 << kPsiBits);
-  RadiiPass p(s);
-  for (int t = threadIdx.x >> 5; t < ntiles; t += blockDim.x >> 5) {
-    const TileInfo ti = tileInfo(s, nsys_u, t);
-    p.begin(ti.ibase + lane);
-    walkTile(p, ti, lane);
-    if (lane < ti.ni) {
-      atomicAddInt63(p.psi_i * ps, &s.psi[ti.ibase + lane], &s.psio[ti.ibase + lane]);
-    }
-    const int jl = traveledAtom(ti, lane);
-    if (jl < ti.nj) {
-      atomicAddInt63(p.psi_j * ps, &s.psi[ti.jbase + jl], &s.psio[ti.jbase + jl]);
-    }
-  }
-}
-
-template <bool FORCE, bool ENERGY, bool NB, bool GB>
-__device__ void pairTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u, int ntiles) {
-  const int lane = threadIdx.x & 31;
-  const float fs = d.frc_scale;
-  const float es = d.nrg_scale;
-  const float ds = static_cast<float>(1 << kDeijdaBits);
-  PairPass<FORCE, ENERGY, NB, GB> p(s, d.kappa, d.inv_dielectric);
-  long long acc_elec = 0, acc_vdw = 0, acc_gb = 0;
-  int acc_k = -1;
-  for (int t = threadIdx.x >> 5; t < ntiles; t += blockDim.x >> 5) {
-    const TileInfo ti = tileInfo(s, nsys_u, t);
-    if (ENERGY && ti.k != acc_k) {
-      if (acc_k >= 0) {
-        const long long se = warpSum(acc_elec), sv = warpSum(acc_vdw), sg = warpSum(acc_gb);
-        if (lane == 0) {
-          if (NB) {
-            atomicAdd(&s.nrg[acc_k * kNrgStride + kElec], static_cast<unsigned long long>(se));
-            atomicAdd(&s.nrg[acc_k * kNrgStride + kVdw], static_cast<unsigned long long>(sv));
-          }
-          if (GB) {
-            atomicAdd(&s.nrg[acc_k * kNrgStride + kGb], static_cast<unsigned long long>(sg));
-          }
-        }
-      }
-      acc_elec = acc_vdw = acc_gb = 0;
-      acc_k = ti.k;
-    }
-    unsigned mask = 0u;
-    if (NB) {
-      const int midx = d.tile_mask_idx[d.tile_start[s.sys[ti.k]] + ti.local];
-      if (midx != 0) {
-        mask = __ldg(&d.mask_pool[static_cast<size_t>(midx) * 32 + lane]);
-      }
-    }
-    p.begin(ti.ibase + lane, mask);
-    walkTile(p, ti, lane);
-    if (FORCE) {
-      if (lane < ti.ni) {
-        const int is = ti.ibase + lane;
-        addForce(s, is, p.fxi, p.fyi, p.fzi, fs);
-        if (GB) {
-          atomicAddInt63(p.dei * ds, &s.de[is], &s.deo[is]);
-        }
-      }
-      const int jl = traveledAtom(ti, lane);
-      if (jl < ti.nj) {
-        const int js = ti.jbase + jl;
-        addForce(s, js, p.fxj, p.fyj, p.fzj, fs);
-        if (GB) {
-          atomicAddInt63(p.dej * ds, &s.de[js], &s.deo[js]);
-        }
-      }
-    }
-    if (ENERGY) {
-      acc_elec += __float2ll_rn(p.e_elec * es);
-      acc_vdw += __float2ll_rn(p.e_vdw * es);
-      acc_gb += __float2ll_rn(p.e_gb * es);
-    }
-  }
-  if (ENERGY) {
-    const long long se = warpSum(acc_elec), sv = warpSum(acc_vdw), sg = warpSum(acc_gb);
-    if (lane == 0 && acc_k >= 0) {
-      if (NB) {
-        atomicAdd(&s.nrg[acc_k * kNrgStride + kElec], static_cast<unsigned long long>(se));
-        atomicAdd(&s.nrg[acc_k * kNrgStride + kVdw], static_cast<unsigned long long>(sv));
-      }
-      if (GB) {
-        atomicAdd(&s.nrg[acc_k * kNrgStride + kGb], static_cast<unsigned long long>(sg));
-      }
-    }
-  }
-}
-
-__device__ void gbDerivativeTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u,
-                                  int ntiles) {
-  const int lane = threadIdx.x & 31;
-  const float fs = d.frc_scale;
-  DerivPass p(s);
-  for (int t = threadIdx.x >> 5; t < ntiles; t += blockDim.x >> 5) {
-    const TileInfo ti = tileInfo(s, nsys_u, t);
-    p.begin(ti.ibase + lane);
-    walkTile(p, ti, lane);
-    if (lane < ti.ni) {
-      addForce(s, ti.ibase + lane, p.fxi, p.fyi, p.fzi, fs);
-    }
-    const int jl = traveledAtom(ti, lane);
-    if (jl < ti.nj) {
-      addForce(s, ti.jbase + jl, p.fxj, p.fyj, p.fzj, fs);
-    }
-  }
-}
-
-}  // namespace
-
-// ------------------------------------------------------------------------------------------------
-// The fused kernel
+// The fused kernel: stage, evaluate, commit, one work unit at a time
 // ------------------------------------------------------------------------------------------------
 template <bool FORCE, bool ENERGY, int TERMS>
 __global__ void __launch_bounds__(256, 4)
 kEvalFused(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
   extern __shared__ __align__(16) char smem_raw[];
   const UnitSmem s = carveSmem(smem_raw, d.max_unit_slots, max_lj);
-  constexpr bool VALE = (TERMS & 1) != 0;
-  constexpr bool NB = (TERMS & 2) != 0;
-  const bool gb = ((TERMS & 4) != 0) && (d.igb != 0);
   for (int u = unit_begin + blockIdx.x; u < unit_end; u += gridDim.x) {
-    const int4 desc = d.unit_desc[u];
-    const int nsys_u = desc.y;
-    const int nslots = desc.z;
-    const int ntiles = desc.w;
-
-    // unit molecule table and prefix sums
-    if (threadIdx.x < nsys_u) {
-      const int sysid = d.unit_systems[desc.x + threadIdx.x];
-      s.sys[threadIdx.x] = sysid;
-      s.natom[threadIdx.x] = d.atom_count[sysid];
+    UnitShape us;
+    if (!stageUnitTables(d, s, u, max_lj, &us)) {
+      continue;
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int slot = 0, tile = 0, lj = 0, nb = 0, na = 0, nd = 0;
-      for (int k = 0; k < nsys_u; k++) {
-        const int sysid = s.sys[k];
-        const int n = s.natom[k];
-        const int nblk = (n + kTile - 1) / kTile;
-        s.slot0[k] = slot;
-        s.tile0[k] = tile;
-        s.ljbase[k] = lj;
-        s.bchunk0[k] = nb;
-        s.achunk0[k] = na;
-        s.dchunk0[k] = nd;
-        slot += nblk * kTile;
-        tile += nblk * (nblk + 1) / 2;
-        const int nt = d.lj_ntypes[sysid];
-        lj += 2 * nt * nt;
-        nb += (d.bond_start[sysid + 1] - d.bond_start[sysid] + 31) / 32;
-        na += (d.angl_start[sysid + 1] - d.angl_start[sysid] + 31) / 32;
-        nd += (d.dihe_start[sysid + 1] - d.dihe_start[sysid] + 31) / 32;
-      }
-      s.tile0[nsys_u] = tile;
-      s.bchunk0[nsys_u] = nb;
-      s.achunk0[nsys_u] = na;
-      s.dchunk0[nsys_u] = nd;
-      if (slot != nslots || tile != ntiles || lj > max_lj || slot > d.max_unit_slots) {
-        atomicOr(d.status, 1);
-      }
-    }
-    for (int e = threadIdx.x; e < nsys_u * kNrgStride; e += blockDim.x) {
+    for (int e = threadIdx.x; e < us.nsys * kNrgStride; e += blockDim.x) {
       s.nrg[e] = 0ull;
     }
-    __syncthreads();
-    if (nslots > d.max_unit_slots) {
-      continue;   // reported through the status word; nothing in the unit is touched
-    }
-
-    // stage Lennard-Jones tables (standard then 1-4) of every molecule
-    for (int k = 0; k < nsys_u; k++) {
-      const int sysid = s.sys[k];
-      const int nt = d.lj_ntypes[sysid];
-      const int src = d.lj_start[sysid];
-      for (int e = threadIdx.x; e < nt * nt; e += blockDim.x) {
-        s.lj[s.ljbase[k] + e] = d.ljab[src + e];
-        s.lj[s.ljbase[k] + nt * nt + e] = d.ljab14[src + e];
-      }
-    }
-
     // stage atoms (a warp's 32 consecutive slots always belong to one molecule)
-    for (int slot = threadIdx.x; slot < nslots; slot += blockDim.x) {
-      const int k = findOwner(s.slot0, nsys_u, slot);
-      const int sysid = s.sys[k];
+    for (int slot = threadIdx.x; slot < us.nslots; slot += blockDim.x) {
+      const int k = findOwner(s.slot0, us.nsys, slot);
       const int a = slot - s.slot0[k];
-      float4 pa, pb, prm;
-      if (a < s.natom[k]) {
-        const int gi = d.atom_start[sysid] + a;
-        const double x = static_cast<double>(d.xcrd[gi]) * d.inv_gpos_scale;
-        const double y = static_cast<double>(d.ycrd[gi]) * d.inv_gpos_scale;
-        const double z = static_cast<double>(d.zcrd[gi]) * d.inv_gpos_scale;
-        pa.x = static_cast<float>(x);
-        pa.y = static_cast<float>(y);
-        pa.z = static_cast<float>(z);
-        pb.x = static_cast<float>(x - static_cast<double>(pa.x));
-        pb.y = static_cast<float>(y - static_cast<double>(pa.y));
-        pb.z = static_cast<float>(z - static_cast<double>(pa.z));
-        const int nt = d.lj_ntypes[sysid];
-        const int ty = d.lj_idx[gi];
-        prm.x = d.charge[gi];
-        prm.y = __int_as_float((s.ljbase[k] + ty * nt) | (ty << 16));
-        prm.z = d.rho[gi];
-        prm.w = d.srho[gi];
-      }
-      else {
-        // padding slot: far from everything (16 A apart along x beyond 5000 A), no charge,
-        // zero screened radius, masked from Coulomb / Lennard-Jones: every pair term it enters
-        // is exactly zero for the real atom
-        pa = make_float4(5000.0f + 16.0f * static_cast<float>(slot), 0.0f, 0.0f, 0.0f);
-        pb = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
-        prm = make_float4(0.0f, __int_as_float(s.ljbase[k]), 1.0f, 0.0f);
-      }
-      pa.w = prm.w;   // pass 1 payload: s * rho
-      pb.w = prm.z;   //                 rho
-      s.pa[slot] = pa;
-      s.pb[slot] = pb;
-      s.prm[slot] = prm;
-      s.gbv[slot] = make_float2(1.0f, 0.0f);
-      s.fx[slot] = 0;
-      s.fy[slot] = 0;
-      s.fz[slot] = 0;
-      s.fxo[slot] = 0;
-      s.fyo[slot] = 0;
-      s.fzo[slot] = 0;
-      s.psi[slot] = 0;
-      s.psio[slot] = 0;
-      s.de[slot] = 0;
-      s.deo[slot] = 0;
+      s.prm[slot] = slotParameters(d, s, k, a);
+      const bool real = a < s.natom[k];
+      const int gi = d.atom_start[s.sys[k]] + (real ? a : 0);
+      placeSlot(d, s, slot, real, real ? d.xcrd[gi] : 0ll, real ? d.ycrd[gi] : 0ll,
+                real ? d.zcrd[gi] : 0ll);
     }
     __syncthreads();
-
-    // valence terms and GB pass 1 touch disjoint accumulators: no barrier between them
-    if (VALE) {
-      valenceTerms<FORCE, ENERGY>(d, s, nsys_u);
-      if (!gb) {
-        __syncthreads();
-      }
-    }
-    if (gb) {
-      gbRadiiTiles(s, nsys_u, ntiles);
-      __syncthreads();
-      // effective radii, self terms (nonbonded_potential.tpp:730-805); a warp's 32 slots
-      // belong to one molecule, so the self energies reduce across the warp
-      const float inv_ps = 1.0f / static_cast<float>(1 << kPsiBits);
-      const float ds = static_cast<float>(1 << kDeijdaBits);
-      for (int slot = threadIdx.x; slot < nslots; slot += blockDim.x) {
-        const int k = findOwner(s.slot0, nsys_u, slot);
-        const int a = slot - s.slot0[k];
-        float e_self = 0.0f;
-        float4 pa = s.pa[slot];
-        float4 pb = s.pb[slot];
-        const float4 prm = s.prm[slot];
-        float egbi = 1.0f;
-        if (a < s.natom[k]) {
-          const int gi = d.atom_start[s.sys[k]] + a;
-          const float psi = static_cast<float>(int63ToLong(s.psi[slot], s.psio[slot])) * inv_ps;
-          const float rho = prm.z;
-          if (d.igb == 1) {
-            egbi = 1.0f / (1.0f / rho + psi);
-            if (egbi < 0.0f) egbi = 30.0f;
-          }
-          else {
-            const float fipsi = psi * (-rho);
-            egbi = 1.0f / (1.0f / rho - tanhf((d.gb_alpha[gi] - d.gb_beta[gi] * fipsi +
-                                               d.gb_gamma[gi] * fipsi * fipsi) * fipsi) /
-                                        d.pb_radii[gi]);
-          }
-          const float q = prm.x;   // already scaled by sqrt(Coulomb constant)
-          const float expmkf = ((d.kappa > 0.0f) ? expf(-kGbKscale * d.kappa * egbi) : 1.0f) *
-                               d.inv_dielectric;
-          const float dielfac = 1.0f - expmkf;
-          const float atmq2h = 0.5f * q * q;
-          const float atmqd2h = atmq2h * dielfac;
-          e_self = -__fdiv_rn(atmqd2h, egbi);
-          if (FORCE) {
-            const float self_de = atmqd2h - kGbKscale * d.kappa * atmq2h * expmkf * egbi;
-            atomicAddInt63(self_de * ds, &s.de[slot], &s.deo[slot]);
-          }
-          d.born_radii[gi] = egbi;
-          d.psi[gi] = __double2ll_rn(static_cast<double>(psi) * d.psi_out_scale);
-          d.psi_ovrf[gi] = 0;
-          pa.w = prm.x;   // pass 2 payload: charge
-          pb.w = egbi;    //                 effective radius
-        }
-        else {
-          pa.w = 0.0f;
-          pb.w = 1.0f;
-        }
-        s.pa[slot] = pa;
-        s.pb[slot] = pb;
-        s.gbv[slot].x = 1.0f / egbi;
-        if (ENERGY) {
-          warpEnergy(s, k, kGb, e_self, d.nrg_scale);
-        }
-      }
-      __syncthreads();
-    }
-    else if (NB) {
-      // pass 2 payload for Coulomb / Lennard-Jones alone: charge in w1
-      for (int slot = threadIdx.x; slot < nslots; slot += blockDim.x) {
-        float4 pa = s.pa[slot];
-        pa.w = s.prm[slot].x;
-        s.pa[slot] = pa;
-      }
-      __syncthreads();
-    }
-    if (NB || gb) {
-      if (NB && gb) {
-        pairTiles<FORCE, ENERGY, true, true>(d, s, nsys_u, ntiles);
-      }
-      else if (NB) {
-        pairTiles<FORCE, ENERGY, true, false>(d, s, nsys_u, ntiles);
-      }
-      else {
-        pairTiles<FORCE, ENERGY, false, true>(d, s, nsys_u, ntiles);
-      }
-      __syncthreads();
-    }
-    if (gb && FORCE) {
-      // chain-rule prefactor of the OBC radii (nonbonded_potential.tpp:982-1021), and the
-      // pass 3 payloads
-      const float inv_ds = 1.0f / static_cast<float>(1 << kDeijdaBits);
-      const float inv_ps = 1.0f / static_cast<float>(1 << kPsiBits);
-      for (int slot = threadIdx.x; slot < nslots; slot += blockDim.x) {
-        const int k = findOwner(s.slot0, nsys_u, slot);
-        const int a = slot - s.slot0[k];
-        const float4 prm = s.prm[slot];
-        float4 pa = s.pa[slot];
-        float4 pb = s.pb[slot];
-        pa.w = prm.w;   // s * rho
-        pb.w = prm.z;   // rho
-        float sde = 0.0f;
-        if (a < s.natom[k]) {
-          const int gi = d.atom_start[s.sys[k]] + a;
-          sde = static_cast<float>(int63ToLong(s.de[slot], s.deo[slot])) * inv_ds;
-          if (d.igb != 1) {
-            const float psi = static_cast<float>(int63ToLong(s.psi[slot], s.psio[slot])) * inv_ps;
-            const float rho = prm.z;
-            const float fipsi = psi * (-rho);
-            const float al = d.gb_alpha[gi], be = d.gb_beta[gi], ga = d.gb_gamma[gi];
-            const float thi = tanhf((al - (be - ga * fipsi) * fipsi) * fipsi);
-            sde *= (al - (2.0f * be - 3.0f * ga * fipsi) * fipsi) * (1.0f - thi * thi) * rho /
-                   d.pb_radii[gi];
-          }
-          d.sumdeijda[gi] = __double2ll_rn(static_cast<double>(sde) * d.psi_out_scale);
-          d.sumdeijda_ovrf[gi] = 0;
-        }
-        s.pa[slot] = pa;
-        s.pb[slot] = pb;
-        s.gbv[slot].y = sde;
-      }
-      __syncthreads();
-      gbDerivativeTiles(d, s, nsys_u, ntiles);
-      __syncthreads();
-    }
+    evaluateStaged<FORCE, ENERGY, TERMS, true>(d, s, us);
 
     // commit forces (each atom belongs to exactly one unit) and energies
     if (FORCE) {
-      for (int slot = threadIdx.x; slot < nslots; slot += blockDim.x) {
-        const int k = findOwner(s.slot0, nsys_u, slot);
+      for (int slot = threadIdx.x; slot < us.nslots; slot += blockDim.x) {
+        const int k = findOwner(s.slot0, us.nsys, slot);
         const int a = slot - s.slot0[k];
         if (a >= s.natom[k]) continue;
         const int gi = d.atom_start[s.sys[k]] + a;
@@ -1098,7 +76,7 @@ kEvalFused(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
       }
     }
     if (ENERGY) {
-      for (int e = threadIdx.x; e < nsys_u * kNrgStride; e += blockDim.x) {
+      for (int e = threadIdx.x; e < us.nsys * kNrgStride; e += blockDim.x) {
         const unsigned long long v = s.nrg[e];
         if (v != 0ull) {
           atomicAdd(&d.energies[s.sys[e / kNrgStride] * kNrgStride + (e % kNrgStride)], v);
@@ -1149,3 +127,4 @@ cudaError_t launchEvalFused(const DevSynthesis &d, int unit_begin, int unit_end,
 }
 
 }  // namespace sb
+

@@ -1,0 +1,523 @@
+// Batched line minimization: STORMM's GPU minimizer (MolecularMechanics/hpc_minimization.cu:
+// 129-600) restated as one persistent kernel.
+//
+// STORMM runs each cycle as about thirty launches over the whole synthesis: a force + energy
+// evaluation, the conjugate-gradient gather / scatter / rescale (Math/conjugate_gradient.cui),
+// then three rounds of line advance + energy-only evaluation and a final cubic-fit placement
+// (MolecularMechanics/line_movement.cui).  Molecules never interact, so here a thread block takes
+// one work unit (whole molecules whose atoms fit in shared memory) and runs every cycle of every
+// molecule in it without leaving the kernel: the unit's parameters and Lennard-Jones tables are
+// staged once, each evaluation reuses them, and the per-molecule decisions are made by one thread
+// per molecule between block barriers.  Blocks pull units from a device counter, largest first.
+//
+// Per cycle and molecule, following the reference:
+//   1. forces and energy E0 at the line start
+//   2. gg = |f_prev|^2, dgg = (f - f_prev) . f, gamma = dgg / gg once the cycle count reaches the
+//      steepest-descent cycles (0 before), direction d = f + gamma d (conjugate_gradient.cui:
+//      8-140), normalized per molecule
+//   3. trial moves of 1 x, then 1.04 or 0.8 x, then 1.03 or 0.85 x the last factor, times the
+//      move length, with an energy after each (line_movement.cui:88-126)
+//   4. a cubic through the four energies places the molecule and scales the next move length
+//      (line_movement.cui:236-336)
+// Energies, gg, dgg, the direction norm, gamma and move lengths are FP64 per molecule; per-atom
+// arithmetic is FP32 on top of the int64 fixed-point coordinates.  Every per-molecule sum is an
+// integer sum or a fixed-order FP64 sum over that molecule's own 32-atom chunks, so a molecule's
+// trajectory is bit-identical whichever unit, launch or neighbours it has.
+#include <cuda_runtime.h>
+
+#include "unit_eval.cuh"
+
+namespace sb {
+
+namespace {
+
+constexpr double kVeryTiny = 1.0e-12;   // Constants/scaling.h verytiny
+constexpr int kMolDoubles = 12;
+
+// Per-molecule line-search scalars, kMaxUnitSystems of each
+enum MolSlot : int {
+  kE0 = 0, kE1, kE2, kE3,      // energies at the line start and the three trial points
+  kMv1, kMv2, kMv3,            // cumulative move factors of the trial points
+  kMfac,                       // factor of the latest trial move
+  kSMove,                      // move length of this cycle (A)
+  kLMove,                      // baseline move length of the next cycle (A)
+  kInvNorm,                    // 1 / |direction|
+  kStep                        // coordinate increment per unit direction, fixed-point units
+};
+
+struct MinSmem {
+  double* part;   // three partial sums per 32-slot chunk
+  double* mol;    // kMolDoubles x kMaxUnitSystems
+  int* cyc;       // completed cycles
+  int* done;      // converged (no further moves)
+};
+
+__host__ __device__ inline size_t minSmemBytes(int max_slots) {
+  return sizeof(double) * (3 * (max_slots / kTile) + kMolDoubles * kMaxUnitSystems) +
+         sizeof(int) * 2 * kMaxUnitSystems;
+}
+
+__device__ MinSmem carveMinSmem(char* base, int max_slots) {
+  MinSmem m;
+  m.part = reinterpret_cast<double*>(base);
+  m.mol = m.part + 3 * (max_slots / kTile);
+  m.cyc = reinterpret_cast<int*>(m.mol + kMolDoubles * kMaxUnitSystems);
+  m.done = m.cyc + kMaxUnitSystems;
+  return m;
+}
+
+__device__ __forceinline__ double& molValue(const MinSmem &ms, int slot, int k) {
+  return ms.mol[slot * kMaxUnitSystems + k];
+}
+
+__device__ __forceinline__ double warpSumDouble(double v) {
+  for (int o = 16; o > 0; o >>= 1) {
+    v += __shfl_xor_sync(0xffffffffu, v, o);
+  }
+  return v;
+}
+
+// Fixed-order sum of molecule k's chunk partials (component c of three)
+__device__ __forceinline__ double moleculeSum(const UnitSmem &s, const MinSmem &ms, int k,
+                                              int c) {
+  const int c0 = s.slot0[k] / kTile;
+  const int c1 = c0 + (s.natom[k] + kTile - 1) / kTile;
+  double t = 0.0;
+  for (int q = c0; q < c1; q++) {
+    t += ms.part[3 * q + c];
+  }
+  return t;
+}
+
+// Total potential energy of unit molecule k from its integer energy slots
+__device__ __forceinline__ double moleculeEnergy(const DevSynthesis &d, const UnitSmem &s, int k) {
+  long long t = 0;
+  for (int q = 0; q < kNrgStride; q++) {
+    t += static_cast<long long>(s.nrg[k * kNrgStride + q]);
+  }
+  return static_cast<double>(t) / static_cast<double>(d.nrg_scale);
+}
+
+// Place every slot of the unit at the current coordinates and clear the accumulators
+__device__ void placeUnit(const DevSynthesis &d, const DevMinimizer &m, const UnitSmem &s,
+                          const UnitShape &us) {
+  for (int e = threadIdx.x; e < us.nsys * kNrgStride; e += blockDim.x) {
+    s.nrg[e] = 0ull;
+  }
+  for (int slot = threadIdx.x; slot < us.nslots; slot += blockDim.x) {
+    const int k = findOwner(s.slot0, us.nsys, slot);
+    const int a = slot - s.slot0[k];
+    const bool real = a < s.natom[k];
+    const int gi = d.atom_start[s.sys[k]] + (real ? a : 0);
+    placeSlot(d, s, slot, real, real ? m.xcrd[gi] : 0ll, real ? m.ycrd[gi] : 0ll,
+              real ? m.zcrd[gi] : 0ll);
+  }
+  __syncthreads();
+}
+
+// Move every atom of the molecules with a nonzero step along the direction
+__device__ void moveUnit(const DevSynthesis &d, const DevMinimizer &m, const UnitSmem &s,
+                         const MinSmem &ms, const UnitShape &us) {
+  for (int slot = threadIdx.x; slot < us.nslots; slot += blockDim.x) {
+    const int k = findOwner(s.slot0, us.nsys, slot);
+    const int a = slot - s.slot0[k];
+    const double step = molValue(ms, kStep, k);
+    if (a < s.natom[k] && step != 0.0) {
+      const int gi = d.atom_start[s.sys[k]] + a;
+      m.xcrd[gi] += __double2ll_rn(static_cast<double>(m.xcg[gi]) * step);
+      m.ycrd[gi] += __double2ll_rn(static_cast<double>(m.ycg[gi]) * step);
+      m.zcrd[gi] += __double2ll_rn(static_cast<double>(m.zcg[gi]) * step);
+    }
+  }
+}
+
+// Cubic through (0, e0), (x1, e1), (x2, e2), (x3, e3): Gauss-Jordan elimination with partial
+// pivoting on the 4 x 4 Vandermonde system, the elimination line_movement.cui:160-236 performs
+__device__ void cubicFit(const double* x, const double* e, double* abcd) {
+  double mtx[4][5];
+  for (int r = 0; r < 4; r++) {
+    mtx[r][0] = x[r] * x[r] * x[r];
+    mtx[r][1] = x[r] * x[r];
+    mtx[r][2] = x[r];
+    mtx[r][3] = 1.0;
+    mtx[r][4] = e[r];
+  }
+  for (int col = 0; col < 4; col++) {
+    int piv = col;
+    for (int r = col + 1; r < 4; r++) {
+      if (fabs(mtx[r][col]) > fabs(mtx[piv][col])) piv = r;
+    }
+    if (piv != col) {
+      for (int q = 0; q < 5; q++) {
+        const double t = mtx[col][q];
+        mtx[col][q] = mtx[piv][q];
+        mtx[piv][q] = t;
+      }
+    }
+    const double p = mtx[col][col];
+    for (int q = 0; q < 5; q++) mtx[col][q] /= p;
+    for (int r = 0; r < 4; r++) {
+      if (r == col) continue;
+      const double f = mtx[r][col];
+      for (int q = 0; q < 5; q++) mtx[r][q] -= f * mtx[col][q];
+    }
+  }
+  for (int r = 0; r < 4; r++) abcd[r] = mtx[r][4];
+}
+
+// Final placement along the line from the four energies (line_movement.cui:236-336): returns the
+// move factor relative to the third trial point and sets the next move length's scale
+__device__ double finalPlacement(const double* ev, const double* mv, double* new_base) {
+  if (ev[0] < ev[1] && ev[0] < ev[2] && ev[0] < ev[3]) {
+    *new_base = 0.8;
+    return -mv[3];
+  }
+  double abcd[4];
+  cubicFit(mv, ev, abcd);
+  const double d0 = 3.0 * abcd[0], d1 = 2.0 * abcd[1], d2 = abcd[2];
+  const double sqrt_arg = d1 * d1 - 4.0 * d0 * d2;
+  if (sqrt_arg < 0.0) {
+    if (ev[0] < ev[3]) {
+      *new_base = 0.8;
+      return -mv[3];
+    }
+    *new_base = 1.2;
+    return 0.0;
+  }
+  const double ext_i = (-d1 + sqrt(sqrt_arg)) / (2.0 * d0);
+  const double ext_ii = (-d1 - sqrt(sqrt_arg)) / (2.0 * d0);
+  const double min_pos = (2.0 * d0 * ext_i + d1 > 0.0) ? ext_i : ext_ii;
+  if (min_pos <= 0.0) {
+    if (ev[3] >= ev[0]) {
+      *new_base = 0.8;
+      return -mv[3];
+    }
+    *new_base = 1.2;
+    return 0.0;
+  }
+  if (min_pos < mv[3]) {
+    const double epred = ((abcd[0] * min_pos + abcd[1]) * min_pos + abcd[2]) * min_pos + abcd[3];
+    if (epred > ev[0]) {
+      *new_base = 0.8;
+      return -mv[3];
+    }
+    if (epred < ev[3]) {
+      *new_base = (min_pos > 0.6) ? 1.05 : 0.95;
+      return min_pos - mv[3];
+    }
+    *new_base = 1.05;
+    return 0.0;
+  }
+  *new_base = 1.05;
+  return 0.0;
+}
+
+// One line-minimization cycle of every unit molecule that has not converged
+template <bool HIST>
+__device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
+                                  const UnitSmem &s, const MinSmem &ms, const UnitShape &us) {
+  const int lane = threadIdx.x & 31;
+  const double inv_fs = 1.0 / static_cast<double>(d.frc_scale);
+  const double gpos_scale = 1.0 / d.inv_gpos_scale;
+
+  // 1. forces and energy at the line start
+  placeUnit(d, m, s, us);
+  evaluateStaged<true, true, 7, false>(d, s, us);
+
+  // 2. gg, dgg and |f|^2 per 32-slot chunk (a chunk never straddles two molecules)
+  for (int slot = threadIdx.x; slot < us.nslots; slot += blockDim.x) {
+    const int k = findOwner(s.slot0, us.nsys, slot);
+    const int a = slot - s.slot0[k];
+    double gg = 0.0, dgg = 0.0, ff = 0.0;
+    if (a < s.natom[k]) {
+      const int gi = d.atom_start[s.sys[k]] + a;
+      const double fx = static_cast<double>(int63ToLong(s.fx[slot], s.fxo[slot]));
+      const double fy = static_cast<double>(int63ToLong(s.fy[slot], s.fyo[slot]));
+      const double fz = static_cast<double>(int63ToLong(s.fz[slot], s.fzo[slot]));
+      const double px = static_cast<double>(m.xprv[gi]);
+      const double py = static_cast<double>(m.yprv[gi]);
+      const double pz = static_cast<double>(m.zprv[gi]);
+      gg = px * px + py * py + pz * pz;
+      dgg = (fx - px) * fx + (fy - py) * fy + (fz - pz) * fz;
+      ff = fx * fx + fy * fy + fz * fz;
+    }
+    gg = warpSumDouble(gg);
+    dgg = warpSumDouble(dgg);
+    ff = warpSumDouble(ff);
+    if (lane == 0) {
+      const int q = slot / kTile;
+      ms.part[3 * q] = gg;
+      ms.part[3 * q + 1] = dgg;
+      ms.part[3 * q + 2] = ff;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < us.nsys) {
+    const int k = threadIdx.x;
+    const int sysid = s.sys[k];
+    const double gg = moleculeSum(s, ms, k, 0) * inv_fs * inv_fs;
+    const double dgg = moleculeSum(s, ms, k, 1) * inv_fs * inv_fs;
+    const double ff = moleculeSum(s, ms, k, 2) * inv_fs * inv_fs;
+    const double e0 = moleculeEnergy(d, s, k);
+    molValue(ms, kE0, k) = e0;
+    if (!ms.done[k]) {
+      const double rms = sqrt(ff / (3.0 * static_cast<double>(s.natom[k])));
+      m.rms_force[sysid] = rms;
+      if (HIST && ms.cyc[k] < m.hist_stride) {
+        m.history[static_cast<size_t>(sysid) * m.hist_stride + ms.cyc[k]] = e0;
+      }
+      if (m.drms > 0.0 && rms <= m.drms) {
+        ms.done[k] = 1;
+      }
+    }
+    // the reference advances its step counter before the gather (hpc_minimization.cu:470)
+    const int step = ms.cyc[k] + 1;
+    molValue(ms, kMfac, k) = (step >= m.sd_cycles && gg > 0.0) ? dgg / gg : 0.0;   // gamma
+  }
+  __syncthreads();
+
+  // conjugate direction, previous force, |direction|^2
+  for (int slot = threadIdx.x; slot < us.nslots; slot += blockDim.x) {
+    const int k = findOwner(s.slot0, us.nsys, slot);
+    const int a = slot - s.slot0[k];
+    double msum = 0.0;
+    if (a < s.natom[k] && !ms.done[k]) {
+      const int gi = d.atom_start[s.sys[k]] + a;
+      const long long ix = int63ToLong(s.fx[slot], s.fxo[slot]);
+      const long long iy = int63ToLong(s.fy[slot], s.fyo[slot]);
+      const long long iz = int63ToLong(s.fz[slot], s.fzo[slot]);
+      const double gam = molValue(ms, kMfac, k);
+      float cx = static_cast<float>(static_cast<double>(ix) * inv_fs);
+      float cy = static_cast<float>(static_cast<double>(iy) * inv_fs);
+      float cz = static_cast<float>(static_cast<double>(iz) * inv_fs);
+      if (fabs(gam) > kVeryTiny) {
+        const float g = static_cast<float>(gam);
+        cx = fmaf(g, m.xcg[gi], cx);
+        cy = fmaf(g, m.ycg[gi], cy);
+        cz = fmaf(g, m.zcg[gi], cz);
+      }
+      m.xcg[gi] = cx;
+      m.ycg[gi] = cy;
+      m.zcg[gi] = cz;
+      m.xprv[gi] = ix;
+      m.yprv[gi] = iy;
+      m.zprv[gi] = iz;
+      msum = static_cast<double>(cx) * cx + static_cast<double>(cy) * cy +
+             static_cast<double>(cz) * cz;
+    }
+    msum = warpSumDouble(msum);
+    if (lane == 0) {
+      ms.part[3 * (slot / kTile)] = msum;
+    }
+  }
+  __syncthreads();
+
+  // 3. first trial move: 1 x the move length
+  if (threadIdx.x < us.nsys) {
+    const int k = threadIdx.x;
+    if (!ms.done[k]) {
+      const double msum = moleculeSum(s, ms, k, 0);
+      const double inv_norm = (msum > 0.0) ? 1.0 / sqrt(msum) : 0.0;
+      const double s_move = molValue(ms, kLMove, k);
+      molValue(ms, kInvNorm, k) = inv_norm;
+      molValue(ms, kSMove, k) = s_move;
+      molValue(ms, kMfac, k) = 1.0;
+      molValue(ms, kMv1, k) = 1.0;
+      molValue(ms, kStep, k) = inv_norm * s_move * gpos_scale;
+    }
+    else {
+      molValue(ms, kStep, k) = 0.0;
+    }
+  }
+  __syncthreads();
+  moveUnit(d, m, s, ms, us);
+  placeUnit(d, m, s, us);
+  evaluateStaged<false, true, 7, false>(d, s, us);
+
+  // second trial move: 1.04 x after a decrease, else 0.8 x
+  if (threadIdx.x < us.nsys) {
+    const int k = threadIdx.x;
+    const double e1 = moleculeEnergy(d, s, k);
+    molValue(ms, kE1, k) = e1;
+    if (!ms.done[k]) {
+      const double mfac = (e1 < molValue(ms, kE0, k)) ? 1.04 : 0.8;
+      molValue(ms, kMfac, k) = mfac;
+      molValue(ms, kMv2, k) = molValue(ms, kMv1, k) + mfac;
+      molValue(ms, kStep, k) = molValue(ms, kInvNorm, k) * mfac * molValue(ms, kSMove, k) *
+                               gpos_scale;
+    }
+  }
+  __syncthreads();
+  moveUnit(d, m, s, ms, us);
+  placeUnit(d, m, s, us);
+  evaluateStaged<false, true, 7, false>(d, s, us);
+
+  // third trial move: the last factor x 1.03 after a decrease, else x 0.85
+  if (threadIdx.x < us.nsys) {
+    const int k = threadIdx.x;
+    const double e2 = moleculeEnergy(d, s, k);
+    molValue(ms, kE2, k) = e2;
+    if (!ms.done[k]) {
+      const double mfac = molValue(ms, kMfac, k) * ((e2 < molValue(ms, kE1, k)) ? 1.03 : 0.85);
+      molValue(ms, kMfac, k) = mfac;
+      molValue(ms, kMv3, k) = molValue(ms, kMv2, k) + mfac;
+      molValue(ms, kStep, k) = molValue(ms, kInvNorm, k) * mfac * molValue(ms, kSMove, k) *
+                               gpos_scale;
+    }
+  }
+  __syncthreads();
+  moveUnit(d, m, s, ms, us);
+  placeUnit(d, m, s, us);
+  evaluateStaged<false, true, 7, false>(d, s, us);
+
+  // 4. cubic fit and final placement
+  if (threadIdx.x < us.nsys) {
+    const int k = threadIdx.x;
+    const double e3 = moleculeEnergy(d, s, k);
+    if (!ms.done[k]) {
+      const double ev[4] = {molValue(ms, kE0, k), molValue(ms, kE1, k), molValue(ms, kE2, k), e3};
+      const double mv[4] = {0.0, molValue(ms, kMv1, k), molValue(ms, kMv2, k),
+                            molValue(ms, kMv3, k)};
+      double new_base;
+      const double mfac = finalPlacement(ev, mv, &new_base);
+      const double s_move = molValue(ms, kSMove, k);
+      molValue(ms, kLMove, k) = s_move * new_base;
+      molValue(ms, kStep, k) = (fabs(mfac) > kVeryTiny) ?
+                               molValue(ms, kInvNorm, k) * mfac * s_move * gpos_scale : 0.0;
+      ms.cyc[k] += 1;
+    }
+    else {
+      molValue(ms, kStep, k) = 0.0;
+    }
+  }
+  __syncthreads();
+  moveUnit(d, m, s, ms, us);
+  __syncthreads();
+}
+
+template <bool HIST>
+__global__ void __launch_bounds__(256, 4)
+kMinimize(const DevSynthesis d, const DevMinimizer m, int unit_begin, int unit_end, int max_lj,
+          int cycles, int final_energy) {
+  extern __shared__ __align__(16) char smem_raw[];
+  const UnitSmem s = carveSmem(smem_raw, d.max_unit_slots, max_lj);
+  const MinSmem ms = carveMinSmem(smem_raw + alignUp(unitSmemBytes(d.max_unit_slots, max_lj), 16),
+                                  d.max_unit_slots);
+  __shared__ int next_unit;
+  int u = unit_begin + blockIdx.x;
+  while (u < unit_end) {
+    UnitShape us;
+    if (stageUnitTables(d, s, u, max_lj, &us)) {
+      for (int slot = threadIdx.x; slot < us.nslots; slot += blockDim.x) {
+        const int k = findOwner(s.slot0, us.nsys, slot);
+        s.prm[slot] = slotParameters(d, s, k, slot - s.slot0[k]);
+      }
+      if (threadIdx.x < us.nsys) {
+        const int k = threadIdx.x;
+        const int sysid = s.sys[k];
+        ms.cyc[k] = m.cycle[sysid];
+        ms.done[k] = m.done[sysid];
+        molValue(ms, kLMove, k) = m.l_move[sysid];
+      }
+      __syncthreads();
+      for (int c = 0; c < cycles; c++) {
+        const int moving = (threadIdx.x < us.nsys) ? !ms.done[threadIdx.x] : 0;
+        if (!__syncthreads_or(moving)) {
+          break;
+        }
+        minimizationCycle<HIST>(d, m, s, ms, us);
+      }
+      if (final_energy) {
+        // one more energy evaluation at the final coordinates (hpc_minimization.cu:372-383)
+        placeUnit(d, m, s, us);
+        evaluateStaged<false, true, 7, false>(d, s, us);
+        for (int e = threadIdx.x; e < us.nsys * kNrgStride; e += blockDim.x) {
+          d.energies[s.sys[e / kNrgStride] * kNrgStride + (e % kNrgStride)] = s.nrg[e];
+        }
+        if (HIST && threadIdx.x < us.nsys) {
+          const int k = threadIdx.x;
+          if (ms.cyc[k] < m.hist_stride) {
+            m.history[static_cast<size_t>(s.sys[k]) * m.hist_stride + ms.cyc[k]] =
+              moleculeEnergy(d, s, k);
+          }
+        }
+      }
+      if (threadIdx.x < us.nsys) {
+        const int k = threadIdx.x;
+        const int sysid = s.sys[k];
+        m.cycle[sysid] = ms.cyc[k];
+        m.done[sysid] = ms.done[k];
+        m.l_move[sysid] = molValue(ms, kLMove, k);
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      next_unit = unit_begin + static_cast<int>(gridDim.x) + atomicAdd(m.queue, 1);
+    }
+    __syncthreads();
+    u = next_unit;
+  }
+}
+
+__global__ void kMinimizerReset(DevMinimizer m, int nsys, int natom_padded, double dx0) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < natom_padded; i += stride) {
+    m.xprv[i] = 0;
+    m.yprv[i] = 0;
+    m.zprv[i] = 0;
+    m.xcg[i] = 0.0f;
+    m.ycg[i] = 0.0f;
+    m.zcg[i] = 0.0f;
+  }
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nsys; i += stride) {
+    m.l_move[i] = dx0;
+    m.cycle[i] = 0;
+    m.done[i] = 0;
+    m.rms_force[i] = 0.0;
+  }
+}
+
+}  // namespace
+
+size_t minimizeSmemBytes(int max_slots, int max_lj) {
+  return alignUp(unitSmemBytes(max_slots, max_lj), 16) + minSmemBytes(max_slots);
+}
+
+cudaError_t launchMinimizerReset(const DevMinimizer &m, const DevSynthesis &d, double dx0,
+                                 cudaStream_t stream) {
+  const int n = d.natom_padded > d.nsys ? d.natom_padded : d.nsys;
+  int blocks = (n + 255) / 256;
+  blocks = blocks < 1 ? 1 : (blocks > 1024 ? 1024 : blocks);
+  kMinimizerReset<<<blocks, 256, 0, stream>>>(m, d.nsys, d.natom_padded, dx0);
+  return cudaGetLastError();
+}
+
+// Units [unit_begin, unit_end) for up to `cycles` cycles on at most max_blocks resident blocks.
+// m.queue must hold zero when the kernel starts.
+cudaError_t launchMinimize(const DevSynthesis &d, const DevMinimizer &m, int unit_begin,
+                           int unit_end, int max_lj, int cycles, bool final_energy, int threads,
+                           int sm_count, cudaStream_t stream) {
+  if (unit_end <= unit_begin) {
+    return cudaSuccess;
+  }
+  const size_t smem = minimizeSmemBytes(d.max_unit_slots, max_lj);
+  auto kern = (m.history != nullptr) ? kMinimize<true> : kMinimize<false>;
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+  if (err != cudaSuccess) return err;
+  int per_sm = 0;
+  err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+  if (err != cudaSuccess) return err;
+  if (per_sm < 1) {
+    return cudaErrorInvalidConfiguration;
+  }
+  int blocks = per_sm * sm_count;
+  if (blocks > unit_end - unit_begin) {
+    blocks = unit_end - unit_begin;
+  }
+  kern<<<blocks, threads, smem, stream>>>(d, m, unit_begin, unit_end, max_lj, cycles,
+                                          final_energy ? 1 : 0);
+  return cudaGetLastError();
+}
+
+}  // namespace sb

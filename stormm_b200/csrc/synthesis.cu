@@ -25,6 +25,12 @@ size_t fusedSmemBytes(int max_slots, int max_lj);
 cudaError_t launchEvalFused(const DevSynthesis &d, int unit_begin, int unit_end, int max_lj,
                             int terms, bool force, bool energy, int blocks, int threads,
                             cudaStream_t stream);
+size_t minimizeSmemBytes(int max_slots, int max_lj);
+cudaError_t launchMinimizerReset(const DevMinimizer &m, const DevSynthesis &d, double dx0,
+                                 cudaStream_t stream);
+cudaError_t launchMinimize(const DevSynthesis &d, const DevMinimizer &m, int unit_begin,
+                           int unit_end, int max_lj, int cycles, bool final_energy, int threads,
+                           int sm_count, cudaStream_t stream);
 cudaError_t launchImportCoordinates(const double* d_xyz, const int* d_map, int natom,
                                     double scale, long long* xcrd, long long* ycrd,
                                     long long* zcrd, int* xo, int* yo, int* zo, int* status,
@@ -659,6 +665,141 @@ int Synthesis::checkStatus(cudaStream_t stream) {
   return st;
 }
 
+// ------------------------------------------------------------------------------------------------
+// Line minimization (MolecularMechanics/hpc_minimization.cu:129-600)
+// ------------------------------------------------------------------------------------------------
+DevMinimizer Synthesis::prepareMinimizer(const sb_minimize_controls &ctl, cudaStream_t stream) {
+  if (ctl.total_cycles < 0 || ctl.sd_cycles < 0) {
+    throw Error(SB_ERR_ARGUMENT, "cycle counts must not be negative");
+  }
+  if (ctl.clash_cycles != 0) {
+    throw Error(SB_ERR_UNSUPPORTED, "clash-damping cycles (softened cores) are not provided; "
+                "set clash_cycles to 0");
+  }
+  if (!(ctl.initial_step > 0.0) || !(ctl.convergence_rms >= 0.0)) {
+    throw Error(SB_ERR_ARGUMENT, "initial step must be positive and the RMS target not negative");
+  }
+  const size_t np = natom_padded;
+  if (d_mcycle.p == nullptr) {
+    d_xprv.allocate(np);
+    d_yprv.allocate(np);
+    d_zprv.allocate(np);
+    d_xcg.allocate(np);
+    d_ycg.allocate(np);
+    d_zcg.allocate(np);
+    d_lmove.allocate(nsys);
+    d_rmsf.allocate(nsys);
+    d_mcycle.allocate(nsys);
+    d_mdone.allocate(nsys);
+    d_queue.allocate(2);
+  }
+  history_stride = 0;
+  if (ctl.record_history) {
+    history_stride = ctl.total_cycles + 1;
+    const size_t need = static_cast<size_t>(nsys) * history_stride;
+    if (d_history.n < need) {
+      d_history.allocate(need);
+    }
+    cudaCheck(cudaMemsetAsync(d_history.p, 0, need * sizeof(double), stream), "memset");
+  }
+  DevMinimizer m;
+  std::memset(&m, 0, sizeof(DevMinimizer));
+  m.xcrd = d_xcrd.p;
+  m.ycrd = d_ycrd.p;
+  m.zcrd = d_zcrd.p;
+  m.xprv = d_xprv.p;
+  m.yprv = d_yprv.p;
+  m.zprv = d_zprv.p;
+  m.xcg = d_xcg.p;
+  m.ycg = d_ycg.p;
+  m.zcg = d_zcg.p;
+  m.l_move = d_lmove.p;
+  m.cycle = d_mcycle.p;
+  m.done = d_mdone.p;
+  m.rms_force = d_rmsf.p;
+  m.history = ctl.record_history ? d_history.p : nullptr;
+  m.hist_stride = history_stride;
+  m.sd_cycles = ctl.sd_cycles;
+  m.drms = ctl.convergence_rms;
+  m.queue = d_queue.p;
+  cudaCheck(launchMinimizerReset(m, dev, ctl.initial_step, stream), "minimizer reset");
+  return m;
+}
+
+void Synthesis::minimize(const sb_minimize_controls &ctl, cudaStream_t stream) {
+  DevMinimizer m = prepareMinimizer(ctl, stream);
+  cudaCheck(cudaMemsetAsync(d_queue.p, 0, 2 * sizeof(int), stream), "memset");
+  const int nunit = h_units.size();
+  if (n_big_units > 0) {
+    DevSynthesis d = dev;
+    d.max_unit_slots = big_slots;
+    m.queue = d_queue.p;
+    if (static_cast<int>(minimizeSmemBytes(big_slots, big_lj)) > max_smem_optin) {
+      throw Error(SB_ERR_UNSUPPORTED, "a molecule is too large for on-chip minimization");
+    }
+    cudaCheck(launchMinimize(d, m, 0, n_big_units, big_lj, ctl.total_cycles, true, threads,
+                             sm_count, stream), "minimization launch (large molecules)");
+  }
+  if (nunit > n_big_units) {
+    DevSynthesis d = dev;
+    d.max_unit_slots = small_slots;
+    m.queue = d_queue.p + 1;
+    cudaCheck(launchMinimize(d, m, n_big_units, nunit, small_lj, ctl.total_cycles, true, threads,
+                             sm_count, stream), "minimization launch");
+  }
+}
+
+void Synthesis::minimizeRange(int first, int count, const sb_minimize_controls &ctl,
+                              cudaStream_t stream) {
+  if (first < 0 || count < 0 || first + count > nsys) {
+    throw Error(SB_ERR_ARGUMENT, "system range out of bounds");
+  }
+  DevMinimizer m = prepareMinimizer(ctl, stream);
+  DevSynthesis d = dev;
+  d.unit_desc = d_single_units.p;
+  d.unit_systems = d_single_systems.p;
+  d.nunit = nsys;
+  d.max_unit_slots = single_slots;
+  if (static_cast<int>(minimizeSmemBytes(single_slots, single_lj)) > max_smem_optin) {
+    throw Error(SB_ERR_UNSUPPORTED, "a molecule is too large for on-chip minimization");
+  }
+  // one block per launch: the unit counter is never consulted for a second unit
+  for (int s = first; s < first + count; s++) {
+    cudaCheck(launchMinimize(d, m, s, s + 1, single_lj, ctl.total_cycles, true, threads,
+                             sm_count, stream), "per-system minimization launch");
+  }
+}
+
+void Synthesis::getMinimizeHistory(double* out, cudaStream_t stream) {
+  if (history_stride == 0) {
+    throw Error(SB_ERR_ARGUMENT, "the last minimization kept no history");
+  }
+  cudaCheck(cudaMemcpyAsync(out, d_history.p,
+                            sizeof(double) * static_cast<size_t>(nsys) * history_stride,
+                            cudaMemcpyDeviceToHost, stream), "history download");
+  cudaCheck(cudaStreamSynchronize(stream), "history download");
+}
+
+void Synthesis::getMinimizeProgress(int* cycles, int* converged, double* rms,
+                                    cudaStream_t stream) {
+  if (d_mcycle.p == nullptr) {
+    throw Error(SB_ERR_ARGUMENT, "no minimization has run");
+  }
+  if (cycles) {
+    cudaCheck(cudaMemcpyAsync(cycles, d_mcycle.p, sizeof(int) * nsys, cudaMemcpyDeviceToHost,
+                              stream), "progress download");
+  }
+  if (converged) {
+    cudaCheck(cudaMemcpyAsync(converged, d_mdone.p, sizeof(int) * nsys, cudaMemcpyDeviceToHost,
+                              stream), "progress download");
+  }
+  if (rms) {
+    cudaCheck(cudaMemcpyAsync(rms, d_rmsf.p, sizeof(double) * nsys, cudaMemcpyDeviceToHost,
+                              stream), "progress download");
+  }
+  cudaCheck(cudaStreamSynchronize(stream), "progress download");
+}
+
 }  // namespace sb
 
 // ------------------------------------------------------------------------------------------------
@@ -837,6 +978,45 @@ int sb_check_status(sb_synthesis* syn, int* status) {
   return guarded([&]() {
     const int st = need(syn)->checkStatus(nullptr);
     if (status) *status = st;
+  });
+}
+
+void sb_default_minimize_controls(sb_minimize_controls* ctl) {
+  std::memset(ctl, 0, sizeof(sb_minimize_controls));
+  ctl->total_cycles = 200;
+  ctl->sd_cycles = 50;
+  ctl->clash_cycles = 0;
+  ctl->initial_step = 0.01;
+  ctl->convergence_rms = 0.0;
+  ctl->record_history = 0;
+}
+
+int sb_minimize(sb_synthesis* syn, const sb_minimize_controls* ctl, void* stream) {
+  return guarded([&]() {
+    if (ctl == nullptr) throw sb::Error(SB_ERR_ARGUMENT, "null minimization controls");
+    need(syn)->minimize(*ctl, asStream(stream));
+  });
+}
+
+int sb_minimize_range(sb_synthesis* syn, int first, int count, const sb_minimize_controls* ctl,
+                      void* stream) {
+  return guarded([&]() {
+    if (ctl == nullptr) throw sb::Error(SB_ERR_ARGUMENT, "null minimization controls");
+    need(syn)->minimizeRange(first, count, *ctl, asStream(stream));
+  });
+}
+
+int sb_get_minimize_history(sb_synthesis* syn, double* history, void* stream) {
+  return guarded([&]() {
+    if (history == nullptr) throw sb::Error(SB_ERR_ARGUMENT, "null output");
+    need(syn)->getMinimizeHistory(history, asStream(stream));
+  });
+}
+
+int sb_get_minimize_progress(sb_synthesis* syn, int* cycles_done, int* converged,
+                             double* rms_force, void* stream) {
+  return guarded([&]() {
+    need(syn)->getMinimizeProgress(cycles_done, converged, rms_force, asStream(stream));
   });
 }
 

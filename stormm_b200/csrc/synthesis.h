@@ -81,6 +81,10 @@ public:
   void getEnergiesFixed(long long* out, cudaStream_t stream);
   void getGbWorkspace(double* psi, double* radii, double* sde, cudaStream_t stream);
   int checkStatus(cudaStream_t stream);
+  void minimize(const sb_minimize_controls &ctl, cudaStream_t stream);
+  void minimizeRange(int first, int count, const sb_minimize_controls &ctl, cudaStream_t stream);
+  void getMinimizeHistory(double* out, cudaStream_t stream);
+  void getMinimizeProgress(int* cycles, int* converged, double* rms, cudaStream_t stream);
 
   sb_options opt;
   int nsys = 0;
@@ -129,10 +133,18 @@ public:
   DeviceArray<int> d_unpadded_map;
   DeviceArray<double> d_stage_xyz, d_stage_nrg;
 
+  // line-minimization state, allocated by the first minimization
+  DeviceArray<long long> d_xprv, d_yprv, d_zprv;
+  DeviceArray<float> d_xcg, d_ycg, d_zcg;
+  DeviceArray<double> d_lmove, d_rmsf, d_history;
+  DeviceArray<int> d_mcycle, d_mdone, d_queue;
+  int history_stride = 0;
+
   DevSynthesis dev;
 
 private:
   void buildLayout(const sb_topology* tops, int ntop);
+  DevMinimizer prepareMinimizer(const sb_minimize_controls &ctl, cudaStream_t stream);
   void buildUnits();
   void upload();
 };
