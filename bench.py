@@ -1,14 +1,20 @@
-"""Benchmark of the batched implicit-solvent single point (force + energy) on B200.
+"""Benchmark of the batched implicit-solvent path on B200: single points and minimizations.
 
-Workload: 1,024 distinct synthetic molecules with 16-256 atoms (uniform), OBC-II GB (dielectric
-80, no salt), Coulomb + Lennard-Jones with 1-2/1-3/1-4 exclusions and scaled 1-4 pairs, valence
-terms; FP32 arithmetic with int64 fixed-point forces (2^-23) and energies (2^-26).  A step is one
-force + energy evaluation of every molecule: clearing the accumulators and one fused launch.
+Headline workload (value): 1,024 distinct synthetic molecules with 16-256 atoms (uniform), OBC-II
+GB (dielectric 80, no salt), Coulomb + Lennard-Jones with 1-2/1-3/1-4 exclusions and scaled 1-4
+pairs, valence terms; FP32 arithmetic with int64 fixed-point forces (2^-23) and energies
+(2^-26).  A step is one force + energy evaluation of every molecule: clearing the accumulators
+and one fused launch.
+
+Second workload (the "minimization" object): 4,096 molecules with 24-96 atoms, starting
+coordinates perturbed by 0.3 A, 500 line-minimization cycles (50 steepest descent, then
+conjugate gradient, no clash damping), each cycle a force evaluation and three energy-only
+trial points; one step is one whole minimization of every molecule.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-N > 1 runs under torchrun, one process per GPU; each rank evaluates its own 1,024 molecules
-(weak scaling, no collective on the data path; the only collective is the max-over-ranks of the
+N > 1 runs under torchrun, one process per GPU; each rank works on its own molecules (weak
+scaling, no collective on the data path; the only collective is the max-over-ranks of the
 timing).  Rank 0 prints one JSON line.
 """
 from __future__ import annotations
@@ -29,6 +35,11 @@ sys.path.insert(0, ROOT)
 NSYS = 1024
 WORKLOAD = "batched single point: 1024 molecules, 16-256 atoms, OBC-II GB, valence + Coulomb/LJ"
 METRIC = "force-evals/s (batched single point, 1024 molecules of 16-256 atoms)"
+MIN_NSYS = 4096
+MIN_CYCLES = 500
+MIN_SD_CYCLES = 50
+MIN_WORKLOAD = ("batched conformer minimization: 4096 molecules, 24-96 atoms, 0.3 A start noise, "
+                "500 cycles (50 SD then CG), OBC-II GB")
 
 
 def _args():
@@ -39,6 +50,8 @@ def _args():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-minimization", action="store_true")
+    ap.add_argument("--min-steps", type=int, default=2)
     return ap.parse_args()
 
 
@@ -101,29 +114,62 @@ def _dist():
     return world, rank, local
 
 
-def _workload(rank: int):
+def _seed_single(rank: int) -> int:
     from stormm_b200 import synthetic
-    return synthetic.workload_batched_single_point(NSYS, seed=synthetic.SEED_BASE + 1 + 1000 * rank)
+    return synthetic.SEED_BASE + 1 + 1000 * rank
+
+
+def _seed_min(rank: int) -> int:
+    from stormm_b200 import synthetic
+    return synthetic.SEED_BASE + 2 + 1000 * rank
+
+
+def _sample_seeds(seed: int, sizes, count: int, noise: float):
+    from stormm_b200 import synthetic
+    return [(synthetic._seed(seed, k), int(sizes[k]), noise) for k in range(count)]
+
+
+def _cpu_single_point(seconds: float):
+    """STORMM's CPU evaluator on this host's cores over the first 256 molecules."""
+    import oracle.cpu_baseline as cpub
+    from stormm_b200 import synthetic
+    seed = _seed_single(0)
+    sizes = synthetic.batched_sizes(NSYS, seed=seed)
+    n = 256
+    seeds = _sample_seeds(seed, sizes, n, 0.1)
+    mols = [synthetic.make_molecule(s, k, noise=z) for (s, k, z) in seeds]
+    r = cpub.run(mols, seconds=seconds, molecule_seeds=seeds)
+    r["sample"] = (f"first {n} molecules of the workload, {seconds:.0f} s, one single-threaded "
+                   f"FP64 process per core")
+    return r
+
+
+def _cpu_minimization(seconds: float):
+    """STORMM's CPU minimizer on this host's cores over the first 128 molecules."""
+    import oracle.cpu_baseline as cpub
+    from stormm_b200 import synthetic
+    seed = _seed_min(0)
+    sizes = np.random.default_rng(seed).integers(24, 97, size=MIN_NSYS)
+    n = 128
+    seeds = _sample_seeds(seed, sizes, n, 0.3)
+    mols = [synthetic.make_molecule(s, k, noise=z) for (s, k, z) in seeds]
+    r = cpub.run(mols, seconds=seconds, minimize_cycles=MIN_CYCLES, molecule_seeds=seeds,
+                 sd_cycles=MIN_SD_CYCLES)
+    r["sample"] = (f"first {n} molecules of the workload, {MIN_CYCLES} cycles each, "
+                   f"{seconds:.0f} s, one single-threaded FP64 process per core")
+    return r
 
 
 def run_reference(args):
-    """Reference arm: STORMM's own CPU evaluator on this host's cores, same metric/config."""
+    """Reference arm: STORMM's own CPU code on this host's cores, same metric and workloads."""
     world, rank, _ = _dist()
     if rank != 0:
         return
-    import oracle.cpu_baseline as cpub
-    from stormm_b200 import synthetic
-    sizes = synthetic.batched_sizes(NSYS)
-    sample_n = 256
-    mols = [synthetic.make_molecule(synthetic._seed(synthetic.SEED_BASE + 1, k), int(sizes[k]))
-            for k in range(sample_n)]
-    seeds = [(synthetic._seed(synthetic.SEED_BASE + 1, k), int(sizes[k]), 0.1)
-             for k in range(sample_n)]
     step_seconds = max(1.0, min(4.0, 60.0 / max(1, args.steps + args.warmup)))
     values = []
     info = None
     for s in range(args.warmup + args.steps):
-        info = cpub.run(mols, seconds=step_seconds, molecule_seeds=seeds)
+        info = _cpu_single_point(step_seconds)
         if s >= args.warmup:
             values.append(info["value"])
     value = float(np.mean(values))
@@ -134,15 +180,206 @@ def run_reference(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded), first 256 molecules of the workload as the bounded sample",
         "config": {"workload": WORKLOAD, "molecules": NSYS, "atoms": "16-256",
-                   "gb": "OBC-II", "sample_molecules": sample_n},
+                   "gb": "OBC-II", "sample_molecules": 256},
         "cpu_baseline": {"value": value, "unit": "force-evals/s", "cores": info["cores"],
                          "kind": info["kind"],
-                         "sample": f"{sample_n} molecules, {step_seconds:.1f} s per step, "
+                         "sample": f"256 molecules, {step_seconds:.1f} s per step, "
                                    f"one single-threaded FP64 process per core"},
         "e2e": {"value": value, "unit": "force-evals/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    if not args.no_minimization:
+        m = _cpu_minimization(max(4.0, args.cpu_seconds))
+        line["minimization"] = {"value": m["value"], "unit": "minimizations/s",
+                                "workload": MIN_WORKLOAD, "cores": m["cores"],
+                                "kind": m["kind"], "sample": m["sample"]}
     print(json.dumps(line), flush=True)
+
+
+def _event_pair():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    t = torch.tensor([x], device="cuda")
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(world: int):
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+
+
+def bench_single_point(args, world, rank, local, flush):
+    import torch
+    import stormm_b200 as sb
+    from stormm_b200 import roofline, synthetic
+
+    mols = synthetic.workload_batched_single_point(NSYS, seed=_seed_single(rank))
+    natoms = np.array([m.natom for m in mols])
+    syn = sb.Synthesis(mols, device=local)
+    xyz = np.concatenate([m.coords for m in mols])
+    syn.set_coordinates(xyz)
+    info = syn.launch_info()
+
+    def step():
+        syn.initialize(sb.INIT_FORCES | sb.INIT_ENERGIES)
+        syn.evaluate()
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    assert syn.status() == 0
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    kbeg = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    _barrier(world)
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        flush.zero_()
+        starts[k].record()
+        syn.initialize(sb.INIT_FORCES | sb.INIT_ENERGIES)
+        kbeg[k].record()
+        syn.evaluate()
+        ends[k].record()
+    torch.cuda.synchronize()
+    _barrier(world)
+    step_ms = np.array([s.elapsed_time(e) for s, e in zip(starts, ends)])
+    kern_ms = np.array([s.elapsed_time(e) for s, e in zip(kbeg, ends)])
+    total_ms = _max_over_ranks(float(step_ms.sum()), world)
+    value = world * NSYS * args.steps / (total_ms / 1000.0)
+
+    # end to end through the C ABI with host buffers: upload coordinates, evaluate, read back
+    # forces and energies every step
+    pinned_xyz = torch.from_numpy(xyz.copy()).pin_memory().numpy()
+    for _ in range(2):
+        syn.set_coordinates(pinned_xyz)
+        step()
+        syn.forces()
+        syn.energies()
+    torch.cuda.synchronize()
+    _barrier(world)
+    t0 = time.perf_counter()
+    lat = []
+    for _ in range(args.steps):
+        ts = time.perf_counter()
+        syn.set_coordinates(pinned_xyz)
+        step()
+        f = syn.forces()
+        e = syn.energies()
+        lat.append(time.perf_counter() - ts)
+    torch.cuda.synchronize()
+    e2e_s = _max_over_ranks(time.perf_counter() - t0, world)
+    e2e_value = world * NSYS * args.steps / e2e_s
+
+    # per-system drop-in: one launch per molecule (same kernel, one molecule each)
+    per_sys = None
+    if rank == 0:
+        syn.initialize()
+        syn.evaluate_range(0, NSYS)
+        torch.cuda.synchronize()
+        ev0, ev1 = _event_pair()
+        reps = 3
+        ev0.record()
+        for _ in range(reps):
+            syn.initialize(sb.INIT_FORCES | sb.INIT_ENERGIES)
+            syn.evaluate_range(0, NSYS)
+        ev1.record()
+        torch.cuda.synchronize()
+        per_sys = NSYS * reps / (ev0.elapsed_time(ev1) / 1000.0)
+    syn.close()
+
+    flops = roofline.flops_per_evaluation(natoms, force=True)
+    kern_avg_s = float(kern_ms.mean()) / 1000.0
+    return {
+        "value": value, "total_ms": total_ms, "step_ms": step_ms, "natoms": natoms,
+        "info": info, "per_sys": per_sys, "e2e_value": e2e_value, "lat": lat,
+        "h2d": int(xyz.size * 8), "d2h": int(f.size * 8 + e.size * 8),
+        "flops": flops, "kern_avg_s": kern_avg_s,
+    }
+
+
+def bench_minimization(args, world, rank, local, flush):
+    import torch
+    import stormm_b200 as sb
+    from stormm_b200 import synthetic
+
+    mols = synthetic.workload_minimization(MIN_NSYS, seed=_seed_min(rank))
+    syn = sb.Synthesis(mols, device=local)
+    xyz = np.concatenate([m.coords for m in mols])
+    ctl = dict(total_cycles=MIN_CYCLES, sd_cycles=MIN_SD_CYCLES)
+    for _ in range(3):
+        syn.set_coordinates(xyz)
+        syn.minimize(total_cycles=5, sd_cycles=2)
+    torch.cuda.synchronize()
+    assert syn.status() == 0
+    times = []
+    _barrier(world)
+    for _ in range(args.min_steps):
+        syn.set_coordinates(xyz)
+        flush.zero_()
+        ev0, ev1 = _event_pair()
+        ev0.record()
+        syn.minimize(**ctl)
+        ev1.record()
+        torch.cuda.synchronize()
+        times.append(ev0.elapsed_time(ev1))
+    _barrier(world)
+    total_ms = _max_over_ranks(float(np.sum(times)), world)
+    value = world * MIN_NSYS * args.min_steps / (total_ms / 1000.0)
+    e_final = syn.energy_terms().sum(axis=1)
+    e_start = None
+    # end to end: pinned host coordinates in, minimize, coordinates and energies out
+    pinned_xyz = torch.from_numpy(xyz.copy()).pin_memory().numpy()
+    torch.cuda.synchronize()
+    _barrier(world)
+    t0 = time.perf_counter()
+    syn.set_coordinates(pinned_xyz)
+    syn.minimize(**ctl)
+    c = syn.coordinates()
+    e = syn.energies()
+    e2e_s = _max_over_ranks(time.perf_counter() - t0, world)
+    # per-system drop-in: one launch per molecule for the first 16 molecules
+    per_sys = None
+    if rank == 0:
+        syn.set_coordinates(xyz)
+        ev0, ev1 = _event_pair()
+        ev0.record()
+        syn.minimize_range(0, 16, **ctl)
+        ev1.record()
+        torch.cuda.synchronize()
+        per_sys = 16 / (ev0.elapsed_time(ev1) / 1000.0)
+        syn.set_coordinates(xyz)
+        syn.initialize()
+        syn.evaluate(force=False, energy=True)
+        e_start = syn.energy_terms().sum(axis=1)
+    assert syn.status() == 0
+    syn.close()
+    evals = MIN_NSYS * (4 * MIN_CYCLES + 1)
+    return {
+        "value": value, "unit": "minimizations/s", "workload": MIN_WORKLOAD,
+        "molecules_per_gpu": MIN_NSYS, "cycles": MIN_CYCLES, "sd_cycles": MIN_SD_CYCLES,
+        "clash_cycles": 0, "steps": args.min_steps, "ms_per_step": total_ms / args.min_steps,
+        "p50_ms": float(np.percentile(times, 50)), "p99_ms": float(np.percentile(times, 99)),
+        "evals_per_s": world * evals * args.min_steps / (total_ms / 1000.0),
+        "evals_per_minimization": 4 * MIN_CYCLES + 1,
+        "per_system_dropin": {"value": per_sys, "unit": "minimizations/s",
+                              "sample": "first 16 molecules, one launch each",
+                              "batched_speedup": (value / world / per_sys) if per_sys else None},
+        "e2e": {"value": world * MIN_NSYS / e2e_s, "unit": "minimizations/s",
+                "h2d_bytes_per_step": int(xyz.size * 8),
+                "d2h_bytes_per_step": int(c.size * 8 + e.size * 8)},
+        "mean_energy_drop": (float(np.mean(e_start - e_final)) if e_start is not None else None),
+        "gpu_launches_per_step": 2,
+        "l2": "flushed (256 MB write) before every timed step",
+    }
 
 
 def main():
@@ -157,131 +394,42 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    import stormm_b200 as sb
     from stormm_b200 import roofline
-
-    mols = _workload(rank)
-    natoms = np.array([m.natom for m in mols])
-    syn = sb.Synthesis(mols, device=local)
-    xyz = np.concatenate([m.coords for m in mols])
-    syn.set_coordinates(xyz)
-    info = syn.launch_info()
 
     # L2 flush buffer (> 126 MB L2), written between timed steps outside the timed events
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
-
-    def step():
-        syn.initialize(sb.INIT_FORCES | sb.INIT_ENERGIES)
-        syn.evaluate()
-
-    for _ in range(max(3, args.warmup)):
-        step()
-    torch.cuda.synchronize()
-    assert syn.status() == 0
-
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    kbeg = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
-        for k in range(args.steps):
-            flush.zero_()
-            starts[k].record()
-            syn.initialize(sb.INIT_FORCES | sb.INIT_ENERGIES)
-            kbeg[k].record()
-            syn.evaluate()
-            ends[k].record()
-        torch.cuda.synchronize()
-        if world > 1:
-            torch.distributed.barrier()
-        step_ms = np.array([s.elapsed_time(e) for s, e in zip(starts, ends)])
-        kern_ms = np.array([s.elapsed_time(e) for s, e in zip(kbeg, ends)])
-    total_ms = float(step_ms.sum())
-    if world > 1:
-        t = torch.tensor([total_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * NSYS * args.steps / (total_ms / 1000.0)
-
-    # end to end through the C ABI with host buffers: upload coordinates, evaluate, read back
-    # forces and energies every step
-    pinned_xyz = torch.from_numpy(xyz.copy()).pin_memory().numpy()
-    for _ in range(2):
-        syn.set_coordinates(pinned_xyz)
-        step()
-        syn.forces()
-        syn.energies()
-    torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
-    t0 = time.perf_counter()
-    lat = []
-    for _ in range(args.steps):
-        ts = time.perf_counter()
-        syn.set_coordinates(pinned_xyz)
-        step()
-        f = syn.forces()
-        e = syn.energies()
-        lat.append(time.perf_counter() - ts)
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * NSYS * args.steps / e2e_s
-    h2d = int(xyz.size * 8)
-    d2h = int(f.size * 8 + e.size * 8)
-
-    # per-system drop-in: one launch sequence per molecule (same kernels, one molecule each)
-    per_sys = None
-    if rank == 0:
-        syn.initialize()
-        syn.evaluate_range(0, NSYS)
-        torch.cuda.synchronize()
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        reps = 3
-        ev0.record()
-        for _ in range(reps):
-            syn.initialize(sb.INIT_FORCES | sb.INIT_ENERGIES)
-            syn.evaluate_range(0, NSYS)
-        ev1.record()
-        torch.cuda.synchronize()
-        per_sys = NSYS * reps / (ev0.elapsed_time(ev1) / 1000.0)
-
-    flops = roofline.flops_per_evaluation(natoms, force=True)
-    kern_avg_s = float(kern_ms.mean()) / 1000.0
-    achieved = flops / kern_avg_s / 1.0e12
-    peak = roofline.fp32_peak_tflops(1965.0)
+        sp = bench_single_point(args, world, rank, local, flush)
+        mn = None if args.no_minimization else bench_minimization(args, world, rank, local, flush)
     csum = clocks.summary()
+
+    achieved = sp["flops"] / sp["kern_avg_s"] / 1.0e12
+    peak = roofline.fp32_peak_tflops(1965.0)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            import oracle.cpu_baseline as cpub
-            from stormm_b200 import synthetic
-            sizes = synthetic.batched_sizes(NSYS)
-            sample_n = 256
-            sample = mols[:sample_n]
-            seeds = [(synthetic._seed(synthetic.SEED_BASE + 1, k), int(sizes[k]), 0.1)
-                     for k in range(sample_n)]
-            r = cpub.run(sample, seconds=args.cpu_seconds, molecule_seeds=seeds)
+            r = _cpu_single_point(args.cpu_seconds)
             cpu = {"value": r["value"], "unit": "force-evals/s", "cores": r["cores"],
-                   "kind": r["kind"],
-                   "sample": f"first {sample_n} molecules of the workload, "
-                             f"{args.cpu_seconds:.0f} s, one FP64 process per core"}
+                   "kind": r["kind"], "sample": r["sample"]}
+            if mn is not None:
+                rm = _cpu_minimization(args.cpu_seconds)
+                mn["cpu_baseline"] = {"value": rm["value"], "unit": "minimizations/s",
+                                      "cores": rm["cores"], "kind": rm["kind"],
+                                      "sample": rm["sample"]}
         except Exception as exc:  # reported, not fatal
             cpu = {"value": None, "unit": "force-evals/s", "cores": 0, "kind": "unavailable",
                    "sample": str(exc)[:200]}
 
     if rank == 0:
+        info = sp["info"]
+        natoms = sp["natoms"]
         line = {
-            "metric": METRIC, "value": value, "unit": "force-evals/s", "n_gpus": world,
+            "metric": METRIC, "value": sp["value"], "unit": "force-evals/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32 (int64 fixed-point accumulation)",
+            "ms_per_step": sp["total_ms"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (int64 fixed-point accumulation)",
             "data": "synthetic (seeded generator, no dataset)",
             "config": {"workload": WORKLOAD, "molecules_per_gpu": NSYS,
                        "atoms_total_per_gpu": int(natoms.sum()),
@@ -289,26 +437,28 @@ def main():
                        "dielectric": 80.0, "parallelism": f"weak x{world} (independent shards)",
                        "l2": "flushed (256 MB write) before every timed step",
                        "work_units": info["work_units"], "threads_per_block": info["threads"]},
-            "p50_ms": float(np.percentile(step_ms, 50)),
-            "p99_ms": float(np.percentile(step_ms, 99)),
-            "per_system_dropin": {"value": per_sys, "unit": "force-evals/s",
+            "p50_ms": float(np.percentile(sp["step_ms"], 50)),
+            "p99_ms": float(np.percentile(sp["step_ms"], 99)),
+            "per_system_dropin": {"value": sp["per_sys"], "unit": "force-evals/s",
                                   "launches_per_step": NSYS,
-                                  "batched_speedup": (value / world / per_sys) if per_sys else None},
-            "e2e": {"value": e2e_value, "unit": "force-evals/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h,
-                    "p50_ms": float(np.percentile(lat, 50)) * 1000.0,
-                    "p99_ms": float(np.percentile(lat, 99)) * 1000.0},
+                                  "batched_speedup": (sp["value"] / world / sp["per_sys"])
+                                  if sp["per_sys"] else None},
+            "e2e": {"value": sp["e2e_value"], "unit": "force-evals/s",
+                    "h2d_bytes_per_step": sp["h2d"], "d2h_bytes_per_step": sp["d2h"],
+                    "p50_ms": float(np.percentile(sp["lat"], 50)) * 1000.0,
+                    "p99_ms": float(np.percentile(sp["lat"], 99)) * 1000.0},
             "gpu_launches": args.steps * (1 if info["work_units"] else 0),
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
-                         "kernel": "kEvalFused", "flops_per_launch": flops,
-                         "kernel_ms": kern_avg_s * 1000.0,
-                         "peak_source": "nominal FP32 FMA pipe: 148 SM x 128 lanes x 2 x 1965 MHz"},
+                         "kernel": "kEvalFused", "flops_per_launch": sp["flops"],
+                         "kernel_ms": sp["kern_avg_s"] * 1000.0,
+                         "peak_source": "nominal FP32 FMA pipe: 148 SM x 128 lanes x 2 x "
+                                        "1965 MHz (no measured FP32 figure on this pool)"},
             "clocks": csum,
             "cpu_baseline": cpu,
+            "minimization": mn,
         }
         print(json.dumps(line), flush=True)
-    syn.close()
     if world > 1:
         torch.distributed.destroy_process_group()
 

@@ -44,7 +44,7 @@ def _write_shards(molecules, nproc, tmpdir):
 
 def _port_worker(args):
     """Evaluate molecules with the FP64 oracle for a fixed wall time (one process)."""
-    idx, seconds, minimize_cycles, seed_list = args
+    idx, seconds, minimize_cycles, sd_cycles, seed_list = args
     import oracle
     from stormm_b200 import synthetic
     mols = [synthetic.make_molecule(s, n, noise=nz) for (s, n, nz) in seed_list]
@@ -54,7 +54,7 @@ def _port_worker(args):
     k = 0
     while time.perf_counter() - t0 < seconds:
         if minimize_cycles > 0:
-            systems[k].minimize(mols[k].coords, minimize_cycles, min(50, minimize_cycles))
+            systems[k].minimize(mols[k].coords, minimize_cycles, sd_cycles)
         else:
             systems[k].evaluate(mols[k].coords)
         count += 1
@@ -63,7 +63,7 @@ def _port_worker(args):
 
 
 def run(molecules, seconds: float = 10.0, nproc: int | None = None, minimize_cycles: int = 0,
-        molecule_seeds=None):
+        molecule_seeds=None, sd_cycles: int = 50):
     """Aggregate evaluations (or minimizations) per second of the CPU baseline.
 
     molecules: the bounded sample (Molecule objects).  molecule_seeds: optional list of
@@ -75,7 +75,8 @@ def run(molecules, seconds: float = 10.0, nproc: int | None = None, minimize_cyc
     if reference_available():
         with tempfile.TemporaryDirectory() as tmp:
             lists = _write_shards(molecules, nproc, tmp)
-            extra = ["--minimize", str(minimize_cycles)] if minimize_cycles > 0 else []
+            extra = (["--minimize", str(minimize_cycles), "--ncyc", str(sd_cycles)]
+                     if minimize_cycles > 0 else [])
             procs = [subprocess.Popen([DRIVER, "time", lst, str(seconds)] + extra,
                                       stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
                      for lst in lists]
@@ -94,7 +95,7 @@ def run(molecules, seconds: float = 10.0, nproc: int | None = None, minimize_cyc
         ctx = mp.get_context("spawn")
         shards = [molecule_seeds[p::nproc] for p in range(nproc)]
         with ctx.Pool(nproc) as pool:
-            res = pool.map(_port_worker, [(p, seconds, minimize_cycles, shards[p])
+            res = pool.map(_port_worker, [(p, seconds, minimize_cycles, sd_cycles, shards[p])
                                           for p in range(nproc)])
         total = sum(r[0] for r in res)
         tmax = max(r[1] for r in res)

@@ -1,10 +1,12 @@
-"""Small, fixed profiling case for the fused evaluation kernel.
+"""Small, fixed profiling cases for the evaluation and minimization kernels.
 
   python -m stormm_b200.profile_case [--molecules 256] [--evals 4] [--energy-only]
+  python -m stormm_b200.profile_case --workload minimization --molecules 4096 --minimize 20
 
-Builds the first molecules of the batched single-point workload (16-256 atoms), uploads them and
-runs a few force + energy evaluations, so a profiler can capture single launches of the kernel
-on a case that finishes in seconds.
+The first form builds the first molecules of the batched single-point workload (16-256 atoms),
+uploads them and runs a few force + energy evaluations; the second builds the first molecules
+of the minimization workload (24-96 atoms, 0.3 A noise) and runs a short minimization.  Both
+finish in seconds, so a profiler can capture single launches of each kernel.
 """
 from __future__ import annotations
 
@@ -15,18 +17,26 @@ import numpy as np
 
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="single-point", choices=["single-point", "minimization"])
     ap.add_argument("--molecules", type=int, default=256)
     ap.add_argument("--evals", type=int, default=4)
     ap.add_argument("--energy-only", action="store_true")
+    ap.add_argument("--minimize", type=int, default=0, help="minimization cycles")
     args = ap.parse_args()
     import stormm_b200 as sb
     from stormm_b200 import synthetic
-    mols = synthetic.workload_batched_single_point(args.molecules)
+    if args.workload == "minimization":
+        mols = synthetic.workload_minimization(args.molecules)
+    else:
+        mols = synthetic.workload_batched_single_point(args.molecules)
     syn = sb.Synthesis(mols)
     syn.set_coordinates(np.concatenate([m.coords for m in mols]))
-    for _ in range(args.evals):
-        syn.initialize(sb.INIT_FORCES | sb.INIT_ENERGIES)
-        syn.evaluate(force=not args.energy_only, energy=True)
+    if args.minimize > 0:
+        syn.minimize(total_cycles=args.minimize, sd_cycles=min(50, args.minimize))
+    else:
+        for _ in range(args.evals):
+            syn.initialize(sb.INIT_FORCES | sb.INIT_ENERGIES)
+            syn.evaluate(force=not args.energy_only, energy=True)
     e = syn.energy_terms()
     if syn.status() != 0:
         raise SystemExit("device status word set")
