@@ -227,6 +227,23 @@ int sb_get_minimize_history(sb_synthesis* syn, double* history, void* stream);
 int sb_get_minimize_progress(sb_synthesis* syn, int* cycles_done, int* converged,
                              double* rms_force, void* stream);
 
+/* ------------------------------------------------------------------------------------------ */
+/* Energy export without allocation                                                            */
+/* ------------------------------------------------------------------------------------------ */
+/* No counterpart in the reference.  Converts nsys * stride int64 energies in device memory
+ * (nrg_bits fraction bits, STORMM's ScoreCard format, e.g. a synthesis' or a ScoreCard's device
+ * accumulators) to doubles in host memory through a scratch array compiled into the library,
+ * allocating nothing.  For callers that must not allocate device memory where they read
+ * energies: a loop whose device memory is committed to the work in flight, or a ScoreCard
+ * that has no synthesis handle and so no staging buffer.
+ * Limit: nsys * stride <= 65,536 values (4,096 systems of 16 slots); larger requests return
+ * SB_ERR_ARGUMENT.  The first call on each device (nsys = 0 does only this) looks up the
+ * scratch address with that device current: make it before any stream capture begins.
+ * Nothing has to be zeroed first.  Calls on one device share the scratch: calls that overlap
+ * in time race, so order them.  Synchronizes the stream before returning. */
+int sb_energies_to_host_static(const int64_t* d_energies, int nsys, int stride, int nrg_bits,
+                               double* energies, void* stream);
+
 /* Read and clear the device status word that bounded device-side waits and checks set */
 int sb_check_status(sb_synthesis* syn, int* status);
 
