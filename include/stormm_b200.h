@@ -218,6 +218,15 @@ int sb_minimize(sb_synthesis* syn, const sb_minimize_controls* ctl, void* stream
 /* Systems [first, first + count) with one launch per system: the per-system drop-in sequence */
 int sb_minimize_range(sb_synthesis* syn, int first, int count, const sb_minimize_controls* ctl,
                       void* stream);
+/* The same minimization in steps: sb_minimize_begin resets every system's minimizer state
+ * (move length dx0, no previous force or direction, zero cycles) without moving anything;
+ * each sb_minimize_advance runs up to `cycles` more cycles of every system that has neither
+ * converged nor reached total_cycles, and with final_energy nonzero re-evaluates the energies
+ * at the coordinates reached.  Begin + one advance of total_cycles equals sb_minimize, and the
+ * trajectory does not depend on how the cycles are split between advances. */
+int sb_minimize_begin(sb_synthesis* syn, const sb_minimize_controls* ctl, void* stream);
+int sb_minimize_advance(sb_synthesis* syn, int cycles, int final_energy, void* stream);
+
 /* Energy history of the last minimization that recorded one: nsys * (total_cycles + 1) doubles,
  * system-major.  Entry c is the energy at the start of cycle c; the entry after a system's last
  * cycle is its final energy (later entries stay 0 for a system that converged early). */
@@ -226,6 +235,20 @@ int sb_get_minimize_history(sb_synthesis* syn, double* history, void* stream);
  * output may be NULL. */
 int sb_get_minimize_progress(sb_synthesis* syn, int* cycles_done, int* converged,
                              double* rms_force, void* stream);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Autotuning                                                                                  */
+/* ------------------------------------------------------------------------------------------ */
+#define SB_TUNE_EVALUATE 1
+#define SB_TUNE_MINIMIZE 2
+/* Times candidate work-unit packings (atom slots and tiles per unit) of the batched evaluation
+ * or minimization kernel on this synthesis and keeps the fastest, in place of STORMM's fixed
+ * launch tables (Structure/core_kernel_manager.h:83-195).  Results do not depend on the packing.
+ * Tuning the evaluation clears forces, energies and the GB workspace; tuning the minimizer
+ * leaves coordinates as they were and requires a new sb_minimize_begin before an advance.
+ * Outputs may be NULL. */
+int sb_autotune(sb_synthesis* syn, int what, int* max_atoms_per_unit, int* max_tiles_per_unit,
+                double* best_ms, void* stream);
 
 /* ------------------------------------------------------------------------------------------ */
 /* Energy export without allocation                                                            */

@@ -17,6 +17,7 @@ LIB_PATH = os.path.join(PKG, "libstormm_b200.so")
 SB_OK = 0
 SB_GB_NONE, SB_GB_HCT, SB_GB_OBC, SB_GB_OBC2 = 0, 1, 2, 5
 TERM_VALENCE, TERM_NONBONDED, TERM_GB, TERM_ALL = 1, 2, 4, 7
+TUNE_EVALUATE, TUNE_MINIMIZE = 1, 2
 INIT_FORCES, INIT_ENERGIES, INIT_GB_WORKSPACE = 1, 2, 4
 NRG_STRIDE = 16
 # StateVariable slots (STORMM Potential/energy_enumerators.h:36-50)
@@ -108,6 +109,11 @@ def library() -> ctypes.CDLL:
             "sb_minimize_range": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int,
                                                  ctypes.POINTER(MinimizeControls), vp]),
             "sb_get_minimize_history": (ctypes.c_int, [vp, vp, vp]),
+            "sb_minimize_begin": (ctypes.c_int, [vp, ctypes.POINTER(MinimizeControls), vp]),
+            "sb_minimize_advance": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, vp]),
+            "sb_autotune": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                           ctypes.POINTER(ctypes.c_int),
+                                           ctypes.POINTER(ctypes.c_double), vp]),
             "sb_get_minimize_progress": (ctypes.c_int, [vp, vp, vp, vp, vp]),
             "sb_last_error": (ctypes.c_char_p, []),
             "sb_version": (ctypes.c_char_p, []),
@@ -320,6 +326,25 @@ class Synthesis:
         c = minimize_controls(**controls)
         self._history_stride = c.total_cycles + 1 if c.record_history else 0
         _check(library().sb_minimize(self.handle, ctypes.byref(c), stream), "sb_minimize")
+
+    def minimize_begin(self, stream=None, **controls):
+        """Reset every system's minimizer state (sb_minimize_begin)."""
+        c = minimize_controls(**controls)
+        self._history_stride = c.total_cycles + 1 if c.record_history else 0
+        _check(library().sb_minimize_begin(self.handle, ctypes.byref(c), stream),
+               "sb_minimize_begin")
+
+    def minimize_advance(self, cycles, final_energy=True, stream=None):
+        """Run up to `cycles` more cycles of every unfinished system (sb_minimize_advance)."""
+        _check(library().sb_minimize_advance(self.handle, int(cycles), int(final_energy), stream),
+               "sb_minimize_advance")
+
+    def autotune(self, what=TUNE_EVALUATE, stream=None):
+        """Pick the fastest work-unit packing; returns (atoms per unit, tiles per unit, ms)."""
+        a, t, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        _check(library().sb_autotune(self.handle, what, ctypes.byref(a), ctypes.byref(t),
+                                     ctypes.byref(ms), stream), "sb_autotune")
+        return a.value, t.value, ms.value
 
     def minimize_range(self, first, count, stream=None, **controls):
         """The same with one launch per system, systems [first, first + count)."""

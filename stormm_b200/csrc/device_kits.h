@@ -127,6 +127,7 @@ struct DevMinimizer {
   double* history;               // per system: energy at the start of each cycle (may be null)
   int hist_stride;               // history entries per system
   int sd_cycles;                 // steepest-descent cycles before conjugate gradient
+  int max_cycles;                // a system stops moving after this many cycles in total
   double drms;                   // RMS force target (kcal/mol/A), 0: none
   int* queue;                    // work-unit counter, zero before each launch
 };

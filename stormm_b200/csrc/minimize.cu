@@ -50,11 +50,12 @@ struct MinSmem {
   double* mol;    // kMolDoubles x kMaxUnitSystems
   int* cyc;       // completed cycles
   int* done;      // converged (no further moves)
+  int* act;       // moving in the current cycle: not converged, below the cycle limit
 };
 
 __host__ __device__ inline size_t minSmemBytes(int max_slots) {
   return sizeof(double) * (3 * (max_slots / kTile) + kMolDoubles * kMaxUnitSystems) +
-         sizeof(int) * 2 * kMaxUnitSystems;
+         sizeof(int) * 3 * kMaxUnitSystems;
 }
 
 __device__ MinSmem carveMinSmem(char* base, int max_slots) {
@@ -63,6 +64,7 @@ __device__ MinSmem carveMinSmem(char* base, int max_slots) {
   m.mol = m.part + 3 * (max_slots / kTile);
   m.cyc = reinterpret_cast<int*>(m.mol + kMolDoubles * kMaxUnitSystems);
   m.done = m.cyc + kMaxUnitSystems;
+  m.act = m.done + kMaxUnitSystems;
   return m;
 }
 
@@ -260,7 +262,7 @@ __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
     const double ff = moleculeSum(s, ms, k, 2) * inv_fs * inv_fs;
     const double e0 = moleculeEnergy(d, s, k);
     molValue(ms, kE0, k) = e0;
-    if (!ms.done[k]) {
+    if (ms.act[k]) {
       const double rms = sqrt(ff / (3.0 * static_cast<double>(s.natom[k])));
       m.rms_force[sysid] = rms;
       if (HIST && ms.cyc[k] < m.hist_stride) {
@@ -268,6 +270,7 @@ __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
       }
       if (m.drms > 0.0 && rms <= m.drms) {
         ms.done[k] = 1;
+        ms.act[k] = 0;
       }
     }
     // the reference advances its step counter before the gather (hpc_minimization.cu:470)
@@ -281,7 +284,7 @@ __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
     const int k = findOwner(s.slot0, us.nsys, slot);
     const int a = slot - s.slot0[k];
     double msum = 0.0;
-    if (a < s.natom[k] && !ms.done[k]) {
+    if (a < s.natom[k] && ms.act[k]) {
       const int gi = d.atom_start[s.sys[k]] + a;
       const long long ix = int63ToLong(s.fx[slot], s.fxo[slot]);
       const long long iy = int63ToLong(s.fy[slot], s.fyo[slot]);
@@ -315,7 +318,7 @@ __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
   // 3. first trial move: 1 x the move length
   if (threadIdx.x < us.nsys) {
     const int k = threadIdx.x;
-    if (!ms.done[k]) {
+    if (ms.act[k]) {
       const double msum = moleculeSum(s, ms, k, 0);
       const double inv_norm = (msum > 0.0) ? 1.0 / sqrt(msum) : 0.0;
       const double s_move = molValue(ms, kLMove, k);
@@ -339,7 +342,7 @@ __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
     const int k = threadIdx.x;
     const double e1 = moleculeEnergy(d, s, k);
     molValue(ms, kE1, k) = e1;
-    if (!ms.done[k]) {
+    if (ms.act[k]) {
       const double mfac = (e1 < molValue(ms, kE0, k)) ? 1.04 : 0.8;
       molValue(ms, kMfac, k) = mfac;
       molValue(ms, kMv2, k) = molValue(ms, kMv1, k) + mfac;
@@ -357,7 +360,7 @@ __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
     const int k = threadIdx.x;
     const double e2 = moleculeEnergy(d, s, k);
     molValue(ms, kE2, k) = e2;
-    if (!ms.done[k]) {
+    if (ms.act[k]) {
       const double mfac = molValue(ms, kMfac, k) * ((e2 < molValue(ms, kE1, k)) ? 1.03 : 0.85);
       molValue(ms, kMfac, k) = mfac;
       molValue(ms, kMv3, k) = molValue(ms, kMv2, k) + mfac;
@@ -374,7 +377,7 @@ __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
   if (threadIdx.x < us.nsys) {
     const int k = threadIdx.x;
     const double e3 = moleculeEnergy(d, s, k);
-    if (!ms.done[k]) {
+    if (ms.act[k]) {
       const double ev[4] = {molValue(ms, kE0, k), molValue(ms, kE1, k), molValue(ms, kE2, k), e3};
       const double mv[4] = {0.0, molValue(ms, kMv1, k), molValue(ms, kMv2, k),
                             molValue(ms, kMv3, k)};
@@ -421,7 +424,12 @@ kMinimize(const DevSynthesis d, const DevMinimizer m, int unit_begin, int unit_e
       }
       __syncthreads();
       for (int c = 0; c < cycles; c++) {
-        const int moving = (threadIdx.x < us.nsys) ? !ms.done[threadIdx.x] : 0;
+        int moving = 0;
+        if (threadIdx.x < us.nsys) {
+          const int k = threadIdx.x;
+          moving = (!ms.done[k] && ms.cyc[k] < m.max_cycles) ? 1 : 0;
+          ms.act[k] = moving;
+        }
         if (!__syncthreads_or(moving)) {
           break;
         }

@@ -306,13 +306,15 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
   }
 }
 
-void Synthesis::buildUnits() {
-  const int max_slots_cap = (opt.max_atoms_per_unit > 0) ? opt.max_atoms_per_unit : 256;
-  const int max_tiles_cap = (opt.max_tiles_per_unit > 0) ? opt.max_tiles_per_unit : 36;
-  threads = (opt.threads_per_block > 0) ? opt.threads_per_block : 256;
-  if (threads % 32 != 0 || threads < 64 || threads > 256) {
-    throw Error(SB_ERR_ARGUMENT, "threads per block must be a multiple of 32 in [64, 256]");
+std::unique_ptr<UnitPlan> Synthesis::makePlan(int max_slots_cap, int max_tiles_cap) const {
+  if (max_slots_cap < kTile || max_slots_cap % kTile != 0 || max_slots_cap > kMaxFusedAtoms ||
+      max_tiles_cap < 1) {
+    throw Error(SB_ERR_ARGUMENT, "work-unit caps must be a multiple of 32 atoms in [32, 2048] "
+                "and at least one tile");
   }
+  auto plan = std::make_unique<UnitPlan>();
+  plan->max_slots_cap = max_slots_cap;
+  plan->max_tiles_cap = max_tiles_cap;
   std::vector<int> order(nsys);
   for (int s = 0; s < nsys; s++) order[s] = s;
   std::stable_sort(order.begin(), order.end(),
@@ -324,12 +326,9 @@ void Synthesis::buildUnits() {
   };
   auto lj_of = [&](int s) { return 2 * h_lj_ntypes[s] * h_lj_ntypes[s]; };
   const int max_lj_cap = 2048;
-  h_units.clear();
-  h_unit_systems.clear();
+  std::vector<int4> &units = plan->units;
+  std::vector<int> &systems = plan->systems;
   // molecules above the packing cap: one unit each, at the front (largest first)
-  n_big_units = 0;
-  big_slots = 0;
-  big_lj = 0;
   size_t first_small = 0;
   while (first_small < order.size() && slots_of(order[first_small]) > max_slots_cap) {
     const int s = order[first_small];
@@ -338,42 +337,66 @@ void Synthesis::buildUnits() {
                   std::to_string(atom_count[s]) + " atoms; the fused path holds up to " +
                   std::to_string(kMaxFusedAtoms) + " atoms per molecule");
     }
-    h_units.push_back(make_int4(static_cast<int>(h_unit_systems.size()), 1, slots_of(s),
-                                tiles_of(s)));
-    h_unit_systems.push_back(s);
-    big_slots = std::max(big_slots, slots_of(s));
-    big_lj = std::max(big_lj, lj_of(s));
-    n_big_units++;
+    units.push_back(make_int4(static_cast<int>(systems.size()), 1, slots_of(s), tiles_of(s)));
+    systems.push_back(s);
+    plan->big_slots = std::max(plan->big_slots, slots_of(s));
+    plan->big_lj = std::max(plan->big_lj, lj_of(s));
+    plan->n_big++;
     first_small++;
   }
-  int4 cur = make_int4(static_cast<int>(h_unit_systems.size()), 0, 0, 0);
+  int4 cur = make_int4(static_cast<int>(systems.size()), 0, 0, 0);
   int cur_lj = 0;
-  small_slots = 0;
-  small_lj = 0;
   for (size_t oi = first_small; oi < order.size(); oi++) {
     const int s = order[oi];
     const bool fits = cur.y > 0 && cur.y < kMaxUnitSystems &&
                       cur.z + slots_of(s) <= max_slots_cap &&
                       cur.w + tiles_of(s) <= max_tiles_cap && cur_lj + lj_of(s) <= max_lj_cap;
     if (!fits && cur.y > 0) {
-      h_units.push_back(cur);
-      small_lj = std::max(small_lj, cur_lj);
-      small_slots = std::max(small_slots, cur.z);
-      cur = make_int4(static_cast<int>(h_unit_systems.size()), 0, 0, 0);
+      units.push_back(cur);
+      plan->small_lj = std::max(plan->small_lj, cur_lj);
+      plan->small_slots = std::max(plan->small_slots, cur.z);
+      cur = make_int4(static_cast<int>(systems.size()), 0, 0, 0);
       cur_lj = 0;
     }
-    h_unit_systems.push_back(s);
+    systems.push_back(s);
     cur.y++;
     cur.z += slots_of(s);
     cur.w += tiles_of(s);
     cur_lj += lj_of(s);
   }
   if (cur.y > 0) {
-    h_units.push_back(cur);
-    small_lj = std::max(small_lj, cur_lj);
-    small_slots = std::max(small_slots, cur.z);
+    units.push_back(cur);
+    plan->small_lj = std::max(plan->small_lj, cur_lj);
+    plan->small_slots = std::max(plan->small_slots, cur.z);
   }
+  const size_t smem = fusedSmemBytes(std::max(plan->big_slots, plan->small_slots),
+                                     std::max(plan->big_lj, plan->small_lj));
+  if (static_cast<int>(smem) > max_smem_optin) {
+    throw Error(SB_ERR_ARGUMENT, "work units need " + std::to_string(smem) +
+                " bytes of shared memory, above the device limit");
+  }
+  plan->d_units.upload(units);
+  plan->d_systems.upload(systems);
+  return plan;
+}
+
+void Synthesis::buildUnits() {
+  threads = (opt.threads_per_block > 0) ? opt.threads_per_block : 256;
+  if (threads % 32 != 0 || threads < 64 || threads > 256) {
+    throw Error(SB_ERR_ARGUMENT, "threads per block must be a multiple of 32 in [64, 256]");
+  }
+  const int slots_cap = (opt.max_atoms_per_unit > 0) ? opt.max_atoms_per_unit : 256;
+  const int tiles_cap = (opt.max_tiles_per_unit > 0) ? opt.max_tiles_per_unit : 36;
+  eval_plan = makePlan(slots_cap, tiles_cap);
+  // minimization keeps whole molecules on chip for hundreds of cycles: smaller units balance
+  // the persistent grid better (sb_autotune can choose another packing)
+  min_plan = makePlan(128, 16);
   // one unit per system, in system order, for the per-system launches
+  auto slots_of = [&](int s) { return (atom_count[s] + kTile - 1) / kTile * kTile; };
+  auto tiles_of = [&](int s) {
+    const int nb = (atom_count[s] + kTile - 1) / kTile;
+    return nb * (nb + 1) / 2;
+  };
   h_single_units.resize(nsys);
   h_single_systems.resize(nsys);
   single_slots = 0;
@@ -382,14 +405,12 @@ void Synthesis::buildUnits() {
     h_single_units[s] = make_int4(s, 1, slots_of(s), tiles_of(s));
     h_single_systems[s] = s;
     single_slots = std::max(single_slots, slots_of(s));
-    single_lj = std::max(single_lj, lj_of(s));
+    single_lj = std::max(single_lj, 2 * h_lj_ntypes[s] * h_lj_ntypes[s]);
   }
-  max_unit_slots = std::max(std::max(big_slots, small_slots), single_slots);
-  max_lj = std::max(std::max(big_lj, small_lj), single_lj);
-  const size_t smem = fusedSmemBytes(max_unit_slots, max_lj);
-  if (static_cast<int>(smem) > max_smem_optin) {
-    throw Error(SB_ERR_ARGUMENT, "work units need " + std::to_string(smem) +
-                " bytes of shared memory, above the device limit");
+  max_unit_slots = single_slots;
+  max_lj = single_lj;
+  if (static_cast<int>(fusedSmemBytes(single_slots, single_lj)) > max_smem_optin) {
+    throw Error(SB_ERR_ARGUMENT, "a molecule needs more shared memory than the device has");
   }
 }
 
@@ -418,8 +439,6 @@ void Synthesis::upload() {
   d_dihe_b.upload(h_dihe_b);
   d_tile_mask_idx.upload(h_tile_mask_idx);
   d_mask_pool.upload(h_mask_pool);
-  d_units.upload(h_units);
-  d_unit_systems.upload(h_unit_systems);
   d_single_units.upload(h_single_units);
   d_single_systems.upload(h_single_systems);
   d_unpadded_map.upload(h_unpadded_map);
@@ -496,11 +515,30 @@ void Synthesis::upload() {
   d.sumdeijda = d_sumdeijda.p;
   d.sumdeijda_ovrf = d_sumdeijda_ovrf.p;
   d.born_radii = d_born_radii.p;
-  d.nunit = h_units.size();
-  d.unit_desc = d_units.p;
-  d.unit_systems = d_unit_systems.p;
+  d.nunit = eval_plan->units.size();
+  d.unit_desc = eval_plan->d_units.p;
+  d.unit_systems = eval_plan->d_systems.p;
   d.max_unit_slots = max_unit_slots;
   d.status = d_status.p;
+}
+
+void Synthesis::launchPlan(const UnitPlan &plan, int terms, bool force, bool energy,
+                           cudaStream_t stream) {
+  const int nunit = plan.units.size();
+  DevSynthesis d = dev;
+  d.nunit = nunit;
+  d.unit_desc = plan.d_units.p;
+  d.unit_systems = plan.d_systems.p;
+  if (plan.n_big > 0) {
+    d.max_unit_slots = plan.big_slots;
+    cudaCheck(launchEvalFused(d, 0, plan.n_big, plan.big_lj, terms, force, energy, plan.n_big,
+                              threads, stream), "fused evaluation launch (large molecules)");
+  }
+  if (nunit > plan.n_big) {
+    d.max_unit_slots = plan.small_slots;
+    cudaCheck(launchEvalFused(d, plan.n_big, nunit, plan.small_lj, terms, force, energy,
+                              nunit - plan.n_big, threads, stream), "fused evaluation launch");
+  }
 }
 
 void Synthesis::evaluate(int terms, bool force, bool energy, cudaStream_t stream) {
@@ -510,19 +548,7 @@ void Synthesis::evaluate(int terms, bool force, bool energy, cudaStream_t stream
   if (!force && !energy) {
     return;
   }
-  const int nunit = h_units.size();
-  if (n_big_units > 0) {
-    DevSynthesis d = dev;
-    d.max_unit_slots = big_slots;
-    cudaCheck(launchEvalFused(d, 0, n_big_units, big_lj, terms, force, energy, n_big_units,
-                              threads, stream), "fused evaluation launch (large molecules)");
-  }
-  if (nunit > n_big_units) {
-    DevSynthesis d = dev;
-    d.max_unit_slots = small_slots;
-    cudaCheck(launchEvalFused(d, n_big_units, nunit, small_lj, terms, force, energy,
-                              nunit - n_big_units, threads, stream), "fused evaluation launch");
-  }
+  launchPlan(*eval_plan, terms, force, energy, stream);
 }
 
 void Synthesis::evaluateRange(int first, int count, int terms, bool force, bool energy,
@@ -668,7 +694,7 @@ int Synthesis::checkStatus(cudaStream_t stream) {
 // ------------------------------------------------------------------------------------------------
 // Line minimization (MolecularMechanics/hpc_minimization.cu:129-600)
 // ------------------------------------------------------------------------------------------------
-DevMinimizer Synthesis::prepareMinimizer(const sb_minimize_controls &ctl, cudaStream_t stream) {
+void Synthesis::minimizeBegin(const sb_minimize_controls &ctl, cudaStream_t stream) {
   if (ctl.total_cycles < 0 || ctl.sd_cycles < 0) {
     throw Error(SB_ERR_ARGUMENT, "cycle counts must not be negative");
   }
@@ -702,7 +728,7 @@ DevMinimizer Synthesis::prepareMinimizer(const sb_minimize_controls &ctl, cudaSt
     }
     cudaCheck(cudaMemsetAsync(d_history.p, 0, need * sizeof(double), stream), "memset");
   }
-  DevMinimizer m;
+  DevMinimizer &m = dev_min;
   std::memset(&m, 0, sizeof(DevMinimizer));
   m.xcrd = d_xcrd.p;
   m.ycrd = d_ycrd.p;
@@ -720,33 +746,52 @@ DevMinimizer Synthesis::prepareMinimizer(const sb_minimize_controls &ctl, cudaSt
   m.history = ctl.record_history ? d_history.p : nullptr;
   m.hist_stride = history_stride;
   m.sd_cycles = ctl.sd_cycles;
+  m.max_cycles = ctl.total_cycles;
   m.drms = ctl.convergence_rms;
   m.queue = d_queue.p;
   cudaCheck(launchMinimizerReset(m, dev, ctl.initial_step, stream), "minimizer reset");
-  return m;
+  min_ready = true;
+}
+
+void Synthesis::launchMinPlan(const UnitPlan &plan, int cycles, bool final_energy,
+                              cudaStream_t stream) {
+  DevMinimizer m = dev_min;
+  cudaCheck(cudaMemsetAsync(d_queue.p, 0, 2 * sizeof(int), stream), "memset");
+  const int nunit = plan.units.size();
+  DevSynthesis d = dev;
+  d.nunit = nunit;
+  d.unit_desc = plan.d_units.p;
+  d.unit_systems = plan.d_systems.p;
+  if (plan.n_big > 0) {
+    d.max_unit_slots = plan.big_slots;
+    m.queue = d_queue.p;
+    if (static_cast<int>(minimizeSmemBytes(plan.big_slots, plan.big_lj)) > max_smem_optin) {
+      throw Error(SB_ERR_UNSUPPORTED, "a molecule is too large for on-chip minimization");
+    }
+    cudaCheck(launchMinimize(d, m, 0, plan.n_big, plan.big_lj, cycles, final_energy, threads,
+                             sm_count, stream), "minimization launch (large molecules)");
+  }
+  if (nunit > plan.n_big) {
+    d.max_unit_slots = plan.small_slots;
+    m.queue = d_queue.p + 1;
+    cudaCheck(launchMinimize(d, m, plan.n_big, nunit, plan.small_lj, cycles, final_energy,
+                             threads, sm_count, stream), "minimization launch");
+  }
+}
+
+void Synthesis::minimizeAdvance(int cycles, bool final_energy, cudaStream_t stream) {
+  if (!min_ready) {
+    throw Error(SB_ERR_ARGUMENT, "no minimization has begun on this synthesis");
+  }
+  if (cycles < 0) {
+    throw Error(SB_ERR_ARGUMENT, "cycle count must not be negative");
+  }
+  launchMinPlan(*min_plan, cycles, final_energy, stream);
 }
 
 void Synthesis::minimize(const sb_minimize_controls &ctl, cudaStream_t stream) {
-  DevMinimizer m = prepareMinimizer(ctl, stream);
-  cudaCheck(cudaMemsetAsync(d_queue.p, 0, 2 * sizeof(int), stream), "memset");
-  const int nunit = h_units.size();
-  if (n_big_units > 0) {
-    DevSynthesis d = dev;
-    d.max_unit_slots = big_slots;
-    m.queue = d_queue.p;
-    if (static_cast<int>(minimizeSmemBytes(big_slots, big_lj)) > max_smem_optin) {
-      throw Error(SB_ERR_UNSUPPORTED, "a molecule is too large for on-chip minimization");
-    }
-    cudaCheck(launchMinimize(d, m, 0, n_big_units, big_lj, ctl.total_cycles, true, threads,
-                             sm_count, stream), "minimization launch (large molecules)");
-  }
-  if (nunit > n_big_units) {
-    DevSynthesis d = dev;
-    d.max_unit_slots = small_slots;
-    m.queue = d_queue.p + 1;
-    cudaCheck(launchMinimize(d, m, n_big_units, nunit, small_lj, ctl.total_cycles, true, threads,
-                             sm_count, stream), "minimization launch");
-  }
+  minimizeBegin(ctl, stream);
+  launchMinPlan(*min_plan, ctl.total_cycles, true, stream);
 }
 
 void Synthesis::minimizeRange(int first, int count, const sb_minimize_controls &ctl,
@@ -754,7 +799,7 @@ void Synthesis::minimizeRange(int first, int count, const sb_minimize_controls &
   if (first < 0 || count < 0 || first + count > nsys) {
     throw Error(SB_ERR_ARGUMENT, "system range out of bounds");
   }
-  DevMinimizer m = prepareMinimizer(ctl, stream);
+  minimizeBegin(ctl, stream);
   DevSynthesis d = dev;
   d.unit_desc = d_single_units.p;
   d.unit_systems = d_single_systems.p;
@@ -765,8 +810,98 @@ void Synthesis::minimizeRange(int first, int count, const sb_minimize_controls &
   }
   // one block per launch: the unit counter is never consulted for a second unit
   for (int s = first; s < first + count; s++) {
-    cudaCheck(launchMinimize(d, m, s, s + 1, single_lj, ctl.total_cycles, true, threads,
+    cudaCheck(launchMinimize(d, dev_min, s, s + 1, single_lj, ctl.total_cycles, true, threads,
                              sm_count, stream), "per-system minimization launch");
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Autotuning of the work-unit packing (in place of CoreKlManager's fixed launch tables,
+// Structure/core_kernel_manager.cpp:538-600).  Results do not depend on the packing (every sum
+// is per molecule and order-independent), so the fastest candidate is simply kept.
+// ------------------------------------------------------------------------------------------------
+void Synthesis::autotune(int what, int* chosen_slots, int* chosen_tiles, double* best_ms,
+                         cudaStream_t stream) {
+  if (what != SB_TUNE_EVALUATE && what != SB_TUNE_MINIMIZE) {
+    throw Error(SB_ERR_ARGUMENT, "autotune target must be SB_TUNE_EVALUATE or SB_TUNE_MINIMIZE");
+  }
+  static const int kCandidates[][2] = {{256, 36}, {256, 24}, {192, 21}, {160, 15}, {128, 16},
+                                       {128, 10}, {96, 12}, {96, 6}, {64, 6}};
+  cudaEvent_t e0, e1;
+  cudaCheck(cudaEventCreate(&e0), "cudaEventCreate");
+  cudaCheck(cudaEventCreate(&e1), "cudaEventCreate");
+  // the minimizer moves coordinates: keep a copy to restore between candidates
+  const size_t np = natom_padded;
+  DeviceArray<long long> keep;
+  auto copy3 = [&](long long* dx, long long* dy, long long* dz, const long long* sx,
+                   const long long* sy, const long long* sz) {
+    cudaCheck(cudaMemcpyAsync(dx, sx, np * 8, cudaMemcpyDeviceToDevice, stream), "copy");
+    cudaCheck(cudaMemcpyAsync(dy, sy, np * 8, cudaMemcpyDeviceToDevice, stream), "copy");
+    cudaCheck(cudaMemcpyAsync(dz, sz, np * 8, cudaMemcpyDeviceToDevice, stream), "copy");
+  };
+  if (what == SB_TUNE_MINIMIZE) {
+    keep.allocate(3 * np);
+    copy3(keep.p, keep.p + np, keep.p + 2 * np, d_xcrd.p, d_ycrd.p, d_zcrd.p);
+  }
+  sb_minimize_controls ctl;
+  sb_default_minimize_controls(&ctl);
+  ctl.total_cycles = 8;
+  ctl.sd_cycles = 4;
+  double best = 1.0e30;
+  std::unique_ptr<UnitPlan> best_plan;
+  for (const auto &c : kCandidates) {
+    std::unique_ptr<UnitPlan> plan;
+    try {
+      plan = makePlan(c[0], c[1]);
+    }
+    catch (const Error &) {
+      continue;   // a candidate that does not fit this synthesis
+    }
+    float ms = 0.0f;
+    if (what == SB_TUNE_EVALUATE) {
+      launchPlan(*plan, SB_TERM_ALL, true, true, stream);
+      cudaCheck(cudaEventRecord(e0, stream), "cudaEventRecord");
+      for (int r = 0; r < 3; r++) {
+        launchPlan(*plan, SB_TERM_ALL, true, true, stream);
+      }
+      cudaCheck(cudaEventRecord(e1, stream), "cudaEventRecord");
+    }
+    else {
+      minimizeBegin(ctl, stream);
+      cudaCheck(cudaEventRecord(e0, stream), "cudaEventRecord");
+      launchMinPlan(*plan, ctl.total_cycles, false, stream);
+      cudaCheck(cudaEventRecord(e1, stream), "cudaEventRecord");
+      copy3(d_xcrd.p, d_ycrd.p, d_zcrd.p, keep.p, keep.p + np, keep.p + 2 * np);
+    }
+    cudaCheck(cudaEventSynchronize(e1), "cudaEventSynchronize");
+    cudaCheck(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+    if (ms < best) {
+      best = ms;
+      best_plan = std::move(plan);
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (what == SB_TUNE_EVALUATE) {
+    // the candidates' evaluations accumulated into forces and energies: clear them
+    initialize(SB_INIT_FORCES | SB_INIT_ENERGIES | SB_INIT_GB_WORKSPACE, stream);
+  }
+  cudaCheck(cudaStreamSynchronize(stream), "autotune");
+  if (!best_plan) {
+    throw Error(SB_ERR_ARGUMENT, "no work-unit packing fits this synthesis");
+  }
+  if (chosen_slots) *chosen_slots = best_plan->max_slots_cap;
+  if (chosen_tiles) *chosen_tiles = best_plan->max_tiles_cap;
+  if (best_ms) *best_ms = best;
+  if (what == SB_TUNE_EVALUATE) {
+    eval_plan = std::move(best_plan);
+    dev.nunit = eval_plan->units.size();
+    dev.unit_desc = eval_plan->d_units.p;
+    dev.unit_systems = eval_plan->d_systems.p;
+  }
+  else {
+    min_plan = std::move(best_plan);
+    min_ready = false;
   }
 }
 
@@ -968,8 +1103,8 @@ int sb_launch_valence(sb_synthesis* syn, int eval_force, int eval_energy, void* 
 int sb_launch_info(const sb_synthesis* syn, int* work_units, int* blocks, int* threads) {
   return guarded([&]() {
     const sb::Synthesis* s = need(syn);
-    if (work_units) *work_units = s->h_units.size();
-    if (blocks) *blocks = s->h_units.size();
+    if (work_units) *work_units = s->eval_plan->units.size();
+    if (blocks) *blocks = s->eval_plan->units.size();
     if (threads) *threads = s->threads;
   });
 }
@@ -1003,6 +1138,26 @@ int sb_minimize_range(sb_synthesis* syn, int first, int count, const sb_minimize
   return guarded([&]() {
     if (ctl == nullptr) throw sb::Error(SB_ERR_ARGUMENT, "null minimization controls");
     need(syn)->minimizeRange(first, count, *ctl, asStream(stream));
+  });
+}
+
+int sb_minimize_begin(sb_synthesis* syn, const sb_minimize_controls* ctl, void* stream) {
+  return guarded([&]() {
+    if (ctl == nullptr) throw sb::Error(SB_ERR_ARGUMENT, "null minimization controls");
+    need(syn)->minimizeBegin(*ctl, asStream(stream));
+  });
+}
+
+int sb_minimize_advance(sb_synthesis* syn, int cycles, int final_energy, void* stream) {
+  return guarded([&]() {
+    need(syn)->minimizeAdvance(cycles, final_energy != 0, asStream(stream));
+  });
+}
+
+int sb_autotune(sb_synthesis* syn, int what, int* max_atoms_per_unit, int* max_tiles_per_unit,
+                double* best_ms, void* stream) {
+  return guarded([&]() {
+    need(syn)->autotune(what, max_atoms_per_unit, max_tiles_per_unit, best_ms, asStream(stream));
   });
 }
 

@@ -11,6 +11,7 @@
 
 #include <cuda_runtime.h>
 
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -64,6 +65,19 @@ template <typename T> struct DeviceArray {
   }
 };
 
+// Packing of molecules into work units and the launch parameters of each size class
+struct UnitPlan {
+  int max_slots_cap = 0;
+  int max_tiles_cap = 0;
+  std::vector<int4> units;       // x = first index in systems, y = count, z = slots, w = tiles
+  std::vector<int> systems;
+  int n_big = 0;                 // units [0, n_big) hold one molecule above the packing cap
+  int big_slots = 0, big_lj = 0;
+  int small_slots = 0, small_lj = 0;
+  DeviceArray<int4> d_units;
+  DeviceArray<int> d_systems;
+};
+
 class Synthesis {
 public:
   Synthesis(const sb_topology* tops, int ntop, const int* topology_index, int nsys,
@@ -82,6 +96,10 @@ public:
   void getGbWorkspace(double* psi, double* radii, double* sde, cudaStream_t stream);
   int checkStatus(cudaStream_t stream);
   void minimize(const sb_minimize_controls &ctl, cudaStream_t stream);
+  void minimizeBegin(const sb_minimize_controls &ctl, cudaStream_t stream);
+  void minimizeAdvance(int cycles, bool final_energy, cudaStream_t stream);
+  void autotune(int what, int* chosen_slots, int* chosen_tiles, double* best_ms,
+                cudaStream_t stream);
   void minimizeRange(int first, int count, const sb_minimize_controls &ctl, cudaStream_t stream);
   void getMinimizeHistory(double* out, cudaStream_t stream);
   void getMinimizeProgress(int* cycles, int* converged, double* rms, cudaStream_t stream);
@@ -95,9 +113,8 @@ public:
   int threads = 256;
   int max_lj = 0;
   int max_unit_slots = 0;
-  int n_big_units = 0;       // units [0, n_big_units) hold one molecule above the packing cap
-  int big_slots = 0, big_lj = 0;
-  int small_slots = 0, small_lj = 0;
+  std::unique_ptr<UnitPlan> eval_plan;   // batched evaluation
+  std::unique_ptr<UnitPlan> min_plan;    // batched minimization
   int single_slots = 0, single_lj = 0;
   std::vector<int> topo;
   std::vector<int> atom_start;
@@ -110,8 +127,8 @@ public:
   std::vector<float2> h_ljab, h_ljab14;
   std::vector<uint4> h_bonds, h_angles, h_dihe_a, h_dihe_b;
   std::vector<unsigned int> h_mask_pool;
-  std::vector<int4> h_units, h_single_units;
-  std::vector<int> h_unit_systems, h_single_systems;
+  std::vector<int4> h_single_units;
+  std::vector<int> h_single_systems;
   std::vector<long long> h_stage_ll;
   std::vector<int> h_unpadded_map;   // padded index of each unpadded atom
 
@@ -122,8 +139,8 @@ public:
   DeviceArray<float2> d_ljab, d_ljab14;
   DeviceArray<uint4> d_bonds, d_angles, d_dihe_a, d_dihe_b;
   DeviceArray<unsigned int> d_mask_pool;
-  DeviceArray<int4> d_units, d_single_units;
-  DeviceArray<int> d_unit_systems, d_single_systems;
+  DeviceArray<int4> d_single_units;
+  DeviceArray<int> d_single_systems;
   DeviceArray<long long> d_xcrd, d_ycrd, d_zcrd, d_xfrc, d_yfrc, d_zfrc;
   DeviceArray<int> d_xcrd_ovrf, d_ycrd_ovrf, d_zcrd_ovrf, d_xfrc_ovrf, d_yfrc_ovrf, d_zfrc_ovrf;
   DeviceArray<unsigned long long> d_energies;
@@ -139,12 +156,16 @@ public:
   DeviceArray<double> d_lmove, d_rmsf, d_history;
   DeviceArray<int> d_mcycle, d_mdone, d_queue;
   int history_stride = 0;
+  DevMinimizer dev_min{};
+  bool min_ready = false;
 
   DevSynthesis dev;
 
 private:
   void buildLayout(const sb_topology* tops, int ntop);
-  DevMinimizer prepareMinimizer(const sb_minimize_controls &ctl, cudaStream_t stream);
+  std::unique_ptr<UnitPlan> makePlan(int max_slots_cap, int max_tiles_cap) const;
+  void launchPlan(const UnitPlan &plan, int terms, bool force, bool energy, cudaStream_t stream);
+  void launchMinPlan(const UnitPlan &plan, int cycles, bool final_energy, cudaStream_t stream);
   void buildUnits();
   void upload();
 };

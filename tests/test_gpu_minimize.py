@@ -134,3 +134,52 @@ def test_clash_damping_is_rejected():
     syn.set_coordinates(mol.coords)
     with pytest.raises(sb.StormmB200Error):
         syn.minimize(total_cycles=5, clash_cycles=2)
+
+
+def test_stepwise_advance_equals_one_shot():
+    mols = [synthetic.make_molecule(synthetic._seed(2718, k), 20 + 17 * k, 0.3) for k in range(5)]
+    xyz = np.concatenate([m.coords for m in mols])
+    syn = sb.Synthesis(mols)
+    syn.set_coordinates(xyz)
+    syn.minimize(total_cycles=45, sd_cycles=10, convergence_rms=0.05)
+    c_ref = syn.coordinates().copy()
+    e_ref = syn.energies_fixed().copy()
+    prog_ref = syn.minimize_progress()
+    syn.set_coordinates(xyz)
+    syn.minimize_begin(total_cycles=45, sd_cycles=10, convergence_rms=0.05)
+    for chunk in (7, 13, 1, 30):
+        syn.minimize_advance(chunk, final_energy=False)
+    syn.minimize_advance(0, final_energy=True)
+    assert np.array_equal(syn.coordinates(), c_ref)
+    assert np.array_equal(syn.energies_fixed(), e_ref)
+    prog = syn.minimize_progress()
+    assert np.array_equal(prog[0], prog_ref[0]) and np.array_equal(prog[1], prog_ref[1])
+    assert np.all(prog[0] <= 45)
+
+
+def test_autotune_keeps_results():
+    mols = [synthetic.make_molecule(synthetic._seed(1618, k), n, 0.3)
+            for k, n in enumerate([24, 40, 64, 96, 130, 200, 256, 300])]
+    xyz = np.concatenate([m.coords for m in mols])
+    syn = sb.Synthesis(mols)
+    syn.set_coordinates(xyz)
+    syn.initialize()
+    syn.evaluate()
+    f_ref = syn.forces_fixed()
+    e_ref = syn.energies_fixed().copy()
+    syn.minimize(total_cycles=20, sd_cycles=5)
+    c_min = syn.coordinates().copy()
+    slots, tiles, ms = syn.autotune(sb.TUNE_EVALUATE)
+    assert slots % 32 == 0 and tiles > 0 and ms > 0
+    syn.set_coordinates(xyz)
+    syn.initialize()
+    syn.evaluate()
+    f = syn.forces_fixed()
+    assert np.array_equal(f[0], f_ref[0]) and np.array_equal(f[1], f_ref[1])
+    assert np.array_equal(syn.energies_fixed(), e_ref)
+    before = syn.coordinates().copy()
+    syn.autotune(sb.TUNE_MINIMIZE)
+    assert np.array_equal(syn.coordinates(), before)
+    syn.set_coordinates(xyz)
+    syn.minimize(total_cycles=20, sd_cycles=5)
+    assert np.array_equal(syn.coordinates(), c_min)
