@@ -237,6 +237,71 @@ int sb_get_minimize_progress(sb_synthesis* syn, int* cycles_done, int* converged
                              double* rms_force, void* stream);
 
 /* ------------------------------------------------------------------------------------------ */
+/* Request server: continuous batching of minimization requests                                */
+/* ------------------------------------------------------------------------------------------ */
+/* No single counterpart in the reference: it serves conformer-minimization requests the way
+ * apps/Conf/src/conformer.cpp:118-172 drives launchMinimization, but as a stream.  A worker
+ * thread admits queued requests into batches while an HBM budget allows, keeps each batch's
+ * topology, coordinates and minimizer state resident on the device, runs its minimization in
+ * launches of cycles_per_launch cycles on a stream of its own (batches overlap on the GPU),
+ * retires every molecule that converged or reached total_cycles after each launch, and
+ * backfills: new batches start while older ones are still running.  A molecule's result does
+ * not depend on the batch it ran in. */
+#define SB_TIMEOUT 1            /* sb_server_drain: work still in flight when time ran out */
+
+typedef struct {
+  sb_options options;                /* GB model, fixed-point bits, device */
+  sb_minimize_controls controls;     /* per request: cycle cap, convergence target, ... */
+  double hbm_budget_bytes;           /* device memory for molecules in flight (estimated) */
+  int max_batch_molecules;           /* most molecules admitted into one batch */
+  int max_batches;                   /* batches in flight at once, one CUDA stream each */
+  int cycles_per_launch;             /* minimization cycles per launch of a batch */
+} sb_server_options;
+
+typedef struct {
+  long long request_id;
+  int natom;
+  int cycles;                        /* line-minimization cycles run */
+  int converged;                     /* nonzero: the RMS force met controls.convergence_rms */
+  double rms_force;                  /* kcal/mol/A at the start of the last cycle */
+  double energy;                     /* total potential energy at the final coordinates */
+  double energies[SB_NRG_STRIDE];    /* the terms, StateVariable order */
+  double submit_time;                /* seconds since the server started */
+  double admit_time;
+  double finish_time;
+} sb_served_result;
+
+typedef struct {
+  long long submitted;
+  long long admitted;
+  long long completed;
+  int pending;                       /* queued, not yet admitted */
+  int in_flight;                     /* admitted molecules still minimizing */
+  int batches;
+  double bytes_in_flight;
+} sb_server_stats;
+
+typedef struct sb_server sb_server;
+
+/* Defaults: OBC-II, controls as sb_default_minimize_controls with total_cycles 2000 and
+ * convergence_rms 0.01, 2 GB budget, 512 molecules per batch, 16 batches, 50 cycles a launch */
+void sb_default_server_options(sb_server_options* opt);
+int sb_server_create(const sb_server_options* opt, sb_server** out);
+/* Queue one molecule (topology and coordinates are copied); thread-safe */
+int sb_server_submit(sb_server* srv, const sb_topology* top, const double* xyz,
+                     long long* request_id);
+/* Completed requests, oldest first: up to max_results, each with its final coordinates packed
+ * into xyz (natom * 3 doubles per result, in result order) while xyz_capacity doubles last;
+ * xyz may be NULL to take results without coordinates.  *count receives the number returned. */
+int sb_server_poll(sb_server* srv, sb_served_result* results, int max_results, double* xyz,
+                   long long xyz_capacity, int* count);
+/* Wait until nothing is queued or in flight: SB_OK, or SB_TIMEOUT after timeout_seconds */
+int sb_server_drain(sb_server* srv, double timeout_seconds);
+int sb_server_get_stats(sb_server* srv, sb_server_stats* stats);
+/* Stops the worker after the launches in flight and releases everything */
+int sb_server_destroy(sb_server* srv);
+
+/* ------------------------------------------------------------------------------------------ */
 /* Autotuning                                                                                  */
 /* ------------------------------------------------------------------------------------------ */
 #define SB_TUNE_EVALUATE 1

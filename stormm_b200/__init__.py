@@ -61,6 +61,31 @@ class MinimizeControls(ctypes.Structure):
     ]
 
 
+class ServerOptions(ctypes.Structure):
+    _fields_ = [
+        ("options", Options), ("controls", MinimizeControls),
+        ("hbm_budget_bytes", ctypes.c_double), ("max_batch_molecules", ctypes.c_int),
+        ("max_batches", ctypes.c_int), ("cycles_per_launch", ctypes.c_int),
+    ]
+
+
+class ServedResult(ctypes.Structure):
+    _fields_ = [
+        ("request_id", ctypes.c_longlong), ("natom", ctypes.c_int), ("cycles", ctypes.c_int),
+        ("converged", ctypes.c_int), ("rms_force", ctypes.c_double), ("energy", ctypes.c_double),
+        ("energies", ctypes.c_double * 16), ("submit_time", ctypes.c_double),
+        ("admit_time", ctypes.c_double), ("finish_time", ctypes.c_double),
+    ]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("submitted", ctypes.c_longlong), ("admitted", ctypes.c_longlong),
+        ("completed", ctypes.c_longlong), ("pending", ctypes.c_int), ("in_flight", ctypes.c_int),
+        ("batches", ctypes.c_int), ("bytes_in_flight", ctypes.c_double),
+    ]
+
+
 class StormmB200Error(RuntimeError):
     pass
 
@@ -115,6 +140,16 @@ def library() -> ctypes.CDLL:
                                            ctypes.POINTER(ctypes.c_int),
                                            ctypes.POINTER(ctypes.c_double), vp]),
             "sb_get_minimize_progress": (ctypes.c_int, [vp, vp, vp, vp, vp]),
+            "sb_default_server_options": (None, [ctypes.POINTER(ServerOptions)]),
+            "sb_server_create": (ctypes.c_int, [ctypes.POINTER(ServerOptions),
+                                                ctypes.POINTER(vp)]),
+            "sb_server_submit": (ctypes.c_int, [vp, ctypes.POINTER(Topology), vp,
+                                                ctypes.POINTER(ctypes.c_longlong)]),
+            "sb_server_poll": (ctypes.c_int, [vp, ctypes.POINTER(ServedResult), ctypes.c_int, vp,
+                                              ctypes.c_longlong, ctypes.POINTER(ctypes.c_int)]),
+            "sb_server_drain": (ctypes.c_int, [vp, ctypes.c_double]),
+            "sb_server_get_stats": (ctypes.c_int, [vp, ctypes.POINTER(ServerStats)]),
+            "sb_server_destroy": (ctypes.c_int, [vp]),
             "sb_last_error": (ctypes.c_char_p, []),
             "sb_version": (ctypes.c_char_p, []),
         }
@@ -387,3 +422,92 @@ class Synthesis:
     def split(self, per_atom):
         """Split a per-atom array of the whole synthesis into per-system arrays."""
         return [per_atom[self.offsets[k]:self.offsets[k + 1]] for k in range(self.nsys)]
+
+
+SB_TIMEOUT = 1
+
+
+class Server:
+    """Continuous-batching minimization server (sb_server_*).  Submit molecules at any time;
+    completed requests come back from poll() with their final coordinates."""
+
+    def __init__(self, budget_bytes=2.0e9, max_batch_molecules=512, max_batches=16,
+                 cycles_per_launch=50, options: Options | None = None, **controls):
+        lib = library()
+        o = ServerOptions()
+        lib.sb_default_server_options(ctypes.byref(o))
+        if options is not None:
+            o.options = options
+        for k, v in controls.items():
+            setattr(o.controls, k, v)
+        o.hbm_budget_bytes = float(budget_bytes)
+        o.max_batch_molecules = int(max_batch_molecules)
+        o.max_batches = int(max_batches)
+        o.cycles_per_launch = int(cycles_per_launch)
+        self.options = o
+        handle = ctypes.c_void_p()
+        _check(lib.sb_server_create(ctypes.byref(o), ctypes.byref(handle)), "sb_server_create")
+        self.handle = handle
+        self._natom = {}
+
+    def prepare(self, molecule):
+        """Topology arrays of a molecule, reusable for many submissions."""
+        return _TopologyArrays(molecule)
+
+    def submit(self, molecule, coords=None, prepared=None):
+        t = prepared if prepared is not None else _TopologyArrays(molecule)
+        xyz = np.ascontiguousarray(np.asarray(molecule.coords if coords is None else coords,
+                                              dtype=np.float64).reshape(-1))
+        rid = ctypes.c_longlong()
+        _check(library().sb_server_submit(self.handle, ctypes.byref(t.struct), xyz.ctypes.data,
+                                          ctypes.byref(rid)), "sb_server_submit")
+        self._natom[rid.value] = molecule.natom
+        return rid.value
+
+    def poll(self, max_results=4096, coordinates=True):
+        """List of (result dict, coordinates or None) for the requests completed so far."""
+        res = (ServedResult * max_results)()
+        cap = 3 * sum(self._natom.values()) if coordinates else 0
+        buf = np.zeros(max(cap, 1)) if coordinates else None
+        n = ctypes.c_int()
+        _check(library().sb_server_poll(self.handle, res, max_results,
+                                        buf.ctypes.data if coordinates else None, cap,
+                                        ctypes.byref(n)), "sb_server_poll")
+        out = []
+        off = 0
+        for k in range(n.value):
+            r = res[k]
+            d = {"request_id": r.request_id, "natom": r.natom, "cycles": r.cycles,
+                 "converged": bool(r.converged), "rms_force": r.rms_force, "energy": r.energy,
+                 "energies": np.array(r.energies[:]), "submit_time": r.submit_time,
+                 "admit_time": r.admit_time, "finish_time": r.finish_time}
+            xyz = None
+            if coordinates:
+                xyz = buf[off:off + 3 * r.natom].reshape(-1, 3).copy()
+                off += 3 * r.natom
+            self._natom.pop(r.request_id, None)
+            out.append((d, xyz))
+        return out
+
+    def drain(self, timeout=60.0):
+        rc = library().sb_server_drain(self.handle, float(timeout))
+        if rc == SB_TIMEOUT:
+            return False
+        _check(rc, "sb_server_drain")
+        return True
+
+    def stats(self):
+        st = ServerStats()
+        _check(library().sb_server_get_stats(self.handle, ctypes.byref(st)), "sb_server_get_stats")
+        return {f: getattr(st, f) for f, _ in ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            library().sb_server_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

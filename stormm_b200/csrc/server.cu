@@ -1,0 +1,580 @@
+// Request server: continuous batching of conformer-minimization requests on one GPU.
+//
+// Requests arrive on any host thread (sb_server_submit copies the topology and coordinates) and
+// wait in a queue.  One worker thread owns the GPU side:
+//   admit     while fewer than max_batches batches are in flight, take queued requests in
+//             arrival order while the estimated device memory of the molecules in flight stays
+//             within the HBM budget, build a synthesis of them on a stream of the batch's own
+//             (stream-ordered allocations, so building never waits for other batches), upload
+//             coordinates, reset the minimizer and launch the first cycles_per_launch cycles
+//   poll      when a batch's launch has finished (event query, no blocking), read every
+//             molecule's progress, retire the molecules that converged or reached the cycle cap
+//             (final energies and coordinates are copied out), and launch the next cycles for
+//             the rest; a batch whose molecules have all retired is freed on its stream
+// Batches overlap on the device, new batches start while older ones run (backfill), and a
+// molecule's trajectory is bit-identical whichever batch, unit or launch split it gets.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "stormm_b200.h"
+#include "synthesis.h"
+
+namespace sb {
+
+namespace {
+
+template <typename T> void copyArray(std::vector<T>* dst, const T* src, size_t n) {
+  if (src != nullptr && n > 0) {
+    dst->assign(src, src + n);
+  }
+  else {
+    dst->clear();
+  }
+}
+
+template <typename T> const T* ptrOrNull(const std::vector<T> &v) {
+  return v.empty() ? nullptr : v.data();
+}
+
+// A request's own copy of its topology and coordinates
+struct Request {
+  long long id = 0;
+  int natom = 0;
+  int n_lj = 0;
+  int nbond = 0;
+  int nangl = 0;
+  int ndihe = 0;
+  std::vector<double> charge, lja, ljb, lja14, ljb14, pb_radii, gb_screen, gb_alpha, gb_beta;
+  std::vector<double> gb_gamma, bond_keq, bond_leq, angl_keq, angl_theta0, dihe_amp, dihe_freq;
+  std::vector<double> dihe_phase, dihe_scee, dihe_scnb, xyz;
+  std::vector<int> lj_idx, excl_bounds, excl_list, bond_atoms, angl_atoms, dihe_atoms;
+  std::vector<int> dihe_improper;
+  double bytes = 0.0;
+  double t_submit = 0.0;
+  double t_admit = 0.0;
+
+  Request(const sb_topology &t, const double* coords) {
+    natom = t.natom;
+    n_lj = t.n_lj_types;
+    nbond = t.nbond;
+    nangl = t.nangl;
+    ndihe = t.ndihe;
+    const size_t n = natom;
+    const size_t nt2 = static_cast<size_t>(n_lj) * n_lj;
+    copyArray(&charge, t.charge, n);
+    copyArray(&lj_idx, t.lj_idx, n);
+    copyArray(&lja, t.lja, nt2);
+    copyArray(&ljb, t.ljb, nt2);
+    copyArray(&lja14, t.lja14, nt2);
+    copyArray(&ljb14, t.ljb14, nt2);
+    copyArray(&excl_bounds, t.excl_bounds, n + 1);
+    const size_t nexcl = (t.excl_bounds != nullptr) ? static_cast<size_t>(t.excl_bounds[n]) : 0;
+    copyArray(&excl_list, t.excl_list, nexcl);
+    copyArray(&pb_radii, t.pb_radii, n);
+    copyArray(&gb_screen, t.gb_screen, n);
+    copyArray(&gb_alpha, t.gb_alpha, n);
+    copyArray(&gb_beta, t.gb_beta, n);
+    copyArray(&gb_gamma, t.gb_gamma, n);
+    copyArray(&bond_atoms, t.bond_atoms, 2 * static_cast<size_t>(nbond));
+    copyArray(&bond_keq, t.bond_keq, nbond);
+    copyArray(&bond_leq, t.bond_leq, nbond);
+    copyArray(&angl_atoms, t.angl_atoms, 3 * static_cast<size_t>(nangl));
+    copyArray(&angl_keq, t.angl_keq, nangl);
+    copyArray(&angl_theta0, t.angl_theta0, nangl);
+    copyArray(&dihe_atoms, t.dihe_atoms, 4 * static_cast<size_t>(ndihe));
+    copyArray(&dihe_amp, t.dihe_amp, ndihe);
+    copyArray(&dihe_freq, t.dihe_freq, ndihe);
+    copyArray(&dihe_phase, t.dihe_phase, ndihe);
+    copyArray(&dihe_scee, t.dihe_scee, ndihe);
+    copyArray(&dihe_scnb, t.dihe_scnb, ndihe);
+    copyArray(&dihe_improper, t.dihe_improper, ndihe);
+    copyArray(&xyz, coords, 3 * n);
+    // device memory the molecule holds while in flight: per-atom arrays (coordinates, forces,
+    // parameters, GB workspace, minimizer state) on the padded atom count, valence records,
+    // Lennard-Jones tables and exclusion masks
+    const double padded = static_cast<double>((natom + 31) / 32 * 32);
+    const double nblk = padded / 32.0;
+    bytes = 256.0 * padded + 16.0 * (nbond + nangl + 2.0 * ndihe) + 16.0 * nt2 +
+            128.0 * nblk * (nblk + 1.0) / 2.0 + 1024.0;
+  }
+
+  sb_topology view() const {
+    sb_topology t;
+    std::memset(&t, 0, sizeof(sb_topology));
+    t.natom = natom;
+    t.charge = ptrOrNull(charge);
+    t.lj_idx = ptrOrNull(lj_idx);
+    t.n_lj_types = n_lj;
+    t.lja = ptrOrNull(lja);
+    t.ljb = ptrOrNull(ljb);
+    t.lja14 = ptrOrNull(lja14);
+    t.ljb14 = ptrOrNull(ljb14);
+    t.excl_bounds = ptrOrNull(excl_bounds);
+    t.excl_list = ptrOrNull(excl_list);
+    t.pb_radii = ptrOrNull(pb_radii);
+    t.gb_screen = ptrOrNull(gb_screen);
+    t.gb_alpha = ptrOrNull(gb_alpha);
+    t.gb_beta = ptrOrNull(gb_beta);
+    t.gb_gamma = ptrOrNull(gb_gamma);
+    t.nbond = nbond;
+    t.bond_atoms = ptrOrNull(bond_atoms);
+    t.bond_keq = ptrOrNull(bond_keq);
+    t.bond_leq = ptrOrNull(bond_leq);
+    t.nangl = nangl;
+    t.angl_atoms = ptrOrNull(angl_atoms);
+    t.angl_keq = ptrOrNull(angl_keq);
+    t.angl_theta0 = ptrOrNull(angl_theta0);
+    t.ndihe = ndihe;
+    t.dihe_atoms = ptrOrNull(dihe_atoms);
+    t.dihe_amp = ptrOrNull(dihe_amp);
+    t.dihe_freq = ptrOrNull(dihe_freq);
+    t.dihe_phase = ptrOrNull(dihe_phase);
+    t.dihe_scee = ptrOrNull(dihe_scee);
+    t.dihe_scnb = ptrOrNull(dihe_scnb);
+    t.dihe_improper = ptrOrNull(dihe_improper);
+    return t;
+  }
+};
+
+struct Result {
+  sb_served_result r;
+  std::vector<double> xyz;
+};
+
+// Admitted requests minimizing together on one stream
+struct Batch {
+  std::vector<Request> reqs;
+  std::vector<char> finished;
+  int remaining = 0;
+  double bytes = 0.0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t event = nullptr;
+  std::unique_ptr<Synthesis> syn;
+};
+
+}  // namespace
+
+class Server {
+public:
+  explicit Server(const sb_server_options &o) : opt_(o), t0_(std::chrono::steady_clock::now()) {
+    if (o.hbm_budget_bytes <= 0.0 || o.max_batch_molecules < 1 || o.max_batches < 1 ||
+        o.cycles_per_launch < 1) {
+      throw Error(SB_ERR_ARGUMENT, "server budget, batch limits and cycles per launch must be "
+                  "positive");
+    }
+    if (o.controls.clash_cycles != 0) {
+      throw Error(SB_ERR_UNSUPPORTED, "clash-damping cycles are not provided; set them to 0");
+    }
+    int ndev = 0;
+    cudaCheck(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+    if (o.options.device < 0 || o.options.device >= ndev) {
+      throw Error(SB_ERR_DEVICE, "CUDA device " + std::to_string(o.options.device) +
+                  " not present");
+    }
+    worker_ = std::thread([this]() { this->run(); });
+  }
+
+  ~Server() {
+    {
+      std::lock_guard<std::mutex> lock(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    if (worker_.joinable()) {
+      worker_.join();
+    }
+  }
+
+  long long submit(const sb_topology* top, const double* xyz) {
+    if (top == nullptr || xyz == nullptr || top->natom <= 0) {
+      throw Error(SB_ERR_ARGUMENT, "a request needs a topology with atoms and coordinates");
+    }
+    Request req(*top, xyz);
+    if (req.bytes > opt_.hbm_budget_bytes) {
+      throw Error(SB_ERR_ARGUMENT, "the molecule alone exceeds the server's HBM budget");
+    }
+    std::lock_guard<std::mutex> lock(mu_);
+    failIfBroken();
+    req.id = next_id_++;
+    req.t_submit = now();
+    const long long id = req.id;
+    pending_.push_back(std::move(req));
+    submitted_++;
+    cv_.notify_all();
+    return id;
+  }
+
+  int poll(sb_served_result* out, int max_results, double* xyz, long long cap) {
+    std::lock_guard<std::mutex> lock(mu_);
+    failIfBroken();
+    int n = 0;
+    long long used = 0;
+    while (n < max_results && !results_.empty()) {
+      const Result &r = results_.front();
+      const long long need = static_cast<long long>(r.xyz.size());
+      if (xyz != nullptr) {
+        if (used + need > cap) {
+          break;
+        }
+        std::memcpy(xyz + used, r.xyz.data(), sizeof(double) * need);
+        used += need;
+      }
+      out[n++] = r.r;
+      results_.pop_front();
+    }
+    return n;
+  }
+
+  bool drain(double timeout) {
+    std::unique_lock<std::mutex> lock(mu_);
+    const auto until = std::chrono::steady_clock::now() +
+                       std::chrono::duration_cast<std::chrono::steady_clock::duration>(
+                           std::chrono::duration<double>(timeout));
+    while (!(pending_.empty() && in_flight_ == 0) && error_.empty()) {
+      if (idle_cv_.wait_until(lock, until) == std::cv_status::timeout) {
+        break;
+      }
+    }
+    failIfBroken();
+    return pending_.empty() && in_flight_ == 0;
+  }
+
+  sb_server_stats stats() {
+    std::lock_guard<std::mutex> lock(mu_);
+    sb_server_stats s;
+    s.submitted = submitted_;
+    s.admitted = admitted_;
+    s.completed = completed_;
+    s.pending = static_cast<int>(pending_.size());
+    s.in_flight = in_flight_;
+    s.batches = nbatches_;
+    s.bytes_in_flight = bytes_in_flight_;
+    return s;
+  }
+
+private:
+  double now() const {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0_).count();
+  }
+
+  void failIfBroken() const {
+    if (!error_.empty()) {
+      throw Error(SB_ERR_CUDA, "server worker stopped: " + error_);
+    }
+  }
+
+  void run() {
+    try {
+      cudaCheck(cudaSetDevice(opt_.options.device), "cudaSetDevice");
+      std::vector<std::unique_ptr<Batch>> batches;
+      while (true) {
+        bool progress = false;
+        for (size_t b = 0; b < batches.size();) {
+          const cudaError_t q = cudaEventQuery(batches[b]->event);
+          if (q == cudaErrorNotReady) {
+            b++;
+            continue;
+          }
+          cudaCheck(q, "batch launch");
+          progress = true;
+          if (service(batches[b].get())) {
+            retire(std::move(batches[b]));
+            batches.erase(batches.begin() + b);
+          }
+          else {
+            b++;
+          }
+        }
+        std::vector<Request> take;
+        {
+          std::unique_lock<std::mutex> lock(mu_);
+          if (stop_) {
+            break;
+          }
+          if (static_cast<int>(batches.size()) < opt_.max_batches) {
+            double bytes = bytes_in_flight_;
+            while (!pending_.empty() &&
+                   static_cast<int>(take.size()) < opt_.max_batch_molecules &&
+                   bytes + pending_.front().bytes <= opt_.hbm_budget_bytes) {
+              bytes += pending_.front().bytes;
+              take.push_back(std::move(pending_.front()));
+              pending_.pop_front();
+            }
+            if (!take.empty()) {
+              bytes_in_flight_ = bytes;
+              in_flight_ += static_cast<int>(take.size());
+              admitted_ += static_cast<long long>(take.size());
+              nbatches_++;
+            }
+          }
+          if (take.empty() && !progress) {
+            // nothing to launch or collect: sleep until a submission or a short timeout
+            cv_.wait_for(lock, std::chrono::microseconds(batches.empty() ? 2000 : 100));
+            continue;
+          }
+        }
+        if (!take.empty()) {
+          batches.push_back(admit(std::move(take)));
+        }
+      }
+      // stop: let the launches in flight finish, then release every batch on its stream
+      for (auto &b : batches) {
+        cudaEventSynchronize(b->event);
+        retire(std::move(b));
+      }
+    }
+    catch (const std::exception &e) {
+      std::lock_guard<std::mutex> lock(mu_);
+      error_ = e.what();
+      idle_cv_.notify_all();
+    }
+  }
+
+  // Build, upload and start a batch on a stream of its own
+  std::unique_ptr<Batch> admit(std::vector<Request> take) {
+    auto b = std::make_unique<Batch>();
+    b->reqs = std::move(take);
+    b->finished.assign(b->reqs.size(), 0);
+    b->remaining = static_cast<int>(b->reqs.size());
+    cudaCheck(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    cudaCheck(cudaEventCreateWithFlags(&b->event, cudaEventDisableTiming), "cudaEventCreate");
+    const double t = now();
+    std::vector<sb_topology> tops;
+    std::vector<int> index;
+    std::vector<double> xyz;
+    for (size_t k = 0; k < b->reqs.size(); k++) {
+      Request &r = b->reqs[k];
+      r.t_admit = t;
+      b->bytes += r.bytes;
+      tops.push_back(r.view());
+      index.push_back(static_cast<int>(k));
+      xyz.insert(xyz.end(), r.xyz.begin(), r.xyz.end());
+    }
+    {
+      AllocationStreamGuard guard(b->stream);
+      b->syn = std::make_unique<Synthesis>(tops.data(), static_cast<int>(tops.size()),
+                                           index.data(), static_cast<int>(tops.size()),
+                                           opt_.options);
+      b->syn->setCoordinates(xyz.data(), b->stream);
+      b->syn->minimizeBegin(opt_.controls, b->stream);
+    }
+    b->syn->minimizeAdvance(opt_.cycles_per_launch, true, b->stream);
+    cudaCheck(cudaEventRecord(b->event, b->stream), "cudaEventRecord");
+    return b;
+  }
+
+  // After a launch of the batch finished: retire what is done, relaunch the rest.  Returns true
+  // when every molecule of the batch has retired.
+  bool service(Batch* b) {
+    const int n = static_cast<int>(b->reqs.size());
+    std::vector<int> cycles(n), done(n);
+    std::vector<double> rms(n);
+    b->syn->getMinimizeProgress(cycles.data(), done.data(), rms.data(), b->stream);
+    std::vector<int> newly;
+    for (int k = 0; k < n; k++) {
+      if (!b->finished[k] && (done[k] || cycles[k] >= opt_.controls.total_cycles)) {
+        newly.push_back(k);
+      }
+    }
+    if (!newly.empty()) {
+      std::vector<double> nrg(static_cast<size_t>(n) * SB_NRG_STRIDE);
+      std::vector<double> xyz(3 * static_cast<size_t>(b->syn->natom_total));
+      b->syn->getEnergies(nrg.data(), b->stream);
+      b->syn->getCoordinates(xyz.data(), b->stream);
+      const double t = now();
+      std::vector<size_t> first(n + 1, 0);   // unpadded atom offsets, systems in batch order
+      for (int k = 0; k < n; k++) {
+        first[k + 1] = first[k] + static_cast<size_t>(b->reqs[k].natom);
+      }
+      std::vector<Result> out;
+      for (int k : newly) {
+        const Request &r = b->reqs[k];
+        Result res;
+        std::memset(&res.r, 0, sizeof(sb_served_result));
+        res.r.request_id = r.id;
+        res.r.natom = r.natom;
+        res.r.cycles = cycles[k];
+        res.r.converged = done[k];
+        res.r.rms_force = rms[k];
+        double total = 0.0;
+        for (int q = 0; q < SB_NRG_STRIDE; q++) {
+          res.r.energies[q] = nrg[static_cast<size_t>(k) * SB_NRG_STRIDE + q];
+          total += res.r.energies[q];
+        }
+        res.r.energy = total;
+        res.r.submit_time = r.t_submit;
+        res.r.admit_time = r.t_admit;
+        res.r.finish_time = t;
+        const size_t off = 3 * first[k];
+        res.xyz.assign(xyz.begin() + off, xyz.begin() + off + 3 * static_cast<size_t>(r.natom));
+        out.push_back(std::move(res));
+        b->finished[k] = 1;
+        b->remaining--;
+      }
+      std::lock_guard<std::mutex> lock(mu_);
+      for (auto &res : out) {
+        results_.push_back(std::move(res));
+      }
+      in_flight_ -= static_cast<int>(newly.size());
+      completed_ += static_cast<long long>(newly.size());
+      if (pending_.empty() && in_flight_ == 0) {
+        idle_cv_.notify_all();
+      }
+    }
+    if (b->remaining == 0) {
+      return true;
+    }
+    b->syn->minimizeAdvance(opt_.cycles_per_launch, true, b->stream);
+    cudaCheck(cudaEventRecord(b->event, b->stream), "cudaEventRecord");
+    return false;
+  }
+
+  // Free a batch's device memory in its stream's order, then its stream
+  void retire(std::unique_ptr<Batch> b) {
+    {
+      AllocationStreamGuard guard(b->stream);
+      b->syn.reset();
+    }
+    cudaEventDestroy(b->event);
+    cudaStreamDestroy(b->stream);
+    std::lock_guard<std::mutex> lock(mu_);
+    bytes_in_flight_ -= b->bytes;
+    if (bytes_in_flight_ < 0.0) {
+      bytes_in_flight_ = 0.0;
+    }
+    nbatches_--;
+    cv_.notify_all();
+  }
+
+  sb_server_options opt_;
+  std::chrono::steady_clock::time_point t0_;
+  std::thread worker_;
+  std::mutex mu_;
+  std::condition_variable cv_;        // worker wake-up: submissions, stop
+  std::condition_variable idle_cv_;   // drain: nothing queued or in flight
+  std::deque<Request> pending_;
+  std::deque<Result> results_;
+  long long next_id_ = 1;
+  long long submitted_ = 0;
+  long long admitted_ = 0;
+  long long completed_ = 0;
+  int in_flight_ = 0;
+  int nbatches_ = 0;
+  double bytes_in_flight_ = 0.0;
+  bool stop_ = false;
+  std::string error_;
+};
+
+}  // namespace sb
+
+// ------------------------------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------------------------------
+struct sb_server {
+  std::unique_ptr<sb::Server> impl;
+};
+
+namespace {
+
+template <typename F> int serverGuarded(F &&f) {
+  try {
+    f();
+    return SB_OK;
+  }
+  catch (const sb::Error &e) {
+    sb::setLastError(e.what());
+    return e.code;
+  }
+  catch (const std::exception &e) {
+    sb::setLastError(e.what());
+    return SB_ERR_ARGUMENT;
+  }
+}
+
+sb::Server* needServer(sb_server* s) {
+  if (s == nullptr || !s->impl) {
+    throw sb::Error(SB_ERR_ARGUMENT, "null server handle");
+  }
+  return s->impl.get();
+}
+
+}  // namespace
+
+extern "C" {
+
+void sb_default_server_options(sb_server_options* opt) {
+  std::memset(opt, 0, sizeof(sb_server_options));
+  sb_default_options(&opt->options);
+  sb_default_minimize_controls(&opt->controls);
+  opt->controls.total_cycles = 2000;
+  opt->controls.convergence_rms = 0.01;
+  opt->hbm_budget_bytes = 2.0e9;
+  opt->max_batch_molecules = 512;
+  opt->max_batches = 16;
+  opt->cycles_per_launch = 50;
+}
+
+int sb_server_create(const sb_server_options* opt, sb_server** out) {
+  return serverGuarded([&]() {
+    if (out == nullptr) throw sb::Error(SB_ERR_ARGUMENT, "null output handle");
+    *out = nullptr;
+    sb_server_options o;
+    if (opt != nullptr) {
+      o = *opt;
+    }
+    else {
+      sb_default_server_options(&o);
+    }
+    auto h = std::make_unique<sb_server>();
+    h->impl = std::make_unique<sb::Server>(o);
+    *out = h.release();
+  });
+}
+
+int sb_server_submit(sb_server* srv, const sb_topology* top, const double* xyz,
+                     long long* request_id) {
+  return serverGuarded([&]() {
+    const long long id = needServer(srv)->submit(top, xyz);
+    if (request_id) *request_id = id;
+  });
+}
+
+int sb_server_poll(sb_server* srv, sb_served_result* results, int max_results, double* xyz,
+                   long long xyz_capacity, int* count) {
+  return serverGuarded([&]() {
+    if (results == nullptr && max_results > 0) {
+      throw sb::Error(SB_ERR_ARGUMENT, "null result array");
+    }
+    const int n = needServer(srv)->poll(results, max_results, xyz, xyz_capacity);
+    if (count) *count = n;
+  });
+}
+
+int sb_server_drain(sb_server* srv, double timeout_seconds) {
+  bool drained = false;
+  const int rc = serverGuarded([&]() { drained = needServer(srv)->drain(timeout_seconds); });
+  if (rc != SB_OK) return rc;
+  return drained ? SB_OK : SB_TIMEOUT;
+}
+
+int sb_server_get_stats(sb_server* srv, sb_server_stats* stats) {
+  return serverGuarded([&]() {
+    if (stats == nullptr) throw sb::Error(SB_ERR_ARGUMENT, "null stats");
+    *stats = needServer(srv)->stats();
+  });
+}
+
+int sb_server_destroy(sb_server* srv) {
+  return serverGuarded([&]() { delete srv; });
+}
+
+}  // extern "C"

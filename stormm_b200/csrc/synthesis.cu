@@ -48,6 +48,11 @@ namespace {
 thread_local std::string g_last_error;
 }
 
+cudaStream_t &allocationStream() {
+  static thread_local cudaStream_t s = nullptr;
+  return s;
+}
+
 void setLastError(const std::string &msg) { g_last_error = msg; }
 const char* lastError() { return g_last_error.c_str(); }
 
@@ -100,13 +105,16 @@ Synthesis::Synthesis(const sb_topology* tops, int ntop, const int* topology_inde
     throw Error(SB_ERR_DEVICE, "CUDA device " + std::to_string(opt.device) + " not present");
   }
   cudaCheck(cudaSetDevice(opt.device), "cudaSetDevice");
-  cudaDeviceProp prop;
-  cudaCheck(cudaGetDeviceProperties(&prop, opt.device), "cudaGetDeviceProperties");
-  if (prop.major < 10) {
-    throw Error(SB_ERR_DEVICE, std::string("device ") + prop.name + " is not sm_100 class");
+  int major = 0;
+  cudaCheck(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, opt.device),
+            "cudaDeviceGetAttribute");
+  if (major < 10) {
+    throw Error(SB_ERR_DEVICE, "device " + std::to_string(opt.device) + " is not sm_100 class");
   }
-  sm_count = prop.multiProcessorCount;
-  max_smem_optin = static_cast<int>(prop.sharedMemPerBlockOptin);
+  cudaCheck(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, opt.device),
+            "cudaDeviceGetAttribute");
+  cudaCheck(cudaDeviceGetAttribute(&max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin,
+                                   opt.device), "cudaDeviceGetAttribute");
 
   topo.assign(topology_index, topology_index + nsys);
   for (int s = 0; s < nsys; s++) {

@@ -31,26 +31,54 @@ void cudaCheck(cudaError_t err, const char* what);
 void setLastError(const std::string &msg);
 const char* lastError();
 
-// Device array owned by the synthesis (cudaMalloc / cudaFree)
+// Stream for stream-ordered allocation by the calling thread; null (the default) means plain
+// cudaMalloc / cudaFree.  The request server sets it while it builds or retires a batch, so that
+// allocating and freeing device memory does not wait for the other batches' kernels.
+cudaStream_t &allocationStream();
+
+class AllocationStreamGuard {
+public:
+  explicit AllocationStreamGuard(cudaStream_t s) : prev_(allocationStream()) {
+    allocationStream() = s;
+  }
+  ~AllocationStreamGuard() { allocationStream() = prev_; }
+private:
+  cudaStream_t prev_;
+};
+
+// Device array owned by the synthesis
 template <typename T> struct DeviceArray {
   T* p = nullptr;
   size_t n = 0;
+  cudaStream_t s = nullptr;      // stream of a stream-ordered allocation
   DeviceArray() = default;
   DeviceArray(const DeviceArray &) = delete;
   DeviceArray& operator=(const DeviceArray &) = delete;
-  ~DeviceArray() {
+  ~DeviceArray() { release(); }
+  void release() {
     if (p != nullptr) {
-      cudaFree(p);
+      if (s != nullptr) {
+        cudaFreeAsync(p, s);
+      }
+      else {
+        cudaFree(p);
+      }
+      p = nullptr;
     }
   }
   void allocate(size_t count) {
-    if (p != nullptr) {
-      cudaFree(p);
-      p = nullptr;
-    }
+    release();
     n = count;
-    cudaCheck(cudaMalloc(reinterpret_cast<void**>(&p), sizeof(T) * (count > 0 ? count : 1)),
-              "cudaMalloc");
+    s = allocationStream();
+    const size_t bytes = sizeof(T) * (count > 0 ? count : 1);
+    if (s != nullptr) {
+      cudaCheck(cudaMallocAsync(reinterpret_cast<void**>(&p), bytes, s), "cudaMallocAsync");
+      // usable by the synchronous copies that follow
+      cudaCheck(cudaStreamSynchronize(s), "cudaMallocAsync");
+    }
+    else {
+      cudaCheck(cudaMalloc(reinterpret_cast<void**>(&p), bytes), "cudaMalloc");
+    }
   }
   void zeros(size_t count) {
     allocate(count);
