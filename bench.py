@@ -40,6 +40,11 @@ MIN_CYCLES = 500
 MIN_SD_CYCLES = 50
 MIN_WORKLOAD = ("batched conformer minimization: 4096 molecules, 24-96 atoms, 0.3 A start noise, "
                 "500 cycles (50 SD then CG), OBC-II GB")
+SERVED_RATES = (250.0, 1000.0, 4000.0)
+SERVED_WINDOW_S = 1.0
+SERVED_WORKLOAD = ("served minimization stream: Poisson arrivals, lognormal sizes (median 48 atoms, "
+                   "sigma 0.6, clipped 12-512), 0.3 A start noise, each to RMS force <= 0.01 "
+                   "kcal/mol/A or 2000 cycles")
 
 
 def _args():
@@ -52,6 +57,7 @@ def _args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-minimization", action="store_true")
     ap.add_argument("--min-steps", type=int, default=2)
+    ap.add_argument("--no-served", action="store_true")
     return ap.parse_args()
 
 
@@ -386,6 +392,47 @@ def bench_minimization(args, world, rank, local, flush):
     }
 
 
+def bench_served(local):
+    """Poisson request streams at several rates through the continuous-batching server."""
+    import stormm_b200 as sb
+    from stormm_b200 import synthetic
+    mols = synthetic.workload_served(1600)
+    srv = sb.Server(options=sb.default_options(device=local))
+    prepared = [srv.prepare(m) for m in mols]
+    srv.close()
+    sweeps = []
+    for rate in SERVED_RATES:
+        srv = sb.Server(options=sb.default_options(device=local), cycles_per_launch=50)
+        rng = np.random.default_rng(int(rate))
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, size=int(rate * SERVED_WINDOW_S * 2) + 8))
+        arrivals = arrivals[arrivals < SERVED_WINDOW_S]
+        start = time.perf_counter()
+        for k, ta in enumerate(arrivals):
+            while time.perf_counter() - start < ta:
+                pass
+            srv.submit(mols[k % len(mols)], prepared=prepared[k % len(mols)])
+        drained = srv.drain(600.0)
+        res = [r for r, _ in srv.poll(max_results=len(arrivals) + 16, coordinates=False)]
+        srv.close()
+        lat = np.array([r["finish_time"] - r["submit_time"] for r in res])
+        wait = np.array([r["admit_time"] - r["submit_time"] for r in res])
+        first = min(r["submit_time"] for r in res)
+        last = max(r["finish_time"] for r in res)
+        sweeps.append({
+            "offered_per_s": rate, "requests": len(arrivals), "completed": len(res),
+            "drained": bool(drained),
+            "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+            "admission_wait_p50_ms": float(np.percentile(wait, 50) * 1e3),
+            "throughput_per_s": len(res) / (last - first),
+            "mean_cycles": float(np.mean([r["cycles"] for r in res])),
+            "converged_fraction": float(np.mean([r["converged"] for r in res])),
+        })
+    return {"workload": SERVED_WORKLOAD, "unit": "requests/s, latency ms (submit to result)",
+            "arrival_window_s": SERVED_WINDOW_S, "cycles_per_launch": 50,
+            "throughput_note": "completions over first submit to last result, drain tail included",
+            "sweep": sweeps}
+
+
 def main():
     args = _args()
     if args.impl == "reference":
@@ -405,6 +452,7 @@ def main():
     with ClockSampler(local) as clocks:
         sp = bench_single_point(args, world, rank, local, flush)
         mn = None if args.no_minimization else bench_minimization(args, world, rank, local, flush)
+        served = None if (args.no_served or rank != 0) else bench_served(local)
     csum = clocks.summary()
 
     achieved = sp["flops"] / sp["kern_avg_s"] / 1.0e12
@@ -461,6 +509,7 @@ def main():
             "clocks": csum,
             "cpu_baseline": cpu,
             "minimization": mn,
+            "served": served,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

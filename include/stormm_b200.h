@@ -132,6 +132,9 @@ typedef struct {
   int max_tiles_per_unit;      /* work-unit packing limit, 0: tuned default */
   int threads_per_block;       /* 0: tuned default */
   int device;                  /* CUDA device ordinal */
+  int tiled_above_atoms;       /* molecules with more atoms are evaluated tile by tile from global
+                                  memory, spread over the whole GPU (0: 2048, the on-chip limit;
+                                  32-2048); they cannot be minimized */
 } sb_options;
 
 /* Fill *opt with STORMM's defaults (OBC-II, dielectric 80, no salt, 32/23/26 fixed-point bits) */

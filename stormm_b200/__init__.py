@@ -50,6 +50,7 @@ class Options(ctypes.Structure):
         ("frc_bits", ctypes.c_int), ("nrg_bits", ctypes.c_int),
         ("max_atoms_per_unit", ctypes.c_int), ("max_tiles_per_unit", ctypes.c_int),
         ("threads_per_block", ctypes.c_int), ("device", ctypes.c_int),
+        ("tiled_above_atoms", ctypes.c_int),
     ]
 
 

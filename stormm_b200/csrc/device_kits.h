@@ -107,6 +107,22 @@ struct DevSynthesis {
   int* status;                   // device status word (0 = fine)
 };
 
+// Molecules evaluated tile by tile from global memory (too large for one block's shared memory,
+// or routed there by the tiled_above_atoms option): every 32 x 32 tile of every such molecule is
+// an independent warp task, so one molecule spreads over the whole GPU.  Pair passes accumulate
+// into global integer arrays; per-atom steps run between the passes as separate kernels.
+struct DevTiled {
+  int nmol;                      // molecules on the tiled path
+  int ntiles;                    // their tiles in total
+  const int* systems;            // system index of each
+  const int* tile_prefix;        // nmol + 1: first tile of each molecule
+  const int* atom_prefix;        // nmol + 1: first padded atom of each, counted over these only
+  long long* psi_acc;            // per padded atom: psi at 2^kPsiBits
+  long long* de_acc;             // per padded atom: dE/dR at 2^kDeijdaBits
+  float* radius;                 // per padded atom: effective GB radius
+  float* sde;                    // per padded atom: dE/dR after the chain-rule prefactor
+};
+
 // Line-minimization state (MolecularMechanics/line_minimization.h:15-221 and the conjugate
 // gradient substrate, Math/hpc_reduction.h:55-63), per system and per padded atom.  It persists
 // between launches, so a minimization can run in several launches of a few cycles each.

@@ -31,6 +31,10 @@ cudaError_t launchMinimizerReset(const DevMinimizer &m, const DevSynthesis &d, d
 cudaError_t launchMinimize(const DevSynthesis &d, const DevMinimizer &m, int unit_begin,
                            int unit_end, int max_lj, int cycles, bool final_energy, int threads,
                            int sm_count, cudaStream_t stream);
+cudaError_t launchTiled(const DevSynthesis &d, const DevTiled &t, const int* h_tile_prefix,
+                        const int* h_atom_prefix, int mol_begin, int mol_end, int terms,
+                        bool force, bool energy, bool workspace, int sm_count,
+                        cudaStream_t stream);
 cudaError_t launchImportCoordinates(const double* d_xyz, const int* d_map, int natom,
                                     double scale, long long* xcrd, long long* ycrd,
                                     long long* zcrd, int* xo, int* yo, int* zo, int* status,
@@ -323,8 +327,12 @@ std::unique_ptr<UnitPlan> Synthesis::makePlan(int max_slots_cap, int max_tiles_c
   auto plan = std::make_unique<UnitPlan>();
   plan->max_slots_cap = max_slots_cap;
   plan->max_tiles_cap = max_tiles_cap;
-  std::vector<int> order(nsys);
-  for (int s = 0; s < nsys; s++) order[s] = s;
+  std::vector<int> order;
+  for (int s = 0; s < nsys; s++) {
+    if (atom_count[s] <= tiled_threshold) {
+      order.push_back(s);   // molecules above the threshold take the tiled path
+    }
+  }
   std::stable_sort(order.begin(), order.end(),
                    [&](int a, int b) { return atom_count[a] > atom_count[b]; });
   auto slots_of = [&](int s) { return (atom_count[s] + kTile - 1) / kTile * kTile; };
@@ -393,6 +401,28 @@ void Synthesis::buildUnits() {
   if (threads % 32 != 0 || threads < 64 || threads > 256) {
     throw Error(SB_ERR_ARGUMENT, "threads per block must be a multiple of 32 in [64, 256]");
   }
+  tiled_threshold = (opt.tiled_above_atoms > 0) ? opt.tiled_above_atoms : kMaxFusedAtoms;
+  if (tiled_threshold < kTile || tiled_threshold > kMaxFusedAtoms) {
+    throw Error(SB_ERR_ARGUMENT, "tiled_above_atoms must lie in [32, 2048]");
+  }
+  // molecules above the threshold: tiles of every one, in system order
+  tiled_index.assign(nsys, -1);
+  h_tiled_systems.clear();
+  h_tile_prefix.assign(1, 0);
+  h_atom_prefix.assign(1, 0);
+  for (int s = 0; s < nsys; s++) {
+    if (atom_count[s] > tiled_threshold) {
+      const long long nb = (atom_count[s] + kTile - 1) / kTile;
+      const long long tiles = static_cast<long long>(h_tile_prefix.back()) + nb * (nb + 1) / 2;
+      if (tiles > 2000000000LL) {
+        throw Error(SB_ERR_UNSUPPORTED, "too many tiles on the tiled path");
+      }
+      tiled_index[s] = static_cast<int>(h_tiled_systems.size());
+      h_tiled_systems.push_back(s);
+      h_tile_prefix.push_back(static_cast<int>(tiles));
+      h_atom_prefix.push_back(h_atom_prefix.back() + static_cast<int>(nb) * kTile);
+    }
+  }
   const int slots_cap = (opt.max_atoms_per_unit > 0) ? opt.max_atoms_per_unit : 256;
   const int tiles_cap = (opt.max_tiles_per_unit > 0) ? opt.max_tiles_per_unit : 36;
   eval_plan = makePlan(slots_cap, tiles_cap);
@@ -412,8 +442,10 @@ void Synthesis::buildUnits() {
   for (int s = 0; s < nsys; s++) {
     h_single_units[s] = make_int4(s, 1, slots_of(s), tiles_of(s));
     h_single_systems[s] = s;
-    single_slots = std::max(single_slots, slots_of(s));
-    single_lj = std::max(single_lj, 2 * h_lj_ntypes[s] * h_lj_ntypes[s]);
+    if (tiled_index[s] < 0) {
+      single_slots = std::max(single_slots, slots_of(s));
+      single_lj = std::max(single_lj, 2 * h_lj_ntypes[s] * h_lj_ntypes[s]);
+    }
   }
   max_unit_slots = single_slots;
   max_lj = single_lj;
@@ -448,6 +480,24 @@ void Synthesis::upload() {
   d_tile_mask_idx.upload(h_tile_mask_idx);
   d_mask_pool.upload(h_mask_pool);
   d_single_units.upload(h_single_units);
+  d_tiled_systems.upload(h_tiled_systems);
+  d_tile_prefix.upload(h_tile_prefix);
+  d_atom_prefix.upload(h_atom_prefix);
+  if (!h_tiled_systems.empty()) {
+    d_tiled_psi.zeros(natom_padded);
+    d_tiled_de.zeros(natom_padded);
+    d_tiled_radius.zeros(natom_padded);
+    d_tiled_sde.zeros(natom_padded);
+  }
+  dev_tiled.nmol = static_cast<int>(h_tiled_systems.size());
+  dev_tiled.ntiles = h_tile_prefix.back();
+  dev_tiled.systems = d_tiled_systems.p;
+  dev_tiled.tile_prefix = d_tile_prefix.p;
+  dev_tiled.atom_prefix = d_atom_prefix.p;
+  dev_tiled.psi_acc = d_tiled_psi.p;
+  dev_tiled.de_acc = d_tiled_de.p;
+  dev_tiled.radius = d_tiled_radius.p;
+  dev_tiled.sde = d_tiled_sde.p;
   d_single_systems.upload(h_single_systems);
   d_unpadded_map.upload(h_unpadded_map);
   d_stage_xyz.zeros(static_cast<size_t>(3) * natom_total);
@@ -557,6 +607,27 @@ void Synthesis::evaluate(int terms, bool force, bool energy, cudaStream_t stream
     return;
   }
   launchPlan(*eval_plan, terms, force, energy, stream);
+  launchTiledRange(0, static_cast<int>(h_tiled_systems.size()), terms, force, energy, stream);
+}
+
+void Synthesis::launchTiledRange(int mol_begin, int mol_end, int terms, bool force, bool energy,
+                                 cudaStream_t stream) {
+  if (mol_end <= mol_begin) {
+    return;
+  }
+  const size_t np = natom_padded;
+  cudaCheck(cudaMemsetAsync(d_tiled_psi.p, 0, np * sizeof(long long), stream), "memset");
+  cudaCheck(cudaMemsetAsync(d_tiled_de.p, 0, np * sizeof(long long), stream), "memset");
+  cudaCheck(launchTiled(dev, dev_tiled, h_tile_prefix.data(), h_atom_prefix.data(), mol_begin,
+                        mol_end, terms, force, energy, true, sm_count, stream),
+            "tiled evaluation launch");
+}
+
+void Synthesis::rejectTiledMinimization() const {
+  if (!h_tiled_systems.empty()) {
+    throw Error(SB_ERR_UNSUPPORTED, "molecules above " + std::to_string(tiled_threshold) +
+                " atoms are evaluated tile by tile and cannot be minimized on chip");
+  }
 }
 
 void Synthesis::evaluateRange(int first, int count, int terms, bool force, bool energy,
@@ -576,6 +647,10 @@ void Synthesis::evaluateRange(int first, int count, int terms, bool force, bool 
   d.nunit = nsys;
   d.max_unit_slots = single_slots;
   for (int s = first; s < first + count; s++) {
+    if (tiled_index[s] >= 0) {
+      launchTiledRange(tiled_index[s], tiled_index[s] + 1, terms, force, energy, stream);
+      continue;
+    }
     cudaCheck(launchEvalFused(d, s, s + 1, single_lj, terms, force, energy, 1, threads, stream),
               "per-system evaluation launch");
   }
@@ -703,6 +778,7 @@ int Synthesis::checkStatus(cudaStream_t stream) {
 // Line minimization (MolecularMechanics/hpc_minimization.cu:129-600)
 // ------------------------------------------------------------------------------------------------
 void Synthesis::minimizeBegin(const sb_minimize_controls &ctl, cudaStream_t stream) {
+  rejectTiledMinimization();
   if (ctl.total_cycles < 0 || ctl.sd_cycles < 0) {
     throw Error(SB_ERR_ARGUMENT, "cycle counts must not be negative");
   }

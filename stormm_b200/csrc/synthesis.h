@@ -143,6 +143,9 @@ public:
   int max_unit_slots = 0;
   std::unique_ptr<UnitPlan> eval_plan;   // batched evaluation
   std::unique_ptr<UnitPlan> min_plan;    // batched minimization
+  int tiled_threshold = kMaxFusedAtoms;  // molecules above it take the tiled path
+  std::vector<int> h_tiled_systems, h_tile_prefix, h_atom_prefix;
+  std::vector<int> tiled_index;          // per system: index among tiled molecules, or -1
   int single_slots = 0, single_lj = 0;
   std::vector<int> topo;
   std::vector<int> atom_start;
@@ -177,6 +180,10 @@ public:
   DeviceArray<float> d_born_radii;
   DeviceArray<int> d_unpadded_map;
   DeviceArray<double> d_stage_xyz, d_stage_nrg;
+  DeviceArray<int> d_tiled_systems, d_tile_prefix, d_atom_prefix;
+  DeviceArray<long long> d_tiled_psi, d_tiled_de;
+  DeviceArray<float> d_tiled_radius, d_tiled_sde;
+  DevTiled dev_tiled{};
 
   // line-minimization state, allocated by the first minimization
   DeviceArray<long long> d_xprv, d_yprv, d_zprv;
@@ -194,6 +201,9 @@ private:
   std::unique_ptr<UnitPlan> makePlan(int max_slots_cap, int max_tiles_cap) const;
   void launchPlan(const UnitPlan &plan, int terms, bool force, bool energy, cudaStream_t stream);
   void launchMinPlan(const UnitPlan &plan, int cycles, bool final_energy, cudaStream_t stream);
+  void launchTiledRange(int mol_begin, int mol_end, int terms, bool force, bool energy,
+                        cudaStream_t stream);
+  void rejectTiledMinimization() const;
   void buildUnits();
   void upload();
 };

@@ -249,30 +249,57 @@ __device__ __forceinline__ float3 slotDelta(const UnitSmem &s, int a, int b) {
 // Valence terms (Potential/valence_potential.tpp).  Warps take chunks of 32 terms of one molecule,
 // so each chunk's energies reduce across the warp into a single shared-memory update.
 // ------------------------------------------------------------------------------------------------
-template <bool FORCE, bool ENERGY>
-__device__ void valenceTerms(const DevSynthesis &d, const UnitSmem &s, int nsys_u) {
+// Where valence terms read their atoms and put forces and energies: a work unit's shared memory
+struct SmemValence {
+  const UnitSmem &s;
+  const int* bchunk0;
+  const int* achunk0;
+  const int* dchunk0;
+  const int* sys;
+  const int* slot0;
+  __device__ explicit SmemValence(const UnitSmem &s_in) :
+      s(s_in), bchunk0(s_in.bchunk0), achunk0(s_in.achunk0), dchunk0(s_in.dchunk0),
+      sys(s_in.sys), slot0(s_in.slot0) {}
+  __device__ __forceinline__ int chunkBegin() const { return threadIdx.x >> 5; }
+  __device__ __forceinline__ int chunkStride() const { return blockDim.x >> 5; }
+  __device__ __forceinline__ float4 pa(int i) const { return s.pa[i]; }
+  __device__ __forceinline__ float4 pb(int i) const { return s.pb[i]; }
+  __device__ __forceinline__ float4 prm(int i) const { return s.prm[i]; }
+  __device__ __forceinline__ float3 delta(int a, int b) const { return slotDelta(s, a, b); }
+  __device__ __forceinline__ void force(int i, float fx, float fy, float fz, float scale) const {
+    addForce(s, i, fx, fy, fz, scale);
+  }
+  __device__ __forceinline__ void energy(int k, int slot, float e, float scale) const {
+    warpEnergy(s, k, slot, e, scale);
+  }
+  // the molecule's 1-4 table follows its standard table in shared memory
+  __device__ __forceinline__ float2 lj14(int code_i, int code_l, int nt) const {
+    return s.lj[(code_i & 0xffff) + (code_l >> 16) + nt * nt];
+  }
+};
+
+template <bool FORCE, bool ENERGY, class V>
+__device__ void valenceTerms(const DevSynthesis &d, const V &v, int nsys_u) {
   const float fs = d.frc_scale;
   const float es = d.nrg_scale;
   const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const int nwarp = blockDim.x >> 5;
 
   // bonds, valence_potential.tpp:9-97; the equilibrium length is a float pair so that r - r0
   // loses nothing to the rounding of r0, and the bond length itself is an unevaluated pair
-  for (int c = warp; c < s.bchunk0[nsys_u]; c += nwarp) {
-    const int k = findOwner(s.bchunk0, nsys_u, c);
-    const int sysid = s.sys[k];
-    const int t = (c - s.bchunk0[k]) * 32 + lane;
+  for (int c = v.chunkBegin(); c < v.bchunk0[nsys_u]; c += v.chunkStride()) {
+    const int k = findOwner(v.bchunk0, nsys_u, c);
+    const int sysid = v.sys[k];
+    const int t = (c - v.bchunk0[k]) * 32 + lane;
     const int nterm = d.bond_start[sysid + 1] - d.bond_start[sysid];
     float e = 0.0f;
     if (t < nterm) {
       const uint4 rec = d.bonds[d.bond_start[sysid] + t];
-      const int ia = s.slot0[k] + static_cast<int>(rec.x & 0xffffu);
-      const int ja = s.slot0[k] + static_cast<int>(rec.x >> 16);
+      const int ia = v.slot0[k] + static_cast<int>(rec.x & 0xffffu);
+      const int ja = v.slot0[k] + static_cast<int>(rec.x >> 16);
       const float keq = __uint_as_float(rec.y);
       const float leq_hi = __uint_as_float(rec.z);
       const float leq_lo = __uint_as_float(rec.w);
-      const float4 ai = s.pa[ia], aj = s.pa[ja], bi = s.pb[ia], bj = s.pb[ja];
+      const float4 ai = v.pa(ia), aj = v.pa(ja), bi = v.pb(ia), bj = v.pb(ja);
       const float av[3] = {aj.x, aj.y, aj.z};
       const float bv[3] = {ai.x, ai.y, ai.z};
       const float lav[3] = {bj.x, bj.y, bj.z};
@@ -303,34 +330,34 @@ __device__ void valenceTerms(const DevSynthesis &d, const UnitSmem &s, int nsys_
       const float dl = ((r - leq_hi) + r_lo) - leq_lo;
       if (FORCE) {
         const float fmag = 2.0f * keq * dl / r;
-        addForce(s, ia, fmag * dh[0], fmag * dh[1], fmag * dh[2], fs);
-        addForce(s, ja, -fmag * dh[0], -fmag * dh[1], -fmag * dh[2], fs);
+        v.force(ia, fmag * dh[0], fmag * dh[1], fmag * dh[2], fs);
+        v.force(ja, -fmag * dh[0], -fmag * dh[1], -fmag * dh[2], fs);
       }
       e = __fmul_rn(__fmul_rn(keq, dl), dl);
     }
     if (ENERGY) {
-      warpEnergy(s, k, kBond, e, es);
+      v.energy(k, kBond, e, es);
     }
   }
 
   // angles, valence_potential.tpp:170-288.  theta - theta0 comes from rotating (cos, sin) of
   // theta, taken from the dot and cross products, by theta0: well conditioned everywhere.
-  for (int c = warp; c < s.achunk0[nsys_u]; c += nwarp) {
-    const int k = findOwner(s.achunk0, nsys_u, c);
-    const int sysid = s.sys[k];
-    const int t = (c - s.achunk0[k]) * 32 + lane;
+  for (int c = v.chunkBegin(); c < v.achunk0[nsys_u]; c += v.chunkStride()) {
+    const int k = findOwner(v.achunk0, nsys_u, c);
+    const int sysid = v.sys[k];
+    const int t = (c - v.achunk0[k]) * 32 + lane;
     const int nterm = d.angl_start[sysid + 1] - d.angl_start[sysid];
     float e = 0.0f;
     if (t < nterm) {
       const uint4 rec = d.angles[d.angl_start[sysid] + t];
-      const int ia = s.slot0[k] + static_cast<int>(rec.x & 0xffffu);
-      const int ja = s.slot0[k] + static_cast<int>(rec.x >> 16);
-      const int ka = s.slot0[k] + static_cast<int>(rec.y);
+      const int ia = v.slot0[k] + static_cast<int>(rec.x & 0xffffu);
+      const int ja = v.slot0[k] + static_cast<int>(rec.x >> 16);
+      const int ka = v.slot0[k] + static_cast<int>(rec.y);
       const float keq = __uint_as_float(rec.z);
       const float cth0 = __uint_as_float(rec.w);
       const float sth0 = sqrtf(fmaxf(0.0f, fmaf(-cth0, cth0, 1.0f)));
-      const float3 ba = slotDelta(s, ja, ia);
-      const float3 bc = slotDelta(s, ja, ka);
+      const float3 ba = v.delta(ja, ia);
+      const float3 bc = v.delta(ja, ka);
       const float mgba = ba.x * ba.x + ba.y * ba.y + ba.z * ba.z;
       const float mgbc = bc.x * bc.x + bc.y * bc.y + bc.z * bc.z;
       const float invbabc = rsqrtf(mgba * mgbc);
@@ -353,14 +380,14 @@ __device__ void valenceTerms(const DevSynthesis &d, const UnitSmem &s, int nsys_
         const float cdx = ba.x * mbabc - cth * bc.x * sqbc;
         const float cdy = ba.y * mbabc - cth * bc.y * sqbc;
         const float cdz = ba.z * mbabc - cth * bc.z * sqbc;
-        addForce(s, ia, -adx, -ady, -adz, fs);
-        addForce(s, ja, adx + cdx, ady + cdy, adz + cdz, fs);
-        addForce(s, ka, -cdx, -cdy, -cdz, fs);
+        v.force(ia, -adx, -ady, -adz, fs);
+        v.force(ja, adx + cdx, ady + cdy, adz + cdz, fs);
+        v.force(ka, -cdx, -cdy, -cdz, fs);
       }
       e = __fmul_rn(__fmul_rn(keq, dtheta), dtheta);
     }
     if (ENERGY) {
-      warpEnergy(s, k, kAngle, e, es);
+      v.energy(k, kAngle, e, es);
     }
   }
 
@@ -369,28 +396,28 @@ __device__ void valenceTerms(const DevSynthesis &d, const UnitSmem &s, int nsys_
   // the angle STORMM's acos / arcsine route gives (Math/rounding.tpp:25-80) without its ill
   // conditioning near 0 and pi; cos(n theta - phase) and sin(n theta - phase) follow from the
   // multiple-angle recurrence for integer periodicities.
-  for (int c = warp; c < s.dchunk0[nsys_u]; c += nwarp) {
-    const int k = findOwner(s.dchunk0, nsys_u, c);
-    const int sysid = s.sys[k];
-    const int t = (c - s.dchunk0[k]) * 32 + lane;
+  for (int c = v.chunkBegin(); c < v.dchunk0[nsys_u]; c += v.chunkStride()) {
+    const int k = findOwner(v.dchunk0, nsys_u, c);
+    const int sysid = v.sys[k];
+    const int t = (c - v.dchunk0[k]) * 32 + lane;
     const int nterm = d.dihe_start[sysid + 1] - d.dihe_start[sysid];
     float e_prop = 0.0f, e_impr = 0.0f, e_el14 = 0.0f, e_lj14 = 0.0f;
     if (t < nterm) {
       const int pos = d.dihe_start[sysid] + t;
       const uint4 ra = d.dihe_a[pos];
       const uint4 rb = d.dihe_b[pos];
-      const int ia = s.slot0[k] + static_cast<int>(ra.x & 0xffffu);
-      const int ja = s.slot0[k] + static_cast<int>(ra.x >> 16);
-      const int ka = s.slot0[k] + static_cast<int>(ra.y & 0xffffu);
-      const int la = s.slot0[k] + static_cast<int>((ra.y >> 16) & 0x7fffu);
+      const int ia = v.slot0[k] + static_cast<int>(ra.x & 0xffffu);
+      const int ja = v.slot0[k] + static_cast<int>(ra.x >> 16);
+      const int ka = v.slot0[k] + static_cast<int>(ra.y & 0xffffu);
+      const int la = v.slot0[k] + static_cast<int>((ra.y >> 16) & 0x7fffu);
       const bool improper = (ra.y & 0x80000000u) != 0u;
       const float amp = __uint_as_float(ra.z);
       const float freq = __uint_as_float(ra.w);
       const float cphase = __uint_as_float(rb.x);
       const float sphase = __uint_as_float(rb.y);
-      const float3 ab = slotDelta(s, ia, ja);
-      const float3 bc = slotDelta(s, ja, ka);
-      const float3 cd = slotDelta(s, ka, la);
+      const float3 ab = v.delta(ia, ja);
+      const float3 bc = v.delta(ja, ka);
+      const float3 cd = v.delta(ka, la);
       float3 crabbc = make_float3(ab.y * bc.z - ab.z * bc.y, ab.z * bc.x - ab.x * bc.z,
                                   ab.x * bc.y - ab.y * bc.x);
       float3 crbccd = make_float3(bc.y * cd.z - bc.z * cd.y, bc.z * cd.x - bc.x * cd.z,
@@ -447,10 +474,10 @@ __device__ void valenceTerms(const DevSynthesis &d, const UnitSmem &s, int nsys_
         const float fjy = fb1 * crabbc.y - fb2 * crbccd.y;
         const float fjz = fb1 * crabbc.z - fb2 * crbccd.z;
         const float flx = -fd * crbccd.x, fly = -fd * crbccd.y, flz = -fd * crbccd.z;
-        addForce(s, ia, fix, fiy, fiz, fs);
-        addForce(s, ja, fjx, fjy, fjz, fs);
-        addForce(s, ka, -(fix + fjx + flx), -(fiy + fjy + fly), -(fiz + fjz + flz), fs);
-        addForce(s, la, flx, fly, flz, fs);
+        v.force(ia, fix, fiy, fiz, fs);
+        v.force(ja, fjx, fjy, fjz, fs);
+        v.force(ka, -(fix + fjx + flx), -(fiy + fjy + fly), -(fiz + fjz + flz), fs);
+        v.force(la, flx, fly, flz, fs);
       }
       const float edih = __fmul_rn(amp, __fadd_rn(1.0f, cos_sangle));
       if (improper) {
@@ -463,14 +490,13 @@ __device__ void valenceTerms(const DevSynthesis &d, const UnitSmem &s, int nsys_
       const float inv_scee = __uint_as_float(rb.z);
       if (inv_scee > 0.0f) {
         const float inv_scnb = __uint_as_float(rb.w);
-        const float3 dv = slotDelta(s, ia, la);
-        const float4 pi = s.prm[ia];
-        const float4 pl = s.prm[la];
+        const float3 dv = v.delta(ia, la);
+        const float4 pi = v.prm(ia);
+        const float4 pl = v.prm(la);
         const int code_i = __float_as_int(pi.y);
         const int code_l = __float_as_int(pl.y);
-        // the molecule's 1-4 table follows its standard table in shared memory
         const int nt = d.lj_ntypes[sysid];
-        const float2 ab14 = s.lj[(code_i & 0xffff) + (code_l >> 16) + nt * nt];
+        const float2 ab14 = v.lj14(code_i, code_l, nt);
         const float lja = ab14.x * inv_scnb;
         const float ljb = ab14.y * inv_scnb;
         const float qiqj = pi.x * pl.x * inv_scee;
@@ -480,8 +506,8 @@ __device__ void valenceTerms(const DevSynthesis &d, const UnitSmem &s, int nsys_
         if (FORCE) {
           const float fmag = -(qiqj * invr * invr2) +
                              (6.0f * ljb - 12.0f * lja * invr4 * invr2) * invr4 * invr4;
-          addForce(s, ia, fmag * dv.x, fmag * dv.y, fmag * dv.z, fs);
-          addForce(s, la, -fmag * dv.x, -fmag * dv.y, -fmag * dv.z, fs);
+          v.force(ia, fmag * dv.x, fmag * dv.y, fmag * dv.z, fs);
+          v.force(la, -fmag * dv.x, -fmag * dv.y, -fmag * dv.z, fs);
         }
         e_el14 = __fmul_rn(qiqj, invr);
         e_lj14 = __fsub_rn(__fmul_rn(__fmul_rn(__fmul_rn(lja, invr4), invr4), invr4),
@@ -489,10 +515,10 @@ __device__ void valenceTerms(const DevSynthesis &d, const UnitSmem &s, int nsys_
       }
     }
     if (ENERGY) {
-      warpEnergy(s, k, kProperDihedral, e_prop, es);
-      warpEnergy(s, k, kImproperDihedral, e_impr, es);
-      warpEnergy(s, k, kElec14, e_el14, es);
-      warpEnergy(s, k, kVdw14, e_lj14, es);
+      v.energy(k, kProperDihedral, e_prop, es);
+      v.energy(k, kImproperDihedral, e_impr, es);
+      v.energy(k, kElec14, e_el14, es);
+      v.energy(k, kVdw14, e_lj14, es);
     }
   }
 }
@@ -836,6 +862,49 @@ __device__ void gbDerivativeTiles(const DevSynthesis &d, const UnitSmem &s, int 
   }
 }
 // ------------------------------------------------------------------------------------------------
+// Per-atom GB steps between the pair passes (nonbonded_potential.tpp:730-805, 982-1021)
+// ------------------------------------------------------------------------------------------------
+// Effective radius of atom gi from its descreening sum psi (HCT, or OBC / OBC-II)
+__device__ __forceinline__ float effectiveRadius(const DevSynthesis &d, int gi, float psi,
+                                                 float rho) {
+  float egbi;
+  if (d.igb == 1) {
+    egbi = 1.0f / (1.0f / rho + psi);
+    if (egbi < 0.0f) egbi = 30.0f;
+  }
+  else {
+    const float fipsi = psi * (-rho);
+    egbi = 1.0f / (1.0f / rho - tanhf((d.gb_alpha[gi] - d.gb_beta[gi] * fipsi +
+                                       d.gb_gamma[gi] * fipsi * fipsi) * fipsi) /
+                                d.pb_radii[gi]);
+  }
+  return egbi;
+}
+
+// GB self energy of a charge q (scaled by sqrt of the Coulomb constant) with effective radius
+// egbi; *self_de receives its dE/dR contribution
+__device__ __forceinline__ float gbSelfTerm(const DevSynthesis &d, float q, float egbi,
+                                            float* self_de) {
+  const float expmkf = ((d.kappa > 0.0f) ? expf(-kGbKscale * d.kappa * egbi) : 1.0f) *
+                       d.inv_dielectric;
+  const float dielfac = 1.0f - expmkf;
+  const float atmq2h = 0.5f * q * q;
+  const float atmqd2h = atmq2h * dielfac;
+  *self_de = atmqd2h - kGbKscale * d.kappa * atmq2h * expmkf * egbi;
+  return -__fdiv_rn(atmqd2h, egbi);
+}
+
+// OBC chain-rule factor dR/dpsi-type prefactor applied to the summed dE/dR
+__device__ __forceinline__ float obcChainFactor(const DevSynthesis &d, int gi, float psi,
+                                                float rho) {
+  const float fipsi = psi * (-rho);
+  const float al = d.gb_alpha[gi], be = d.gb_beta[gi], ga = d.gb_gamma[gi];
+  const float thi = tanhf((al - (be - ga * fipsi) * fipsi) * fipsi);
+  return (al - (2.0f * be - 3.0f * ga * fipsi) * fipsi) * (1.0f - thi * thi) * rho /
+         d.pb_radii[gi];
+}
+
+// ------------------------------------------------------------------------------------------------
 // Work-unit staging and the staged evaluation, shared by the evaluation and minimization kernels
 // ------------------------------------------------------------------------------------------------
 struct UnitShape {
@@ -976,7 +1045,7 @@ __device__ void evaluateStaged(const DevSynthesis &d, const UnitSmem &s, const U
 
   // valence terms and GB pass 1 touch disjoint accumulators: no barrier between them
   if (VALE) {
-    valenceTerms<FORCE, ENERGY>(d, s, nsys_u);
+    valenceTerms<FORCE, ENERGY>(d, SmemValence(s), nsys_u);
     if (!gb) {
       __syncthreads();
     }
@@ -999,26 +1068,10 @@ __device__ void evaluateStaged(const DevSynthesis &d, const UnitSmem &s, const U
       if (a < s.natom[k]) {
         const int gi = d.atom_start[s.sys[k]] + a;
         const float psi = static_cast<float>(int63ToLong(s.psi[slot], s.psio[slot])) * inv_ps;
-        const float rho = prm.z;
-        if (d.igb == 1) {
-          egbi = 1.0f / (1.0f / rho + psi);
-          if (egbi < 0.0f) egbi = 30.0f;
-        }
-        else {
-          const float fipsi = psi * (-rho);
-          egbi = 1.0f / (1.0f / rho - tanhf((d.gb_alpha[gi] - d.gb_beta[gi] * fipsi +
-                                             d.gb_gamma[gi] * fipsi * fipsi) * fipsi) /
-                                      d.pb_radii[gi]);
-        }
-        const float q = prm.x;   // already scaled by sqrt(Coulomb constant)
-        const float expmkf = ((d.kappa > 0.0f) ? expf(-kGbKscale * d.kappa * egbi) : 1.0f) *
-                             d.inv_dielectric;
-        const float dielfac = 1.0f - expmkf;
-        const float atmq2h = 0.5f * q * q;
-        const float atmqd2h = atmq2h * dielfac;
-        e_self = -__fdiv_rn(atmqd2h, egbi);
+        egbi = effectiveRadius(d, gi, psi, prm.z);
+        float self_de;
+        e_self = gbSelfTerm(d, prm.x, egbi, &self_de);
         if (FORCE) {
-          const float self_de = atmqd2h - kGbKscale * d.kappa * atmq2h * expmkf * egbi;
           atomicAddInt63(self_de * ds, &s.de[slot], &s.deo[slot]);
         }
         if (WS) {
@@ -1082,12 +1135,7 @@ __device__ void evaluateStaged(const DevSynthesis &d, const UnitSmem &s, const U
         sde = static_cast<float>(int63ToLong(s.de[slot], s.deo[slot])) * inv_ds;
         if (d.igb != 1) {
           const float psi = static_cast<float>(int63ToLong(s.psi[slot], s.psio[slot])) * inv_ps;
-          const float rho = prm.z;
-          const float fipsi = psi * (-rho);
-          const float al = d.gb_alpha[gi], be = d.gb_beta[gi], ga = d.gb_gamma[gi];
-          const float thi = tanhf((al - (be - ga * fipsi) * fipsi) * fipsi);
-          sde *= (al - (2.0f * be - 3.0f * ga * fipsi) * fipsi) * (1.0f - thi * thi) * rho /
-                 d.pb_radii[gi];
+          sde *= obcChainFactor(d, gi, psi, prm.z);
         }
         if (WS) {
           d.sumdeijda[gi] = __double2ll_rn(static_cast<double>(sde) * d.psi_out_scale);

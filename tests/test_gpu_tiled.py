@@ -1,0 +1,105 @@
+"""The tiled path for large molecules (2,000-5,000-atom chains, or any molecule routed there by
+tiled_above_atoms) against the fused path, STORMM's own results and the FP64 oracle.
+
+The tiled path runs the fused kernel's pair functors and valence code with the same integer
+accumulation; compiled into different kernels, the FP32 arithmetic may round a few operations
+differently, so the two paths agree to a few units of the last fixed-point bit (forces within
+1e-6 RMS relative, energies within 1e-7 of the summed terms), and each is bit-identical from run
+to run.  Against FP64 the tolerances are those of the single-point tests."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+import stormm_b200 as sb
+from stormm_b200 import synthetic
+from fixtures import load, molecule_from_fixture, reference_forces, rms_rel
+
+pytestmark = pytest.mark.gpu
+
+ENERGY_TOL = 1.0e-6
+FORCE_TOL = 5.0e-6
+
+
+def _evaluate(mols, **opts):
+    syn = sb.Synthesis(mols, **opts)
+    syn.set_coordinates(np.concatenate([m.coords for m in mols]))
+    syn.initialize()
+    syn.evaluate()
+    assert syn.status() == 0
+    return syn
+
+
+def _close(fused, tiled):
+    e_f, e_t = fused.energy_terms(), tiled.energy_terms()
+    scale = np.maximum(np.abs(e_f).sum(axis=1), 10.0)[:, None]
+    assert np.all(np.abs(e_f - e_t) <= 1e-7 * scale)
+    assert rms_rel(tiled.forces(), fused.forces()) <= 1e-6
+
+
+def test_tiled_path_agrees_with_fused_and_repeats_exactly():
+    mols = [synthetic.make_molecule(synthetic._seed(6060, k), n, 0.1)
+            for k, n in enumerate([40, 100, 257, 300, 31])]
+    mols.append(molecule_from_fixture(load("synthetic_C600.npz")))
+    fused = _evaluate(mols)
+    tiled = _evaluate(mols, tiled_above_atoms=32)
+    _close(fused, tiled)
+    fp, _ = fused.forces_fixed()
+    tp, _ = tiled.forces_fixed()
+    assert np.abs(fp - tp).max() <= 64
+    for a, b in zip(fused.gb_workspace(), tiled.gb_workspace()):
+        np.testing.assert_allclose(b, a, rtol=1e-6, atol=1e-6)
+    prim, ovrf = tiled.forces_fixed()
+    nrg = tiled.energies_fixed().copy()
+    tiled.initialize()
+    tiled.evaluate()
+    assert np.array_equal(tiled.forces_fixed()[0], prim)
+    assert np.array_equal(tiled.energies_fixed(), nrg)
+    # energy-only and separate launchers as well
+    for syn in (fused, tiled):
+        syn.initialize()
+        syn.evaluate(force=False, energy=True)
+    e_f, e_t = fused.energy_terms(), tiled.energy_terms()
+    assert np.all(np.abs(e_f - e_t) <= 1e-7 * np.maximum(np.abs(e_f).sum(axis=1), 10.0)[:, None])
+    for syn in (fused, tiled):
+        syn.initialize()
+        syn.launch_valence()
+        syn.launch_nonbonded()
+    _close(fused, tiled)
+
+
+def test_tiled_chain_fixture_matches_stormm():
+    g = load("synthetic_C600.npz")
+    syn = _evaluate([molecule_from_fixture(g)], tiled_above_atoms=256)
+    e = syn.energy_terms()[0]
+    scale = max(np.abs(g["energy_terms"]).sum(), 10.0)
+    assert np.all(np.abs(e - g["energy_terms"]) <= ENERGY_TOL * scale)
+    assert rms_rel(syn.forces(), reference_forces(g)) <= FORCE_TOL
+
+
+def test_large_chains_against_oracle():
+    mols = [synthetic.make_chain(synthetic._seed(7070, k), n) for k, n in enumerate([2100, 2700])]
+    syn = _evaluate(mols)
+    energies = syn.energy_terms()
+    forces = syn.split(syn.forces())
+    for k, m in enumerate(mols):
+        ref = oracle.from_molecule(m).evaluate(m.coords)
+        scale = max(np.abs(ref["energies"]).sum(), 10.0)
+        assert np.all(np.abs(energies[k] - ref["energies"]) <= ENERGY_TOL * scale), k
+        assert rms_rel(forces[k], ref["forces"]) <= FORCE_TOL, k
+
+
+def test_tiled_per_system_launches_equal_batched_and_minimization_is_rejected():
+    mols = [synthetic.make_chain(synthetic._seed(7171, 0), 2200),
+            synthetic.make_molecule(synthetic._seed(7171, 1), 90, 0.1),
+            synthetic.make_chain(synthetic._seed(7171, 2), 2050)]
+    syn = _evaluate(mols)
+    f_b = syn.forces_fixed()
+    e_b = syn.energies_fixed().copy()
+    syn.initialize()
+    syn.evaluate_range(0, len(mols))
+    assert np.array_equal(syn.forces_fixed()[0], f_b[0])
+    assert np.array_equal(syn.energies_fixed(), e_b)
+    with pytest.raises(sb.StormmB200Error):
+        syn.minimize(total_cycles=2)
