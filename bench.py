@@ -40,6 +40,10 @@ MIN_CYCLES = 500
 MIN_SD_CYCLES = 50
 MIN_WORKLOAD = ("batched conformer minimization: 4096 molecules, 24-96 atoms, 0.3 A start noise, "
                 "500 cycles (50 SD then CG), OBC-II GB")
+LARGE_NSYS = 256
+LARGE_WORKLOAD = ("large implicit-solvent systems: 256 polymer-like chains of 2000-5000 atoms "
+                  "(seeded random walk, 1.5 A bonds, 2.5 A clash rejection), OBC-II GB, "
+                  "force + energy, tiled path")
 SERVED_RATES = (250.0, 1000.0, 4000.0)
 SERVED_WINDOW_S = 1.0
 SERVED_WORKLOAD = ("served minimization stream: Poisson arrivals, lognormal sizes (median 48 atoms, "
@@ -58,6 +62,7 @@ def _args():
     ap.add_argument("--no-minimization", action="store_true")
     ap.add_argument("--min-steps", type=int, default=2)
     ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--no-large", action="store_true")
     return ap.parse_args()
 
 
@@ -210,10 +215,8 @@ def _event_pair():
 def _max_over_ranks(x: float, world: int) -> float:
     if world == 1:
         return x
-    import torch
-    t = torch.tensor([x], device="cuda")
-    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    return float(t.item())
+    from stormm_b200 import sharding
+    return sharding.max_over_ranks(x, device="cuda")
 
 
 def _barrier(world: int):
@@ -392,6 +395,75 @@ def bench_minimization(args, world, rank, local, flush):
     }
 
 
+def _cpu_large(seconds: float):
+    """STORMM's CPU evaluator on this host's cores over the first 32 chains."""
+    import oracle.cpu_baseline as cpub
+    from stormm_b200 import synthetic
+    seed = synthetic.SEED_BASE + 4
+    sizes = np.random.default_rng(seed).integers(2000, 5001, size=LARGE_NSYS)
+    n = 32
+    mols = [synthetic.make_chain(synthetic._seed(seed, k), int(sizes[k])) for k in range(n)]
+    r = cpub.run(mols, seconds=seconds)
+    r["sample"] = (f"first {n} chains of the workload, {seconds:.0f} s, one single-threaded FP64 "
+                   f"process per core")
+    return r
+
+
+def bench_large(args, world, rank, local, flush):
+    """Config of 256 chains of 2,000-5,000 atoms through the tiled path."""
+    import torch
+    import stormm_b200 as sb
+    from stormm_b200 import roofline, synthetic
+    mols = synthetic.workload_chains(LARGE_NSYS, seed=synthetic.SEED_BASE + 4 + 1000 * rank)
+    natoms = np.array([m.natom for m in mols])
+    syn = sb.Synthesis(mols, device=local)
+    syn.set_coordinates(np.concatenate([m.coords for m in mols]))
+    for _ in range(3):
+        syn.initialize(sb.INIT_FORCES | sb.INIT_ENERGIES)
+        syn.evaluate()
+    torch.cuda.synchronize()
+    assert syn.status() == 0
+    times = []
+    _barrier(world)
+    for _ in range(5):
+        flush.zero_()
+        ev0, ev1 = _event_pair()
+        ev0.record()
+        syn.initialize(sb.INIT_FORCES | sb.INIT_ENERGIES)
+        syn.evaluate()
+        ev1.record()
+        torch.cuda.synchronize()
+        times.append(ev0.elapsed_time(ev1))
+    _barrier(world)
+    total_ms = _max_over_ranks(float(np.sum(times)), world)
+    value = world * LARGE_NSYS * len(times) / (total_ms / 1000.0)
+    per_sys = None
+    if rank == 0:
+        ev0, ev1 = _event_pair()
+        ev0.record()
+        syn.initialize(sb.INIT_FORCES | sb.INIT_ENERGIES)
+        syn.evaluate_range(0, 16)
+        ev1.record()
+        torch.cuda.synchronize()
+        per_sys = 16 / (ev0.elapsed_time(ev1) / 1000.0)
+    syn.close()
+    flops = roofline.flops_per_evaluation(natoms, force=True)
+    achieved = flops / (float(np.mean(times)) / 1000.0) / 1.0e12
+    peak = roofline.fp32_peak_tflops(1965.0)
+    out = {"workload": LARGE_WORKLOAD, "value": value, "unit": "force-evals/s",
+           "molecules_per_gpu": LARGE_NSYS, "atoms_total_per_gpu": int(natoms.sum()),
+           "pairs_per_pass": roofline.pair_count(natoms), "steps": len(times),
+           "ms_per_step": total_ms / len(times),
+           "p50_ms": float(np.percentile(times, 50)), "p99_ms": float(np.percentile(times, 99)),
+           "per_system_dropin": {"value": per_sys, "unit": "force-evals/s",
+                                 "sample": "first 16 chains, one launch sequence each"},
+           "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                        "frac": achieved / peak, "flops_per_step": flops},
+           "l2": "flushed (256 MB write) before every timed step",
+           "fp64_gpu_mode": "not built"}
+    return out
+
+
 def bench_served(local):
     """Poisson request streams at several rates through the continuous-batching server."""
     import stormm_b200 as sb
@@ -453,6 +525,7 @@ def main():
         sp = bench_single_point(args, world, rank, local, flush)
         mn = None if args.no_minimization else bench_minimization(args, world, rank, local, flush)
         served = None if (args.no_served or rank != 0) else bench_served(local)
+        large = None if args.no_large else bench_large(args, world, rank, local, flush)
     csum = clocks.summary()
 
     achieved = sp["flops"] / sp["kern_avg_s"] / 1.0e12
@@ -469,6 +542,15 @@ def main():
                 mn["cpu_baseline"] = {"value": rm["value"], "unit": "minimizations/s",
                                       "cores": rm["cores"], "kind": rm["kind"],
                                       "sample": rm["sample"]}
+            if large is not None:
+                try:
+                    rl = _cpu_large(args.cpu_seconds)
+                    large["cpu_baseline"] = {"value": rl["value"], "unit": "force-evals/s",
+                                             "cores": rl["cores"], "kind": rl["kind"],
+                                             "sample": rl["sample"]}
+                except Exception as exc:  # reported, not fatal
+                    large["cpu_baseline"] = {"value": None, "kind": "unavailable",
+                                             "sample": str(exc)[:200]}
         except Exception as exc:  # reported, not fatal
             cpu = {"value": None, "unit": "force-evals/s", "cores": 0, "kind": "unavailable",
                    "sample": str(exc)[:200]}
@@ -510,6 +592,7 @@ def main():
             "cpu_baseline": cpu,
             "minimization": mn,
             "served": served,
+            "large": large,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -23,6 +23,7 @@ constexpr int kTile = 32;                 // atoms per tile edge (one warp lane 
 constexpr int kMaxUnitSystems = 32;       // systems per fused work unit
 constexpr int kMaxFusedAtoms = 2048;      // largest molecule the fused path holds on chip
 constexpr int kNrgStride = 16;            // energy slots per system (STORMM StateVariable order)
+constexpr int kUnitMetaFields = 8;        // ints per unit-molecule row of DevSynthesis::unit_meta
 constexpr float kGbRadiiOffset = 0.09f;   // Constants/generalized_born.h:114
 constexpr float kGbKscale = 0.73f;        // Constants/generalized_born.h:123
 constexpr int kPsiBits = 29;              // fixed-point bits of the in-block psi accumulators
@@ -97,11 +98,14 @@ struct DevSynthesis {
   int* sumdeijda_ovrf;
   float* born_radii;             // effective radii of the last evaluation
 
-  // work units: consecutive entries of unit_systems, described by unit_desc
+  // work units, described by unit_desc, molecule tables in unit_meta
   int nunit;
-  const int4* unit_desc;         // x = first index in unit_systems, y = system count,
+  const int4* unit_desc;         // x = first row in unit_meta, y = system count,
                                  // z = atom slots (sum of padded sizes), w = tile count
-  const int* unit_systems;
+  const int* unit_meta;          // kUnitMetaFields ints per unit molecule plus a closing row per
+                                 // unit (unit_desc.x is the first row): system, atoms, first
+                                 // slot, first tile, LJ table offset, bond / angle / dihedral
+                                 // chunk offsets; the closing row holds the totals
   int max_unit_slots;
 
   int* status;                   // device status word (0 = fine)

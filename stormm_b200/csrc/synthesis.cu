@@ -391,9 +391,40 @@ std::unique_ptr<UnitPlan> Synthesis::makePlan(int max_slots_cap, int max_tiles_c
     throw Error(SB_ERR_ARGUMENT, "work units need " + std::to_string(smem) +
                 " bytes of shared memory, above the device limit");
   }
-  plan->d_units.upload(units);
-  plan->d_systems.upload(systems);
+  finalizePlan(plan.get());
   return plan;
+}
+
+// Molecule table of every unit (what each block would otherwise rebuild serially) and the
+// device descriptors pointing into it
+void Synthesis::finalizePlan(UnitPlan* plan) const {
+  std::vector<int4> desc = plan->units;
+  plan->meta.clear();
+  for (size_t u = 0; u < plan->units.size(); u++) {
+    const int4 un = plan->units[u];
+    desc[u].x = static_cast<int>(plan->meta.size() / kUnitMetaFields);
+    int slot = 0, tile = 0, lj = 0, nb = 0, na = 0, nd = 0;
+    for (int k = 0; k < un.y; k++) {
+      const int sid = plan->systems[un.x + k];
+      const int n = atom_count[sid];
+      const int nblk = (n + kTile - 1) / kTile;
+      const int row[kUnitMetaFields] = {sid, n, slot, tile, lj, nb, na, nd};
+      plan->meta.insert(plan->meta.end(), row, row + kUnitMetaFields);
+      slot += nblk * kTile;
+      tile += nblk * (nblk + 1) / 2;
+      lj += 2 * h_lj_ntypes[sid] * h_lj_ntypes[sid];
+      nb += (h_bond_start[sid + 1] - h_bond_start[sid] + 31) / 32;
+      na += (h_angl_start[sid + 1] - h_angl_start[sid] + 31) / 32;
+      nd += (h_dihe_start[sid + 1] - h_dihe_start[sid] + 31) / 32;
+    }
+    const int last[kUnitMetaFields] = {-1, 0, slot, tile, lj, nb, na, nd};
+    plan->meta.insert(plan->meta.end(), last, last + kUnitMetaFields);
+    if (slot != un.z || tile != un.w) {
+      throw Error(SB_ERR_ARGUMENT, "inconsistent work-unit descriptor");
+    }
+  }
+  plan->d_units.upload(desc);
+  plan->d_meta.upload(plan->meta);
 }
 
 void Synthesis::buildUnits() {
@@ -435,13 +466,14 @@ void Synthesis::buildUnits() {
     const int nb = (atom_count[s] + kTile - 1) / kTile;
     return nb * (nb + 1) / 2;
   };
-  h_single_units.resize(nsys);
-  h_single_systems.resize(nsys);
+  single_plan = std::make_unique<UnitPlan>();
+  single_plan->units.resize(nsys);
+  single_plan->systems.resize(nsys);
   single_slots = 0;
   single_lj = 0;
   for (int s = 0; s < nsys; s++) {
-    h_single_units[s] = make_int4(s, 1, slots_of(s), tiles_of(s));
-    h_single_systems[s] = s;
+    single_plan->units[s] = make_int4(s, 1, slots_of(s), tiles_of(s));
+    single_plan->systems[s] = s;
     if (tiled_index[s] < 0) {
       single_slots = std::max(single_slots, slots_of(s));
       single_lj = std::max(single_lj, 2 * h_lj_ntypes[s] * h_lj_ntypes[s]);
@@ -479,7 +511,7 @@ void Synthesis::upload() {
   d_dihe_b.upload(h_dihe_b);
   d_tile_mask_idx.upload(h_tile_mask_idx);
   d_mask_pool.upload(h_mask_pool);
-  d_single_units.upload(h_single_units);
+  finalizePlan(single_plan.get());
   d_tiled_systems.upload(h_tiled_systems);
   d_tile_prefix.upload(h_tile_prefix);
   d_atom_prefix.upload(h_atom_prefix);
@@ -498,7 +530,6 @@ void Synthesis::upload() {
   dev_tiled.de_acc = d_tiled_de.p;
   dev_tiled.radius = d_tiled_radius.p;
   dev_tiled.sde = d_tiled_sde.p;
-  d_single_systems.upload(h_single_systems);
   d_unpadded_map.upload(h_unpadded_map);
   d_stage_xyz.zeros(static_cast<size_t>(3) * natom_total);
   d_stage_nrg.zeros(static_cast<size_t>(nsys) * kNrgStride);
@@ -575,7 +606,7 @@ void Synthesis::upload() {
   d.born_radii = d_born_radii.p;
   d.nunit = eval_plan->units.size();
   d.unit_desc = eval_plan->d_units.p;
-  d.unit_systems = eval_plan->d_systems.p;
+  d.unit_meta = eval_plan->d_meta.p;
   d.max_unit_slots = max_unit_slots;
   d.status = d_status.p;
 }
@@ -586,7 +617,7 @@ void Synthesis::launchPlan(const UnitPlan &plan, int terms, bool force, bool ene
   DevSynthesis d = dev;
   d.nunit = nunit;
   d.unit_desc = plan.d_units.p;
-  d.unit_systems = plan.d_systems.p;
+  d.unit_meta = plan.d_meta.p;
   if (plan.n_big > 0) {
     d.max_unit_slots = plan.big_slots;
     cudaCheck(launchEvalFused(d, 0, plan.n_big, plan.big_lj, terms, force, energy, plan.n_big,
@@ -642,8 +673,8 @@ void Synthesis::evaluateRange(int first, int count, int terms, bool force, bool 
     return;
   }
   DevSynthesis d = dev;
-  d.unit_desc = d_single_units.p;
-  d.unit_systems = d_single_systems.p;
+  d.unit_desc = single_plan->d_units.p;
+  d.unit_meta = single_plan->d_meta.p;
   d.nunit = nsys;
   d.max_unit_slots = single_slots;
   for (int s = first; s < first + count; s++) {
@@ -845,7 +876,7 @@ void Synthesis::launchMinPlan(const UnitPlan &plan, int cycles, bool final_energ
   DevSynthesis d = dev;
   d.nunit = nunit;
   d.unit_desc = plan.d_units.p;
-  d.unit_systems = plan.d_systems.p;
+  d.unit_meta = plan.d_meta.p;
   if (plan.n_big > 0) {
     d.max_unit_slots = plan.big_slots;
     m.queue = d_queue.p;
@@ -885,8 +916,8 @@ void Synthesis::minimizeRange(int first, int count, const sb_minimize_controls &
   }
   minimizeBegin(ctl, stream);
   DevSynthesis d = dev;
-  d.unit_desc = d_single_units.p;
-  d.unit_systems = d_single_systems.p;
+  d.unit_desc = single_plan->d_units.p;
+  d.unit_meta = single_plan->d_meta.p;
   d.nunit = nsys;
   d.max_unit_slots = single_slots;
   if (static_cast<int>(minimizeSmemBytes(single_slots, single_lj)) > max_smem_optin) {
@@ -981,7 +1012,7 @@ void Synthesis::autotune(int what, int* chosen_slots, int* chosen_tiles, double*
     eval_plan = std::move(best_plan);
     dev.nunit = eval_plan->units.size();
     dev.unit_desc = eval_plan->d_units.p;
-    dev.unit_systems = eval_plan->d_systems.p;
+    dev.unit_meta = eval_plan->d_meta.p;
   }
   else {
     min_plan = std::move(best_plan);

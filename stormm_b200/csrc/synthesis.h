@@ -102,8 +102,9 @@ struct UnitPlan {
   int n_big = 0;                 // units [0, n_big) hold one molecule above the packing cap
   int big_slots = 0, big_lj = 0;
   int small_slots = 0, small_lj = 0;
-  DeviceArray<int4> d_units;
-  DeviceArray<int> d_systems;
+  std::vector<int> meta;         // kUnitMetaFields ints per molecule row, plus a closing row
+  DeviceArray<int4> d_units;     // as units, but x = first row of the unit in meta
+  DeviceArray<int> d_meta;
 };
 
 class Synthesis {
@@ -143,6 +144,7 @@ public:
   int max_unit_slots = 0;
   std::unique_ptr<UnitPlan> eval_plan;   // batched evaluation
   std::unique_ptr<UnitPlan> min_plan;    // batched minimization
+  std::unique_ptr<UnitPlan> single_plan; // one unit per system, in system order
   int tiled_threshold = kMaxFusedAtoms;  // molecules above it take the tiled path
   std::vector<int> h_tiled_systems, h_tile_prefix, h_atom_prefix;
   std::vector<int> tiled_index;          // per system: index among tiled molecules, or -1
@@ -158,8 +160,6 @@ public:
   std::vector<float2> h_ljab, h_ljab14;
   std::vector<uint4> h_bonds, h_angles, h_dihe_a, h_dihe_b;
   std::vector<unsigned int> h_mask_pool;
-  std::vector<int4> h_single_units;
-  std::vector<int> h_single_systems;
   std::vector<long long> h_stage_ll;
   std::vector<int> h_unpadded_map;   // padded index of each unpadded atom
 
@@ -170,8 +170,6 @@ public:
   DeviceArray<float2> d_ljab, d_ljab14;
   DeviceArray<uint4> d_bonds, d_angles, d_dihe_a, d_dihe_b;
   DeviceArray<unsigned int> d_mask_pool;
-  DeviceArray<int4> d_single_units;
-  DeviceArray<int> d_single_systems;
   DeviceArray<long long> d_xcrd, d_ycrd, d_zcrd, d_xfrc, d_yfrc, d_zfrc;
   DeviceArray<int> d_xcrd_ovrf, d_ycrd_ovrf, d_zcrd_ovrf, d_xfrc_ovrf, d_yfrc_ovrf, d_zfrc_ovrf;
   DeviceArray<unsigned long long> d_energies;
@@ -199,6 +197,7 @@ public:
 private:
   void buildLayout(const sb_topology* tops, int ntop);
   std::unique_ptr<UnitPlan> makePlan(int max_slots_cap, int max_tiles_cap) const;
+  void finalizePlan(UnitPlan* plan) const;
   void launchPlan(const UnitPlan &plan, int terms, bool force, bool energy, cudaStream_t stream);
   void launchMinPlan(const UnitPlan &plan, int cycles, bool final_energy, cudaStream_t stream);
   void launchTiledRange(int mol_begin, int mol_end, int terms, bool force, bool energy,

@@ -923,54 +923,37 @@ __device__ bool stageUnitTables(const DevSynthesis &d, const UnitSmem &s, int u,
   shape->nsys = nsys_u;
   shape->nslots = desc.z;
   shape->ntiles = desc.w;
-  if (threadIdx.x < nsys_u) {
-    const int sysid = d.unit_systems[desc.x + threadIdx.x];
-    s.sys[threadIdx.x] = sysid;
-    s.natom[threadIdx.x] = d.atom_count[sysid];
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int slot = 0, tile = 0, lj = 0, nb = 0, na = 0, nd = 0;
-    for (int k = 0; k < nsys_u; k++) {
-      const int sysid = s.sys[k];
-      const int n = s.natom[k];
-      const int nblk = (n + kTile - 1) / kTile;
-      s.slot0[k] = slot;
-      s.tile0[k] = tile;
-      s.ljbase[k] = lj;
-      s.bchunk0[k] = nb;
-      s.achunk0[k] = na;
-      s.dchunk0[k] = nd;
-      slot += nblk * kTile;
-      tile += nblk * (nblk + 1) / 2;
-      const int nt = d.lj_ntypes[sysid];
-      lj += 2 * nt * nt;
-      nb += (d.bond_start[sysid + 1] - d.bond_start[sysid] + 31) / 32;
-      na += (d.angl_start[sysid + 1] - d.angl_start[sysid] + 31) / 32;
-      nd += (d.dihe_start[sysid + 1] - d.dihe_start[sysid] + 31) / 32;
-    }
-    s.tile0[nsys_u] = tile;
-    s.bchunk0[nsys_u] = nb;
-    s.achunk0[nsys_u] = na;
-    s.dchunk0[nsys_u] = nd;
-    s.ljbase[nsys_u] = lj;
-    if (slot != desc.z || tile != desc.w || lj > max_lj || slot > d.max_unit_slots) {
-      atomicOr(d.status, 1);
+  // the unit's molecule table, precomputed on the host: one coalesced load per field
+  const int* meta = d.unit_meta + static_cast<size_t>(desc.x) * kUnitMetaFields;
+  for (int e = threadIdx.x; e < (nsys_u + 1) * kUnitMetaFields; e += blockDim.x) {
+    const int k = e / kUnitMetaFields;
+    const int v = meta[e];
+    switch (e % kUnitMetaFields) {
+      case 0: if (k < nsys_u) s.sys[k] = v; break;
+      case 1: if (k < nsys_u) s.natom[k] = v; break;
+      case 2: if (k < nsys_u) s.slot0[k] = v; break;
+      case 3: s.tile0[k] = v; break;
+      case 4: s.ljbase[k] = v; break;
+      case 5: s.bchunk0[k] = v; break;
+      case 6: s.achunk0[k] = v; break;
+      default: s.dchunk0[k] = v; break;
     }
   }
   __syncthreads();
   if (desc.z > d.max_unit_slots || s.ljbase[nsys_u] > max_lj) {
+    if (threadIdx.x == 0) {
+      atomicOr(d.status, 1);
+    }
     return false;   // reported through the status word; nothing in the unit is touched
   }
-  // Lennard-Jones tables (standard then 1-4) of every molecule
-  for (int k = 0; k < nsys_u; k++) {
+  // Lennard-Jones tables (standard then 1-4) of every molecule, all entries in parallel
+  for (int e = threadIdx.x; e < s.ljbase[nsys_u]; e += blockDim.x) {
+    const int k = findOwner(s.ljbase, nsys_u, e);
     const int sysid = s.sys[k];
     const int nt = d.lj_ntypes[sysid];
-    const int src = d.lj_start[sysid];
-    for (int e = threadIdx.x; e < nt * nt; e += blockDim.x) {
-      s.lj[s.ljbase[k] + e] = d.ljab[src + e];
-      s.lj[s.ljbase[k] + nt * nt + e] = d.ljab14[src + e];
-    }
+    const int rel = e - s.ljbase[k];
+    const int src = d.lj_start[sysid] + (rel < nt * nt ? rel : rel - nt * nt);
+    s.lj[e] = (rel < nt * nt) ? d.ljab[src] : d.ljab14[src];
   }
   __syncthreads();
   return true;
