@@ -44,7 +44,7 @@ kEvalFused(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
   const UnitSmem s = carveSmem(smem_raw, d.max_unit_slots, max_lj);
   for (int u = unit_begin + blockIdx.x; u < unit_end; u += gridDim.x) {
     UnitShape us;
-    if (!stageUnitTables(d, s, u, max_lj, &us)) {
+    if (!stageUnitTables(d, s, u, max_lj, &us, BlockTeam())) {
       continue;
     }
     for (int e = threadIdx.x; e < us.nsys * kNrgStride; e += blockDim.x) {
@@ -61,7 +61,7 @@ kEvalFused(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
                 real ? d.zcrd[gi] : 0ll);
     }
     __syncthreads();
-    evaluateStaged<FORCE, ENERGY, TERMS, true>(d, s, us);
+    evaluateStaged<FORCE, ENERGY, TERMS, true>(d, s, us, BlockTeam());
 
     // commit forces (each atom belongs to exactly one unit) and energies
     if (FORCE) {

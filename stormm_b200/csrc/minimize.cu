@@ -46,30 +46,32 @@ enum MolSlot : int {
 };
 
 struct MinSmem {
+  int msys;       // molecules the carve-out holds (stride of mol)
   double* part;   // three partial sums per 32-slot chunk
-  double* mol;    // kMolDoubles x kMaxUnitSystems
+  double* mol;    // kMolDoubles x msys
   int* cyc;       // completed cycles
   int* done;      // converged (no further moves)
   int* act;       // moving in the current cycle: not converged, below the cycle limit
 };
 
-__host__ __device__ inline size_t minSmemBytes(int max_slots) {
-  return sizeof(double) * (3 * (max_slots / kTile) + kMolDoubles * kMaxUnitSystems) +
-         sizeof(int) * 3 * kMaxUnitSystems;
+__host__ __device__ inline size_t minSmemBytes(int max_slots, int max_sys) {
+  return alignUp(sizeof(double) * (3 * (max_slots / kTile) + kMolDoubles * max_sys) +
+                 sizeof(int) * 3 * max_sys, 16);
 }
 
-__device__ MinSmem carveMinSmem(char* base, int max_slots) {
+__device__ MinSmem carveMinSmem(char* base, int max_slots, int max_sys) {
   MinSmem m;
+  m.msys = max_sys;
   m.part = reinterpret_cast<double*>(base);
   m.mol = m.part + 3 * (max_slots / kTile);
-  m.cyc = reinterpret_cast<int*>(m.mol + kMolDoubles * kMaxUnitSystems);
-  m.done = m.cyc + kMaxUnitSystems;
-  m.act = m.done + kMaxUnitSystems;
+  m.cyc = reinterpret_cast<int*>(m.mol + kMolDoubles * max_sys);
+  m.done = m.cyc + max_sys;
+  m.act = m.done + max_sys;
   return m;
 }
 
 __device__ __forceinline__ double& molValue(const MinSmem &ms, int slot, int k) {
-  return ms.mol[slot * kMaxUnitSystems + k];
+  return ms.mol[slot * ms.msys + k];
 }
 
 __device__ __forceinline__ double warpSumDouble(double v) {
@@ -101,12 +103,13 @@ __device__ __forceinline__ double moleculeEnergy(const DevSynthesis &d, const Un
 }
 
 // Place every slot of the unit at the current coordinates and clear the accumulators
+template <class Team>
 __device__ void placeUnit(const DevSynthesis &d, const DevMinimizer &m, const UnitSmem &s,
-                          const UnitShape &us) {
-  for (int e = threadIdx.x; e < us.nsys * kNrgStride; e += blockDim.x) {
+                          const UnitShape &us, const Team &team) {
+  for (int e = team.rank(); e < us.nsys * kNrgStride; e += team.size()) {
     s.nrg[e] = 0ull;
   }
-  for (int slot = threadIdx.x; slot < us.nslots; slot += blockDim.x) {
+  for (int slot = team.rank(); slot < us.nslots; slot += team.size()) {
     const int k = findOwner(s.slot0, us.nsys, slot);
     const int a = slot - s.slot0[k];
     const bool real = a < s.natom[k];
@@ -114,13 +117,14 @@ __device__ void placeUnit(const DevSynthesis &d, const DevMinimizer &m, const Un
     placeSlot(d, s, slot, real, real ? m.xcrd[gi] : 0ll, real ? m.ycrd[gi] : 0ll,
               real ? m.zcrd[gi] : 0ll);
   }
-  __syncthreads();
+  team.sync();
 }
 
 // Move every atom of the molecules with a nonzero step along the direction
+template <class Team>
 __device__ void moveUnit(const DevSynthesis &d, const DevMinimizer &m, const UnitSmem &s,
-                         const MinSmem &ms, const UnitShape &us) {
-  for (int slot = threadIdx.x; slot < us.nslots; slot += blockDim.x) {
+                         const MinSmem &ms, const UnitShape &us, const Team &team) {
+  for (int slot = team.rank(); slot < us.nslots; slot += team.size()) {
     const int k = findOwner(s.slot0, us.nsys, slot);
     const int a = slot - s.slot0[k];
     const double step = molValue(ms, kStep, k);
@@ -215,19 +219,20 @@ __device__ double finalPlacement(const double* ev, const double* mv, double* new
 }
 
 // One line-minimization cycle of every unit molecule that has not converged
-template <bool HIST>
+template <bool HIST, class Team>
 __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
-                                  const UnitSmem &s, const MinSmem &ms, const UnitShape &us) {
+                                  const UnitSmem &s, const MinSmem &ms, const UnitShape &us,
+                                  const Team &team) {
   const int lane = threadIdx.x & 31;
   const double inv_fs = 1.0 / static_cast<double>(d.frc_scale);
   const double gpos_scale = 1.0 / d.inv_gpos_scale;
 
   // 1. forces and energy at the line start
-  placeUnit(d, m, s, us);
-  evaluateStaged<true, true, 7, false>(d, s, us);
+  placeUnit(d, m, s, us, team);
+  evaluateStaged<true, true, 7, false>(d, s, us, team);
 
   // 2. gg, dgg and |f|^2 per 32-slot chunk (a chunk never straddles two molecules)
-  for (int slot = threadIdx.x; slot < us.nslots; slot += blockDim.x) {
+  for (int slot = team.rank(); slot < us.nslots; slot += team.size()) {
     const int k = findOwner(s.slot0, us.nsys, slot);
     const int a = slot - s.slot0[k];
     double gg = 0.0, dgg = 0.0, ff = 0.0;
@@ -253,9 +258,9 @@ __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
       ms.part[3 * q + 2] = ff;
     }
   }
-  __syncthreads();
-  if (threadIdx.x < us.nsys) {
-    const int k = threadIdx.x;
+  team.sync();
+  if (team.rank() < us.nsys) {
+    const int k = team.rank();
     const int sysid = s.sys[k];
     const double gg = moleculeSum(s, ms, k, 0) * inv_fs * inv_fs;
     const double dgg = moleculeSum(s, ms, k, 1) * inv_fs * inv_fs;
@@ -277,10 +282,10 @@ __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
     const int step = ms.cyc[k] + 1;
     molValue(ms, kMfac, k) = (step >= m.sd_cycles && gg > 0.0) ? dgg / gg : 0.0;   // gamma
   }
-  __syncthreads();
+  team.sync();
 
   // conjugate direction, previous force, |direction|^2
-  for (int slot = threadIdx.x; slot < us.nslots; slot += blockDim.x) {
+  for (int slot = team.rank(); slot < us.nslots; slot += team.size()) {
     const int k = findOwner(s.slot0, us.nsys, slot);
     const int a = slot - s.slot0[k];
     double msum = 0.0;
@@ -313,11 +318,11 @@ __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
       ms.part[3 * (slot / kTile)] = msum;
     }
   }
-  __syncthreads();
+  team.sync();
 
   // 3. first trial move: 1 x the move length
-  if (threadIdx.x < us.nsys) {
-    const int k = threadIdx.x;
+  if (team.rank() < us.nsys) {
+    const int k = team.rank();
     if (ms.act[k]) {
       const double msum = moleculeSum(s, ms, k, 0);
       const double inv_norm = (msum > 0.0) ? 1.0 / sqrt(msum) : 0.0;
@@ -332,14 +337,14 @@ __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
       molValue(ms, kStep, k) = 0.0;
     }
   }
-  __syncthreads();
-  moveUnit(d, m, s, ms, us);
-  placeUnit(d, m, s, us);
-  evaluateStaged<false, true, 7, false>(d, s, us);
+  team.sync();
+  moveUnit(d, m, s, ms, us, team);
+  placeUnit(d, m, s, us, team);
+  evaluateStaged<false, true, 7, false>(d, s, us, team);
 
   // second trial move: 1.04 x after a decrease, else 0.8 x
-  if (threadIdx.x < us.nsys) {
-    const int k = threadIdx.x;
+  if (team.rank() < us.nsys) {
+    const int k = team.rank();
     const double e1 = moleculeEnergy(d, s, k);
     molValue(ms, kE1, k) = e1;
     if (ms.act[k]) {
@@ -350,14 +355,14 @@ __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
                                gpos_scale;
     }
   }
-  __syncthreads();
-  moveUnit(d, m, s, ms, us);
-  placeUnit(d, m, s, us);
-  evaluateStaged<false, true, 7, false>(d, s, us);
+  team.sync();
+  moveUnit(d, m, s, ms, us, team);
+  placeUnit(d, m, s, us, team);
+  evaluateStaged<false, true, 7, false>(d, s, us, team);
 
   // third trial move: the last factor x 1.03 after a decrease, else x 0.85
-  if (threadIdx.x < us.nsys) {
-    const int k = threadIdx.x;
+  if (team.rank() < us.nsys) {
+    const int k = team.rank();
     const double e2 = moleculeEnergy(d, s, k);
     molValue(ms, kE2, k) = e2;
     if (ms.act[k]) {
@@ -368,14 +373,14 @@ __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
                                gpos_scale;
     }
   }
-  __syncthreads();
-  moveUnit(d, m, s, ms, us);
-  placeUnit(d, m, s, us);
-  evaluateStaged<false, true, 7, false>(d, s, us);
+  team.sync();
+  moveUnit(d, m, s, ms, us, team);
+  placeUnit(d, m, s, us, team);
+  evaluateStaged<false, true, 7, false>(d, s, us, team);
 
   // 4. cubic fit and final placement
-  if (threadIdx.x < us.nsys) {
-    const int k = threadIdx.x;
+  if (team.rank() < us.nsys) {
+    const int k = team.rank();
     const double e3 = moleculeEnergy(d, s, k);
     if (ms.act[k]) {
       const double ev[4] = {molValue(ms, kE0, k), molValue(ms, kE1, k), molValue(ms, kE2, k), e3};
@@ -393,72 +398,83 @@ __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
       molValue(ms, kStep, k) = 0.0;
     }
   }
-  __syncthreads();
-  moveUnit(d, m, s, ms, us);
-  __syncthreads();
+  team.sync();
+  moveUnit(d, m, s, ms, us, team);
+  team.sync();
 }
 
+// Every cycle of one work unit, then its final energies and state
+template <bool HIST, class Team>
+__device__ void minimizeUnit(const DevSynthesis &d, const DevMinimizer &m, const UnitSmem &s,
+                             const MinSmem &ms, int u, int max_lj, int max_sys, int cycles,
+                             int final_energy, const Team &team) {
+  UnitShape us;
+  if (!stageUnitTables(d, s, u, max_lj, &us, team, max_sys)) {
+    return;
+  }
+  for (int slot = team.rank(); slot < us.nslots; slot += team.size()) {
+    const int k = findOwner(s.slot0, us.nsys, slot);
+    s.prm[slot] = slotParameters(d, s, k, slot - s.slot0[k]);
+  }
+  if (team.rank() < us.nsys) {
+    const int k = team.rank();
+    const int sysid = s.sys[k];
+    ms.cyc[k] = m.cycle[sysid];
+    ms.done[k] = m.done[sysid];
+    molValue(ms, kLMove, k) = m.l_move[sysid];
+  }
+  team.sync();
+  for (int c = 0; c < cycles; c++) {
+    int moving = 0;
+    if (team.rank() < us.nsys) {
+      const int k = team.rank();
+      moving = (!ms.done[k] && ms.cyc[k] < m.max_cycles) ? 1 : 0;
+      ms.act[k] = moving;
+    }
+    if (!team.any(moving != 0)) {
+      break;
+    }
+    minimizationCycle<HIST>(d, m, s, ms, us, team);
+  }
+  if (final_energy) {
+    // one more energy evaluation at the final coordinates (hpc_minimization.cu:372-383)
+    placeUnit(d, m, s, us, team);
+    evaluateStaged<false, true, 7, false>(d, s, us, team);
+    for (int e = team.rank(); e < us.nsys * kNrgStride; e += team.size()) {
+      d.energies[s.sys[e / kNrgStride] * kNrgStride + (e % kNrgStride)] = s.nrg[e];
+    }
+    if (HIST && team.rank() < us.nsys) {
+      const int k = team.rank();
+      if (ms.cyc[k] < m.hist_stride) {
+        m.history[static_cast<size_t>(s.sys[k]) * m.hist_stride + ms.cyc[k]] =
+          moleculeEnergy(d, s, k);
+      }
+    }
+  }
+  if (team.rank() < us.nsys) {
+    const int k = team.rank();
+    const int sysid = s.sys[k];
+    m.cycle[sysid] = ms.cyc[k];
+    m.done[sysid] = ms.done[k];
+    m.l_move[sysid] = molValue(ms, kLMove, k);
+  }
+  team.sync();
+}
+
+// One thread block per work unit (molecules of up to 2,048 atoms)
 template <bool HIST>
 __global__ void __launch_bounds__(256, 4)
 kMinimize(const DevSynthesis d, const DevMinimizer m, int unit_begin, int unit_end, int max_lj,
           int cycles, int final_energy) {
   extern __shared__ __align__(16) char smem_raw[];
   const UnitSmem s = carveSmem(smem_raw, d.max_unit_slots, max_lj);
-  const MinSmem ms = carveMinSmem(smem_raw + alignUp(unitSmemBytes(d.max_unit_slots, max_lj), 16),
-                                  d.max_unit_slots);
+  const MinSmem ms = carveMinSmem(smem_raw + unitSmemBytes(d.max_unit_slots, max_lj),
+                                  d.max_unit_slots, kMaxUnitSystems);
   __shared__ int next_unit;
+  const BlockTeam team;
   int u = unit_begin + blockIdx.x;
   while (u < unit_end) {
-    UnitShape us;
-    if (stageUnitTables(d, s, u, max_lj, &us)) {
-      for (int slot = threadIdx.x; slot < us.nslots; slot += blockDim.x) {
-        const int k = findOwner(s.slot0, us.nsys, slot);
-        s.prm[slot] = slotParameters(d, s, k, slot - s.slot0[k]);
-      }
-      if (threadIdx.x < us.nsys) {
-        const int k = threadIdx.x;
-        const int sysid = s.sys[k];
-        ms.cyc[k] = m.cycle[sysid];
-        ms.done[k] = m.done[sysid];
-        molValue(ms, kLMove, k) = m.l_move[sysid];
-      }
-      __syncthreads();
-      for (int c = 0; c < cycles; c++) {
-        int moving = 0;
-        if (threadIdx.x < us.nsys) {
-          const int k = threadIdx.x;
-          moving = (!ms.done[k] && ms.cyc[k] < m.max_cycles) ? 1 : 0;
-          ms.act[k] = moving;
-        }
-        if (!__syncthreads_or(moving)) {
-          break;
-        }
-        minimizationCycle<HIST>(d, m, s, ms, us);
-      }
-      if (final_energy) {
-        // one more energy evaluation at the final coordinates (hpc_minimization.cu:372-383)
-        placeUnit(d, m, s, us);
-        evaluateStaged<false, true, 7, false>(d, s, us);
-        for (int e = threadIdx.x; e < us.nsys * kNrgStride; e += blockDim.x) {
-          d.energies[s.sys[e / kNrgStride] * kNrgStride + (e % kNrgStride)] = s.nrg[e];
-        }
-        if (HIST && threadIdx.x < us.nsys) {
-          const int k = threadIdx.x;
-          if (ms.cyc[k] < m.hist_stride) {
-            m.history[static_cast<size_t>(s.sys[k]) * m.hist_stride + ms.cyc[k]] =
-              moleculeEnergy(d, s, k);
-          }
-        }
-      }
-      if (threadIdx.x < us.nsys) {
-        const int k = threadIdx.x;
-        const int sysid = s.sys[k];
-        m.cycle[sysid] = ms.cyc[k];
-        m.done[sysid] = ms.done[k];
-        m.l_move[sysid] = molValue(ms, kLMove, k);
-      }
-    }
-    __syncthreads();
+    minimizeUnit<HIST>(d, m, s, ms, u, max_lj, kMaxUnitSystems, cycles, final_energy, team);
     if (threadIdx.x == 0) {
       next_unit = unit_begin + static_cast<int>(gridDim.x) + atomicAdd(m.queue, 1);
     }
@@ -488,8 +504,9 @@ __global__ void kMinimizerReset(DevMinimizer m, int nsys, int natom_padded, doub
 }  // namespace
 
 size_t minimizeSmemBytes(int max_slots, int max_lj) {
-  return alignUp(unitSmemBytes(max_slots, max_lj), 16) + minSmemBytes(max_slots);
+  return unitSmemBytes(max_slots, max_lj) + minSmemBytes(max_slots, kMaxUnitSystems);
 }
+
 
 cudaError_t launchMinimizerReset(const DevMinimizer &m, const DevSynthesis &d, double dx0,
                                  cudaStream_t stream) {

@@ -147,17 +147,19 @@ __host__ __device__ inline size_t alignUp(size_t x, size_t a) { return (x + a - 
 constexpr int kSlotBytes = 3 * 16 + 8 + 10 * 4;
 
 // Dynamic shared memory of one work unit's evaluation: max_slots atom slots, max_lj table entries
-__host__ __device__ inline size_t unitSmemBytes(int max_slots, int max_lj) {
+__host__ __device__ inline size_t unitSmemBytes(int max_slots, int max_lj,
+                                                int max_sys = kMaxUnitSystems) {
   size_t b = static_cast<size_t>(kSlotBytes) * max_slots;
   b = alignUp(b, 16);
   b += sizeof(float2) * max_lj;
   b = alignUp(b, 16);
-  b += sizeof(unsigned long long) * kMaxUnitSystems * kNrgStride;
-  b += sizeof(int) * (3 * kMaxUnitSystems + 5 * (kMaxUnitSystems + 1));
-  return b;
+  b += sizeof(unsigned long long) * max_sys * kNrgStride;
+  b += sizeof(int) * (3 * max_sys + 5 * (max_sys + 1));
+  return alignUp(b, 16);
 }
 
-__device__ UnitSmem carveSmem(char* base, int max_slots, int max_lj) {
+__device__ UnitSmem carveSmem(char* base, int max_slots, int max_lj,
+                              int max_sys = kMaxUnitSystems) {
   UnitSmem s;
   size_t off = 0;
   s.pa = reinterpret_cast<float4*>(base + off); off += sizeof(float4) * max_slots;
@@ -179,18 +181,38 @@ __device__ UnitSmem carveSmem(char* base, int max_slots, int max_lj) {
   s.lj = reinterpret_cast<float2*>(base + off); off += sizeof(float2) * max_lj;
   off = alignUp(off, 16);
   s.nrg = reinterpret_cast<unsigned long long*>(base + off);
-  off += sizeof(unsigned long long) * kMaxUnitSystems * kNrgStride;
+  off += sizeof(unsigned long long) * max_sys * kNrgStride;
   int* q = reinterpret_cast<int*>(base + off);
-  s.sys = q; q += kMaxUnitSystems;
-  s.slot0 = q; q += kMaxUnitSystems;
-  s.natom = q; q += kMaxUnitSystems;
-  s.ljbase = q; q += kMaxUnitSystems + 1;
-  s.tile0 = q; q += kMaxUnitSystems + 1;
-  s.bchunk0 = q; q += kMaxUnitSystems + 1;
-  s.achunk0 = q; q += kMaxUnitSystems + 1;
-  s.dchunk0 = q; q += kMaxUnitSystems + 1;
+  s.sys = q; q += max_sys;
+  s.slot0 = q; q += max_sys;
+  s.natom = q; q += max_sys;
+  s.ljbase = q; q += max_sys + 1;
+  s.tile0 = q; q += max_sys + 1;
+  s.bchunk0 = q; q += max_sys + 1;
+  s.achunk0 = q; q += max_sys + 1;
+  s.dchunk0 = q; q += max_sys + 1;
   return s;
 }
+
+// The threads that evaluate one work unit together: a whole block, or a single warp (small
+// molecules, where block-wide barriers would cost more than the work between them)
+struct BlockTeam {
+  __device__ __forceinline__ int rank() const { return threadIdx.x; }
+  __device__ __forceinline__ int size() const { return blockDim.x; }
+  __device__ __forceinline__ int warp() const { return threadIdx.x >> 5; }
+  __device__ __forceinline__ int warps() const { return blockDim.x >> 5; }
+  __device__ __forceinline__ void sync() const { __syncthreads(); }
+  __device__ __forceinline__ bool any(bool p) const { return __syncthreads_or(p) != 0; }
+};
+
+struct WarpTeam {
+  __device__ __forceinline__ int rank() const { return threadIdx.x & 31; }
+  __device__ __forceinline__ int size() const { return 32; }
+  __device__ __forceinline__ int warp() const { return 0; }
+  __device__ __forceinline__ int warps() const { return 1; }
+  __device__ __forceinline__ void sync() const { __syncwarp(); }
+  __device__ __forceinline__ bool any(bool p) const { return __any_sync(0xffffffffu, p) != 0; }
+};
 
 // Index of the unit molecule that owns position pos of a prefix-sum array of n + 1 entries
 __device__ __forceinline__ int findOwner(const int* prefix, int n, int pos) {
@@ -257,11 +279,13 @@ struct SmemValence {
   const int* dchunk0;
   const int* sys;
   const int* slot0;
-  __device__ explicit SmemValence(const UnitSmem &s_in) :
+  int begin;
+  int stride;
+  __device__ SmemValence(const UnitSmem &s_in, int begin_in, int stride_in) :
       s(s_in), bchunk0(s_in.bchunk0), achunk0(s_in.achunk0), dchunk0(s_in.dchunk0),
-      sys(s_in.sys), slot0(s_in.slot0) {}
-  __device__ __forceinline__ int chunkBegin() const { return threadIdx.x >> 5; }
-  __device__ __forceinline__ int chunkStride() const { return blockDim.x >> 5; }
+      sys(s_in.sys), slot0(s_in.slot0), begin(begin_in), stride(stride_in) {}
+  __device__ __forceinline__ int chunkBegin() const { return begin; }
+  __device__ __forceinline__ int chunkStride() const { return stride; }
   __device__ __forceinline__ float4 pa(int i) const { return s.pa[i]; }
   __device__ __forceinline__ float4 pb(int i) const { return s.pb[i]; }
   __device__ __forceinline__ float4 prm(int i) const { return s.prm[i]; }
@@ -752,11 +776,11 @@ struct DerivPass {
   }
 };
 
-__device__ void gbRadiiTiles(const UnitSmem &s, int nsys_u, int ntiles) {
+__device__ void gbRadiiTiles(const UnitSmem &s, int nsys_u, int ntiles, int first, int stride) {
   const int lane = threadIdx.x & 31;
   const float ps = static_cast<float>(1 << kPsiBits);
   RadiiPass p(s);
-  for (int t = threadIdx.x >> 5; t < ntiles; t += blockDim.x >> 5) {
+  for (int t = first; t < ntiles; t += stride) {
     const TileInfo ti = tileInfo(s, nsys_u, t);
     p.begin(ti.ibase + lane);
     walkTile(p, ti, lane);
@@ -771,7 +795,8 @@ __device__ void gbRadiiTiles(const UnitSmem &s, int nsys_u, int ntiles) {
 }
 
 template <bool FORCE, bool ENERGY, bool NB, bool GB>
-__device__ void pairTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u, int ntiles) {
+__device__ void pairTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u, int ntiles,
+                          int first, int stride) {
   const int lane = threadIdx.x & 31;
   const float fs = d.frc_scale;
   const float es = d.nrg_scale;
@@ -779,7 +804,7 @@ __device__ void pairTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u, 
   PairPass<FORCE, ENERGY, NB, GB> p(s, d.kappa, d.inv_dielectric);
   long long acc_elec = 0, acc_vdw = 0, acc_gb = 0;
   int acc_k = -1;
-  for (int t = threadIdx.x >> 5; t < ntiles; t += blockDim.x >> 5) {
+  for (int t = first; t < ntiles; t += stride) {
     const TileInfo ti = tileInfo(s, nsys_u, t);
     if (ENERGY && ti.k != acc_k) {
       if (acc_k >= 0) {
@@ -844,11 +869,11 @@ __device__ void pairTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u, 
 }
 
 __device__ void gbDerivativeTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u,
-                                  int ntiles) {
+                                  int ntiles, int first, int stride) {
   const int lane = threadIdx.x & 31;
   const float fs = d.frc_scale;
   DerivPass p(s);
-  for (int t = threadIdx.x >> 5; t < ntiles; t += blockDim.x >> 5) {
+  for (int t = first; t < ntiles; t += stride) {
     const TileInfo ti = tileInfo(s, nsys_u, t);
     p.begin(ti.ibase + lane);
     walkTile(p, ti, lane);
@@ -916,16 +941,23 @@ struct UnitShape {
 // Molecule table, prefix sums and Lennard-Jones tables of unit u.  Returns false (after setting
 // bit 0 of the status word) when the unit does not fit the launch's shared-memory carve-out; the
 // caller then skips the unit.  Ends with a barrier.
+template <class Team>
 __device__ bool stageUnitTables(const DevSynthesis &d, const UnitSmem &s, int u, int max_lj,
-                                UnitShape* shape) {
+                                UnitShape* shape, const Team &team, int max_sys = kMaxUnitSystems) {
   const int4 desc = d.unit_desc[u];
   const int nsys_u = desc.y;
   shape->nsys = nsys_u;
   shape->nslots = desc.z;
   shape->ntiles = desc.w;
+  if (nsys_u > max_sys) {
+    if (team.rank() == 0) {
+      atomicOr(d.status, 1);
+    }
+    return false;
+  }
   // the unit's molecule table, precomputed on the host: one coalesced load per field
   const int* meta = d.unit_meta + static_cast<size_t>(desc.x) * kUnitMetaFields;
-  for (int e = threadIdx.x; e < (nsys_u + 1) * kUnitMetaFields; e += blockDim.x) {
+  for (int e = team.rank(); e < (nsys_u + 1) * kUnitMetaFields; e += team.size()) {
     const int k = e / kUnitMetaFields;
     const int v = meta[e];
     switch (e % kUnitMetaFields) {
@@ -939,15 +971,15 @@ __device__ bool stageUnitTables(const DevSynthesis &d, const UnitSmem &s, int u,
       default: s.dchunk0[k] = v; break;
     }
   }
-  __syncthreads();
-  if (desc.z > d.max_unit_slots || s.ljbase[nsys_u] > max_lj) {
-    if (threadIdx.x == 0) {
+  team.sync();
+  if (desc.z > d.max_unit_slots || s.ljbase[nsys_u] > max_lj || nsys_u > max_sys) {
+    if (team.rank() == 0) {
       atomicOr(d.status, 1);
     }
     return false;   // reported through the status word; nothing in the unit is touched
   }
   // Lennard-Jones tables (standard then 1-4) of every molecule, all entries in parallel
-  for (int e = threadIdx.x; e < s.ljbase[nsys_u]; e += blockDim.x) {
+  for (int e = team.rank(); e < s.ljbase[nsys_u]; e += team.size()) {
     const int k = findOwner(s.ljbase, nsys_u, e);
     const int sysid = s.sys[k];
     const int nt = d.lj_ntypes[sysid];
@@ -955,7 +987,7 @@ __device__ bool stageUnitTables(const DevSynthesis &d, const UnitSmem &s, int u,
     const int src = d.lj_start[sysid] + (rel < nt * nt ? rel : rel - nt * nt);
     s.lj[e] = (rel < nt * nt) ? d.ljab[src] : d.ljab14[src];
   }
-  __syncthreads();
+  team.sync();
   return true;
 }
 
@@ -1017,8 +1049,9 @@ __device__ __forceinline__ void placeSlot(const DevSynthesis &d, const UnitSmem 
 // shared memory on entry (and a barrier since); forces in s.fx.. and per-molecule energies in
 // s.nrg on exit, after a barrier.  WS: also write the GB workspace (psi, effective radii, dE/dR)
 // to global memory.
-template <bool FORCE, bool ENERGY, int TERMS, bool WS>
-__device__ void evaluateStaged(const DevSynthesis &d, const UnitSmem &s, const UnitShape &us) {
+template <bool FORCE, bool ENERGY, int TERMS, bool WS, class Team>
+__device__ void evaluateStaged(const DevSynthesis &d, const UnitSmem &s, const UnitShape &us,
+                               const Team &team) {
   constexpr bool VALE = (TERMS & 1) != 0;
   constexpr bool NB = (TERMS & 2) != 0;
   const bool gb = ((TERMS & 4) != 0) && (d.igb != 0);
@@ -1028,19 +1061,19 @@ __device__ void evaluateStaged(const DevSynthesis &d, const UnitSmem &s, const U
 
   // valence terms and GB pass 1 touch disjoint accumulators: no barrier between them
   if (VALE) {
-    valenceTerms<FORCE, ENERGY>(d, SmemValence(s), nsys_u);
+    valenceTerms<FORCE, ENERGY>(d, SmemValence(s, team.warp(), team.warps()), nsys_u);
     if (!gb) {
-      __syncthreads();
+      team.sync();
     }
   }
   if (gb) {
-    gbRadiiTiles(s, nsys_u, ntiles);
-    __syncthreads();
+    gbRadiiTiles(s, nsys_u, ntiles, team.warp(), team.warps());
+    team.sync();
     // effective radii, self terms (nonbonded_potential.tpp:730-805); a warp's 32 slots
     // belong to one molecule, so the self energies reduce across the warp
     const float inv_ps = 1.0f / static_cast<float>(1 << kPsiBits);
     const float ds = static_cast<float>(1 << kDeijdaBits);
-    for (int slot = threadIdx.x; slot < nslots; slot += blockDim.x) {
+    for (int slot = team.rank(); slot < nslots; slot += team.size()) {
       const int k = findOwner(s.slot0, nsys_u, slot);
       const int a = slot - s.slot0[k];
       float e_self = 0.0f;
@@ -1076,35 +1109,35 @@ __device__ void evaluateStaged(const DevSynthesis &d, const UnitSmem &s, const U
         warpEnergy(s, k, kGb, e_self, d.nrg_scale);
       }
     }
-    __syncthreads();
+    team.sync();
   }
   else if (NB) {
     // pass 2 payload for Coulomb / Lennard-Jones alone: charge in w1
-    for (int slot = threadIdx.x; slot < nslots; slot += blockDim.x) {
+    for (int slot = team.rank(); slot < nslots; slot += team.size()) {
       float4 pa = s.pa[slot];
       pa.w = s.prm[slot].x;
       s.pa[slot] = pa;
     }
-    __syncthreads();
+    team.sync();
   }
   if (NB || gb) {
     if (NB && gb) {
-      pairTiles<FORCE, ENERGY, true, true>(d, s, nsys_u, ntiles);
+      pairTiles<FORCE, ENERGY, true, true>(d, s, nsys_u, ntiles, team.warp(), team.warps());
     }
     else if (NB) {
-      pairTiles<FORCE, ENERGY, true, false>(d, s, nsys_u, ntiles);
+      pairTiles<FORCE, ENERGY, true, false>(d, s, nsys_u, ntiles, team.warp(), team.warps());
     }
     else {
-      pairTiles<FORCE, ENERGY, false, true>(d, s, nsys_u, ntiles);
+      pairTiles<FORCE, ENERGY, false, true>(d, s, nsys_u, ntiles, team.warp(), team.warps());
     }
-    __syncthreads();
+    team.sync();
   }
   if (gb && FORCE) {
     // chain-rule prefactor of the OBC radii (nonbonded_potential.tpp:982-1021), and the
     // pass 3 payloads
     const float inv_ds = 1.0f / static_cast<float>(1 << kDeijdaBits);
     const float inv_ps = 1.0f / static_cast<float>(1 << kPsiBits);
-    for (int slot = threadIdx.x; slot < nslots; slot += blockDim.x) {
+    for (int slot = team.rank(); slot < nslots; slot += team.size()) {
       const int k = findOwner(s.slot0, nsys_u, slot);
       const int a = slot - s.slot0[k];
       const float4 prm = s.prm[slot];
@@ -1129,9 +1162,9 @@ __device__ void evaluateStaged(const DevSynthesis &d, const UnitSmem &s, const U
       s.pb[slot] = pb;
       s.gbv[slot].y = sde;
     }
-    __syncthreads();
-    gbDerivativeTiles(d, s, nsys_u, ntiles);
-    __syncthreads();
+    team.sync();
+    gbDerivativeTiles(d, s, nsys_u, ntiles, team.warp(), team.warps());
+    team.sync();
   }
 }
 
