@@ -246,7 +246,7 @@ kTiledRadii(const DevSynthesis d, const DevTiled t, int tile_begin, int tile_end
   int first, last;
   warpTileRange(t, tile_begin, tile_end, &first, &last);
   const UnitSmem v = warpView(pa, pb, prm, gbv, d.ljab);
-  RadiiPass p(v);
+  RadiiPass2 p(v);
   for (int g = first; g < last; g++) {
     const int m = tiledOwner(t, g);
     const int sysid = t.systems[m];
@@ -254,14 +254,14 @@ kTiledRadii(const DevSynthesis d, const DevTiled t, int tile_begin, int tile_end
     const TileInfo ti = tiledTileInfo(d, sysid, g - t.tile_prefix[m], &I, &J);
     stageTile<1, true>(d, t, v, sysid, I, J, ti.diag, lane);
     p.begin(lane);
-    walkTile(p, ti, lane);
+    walkTile2(p, ti, lane);
     const int base = d.atom_start[sysid];
     if (lane < ti.ni) {
       addGlobal(&t.psi_acc[base + I * kTile + lane], p.psi_i * ps);
     }
-    const int jl = traveledAtom(ti, lane);
+    const int jl = traveledAtom2(ti, lane);
     if (jl < ti.nj) {
-      addGlobal(&t.psi_acc[base + J * kTile + jl], p.psi_j * ps);
+      addGlobal(&t.psi_acc[base + J * kTile + jl], p.psi_j1 * ps);
     }
     __syncwarp();
   }

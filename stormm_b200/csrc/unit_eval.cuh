@@ -54,6 +54,15 @@ constexpr float kTaylorHH = 5.45454545454545454545f;
 
 constexpr unsigned kFullMask = 0xffffffffu;
 
+// Packed FP32 pairs (Blackwell FFMA2 / FADD2 / FMUL2): two pairs of one lane in one instruction
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, f2(-1.0f), a); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+
 // HCT descreening of an atom of offset radius rho by a neighbour of screened radius sj at
 // distance r (invr = 1/r); returns the amount psi decreases by.
 //
@@ -84,6 +93,46 @@ __device__ __forceinline__ float hctIntegral(float r, float r2, float invr, floa
     v += 2.0f * (__fdividef(1.0f, rho) - il);
   }
   return (rho < u) ? 0.5f * v : 0.0f;
+}
+
+// hctIntegral for two pairs at once
+__device__ __forceinline__ float2 hctIntegral2(float2 r, float2 r2, float2 invr, float2 rho,
+                                               float2 sj) {
+  const bool far_x = r.x > 4.0f * sj.x;
+  const bool far_y = r.y > 4.0f * sj.y;
+  float2 vf = f2(0.0f);
+  float2 vn = f2(0.0f);
+  if (far_x || far_y) {
+    const float2 invr2 = mul2(invr, invr);
+    const float2 t = mul2(mul2(sj, sj), invr2);
+    float2 dumbo = fma2(t, f2(kTaylorDD), f2(kTaylorD));
+    dumbo = fma2(t, dumbo, f2(kTaylorC));
+    dumbo = fma2(t, dumbo, f2(kTaylorB));
+    dumbo = fma2(t, dumbo, f2(kTaylorA));
+    vf = mul2(mul2(mul2(sj, t), invr2), dumbo);
+  }
+  if (!(far_x && far_y)) {
+    const float2 u = add2(r, sj);
+    const float2 rms = sub2(r, sj);
+    const float2 l = f2(fmaxf(rho.x, fabsf(rms.x)), fmaxf(rho.y, fabsf(rms.y)));
+    const float2 lu = mul2(l, u);
+    const float2 inv_lu = f2(__fdividef(1.0f, lu.x), __fdividef(1.0f, lu.y));
+    const float2 il = mul2(u, inv_lu);
+    const float2 iu = mul2(l, inv_lu);
+    const float2 dlu = sub2(il, iu);
+    const float2 liu = mul2(l, iu);
+    const float2 lg = f2(__logf(liu.x), __logf(liu.y));
+    const float2 q = mul2(mul2(mul2(f2(0.25f), sub2(mul2(sj, sj), r2)), invr), dlu);
+    float2 v = add2(fma2(q, add2(il, iu), dlu), mul2(mul2(f2(0.5f), invr), lg));
+    if (rho.x < -rms.x) {
+      v.x += 2.0f * (__fdividef(1.0f, rho.x) - il.x);
+    }
+    if (rho.y < -rms.y) {
+      v.y += 2.0f * (__fdividef(1.0f, rho.y) - il.y);
+    }
+    vn = f2((rho.x < u.x) ? 0.5f * v.x : 0.0f, (rho.y < u.y) ? 0.5f * v.y : 0.0f);
+  }
+  return f2(far_x ? vf.x : vn.x, far_y ? vf.y : vn.y);
 }
 
 // Radial derivative of hctIntegral, -(1/r) dI/dr, the factor the reference multiplies by the
@@ -604,35 +653,83 @@ __device__ __forceinline__ void walkTile(P &p, const TileInfo &ti, int lane) {
   }
 }
 
+// Walk a tile two pairs per lane per step: an off-diagonal tile in 16 steps pairing j = l + k
+// with j = l + k + 16, a diagonal tile in 8 steps pairing j = l + k with j = l + k + 8 (the
+// second pair of the last step on half the lanes: w2 = 0 elsewhere).  Each of the two j streams
+// carries its own traveling accumulators; p.merge() folds the second into the first, after which
+// lane l holds those of block J's atom (l + 16) mod 32 (off-diagonal) or (l + 9) mod 32.
+template <class P>
+__device__ __forceinline__ void walkTile2(P &p, const TileInfo &ti, int lane) {
+  if (!ti.diag) {
+#pragma unroll 2
+    for (int k = 0; k < 16; k++) {
+      const int j1 = (lane + k) & 31;
+      const int j2 = (lane + k + 16) & 31;
+      p.pair2(ti.jbase + j1, j1, ti.jbase + j2, j2, 1.0f);
+      p.rotate2(lane);
+    }
+    p.merge((lane + 16) & 31);
+  }
+  else {
+#pragma unroll 1
+    for (int k = 1; k <= 8; k++) {
+      const int j1 = (lane + k) & 31;
+      const int j2 = (lane + k + 8) & 31;
+      p.pair2(ti.jbase + j1, j1, ti.jbase + j2, j2, (k == 8 && lane >= 16) ? 0.0f : 1.0f);
+      p.rotate2(lane);
+    }
+    p.merge((lane + 24) & 31);
+  }
+}
+
+__device__ __forceinline__ int traveledAtom2(const TileInfo &ti, int lane) {
+  return (lane + (ti.diag ? 9 : 16)) & 31;
+}
+
 // Lane that holds block J's atom jl's traveling accumulator once the walk is over
 __device__ __forceinline__ int traveledAtom(const TileInfo &ti, int lane) {
   return (lane + (ti.diag ? 17 : 32)) & 31;
 }
 
-// GB pass 1: psi_i -= H(r, rho_i, s_j rho_j) and psi_j -= H(r, rho_j, s_i rho_i)
-struct RadiiPass {
+// GB pass 1, two pairs per lane per step: psi_i -= H(r, rho_i, s_j rho_j) and
+// psi_j -= H(r, rho_j, s_i rho_i)
+struct RadiiPass2 {
   const UnitSmem &s;
   float4 ai, bi;
-  float psi_i, psi_j;
-  __device__ RadiiPass(const UnitSmem &s_in) : s(s_in) {}
+  float2 psi_i2;    // i-side sums of the two pair streams
+  float2 psi_j;     // traveling j-side sums: x for stream 1, y for stream 2
+  float psi_i, psi_j1;
+  __device__ RadiiPass2(const UnitSmem &s_in) : s(s_in) {}
   __device__ __forceinline__ void begin(int islot) {
     ai = s.pa[islot];
     bi = s.pb[islot];
-    psi_i = 0.0f;
-    psi_j = 0.0f;
+    psi_i2 = f2(0.0f);
+    psi_j = f2(0.0f);
   }
-  __device__ __forceinline__ void pair(int jslot, int) {
-    const float4 aj = s.pa[jslot];
-    const float4 bj = s.pb[jslot];
-    const float3 dv = pairDelta(ai, bi, aj, bj);
-    const float r2 = fmaf(dv.x, dv.x, fmaf(dv.y, dv.y, dv.z * dv.z));
-    const float invr = rsqrtf(r2);
-    const float r = r2 * invr;
-    psi_i -= hctIntegral(r, r2, invr, bi.w, aj.w);
-    psi_j -= hctIntegral(r, r2, invr, bj.w, ai.w);
+  __device__ __forceinline__ void pair2(int js1, int, int js2, int, float w2) {
+    const float4 aj1 = s.pa[js1];
+    const float4 bj1 = s.pb[js1];
+    const float4 aj2 = s.pa[js2];
+    const float4 bj2 = s.pb[js2];
+    const float2 dx = add2(sub2(f2(aj1.x, aj2.x), f2(ai.x)), sub2(f2(bj1.x, bj2.x), f2(bi.x)));
+    const float2 dy = add2(sub2(f2(aj1.y, aj2.y), f2(ai.y)), sub2(f2(bj1.y, bj2.y), f2(bi.y)));
+    const float2 dz = add2(sub2(f2(aj1.z, aj2.z), f2(ai.z)), sub2(f2(bj1.z, bj2.z), f2(bi.z)));
+    const float2 r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
+    const float2 invr = f2(rsqrtf(r2.x), rsqrtf(r2.y));
+    const float2 r = mul2(r2, invr);
+    const float2 hi = hctIntegral2(r, r2, invr, f2(bi.w), f2(aj1.w, aj2.w));
+    const float2 hj = hctIntegral2(r, r2, invr, f2(bj1.w, bj2.w), f2(ai.w));
+    const float2 wneg = f2(-1.0f, -w2);
+    psi_i2 = fma2(hi, wneg, psi_i2);
+    psi_j = fma2(hj, wneg, psi_j);
   }
-  __device__ __forceinline__ void rotate(int lane) {
-    psi_j = __shfl_sync(kFullMask, psi_j, (lane + 1) & 31);
+  __device__ __forceinline__ void rotate2(int lane) {
+    psi_j.x = __shfl_sync(kFullMask, psi_j.x, (lane + 1) & 31);
+    psi_j.y = __shfl_sync(kFullMask, psi_j.y, (lane + 1) & 31);
+  }
+  __device__ __forceinline__ void merge(int src) {
+    psi_i = psi_i2.x + psi_i2.y;
+    psi_j1 = psi_j.x + __shfl_sync(kFullMask, psi_j.y, src);
   }
 };
 
@@ -779,17 +876,17 @@ struct DerivPass {
 __device__ void gbRadiiTiles(const UnitSmem &s, int nsys_u, int ntiles, int first, int stride) {
   const int lane = threadIdx.x & 31;
   const float ps = static_cast<float>(1 << kPsiBits);
-  RadiiPass p(s);
+  RadiiPass2 p(s);
   for (int t = first; t < ntiles; t += stride) {
     const TileInfo ti = tileInfo(s, nsys_u, t);
     p.begin(ti.ibase + lane);
-    walkTile(p, ti, lane);
+    walkTile2(p, ti, lane);
     if (lane < ti.ni) {
       atomicAddInt63(p.psi_i * ps, &s.psi[ti.ibase + lane], &s.psio[ti.ibase + lane]);
     }
-    const int jl = traveledAtom(ti, lane);
+    const int jl = traveledAtom2(ti, lane);
     if (jl < ti.nj) {
-      atomicAddInt63(p.psi_j * ps, &s.psi[ti.jbase + jl], &s.psio[ti.jbase + jl]);
+      atomicAddInt63(p.psi_j1 * ps, &s.psi[ti.jbase + jl], &s.psio[ti.jbase + jl]);
     }
   }
 }
