@@ -461,9 +461,11 @@ __device__ void minimizeUnit(const DevSynthesis &d, const DevMinimizer &m, const
   team.sync();
 }
 
-// One thread block per work unit (molecules of up to 2,048 atoms)
+// One thread block per work unit (molecules of up to 2,048 atoms).  The minimizer keeps more
+// state live than a single evaluation; two blocks per SM with up to 128 registers a thread run
+// faster than four with 64, where the pair loops spill.
 template <bool HIST>
-__global__ void __launch_bounds__(256, 4)
+__global__ void __launch_bounds__(256, 2)
 kMinimize(const DevSynthesis d, const DevMinimizer m, int unit_begin, int unit_end, int max_lj,
           int cycles, int final_energy) {
   extern __shared__ __align__(16) char smem_raw[];
