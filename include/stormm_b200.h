@@ -208,7 +208,17 @@ typedef struct {
                                   STORMM's GPU minimizer does */
   int record_history;          /* nonzero: keep each system's energy at the start of every cycle
                                   and the final energy (total_cycles + 1 values per system) */
+  int kernel;                  /* SB_MIN_GRAPH (default) or SB_MIN_PERSISTENT */
 } sb_minimize_controls;
+
+/* How a minimization runs.  Both follow the same algorithm; their FP32 evaluations are separate
+ * compiled codes, so their trajectories agree to rounding, not bit for bit.
+ *   SB_MIN_GRAPH       each cycle is one CUDA graph, captured once per synthesis: the batched
+ *                      evaluation kernel (force + energy, then three energy-only evaluations)
+ *                      with a per-system line-search kernel after each
+ *   SB_MIN_PERSISTENT  one persistent kernel runs every cycle of a work unit on chip */
+#define SB_MIN_GRAPH 0
+#define SB_MIN_PERSISTENT 1
 
 void sb_default_minimize_controls(sb_minimize_controls* ctl);
 

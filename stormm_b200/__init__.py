@@ -18,6 +18,7 @@ SB_OK = 0
 SB_GB_NONE, SB_GB_HCT, SB_GB_OBC, SB_GB_OBC2 = 0, 1, 2, 5
 TERM_VALENCE, TERM_NONBONDED, TERM_GB, TERM_ALL = 1, 2, 4, 7
 TUNE_EVALUATE, TUNE_MINIMIZE = 1, 2
+MIN_GRAPH, MIN_PERSISTENT = 0, 1
 INIT_FORCES, INIT_ENERGIES, INIT_GB_WORKSPACE = 1, 2, 4
 NRG_STRIDE = 16
 # StateVariable slots (STORMM Potential/energy_enumerators.h:36-50)
@@ -59,6 +60,7 @@ class MinimizeControls(ctypes.Structure):
         ("total_cycles", ctypes.c_int), ("sd_cycles", ctypes.c_int),
         ("clash_cycles", ctypes.c_int), ("initial_step", ctypes.c_double),
         ("convergence_rms", ctypes.c_double), ("record_history", ctypes.c_int),
+        ("kernel", ctypes.c_int),
     ]
 
 

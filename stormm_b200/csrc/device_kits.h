@@ -150,6 +150,13 @@ struct DevMinimizer {
   int max_cycles;                // a system stops moving after this many cycles in total
   double drms;                   // RMS force target (kcal/mol/A), 0: none
   int* queue;                    // work-unit counter, zero before each launch
+  double* line;                  // per system: kLineFields line-search scalars (graph minimizer)
+};
+
+// Line-search scalars per system between the graph minimizer's kernels
+enum LineField : int {
+  kLineE0 = 0, kLineE1, kLineE2, kLineMv1, kLineMv2, kLineMv3, kLineMfac, kLineSMove,
+  kLineInvNorm, kLineAct, kLineFields
 };
 
 }  // namespace sb

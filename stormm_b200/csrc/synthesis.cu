@@ -31,6 +31,8 @@ cudaError_t launchMinimizerReset(const DevMinimizer &m, const DevSynthesis &d, d
 cudaError_t launchMinimize(const DevSynthesis &d, const DevMinimizer &m, int unit_begin,
                            int unit_end, int max_lj, int cycles, bool final_energy, int threads,
                            int sm_count, cudaStream_t stream);
+cudaError_t launchLineStep(const DevSynthesis &d, const DevMinimizer &m, int first, int count,
+                           int step, cudaStream_t stream);
 cudaError_t launchTiled(const DevSynthesis &d, const DevTiled &t, const int* h_tile_prefix,
                         const int* h_atom_prefix, int mol_begin, int mol_end, int terms,
                         bool force, bool energy, bool workspace, int sm_count,
@@ -832,6 +834,7 @@ void Synthesis::minimizeBegin(const sb_minimize_controls &ctl, cudaStream_t stre
     d_rmsf.allocate(nsys);
     d_mcycle.allocate(nsys);
     d_mdone.allocate(nsys);
+    d_line.allocate(static_cast<size_t>(nsys) * kLineFields);
     d_queue.allocate(2);
   }
   history_stride = 0;
@@ -864,8 +867,63 @@ void Synthesis::minimizeBegin(const sb_minimize_controls &ctl, cudaStream_t stre
   m.max_cycles = ctl.total_cycles;
   m.drms = ctl.convergence_rms;
   m.queue = d_queue.p;
+  m.line = d_line.p;
+  if (ctl.kernel != SB_MIN_GRAPH && ctl.kernel != SB_MIN_PERSISTENT) {
+    throw Error(SB_ERR_ARGUMENT, "unknown minimization kernel choice");
+  }
+  min_kernel = ctl.kernel;
+  min_total_cycles = ctl.total_cycles;
   cudaCheck(launchMinimizerReset(m, dev, ctl.initial_step, stream), "minimizer reset");
   min_ready = true;
+}
+
+Synthesis::~Synthesis() {
+  if (cycle_graph != nullptr) {
+    cudaGraphExecDestroy(cycle_graph);
+  }
+  if (capture_stream != nullptr) {
+    cudaStreamDestroy(capture_stream);
+  }
+}
+
+// One batched evaluation of all systems (single = false) or of systems [first, first + count)
+// one launch each (single = true)
+void Synthesis::evaluateFor(int first, int count, bool single, bool force, cudaStream_t stream) {
+  if (!single) {
+    launchPlan(*eval_plan, SB_TERM_ALL, force, true, stream);
+    return;
+  }
+  DevSynthesis d = dev;
+  d.unit_desc = single_plan->d_units.p;
+  d.unit_meta = single_plan->d_meta.p;
+  d.nunit = nsys;
+  d.max_unit_slots = single_slots;
+  for (int s = first; s < first + count; s++) {
+    cudaCheck(launchEvalFused(d, s, s + 1, single_lj, SB_TERM_ALL, force, true, 1, threads,
+                              stream), "per-system evaluation launch");
+  }
+}
+
+// One graph-mode cycle: evaluations by the batched evaluation kernel, line-search steps by a warp
+// per system (line_search.cu)
+void Synthesis::graphCycle(int first, int count, bool single, cudaStream_t stream) {
+  const size_t nrg_bytes = d_energies.n * sizeof(unsigned long long);
+  initialize(SB_INIT_FORCES | SB_INIT_ENERGIES, stream);
+  evaluateFor(first, count, single, true, stream);
+  cudaCheck(launchLineStep(dev, dev_min, first, count, 0, stream), "line search launch");
+  for (int step = 1; step <= 3; step++) {
+    cudaCheck(cudaMemsetAsync(d_energies.p, 0, nrg_bytes, stream), "memset");
+    evaluateFor(first, count, single, false, stream);
+    cudaCheck(launchLineStep(dev, dev_min, first, count, step, stream), "line search launch");
+  }
+}
+
+// Energies at the coordinates reached, and their history entry
+void Synthesis::graphFinalEnergy(int first, int count, bool single, cudaStream_t stream) {
+  cudaCheck(cudaMemsetAsync(d_energies.p, 0, d_energies.n * sizeof(unsigned long long), stream),
+            "memset");
+  evaluateFor(first, count, single, false, stream);
+  cudaCheck(launchLineStep(dev, dev_min, first, count, 4, stream), "line search launch");
 }
 
 void Synthesis::launchMinPlan(const UnitPlan &plan, int cycles, bool final_energy,
@@ -901,12 +959,56 @@ void Synthesis::minimizeAdvance(int cycles, bool final_energy, cudaStream_t stre
   if (cycles < 0) {
     throw Error(SB_ERR_ARGUMENT, "cycle count must not be negative");
   }
-  launchMinPlan(*min_plan, cycles, final_energy, stream);
+  if (min_kernel == SB_MIN_PERSISTENT) {
+    launchMinPlan(*min_plan, cycles, final_energy, stream);
+    return;
+  }
+  if (cycles > 0) {
+    // the graph holds its kernels' arguments by value: capture again when any of them changed
+    const bool stale = cycle_graph == nullptr || cycle_graph_plan != eval_plan.get() ||
+                       std::memcmp(&cycle_graph_min, &dev_min, sizeof(DevMinimizer)) != 0 ||
+                       std::memcmp(&cycle_graph_dev, &dev, sizeof(DevSynthesis)) != 0;
+    if (stale) {
+      // capture one cycle on a stream of the synthesis' own, then replay it on the caller's
+      if (cycle_graph != nullptr) {
+        cudaCheck(cudaGraphExecDestroy(cycle_graph), "cudaGraphExecDestroy");
+        cycle_graph = nullptr;
+      }
+      if (capture_stream == nullptr) {
+        cudaCheck(cudaStreamCreateWithFlags(&capture_stream, cudaStreamNonBlocking),
+                  "cudaStreamCreate");
+      }
+      cudaCheck(cudaStreamBeginCapture(capture_stream, cudaStreamCaptureModeRelaxed),
+                "cudaStreamBeginCapture");
+      cudaGraph_t graph = nullptr;
+      try {
+        graphCycle(0, nsys, false, capture_stream);
+      }
+      catch (...) {
+        cudaStreamEndCapture(capture_stream, &graph);
+        if (graph != nullptr) cudaGraphDestroy(graph);
+        throw;
+      }
+      cudaCheck(cudaStreamEndCapture(capture_stream, &graph), "cudaStreamEndCapture");
+      const cudaError_t err = cudaGraphInstantiate(&cycle_graph, graph, 0);
+      cudaGraphDestroy(graph);
+      cudaCheck(err, "cudaGraphInstantiate");
+      cycle_graph_plan = eval_plan.get();
+      cycle_graph_min = dev_min;
+      cycle_graph_dev = dev;
+    }
+    for (int c = 0; c < cycles; c++) {
+      cudaCheck(cudaGraphLaunch(cycle_graph, stream), "cudaGraphLaunch");
+    }
+  }
+  if (final_energy) {
+    graphFinalEnergy(0, nsys, false, stream);
+  }
 }
 
 void Synthesis::minimize(const sb_minimize_controls &ctl, cudaStream_t stream) {
   minimizeBegin(ctl, stream);
-  launchMinPlan(*min_plan, ctl.total_cycles, true, stream);
+  minimizeAdvance(ctl.total_cycles, true, stream);
 }
 
 void Synthesis::minimizeRange(int first, int count, const sb_minimize_controls &ctl,
@@ -915,6 +1017,16 @@ void Synthesis::minimizeRange(int first, int count, const sb_minimize_controls &
     throw Error(SB_ERR_ARGUMENT, "system range out of bounds");
   }
   minimizeBegin(ctl, stream);
+  if (min_kernel == SB_MIN_GRAPH) {
+    // the per-system sequence: every launch of every cycle for one system at a time
+    for (int s = first; s < first + count; s++) {
+      for (int c = 0; c < ctl.total_cycles; c++) {
+        graphCycle(s, 1, true, stream);
+      }
+    }
+    graphFinalEnergy(first, count, true, stream);
+    return;
+  }
   DevSynthesis d = dev;
   d.unit_desc = single_plan->d_units.p;
   d.unit_meta = single_plan->d_meta.p;
@@ -1233,6 +1345,7 @@ int sb_check_status(sb_synthesis* syn, int* status) {
 
 void sb_default_minimize_controls(sb_minimize_controls* ctl) {
   std::memset(ctl, 0, sizeof(sb_minimize_controls));
+  ctl->kernel = SB_MIN_GRAPH;
   ctl->total_cycles = 200;
   ctl->sd_cycles = 50;
   ctl->clash_cycles = 0;

@@ -189,8 +189,18 @@ public:
   DeviceArray<double> d_lmove, d_rmsf, d_history;
   DeviceArray<int> d_mcycle, d_mdone, d_queue;
   int history_stride = 0;
+  DeviceArray<double> d_line;
   DevMinimizer dev_min{};
   bool min_ready = false;
+  int min_kernel = SB_MIN_GRAPH;
+  int min_total_cycles = 0;
+  // captured minimization cycle (graph mode) and what it was captured for
+  cudaGraphExec_t cycle_graph = nullptr;
+  const UnitPlan* cycle_graph_plan = nullptr;
+  DevMinimizer cycle_graph_min{};   // kernel arguments the graph was captured with
+  DevSynthesis cycle_graph_dev{};
+  cudaStream_t capture_stream = nullptr;
+  ~Synthesis();
 
   DevSynthesis dev;
 
@@ -203,6 +213,9 @@ private:
   void launchTiledRange(int mol_begin, int mol_end, int terms, bool force, bool energy,
                         cudaStream_t stream);
   void rejectTiledMinimization() const;
+  void graphCycle(int first, int count, bool single, cudaStream_t stream);
+  void graphFinalEnergy(int first, int count, bool single, cudaStream_t stream);
+  void evaluateFor(int first, int count, bool single, bool force, cudaStream_t stream);
   void buildUnits();
   void upload();
 };

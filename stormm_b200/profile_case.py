@@ -2,10 +2,12 @@
 
   python -m stormm_b200.profile_case [--molecules 256] [--evals 4] [--energy-only]
   python -m stormm_b200.profile_case --workload minimization --molecules 4096 --minimize 20
+  python -m stormm_b200.profile_case --workload chains --molecules 16 --evals 3
 
 The first form builds the first molecules of the batched single-point workload (16-256 atoms),
 uploads them and runs a few force + energy evaluations; the second builds the first molecules
-of the minimization workload (24-96 atoms, 0.3 A noise) and runs a short minimization.  Both
+of the minimization workload (24-96 atoms, 0.3 A noise) and runs a short minimization; the third
+evaluates the first chains of the large-system workload (2,000-5,000 atoms, tiled path).  All
 finish in seconds, so a profiler can capture single launches of each kernel.
 """
 from __future__ import annotations
@@ -17,7 +19,8 @@ import numpy as np
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="single-point", choices=["single-point", "minimization"])
+    ap.add_argument("--workload", default="single-point",
+                    choices=["single-point", "minimization", "chains"])
     ap.add_argument("--molecules", type=int, default=256)
     ap.add_argument("--evals", type=int, default=4)
     ap.add_argument("--energy-only", action="store_true")
@@ -27,6 +30,8 @@ def main():
     from stormm_b200 import synthetic
     if args.workload == "minimization":
         mols = synthetic.workload_minimization(args.molecules)
+    elif args.workload == "chains":
+        mols = synthetic.workload_chains(args.molecules)
     else:
         mols = synthetic.workload_batched_single_point(args.molecules)
     syn = sb.Synthesis(mols)

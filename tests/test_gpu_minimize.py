@@ -183,3 +183,35 @@ def test_autotune_keeps_results():
     syn.set_coordinates(xyz)
     syn.minimize(total_cycles=20, sd_cycles=5)
     assert np.array_equal(syn.coordinates(), c_min)
+
+
+def test_controls_change_between_minimizations():
+    """The graph minimizer captures its kernels' arguments: a second minimization with other
+    controls on the same synthesis must match a fresh synthesis."""
+    mols = [synthetic.make_molecule(synthetic._seed(3141, k), 30 + 11 * k, 0.3) for k in range(5)]
+    xyz = np.concatenate([m.coords for m in mols])
+    syn = sb.Synthesis(mols)
+    syn.set_coordinates(xyz)
+    syn.minimize(total_cycles=5, sd_cycles=2)
+    syn.set_coordinates(xyz)
+    syn.minimize(total_cycles=30, sd_cycles=10, convergence_rms=0.2, record_history=True)
+    fresh = sb.Synthesis(mols)
+    fresh.set_coordinates(xyz)
+    fresh.minimize(total_cycles=30, sd_cycles=10, convergence_rms=0.2, record_history=True)
+    assert np.array_equal(syn.coordinates(), fresh.coordinates())
+    assert np.array_equal(syn.minimize_history(), fresh.minimize_history())
+
+
+def test_graph_and_persistent_kernels_agree():
+    mols = [synthetic.make_molecule(synthetic._seed(2718, k), 24 + 9 * k, 0.3) for k in range(8)]
+    xyz = np.concatenate([m.coords for m in mols])
+    out = {}
+    for kernel in (sb.MIN_GRAPH, sb.MIN_PERSISTENT):
+        syn = sb.Synthesis(mols)
+        syn.set_coordinates(xyz)
+        syn.minimize(total_cycles=40, sd_cycles=10, record_history=True, kernel=kernel)
+        out[kernel] = syn.minimize_history()
+    h_g, h_p = out[sb.MIN_GRAPH], out[sb.MIN_PERSISTENT]
+    np.testing.assert_allclose(h_g[:, :3], h_p[:, :3], rtol=1e-5)
+    drop = h_p[:, 0] - h_p[:, -1]
+    assert np.all(np.abs(h_g[:, -1] - h_p[:, -1]) <= 0.01 * drop + 1e-3)
