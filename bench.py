@@ -323,12 +323,13 @@ def bench_minimization(args, world, rank, local, flush):
     mols = synthetic.workload_minimization(MIN_NSYS, seed=_seed_min(rank))
     syn = sb.Synthesis(mols, device=local)
     xyz = np.concatenate([m.coords for m in mols])
-    ctl = dict(total_cycles=MIN_CYCLES, sd_cycles=MIN_SD_CYCLES)
+    ctl = dict(total_cycles=MIN_CYCLES, sd_cycles=MIN_SD_CYCLES, kernel=sb.MIN_GRAPH)
     syn.set_coordinates(xyz)
-    tuned = syn.autotune(sb.TUNE_MINIMIZE)   # untimed: picks the unit packing
+    # untimed: the graph minimizer's evaluations use the evaluation packing
+    tuned = syn.autotune(sb.TUNE_EVALUATE)
     for _ in range(3):
         syn.set_coordinates(xyz)
-        syn.minimize(total_cycles=5, sd_cycles=2)
+        syn.minimize(total_cycles=5, sd_cycles=2, kernel=sb.MIN_GRAPH)
     torch.cuda.synchronize()
     assert syn.status() == 0
     times = []
@@ -371,6 +372,16 @@ def bench_minimization(args, world, rank, local, flush):
         syn.initialize()
         syn.evaluate(force=False, energy=True)
         e_start = syn.energy_terms().sum(axis=1)
+    # the persistent-kernel minimizer on the same workload, one run, for comparison
+    syn.set_coordinates(xyz)
+    syn.autotune(sb.TUNE_MINIMIZE)
+    syn.set_coordinates(xyz)
+    ev0, ev1 = _event_pair()
+    ev0.record()
+    syn.minimize(total_cycles=MIN_CYCLES, sd_cycles=MIN_SD_CYCLES, kernel=sb.MIN_PERSISTENT)
+    ev1.record()
+    torch.cuda.synchronize()
+    persistent = MIN_NSYS / (ev0.elapsed_time(ev1) / 1000.0)
     assert syn.status() == 0
     syn.close()
     evals = MIN_NSYS * (4 * MIN_CYCLES + 1)
@@ -388,9 +399,11 @@ def bench_minimization(args, world, rank, local, flush):
                 "h2d_bytes_per_step": int(xyz.size * 8),
                 "d2h_bytes_per_step": int(c.size * 8 + e.size * 8)},
         "mean_energy_drop": (float(np.mean(e_start - e_final)) if e_start is not None else None),
-        "gpu_launches_per_step": 2,
+        "kernel": "graph (one CUDA graph per cycle: 4 batched evaluations + 4 line-search kernels)",
+        "persistent_kernel_value": persistent,
+        "gpu_launches_per_step": 1 + 8 * MIN_CYCLES + 2,
         "unit_packing": {"atoms_per_unit": tuned[0], "tiles_per_unit": tuned[1],
-                         "chosen_by": "sb_autotune over 9 packings, 8 cycles each"},
+                         "chosen_by": "sb_autotune of the evaluation over 9 packings"},
         "l2": "flushed (256 MB write) before every timed step",
     }
 

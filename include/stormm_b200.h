@@ -296,8 +296,9 @@ typedef struct {
 
 typedef struct sb_server sb_server;
 
-/* Defaults: OBC-II, controls as sb_default_minimize_controls with total_cycles 2000 and
- * convergence_rms 0.01, 2 GB budget, 512 molecules per batch, 16 batches, 50 cycles a launch */
+/* Defaults: OBC-II, controls as sb_default_minimize_controls with total_cycles 2000,
+ * convergence_rms 0.01 and the persistent kernel (lower latency for small batches), 2 GB budget,
+ * 512 molecules per batch, 16 batches, 50 cycles a launch */
 void sb_default_server_options(sb_server_options* opt);
 int sb_server_create(const sb_server_options* opt, sb_server** out);
 /* Queue one molecule (topology and coordinates are copied); thread-safe */

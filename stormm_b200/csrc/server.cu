@@ -517,6 +517,8 @@ void sb_default_server_options(sb_server_options* opt) {
   sb_default_minimize_controls(&opt->controls);
   opt->controls.total_cycles = 2000;
   opt->controls.convergence_rms = 0.01;
+  // small batches: the persistent kernel's on-chip cycles beat per-cycle graph launches
+  opt->controls.kernel = SB_MIN_PERSISTENT;
   opt->hbm_budget_bytes = 2.0e9;
   opt->max_batch_molecules = 512;
   opt->max_batches = 16;

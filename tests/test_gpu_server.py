@@ -14,7 +14,7 @@ from stormm_b200 import synthetic
 
 pytestmark = pytest.mark.gpu
 
-CONTROLS = dict(total_cycles=150, sd_cycles=30, convergence_rms=0.5)
+CONTROLS = dict(total_cycles=150, sd_cycles=30, convergence_rms=0.5, kernel=sb.MIN_PERSISTENT)
 
 
 def _alone(mol):
