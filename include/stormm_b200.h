@@ -316,6 +316,21 @@ int sb_server_get_stats(sb_server* srv, sb_server_stats* stats);
 int sb_server_destroy(sb_server* srv);
 
 /* ------------------------------------------------------------------------------------------ */
+/* STORMM's exclusion-mask tables                                                              */
+/* ------------------------------------------------------------------------------------------ */
+/* STORMM's StaticExclusionMask of one topology (Potential/static_exclusionmask.cpp:20-260, the
+ * per-system part of StaticExclusionMaskSynthesis, Synthesis/static_mask_synthesis.h:54), built
+ * on the host in STORMM's layout from the topology's exclusion lists: 256-atom supertiles and
+ * 16 x 16 tiles, supertile_map_idx (stride^2 ints), tile_map_idx (256 ints per stored
+ * supertile) and mask_data (32 words per stored tile).  Host only, no device needed.  Each
+ * n_* is the capacity of its array on input (ignored when the array is NULL) and the size
+ * needed on output: call once with NULL arrays to size them. */
+int sb_static_exclusion_mask(const sb_topology* top, int* supertile_stride_count,
+                             int* supertile_map_idx, long long* n_supertile_map,
+                             int* tile_map_idx, long long* n_tile_map, uint32_t* mask_data,
+                             long long* n_mask_data);
+
+/* ------------------------------------------------------------------------------------------ */
 /* Autotuning                                                                                  */
 /* ------------------------------------------------------------------------------------------ */
 #define SB_TUNE_EVALUATE 1

@@ -153,6 +153,8 @@ def library() -> ctypes.CDLL:
             "sb_server_drain": (ctypes.c_int, [vp, ctypes.c_double]),
             "sb_server_get_stats": (ctypes.c_int, [vp, ctypes.POINTER(ServerStats)]),
             "sb_server_destroy": (ctypes.c_int, [vp]),
+            "sb_static_exclusion_mask": (ctypes.c_int, [ctypes.POINTER(Topology), vp, vp, vp, vp,
+                                                        vp, vp, vp]),
             "sb_last_error": (ctypes.c_char_p, []),
             "sb_version": (ctypes.c_char_p, []),
         }
@@ -239,6 +241,27 @@ class _TopologyArrays:
         impr = getattr(mol, "dihe_improper", None)
         t.dihe_improper = ptr(impr, np.int32) if impr is not None else None
         self.struct = t
+
+
+def static_exclusion_mask(molecule):
+    """STORMM's StaticExclusionMask tables of one molecule (host only): a dict with
+    supertile_stride_count, supertile_map_idx, tile_map_idx and mask_data."""
+    lib = library()
+    t = _TopologyArrays(molecule)
+    nst = ctypes.c_int()
+    n = [ctypes.c_longlong(0) for _ in range(3)]
+    _check(lib.sb_static_exclusion_mask(ctypes.byref(t.struct), ctypes.byref(nst), None,
+                                        ctypes.byref(n[0]), None, ctypes.byref(n[1]), None,
+                                        ctypes.byref(n[2])), "sb_static_exclusion_mask")
+    sup = np.zeros(n[0].value, dtype=np.int32)
+    til = np.zeros(n[1].value, dtype=np.int32)
+    msk = np.zeros(n[2].value, dtype=np.uint32)
+    _check(lib.sb_static_exclusion_mask(ctypes.byref(t.struct), ctypes.byref(nst),
+                                        sup.ctypes.data, ctypes.byref(n[0]), til.ctypes.data,
+                                        ctypes.byref(n[1]), msk.ctypes.data,
+                                        ctypes.byref(n[2])), "sb_static_exclusion_mask")
+    return {"supertile_stride_count": nst.value, "supertile_map_idx": sup,
+            "tile_map_idx": til, "mask_data": msk}
 
 
 def minimize_controls(**overrides) -> MinimizeControls:
