@@ -16,6 +16,18 @@ def synthetic_paths():
     return sorted(glob.glob(os.path.join(GOLDEN, "synthetic_*.npz")))
 
 
+def default_solvent_paths():
+    """Synthetic fixtures evaluated with the library's default solvent model (OBC-II,
+    dielectric 80, no salt), which can share one synthesis."""
+    out = []
+    for p in synthetic_paths():
+        g = load(os.path.basename(p))
+        if (int(g["igb"][0]) == 3 and float(g["dielectric"][0]) == 80.0 and
+                float(g["saltcon"][0]) == 0.0):
+            out.append(p)
+    return out
+
+
 def reference_paths():
     return sorted(glob.glob(os.path.join(GOLDEN, "reference_*.npz")))
 

@@ -15,6 +15,8 @@ Fixtures written (numpy .npz, one per case):
 * ``reference_<system>_igb<k>.npz``: the reference's own test systems (Trp-cage, alanine
   dipeptide) under the settings of test/Potential/test_generalized_born.cpp:236-301, with the
   known-answer GB energies that test file asserts.
+* ``synthetic_{S64,H100,O100,V100}.npz``: solvent-model variants (salt 0.15 M with dielectric
+  78.5; HCT; OBC-I with dielectric 40; vacuum), run with ``--variants-only`` on its own.
 * ``minimize_m0.npz``: STORMM's CPU line minimizer (MolecularMechanics/minimization.tpp) on the
   64-atom molecule, energy history and final coordinates.
 """
@@ -86,10 +88,25 @@ def gb_known_answers(ref_root):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference-root", default="/root/reference")
+    ap.add_argument("--variants-only", action="store_true",
+                    help="write only the solvent-model variant fixtures")
     args = ap.parse_args()
     if not os.path.exists(DRIVER):
         raise SystemExit("build the reference driver first: make -C oracle/ref -j8")
     with tempfile.TemporaryDirectory() as tmp:
+        # 0. solvent-model variants of synthetic molecules: salt (Debye-Hueckel kappa) with a
+        #    different dielectric, HCT, OBC-I and vacuum
+        variants = (("S64", 8800, 64, ["--salt", "0.15", "--diel", "78.5"]),
+                    ("H100", 8801, 100, ["--igb", "1"]),
+                    ("O100", 8802, 100, ["--igb", "2", "--diel", "40"]),
+                    ("V100", 8803, 100, ["--igb", "0"]))
+        for name, seed, n, extra in variants:
+            mol = synthetic.make_molecule(seed, n, noise=0.1, name=name)
+            rec, _, _ = eval_molecule(mol, tmp, extra)
+            np.savez_compressed(os.path.join(HERE, f"synthetic_{name}.npz"), **rec)
+            print("wrote", name, rec["energy_terms"])
+        if args.variants_only:
+            return
         # 1. the single-point molecule and edge-case sizes
         mols = synthetic.workload_single()
         for n in (2, 12, 16, 17, 31, 32, 33, 48, 100, 255, 256, 257, 300):

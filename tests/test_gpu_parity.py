@@ -15,8 +15,8 @@ import pytest
 
 import oracle
 import stormm_b200 as sb
-from fixtures import (igb_of_fixture, load, molecule_from_fixture, reference_forces,
-                      reference_paths, rms_rel, synthetic_paths)
+from fixtures import (default_solvent_paths, igb_of_fixture, load, molecule_from_fixture,
+                      reference_forces, reference_paths, rms_rel, synthetic_paths)
 
 pytestmark = pytest.mark.gpu
 
@@ -45,7 +45,8 @@ def _check_energy(e_gpu, e_ref):
 def test_single_system_matches_stormm(path):
     g = load(os.path.basename(path))
     mol = molecule_from_fixture(g)
-    r = _run([mol], igb=igb_of_fixture(g), dielectric=float(g["dielectric"][0]))
+    r = _run([mol], igb=igb_of_fixture(g), dielectric=float(g["dielectric"][0]),
+             saltcon=float(g["saltcon"][0]))
     _check_energy(r["energies"][0], g["energy_terms"])
     err = rms_rel(r["forces"], reference_forces(g))
     assert err <= FORCE_TOL, err
@@ -73,7 +74,7 @@ def test_gb_workspace_matches_stormm():
 
 
 def test_batch_of_mixed_sizes_is_bit_identical_to_single_runs():
-    paths = synthetic_paths()
+    paths = default_solvent_paths()
     mols = [molecule_from_fixture(load(os.path.basename(p))) for p in paths]
     batch = _run(mols)
     prim_b, ovrf_b = batch["syn"].forces_fixed()
@@ -116,7 +117,8 @@ def test_run_to_run_bit_identical():
 
 
 def test_per_system_launches_match_batched():
-    mols = [molecule_from_fixture(load(os.path.basename(p))) for p in synthetic_paths()[:6]]
+    mols = [molecule_from_fixture(load(os.path.basename(p)))
+            for p in default_solvent_paths()[:6]]
     batch = _run(mols)["syn"]
     ref_prim, ref_ovrf = batch.forces_fixed()
     ref_e = batch.energies_fixed()
