@@ -24,6 +24,7 @@ constexpr int kMaxUnitSystems = 32;       // systems per fused work unit
 constexpr int kMaxFusedAtoms = 2048;      // largest molecule the fused path holds on chip
 constexpr int kNrgStride = 16;            // energy slots per system (STORMM StateVariable order)
 constexpr int kUnitMetaFields = 8;        // ints per unit-molecule row of DevSynthesis::unit_meta
+constexpr int kPairDerivPerTile = 1024;  // float2 entries per tile of DevSynthesis::pair_deriv
 constexpr float kGbRadiiOffset = 0.09f;   // Constants/generalized_born.h:114
 constexpr float kGbKscale = 0.73f;        // Constants/generalized_born.h:123
 constexpr int kPsiBits = 29;              // fixed-point bits of the in-block psi accumulators
@@ -107,6 +108,10 @@ struct DevSynthesis {
                                  // slot, first tile, LJ table offset, bond / angle / dihedral
                                  // chunk offsets; the closing row holds the totals
   int max_unit_slots;
+  // HCT pair derivatives of the work units' tiles, written by GB pass 1 of a force evaluation
+  // and read by pass 3: 32 steps x 32 lanes of (i-side, j-side) values per tile, a unit's tiles
+  // from the base in its closing unit_meta row
+  float2* pair_deriv;
 
   int* status;                   // device status word (0 = fine)
 };

@@ -100,11 +100,11 @@ struct Request {
     copyArray(&xyz, coords, 3 * n);
     // device memory the molecule holds while in flight: per-atom arrays (coordinates, forces,
     // parameters, GB workspace, minimizer state) on the padded atom count, valence records,
-    // Lennard-Jones tables and exclusion masks
+    // Lennard-Jones tables, and per tile its exclusion mask and stored pair derivatives
     const double padded = static_cast<double>((natom + 31) / 32 * 32);
     const double nblk = padded / 32.0;
     bytes = 256.0 * padded + 16.0 * (nbond + nangl + 2.0 * ndihe) + 16.0 * nt2 +
-            128.0 * nblk * (nblk + 1.0) / 2.0 + 1024.0;
+            (128.0 + 8.0 * kPairDerivPerTile) * nblk * (nblk + 1.0) / 2.0 + 1024.0;
   }
 
   sb_topology view() const {

@@ -402,12 +402,15 @@ std::unique_ptr<UnitPlan> Synthesis::makePlan(int max_slots_cap, int max_tiles_c
 void Synthesis::finalizePlan(UnitPlan* plan) const {
   std::vector<int4> desc = plan->units;
   plan->meta.clear();
+  int tile_base = 0;   // first tile of the unit in the pair-derivative store
   for (size_t u = 0; u < plan->units.size(); u++) {
     const int4 un = plan->units[u];
     desc[u].x = static_cast<int>(plan->meta.size() / kUnitMetaFields);
     int slot = 0, tile = 0, lj = 0, nb = 0, na = 0, nd = 0;
+    bool fused = true;
     for (int k = 0; k < un.y; k++) {
       const int sid = plan->systems[un.x + k];
+      fused = fused && (tiled_index[sid] < 0);
       const int n = atom_count[sid];
       const int nblk = (n + kTile - 1) / kTile;
       const int row[kUnitMetaFields] = {sid, n, slot, tile, lj, nb, na, nd};
@@ -419,11 +422,19 @@ void Synthesis::finalizePlan(UnitPlan* plan) const {
       na += (h_angl_start[sid + 1] - h_angl_start[sid] + 31) / 32;
       nd += (h_dihe_start[sid + 1] - h_dihe_start[sid] + 31) / 32;
     }
-    const int last[kUnitMetaFields] = {-1, 0, slot, tile, lj, nb, na, nd};
+    // closing row: the unit's first tile in the pair-derivative store, then the totals (units
+    // of molecules on the tiled path never run the fused kernels and take no store)
+    const int last[kUnitMetaFields] = {fused ? tile_base : 0, 0, slot, tile, lj, nb, na, nd};
     plan->meta.insert(plan->meta.end(), last, last + kUnitMetaFields);
     if (slot != un.z || tile != un.w) {
       throw Error(SB_ERR_ARGUMENT, "inconsistent work-unit descriptor");
     }
+    if (fused) {
+      tile_base += tile;
+    }
+  }
+  if (tile_base > fused_tiles) {
+    throw Error(SB_ERR_ARGUMENT, "work units hold more tiles than the molecules");
   }
   plan->d_units.upload(desc);
   plan->d_meta.upload(plan->meta);
@@ -456,6 +467,17 @@ void Synthesis::buildUnits() {
       h_atom_prefix.push_back(h_atom_prefix.back() + static_cast<int>(nb) * kTile);
     }
   }
+  long long ftiles = 0;
+  for (int s = 0; s < nsys; s++) {
+    if (tiled_index[s] < 0) {
+      const long long nb = (atom_count[s] + kTile - 1) / kTile;
+      ftiles += nb * (nb + 1) / 2;
+    }
+  }
+  if (ftiles > 200000000LL) {
+    throw Error(SB_ERR_UNSUPPORTED, "too many tiles on the fused path");
+  }
+  fused_tiles = static_cast<int>(ftiles);
   const int slots_cap = (opt.max_atoms_per_unit > 0) ? opt.max_atoms_per_unit : 256;
   const int tiles_cap = (opt.max_tiles_per_unit > 0) ? opt.max_tiles_per_unit : 36;
   eval_plan = makePlan(slots_cap, tiles_cap);
@@ -555,6 +577,8 @@ void Synthesis::upload() {
   d_sumdeijda_ovrf.zeros(np);
   d_born_radii.zeros(np);
   d_status.zeros(1);
+  // one tile beyond the last unit's, so no store or load of a tile walk can leave the buffer
+  d_pair_deriv.zeros(static_cast<size_t>(fused_tiles + 1) * kPairDerivPerTile);
 
   DevSynthesis &d = dev;
   std::memset(&d, 0, sizeof(DevSynthesis));
@@ -610,6 +634,7 @@ void Synthesis::upload() {
   d.unit_desc = eval_plan->d_units.p;
   d.unit_meta = eval_plan->d_meta.p;
   d.max_unit_slots = max_unit_slots;
+  d.pair_deriv = d_pair_deriv.p;
   d.status = d_status.p;
 }
 

@@ -176,6 +176,8 @@ public:
   DeviceArray<long long> d_psi, d_sumdeijda;
   DeviceArray<int> d_psi_ovrf, d_sumdeijda_ovrf, d_status;
   DeviceArray<float> d_born_radii;
+  DeviceArray<float2> d_pair_deriv;
+  int fused_tiles = 0;           // tiles of all molecules on the fused path
   DeviceArray<int> d_unpadded_map;
   DeviceArray<double> d_stage_xyz, d_stage_nrg;
   DeviceArray<int> d_tiled_systems, d_tile_prefix, d_atom_prefix;

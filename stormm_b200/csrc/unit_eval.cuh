@@ -64,7 +64,8 @@ __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __
 
 
 // HCT descreening of an atom of offset radius rho by a neighbour of screened radius sj at
-// distance r (invr = 1/r); returns the amount psi decreases by.
+// distance r (invr = 1/r), for two (r, rho, sj) combinations at once in packed FP32; returns the
+// amounts psi decreases by.
 //
 // Beyond r = 4 sj the reference's Taylor series applies (nonbonded_potential.tpp:590-596).
 // Closer in, the three closed forms the reference selects by overlap case (no overlap, partial
@@ -72,30 +73,8 @@ __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __
 // expression in U = r + sj and L = max(rho, |r - sj|):
 //   I = 1/2 [1/L - 1/U + (sj^2 - r^2)/(4r) (1/L^2 - 1/U^2) + ln(L/U) / (2r)]
 //       + (1/rho - 1/L) when rho < sj - r,
-// and I = 0 when rho >= U.  One formula instead of four keeps a warp on at most two paths.
-__device__ __forceinline__ float hctIntegral(float r, float r2, float invr, float rho, float sj) {
-  if (r > 4.0f * sj) {
-    const float sj2 = sj * sj;
-    const float invr2 = invr * invr;
-    const float t = sj2 * invr2;
-    const float dumbo = kTaylorA + t * (kTaylorB + t * (kTaylorC + t * (kTaylorD + t * kTaylorDD)));
-    return sj * t * invr2 * dumbo;
-  }
-  const float u = r + sj;
-  const float l = fmaxf(rho, fabsf(r - sj));
-  const float inv_lu = __fdividef(1.0f, l * u);
-  const float il = u * inv_lu;
-  const float iu = l * inv_lu;
-  const float dlu = il - iu;
-  float v = dlu + 0.25f * (sj * sj - r2) * invr * dlu * (il + iu) + 0.5f * invr * __logf(l * iu);
-  if (rho < sj - r) {
-    // the atom sits inside the neighbour's sphere: rare, so a branch beats a reciprocal per pair
-    v += 2.0f * (__fdividef(1.0f, rho) - il);
-  }
-  return (rho < u) ? 0.5f * v : 0.0f;
-}
-
-// hctIntegral for two pairs at once
+// and I = 0 when rho >= U.  One formula instead of four keeps a warp on at most two paths; the
+// inside case is rare, so a branch there beats a reciprocal per pair.
 __device__ __forceinline__ float2 hctIntegral2(float2 r, float2 r2, float2 invr, float2 rho,
                                                float2 sj) {
   const bool far_x = r.x > 4.0f * sj.x;
@@ -135,32 +114,126 @@ __device__ __forceinline__ float2 hctIntegral2(float2 r, float2 r2, float2 invr,
   return f2(far_x ? vf.x : vn.x, far_y ? vf.y : vn.y);
 }
 
-// Radial derivative of hctIntegral, -(1/r) dI/dr, the factor the reference multiplies by the
-// chain-rule dE/dR (nonbonded_potential.tpp:1116-1165), from the same unified expression
-// (lambda = dL/dr: 1 without overlap, 0 on partial overlap, -1 inside the neighbour).
-__device__ __forceinline__ float hctDerivative(float r, float r2, float invr, float rho,
-                                               float sj) {
+// Radial derivative of the HCT integral, -(1/r) dI/dr, the factor the reference multiplies by
+// the chain-rule dE/dR (nonbonded_potential.tpp:1116-1165), from the same unified expression
+// (lambda = dL/dr: 1 without overlap, 0 on partial overlap, -1 inside the neighbour):
+//   dI/dr = 1/2 [-lambda/L^2 + 1/U^2 + q'(1/L^2 - 1/U^2) + 2q (1/U^3 - lambda/L^3)
+//                + (lambda/L - 1/U - ln(L/U)/r) / (2r)] - 1/L^2 (inside),
+// q = (sj^2 - r^2)/(4r), q' = dq/dr.  Here for both directions of one pair at once: x for
+// (rho.x, sj.x), y for (rho.y, sj.y), sharing r; the far and near forms run only when some lane
+// of the warp needs them.
+__device__ __forceinline__ float2 hctDerivative2(float r, float r2, float invr, float2 rho,
+                                                 float2 sj) {
   const float invr2 = invr * invr;
-  if (r > 4.0f * sj) {
-    const float t = sj * sj * invr2;
-    const float dumbo = kTaylorE + t * (kTaylorF + t * (kTaylorG + t * (kTaylorH + t * kTaylorHH)));
-    return t * sj * invr2 * invr2 * dumbo;
+  const bool far_x = r > 4.0f * sj.x;
+  const bool far_y = r > 4.0f * sj.y;
+  const float2 sj2 = mul2(sj, sj);
+  float2 vf = f2(0.0f);
+  float2 vn = f2(0.0f);
+  if (far_x || far_y) {
+    const float2 t = mul2(sj2, f2(invr2));
+    float2 dumbo = fma2(t, f2(kTaylorHH), f2(kTaylorH));
+    dumbo = fma2(t, dumbo, f2(kTaylorG));
+    dumbo = fma2(t, dumbo, f2(kTaylorF));
+    dumbo = fma2(t, dumbo, f2(kTaylorE));
+    vf = mul2(mul2(mul2(t, sj), f2(invr2 * invr2)), dumbo);
   }
-  const float u = r + sj;
-  const float rms = r - sj;
-  const float l = fmaxf(rho, fabsf(rms));
-  const float lam = (rms >= rho) ? 1.0f : ((-rms > rho) ? -1.0f : 0.0f);
-  const float inv_lu = __fdividef(1.0f, l * u);
-  const float il = u * inv_lu;
-  const float iu = l * inv_lu;
-  const float il2 = il * il;
-  const float iu2 = iu * iu;
-  const float q = 0.25f * (sj * sj - r2) * invr;
-  const float dq = -0.25f * fmaf(sj * sj, invr2, 1.0f);
-  float di = -lam * il2 + iu2 + dq * (il2 - iu2) + 2.0f * q * (iu2 * iu - lam * il2 * il) +
-             0.5f * invr * (lam * il - iu - invr * __logf(l * iu));
-  di = 0.5f * di - ((-rms > rho) ? il2 : 0.0f);
-  return (rho < u) ? -di * invr : 0.0f;
+  if (!(far_x && far_y)) {
+    const float2 u = add2(f2(r), sj);
+    const float2 rms = sub2(f2(r), sj);
+    const float2 l = f2(fmaxf(rho.x, fabsf(rms.x)), fmaxf(rho.y, fabsf(rms.y)));
+    const bool in_x = -rms.x > rho.x;
+    const bool in_y = -rms.y > rho.y;
+    const float2 lam = f2((rms.x >= rho.x) ? 1.0f : (in_x ? -1.0f : 0.0f),
+                          (rms.y >= rho.y) ? 1.0f : (in_y ? -1.0f : 0.0f));
+    const float2 lu = mul2(l, u);
+    const float2 inv_lu = f2(__fdividef(1.0f, lu.x), __fdividef(1.0f, lu.y));
+    const float2 il = mul2(u, inv_lu);
+    const float2 iu = mul2(l, inv_lu);
+    const float2 il2 = mul2(il, il);
+    const float2 iu2 = mul2(iu, iu);
+    const float2 liu = mul2(l, iu);
+    const float2 lg = f2(__logf(liu.x), __logf(liu.y));
+    const float2 q2 = mul2(f2(0.5f * invr), sub2(sj2, f2(r2)));        // 2 q
+    const float2 dq = mul2(f2(-0.25f), fma2(sj2, f2(invr2), f2(1.0f)));
+    const float2 lil2 = mul2(lam, il2);
+    float2 di = sub2(iu2, lil2);
+    di = fma2(dq, sub2(il2, iu2), di);
+    di = fma2(q2, sub2(mul2(iu2, iu), mul2(lil2, il)), di);
+    di = fma2(f2(0.5f * invr), sub2(sub2(mul2(lam, il), iu), mul2(f2(invr), lg)), di);
+    di = sub2(mul2(f2(0.5f), di), f2(in_x ? il2.x : 0.0f, in_y ? il2.y : 0.0f));
+    const float2 v = mul2(di, f2(-invr));
+    vn = f2((rho.x < u.x) ? v.x : 0.0f, (rho.y < u.y) ? v.y : 0.0f);
+  }
+  return f2(far_x ? vf.x : vn.x, far_y ? vf.y : vn.y);
+}
+
+// The HCT integral and its radial derivative together, for both directions of one pair (x for
+// (rho.x, sj.x), y for (rho.y, sj.y)): the Taylor forms share t = (sj / r)^2, the closed forms
+// share the reciprocals and the logarithm.
+__device__ __forceinline__ void hctBoth2(float r, float r2, float invr, float2 rho, float2 sj,
+                                         float2* integral, float2* deriv) {
+  const float invr2 = invr * invr;
+  const bool far_x = r > 4.0f * sj.x;
+  const bool far_y = r > 4.0f * sj.y;
+  const float2 sj2 = mul2(sj, sj);
+  float2 vfi = f2(0.0f), vfd = f2(0.0f), vni = f2(0.0f), vnd = f2(0.0f);
+  if (far_x || far_y) {
+    const float2 t = mul2(sj2, f2(invr2));
+    float2 di = fma2(t, f2(kTaylorDD), f2(kTaylorD));
+    di = fma2(t, di, f2(kTaylorC));
+    di = fma2(t, di, f2(kTaylorB));
+    di = fma2(t, di, f2(kTaylorA));
+    float2 dd = fma2(t, f2(kTaylorHH), f2(kTaylorH));
+    dd = fma2(t, dd, f2(kTaylorG));
+    dd = fma2(t, dd, f2(kTaylorF));
+    dd = fma2(t, dd, f2(kTaylorE));
+    const float2 tsr = mul2(mul2(sj, t), f2(invr2));
+    vfi = mul2(tsr, di);
+    vfd = mul2(mul2(tsr, f2(invr2)), dd);
+  }
+  if (!(far_x && far_y)) {
+    const float2 u = add2(f2(r), sj);
+    const float2 rms = sub2(f2(r), sj);
+    const float2 l = f2(fmaxf(rho.x, fabsf(rms.x)), fmaxf(rho.y, fabsf(rms.y)));
+    const bool in_x = -rms.x > rho.x;      // inside the neighbour's sphere
+    const bool in_y = -rms.y > rho.y;
+    const float2 lu = mul2(l, u);
+    const float2 inv_lu = f2(__fdividef(1.0f, lu.x), __fdividef(1.0f, lu.y));
+    const float2 il = mul2(u, inv_lu);
+    const float2 iu = mul2(l, inv_lu);
+    const float2 liu = mul2(l, iu);
+    const float2 lg = f2(__logf(liu.x), __logf(liu.y));
+    const float2 s2mr2 = sub2(sj2, f2(r2));
+    // the integral
+    const float2 dlu = sub2(il, iu);
+    const float2 q = mul2(mul2(f2(0.25f * invr), s2mr2), dlu);
+    float2 v = add2(fma2(q, add2(il, iu), dlu), mul2(f2(0.5f * invr), lg));
+    if (in_x) {
+      v.x += 2.0f * (__fdividef(1.0f, rho.x) - il.x);
+    }
+    if (in_y) {
+      v.y += 2.0f * (__fdividef(1.0f, rho.y) - il.y);
+    }
+    vni = f2((rho.x < u.x) ? 0.5f * v.x : 0.0f, (rho.y < u.y) ? 0.5f * v.y : 0.0f);
+    // its derivative, lambda = dL/dr
+    const float2 lam = f2((rms.x >= rho.x) ? 1.0f : (in_x ? -1.0f : 0.0f),
+                          (rms.y >= rho.y) ? 1.0f : (in_y ? -1.0f : 0.0f));
+    const float2 il2 = mul2(il, il);
+    const float2 iu2 = mul2(iu, iu);
+    const float2 q2 = mul2(f2(0.5f * invr), s2mr2);
+    const float2 dq = mul2(f2(-0.25f), fma2(sj2, f2(invr2), f2(1.0f)));
+    const float2 lil2 = mul2(lam, il2);
+    float2 dv = sub2(iu2, lil2);
+    dv = fma2(dq, sub2(il2, iu2), dv);
+    dv = fma2(q2, sub2(mul2(iu2, iu), mul2(lil2, il)), dv);
+    dv = fma2(f2(0.5f * invr), sub2(sub2(mul2(lam, il), iu), mul2(f2(invr), lg)), dv);
+    dv = sub2(mul2(f2(0.5f), dv), f2(in_x ? il2.x : 0.0f, in_y ? il2.y : 0.0f));
+    const float2 w = mul2(dv, f2(-invr));
+    vnd = f2((rho.x < u.x) ? w.x : 0.0f, (rho.y < u.y) ? w.y : 0.0f);
+  }
+  *integral = f2(far_x ? vfi.x : vni.x, far_y ? vfi.y : vni.y);
+  *deriv = f2(far_x ? vfd.x : vnd.x, far_y ? vfd.y : vnd.y);
 }
 
 // Shared-memory layout of one work unit
@@ -743,7 +816,9 @@ struct PairPass {
   float inv4ri;     // 1 / (4 R_i)
   int code_i;
   unsigned mask;
-  float fxi, fyi, fzi, dei, fxj, fyj, fzj, dej;
+  float2 fxyi, fxyj;   // x, y force sums: i side, traveling j side
+  float fzi, fzj;
+  float2 de2;          // dE/dR sums: i side, traveling j side
   float e_elec, e_vdw, e_gb;
   __device__ PairPass(const UnitSmem &s_in, float kappa, float inv_dielectric) :
       s(s_in), kk(-kappa * kGbKscale), inv_diel(inv_dielectric), salt(kappa > 0.0f) {}
@@ -753,15 +828,18 @@ struct PairPass {
     inv4ri = 0.25f * s.gbv[islot].x;
     code_i = __float_as_int(s.prm[islot].y) & 0xffff;
     mask = mask_in;
-    fxi = fyi = fzi = dei = 0.0f;
-    fxj = fyj = fzj = dej = 0.0f;
+    fxyi = fxyj = de2 = f2(0.0f);
+    fzi = fzj = 0.0f;
     e_elec = e_vdw = e_gb = 0.0f;
   }
   __device__ __forceinline__ void pair(int jslot, int jl) {
     const float4 aj = s.pa[jslot];
     const float4 bj = s.pb[jslot];
-    const float3 dv = pairDelta(ai, bi, aj, bj);
-    const float r2 = fmaf(dv.x, dv.x, fmaf(dv.y, dv.y, dv.z * dv.z));
+    // x and y in packed FP32: the same roundings as the scalar forms
+    const float2 dxy = add2(sub2(f2(aj.x, aj.y), f2(ai.x, ai.y)),
+                            sub2(f2(bj.x, bj.y), f2(bi.x, bi.y)));
+    const float dz = (aj.z - ai.z) + (bj.z - bi.z);
+    const float r2 = fmaf(dxy.x, dxy.x, fmaf(dxy.y, dxy.y, dz * dz));
     const float qiqj_all = ai.w * aj.w;
     float fmag = 0.0f;
     if (NB) {
@@ -808,27 +886,24 @@ struct PairPass {
         const float temp6 = qiqj * temp4 * fmaf(fgbk, expmkf, dielfac);
         fmag += temp6 * fmaf(-0.25f, efac, 1.0f);
         const float temp5 = 0.5f * efac * temp6 * fmaf(0.25f, r2, ijb);
-        dei = fmaf(bi.w, temp5, dei);
-        dej = fmaf(bj.w, temp5, dej);
+        de2 = fma2(f2(bi.w, bj.w), f2(temp5), de2);
       }
     }
     if (FORCE) {
-      fxi = fmaf(fmag, dv.x, fxi);
-      fyi = fmaf(fmag, dv.y, fyi);
-      fzi = fmaf(fmag, dv.z, fzi);
-      fxj = fmaf(-fmag, dv.x, fxj);
-      fyj = fmaf(-fmag, dv.y, fyj);
-      fzj = fmaf(-fmag, dv.z, fzj);
+      fxyi = fma2(f2(fmag), dxy, fxyi);
+      fzi = fmaf(fmag, dz, fzi);
+      fxyj = fma2(f2(-fmag), dxy, fxyj);
+      fzj = fmaf(-fmag, dz, fzj);
     }
   }
   __device__ __forceinline__ void rotate(int lane) {
     if (FORCE) {
       const int src = (lane + 1) & 31;
-      fxj = __shfl_sync(kFullMask, fxj, src);
-      fyj = __shfl_sync(kFullMask, fyj, src);
+      fxyj.x = __shfl_sync(kFullMask, fxyj.x, src);
+      fxyj.y = __shfl_sync(kFullMask, fxyj.y, src);
       fzj = __shfl_sync(kFullMask, fzj, src);
       if (GB) {
-        dej = __shfl_sync(kFullMask, dej, src);
+        de2.y = __shfl_sync(kFullMask, de2.y, src);
       }
     }
   }
@@ -856,8 +931,8 @@ struct DerivPass {
     const float r2 = fmaf(dv.x, dv.x, fmaf(dv.y, dv.y, dv.z * dv.z));
     const float invr = rsqrtf(r2);
     const float r = r2 * invr;
-    const float fmag = hctDerivative(r, r2, invr, bi.w, aj.w) * de_i +
-                       hctDerivative(r, r2, invr, bj.w, ai.w) * de_j;
+    const float2 hd = hctDerivative2(r, r2, invr, f2(bi.w, bj.w), f2(aj.w, ai.w));
+    const float fmag = fmaf(hd.y, de_j, hd.x * de_i);
     fxi = fmaf(-fmag, dv.x, fxi);
     fyi = fmaf(-fmag, dv.y, fyi);
     fzi = fmaf(-fmag, dv.z, fzi);
@@ -873,9 +948,110 @@ struct DerivPass {
   }
 };
 
-__device__ void gbRadiiTiles(const UnitSmem &s, int nsys_u, int ntiles, int first, int stride) {
+// GB pass 1 of a force evaluation: psi_i -= H(r, rho_i, s_j rho_j), psi_j -= H(r, rho_j,
+// s_i rho_i), and the radial derivatives of both terms stored for pass 3 (one float2 per lane
+// and step of the tile walk, so the stores of a step are one coalesced 256-byte line)
+struct RadiiDerivPass {
+  const UnitSmem &s;
+  float4 ai, bi;
+  float psi_i, psi_j;   // i-side sum, traveling j-side sum
+  float2* out;          // this lane's entry for the current step
+  __device__ RadiiDerivPass(const UnitSmem &s_in) : s(s_in) {}
+  __device__ __forceinline__ void begin(int islot, float2* tile_out) {
+    ai = s.pa[islot];
+    bi = s.pb[islot];
+    psi_i = 0.0f;
+    psi_j = 0.0f;
+    out = tile_out;
+  }
+  __device__ __forceinline__ void pair(int jslot, int) {
+    const float4 aj = s.pa[jslot];
+    const float4 bj = s.pb[jslot];
+    const float2 dxy = add2(sub2(f2(aj.x, aj.y), f2(ai.x, ai.y)),
+                            sub2(f2(bj.x, bj.y), f2(bi.x, bi.y)));
+    const float dz = (aj.z - ai.z) + (bj.z - bi.z);
+    const float r2 = fmaf(dxy.x, dxy.x, fmaf(dxy.y, dxy.y, dz * dz));
+    const float invr = rsqrtf(r2);
+    const float r = r2 * invr;
+    float2 h, hd;
+    hctBoth2(r, r2, invr, f2(bi.w, bj.w), f2(aj.w, ai.w), &h, &hd);
+    psi_i -= h.x;
+    psi_j -= h.y;
+    __stcg(out, hd);
+  }
+  __device__ __forceinline__ void rotate(int lane) {
+    psi_j = __shfl_sync(kFullMask, psi_j, (lane + 1) & 31);
+    out += 32;
+  }
+};
+
+// Pass 3 from the stored derivatives: the force of a pair is (hd_i dE/dR_i + hd_j dE/dR_j) times
+// the separation, with no transcendental left to evaluate
+struct DerivStoredPass {
+  const UnitSmem &s;
+  float4 ai, bi;
+  float de_i;
+  float2 fxyi, fxyj;
+  float fzi, fzj;
+  const float2* in;
+  __device__ DerivStoredPass(const UnitSmem &s_in) : s(s_in) {}
+  __device__ __forceinline__ void begin(int islot, const float2* tile_in) {
+    ai = s.pa[islot];
+    bi = s.pb[islot];
+    de_i = s.gbv[islot].y;
+    fxyi = fxyj = f2(0.0f);
+    fzi = fzj = 0.0f;
+    in = tile_in;
+  }
+  __device__ __forceinline__ void pair(int jslot, int) {
+    const float2 hd = __ldcs(in);
+    const float4 aj = s.pa[jslot];
+    const float4 bj = s.pb[jslot];
+    const float de_j = s.gbv[jslot].y;
+    const float2 dxy = add2(sub2(f2(aj.x, aj.y), f2(ai.x, ai.y)),
+                            sub2(f2(bj.x, bj.y), f2(bi.x, bi.y)));
+    const float dz = (aj.z - ai.z) + (bj.z - bi.z);
+    const float fmag = fmaf(hd.y, de_j, hd.x * de_i);
+    fxyi = fma2(f2(-fmag), dxy, fxyi);
+    fzi = fmaf(-fmag, dz, fzi);
+    fxyj = fma2(f2(fmag), dxy, fxyj);
+    fzj = fmaf(fmag, dz, fzj);
+  }
+  __device__ __forceinline__ void rotate(int lane) {
+    const int src = (lane + 1) & 31;
+    fxyj.x = __shfl_sync(kFullMask, fxyj.x, src);
+    fxyj.y = __shfl_sync(kFullMask, fxyj.y, src);
+    fzj = __shfl_sync(kFullMask, fzj, src);
+    in += 32;
+  }
+};
+
+// Entry of lane 0, step 0 of tile t of a unit whose tiles start at tile_base in the store
+__device__ __forceinline__ size_t pairDerivOffset(int tile_base, int t) {
+  return static_cast<size_t>(tile_base + t) * kPairDerivPerTile;
+}
+
+template <bool STORE>
+__device__ void gbRadiiTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u, int ntiles,
+                             int tile_base, int first, int stride) {
   const int lane = threadIdx.x & 31;
   const float ps = static_cast<float>(1 << kPsiBits);
+  if (STORE) {
+    RadiiDerivPass p(s);
+    for (int t = first; t < ntiles; t += stride) {
+      const TileInfo ti = tileInfo(s, nsys_u, t);
+      p.begin(ti.ibase + lane, d.pair_deriv + pairDerivOffset(tile_base, t) + lane);
+      walkTile(p, ti, lane);
+      if (lane < ti.ni) {
+        atomicAddInt63(p.psi_i * ps, &s.psi[ti.ibase + lane], &s.psio[ti.ibase + lane]);
+      }
+      const int jl = traveledAtom(ti, lane);
+      if (jl < ti.nj) {
+        atomicAddInt63(p.psi_j * ps, &s.psi[ti.jbase + jl], &s.psio[ti.jbase + jl]);
+      }
+    }
+    return;
+  }
   RadiiPass2 p(s);
   for (int t = first; t < ntiles; t += stride) {
     const TileInfo ti = tileInfo(s, nsys_u, t);
@@ -931,17 +1107,17 @@ __device__ void pairTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u, 
     if (FORCE) {
       if (lane < ti.ni) {
         const int is = ti.ibase + lane;
-        addForce(s, is, p.fxi, p.fyi, p.fzi, fs);
+        addForce(s, is, p.fxyi.x, p.fxyi.y, p.fzi, fs);
         if (GB) {
-          atomicAddInt63(p.dei * ds, &s.de[is], &s.deo[is]);
+          atomicAddInt63(p.de2.x * ds, &s.de[is], &s.deo[is]);
         }
       }
       const int jl = traveledAtom(ti, lane);
       if (jl < ti.nj) {
         const int js = ti.jbase + jl;
-        addForce(s, js, p.fxj, p.fyj, p.fzj, fs);
+        addForce(s, js, p.fxyj.x, p.fxyj.y, p.fzj, fs);
         if (GB) {
-          atomicAddInt63(p.dej * ds, &s.de[js], &s.deo[js]);
+          atomicAddInt63(p.de2.y * ds, &s.de[js], &s.deo[js]);
         }
       }
     }
@@ -966,20 +1142,20 @@ __device__ void pairTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u, 
 }
 
 __device__ void gbDerivativeTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u,
-                                  int ntiles, int first, int stride) {
+                                  int ntiles, int tile_base, int first, int stride) {
   const int lane = threadIdx.x & 31;
   const float fs = d.frc_scale;
-  DerivPass p(s);
+  DerivStoredPass p(s);
   for (int t = first; t < ntiles; t += stride) {
     const TileInfo ti = tileInfo(s, nsys_u, t);
-    p.begin(ti.ibase + lane);
+    p.begin(ti.ibase + lane, d.pair_deriv + pairDerivOffset(tile_base, t) + lane);
     walkTile(p, ti, lane);
     if (lane < ti.ni) {
-      addForce(s, ti.ibase + lane, p.fxi, p.fyi, p.fzi, fs);
+      addForce(s, ti.ibase + lane, p.fxyi.x, p.fxyi.y, p.fzi, fs);
     }
     const int jl = traveledAtom(ti, lane);
     if (jl < ti.nj) {
-      addForce(s, ti.jbase + jl, p.fxj, p.fyj, p.fzj, fs);
+      addForce(s, ti.jbase + jl, p.fxyj.x, p.fxyj.y, p.fzj, fs);
     }
   }
 }
@@ -1030,9 +1206,10 @@ __device__ __forceinline__ float obcChainFactor(const DevSynthesis &d, int gi, f
 // Work-unit staging and the staged evaluation, shared by the evaluation and minimization kernels
 // ------------------------------------------------------------------------------------------------
 struct UnitShape {
-  int nsys;     // molecules in the unit
-  int nslots;   // atom slots (sum of the molecules' sizes padded to 32)
-  int ntiles;   // 32 x 32 tiles of the molecules' lower triangles
+  int nsys;       // molecules in the unit
+  int nslots;     // atom slots (sum of the molecules' sizes padded to 32)
+  int ntiles;     // 32 x 32 tiles of the molecules' lower triangles
+  int tile_base;  // first tile of the unit in the pair-derivative store
 };
 
 // Molecule table, prefix sums and Lennard-Jones tables of unit u.  Returns false (after setting
@@ -1054,6 +1231,7 @@ __device__ bool stageUnitTables(const DevSynthesis &d, const UnitSmem &s, int u,
   }
   // the unit's molecule table, precomputed on the host: one coalesced load per field
   const int* meta = d.unit_meta + static_cast<size_t>(desc.x) * kUnitMetaFields;
+  shape->tile_base = meta[nsys_u * kUnitMetaFields];
   for (int e = team.rank(); e < (nsys_u + 1) * kUnitMetaFields; e += team.size()) {
     const int k = e / kUnitMetaFields;
     const int v = meta[e];
@@ -1164,7 +1342,7 @@ __device__ void evaluateStaged(const DevSynthesis &d, const UnitSmem &s, const U
     }
   }
   if (gb) {
-    gbRadiiTiles(s, nsys_u, ntiles, team.warp(), team.warps());
+    gbRadiiTiles<FORCE>(d, s, nsys_u, ntiles, us.tile_base, team.warp(), team.warps());
     team.sync();
     // effective radii, self terms (nonbonded_potential.tpp:730-805); a warp's 32 slots
     // belong to one molecule, so the self energies reduce across the warp
@@ -1260,7 +1438,7 @@ __device__ void evaluateStaged(const DevSynthesis &d, const UnitSmem &s, const U
       s.gbv[slot].y = sde;
     }
     team.sync();
-    gbDerivativeTiles(d, s, nsys_u, ntiles, team.warp(), team.warps());
+    gbDerivativeTiles(d, s, nsys_u, ntiles, us.tile_base, team.warp(), team.warps());
     team.sync();
   }
 }

@@ -1,11 +1,13 @@
 """The tiled path for large molecules (2,000-5,000-atom chains, or any molecule routed there by
 tiled_above_atoms) against the fused path, STORMM's own results and the FP64 oracle.
 
-The tiled path runs the fused kernel's pair functors and valence code with the same integer
-accumulation; compiled into different kernels, the FP32 arithmetic may round a few operations
-differently, so the two paths agree to a few units of the last fixed-point bit (forces within
-1e-6 RMS relative, energies within 1e-7 of the summed terms), and each is bit-identical from run
-to run.  Against FP64 the tolerances are those of the single-point tests."""
+The tiled path runs the fused kernel's valence code and pass-2 functor with the same integer
+accumulation, but its GB passes differ in order: it sums psi over two pair streams per lane and
+recomputes the HCT derivatives in pass 3, where the fused kernel walks one stream and stores the
+derivatives from pass 1.  The two paths therefore agree to FP32 rounding (forces within 1e-6 RMS
+relative and 2e-7 of the largest component, energies within 1e-7 of the summed terms), and each
+is bit-identical from run to run.  Against FP64 the tolerances are those of the single-point
+tests."""
 import os
 
 import numpy as np
@@ -47,9 +49,12 @@ def test_tiled_path_agrees_with_fused_and_repeats_exactly():
     _close(fused, tiled)
     fp, _ = fused.forces_fixed()
     tp, _ = tiled.forces_fixed()
-    assert np.abs(fp - tp).max() <= 64
+    assert np.abs(fp - tp).max() <= 2.0e-7 * np.abs(fp).max()
     for a, b in zip(fused.gb_workspace(), tiled.gb_workspace()):
-        np.testing.assert_allclose(b, a, rtol=1e-6, atol=1e-6)
+        # psi summed in another order: the effective radii and the dE/dR sums (with their
+        # cancellations) carry that FP32 rounding, so compare them as arrays
+        assert rms_rel(b, a) <= 1e-6
+        assert np.abs(b - a).max() <= 1e-6 * np.abs(a).max()
     prim, ovrf = tiled.forces_fixed()
     nrg = tiled.energies_fixed().copy()
     tiled.initialize()
