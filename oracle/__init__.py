@@ -64,6 +64,13 @@ def _lib():
         _LIB.orc_minimize_ex.argtypes = [ctypes.POINTER(_System), ctypes.c_void_p, ctypes.c_int,
                                          ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                          ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+        _LIB.orc_evaluate_clash.argtypes = [ctypes.POINTER(_System)] + [ctypes.c_void_p] * 6 + [
+            ctypes.c_int, ctypes.c_double, ctypes.c_double]
+        _LIB.orc_minimize_clash.argtypes = [ctypes.POINTER(_System), ctypes.c_void_p,
+                                            ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                            ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                            ctypes.c_double, ctypes.c_void_p,
+                                            ctypes.POINTER(ctypes.c_int)]
         _LIB.orc_float_to_int63.argtypes = [ctypes.c_float, ctypes.POINTER(ctypes.c_int32),
                                             ctypes.POINTER(ctypes.c_int32)]
         _LIB.orc_double_to_int95.argtypes = [ctypes.c_double, ctypes.POINTER(ctypes.c_int64),
@@ -94,7 +101,9 @@ class OracleSystem:
         self.struct = s
         self.natom = int(arrays["natom"])
 
-    def evaluate(self, coords, forces=True, terms=7):
+    def evaluate(self, coords, forces=True, terms=7, clash_distance=0.0, clash_ratio=0.0):
+        """Energies (and forces); with clash_distance or clash_ratio positive, the
+        clash-mitigated evaluation (softened Coulomb and Lennard-Jones cores)."""
         lib = _lib()
         c = np.ascontiguousarray(np.asarray(coords, dtype=np.float64).reshape(-1))
         e = np.zeros(NTERMS)
@@ -102,19 +111,24 @@ class OracleSystem:
         psi = np.zeros(self.natom)
         rad = np.zeros(self.natom)
         sde = np.zeros(self.natom)
-        lib.orc_evaluate(ctypes.byref(self.struct), c.ctypes.data,
-                         f.ctypes.data if f is not None else None, e.ctypes.data,
-                         psi.ctypes.data, rad.ctypes.data, sde.ctypes.data, terms)
+        lib.orc_evaluate_clash(ctypes.byref(self.struct), c.ctypes.data,
+                               f.ctypes.data if f is not None else None, e.ctypes.data,
+                               psi.ctypes.data, rad.ctypes.data, sde.ctypes.data, terms,
+                               clash_distance, clash_ratio)
         return {"energies": e, "forces": None if f is None else f.reshape(-1, 3), "psi": psi,
                 "radii": rad, "sumdeijda": sde}
 
-    def minimize(self, coords, maxcyc, sd_cycles, dx0=0.01, drms=0.0, with_cycles=False):
+    def minimize(self, coords, maxcyc, sd_cycles, dx0=0.01, drms=0.0, with_cycles=False,
+                 clash_cycles=0, clash_distance=0.2, clash_ratio=0.5):
+        """Line minimization; the first clash_cycles cycles clash-damped (STORMM's defaults
+        for the distance and the ratio)."""
         lib = _lib()
         c = np.ascontiguousarray(np.asarray(coords, dtype=np.float64).reshape(-1)).copy()
         hist = np.zeros(maxcyc + 1)
         ran = ctypes.c_int(0)
-        lib.orc_minimize_ex(ctypes.byref(self.struct), c.ctypes.data, maxcyc, sd_cycles, dx0,
-                            drms, hist.ctypes.data, ctypes.byref(ran))
+        lib.orc_minimize_clash(ctypes.byref(self.struct), c.ctypes.data, maxcyc, sd_cycles, dx0,
+                               drms, clash_cycles, clash_distance, clash_ratio,
+                               hist.ctypes.data, ctypes.byref(ran))
         if with_cycles:
             return c.reshape(-1, 3), hist, ran.value
         return c.reshape(-1, 3), hist

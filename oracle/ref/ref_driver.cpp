@@ -11,7 +11,8 @@
 //       and the StaticExclusionMask tables.
 //   minimize <prmtop> <inpcrd> <out.bin> --maxcyc N --ncyc N [options]
 //       STORMM's CPU line minimizer (MolecularMechanics/minimization.h:157); writes the energy
-//       history and the final coordinates.
+//       history and the final coordinates.  --cdcyc N runs its first N cycles clash-damped with
+//       --clash-r0 / --clash-ratio (STORMM defaults 0.2 A and 0.5).
 //   time <list-file> <seconds> [options]
 //       Evaluates energy + forces (evalRestrainedMMGB) over the systems named in <list-file>
 //       (one "prmtop inpcrd" pair per line) round-robin until <seconds> of wall time pass, and
@@ -21,6 +22,9 @@
 // Options: --igb {0,1,2,5,7,8} (default 5 = OBC-II), --diel X (80), --salt X (0),
 //          --qtol X --qdisc X (charge smoothing, STORMM defaults), --scee X --scnb X,
 //          --quantize (round coordinates to the 2^-32 Angstrom fixed-point grid first).
+//          In eval mode, --clash-r0 X and --clash-ratio X add the clash-mitigated evaluation
+//          (softened Coulomb and Lennard-Jones cores, Potential/soft_core_potentials.tpp) of the
+//          MM driver as the records clash_frc_total and clash_energy_terms.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -68,6 +72,9 @@ struct Options {
   int ncyc = 0;
   int minimize_cycles = 0;
   double dx0 = 0.01;
+  int cdcyc = 0;
+  double clash_r0 = -1.0;
+  double clash_ratio = -1.0;
 };
 
 // Record file: for each record, int32 name length, name bytes, one dtype char ('d' double,
@@ -350,6 +357,17 @@ int runEval(const std::string &prmtop, const std::string &inpcrd, const std::str
   evalRestrainedMMGB(&ps, &sc_all, ag, ngb_tab, se, ra, EvaluateForce::YES, 0);
   putForces(&rw, "frc_total", psw);
   putScoreCard(&rw, "energy_terms_mm", sc_all);
+  if (opt.clash_r0 >= 0.0 || opt.clash_ratio >= 0.0) {
+    const double r0 = (opt.clash_r0 >= 0.0) ? opt.clash_r0 : 0.0;
+    const double ratio = (opt.clash_ratio >= 0.0) ? opt.clash_ratio : 0.0;
+    zeroForces(psw);
+    ScoreCard sc_clash(1, 1, 26);
+    evalRestrainedMMGB(&ps, &sc_clash, ag, ngb_tab, se, ra, EvaluateForce::YES, 0, 0, r0, ratio);
+    putForces(&rw, "clash_frc_total", psw);
+    putScoreCard(&rw, "clash_energy_terms", sc_clash);
+    rw.scalar("clash_r0", r0);
+    rw.scalar("clash_ratio", ratio);
+  }
   return 0;
 }
 
@@ -357,7 +375,13 @@ MinimizeControls minimizeControls(const Options &opt) {
   MinimizeControls mincon;
   mincon.setTotalCycles(opt.maxcyc);
   mincon.setSteepestDescentCycles(opt.ncyc);
-  mincon.setClashDampingCycles(0);
+  mincon.setClashDampingCycles(opt.cdcyc);
+  if (opt.clash_r0 >= 0.0) {
+    mincon.setAbsoluteClashDistance(opt.clash_r0);
+  }
+  if (opt.clash_ratio >= 0.0) {
+    mincon.setVdwClashRatio(opt.clash_ratio);
+  }
   mincon.setInitialStep(opt.dx0);
   mincon.setDiagnosticPrintFrequency(1);
   return mincon;
@@ -478,6 +502,9 @@ int main(int argc, char* argv[]) {
     else if (a == "--ncyc") opt.ncyc = static_cast<int>(next());
     else if (a == "--dx0") opt.dx0 = next();
     else if (a == "--minimize") opt.minimize_cycles = static_cast<int>(next());
+    else if (a == "--cdcyc") opt.cdcyc = static_cast<int>(next());
+    else if (a == "--clash-r0") opt.clash_r0 = next();
+    else if (a == "--clash-ratio") opt.clash_ratio = next();
     else if (a == "--quantize") opt.quantize = true;
     else pos.push_back(a);
   }

@@ -166,23 +166,78 @@ static double dihedral_term(const double* c, double* f, int i, int j, int k, int
   return amp * (1.0 + cos(sangle));
 }
 
-/* evalAttenuated14Pair (no clash softening), valence_potential.tpp:1288-1420 */
+/* ---------------------------------------------------------------------------------------------
+ * Softened cores for clash damping, Potential/soft_core_potentials.tpp:30-52 (quadratic
+ * Coulomb core below an absolute distance) and :140-180 (quartic Lennard-Jones core below a
+ * ratio of the pair's sigma = (A/B)^(1/6), zero where B <= 1e-6).  Each adds the pair's energy
+ * to *e and its force factor (force = fmag * displacement) to *fmag.
+ * ------------------------------------------------------------------------------------------- */
+static const double SOFT_CORE_TINY = 1.0e-10;
+
+static void quadratic_core_coulomb(double r, double cd, double qiqj, double* e, double* fmag) {
+  if (r < cd) {
+    const double a = -0.5 / (cd * cd * (cd + 1.0));
+    const double b = 1.0 / cd - a * (cd + 1.0) * (cd + 1.0);
+    *e += qiqj * (a * (r + 1.0) * (r + 1.0) + b);
+    if (r > SOFT_CORE_TINY) *fmag += qiqj * (2.0 * a + 2.0 * a / r);
+  }
+  else {
+    const double invr = 1.0 / r;
+    *e += qiqj * invr;
+    *fmag -= qiqj * invr * invr * invr;
+  }
+}
+
+static void quartic_core_lj(double r, double ratio, double lja, double ljb, double* e,
+                            double* fmag) {
+  const double sigma = (ljb > 1.0e-6) ? sqrt(cbrt(lja / ljb)) : 0.0;
+  const double rl = ratio * sigma;
+  if (r < rl) {
+    const double il = 1.0 / rl;
+    const double il6 = il * il * il * il * il * il;
+    const double a = ((6.0 * ljb - 12.0 * lja * il6) * il * il6) /
+                     ((((4.0 * rl + 12.0) * rl + 12.0) * rl) + 4.0);
+    const double rlp = rl + 1.0;
+    const double b = (lja * il6 - ljb) * il6 - a * rlp * rlp * rlp * rlp;
+    const double rp = r + 1.0;
+    const double a3 = a * rp * rp * rp;
+    *e += a3 * rp + b;
+    if (r > SOFT_CORE_TINY) *fmag += 4.0 * a3 / r;
+  }
+  else {
+    const double invr2 = 1.0 / (r * r);
+    const double invr4 = invr2 * invr2;
+    *e += lja * invr4 * invr4 * invr4 - ljb * invr4 * invr2;
+    *fmag += (6.0 * ljb - 12.0 * lja * invr4 * invr2) * invr4 * invr4;
+  }
+}
+
+/* evalAttenuated14Pair, valence_potential.tpp:1288-1420; clash softening when cd > 0 or
+ * ratio > 0 */
 static void pair14_term(const orc_system* s, const double* c, double* f, int i, int l,
-                        double scee, double scnb, double* e_elec, double* e_vdw) {
+                        double scee, double scnb, double cd, double ratio, double* e_elec,
+                        double* e_vdw) {
   double d[3];
   for (int a = 0; a < 3; a++) d[a] = c[3 * l + a] - c[3 * i + a];
   const int t = s->lj_idx[i] * s->n_lj_types + s->lj_idx[l];
   const double lja = s->lja14[t] / scnb;
   const double ljb = s->ljb14[t] / scnb;
   const double qiqj = s->coulomb_constant * s->charge[i] * s->charge[l] / scee;
-  const double invr2 = 1.0 / dot3(d, d);
-  const double invr = sqrt(invr2);
-  const double invr4 = invr2 * invr2;
-  *e_elec += qiqj * invr;
-  *e_vdw += lja * invr4 * invr4 * invr4 - ljb * invr4 * invr2;
+  double fmag = 0.0;
+  if (cd > 0.0 || ratio > 0.0) {
+    const double r = sqrt(dot3(d, d));
+    quadratic_core_coulomb(r, cd, qiqj, e_elec, &fmag);
+    quartic_core_lj(r, ratio, lja, ljb, e_vdw, &fmag);
+  }
+  else {
+    const double invr2 = 1.0 / dot3(d, d);
+    const double invr = sqrt(invr2);
+    const double invr4 = invr2 * invr2;
+    *e_elec += qiqj * invr;
+    *e_vdw += lja * invr4 * invr4 * invr4 - ljb * invr4 * invr2;
+    fmag = -(qiqj * invr * invr2) + (6.0 * ljb - 12.0 * lja * invr4 * invr2) * invr4 * invr4;
+  }
   if (f) {
-    const double fmag = -(qiqj * invr * invr2) +
-                        (6.0 * ljb - 12.0 * lja * invr4 * invr2) * invr4 * invr4;
     for (int a = 0; a < 3; a++) {
       f[3 * i + a] += fmag * d[a];
       f[3 * l + a] -= fmag * d[a];
@@ -193,8 +248,9 @@ static void pair14_term(const orc_system* s, const double* c, double* f, int i, 
 /* ---------------------------------------------------------------------------------------------
  * Coulomb + Lennard-Jones over non-excluded pairs, nonbonded_potential.tpp:8-425
  * ------------------------------------------------------------------------------------------- */
-static void nonbonded_terms(const orc_system* s, const double* c, double* f, double* e_elec,
-                            double* e_vdw) {
+static void nonbonded_terms(const orc_system* s, const double* c, double* f, double cd,
+                            double ratio, double* e_elec, double* e_vdw) {
+  const int soft = (cd > 0.0 || ratio > 0.0);
   const int n = s->natom;
   char* excl = (char*)calloc((size_t)n, 1);
   for (int i = 0; i < n; i++) {
@@ -214,6 +270,20 @@ static void nonbonded_terms(const orc_system* s, const double* c, double* f, dou
       const int t = s->lj_idx[j] * s->n_lj_types + ti;
       const double lja = s->lja[t];
       const double ljb = s->ljb[t];
+      if (soft) {
+        /* clash-mitigated loops, nonbonded_potential.tpp:108-175 */
+        const double r = sqrt(dot3(d, d));
+        double fmag = 0.0;
+        quadratic_core_coulomb(r, cd, qiqj, e_elec, &fmag);
+        quartic_core_lj(r, ratio, lja, ljb, e_vdw, &fmag);
+        if (f) {
+          for (int a = 0; a < 3; a++) {
+            f[3 * i + a] += fmag * d[a];
+            f[3 * j + a] -= fmag * d[a];
+          }
+        }
+        continue;
+      }
       *e_elec += qiqj * invr;
       *e_vdw += (lja * invr4 * invr4 - ljb * invr2) * invr4;
       if (f) {
@@ -421,6 +491,12 @@ static void gb_terms(const orc_system* s, const double* c, double* f, double* e_
 
 void orc_evaluate(const orc_system* s, const double* coords, double* forces, double* energies,
                   double* psi, double* radii, double* sumdeijda, int terms) {
+  orc_evaluate_clash(s, coords, forces, energies, psi, radii, sumdeijda, terms, 0.0, 0.0);
+}
+
+void orc_evaluate_clash(const orc_system* s, const double* coords, double* forces,
+                        double* energies, double* psi, double* radii, double* sumdeijda,
+                        int terms, double clash_distance, double clash_ratio) {
   for (int t = 0; t < ORC_NTERMS; t++) energies[t] = 0.0;
   if (forces) memset(forces, 0, (size_t)s->natom * 3 * sizeof(double));
   if (terms & 1) {
@@ -440,12 +516,14 @@ void orc_evaluate(const orc_system* s, const double* coords, double* forces, dou
                                                           ORC_PROPER_DIHEDRAL] += e;
       if (s->dihe_scee[t] > 0.0) {
         pair14_term(s, coords, forces, s->dihe_i[t], s->dihe_l[t], s->dihe_scee[t],
-                    s->dihe_scnb[t], &energies[ORC_ELEC_ONE_FOUR], &energies[ORC_VDW_ONE_FOUR]);
+                    s->dihe_scnb[t], clash_distance, clash_ratio, &energies[ORC_ELEC_ONE_FOUR],
+                    &energies[ORC_VDW_ONE_FOUR]);
       }
     }
   }
   if (terms & 2) {
-    nonbonded_terms(s, coords, forces, &energies[ORC_ELECTROSTATIC], &energies[ORC_VDW]);
+    nonbonded_terms(s, coords, forces, clash_distance, clash_ratio, &energies[ORC_ELECTROSTATIC],
+                    &energies[ORC_VDW]);
   }
   if ((terms & 4) && s->igb != ORC_GB_NONE) {
     gb_terms(s, coords, forces, &energies[ORC_GENERALIZED_BORN], psi, radii, sumdeijda);
@@ -502,6 +580,12 @@ void orc_minimize(const orc_system* s, double* coords, int maxcyc, int sd_cycles
 
 void orc_minimize_ex(const orc_system* s, double* coords, int maxcyc, int sd_cycles, double dx0,
                      double drms, double* history, int* cycles_run) {
+  orc_minimize_clash(s, coords, maxcyc, sd_cycles, dx0, drms, 0, 0.0, 0.0, history, cycles_run);
+}
+
+void orc_minimize_clash(const orc_system* s, double* coords, int maxcyc, int sd_cycles,
+                        double dx0, double drms, int clash_cycles, double clash_distance,
+                        double clash_ratio, double* history, int* cycles_run) {
   const int n = s->natom;
   const size_t nb = (size_t)n * 3 * sizeof(double);
   double* frc = (double*)malloc(nb);
@@ -512,8 +596,16 @@ void orc_minimize_ex(const orc_system* s, double* coords, int maxcyc, int sd_cyc
   double l_move = dx0;
   int done_at = maxcyc;
   for (int cyc = 0; cyc < maxcyc; cyc++) {
+    /* clash damping for the first clash_cycles cycles, the softened cores shrinking linearly
+     * (minimization.tpp:224-228, hpc_minimization.cu:268-272) */
+    double cd = 0.0, cr = 0.0;
+    if (cyc < clash_cycles) {
+      const double progress = (double)(clash_cycles - cyc) / (double)clash_cycles;
+      cd = clash_distance * progress;
+      cr = clash_ratio * progress;
+    }
     /* force + energy evaluation at the start of the cycle */
-    orc_evaluate(s, coords, frc, e, NULL, NULL, NULL, 7);
+    orc_evaluate_clash(s, coords, frc, e, NULL, NULL, NULL, 7, cd, cr);
     const double e0 = total_energy(e);
     if (history) history[cyc] = e0;
     if (drms > 0.0) {
@@ -566,7 +658,7 @@ void orc_minimize_ex(const orc_system* s, double* coords, int maxcyc, int sd_cyc
       for (int k = 0; k < 3 * n; k++) coords[k] += dir[k] * mfac * s_move;
       cum += mfac;
       mv[mvn + 1] = cum;
-      orc_evaluate(s, coords, NULL, e, NULL, NULL, NULL, 7);
+      orc_evaluate_clash(s, coords, NULL, e, NULL, NULL, NULL, 7, cd, cr);
       ev[mvn + 1] = total_energy(e);
     }
 

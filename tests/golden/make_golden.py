@@ -19,6 +19,10 @@ Fixtures written (numpy .npz, one per case):
   78.5; HCT; OBC-I with dielectric 40; vacuum), run with ``--variants-only`` on its own.
 * ``minimize_m0.npz``: STORMM's CPU line minimizer (MolecularMechanics/minimization.tpp) on the
   64-atom molecule, energy history and final coordinates.
+* ``synthetic_K64.npz`` and ``minimize_clash_k64.npz`` (``--clash-only``): a 64-atom molecule
+  with close contacts (0.45 A start noise), its clash-mitigated evaluation (softened cores below
+  1.5 A and below 0.9 of the pair's sigma) beside the plain one, and a minimization whose first
+  25 cycles are clash-damped.
 """
 from __future__ import annotations
 
@@ -90,10 +94,25 @@ def main():
     ap.add_argument("--reference-root", default="/root/reference")
     ap.add_argument("--variants-only", action="store_true",
                     help="write only the solvent-model variant fixtures")
+    ap.add_argument("--clash-only", action="store_true",
+                    help="write only the clash-damping fixtures")
     args = ap.parse_args()
     if not os.path.exists(DRIVER):
         raise SystemExit("build the reference driver first: make -C oracle/ref -j8")
     with tempfile.TemporaryDirectory() as tmp:
+        if args.clash_only:
+            mol = synthetic.make_molecule(8810, 64, noise=0.45, name="K64")
+            rec, top, crd = eval_molecule(mol, tmp, ["--clash-r0", "1.5", "--clash-ratio", "0.9"])
+            np.savez_compressed(os.path.join(HERE, "synthetic_K64.npz"), **rec)
+            print("wrote K64", rec["energy_terms_mm"], rec["clash_energy_terms"])
+            out = os.path.join(tmp, "k64_min.bin")
+            run_driver(["minimize", top, crd, out, "--quantize", "--maxcyc", "60", "--ncyc", "20",
+                        "--cdcyc", "25", "--clash-r0", "1.0", "--clash-ratio", "0.9"])
+            mrec = read_records(out)
+            np.savez_compressed(os.path.join(HERE, "minimize_clash_k64.npz"), maxcyc=60, ncyc=20,
+                                cdcyc=25, clash_r0=1.0, clash_ratio=0.9, **mrec)
+            print("wrote minimize_clash_k64", mrec["min_potential_history"][[0, 24, 25, -1]])
+            return
         # 0. solvent-model variants of synthetic molecules: salt (Debye-Hueckel kappa) with a
         #    different dielectric, HCT, OBC-I and vacuum
         variants = (("S64", 8800, 64, ["--salt", "0.15", "--diel", "78.5"]),
