@@ -23,6 +23,7 @@
  *   sb_launch_nonbonded      launchNonbonded (Potential/hpc_nonbonded_potential.h:142-157)
  *   sb_launch_valence        launchValence (Potential/hpc_valence_potential.h:167-230)
  *   sb_evaluate              launchNonbonded followed by launchValence, fused into one pass
+ *   sb_evaluate_clash        the same with the clash_min_dist / clash_ratio arguments
  *   sb_minimize              launchMinimization (MolecularMechanics/hpc_minimization.h:122-152)
  */
 #ifndef STORMM_B200_H
@@ -189,6 +190,14 @@ int sb_evaluate_range(sb_synthesis* syn, int first, int count, int terms, int ev
 /* STORMM's two launchers, each alone */
 int sb_launch_nonbonded(sb_synthesis* syn, int eval_force, int eval_energy, void* stream);
 int sb_launch_valence(sb_synthesis* syn, int eval_force, int eval_energy, void* stream);
+/* sb_evaluate with clash mitigation, the clash_min_dist / clash_ratio arguments of
+ * launchNonbonded and launchValence (hpc_nonbonded_potential.h:142-157,
+ * hpc_valence_potential.h:167-230): Coulomb and Lennard-Jones pairs, 1-4 pairs included, take
+ * a quadratic Coulomb core below clash_distance (A) and a quartic Lennard-Jones core below
+ * clash_ratio times the pair's sigma = (A/B)^(1/6) (Potential/soft_core_potentials.tpp).  Both
+ * zero is the plain evaluation; GB terms are never softened. */
+int sb_evaluate_clash(sb_synthesis* syn, int terms, int eval_force, int eval_energy,
+                      double clash_distance, double clash_ratio, void* stream);
 
 /* Number of work units the batched launches use, and the launch shape chosen */
 int sb_launch_info(const sb_synthesis* syn, int* work_units, int* blocks, int* threads);
@@ -201,7 +210,8 @@ int sb_launch_info(const sb_synthesis* syn, int* work_units, int* blocks, int* t
 typedef struct {
   int total_cycles;            /* maxcyc: line-minimization cycles (STORMM default 200) */
   int sd_cycles;               /* ncyc: steepest-descent cycles before conjugate gradient (50) */
-  int clash_cycles;            /* cdcyc: must be 0 (softened-core cycles are not provided) */
+  int clash_cycles;            /* cdcyc: leading cycles evaluated with softened cores (STORMM's
+                                  namelist default is 25; 0 here) */
   double initial_step;         /* dx0: first move length, A (0.01) */
   double convergence_rms;      /* a system stops once its RMS force (kcal/mol/A, over 3N
                                   components) is at or below this; 0: run every cycle, as
@@ -209,6 +219,11 @@ typedef struct {
   int record_history;          /* nonzero: keep each system's energy at the start of every cycle
                                   and the final energy (total_cycles + 1 values per system) */
   int kernel;                  /* SB_MIN_GRAPH (default) or SB_MIN_PERSISTENT */
+  double clash_distance;       /* clash_r0: softened-core distance in cycle 0 (0.2 A) */
+  double clash_ratio;          /* clash_vdw_ratio: softened-core sigma ratio in cycle 0 (0.5);
+                                  cycle c < clash_cycles uses both scaled by
+                                  (clash_cycles - c) / clash_cycles, counted per system, and the
+                                  final energy is undamped (hpc_minimization.cu:266-279) */
 } sb_minimize_controls;
 
 /* How a minimization runs.  Both follow the same algorithm; their FP32 evaluations are separate

@@ -60,7 +60,8 @@ class MinimizeControls(ctypes.Structure):
         ("total_cycles", ctypes.c_int), ("sd_cycles", ctypes.c_int),
         ("clash_cycles", ctypes.c_int), ("initial_step", ctypes.c_double),
         ("convergence_rms", ctypes.c_double), ("record_history", ctypes.c_int),
-        ("kernel", ctypes.c_int),
+        ("kernel", ctypes.c_int), ("clash_distance", ctypes.c_double),
+        ("clash_ratio", ctypes.c_double),
     ]
 
 
@@ -126,6 +127,8 @@ def library() -> ctypes.CDLL:
             "sb_evaluate": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]),
             "sb_evaluate_range": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                  ctypes.c_int, ctypes.c_int, vp]),
+            "sb_evaluate_clash": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.c_double, ctypes.c_double, vp]),
             "sb_launch_nonbonded": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, vp]),
             "sb_launch_valence": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, vp]),
             "sb_launch_info": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int),
@@ -265,8 +268,9 @@ def static_exclusion_mask(molecule):
 
 
 def minimize_controls(**overrides) -> MinimizeControls:
-    """STORMM's minimizer defaults (maxcyc 200, ncyc 50, dx0 0.01, no clash damping) with
-    overrides by field name."""
+    """STORMM's minimizer defaults (maxcyc 200, ncyc 50, dx0 0.01; no clash-damped cycles,
+    softened cores of 0.2 A and 0.5 sigma when clash_cycles is set) with overrides by field
+    name."""
     c = MinimizeControls()
     library().sb_default_minimize_controls(ctypes.byref(c))
     for k, v in overrides.items():
@@ -372,6 +376,13 @@ class Synthesis:
                        stream=None):
         _check(library().sb_evaluate_range(self.handle, first, count, terms, int(force),
                                            int(energy), stream), "sb_evaluate_range")
+
+    def evaluate_clash(self, clash_distance, clash_ratio, terms=TERM_ALL, force=True,
+                       energy=True, stream=None):
+        """evaluate() with softened Coulomb / Lennard-Jones cores (sb_evaluate_clash)."""
+        _check(library().sb_evaluate_clash(self.handle, terms, int(force), int(energy),
+                                           float(clash_distance), float(clash_ratio), stream),
+               "sb_evaluate_clash")
 
     def launch_nonbonded(self, force=True, energy=True, stream=None):
         _check(library().sb_launch_nonbonded(self.handle, int(force), int(energy), stream),

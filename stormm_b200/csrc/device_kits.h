@@ -113,6 +113,15 @@ struct DevSynthesis {
   // from the base in its closing unit_meta row
   float2* pair_deriv;
 
+  // clash damping of a launch (softened Coulomb and Lennard-Jones cores): clash distance (A) and
+  // sigma ratio, off when both are 0.  With clash_cycle set (a minimization), system s uses them
+  // scaled by (clash_cycles - c) / clash_cycles in its cycle c = clash_cycle[s], and not at all
+  // once c >= clash_cycles.
+  float clash_distance;
+  float clash_ratio;
+  int clash_cycles;
+  const int* clash_cycle;
+
   int* status;                   // device status word (0 = fine)
 };
 
@@ -154,6 +163,9 @@ struct DevMinimizer {
   int sd_cycles;                 // steepest-descent cycles before conjugate gradient
   int max_cycles;                // a system stops moving after this many cycles in total
   double drms;                   // RMS force target (kcal/mol/A), 0: none
+  int clash_cycles;              // leading cycles with softened cores (0: none)
+  float clash_distance;          // their clash distance (A) and sigma ratio in cycle 0
+  float clash_ratio;
   int* queue;                    // work-unit counter, zero before each launch
   double* line;                  // per system: kLineFields line-search scalars (graph minimizer)
 };

@@ -11,7 +11,8 @@
 //               (Potential/nonbonded_potential.tpp:511-728)
 //   radii       effective radii, GB self energy and its dE/dR (nonbonded_potential.tpp:730-805)
 //   pass 2      Coulomb + Lennard-Jones on non-excluded pairs, GB pair energy and force, dE/dR
-//               sums (nonbonded_potential.tpp:8-425, 808-975)
+//               sums (nonbonded_potential.tpp:8-425, 808-975); with CLASH, softened cores
+//               (soft_core_potentials.tpp) for molecules given a clash distance or ratio
 //   chain rule  OBC prefactor on dE/dR (nonbonded_potential.tpp:982-1021)
 //   pass 3      radius chain-rule forces (nonbonded_potential.tpp:1022-1290)
 //   commit      forces into the int64 + int32-overflow arrays, energies into per-system slots
@@ -37,7 +38,7 @@ size_t fusedSmemBytes(int max_slots, int max_lj) { return unitSmemBytes(max_slot
 // ------------------------------------------------------------------------------------------------
 // The fused kernel: stage, evaluate, commit, one work unit at a time
 // ------------------------------------------------------------------------------------------------
-template <bool FORCE, bool ENERGY, int TERMS>
+template <bool FORCE, bool ENERGY, int TERMS, bool CLASH>
 __global__ void __launch_bounds__(256, 4)
 kEvalFused(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
   extern __shared__ __align__(16) char smem_raw[];
@@ -50,6 +51,12 @@ kEvalFused(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
     for (int e = threadIdx.x; e < us.nsys * kNrgStride; e += blockDim.x) {
       s.nrg[e] = 0ull;
     }
+    if (CLASH) {
+      for (int k = threadIdx.x; k < us.nsys; k += blockDim.x) {
+        const int cycle = (d.clash_cycle != nullptr) ? d.clash_cycle[s.sys[k]] : -1;
+        s.clash[k] = clashScaled(d.clash_distance, d.clash_ratio, d.clash_cycles, cycle);
+      }
+    }
     // stage atoms (a warp's 32 consecutive slots always belong to one molecule)
     for (int slot = threadIdx.x; slot < us.nslots; slot += blockDim.x) {
       const int k = findOwner(s.slot0, us.nsys, slot);
@@ -61,7 +68,7 @@ kEvalFused(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
                 real ? d.zcrd[gi] : 0ll);
     }
     __syncthreads();
-    evaluateStaged<FORCE, ENERGY, TERMS, true>(d, s, us, BlockTeam());
+    evaluateStaged<FORCE, ENERGY, TERMS, true, CLASH>(d, s, us, BlockTeam());
 
     // commit forces (each atom belongs to exactly one unit) and energies
     if (FORCE) {
@@ -90,11 +97,13 @@ kEvalFused(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
 // Host-side launcher (called from the C++ layer)
 cudaError_t launchEvalFused(const DevSynthesis &d, int unit_begin, int unit_end, int max_lj,
                             int terms, bool force, bool energy, int blocks, int threads,
-                            cudaStream_t stream) {
+                            cudaStream_t stream, bool clash) {
   const size_t smem = fusedSmemBytes(d.max_unit_slots, max_lj);
+  // softened cores change only Coulomb, Lennard-Jones and 1-4 terms
+  clash = clash && (terms & 3) != 0;
 #define SB_LAUNCH(F, E, T)                                                                      \
   {                                                                                             \
-    auto kern = kEvalFused<F, E, T>;                                                            \
+    auto kern = clash ? kEvalFused<F, E, T, ((T) & 3) != 0> : kEvalFused<F, E, T, false>;      \
     cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
                                            static_cast<int>(smem));                             \
     if (err != cudaSuccess) return err;                                                         \

@@ -130,8 +130,9 @@ __device__ void moveUnit(const DevSynthesis &d, const DevMinimizer &m, const Uni
   }
 }
 
-// One line-minimization cycle of every unit molecule that has not converged
-template <bool HIST, class Team>
+// One line-minimization cycle of every unit molecule that has not converged; with CLASH, the
+// four evaluations of a molecule still within m.clash_cycles use softened cores
+template <bool HIST, bool CLASH, class Team>
 __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
                                   const UnitSmem &s, const MinSmem &ms, const UnitShape &us,
                                   const Team &team) {
@@ -139,9 +140,13 @@ __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
   const double inv_fs = 1.0 / static_cast<double>(d.frc_scale);
   const double gpos_scale = 1.0 / d.inv_gpos_scale;
 
-  // 1. forces and energy at the line start
+  // 1. forces and energy at the line start (placeUnit ends with the barrier after s.clash)
+  if (CLASH && team.rank() < us.nsys) {
+    const int k = team.rank();
+    s.clash[k] = clashScaled(m.clash_distance, m.clash_ratio, m.clash_cycles, ms.cyc[k]);
+  }
   placeUnit(d, m, s, us, team);
-  evaluateStaged<true, true, 7, false>(d, s, us, team);
+  evaluateStaged<true, true, 7, false, CLASH>(d, s, us, team);
 
   // 2. gg, dgg and |f|^2 per 32-slot chunk (a chunk never straddles two molecules)
   for (int slot = team.rank(); slot < us.nslots; slot += team.size()) {
@@ -252,7 +257,7 @@ __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
   team.sync();
   moveUnit(d, m, s, ms, us, team);
   placeUnit(d, m, s, us, team);
-  evaluateStaged<false, true, 7, false>(d, s, us, team);
+  evaluateStaged<false, true, 7, false, CLASH>(d, s, us, team);
 
   // second trial move: 1.04 x after a decrease, else 0.8 x
   if (team.rank() < us.nsys) {
@@ -270,7 +275,7 @@ __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
   team.sync();
   moveUnit(d, m, s, ms, us, team);
   placeUnit(d, m, s, us, team);
-  evaluateStaged<false, true, 7, false>(d, s, us, team);
+  evaluateStaged<false, true, 7, false, CLASH>(d, s, us, team);
 
   // third trial move: the last factor x 1.03 after a decrease, else x 0.85
   if (team.rank() < us.nsys) {
@@ -288,7 +293,7 @@ __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
   team.sync();
   moveUnit(d, m, s, ms, us, team);
   placeUnit(d, m, s, us, team);
-  evaluateStaged<false, true, 7, false>(d, s, us, team);
+  evaluateStaged<false, true, 7, false, CLASH>(d, s, us, team);
 
   // 4. cubic fit and final placement
   if (team.rank() < us.nsys) {
@@ -315,8 +320,8 @@ __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
   team.sync();
 }
 
-// Every cycle of one work unit, then its final energies and state
-template <bool HIST, class Team>
+// Every cycle of one work unit, then its final energies (undamped) and state
+template <bool HIST, bool CLASH, class Team>
 __device__ void minimizeUnit(const DevSynthesis &d, const DevMinimizer &m, const UnitSmem &s,
                              const MinSmem &ms, int u, int max_lj, int max_sys, int cycles,
                              int final_energy, const Team &team) {
@@ -346,7 +351,7 @@ __device__ void minimizeUnit(const DevSynthesis &d, const DevMinimizer &m, const
     if (!team.any(moving != 0)) {
       break;
     }
-    minimizationCycle<HIST>(d, m, s, ms, us, team);
+    minimizationCycle<HIST, CLASH>(d, m, s, ms, us, team);
   }
   if (final_energy) {
     // one more energy evaluation at the final coordinates (hpc_minimization.cu:372-383)
@@ -376,7 +381,7 @@ __device__ void minimizeUnit(const DevSynthesis &d, const DevMinimizer &m, const
 // One thread block per work unit (molecules of up to 2,048 atoms).  The minimizer keeps more
 // state live than a single evaluation; two blocks per SM with up to 128 registers a thread run
 // faster than four with 64, where the pair loops spill.
-template <bool HIST>
+template <bool HIST, bool CLASH>
 __global__ void __launch_bounds__(256, 2)
 kMinimize(const DevSynthesis d, const DevMinimizer m, int unit_begin, int unit_end, int max_lj,
           int cycles, int final_energy) {
@@ -388,7 +393,8 @@ kMinimize(const DevSynthesis d, const DevMinimizer m, int unit_begin, int unit_e
   const BlockTeam team;
   int u = unit_begin + blockIdx.x;
   while (u < unit_end) {
-    minimizeUnit<HIST>(d, m, s, ms, u, max_lj, kMaxUnitSystems, cycles, final_energy, team);
+    minimizeUnit<HIST, CLASH>(d, m, s, ms, u, max_lj, kMaxUnitSystems, cycles, final_energy,
+                              team);
     if (threadIdx.x == 0) {
       next_unit = unit_begin + static_cast<int>(gridDim.x) + atomicAdd(m.queue, 1);
     }
@@ -440,7 +446,9 @@ cudaError_t launchMinimize(const DevSynthesis &d, const DevMinimizer &m, int uni
     return cudaSuccess;
   }
   const size_t smem = minimizeSmemBytes(d.max_unit_slots, max_lj);
-  auto kern = (m.history != nullptr) ? kMinimize<true> : kMinimize<false>;
+  const bool clash = m.clash_cycles > 0 && (m.clash_distance > 0.0f || m.clash_ratio > 0.0f);
+  auto kern = (m.history != nullptr) ? (clash ? kMinimize<true, true> : kMinimize<true, false>) :
+                                       (clash ? kMinimize<false, true> : kMinimize<false, false>);
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
   if (err != cudaSuccess) return err;

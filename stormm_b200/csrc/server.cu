@@ -171,9 +171,6 @@ public:
       throw Error(SB_ERR_ARGUMENT, "server budget, batch limits and cycles per launch must be "
                   "positive");
     }
-    if (o.controls.clash_cycles != 0) {
-      throw Error(SB_ERR_UNSUPPORTED, "clash-damping cycles are not provided; set them to 0");
-    }
     int ndev = 0;
     cudaCheck(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
     if (o.options.device < 0 || o.options.device >= ndev) {

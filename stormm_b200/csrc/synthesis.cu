@@ -24,7 +24,7 @@ namespace sb {
 size_t fusedSmemBytes(int max_slots, int max_lj);
 cudaError_t launchEvalFused(const DevSynthesis &d, int unit_begin, int unit_end, int max_lj,
                             int terms, bool force, bool energy, int blocks, int threads,
-                            cudaStream_t stream);
+                            cudaStream_t stream, bool clash);
 size_t minimizeSmemBytes(int max_slots, int max_lj);
 cudaError_t launchMinimizerReset(const DevMinimizer &m, const DevSynthesis &d, double dx0,
                                  cudaStream_t stream);
@@ -36,7 +36,7 @@ cudaError_t launchLineStep(const DevSynthesis &d, const DevMinimizer &m, int fir
 cudaError_t launchTiled(const DevSynthesis &d, const DevTiled &t, const int* h_tile_prefix,
                         const int* h_atom_prefix, int mol_begin, int mol_end, int terms,
                         bool force, bool energy, bool workspace, int sm_count,
-                        cudaStream_t stream);
+                        cudaStream_t stream, bool clash);
 cudaError_t launchImportCoordinates(const double* d_xyz, const int* d_map, int natom,
                                     double scale, long long* xcrd, long long* ycrd,
                                     long long* zcrd, int* xo, int* yo, int* zo, int* status,
@@ -639,46 +639,65 @@ void Synthesis::upload() {
 }
 
 void Synthesis::launchPlan(const UnitPlan &plan, int terms, bool force, bool energy,
-                           cudaStream_t stream) {
+                           cudaStream_t stream, const Clash &clash) {
   const int nunit = plan.units.size();
   DevSynthesis d = dev;
   d.nunit = nunit;
   d.unit_desc = plan.d_units.p;
   d.unit_meta = plan.d_meta.p;
+  clash.apply(&d);
   if (plan.n_big > 0) {
     d.max_unit_slots = plan.big_slots;
     cudaCheck(launchEvalFused(d, 0, plan.n_big, plan.big_lj, terms, force, energy, plan.n_big,
-                              threads, stream), "fused evaluation launch (large molecules)");
+                              threads, stream, clash.on()),
+              "fused evaluation launch (large molecules)");
   }
   if (nunit > plan.n_big) {
     d.max_unit_slots = plan.small_slots;
     cudaCheck(launchEvalFused(d, plan.n_big, nunit, plan.small_lj, terms, force, energy,
-                              nunit - plan.n_big, threads, stream), "fused evaluation launch");
+                              nunit - plan.n_big, threads, stream, clash.on()),
+              "fused evaluation launch");
   }
 }
 
-void Synthesis::evaluate(int terms, bool force, bool energy, cudaStream_t stream) {
+void Synthesis::evaluate(int terms, bool force, bool energy, cudaStream_t stream,
+                         const Clash &clash) {
   if (terms <= 0 || terms > SB_TERM_ALL) {
     throw Error(SB_ERR_ARGUMENT, "terms must be a nonzero mask of SB_TERM_*");
   }
   if (!force && !energy) {
     return;
   }
-  launchPlan(*eval_plan, terms, force, energy, stream);
-  launchTiledRange(0, static_cast<int>(h_tiled_systems.size()), terms, force, energy, stream);
+  launchPlan(*eval_plan, terms, force, energy, stream, clash);
+  launchTiledRange(0, static_cast<int>(h_tiled_systems.size()), terms, force, energy, stream,
+                   clash);
 }
 
 void Synthesis::launchTiledRange(int mol_begin, int mol_end, int terms, bool force, bool energy,
-                                 cudaStream_t stream) {
+                                 cudaStream_t stream, const Clash &clash) {
   if (mol_end <= mol_begin) {
     return;
   }
   const size_t np = natom_padded;
   cudaCheck(cudaMemsetAsync(d_tiled_psi.p, 0, np * sizeof(long long), stream), "memset");
   cudaCheck(cudaMemsetAsync(d_tiled_de.p, 0, np * sizeof(long long), stream), "memset");
-  cudaCheck(launchTiled(dev, dev_tiled, h_tile_prefix.data(), h_atom_prefix.data(), mol_begin,
-                        mol_end, terms, force, energy, true, sm_count, stream),
+  DevSynthesis d = dev;
+  clash.apply(&d);
+  cudaCheck(launchTiled(d, dev_tiled, h_tile_prefix.data(), h_atom_prefix.data(), mol_begin,
+                        mol_end, terms, force, energy, true, sm_count, stream, clash.on()),
             "tiled evaluation launch");
+}
+
+// The clash damping of the current minimization's evaluations: per system by its cycle count
+Clash Synthesis::minimizerClash() const {
+  Clash c;
+  if (dev_min.clash_cycles > 0) {
+    c.distance = dev_min.clash_distance;
+    c.ratio = dev_min.clash_ratio;
+    c.cycles = dev_min.clash_cycles;
+    c.cycle = dev_min.cycle;
+  }
+  return c;
 }
 
 void Synthesis::rejectTiledMinimization() const {
@@ -689,7 +708,7 @@ void Synthesis::rejectTiledMinimization() const {
 }
 
 void Synthesis::evaluateRange(int first, int count, int terms, bool force, bool energy,
-                              cudaStream_t stream) {
+                              cudaStream_t stream, const Clash &clash) {
   if (first < 0 || count < 0 || first + count > nsys) {
     throw Error(SB_ERR_ARGUMENT, "system range out of bounds");
   }
@@ -704,12 +723,14 @@ void Synthesis::evaluateRange(int first, int count, int terms, bool force, bool 
   d.unit_meta = single_plan->d_meta.p;
   d.nunit = nsys;
   d.max_unit_slots = single_slots;
+  clash.apply(&d);
   for (int s = first; s < first + count; s++) {
     if (tiled_index[s] >= 0) {
-      launchTiledRange(tiled_index[s], tiled_index[s] + 1, terms, force, energy, stream);
+      launchTiledRange(tiled_index[s], tiled_index[s] + 1, terms, force, energy, stream, clash);
       continue;
     }
-    cudaCheck(launchEvalFused(d, s, s + 1, single_lj, terms, force, energy, 1, threads, stream),
+    cudaCheck(launchEvalFused(d, s, s + 1, single_lj, terms, force, energy, 1, threads, stream,
+                              clash.on()),
               "per-system evaluation launch");
   }
 }
@@ -840,9 +861,9 @@ void Synthesis::minimizeBegin(const sb_minimize_controls &ctl, cudaStream_t stre
   if (ctl.total_cycles < 0 || ctl.sd_cycles < 0) {
     throw Error(SB_ERR_ARGUMENT, "cycle counts must not be negative");
   }
-  if (ctl.clash_cycles != 0) {
-    throw Error(SB_ERR_UNSUPPORTED, "clash-damping cycles (softened cores) are not provided; "
-                "set clash_cycles to 0");
+  if (ctl.clash_cycles < 0 || !(ctl.clash_distance >= 0.0) || !(ctl.clash_ratio >= 0.0) ||
+      !std::isfinite(ctl.clash_distance) || !std::isfinite(ctl.clash_ratio)) {
+    throw Error(SB_ERR_ARGUMENT, "clash-damping cycles, distance and ratio must not be negative");
   }
   if (!(ctl.initial_step > 0.0) || !(ctl.convergence_rms >= 0.0)) {
     throw Error(SB_ERR_ARGUMENT, "initial step must be positive and the RMS target not negative");
@@ -891,6 +912,11 @@ void Synthesis::minimizeBegin(const sb_minimize_controls &ctl, cudaStream_t stre
   m.sd_cycles = ctl.sd_cycles;
   m.max_cycles = ctl.total_cycles;
   m.drms = ctl.convergence_rms;
+  if (ctl.clash_cycles > 0 && (ctl.clash_distance > 0.0 || ctl.clash_ratio > 0.0)) {
+    m.clash_cycles = ctl.clash_cycles;
+    m.clash_distance = static_cast<float>(ctl.clash_distance);
+    m.clash_ratio = static_cast<float>(ctl.clash_ratio);
+  }
   m.queue = d_queue.p;
   m.line = d_line.p;
   if (ctl.kernel != SB_MIN_GRAPH && ctl.kernel != SB_MIN_PERSISTENT) {
@@ -913,9 +939,10 @@ Synthesis::~Synthesis() {
 
 // One batched evaluation of all systems (single = false) or of systems [first, first + count)
 // one launch each (single = true)
-void Synthesis::evaluateFor(int first, int count, bool single, bool force, cudaStream_t stream) {
+void Synthesis::evaluateFor(int first, int count, bool single, bool force, cudaStream_t stream,
+                            const Clash &clash) {
   if (!single) {
-    launchPlan(*eval_plan, SB_TERM_ALL, force, true, stream);
+    launchPlan(*eval_plan, SB_TERM_ALL, force, true, stream, clash);
     return;
   }
   DevSynthesis d = dev;
@@ -923,9 +950,10 @@ void Synthesis::evaluateFor(int first, int count, bool single, bool force, cudaS
   d.unit_meta = single_plan->d_meta.p;
   d.nunit = nsys;
   d.max_unit_slots = single_slots;
+  clash.apply(&d);
   for (int s = first; s < first + count; s++) {
     cudaCheck(launchEvalFused(d, s, s + 1, single_lj, SB_TERM_ALL, force, true, 1, threads,
-                              stream), "per-system evaluation launch");
+                              stream, clash.on()), "per-system evaluation launch");
   }
 }
 
@@ -933,12 +961,13 @@ void Synthesis::evaluateFor(int first, int count, bool single, bool force, cudaS
 // per system (line_search.cu)
 void Synthesis::graphCycle(int first, int count, bool single, cudaStream_t stream) {
   const size_t nrg_bytes = d_energies.n * sizeof(unsigned long long);
+  const Clash clash = minimizerClash();
   initialize(SB_INIT_FORCES | SB_INIT_ENERGIES, stream);
-  evaluateFor(first, count, single, true, stream);
+  evaluateFor(first, count, single, true, stream, clash);
   cudaCheck(launchLineStep(dev, dev_min, first, count, 0, stream), "line search launch");
   for (int step = 1; step <= 3; step++) {
     cudaCheck(cudaMemsetAsync(d_energies.p, 0, nrg_bytes, stream), "memset");
-    evaluateFor(first, count, single, false, stream);
+    evaluateFor(first, count, single, false, stream, clash);
     cudaCheck(launchLineStep(dev, dev_min, first, count, step, stream), "line search launch");
   }
 }
@@ -1339,6 +1368,20 @@ int sb_evaluate_range(sb_synthesis* syn, int first, int count, int terms, int ev
   });
 }
 
+int sb_evaluate_clash(sb_synthesis* syn, int terms, int eval_force, int eval_energy,
+                      double clash_distance, double clash_ratio, void* stream) {
+  return guarded([&]() {
+    if (!(clash_distance >= 0.0) || !(clash_ratio >= 0.0) || !std::isfinite(clash_distance) ||
+        !std::isfinite(clash_ratio)) {
+      throw sb::Error(SB_ERR_ARGUMENT, "clash distance and ratio must be finite, not negative");
+    }
+    sb::Clash clash;
+    clash.distance = static_cast<float>(clash_distance);
+    clash.ratio = static_cast<float>(clash_ratio);
+    need(syn)->evaluate(terms, eval_force != 0, eval_energy != 0, asStream(stream), clash);
+  });
+}
+
 int sb_launch_nonbonded(sb_synthesis* syn, int eval_force, int eval_energy, void* stream) {
   return guarded([&]() {
     need(syn)->evaluate(SB_TERM_NONBONDED | SB_TERM_GB, eval_force != 0, eval_energy != 0,
@@ -1374,6 +1417,8 @@ void sb_default_minimize_controls(sb_minimize_controls* ctl) {
   ctl->total_cycles = 200;
   ctl->sd_cycles = 50;
   ctl->clash_cycles = 0;
+  ctl->clash_distance = 0.2;
+  ctl->clash_ratio = 0.5;
   ctl->initial_step = 0.01;
   ctl->convergence_rms = 0.0;
   ctl->record_history = 0;

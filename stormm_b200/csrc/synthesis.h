@@ -107,14 +107,31 @@ struct UnitPlan {
   DeviceArray<int> d_meta;
 };
 
+// Softened-core (clash damping) setting of an evaluation: off when both distance and ratio are
+// zero; with cycle set, per system as DevSynthesis::clash_cycle describes
+struct Clash {
+  float distance = 0.0f;
+  float ratio = 0.0f;
+  int cycles = 0;
+  const int* cycle = nullptr;
+  bool on() const { return distance > 0.0f || ratio > 0.0f; }
+  void apply(DevSynthesis* d) const {
+    d->clash_distance = distance;
+    d->clash_ratio = ratio;
+    d->clash_cycles = cycles;
+    d->clash_cycle = cycle;
+  }
+};
+
 class Synthesis {
 public:
   Synthesis(const sb_topology* tops, int ntop, const int* topology_index, int nsys,
             const sb_options &options);
 
-  void evaluate(int terms, bool force, bool energy, cudaStream_t stream);
+  void evaluate(int terms, bool force, bool energy, cudaStream_t stream,
+                const Clash &clash = Clash());
   void evaluateRange(int first, int count, int terms, bool force, bool energy,
-                     cudaStream_t stream);
+                     cudaStream_t stream, const Clash &clash = Clash());
   void initialize(int what, cudaStream_t stream);
   void setCoordinates(const double* xyz, cudaStream_t stream);
   void getCoordinates(double* xyz, cudaStream_t stream);
@@ -210,14 +227,17 @@ private:
   void buildLayout(const sb_topology* tops, int ntop);
   std::unique_ptr<UnitPlan> makePlan(int max_slots_cap, int max_tiles_cap) const;
   void finalizePlan(UnitPlan* plan) const;
-  void launchPlan(const UnitPlan &plan, int terms, bool force, bool energy, cudaStream_t stream);
+  void launchPlan(const UnitPlan &plan, int terms, bool force, bool energy, cudaStream_t stream,
+                  const Clash &clash = Clash());
   void launchMinPlan(const UnitPlan &plan, int cycles, bool final_energy, cudaStream_t stream);
   void launchTiledRange(int mol_begin, int mol_end, int terms, bool force, bool energy,
-                        cudaStream_t stream);
+                        cudaStream_t stream, const Clash &clash = Clash());
+  Clash minimizerClash() const;
   void rejectTiledMinimization() const;
   void graphCycle(int first, int count, bool single, cudaStream_t stream);
   void graphFinalEnergy(int first, int count, bool single, cudaStream_t stream);
-  void evaluateFor(int first, int count, bool single, bool force, cudaStream_t stream);
+  void evaluateFor(int first, int count, bool single, bool force, cudaStream_t stream,
+                   const Clash &clash = Clash());
   void buildUnits();
   void upload();
 };

@@ -91,10 +91,14 @@ struct GlobalValence {
   __device__ __forceinline__ float2 lj14(int code_i, int code_l, int) const {
     return lj14tab[(code_i & 0xffff) + (code_l >> 16)];
   }
+  __device__ __forceinline__ float2 clash(int k) const {
+    const int cycle = (d.clash_cycle != nullptr) ? d.clash_cycle[sys[k]] : -1;
+    return clashScaled(d.clash_distance, d.clash_ratio, d.clash_cycles, cycle);
+  }
 };
 
 // Valence terms of tiled molecule blockIdx.x (plus mol_begin), chunks spread over blockIdx.y
-template <bool FORCE, bool ENERGY>
+template <bool FORCE, bool ENERGY, bool CLASH>
 __global__ void __launch_bounds__(256)
 kTiledValence(const DevSynthesis d, const DevTiled t, int mol_begin) {
   __shared__ int sys[1];
@@ -115,7 +119,7 @@ kTiledValence(const DevSynthesis d, const DevTiled t, int mol_begin) {
   __syncthreads();
   const int s = sys[0];
   const GlobalValence v(d, chunks, sys, slot0, d.ljab14 + d.lj_start[s], d.lj_ntypes[s]);
-  valenceTerms<FORCE, ENERGY>(d, v, 1);
+  valenceTerms<FORCE, ENERGY, GlobalValence, CLASH>(d, v, 1);
 }
 
 // Tiled molecule and tile within it of global tile index g
@@ -268,7 +272,7 @@ kTiledRadii(const DevSynthesis d, const DevTiled t, int tile_begin, int tile_end
 }
 
 // Pass 2 (Coulomb + Lennard-Jones and GB pair terms) over tiles [tile_begin, tile_end)
-template <bool FORCE, bool ENERGY, bool NB, bool GB>
+template <bool FORCE, bool ENERGY, bool NB, bool GB, bool CLASH>
 __global__ void __launch_bounds__(256, 4)
 kTiledPair(const DevSynthesis d, const DevTiled t, int tile_begin, int tile_end) {
   __shared__ float4 pa[kTiledWarps * kStageSlots], pb[kTiledWarps * kStageSlots];
@@ -313,8 +317,13 @@ kTiledPair(const DevSynthesis d, const DevTiled t, int tile_begin, int tile_end)
         mask = __ldg(&d.mask_pool[static_cast<size_t>(midx) * 32 + lane]);
       }
     }
-    PairPass<FORCE, ENERGY, NB, GB> p(v, d.kappa, d.inv_dielectric);
-    p.begin(lane, mask);
+    PairPass<FORCE, ENERGY, NB, GB, CLASH> p(v, d.kappa, d.inv_dielectric);
+    float2 clash = make_float2(0.0f, 0.0f);
+    if (CLASH) {
+      const int cycle = (d.clash_cycle != nullptr) ? d.clash_cycle[sysid] : -1;
+      clash = clashScaled(d.clash_distance, d.clash_ratio, d.clash_cycles, cycle);
+    }
+    p.begin(lane, mask, clash);
     walkTile(p, ti, lane);
     const int base = d.atom_start[sysid];
     if (FORCE) {
@@ -488,7 +497,7 @@ int atomGrid(int natom, int sm_count) {
 cudaError_t launchTiled(const DevSynthesis &d, const DevTiled &t, const int* h_tile_prefix,
                         const int* h_atom_prefix, int mol_begin, int mol_end, int terms,
                         bool force, bool energy, bool workspace, int sm_count,
-                        cudaStream_t stream) {
+                        cudaStream_t stream, bool clash) {
   if (mol_end <= mol_begin) {
     return cudaSuccess;
   }
@@ -502,9 +511,13 @@ cudaError_t launchTiled(const DevSynthesis &d, const DevTiled &t, const int* h_t
   const int nmol = mol_end - mol_begin;
   if (vale) {
     const dim3 vgrid(nmol, 4);
-    if (force && energy) kTiledValence<true, true><<<vgrid, 256, 0, stream>>>(d, t, mol_begin);
-    else if (force) kTiledValence<true, false><<<vgrid, 256, 0, stream>>>(d, t, mol_begin);
-    else kTiledValence<false, true><<<vgrid, 256, 0, stream>>>(d, t, mol_begin);
+#define SB_VALE(C)                                                                             \
+    if (force && energy) kTiledValence<true, true, C><<<vgrid, 256, 0, stream>>>(d, t, mol_begin); \
+    else if (force) kTiledValence<true, false, C><<<vgrid, 256, 0, stream>>>(d, t, mol_begin);   \
+    else kTiledValence<false, true, C><<<vgrid, 256, 0, stream>>>(d, t, mol_begin);
+    if (clash) { SB_VALE(true) }
+    else { SB_VALE(false) }
+#undef SB_VALE
   }
   if (gb) {
     kTiledRadii<<<tgrid, 256, 0, stream>>>(d, t, tb, te);
@@ -517,13 +530,20 @@ cudaError_t launchTiled(const DevSynthesis &d, const DevTiled &t, const int* h_t
 #undef SB_ATOMS
   }
   if (nb || gb) {
-#define SB_PAIR(F, E)                                                                     \
-    if (nb && gb) kTiledPair<F, E, true, true><<<tgrid, 256, 0, stream>>>(d, t, tb, te);   \
-    else if (nb) kTiledPair<F, E, true, false><<<tgrid, 256, 0, stream>>>(d, t, tb, te);  \
-    else kTiledPair<F, E, false, true><<<tgrid, 256, 0, stream>>>(d, t, tb, te);
-    if (force && energy) { SB_PAIR(true, true) }
-    else if (force) { SB_PAIR(true, false) }
-    else { SB_PAIR(false, true) }
+#define SB_PAIR(F, E, C)                                                                      \
+    if (nb && gb) kTiledPair<F, E, true, true, C><<<tgrid, 256, 0, stream>>>(d, t, tb, te);    \
+    else if (nb) kTiledPair<F, E, true, false, C><<<tgrid, 256, 0, stream>>>(d, t, tb, te);   \
+    else kTiledPair<F, E, false, true, false><<<tgrid, 256, 0, stream>>>(d, t, tb, te);
+    if (clash) {
+      if (force && energy) { SB_PAIR(true, true, true) }
+      else if (force) { SB_PAIR(true, false, true) }
+      else { SB_PAIR(false, true, true) }
+    }
+    else {
+      if (force && energy) { SB_PAIR(true, true, false) }
+      else if (force) { SB_PAIR(true, false, false) }
+      else { SB_PAIR(false, true, false) }
+    }
 #undef SB_PAIR
   }
   if (gb && force) {

@@ -54,6 +54,80 @@ constexpr float kTaylorHH = 5.45454545454545454545f;
 
 constexpr unsigned kFullMask = 0xffffffffu;
 
+// ------------------------------------------------------------------------------------------------
+// Clash damping: softened Coulomb and Lennard-Jones cores (Potential/soft_core_potentials.tpp:
+// 30-52 and 140-180, as the clash-forgiving GPU kernels apply them,
+// nonbonded_potential_tilegroups.cui:536-602)
+// ------------------------------------------------------------------------------------------------
+// Clash distance and sigma ratio of a molecule in minimization cycle `cycle` of a damping over
+// `cycles` cycles (both shrink linearly to zero, hpc_minimization.cu:268-272); cycle < 0: the
+// base values unscaled
+__device__ __forceinline__ float2 clashScaled(float distance, float ratio, int cycles, int cycle) {
+  if (cycle < 0) {
+    return make_float2(distance, ratio);
+  }
+  if (cycle >= cycles) {
+    return make_float2(0.0f, 0.0f);
+  }
+  const double progress = static_cast<double>(cycles - cycle) / static_cast<double>(cycles);
+  return make_float2(static_cast<float>(static_cast<double>(distance) * progress),
+                     static_cast<float>(static_cast<double>(ratio) * progress));
+}
+
+// Constants of the quadratic Coulomb core for a clash distance cd > 0: below cd the pair energy
+// is qiqj (a (r + 1)^2 + b), continuous in value and slope with qiqj / r at cd
+__device__ __forceinline__ float2 quadraticCore(float cd) {
+  if (cd <= 0.0f) {
+    return make_float2(0.0f, 0.0f);
+  }
+  const float a = -0.5f / (cd * cd * (cd + 1.0f));
+  return make_float2(a, 1.0f / cd - a * (cd + 1.0f) * (cd + 1.0f));
+}
+
+// Coulomb and Lennard-Jones terms of one pair with softened cores: the quadratic Coulomb core
+// (constants qc from quadraticCore) below the clash distance cd, the quartic Lennard-Jones core
+// below ratio x sigma, sigma = (A / B)^(1/6) (none where B <= 1e-6).  Adds the energies to
+// *e_elec and *e_vdw and returns the force factor (force on j = factor x (r_j - r_i)).
+__device__ __forceinline__ float softCorePair(float r, float invr, float qiqj, float lja,
+                                              float ljb, float cd, float2 qc, float ratio,
+                                              float* e_elec, float* e_vdw) {
+  float fmag;
+  if (r < cd) {
+    const float rp = r + 1.0f;
+    *e_elec = __fadd_rn(*e_elec, __fmul_rn(qiqj, fmaf(qc.x * rp, rp, qc.y)));
+    fmag = (r > 1.0e-10f) ? qiqj * (2.0f * qc.x + 2.0f * qc.x * invr) : 0.0f;
+  }
+  else {
+    *e_elec = __fadd_rn(*e_elec, __fmul_rn(qiqj, invr));
+    fmag = -(qiqj * invr * invr * invr);
+  }
+  const float rl = (ljb > 1.0e-6f) ? ratio * sqrtf(cbrtf(__fdividef(lja, ljb))) : 0.0f;
+  if (r < rl) {
+    const float il = 1.0f / rl;
+    const float il2 = il * il;
+    const float il6 = il2 * il2 * il2;
+    const float a = ((6.0f * ljb - 12.0f * lja * il6) * il * il6) /
+                    (((4.0f * rl + 12.0f) * rl + 12.0f) * rl + 4.0f);
+    const float rlp = rl + 1.0f;
+    const float rlp2 = rlp * rlp;
+    const float b = (lja * il6 - ljb) * il6 - a * rlp2 * rlp2;
+    const float rp = r + 1.0f;
+    const float a3 = a * rp * rp * rp;
+    *e_vdw = __fadd_rn(*e_vdw, fmaf(a3, rp, b));
+    if (r > 1.0e-10f) {
+      fmag += 4.0f * a3 * invr;
+    }
+  }
+  else {
+    const float invr2 = invr * invr;
+    const float invr4 = invr2 * invr2;
+    *e_vdw = __fadd_rn(*e_vdw, __fmul_rn(__fsub_rn(__fmul_rn(__fmul_rn(lja, invr4), invr4),
+                                                   __fmul_rn(ljb, invr2)), invr4));
+    fmag += (6.0f * ljb - 12.0f * lja * invr4 * invr2) * invr4 * invr4;
+  }
+  return fmag;
+}
+
 // Packed FP32 pairs (Blackwell FFMA2 / FADD2 / FMUL2): two pairs of one lane in one instruction
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
@@ -262,6 +336,7 @@ struct UnitSmem {
   int* bchunk0;     // valence work in chunks of 32 terms that never straddle two molecules
   int* achunk0;
   int* dchunk0;
+  float2* clash;    // per unit molecule: clash distance and sigma ratio of this evaluation
 };
 
 __host__ __device__ inline size_t alignUp(size_t x, size_t a) { return (x + a - 1) / a * a; }
@@ -276,6 +351,7 @@ __host__ __device__ inline size_t unitSmemBytes(int max_slots, int max_lj,
   b += sizeof(float2) * max_lj;
   b = alignUp(b, 16);
   b += sizeof(unsigned long long) * max_sys * kNrgStride;
+  b += sizeof(float2) * max_sys;
   b += sizeof(int) * (3 * max_sys + 5 * (max_sys + 1));
   return alignUp(b, 16);
 }
@@ -304,6 +380,8 @@ __device__ UnitSmem carveSmem(char* base, int max_slots, int max_lj,
   off = alignUp(off, 16);
   s.nrg = reinterpret_cast<unsigned long long*>(base + off);
   off += sizeof(unsigned long long) * max_sys * kNrgStride;
+  s.clash = reinterpret_cast<float2*>(base + off);
+  off += sizeof(float2) * max_sys;
   int* q = reinterpret_cast<int*>(base + off);
   s.sys = q; q += max_sys;
   s.slot0 = q; q += max_sys;
@@ -418,13 +496,14 @@ struct SmemValence {
   __device__ __forceinline__ void energy(int k, int slot, float e, float scale) const {
     warpEnergy(s, k, slot, e, scale);
   }
+  __device__ __forceinline__ float2 clash(int k) const { return s.clash[k]; }
   // the molecule's 1-4 table follows its standard table in shared memory
   __device__ __forceinline__ float2 lj14(int code_i, int code_l, int nt) const {
     return s.lj[(code_i & 0xffff) + (code_l >> 16) + nt * nt];
   }
 };
 
-template <bool FORCE, bool ENERGY, class V>
+template <bool FORCE, bool ENERGY, class V, bool CLASH = false>
 __device__ void valenceTerms(const DevSynthesis &d, const V &v, int nsys_u) {
   const float fs = d.frc_scale;
   const float es = d.nrg_scale;
@@ -649,15 +728,27 @@ __device__ void valenceTerms(const DevSynthesis &d, const V &v, int nsys_u) {
         const float invr2 = 1.0f / (dv.x * dv.x + dv.y * dv.y + dv.z * dv.z);
         const float invr = sqrtf(invr2);
         const float invr4 = invr2 * invr2;
-        if (FORCE) {
-          const float fmag = -(qiqj * invr * invr2) +
-                             (6.0f * ljb - 12.0f * lja * invr4 * invr2) * invr4 * invr4;
-          v.force(ia, fmag * dv.x, fmag * dv.y, fmag * dv.z, fs);
-          v.force(la, -fmag * dv.x, -fmag * dv.y, -fmag * dv.z, fs);
+        const float2 cl = CLASH ? v.clash(k) : make_float2(0.0f, 0.0f);
+        if (CLASH && (cl.x > 0.0f || cl.y > 0.0f)) {
+          // clash-softened 1-4 pair (valence_potential.tpp:1337-1357)
+          const float fmag = softCorePair(1.0f / invr, invr, qiqj, lja, ljb, cl.x,
+                                          quadraticCore(cl.x), cl.y, &e_el14, &e_lj14);
+          if (FORCE) {
+            v.force(ia, fmag * dv.x, fmag * dv.y, fmag * dv.z, fs);
+            v.force(la, -fmag * dv.x, -fmag * dv.y, -fmag * dv.z, fs);
+          }
         }
-        e_el14 = __fmul_rn(qiqj, invr);
-        e_lj14 = __fsub_rn(__fmul_rn(__fmul_rn(__fmul_rn(lja, invr4), invr4), invr4),
-                           __fmul_rn(__fmul_rn(ljb, invr4), invr2));
+        else {
+          if (FORCE) {
+            const float fmag = -(qiqj * invr * invr2) +
+                               (6.0f * ljb - 12.0f * lja * invr4 * invr2) * invr4 * invr4;
+            v.force(ia, fmag * dv.x, fmag * dv.y, fmag * dv.z, fs);
+            v.force(la, -fmag * dv.x, -fmag * dv.y, -fmag * dv.z, fs);
+          }
+          e_el14 = __fmul_rn(qiqj, invr);
+          e_lj14 = __fsub_rn(__fmul_rn(__fmul_rn(__fmul_rn(lja, invr4), invr4), invr4),
+                             __fmul_rn(__fmul_rn(ljb, invr4), invr2));
+        }
       }
     }
     if (ENERGY) {
@@ -806,8 +897,10 @@ struct RadiiPass2 {
   }
 };
 
-// Pass 2: Coulomb + Lennard-Jones on non-excluded pairs and the GB pair terms
-template <bool FORCE, bool ENERGY, bool NB, bool GB>
+// Pass 2: Coulomb + Lennard-Jones on non-excluded pairs and the GB pair terms; with CLASH, the
+// Coulomb and Lennard-Jones terms of a molecule given a clash distance or ratio take softened
+// cores (the uniform branch is per tile: a tile belongs to one molecule)
+template <bool FORCE, bool ENERGY, bool NB, bool GB, bool CLASH = false>
 struct PairPass {
   const UnitSmem &s;
   float kk, inv_diel;
@@ -816,18 +909,28 @@ struct PairPass {
   float inv4ri;     // 1 / (4 R_i)
   int code_i;
   unsigned mask;
+  bool soft;        // softened cores on this tile
+  float clash_d, clash_r;
+  float2 qcore;
   float2 fxyi, fxyj;   // x, y force sums: i side, traveling j side
   float fzi, fzj;
   float2 de2;          // dE/dR sums: i side, traveling j side
   float e_elec, e_vdw, e_gb;
   __device__ PairPass(const UnitSmem &s_in, float kappa, float inv_dielectric) :
       s(s_in), kk(-kappa * kGbKscale), inv_diel(inv_dielectric), salt(kappa > 0.0f) {}
-  __device__ __forceinline__ void begin(int islot, unsigned mask_in) {
+  __device__ __forceinline__ void begin(int islot, unsigned mask_in,
+                                        float2 clash = make_float2(0.0f, 0.0f)) {
     ai = s.pa[islot];
     bi = s.pb[islot];
     inv4ri = 0.25f * s.gbv[islot].x;
     code_i = __float_as_int(s.prm[islot].y) & 0xffff;
     mask = mask_in;
+    if (CLASH) {
+      clash_d = clash.x;
+      clash_r = clash.y;
+      soft = (clash.x > 0.0f || clash.y > 0.0f);
+      qcore = quadraticCore(clash.x);
+    }
     fxyi = fxyj = de2 = f2(0.0f);
     fzi = fzj = 0.0f;
     e_elec = e_vdw = e_gb = 0.0f;
@@ -854,13 +957,20 @@ struct PairPass {
       ab.x *= incl;
       ab.y *= incl;
       const float qiqj = qiqj_all * incl;
-      if (ENERGY) {
-        e_elec = __fadd_rn(e_elec, __fmul_rn(qiqj, invr));
-        e_vdw = __fadd_rn(e_vdw, __fmul_rn(__fsub_rn(__fmul_rn(__fmul_rn(ab.x, invr4), invr4),
-                                                     __fmul_rn(ab.y, invr2)), invr4));
+      if (CLASH && soft) {
+        fmag = softCorePair(r2 * invr, invr, qiqj, ab.x, ab.y, clash_d, qcore, clash_r, &e_elec,
+                            &e_vdw);
       }
-      if (FORCE) {
-        fmag = -(qiqj * invr * invr2) + (6.0f * ab.y - 12.0f * ab.x * invr4 * invr2) * invr4 * invr4;
+      else {
+        if (ENERGY) {
+          e_elec = __fadd_rn(e_elec, __fmul_rn(qiqj, invr));
+          e_vdw = __fadd_rn(e_vdw, __fmul_rn(__fsub_rn(__fmul_rn(__fmul_rn(ab.x, invr4), invr4),
+                                                       __fmul_rn(ab.y, invr2)), invr4));
+        }
+        if (FORCE) {
+          fmag = -(qiqj * invr * invr2) +
+                 (6.0f * ab.y - 12.0f * ab.x * invr4 * invr2) * invr4 * invr4;
+        }
       }
     }
     if (GB) {
@@ -1067,14 +1177,14 @@ __device__ void gbRadiiTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_
   }
 }
 
-template <bool FORCE, bool ENERGY, bool NB, bool GB>
+template <bool FORCE, bool ENERGY, bool NB, bool GB, bool CLASH = false>
 __device__ void pairTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u, int ntiles,
                           int first, int stride) {
   const int lane = threadIdx.x & 31;
   const float fs = d.frc_scale;
   const float es = d.nrg_scale;
   const float ds = static_cast<float>(1 << kDeijdaBits);
-  PairPass<FORCE, ENERGY, NB, GB> p(s, d.kappa, d.inv_dielectric);
+  PairPass<FORCE, ENERGY, NB, GB, CLASH> p(s, d.kappa, d.inv_dielectric);
   long long acc_elec = 0, acc_vdw = 0, acc_gb = 0;
   int acc_k = -1;
   for (int t = first; t < ntiles; t += stride) {
@@ -1102,7 +1212,7 @@ __device__ void pairTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u, 
         mask = __ldg(&d.mask_pool[static_cast<size_t>(midx) * 32 + lane]);
       }
     }
-    p.begin(ti.ibase + lane, mask);
+    p.begin(ti.ibase + lane, mask, CLASH ? s.clash[ti.k] : make_float2(0.0f, 0.0f));
     walkTile(p, ti, lane);
     if (FORCE) {
       if (lane < ti.ni) {
@@ -1323,8 +1433,9 @@ __device__ __forceinline__ void placeSlot(const DevSynthesis &d, const UnitSmem 
 // All requested terms of a staged unit: coordinates, parameters and cleared accumulators in
 // shared memory on entry (and a barrier since); forces in s.fx.. and per-molecule energies in
 // s.nrg on exit, after a barrier.  WS: also write the GB workspace (psi, effective radii, dE/dR)
-// to global memory.
-template <bool FORCE, bool ENERGY, int TERMS, bool WS, class Team>
+// to global memory.  CLASH: Coulomb and Lennard-Jones pairs, 1-4 pairs included, take the
+// softened cores of s.clash (per unit molecule, zero for none, set before that barrier).
+template <bool FORCE, bool ENERGY, int TERMS, bool WS, bool CLASH = false, class Team>
 __device__ void evaluateStaged(const DevSynthesis &d, const UnitSmem &s, const UnitShape &us,
                                const Team &team) {
   constexpr bool VALE = (TERMS & 1) != 0;
@@ -1336,7 +1447,8 @@ __device__ void evaluateStaged(const DevSynthesis &d, const UnitSmem &s, const U
 
   // valence terms and GB pass 1 touch disjoint accumulators: no barrier between them
   if (VALE) {
-    valenceTerms<FORCE, ENERGY>(d, SmemValence(s, team.warp(), team.warps()), nsys_u);
+    valenceTerms<FORCE, ENERGY, SmemValence, CLASH>(d, SmemValence(s, team.warp(), team.warps()),
+                                                    nsys_u);
     if (!gb) {
       team.sync();
     }
@@ -1397,10 +1509,12 @@ __device__ void evaluateStaged(const DevSynthesis &d, const UnitSmem &s, const U
   }
   if (NB || gb) {
     if (NB && gb) {
-      pairTiles<FORCE, ENERGY, true, true>(d, s, nsys_u, ntiles, team.warp(), team.warps());
+      pairTiles<FORCE, ENERGY, true, true, CLASH>(d, s, nsys_u, ntiles, team.warp(),
+                                                  team.warps());
     }
     else if (NB) {
-      pairTiles<FORCE, ENERGY, true, false>(d, s, nsys_u, ntiles, team.warp(), team.warps());
+      pairTiles<FORCE, ENERGY, true, false, CLASH>(d, s, nsys_u, ntiles, team.warp(),
+                                                   team.warps());
     }
     else {
       pairTiles<FORCE, ENERGY, false, true>(d, s, nsys_u, ntiles, team.warp(), team.warps());

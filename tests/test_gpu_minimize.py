@@ -128,12 +128,65 @@ def test_convergence_target():
         assert np.all(hist[k, cycles[k] + 1:] == 0.0)
 
 
-def test_clash_damping_is_rejected():
-    mol = synthetic.make_molecule(1, 24, 0.1)
-    syn = sb.Synthesis([mol])
-    syn.set_coordinates(mol.coords)
-    with pytest.raises(sb.StormmB200Error):
-        syn.minimize(total_cycles=5, clash_cycles=2)
+@pytest.mark.parametrize("kernel", [sb.MIN_GRAPH, sb.MIN_PERSISTENT])
+def test_clash_damped_minimization_follows_the_oracle(kernel):
+    """The first 25 cycles with softened cores (1.0 A, 0.9 sigma, shrinking to nothing), as
+    STORMM's minimizer runs its clash-damping cycles, on a molecule with close contacts whose
+    plain Lennard-Jones energy is above 10^6 kcal/mol."""
+    g = load("synthetic_K64.npz")
+    m = load("minimize_clash_k64.npz")
+    mol = molecule_from_fixture(g)
+    ctl = dict(total_cycles=int(m["maxcyc"]), sd_cycles=int(m["ncyc"]),
+               clash_cycles=int(m["cdcyc"]), clash_distance=float(m["clash_r0"]),
+               clash_ratio=float(m["clash_ratio"]))
+    _, h_ref = oracle.from_fixture(g).minimize(mol.coords, ctl["total_cycles"],
+                                               ctl["sd_cycles"], clash_cycles=ctl["clash_cycles"],
+                                               clash_distance=ctl["clash_distance"],
+                                               clash_ratio=ctl["clash_ratio"])
+    # STORMM's own start energy with the softened cores
+    assert abs(h_ref[0] - m["min_potential_history"][0]) < 1e-9 * abs(h_ref[0])
+    r = _minimize([mol], kernel=kernel, **ctl)
+    h = r["history"][0]
+    scale = max(np.abs(g["clash_energy_terms"]).sum(), 10.0)
+    assert abs(h[0] - h_ref[0]) <= 1e-6 * scale
+    np.testing.assert_allclose(h[:3], h_ref[:3], rtol=1e-5)
+    drop = h_ref[0] - h_ref[-1]
+    assert abs(h[-1] - h_ref[-1]) <= 0.01 * drop, (h[-1], h_ref[-1])
+    # the final energies are plain (undamped) ones at the final coordinates
+    syn = r["syn"]
+    final = r["energies"].sum(axis=1)
+    syn.initialize()
+    syn.evaluate(force=False, energy=True)
+    assert abs(syn.energy_terms()[0].sum() - final[0]) <= 1e-6 * max(abs(final[0]), 10.0)
+
+
+def test_clash_damping_is_per_system_and_batch_independent():
+    """Each system's damping follows its own cycle count: a molecule minimized in a batch
+    matches it minimized alone, bit for bit, also when advanced in steps."""
+    mols = [synthetic.make_molecule(synthetic._seed(3131, k), n, 0.45)
+            for k, n in enumerate([24, 40, 64, 33, 90])]
+    ctl = dict(total_cycles=30, sd_cycles=10, clash_cycles=12, clash_distance=1.0,
+               clash_ratio=0.9)
+    xyz = np.concatenate([m.coords for m in mols])
+    syn = sb.Synthesis(mols)
+    syn.set_coordinates(xyz)
+    syn.minimize(**ctl)
+    c_batch = syn.coordinates().copy()
+    syn.set_coordinates(xyz)
+    syn.minimize_begin(**ctl)
+    for _ in range(3):
+        syn.minimize_advance(7, final_energy=False)
+    syn.minimize_advance(9)
+    assert np.array_equal(syn.coordinates(), c_batch)
+    alone = sb.Synthesis([mols[2]])
+    alone.set_coordinates(mols[2].coords)
+    alone.minimize(**ctl)
+    off = sum(m.natom for m in mols[:2])
+    assert np.array_equal(alone.coordinates(), c_batch[off:off + mols[2].natom])
+    # no damping at all gives another trajectory
+    syn.set_coordinates(xyz)
+    syn.minimize(**dict(ctl, clash_cycles=0))
+    assert not np.array_equal(syn.coordinates(), c_batch)
 
 
 def test_stepwise_advance_equals_one_shot():

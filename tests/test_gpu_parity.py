@@ -176,3 +176,26 @@ def test_unsupported_model_is_rejected():
     mol = molecule_from_fixture(load("synthetic_E12.npz"))
     with pytest.raises(sb.StormmB200Error):
         sb.Synthesis([mol], igb=7)
+
+
+def test_clash_mitigated_evaluation_matches_stormm():
+    """sb_evaluate_clash (softened Coulomb and Lennard-Jones cores, 1-4 pairs included) against
+    STORMM's MM driver with the same clash distance and sigma ratio, on a molecule with close
+    contacts; the plain evaluation of the same molecule still matches its plain record."""
+    g = load("synthetic_K64.npz")
+    mol = molecule_from_fixture(g)
+    syn = sb.Synthesis([mol])
+    syn.set_coordinates(mol.coords)
+    syn.initialize()
+    syn.evaluate_clash(float(g["clash_r0"][0]), float(g["clash_ratio"][0]))
+    assert syn.status() == 0
+    _check_energy(syn.energy_terms()[0], g["clash_energy_terms"])
+    assert rms_rel(syn.forces(), g["clash_frc_total"].reshape(-1, 3)) <= FORCE_TOL
+    syn.initialize()
+    syn.evaluate()
+    _check_energy(syn.energy_terms()[0], g["energy_terms_mm"])
+    # zero distance and ratio is the plain evaluation, bit for bit
+    f_plain = syn.forces_fixed()[0].copy()
+    syn.initialize()
+    syn.evaluate_clash(0.0, 0.0)
+    assert np.array_equal(syn.forces_fixed()[0], f_plain)
