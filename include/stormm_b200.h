@@ -136,7 +136,14 @@ typedef struct {
   int tiled_above_atoms;       /* molecules with more atoms are evaluated tile by tile from global
                                   memory, spread over the whole GPU (0: 2048, the on-chip limit;
                                   32-2048); they cannot be minimized */
+  int precision;               /* SB_PRECISION_SINGLE (default): FP32 arithmetic with fixed-point
+                                  accumulation; SB_PRECISION_DOUBLE: FP64 arithmetic from double
+                                  parameters (STORMM's PrecisionModel::DOUBLE), every molecule tile
+                                  by tile; evaluation only */
 } sb_options;
+
+#define SB_PRECISION_SINGLE 0
+#define SB_PRECISION_DOUBLE 1
 
 /* Fill *opt with STORMM's defaults (OBC-II, dielectric 80, no salt, 32/23/26 fixed-point bits) */
 void sb_default_options(sb_options* opt);

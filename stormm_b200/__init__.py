@@ -19,6 +19,7 @@ SB_GB_NONE, SB_GB_HCT, SB_GB_OBC, SB_GB_OBC2 = 0, 1, 2, 5
 TERM_VALENCE, TERM_NONBONDED, TERM_GB, TERM_ALL = 1, 2, 4, 7
 TUNE_EVALUATE, TUNE_MINIMIZE = 1, 2
 MIN_GRAPH, MIN_PERSISTENT = 0, 1
+PRECISION_SINGLE, PRECISION_DOUBLE = 0, 1
 INIT_FORCES, INIT_ENERGIES, INIT_GB_WORKSPACE = 1, 2, 4
 NRG_STRIDE = 16
 # StateVariable slots (STORMM Potential/energy_enumerators.h:36-50)
@@ -51,7 +52,7 @@ class Options(ctypes.Structure):
         ("frc_bits", ctypes.c_int), ("nrg_bits", ctypes.c_int),
         ("max_atoms_per_unit", ctypes.c_int), ("max_tiles_per_unit", ctypes.c_int),
         ("threads_per_block", ctypes.c_int), ("device", ctypes.c_int),
-        ("tiled_above_atoms", ctypes.c_int),
+        ("tiled_above_atoms", ctypes.c_int), ("precision", ctypes.c_int),
     ]
 
 

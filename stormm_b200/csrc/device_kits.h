@@ -141,6 +141,31 @@ struct DevTiled {
   float* sde;                    // per padded atom: dE/dR after the chain-rule prefactor
 };
 
+// Double-precision parameters of the FP64 mode (STORMM's double-precision kits beside the
+// single-precision ones), with the same layouts as their FP32 counterparts in DevSynthesis
+struct DevPrecise {
+  const double* charge;          // per padded atom: charge x sqrt(Coulomb constant)
+  const double* rho;             // intrinsic GB radius - 0.09 A
+  const double* srho;            // screening factor x rho
+  const double* pb_radii;
+  const double* alpha;
+  const double* beta;
+  const double* gamma;
+  const double2* ljab;           // per-topology (A, B) tables at DevSynthesis::lj_start offsets
+  const double2* ljab14;
+  const int2* bond_atoms;        // per bond: molecule-local atoms
+  const double2* bond_prm;       // k, r0
+  const int4* angl_atoms;        // per angle: i, j, k
+  const double2* angl_prm;       // k, theta0
+  const int4* dihe_atoms;        // per dihedral: i, j, k, l
+  const double4* dihe_prm;       // amplitude, periodicity, phase, 1 for an improper
+  const double2* dihe_attn;      // 1 / scee, 1 / scnb of the attached 1-4 pair (0: none)
+  double kappa;                  // Debye-Hueckel screening (1/A)
+  double inv_dielectric;
+  double* radius;                // per padded atom: effective GB radius of the evaluation
+  double* sde;                   // per padded atom: dE/dR after the chain-rule prefactor
+};
+
 // Line-minimization state (MolecularMechanics/line_minimization.h:15-221 and the conjugate
 // gradient substrate, Math/hpc_reduction.h:55-63), per system and per padded atom.  It persists
 // between launches, so a minimization can run in several launches of a few cycles each.

@@ -171,6 +171,9 @@ public:
       throw Error(SB_ERR_ARGUMENT, "server budget, batch limits and cycles per launch must be "
                   "positive");
     }
+    if (o.options.precision != SB_PRECISION_SINGLE) {
+      throw Error(SB_ERR_UNSUPPORTED, "the request server minimizes, which runs in FP32");
+    }
     int ndev = 0;
     cudaCheck(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
     if (o.options.device < 0 || o.options.device >= ndev) {

@@ -37,6 +37,10 @@ cudaError_t launchTiled(const DevSynthesis &d, const DevTiled &t, const int* h_t
                         const int* h_atom_prefix, int mol_begin, int mol_end, int terms,
                         bool force, bool energy, bool workspace, int sm_count,
                         cudaStream_t stream, bool clash);
+cudaError_t launchTiled64(const DevSynthesis &d, const DevPrecise &p, const DevTiled &t,
+                          const int* h_tile_prefix, const int* h_atom_prefix, int mol_begin,
+                          int mol_end, int terms, bool force, bool energy, bool workspace,
+                          int sm_count, cudaStream_t stream);
 cudaError_t launchImportCoordinates(const double* d_xyz, const int* d_map, int natom,
                                     double scale, long long* xcrd, long long* ycrd,
                                     long long* zcrd, int* xo, int* yo, int* zo, int* status,
@@ -105,6 +109,10 @@ Synthesis::Synthesis(const sb_topology* tops, int ntop, const int* topology_inde
       opt.nrg_bits < 22 || opt.nrg_bits > 40) {
     throw Error(SB_ERR_ARGUMENT, "fixed-point bit counts out of range");
   }
+  if (opt.precision != SB_PRECISION_SINGLE && opt.precision != SB_PRECISION_DOUBLE) {
+    throw Error(SB_ERR_ARGUMENT, "precision must be SB_PRECISION_SINGLE or SB_PRECISION_DOUBLE");
+  }
+  fp64 = (opt.precision == SB_PRECISION_DOUBLE);
   int dev_count = 0;
   cudaCheck(cudaGetDeviceCount(&dev_count), "cudaGetDeviceCount");
   if (opt.device < 0 || opt.device >= dev_count) {
@@ -172,6 +180,15 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
   h_alpha.assign(np, 0.0f);
   h_beta.assign(np, 0.0f);
   h_gamma.assign(np, 0.0f);
+  if (fp64) {
+    h64_charge.assign(np, 0.0);
+    h64_rho.assign(np, 1.0);
+    h64_srho.assign(np, 0.0);
+    h64_pb.assign(np, 1.09);
+    h64_alpha.assign(np, 0.0);
+    h64_beta.assign(np, 0.0);
+    h64_gamma.assign(np, 0.0);
+  }
 
   // per-topology Lennard-Jones tables and tile exclusion masks
   std::vector<int> topo_lj_start(ntop), topo_tile_start(ntop);
@@ -185,6 +202,10 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
       const double a14 = (tp.lja14 != nullptr) ? tp.lja14[e] : tp.lja[e];
       const double b14 = (tp.ljb14 != nullptr) ? tp.ljb14[e] : tp.ljb[e];
       h_ljab14.push_back(make_float2(static_cast<float>(a14), static_cast<float>(b14)));
+      if (fp64) {
+        h64_ljab.push_back(make_double2(tp.lja[e], tp.ljb[e]));
+        h64_ljab14.push_back(make_double2(a14, b14));
+      }
     }
     // exclusions as a symmetric set of pairs
     const int n = tp.natom;
@@ -273,6 +294,18 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
         h_beta[base + i] = static_cast<float>(tp.gb_beta ? tp.gb_beta[i] : gbDefault(opt.igb, 1));
         h_gamma[base + i] = static_cast<float>(tp.gb_gamma ? tp.gb_gamma[i] : gbDefault(opt.igb, 2));
       }
+      if (fp64) {
+        h64_charge[base + i] = tp.charge[i] * sqrt_kc;
+        if (opt.igb != SB_GB_NONE) {
+          const double rho = tp.pb_radii[i] - 0.09;
+          h64_rho[base + i] = rho;
+          h64_srho[base + i] = tp.gb_screen[i] * rho;
+          h64_pb[base + i] = tp.pb_radii[i];
+          h64_alpha[base + i] = tp.gb_alpha ? tp.gb_alpha[i] : gbDefault(opt.igb, 0);
+          h64_beta[base + i] = tp.gb_beta ? tp.gb_beta[i] : gbDefault(opt.igb, 1);
+          h64_gamma[base + i] = tp.gb_gamma ? tp.gb_gamma[i] : gbDefault(opt.igb, 2);
+        }
+      }
     }
     auto check_atom = [&](int a) {
       if (a < 0 || a >= tp.natom) {
@@ -287,6 +320,10 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
       const float leq_hi = static_cast<float>(tp.bond_leq[b]);
       h_bonds.push_back(make_uint4(i | (j << 16), fbits(tp.bond_keq[b]), fbits(leq_hi),
                                    fbits(tp.bond_leq[b] - static_cast<double>(leq_hi))));
+      if (fp64) {
+        h64_bond_atoms.push_back(make_int2(i, j));
+        h64_bond_prm.push_back(make_double2(tp.bond_keq[b], tp.bond_leq[b]));
+      }
     }
     h_bond_start[s + 1] = h_bonds.size();
     for (int a = 0; a < tp.nangl; a++) {
@@ -295,6 +332,10 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
       const uint32_t k = check_atom(tp.angl_atoms[3 * a + 2]);
       h_angles.push_back(make_uint4(i | (j << 16), k, fbits(tp.angl_keq[a]),
                                     fbits(std::cos(tp.angl_theta0[a]))));
+      if (fp64) {
+        h64_angl_atoms.push_back(make_int4(i, j, k, 0));
+        h64_angl_prm.push_back(make_double2(tp.angl_keq[a], tp.angl_theta0[a]));
+      }
     }
     h_angl_start[s + 1] = h_angles.size();
     for (int d = 0; d < tp.ndihe; d++) {
@@ -315,6 +356,13 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
                                     fbits(std::sin(tp.dihe_phase[d])),
                                     fbits(scee > 0.0 ? 1.0 / scee : 0.0),
                                     fbits((scee > 0.0 && scnb > 0.0) ? 1.0 / scnb : 0.0)));
+      if (fp64) {
+        h64_dihe_atoms.push_back(make_int4(i, j, k, l));
+        h64_dihe_prm.push_back(make_double4(tp.dihe_amp[d], tp.dihe_freq[d], tp.dihe_phase[d],
+                                            improper ? 1.0 : 0.0));
+        h64_dihe_attn.push_back(make_double2(scee > 0.0 ? 1.0 / scee : 0.0,
+                                             (scee > 0.0 && scnb > 0.0) ? 1.0 / scnb : 0.0));
+      }
     }
     h_dihe_start[s + 1] = h_dihe_a.size();
   }
@@ -446,7 +494,10 @@ void Synthesis::buildUnits() {
     throw Error(SB_ERR_ARGUMENT, "threads per block must be a multiple of 32 in [64, 256]");
   }
   tiled_threshold = (opt.tiled_above_atoms > 0) ? opt.tiled_above_atoms : kMaxFusedAtoms;
-  if (tiled_threshold < kTile || tiled_threshold > kMaxFusedAtoms) {
+  if (fp64) {
+    tiled_threshold = 0;   // the FP64 mode evaluates every molecule tile by tile
+  }
+  else if (tiled_threshold < kTile || tiled_threshold > kMaxFusedAtoms) {
     throw Error(SB_ERR_ARGUMENT, "tiled_above_atoms must lie in [32, 2048]");
   }
   // molecules above the threshold: tiles of every one, in system order
@@ -544,6 +595,46 @@ void Synthesis::upload() {
     d_tiled_de.zeros(natom_padded);
     d_tiled_radius.zeros(natom_padded);
     d_tiled_sde.zeros(natom_padded);
+  }
+  if (fp64) {
+    d64_charge.upload(h64_charge);
+    d64_rho.upload(h64_rho);
+    d64_srho.upload(h64_srho);
+    d64_pb.upload(h64_pb);
+    d64_alpha.upload(h64_alpha);
+    d64_beta.upload(h64_beta);
+    d64_gamma.upload(h64_gamma);
+    d64_ljab.upload(h64_ljab);
+    d64_ljab14.upload(h64_ljab14);
+    d64_bond_atoms.upload(h64_bond_atoms);
+    d64_bond_prm.upload(h64_bond_prm);
+    d64_angl_atoms.upload(h64_angl_atoms);
+    d64_angl_prm.upload(h64_angl_prm);
+    d64_dihe_atoms.upload(h64_dihe_atoms);
+    d64_dihe_prm.upload(h64_dihe_prm);
+    d64_dihe_attn.upload(h64_dihe_attn);
+    d64_radius.zeros(natom_padded);
+    d64_sde.zeros(natom_padded);
+    dev64.charge = d64_charge.p;
+    dev64.rho = d64_rho.p;
+    dev64.srho = d64_srho.p;
+    dev64.pb_radii = d64_pb.p;
+    dev64.alpha = d64_alpha.p;
+    dev64.beta = d64_beta.p;
+    dev64.gamma = d64_gamma.p;
+    dev64.ljab = d64_ljab.p;
+    dev64.ljab14 = d64_ljab14.p;
+    dev64.bond_atoms = d64_bond_atoms.p;
+    dev64.bond_prm = d64_bond_prm.p;
+    dev64.angl_atoms = d64_angl_atoms.p;
+    dev64.angl_prm = d64_angl_prm.p;
+    dev64.dihe_atoms = d64_dihe_atoms.p;
+    dev64.dihe_prm = d64_dihe_prm.p;
+    dev64.dihe_attn = d64_dihe_attn.p;
+    dev64.kappa = (opt.saltcon > 1.0e-8) ? std::sqrt(0.10806 * opt.saltcon) : 0.0;
+    dev64.inv_dielectric = 1.0 / opt.dielectric;
+    dev64.radius = d64_radius.p;
+    dev64.sde = d64_sde.p;
   }
   dev_tiled.nmol = static_cast<int>(h_tiled_systems.size());
   dev_tiled.ntiles = h_tile_prefix.back();
@@ -681,6 +772,15 @@ void Synthesis::launchTiledRange(int mol_begin, int mol_end, int terms, bool for
   const size_t np = natom_padded;
   cudaCheck(cudaMemsetAsync(d_tiled_psi.p, 0, np * sizeof(long long), stream), "memset");
   cudaCheck(cudaMemsetAsync(d_tiled_de.p, 0, np * sizeof(long long), stream), "memset");
+  if (fp64) {
+    if (clash.on()) {
+      throw Error(SB_ERR_UNSUPPORTED, "softened cores are not provided in the FP64 mode");
+    }
+    cudaCheck(launchTiled64(dev, dev64, dev_tiled, h_tile_prefix.data(), h_atom_prefix.data(),
+                            mol_begin, mol_end, terms, force, energy, true, sm_count, stream),
+              "FP64 evaluation launch");
+    return;
+  }
   DevSynthesis d = dev;
   clash.apply(&d);
   cudaCheck(launchTiled(d, dev_tiled, h_tile_prefix.data(), h_atom_prefix.data(), mol_begin,
@@ -701,6 +801,9 @@ Clash Synthesis::minimizerClash() const {
 }
 
 void Synthesis::rejectTiledMinimization() const {
+  if (fp64) {
+    throw Error(SB_ERR_UNSUPPORTED, "the FP64 mode evaluates; minimization runs in FP32");
+  }
   if (!h_tiled_systems.empty()) {
     throw Error(SB_ERR_UNSUPPORTED, "molecules above " + std::to_string(tiled_threshold) +
                 " atoms are evaluated tile by tile and cannot be minimized on chip");
@@ -1105,6 +1208,9 @@ void Synthesis::autotune(int what, int* chosen_slots, int* chosen_tiles, double*
                          cudaStream_t stream) {
   if (what != SB_TUNE_EVALUATE && what != SB_TUNE_MINIMIZE) {
     throw Error(SB_ERR_ARGUMENT, "autotune target must be SB_TUNE_EVALUATE or SB_TUNE_MINIMIZE");
+  }
+  if (fp64) {
+    throw Error(SB_ERR_UNSUPPORTED, "the FP64 mode has no work-unit packing to tune");
   }
   static const int kCandidates[][2] = {{256, 36}, {256, 24}, {192, 21}, {160, 15}, {128, 16},
                                        {128, 10}, {96, 12}, {96, 6}, {64, 6}};

@@ -201,6 +201,20 @@ public:
   DeviceArray<long long> d_tiled_psi, d_tiled_de;
   DeviceArray<float> d_tiled_radius, d_tiled_sde;
   DevTiled dev_tiled{};
+  // FP64 mode (opt.precision == SB_PRECISION_DOUBLE): double parameters and per-atom GB state
+  bool fp64 = false;
+  std::vector<double> h64_charge, h64_rho, h64_srho, h64_pb, h64_alpha, h64_beta, h64_gamma;
+  std::vector<double2> h64_ljab, h64_ljab14, h64_bond_prm, h64_angl_prm, h64_dihe_attn;
+  std::vector<int2> h64_bond_atoms;
+  std::vector<int4> h64_angl_atoms, h64_dihe_atoms;
+  std::vector<double4> h64_dihe_prm;
+  DeviceArray<double> d64_charge, d64_rho, d64_srho, d64_pb, d64_alpha, d64_beta, d64_gamma;
+  DeviceArray<double2> d64_ljab, d64_ljab14, d64_bond_prm, d64_angl_prm, d64_dihe_attn;
+  DeviceArray<int2> d64_bond_atoms;
+  DeviceArray<int4> d64_angl_atoms, d64_dihe_atoms;
+  DeviceArray<double4> d64_dihe_prm;
+  DeviceArray<double> d64_radius, d64_sde;
+  DevPrecise dev64{};
 
   // line-minimization state, allocated by the first minimization
   DeviceArray<long long> d_xprv, d_yprv, d_zprv;

@@ -14,12 +14,12 @@
 #include <cuda_runtime.h>
 
 #include "unit_eval.cuh"
+#include "tile_tasks.cuh"
 
 namespace sb {
 
 namespace {
 
-constexpr int kTiledWarps = 8;            // warps per block of the tile kernels
 constexpr int kStageSlots = 2 * kTile;    // block I in slots 0-31, block J in slots 32-63
 
 // Valence terms reading atoms straight from the global fixed-point arrays and adding forces and
@@ -122,21 +122,6 @@ kTiledValence(const DevSynthesis d, const DevTiled t, int mol_begin) {
   valenceTerms<FORCE, ENERGY, GlobalValence, CLASH>(d, v, 1);
 }
 
-// Tiled molecule and tile within it of global tile index g
-__device__ __forceinline__ int tiledOwner(const DevTiled &t, int g) {
-  int lo = 0, hi = t.nmol - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (t.tile_prefix[mid] <= g) {
-      lo = mid;
-    }
-    else {
-      hi = mid - 1;
-    }
-  }
-  return lo;
-}
-
 // Stage one tile's atom blocks into a warp's slice: block I in slots 0-31, block J in 32-63
 // (a diagonal tile stages block I only).  PASS 1 and 3 carry s * rho and rho, PASS 2 the charge
 // and the effective radius; padding slots get the fused kernel's zero-contribution values.
@@ -194,32 +179,6 @@ __device__ __forceinline__ void stageTile(const DevSynthesis &d, const DevTiled 
     v.gbv[slot] = gbv;
   }
   __syncwarp();
-}
-
-__device__ __forceinline__ TileInfo tiledTileInfo(const DevSynthesis &d, int sysid, int local,
-                                                  int* I, int* J) {
-  tileCoordinates(local, I, J);
-  const int n = d.atom_count[sysid];
-  TileInfo ti;
-  ti.k = 0;
-  ti.local = local;
-  ti.diag = (*I == *J);
-  ti.ibase = 0;
-  ti.jbase = ti.diag ? 0 : kTile;
-  ti.ni = min(kTile, n - *I * kTile);
-  ti.nj = min(kTile, n - *J * kTile);
-  return ti;
-}
-
-// The warp's contiguous run of tiles [first, last)
-__device__ __forceinline__ void warpTileRange(const DevTiled &t, int tile_begin, int tile_end,
-                                              int* first, int* last) {
-  const int nwarps = gridDim.x * kTiledWarps;
-  const int w = blockIdx.x * kTiledWarps + (threadIdx.x >> 5);
-  const int n = tile_end - tile_begin;
-  const int per = (n + nwarps - 1) / nwarps;
-  *first = tile_begin + min(n, w * per);
-  *last = tile_begin + min(n, (w + 1) * per);
 }
 
 __device__ __forceinline__ UnitSmem warpView(float4* pa, float4* pb, float4* prm, float2* gbv,
@@ -397,24 +356,6 @@ kTiledDeriv(const DevSynthesis d, const DevTiled t, int tile_begin, int tile_end
   }
 }
 
-// Tiled molecule owning padded position q of the tiled atoms, and the atom's global index
-__device__ __forceinline__ int tiledAtom(const DevSynthesis &d, const DevTiled &t, int q,
-                                         int* sysid, int* a) {
-  int lo = 0, hi = t.nmol - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (t.atom_prefix[mid] <= q) {
-      lo = mid;
-    }
-    else {
-      hi = mid - 1;
-    }
-  }
-  *sysid = t.systems[lo];
-  *a = q - t.atom_prefix[lo];
-  return d.atom_start[*sysid] + *a;
-}
-
 // Effective radii and GB self terms of the tiled atoms [atom_begin, atom_end) (padded
 // positions; a warp's 32 positions always belong to one molecule)
 template <bool FORCE, bool ENERGY, bool WS>
@@ -476,18 +417,6 @@ kTiledChain(const DevSynthesis d, const DevTiled t, int atom_begin, int atom_end
     }
     t.sde[gi] = sde;
   }
-}
-
-int tileGrid(int ntiles, int sm_count) {
-  const int want = (ntiles + kTiledWarps * 4 - 1) / (kTiledWarps * 4);   // about 4 tiles a warp
-  const int cap = sm_count * 8;
-  return want < 1 ? 1 : (want > cap ? cap : want);
-}
-
-int atomGrid(int natom, int sm_count) {
-  const int want = (natom + 255) / 256;
-  const int cap = sm_count * 8;
-  return want < 1 ? 1 : (want > cap ? cap : want);
 }
 
 }  // namespace

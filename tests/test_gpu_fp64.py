@@ -1,0 +1,111 @@
+"""The FP64-arithmetic mode (precision = SB_PRECISION_DOUBLE, STORMM's PrecisionModel::DOUBLE):
+double parameters and double arithmetic, integer accumulation, every molecule tile by tile.
+
+Against STORMM's FP64 CPU results the mode is limited only by its fixed-point grids, so these
+tests raise the force and energy bits to 36 (2^-36 kcal/mol and kcal/mol/A) and hold energies
+to 1e-10 of the summed terms and forces to 1e-10 RMS relative, four orders below the FP32
+path's tolerances; the FP32 path is checked to sit between the two."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+import stormm_b200 as sb
+from stormm_b200 import synthetic
+from fixtures import (igb_of_fixture, load, molecule_from_fixture, reference_forces,
+                      reference_paths, rms_rel)
+
+pytestmark = pytest.mark.gpu
+
+BITS = dict(frc_bits=36, nrg_bits=36)
+CASES = ["synthetic_M0.npz", "synthetic_E2.npz", "synthetic_E17.npz", "synthetic_E33.npz",
+         "synthetic_E257.npz", "synthetic_C600.npz", "synthetic_S64.npz", "synthetic_H100.npz",
+         "synthetic_O100.npz", "synthetic_V100.npz", "synthetic_K64.npz"]
+
+
+def _evaluate(g, precision, **extra):
+    mol = molecule_from_fixture(g)
+    syn = sb.Synthesis([mol], igb=igb_of_fixture(g), dielectric=float(g["dielectric"][0]),
+                       saltcon=float(g["saltcon"][0]), precision=precision, **extra)
+    syn.set_coordinates(mol.coords)
+    syn.initialize()
+    syn.evaluate()
+    assert syn.status() == 0
+    return syn
+
+
+def _on_grid(xyz):
+    """Coordinates as the synthesis holds them: rounded to its 2^-32 A fixed-point grid."""
+    return np.round(np.asarray(xyz, dtype=np.float64) * 2.0 ** 32) / 2.0 ** 32
+
+
+@pytest.mark.parametrize("name", CASES + [os.path.basename(p) for p in reference_paths()])
+def test_fp64_mode_matches_stormm(name):
+    """Energies against STORMM's FP64 sums; forces against the oracle (pinned to STORMM to
+    1e-12) at the fixed-point coordinates, which the reference systems' coordinates are not on
+    (their forces differ from STORMM's by the ~1e-10 A rounding alone)."""
+    g = load(name)
+    syn = _evaluate(g, sb.PRECISION_DOUBLE, **BITS)
+    e = syn.energy_terms()[0]
+    ref = g["energy_terms"]
+    scale = max(np.abs(ref).sum(), 10.0)
+    assert np.all(np.abs(e - ref) <= 1e-10 * scale), (e - ref)
+    r = oracle.from_fixture(g).evaluate(_on_grid(g["coords"]))
+    assert rms_rel(syn.forces(), r["forces"]) <= 1e-10
+    if name.startswith("synthetic_"):
+        # these fixtures were computed on the grid already
+        assert rms_rel(syn.forces(), reference_forces(g)) <= 1e-10
+
+
+@pytest.mark.parametrize("name", ["synthetic_M0.npz", "synthetic_C600.npz",
+                                  "synthetic_S64.npz"])
+def test_fp32_error_sits_between(name):
+    """FP32 arithmetic loses several digits that the FP64 mode keeps."""
+    g = load(name)
+    ref_f = reference_forces(g)
+    e64 = rms_rel(_evaluate(g, sb.PRECISION_DOUBLE, **BITS).forces(), ref_f)
+    e32 = rms_rel(_evaluate(g, sb.PRECISION_SINGLE).forces(), ref_f)
+    assert e64 * 1000.0 < e32 <= 5e-6, (e64, e32)
+
+
+def test_fp64_mode_batches_repeat_and_match_alone():
+    mols = [synthetic.make_molecule(synthetic._seed(6464, k), n, 0.2)
+            for k, n in enumerate([12, 40, 77, 130, 33])]
+    mols.append(synthetic.make_chain(6465, 900))
+    xyz = np.concatenate([m.coords for m in mols])
+    syn = sb.Synthesis(mols, precision=sb.PRECISION_DOUBLE, **BITS)
+    syn.set_coordinates(xyz)
+    syn.initialize()
+    syn.evaluate()
+    f1, e1 = syn.forces_fixed()[0].copy(), syn.energies_fixed().copy()
+    syn.initialize()
+    syn.evaluate()
+    assert np.array_equal(syn.forces_fixed()[0], f1)
+    assert np.array_equal(syn.energies_fixed(), e1)
+    # the per-system launches give the same integers
+    syn.initialize()
+    syn.evaluate_range(0, len(mols))
+    assert np.array_equal(syn.forces_fixed()[0], f1)
+    assert np.array_equal(syn.energies_fixed(), e1)
+    # and against the oracle, molecule by molecule
+    f = syn.forces()
+    off = 0
+    for k, m in enumerate(mols):
+        r = oracle.from_molecule(m).evaluate(_on_grid(m.coords))
+        assert rms_rel(f[off:off + m.natom], r["forces"]) <= 1e-10, k
+        scale = max(np.abs(r["energies"]).sum(), 10.0)
+        assert np.all(np.abs(syn.energy_terms()[k] - r["energies"]) <= 1e-10 * scale), k
+        off += m.natom
+
+
+def test_fp64_mode_evaluates_only():
+    mol = synthetic.make_molecule(5, 30, 0.1)
+    syn = sb.Synthesis([mol], precision=sb.PRECISION_DOUBLE)
+    syn.set_coordinates(mol.coords)
+    with pytest.raises(sb.StormmB200Error):
+        syn.minimize(total_cycles=3)
+    with pytest.raises(sb.StormmB200Error):
+        syn.evaluate_clash(0.2, 0.5)
+    with pytest.raises(sb.StormmB200Error):
+        sb.Synthesis([mol], precision=7)
