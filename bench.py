@@ -450,6 +450,9 @@ def bench_large(args, world, rank, local, flush):
     _barrier(world)
     total_ms = _max_over_ranks(float(np.sum(times)), world)
     value = world * LARGE_NSYS * len(times) / (total_ms / 1000.0)
+    fp64 = None
+    if rank == 0:
+        fp64 = _large_fp64(mols, local, syn.forces(), syn.energy_terms(), flush)
     per_sys = None
     if rank == 0:
         ev0, ev1 = _event_pair()
@@ -473,8 +476,44 @@ def bench_large(args, world, rank, local, flush):
            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                         "frac": achieved / peak, "flops_per_step": flops},
            "l2": "flushed (256 MB write) before every timed step",
-           "fp64_gpu_mode": "not built"}
+           "fp64_gpu_mode": fp64}
     return out
+
+
+def _large_fp64(mols, local, f32, e32, flush, steps=3):
+    """The same chains in the FP64-arithmetic mode (precision = SB_PRECISION_DOUBLE): its
+    throughput on one GPU, and how far the FP32 path's forces and energies lie from it."""
+    import torch
+    import stormm_b200 as sb
+    syn = sb.Synthesis(mols, device=local, precision=sb.PRECISION_DOUBLE)
+    syn.set_coordinates(np.concatenate([m.coords for m in mols]))
+    syn.initialize(sb.INIT_FORCES | sb.INIT_ENERGIES)
+    syn.evaluate()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(steps):
+        flush.zero_()
+        ev0, ev1 = _event_pair()
+        ev0.record()
+        syn.initialize(sb.INIT_FORCES | sb.INIT_ENERGIES)
+        syn.evaluate()
+        ev1.record()
+        torch.cuda.synchronize()
+        times.append(ev0.elapsed_time(ev1))
+    assert syn.status() == 0
+    f64 = syn.forces()
+    e64 = syn.energy_terms()
+    syn.close()
+    frel = float(np.sqrt(((f32 - f64) ** 2).sum() / (f64 ** 2).sum()))
+    escale = np.maximum(np.abs(e64).sum(axis=1), 10.0)
+    erel = float(np.max(np.abs(e32.sum(axis=1) - e64.sum(axis=1)) / escale))
+    return {"value": len(mols) * steps / (float(np.sum(times)) / 1000.0),
+            "unit": "force-evals/s", "steps": steps, "ms_per_step": float(np.mean(times)),
+            "n_gpus": 1, "fp32_force_rms_rel_vs_fp64": frel,
+            "fp32_energy_rel_vs_fp64_max": erel,
+            "note": "FP64 arithmetic from double parameters, every chain tile by tile, integer "
+                    "accumulation; matches STORMM's FP64 CPU results to 1e-10 "
+                    "(tests/test_gpu_fp64.py)"}
 
 
 def bench_served(local):

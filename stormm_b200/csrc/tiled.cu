@@ -288,21 +288,21 @@ kTiledPair(const DevSynthesis d, const DevTiled t, int tile_begin, int tile_end)
     if (FORCE) {
       if (lane < ti.ni) {
         const int gi = base + I * kTile + lane;
-        addGlobal(&d.xfrc[gi], p.fxyi.x * fs);
-        addGlobal(&d.yfrc[gi], p.fxyi.y * fs);
+        addGlobal(&d.xfrc[gi], p.fxi * fs);
+        addGlobal(&d.yfrc[gi], p.fyi * fs);
         addGlobal(&d.zfrc[gi], p.fzi * fs);
         if (GB) {
-          addGlobal(&t.de_acc[gi], p.de2.x * ds);
+          addGlobal(&t.de_acc[gi], p.dei * ds);
         }
       }
       const int jl = traveledAtom(ti, lane);
       if (jl < ti.nj) {
         const int gj = base + J * kTile + jl;
-        addGlobal(&d.xfrc[gj], p.fxyj.x * fs);
-        addGlobal(&d.yfrc[gj], p.fxyj.y * fs);
+        addGlobal(&d.xfrc[gj], p.fxj * fs);
+        addGlobal(&d.yfrc[gj], p.fyj * fs);
         addGlobal(&d.zfrc[gj], p.fzj * fs);
         if (GB) {
-          addGlobal(&t.de_acc[gj], p.de2.y * ds);
+          addGlobal(&t.de_acc[gj], p.dej * ds);
         }
       }
     }

@@ -193,53 +193,30 @@ __device__ __forceinline__ float2 hctIntegral2(float2 r, float2 r2, float2 invr,
 // (lambda = dL/dr: 1 without overlap, 0 on partial overlap, -1 inside the neighbour):
 //   dI/dr = 1/2 [-lambda/L^2 + 1/U^2 + q'(1/L^2 - 1/U^2) + 2q (1/U^3 - lambda/L^3)
 //                + (lambda/L - 1/U - ln(L/U)/r) / (2r)] - 1/L^2 (inside),
-// q = (sj^2 - r^2)/(4r), q' = dq/dr.  Here for both directions of one pair at once: x for
-// (rho.x, sj.x), y for (rho.y, sj.y), sharing r; the far and near forms run only when some lane
-// of the warp needs them.
-__device__ __forceinline__ float2 hctDerivative2(float r, float r2, float invr, float2 rho,
-                                                 float2 sj) {
+// q = (sj^2 - r^2)/(4r), q' = dq/dr.
+__device__ __forceinline__ float hctDerivative(float r, float r2, float invr, float rho,
+                                               float sj) {
   const float invr2 = invr * invr;
-  const bool far_x = r > 4.0f * sj.x;
-  const bool far_y = r > 4.0f * sj.y;
-  const float2 sj2 = mul2(sj, sj);
-  float2 vf = f2(0.0f);
-  float2 vn = f2(0.0f);
-  if (far_x || far_y) {
-    const float2 t = mul2(sj2, f2(invr2));
-    float2 dumbo = fma2(t, f2(kTaylorHH), f2(kTaylorH));
-    dumbo = fma2(t, dumbo, f2(kTaylorG));
-    dumbo = fma2(t, dumbo, f2(kTaylorF));
-    dumbo = fma2(t, dumbo, f2(kTaylorE));
-    vf = mul2(mul2(mul2(t, sj), f2(invr2 * invr2)), dumbo);
+  if (r > 4.0f * sj) {
+    const float t = sj * sj * invr2;
+    const float dumbo = kTaylorE + t * (kTaylorF + t * (kTaylorG + t * (kTaylorH + t * kTaylorHH)));
+    return t * sj * invr2 * invr2 * dumbo;
   }
-  if (!(far_x && far_y)) {
-    const float2 u = add2(f2(r), sj);
-    const float2 rms = sub2(f2(r), sj);
-    const float2 l = f2(fmaxf(rho.x, fabsf(rms.x)), fmaxf(rho.y, fabsf(rms.y)));
-    const bool in_x = -rms.x > rho.x;
-    const bool in_y = -rms.y > rho.y;
-    const float2 lam = f2((rms.x >= rho.x) ? 1.0f : (in_x ? -1.0f : 0.0f),
-                          (rms.y >= rho.y) ? 1.0f : (in_y ? -1.0f : 0.0f));
-    const float2 lu = mul2(l, u);
-    const float2 inv_lu = f2(__fdividef(1.0f, lu.x), __fdividef(1.0f, lu.y));
-    const float2 il = mul2(u, inv_lu);
-    const float2 iu = mul2(l, inv_lu);
-    const float2 il2 = mul2(il, il);
-    const float2 iu2 = mul2(iu, iu);
-    const float2 liu = mul2(l, iu);
-    const float2 lg = f2(__logf(liu.x), __logf(liu.y));
-    const float2 q2 = mul2(f2(0.5f * invr), sub2(sj2, f2(r2)));        // 2 q
-    const float2 dq = mul2(f2(-0.25f), fma2(sj2, f2(invr2), f2(1.0f)));
-    const float2 lil2 = mul2(lam, il2);
-    float2 di = sub2(iu2, lil2);
-    di = fma2(dq, sub2(il2, iu2), di);
-    di = fma2(q2, sub2(mul2(iu2, iu), mul2(lil2, il)), di);
-    di = fma2(f2(0.5f * invr), sub2(sub2(mul2(lam, il), iu), mul2(f2(invr), lg)), di);
-    di = sub2(mul2(f2(0.5f), di), f2(in_x ? il2.x : 0.0f, in_y ? il2.y : 0.0f));
-    const float2 v = mul2(di, f2(-invr));
-    vn = f2((rho.x < u.x) ? v.x : 0.0f, (rho.y < u.y) ? v.y : 0.0f);
-  }
-  return f2(far_x ? vf.x : vn.x, far_y ? vf.y : vn.y);
+  const float u = r + sj;
+  const float rms = r - sj;
+  const float l = fmaxf(rho, fabsf(rms));
+  const float lam = (rms >= rho) ? 1.0f : ((-rms > rho) ? -1.0f : 0.0f);
+  const float inv_lu = __fdividef(1.0f, l * u);
+  const float il = u * inv_lu;
+  const float iu = l * inv_lu;
+  const float il2 = il * il;
+  const float iu2 = iu * iu;
+  const float q = 0.25f * (sj * sj - r2) * invr;
+  const float dq = -0.25f * fmaf(sj * sj, invr2, 1.0f);
+  float di = -lam * il2 + iu2 + dq * (il2 - iu2) + 2.0f * q * (iu2 * iu - lam * il2 * il) +
+             0.5f * invr * (lam * il - iu - invr * __logf(l * iu));
+  di = 0.5f * di - ((-rms > rho) ? il2 : 0.0f);
+  return (rho < u) ? -di * invr : 0.0f;
 }
 
 // The HCT integral and its radial derivative together, for both directions of one pair (x for
@@ -912,9 +889,7 @@ struct PairPass {
   bool soft;        // softened cores on this tile
   float clash_d, clash_r;
   float2 qcore;
-  float2 fxyi, fxyj;   // x, y force sums: i side, traveling j side
-  float fzi, fzj;
-  float2 de2;          // dE/dR sums: i side, traveling j side
+  float fxi, fyi, fzi, dei, fxj, fyj, fzj, dej;
   float e_elec, e_vdw, e_gb;
   __device__ PairPass(const UnitSmem &s_in, float kappa, float inv_dielectric) :
       s(s_in), kk(-kappa * kGbKscale), inv_diel(inv_dielectric), salt(kappa > 0.0f) {}
@@ -931,18 +906,15 @@ struct PairPass {
       soft = (clash.x > 0.0f || clash.y > 0.0f);
       qcore = quadraticCore(clash.x);
     }
-    fxyi = fxyj = de2 = f2(0.0f);
-    fzi = fzj = 0.0f;
+    fxi = fyi = fzi = dei = 0.0f;
+    fxj = fyj = fzj = dej = 0.0f;
     e_elec = e_vdw = e_gb = 0.0f;
   }
   __device__ __forceinline__ void pair(int jslot, int jl) {
     const float4 aj = s.pa[jslot];
     const float4 bj = s.pb[jslot];
-    // x and y in packed FP32: the same roundings as the scalar forms
-    const float2 dxy = add2(sub2(f2(aj.x, aj.y), f2(ai.x, ai.y)),
-                            sub2(f2(bj.x, bj.y), f2(bi.x, bi.y)));
-    const float dz = (aj.z - ai.z) + (bj.z - bi.z);
-    const float r2 = fmaf(dxy.x, dxy.x, fmaf(dxy.y, dxy.y, dz * dz));
+    const float3 dv = pairDelta(ai, bi, aj, bj);
+    const float r2 = fmaf(dv.x, dv.x, fmaf(dv.y, dv.y, dv.z * dv.z));
     const float qiqj_all = ai.w * aj.w;
     float fmag = 0.0f;
     if (NB) {
@@ -996,24 +968,27 @@ struct PairPass {
         const float temp6 = qiqj * temp4 * fmaf(fgbk, expmkf, dielfac);
         fmag += temp6 * fmaf(-0.25f, efac, 1.0f);
         const float temp5 = 0.5f * efac * temp6 * fmaf(0.25f, r2, ijb);
-        de2 = fma2(f2(bi.w, bj.w), f2(temp5), de2);
+        dei = fmaf(bi.w, temp5, dei);
+        dej = fmaf(bj.w, temp5, dej);
       }
     }
     if (FORCE) {
-      fxyi = fma2(f2(fmag), dxy, fxyi);
-      fzi = fmaf(fmag, dz, fzi);
-      fxyj = fma2(f2(-fmag), dxy, fxyj);
-      fzj = fmaf(-fmag, dz, fzj);
+      fxi = fmaf(fmag, dv.x, fxi);
+      fyi = fmaf(fmag, dv.y, fyi);
+      fzi = fmaf(fmag, dv.z, fzi);
+      fxj = fmaf(-fmag, dv.x, fxj);
+      fyj = fmaf(-fmag, dv.y, fyj);
+      fzj = fmaf(-fmag, dv.z, fzj);
     }
   }
   __device__ __forceinline__ void rotate(int lane) {
     if (FORCE) {
       const int src = (lane + 1) & 31;
-      fxyj.x = __shfl_sync(kFullMask, fxyj.x, src);
-      fxyj.y = __shfl_sync(kFullMask, fxyj.y, src);
+      fxj = __shfl_sync(kFullMask, fxj, src);
+      fyj = __shfl_sync(kFullMask, fyj, src);
       fzj = __shfl_sync(kFullMask, fzj, src);
       if (GB) {
-        de2.y = __shfl_sync(kFullMask, de2.y, src);
+        dej = __shfl_sync(kFullMask, dej, src);
       }
     }
   }
@@ -1041,8 +1016,10 @@ struct DerivPass {
     const float r2 = fmaf(dv.x, dv.x, fmaf(dv.y, dv.y, dv.z * dv.z));
     const float invr = rsqrtf(r2);
     const float r = r2 * invr;
-    const float2 hd = hctDerivative2(r, r2, invr, f2(bi.w, bj.w), f2(aj.w, ai.w));
-    const float fmag = fmaf(hd.y, de_j, hd.x * de_i);
+    // scalar forms: on the long chains of the tiled path nearly every pair is far, and the
+    // packed pair form measured slower there
+    const float fmag = hctDerivative(r, r2, invr, bi.w, aj.w) * de_i +
+                       hctDerivative(r, r2, invr, bj.w, ai.w) * de_j;
     fxi = fmaf(-fmag, dv.x, fxi);
     fyi = fmaf(-fmag, dv.y, fyi);
     fzi = fmaf(-fmag, dv.z, fzi);
@@ -1217,17 +1194,17 @@ __device__ void pairTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u, 
     if (FORCE) {
       if (lane < ti.ni) {
         const int is = ti.ibase + lane;
-        addForce(s, is, p.fxyi.x, p.fxyi.y, p.fzi, fs);
+        addForce(s, is, p.fxi, p.fyi, p.fzi, fs);
         if (GB) {
-          atomicAddInt63(p.de2.x * ds, &s.de[is], &s.deo[is]);
+          atomicAddInt63(p.dei * ds, &s.de[is], &s.deo[is]);
         }
       }
       const int jl = traveledAtom(ti, lane);
       if (jl < ti.nj) {
         const int js = ti.jbase + jl;
-        addForce(s, js, p.fxyj.x, p.fxyj.y, p.fzj, fs);
+        addForce(s, js, p.fxj, p.fyj, p.fzj, fs);
         if (GB) {
-          atomicAddInt63(p.de2.y * ds, &s.de[js], &s.deo[js]);
+          atomicAddInt63(p.dej * ds, &s.de[js], &s.deo[js]);
         }
       }
     }
