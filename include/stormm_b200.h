@@ -53,6 +53,8 @@ extern "C" {
 #define SB_GB_HCT 1
 #define SB_GB_OBC 2
 #define SB_GB_OBC2 5
+#define SB_GB_NECK 7           /* Mongan's neck GB (GBn) */
+#define SB_GB_NECK2 8          /* neck GB model II (GBn2): element-specific alpha / beta / gamma */
 
 /* Energy slots per system, STORMM's StateVariable order (Potential/energy_enumerators.h:36-50) */
 #define SB_BOND 0
@@ -140,6 +142,13 @@ typedef struct {
                                   accumulation; SB_PRECISION_DOUBLE: FP64 arithmetic from double
                                   parameters (STORMM's PrecisionModel::DOUBLE), every molecule tile
                                   by tile; evaluation only */
+  /* Neck GB (igb 7, 8): STORMM's NeckGeneralizedBornTable, neck_table_size^2 maximum
+   * separations and values indexed [j_index * size + i_index], with the per-atom index
+   * round(20 (r_pb - 1)) (radii must lie in [1, 2] A); read by sb_synthesis_create */
+  const double* neck_max_separation;
+  const double* neck_max_value;
+  int neck_table_size;
+  double neck_cut;             /* neck cutoff, A (STORMM's default 6.8) */
 } sb_options;
 
 #define SB_PRECISION_SINGLE 0

@@ -45,7 +45,9 @@ class _System(ctypes.Structure):
         ("dihe_k", ctypes.c_void_p), ("dihe_l", ctypes.c_void_p), ("dihe_amp", ctypes.c_void_p),
         ("dihe_freq", ctypes.c_void_p), ("dihe_phase", ctypes.c_void_p),
         ("dihe_scee", ctypes.c_void_p), ("dihe_scnb", ctypes.c_void_p),
-        ("dihe_improper", ctypes.c_void_p),
+        ("dihe_improper", ctypes.c_void_p), ("neck_idx", ctypes.c_void_p),
+        ("neck_table_size", ctypes.c_int), ("neck_max_sep", ctypes.c_void_p),
+        ("neck_max_val", ctypes.c_void_p), ("neck_cut", ctypes.c_double),
     ]
 
 
@@ -92,12 +94,12 @@ class OracleSystem:
                 dt = np.int32 if name in ("lj_idx", "excl_bounds", "excl_list", "bond_i",
                                           "bond_j", "angl_i", "angl_j", "angl_k", "dihe_i",
                                           "dihe_j", "dihe_k", "dihe_l",
-                                          "dihe_improper") else np.float64
+                                          "dihe_improper", "neck_idx") else np.float64
                 a = np.ascontiguousarray(np.asarray(arrays[name]).reshape(-1), dtype=dt)
                 self._keep[name] = a
                 setattr(s, name, a.ctypes.data)
             else:
-                setattr(s, name, arrays[name])
+                setattr(s, name, arrays.get(name, 0))
         self.struct = s
         self.natom = int(arrays["natom"])
 
@@ -156,9 +158,15 @@ def from_fixture(g) -> OracleSystem:
         sets.append([x[b[i]:b[i + 1]] for i in range(n)])
     eb, el = _csr_from_sets(n, sets)
     igb_enum = int(g["igb"][0])
-    # STORMM's ImplicitSolventModel enumeration: NONE, HCT_GB, OBC_GB, OBC_GB_II, NECK_GB, ...
-    igb = {0: 0, 1: 1, 2: 2, 3: 5}[igb_enum]
-    return OracleSystem(
+    # STORMM's ImplicitSolventModel enumeration: NONE, HCT_GB, OBC_GB, OBC_GB_II, NECK_GB,
+    # NECK_GB_II
+    igb = {0: 0, 1: 1, 2: 2, 3: 5, 4: 7, 5: 8}[igb_enum]
+    neck = {}
+    if igb in (7, 8):
+        neck = dict(neck_idx=g["neck_gb_idx"], neck_table_size=int(g["neck_table_size"][0]),
+                    neck_max_sep=g["neck_max_sep"], neck_max_val=g["neck_max_val"],
+                    neck_cut=float(g["neck_cut"][0]))
+    return OracleSystem(**neck,
         natom=n, coulomb_constant=float(g["coulomb_constant"][0]), charge=g["charge"],
         lj_idx=g["lj_idx"], n_lj_types=int(g["n_lj_types"][0]), lja=g["lja"], ljb=g["ljb"],
         lja14=g["lja14"], ljb14=g["ljb14"], excl_bounds=eb, excl_list=el, igb=igb,
@@ -177,6 +185,8 @@ def from_fixture(g) -> OracleSystem:
 def from_molecule(m, igb: int = 5, dielectric: float = 80.0, saltcon: float = 0.0,
                   coulomb_constant: float = 332.0522172900000) -> OracleSystem:
     """Oracle system from a synthetic Molecule (OBC-II alpha/beta/gamma = 1.0, 0.8, 4.85)."""
+    if igb in (7, 8):
+        raise ValueError("neck GB needs the neck tables: build the oracle system from a fixture")
     n = m.natom
     eb, el = _csr_from_sets(n, [m.excl12, m.excl13, m.excl14])
     ab = {1: (0.0, 0.0, 0.0), 2: (0.8, 0.0, 2.909125), 5: (1.0, 0.8, 4.85)}.get(igb, (0, 0, 0))

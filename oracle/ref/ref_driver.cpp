@@ -256,6 +256,16 @@ void putTopology(RecordWriter *rw, const AtomGraph &ag) {
   rw->i("neck_gb_idx", isk.neck_gb_idx, n);
 }
 
+// The neck GB tables (Constants/generalized_born.h NeckGeneralizedBornTable) and cutoff, which
+// the neck models (igb 7, 8) look up by pairs of per-atom neck indices
+void putNeckTable(RecordWriter *rw, const NeckGeneralizedBornTable &tab) {
+  const NeckGeneralizedBornKit<double> k = tab.dpData();
+  rw->iscalar("neck_table_size", k.table_size);
+  rw->scalar("neck_cut", k.neck_cut);
+  rw->d("neck_max_sep", k.max_separation, static_cast<size_t>(k.table_size) * k.table_size);
+  rw->d("neck_max_val", k.max_value, static_cast<size_t>(k.table_size) * k.table_size);
+}
+
 void putExclusionMask(RecordWriter *rw, const StaticExclusionMask &se) {
   const StaticExclusionMaskReader ser = se.data();
   const int nst = ser.supertile_stride_count;
@@ -303,6 +313,7 @@ int runEval(const std::string &prmtop, const std::string &inpcrd, const std::str
   RecordWriter rw(out);
   putTopology(&rw, ag);
   putExclusionMask(&rw, se);
+  putNeckTable(&rw, ngb_tab);
   PhaseSpaceWriter psw = ps.data();
   putCoordinates(&rw, "coords", psw);
   const ValenceKit<double> vk = ag.getDoublePrecisionValenceKit();

@@ -365,9 +365,31 @@ static double hct_derivative(double r, double rho, double sj) {
   return 0.0;
 }
 
+/* Neck GB (Mongan's union of spheres, nonbonded_potential.tpp:678-702): the amount psi_i
+ * decreases by from neighbour j at distance r, and its radial derivative divided by r, both
+ * from the tables of maximum separation and maximum value for the pair of neck indices */
+static double neck_term(const orc_system* s, int i, int j, double r, double scale,
+                        double* deriv) {
+  const int t = s->neck_table_size * s->neck_idx[j] + s->neck_idx[i];
+  const double m = r - s->neck_max_sep[t];
+  const double m2 = m * m;
+  const double den = 1.0 + m2 + 0.3 * m2 * m2 * m2;
+  *deriv = ((2.0 * m + 1.8 * m2 * m2 * m) * s->neck_max_val[t] * scale) / (den * den * r);
+  return scale * s->neck_max_val[t] / den;
+}
+
+static int is_neck(int igb) { return igb == ORC_GB_NECK || igb == ORC_GB_NECK2; }
+
+/* Baseline radius offset and neck scale of the model (energy_abstracts.tpp:9-31) */
+static double gb_offset(int igb) { return (igb == ORC_GB_NECK2) ? 0.195141 : GB_RADII_OFFSET; }
+static double neck_scale(int igb) { return (igb == ORC_GB_NECK2) ? 0.826836 : 0.361825; }
+
 static void gb_terms(const orc_system* s, const double* c, double* f, double* e_gb,
                      double* psi_out, double* radii_out, double* sdeijda_out) {
   const int n = s->natom;
+  const double offset = gb_offset(s->igb);
+  const int neck = is_neck(s->igb);
+  const double nscale = neck_scale(s->igb);
   double* psi = (double*)calloc((size_t)n, sizeof(double));
   double* rad = (double*)calloc((size_t)n, sizeof(double));
   double* sde = (double*)calloc((size_t)n, sizeof(double));
@@ -376,22 +398,27 @@ static void gb_terms(const orc_system* s, const double* c, double* f, double* e_
 
   /* Pass 1: Born radius descreening sums (psi accumulates the negated integrals) */
   for (int i = 0; i < n; i++) {
-    const double rho_i = s->pb_radii[i] - GB_RADII_OFFSET;
+    const double rho_i = s->pb_radii[i] - offset;
     const double si = s->gb_screen[i] * rho_i;
     for (int j = i + 1; j < n; j++) {
-      const double rho_j = s->pb_radii[j] - GB_RADII_OFFSET;
+      const double rho_j = s->pb_radii[j] - offset;
       const double sj = s->gb_screen[j] * rho_j;
       double d[3];
       for (int a = 0; a < 3; a++) d[a] = c[3 * i + a] - c[3 * j + a];
       const double r = sqrt(dot3(d, d));
       psi[i] -= hct_integral(r, rho_i, sj);
       psi[j] -= hct_integral(r, rho_j, si);
+      if (neck && r < rho_i + rho_j + 2.0 * offset + s->neck_cut) {
+        double unused;
+        psi[i] -= neck_term(s, i, j, r, nscale, &unused);
+        psi[j] -= neck_term(s, j, i, r, nscale, &unused);
+      }
     }
   }
 
   /* Effective radii, nonbonded_potential.tpp:730-781 */
   for (int i = 0; i < n; i++) {
-    const double rho = s->pb_radii[i] - GB_RADII_OFFSET;
+    const double rho = s->pb_radii[i] - offset;
     if (s->igb == ORC_GB_HCT) {
       double egbi = 1.0 / (1.0 / rho + psi[i]);
       if (egbi < 0.0) egbi = 30.0;
@@ -452,7 +479,7 @@ static void gb_terms(const orc_system* s, const double* c, double* f, double* e_
   /* Chain-rule prefactor for the OBC radii, nonbonded_potential.tpp:994-1021 */
   if (s->igb != ORC_GB_HCT) {
     for (int i = 0; i < n; i++) {
-      const double rho = s->pb_radii[i] - GB_RADII_OFFSET;
+      const double rho = s->pb_radii[i] - offset;
       const double fipsi = psi[i] * (-rho);
       const double thi = tanh((s->gb_alpha[i] - (s->gb_beta[i] - s->gb_gamma[i] * fipsi) * fipsi) *
                               fipsi);
@@ -464,16 +491,23 @@ static void gb_terms(const orc_system* s, const double* c, double* f, double* e_
   /* Pass 3: radius chain-rule forces, nonbonded_potential.tpp:1098-1244 */
   if (f) {
     for (int i = 0; i < n; i++) {
-      const double rho_i = s->pb_radii[i] - GB_RADII_OFFSET;
+      const double rho_i = s->pb_radii[i] - offset;
       const double si = s->gb_screen[i] * rho_i;
       for (int j = i + 1; j < n; j++) {
-        const double rho_j = s->pb_radii[j] - GB_RADII_OFFSET;
+        const double rho_j = s->pb_radii[j] - offset;
         const double sj = s->gb_screen[j] * rho_j;
         double d[3];
         for (int a = 0; a < 3; a++) d[a] = c[3 * j + a] - c[3 * i + a];
         const double r = sqrt(dot3(d, d));
-        const double fmag = hct_derivative(r, rho_i, sj) * sde[i] +
-                            hct_derivative(r, rho_j, si) * sde[j];
+        double fmag = hct_derivative(r, rho_i, sj) * sde[i] +
+                      hct_derivative(r, rho_j, si) * sde[j];
+        if (neck && r < rho_i + rho_j + 2.0 * offset + s->neck_cut) {
+          /* nonbonded_potential.tpp:1219-1245 */
+          double dij, dji;
+          neck_term(s, i, j, r, nscale, &dij);
+          neck_term(s, j, i, r, nscale, &dji);
+          fmag += dij * sde[i] + dji * sde[j];
+        }
         for (int a = 0; a < 3; a++) {
           f[3 * i + a] -= fmag * d[a];
           f[3 * j + a] += fmag * d[a];

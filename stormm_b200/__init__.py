@@ -15,7 +15,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "libstormm_b200.so")
 
 SB_OK = 0
-SB_GB_NONE, SB_GB_HCT, SB_GB_OBC, SB_GB_OBC2 = 0, 1, 2, 5
+SB_GB_NONE, SB_GB_HCT, SB_GB_OBC, SB_GB_OBC2, SB_GB_NECK, SB_GB_NECK2 = 0, 1, 2, 5, 7, 8
 TERM_VALENCE, TERM_NONBONDED, TERM_GB, TERM_ALL = 1, 2, 4, 7
 TUNE_EVALUATE, TUNE_MINIMIZE = 1, 2
 MIN_GRAPH, MIN_PERSISTENT = 0, 1
@@ -53,6 +53,8 @@ class Options(ctypes.Structure):
         ("max_atoms_per_unit", ctypes.c_int), ("max_tiles_per_unit", ctypes.c_int),
         ("threads_per_block", ctypes.c_int), ("device", ctypes.c_int),
         ("tiled_above_atoms", ctypes.c_int), ("precision", ctypes.c_int),
+        ("neck_max_separation", ctypes.c_void_p), ("neck_max_value", ctypes.c_void_p),
+        ("neck_table_size", ctypes.c_int), ("neck_cut", ctypes.c_double),
     ]
 
 
@@ -177,10 +179,20 @@ def _check(rc: int, what: str) -> None:
 
 
 def default_options(**overrides) -> Options:
+    """sb_default_options with overrides by field name.  The neck GB tables
+    (neck_max_separation, neck_max_value) may be given as arrays; the returned Options keeps
+    them alive (sb_synthesis_create copies them)."""
     o = Options()
     library().sb_default_options(ctypes.byref(o))
+    keep = []
     for k, v in overrides.items():
+        if k in ("neck_max_separation", "neck_max_value") and v is not None and \
+                not isinstance(v, int):
+            a = np.ascontiguousarray(np.asarray(v, dtype=np.float64).reshape(-1))
+            keep.append(a)
+            v = a.ctypes.data
         setattr(o, k, v)
+    o._keep = keep
     return o
 
 

@@ -113,6 +113,16 @@ struct DevSynthesis {
   // from the base in its closing unit_meta row
   float2* pair_deriv;
 
+  // neck GB (igb 7, 8): per padded atom its table index, the tables (float), their size (0: not
+  // a neck model), and the model's neck scale, cutoff and baseline radius offset
+  const int* neck_idx;
+  const float* neck_sep;
+  const float* neck_val;
+  int neck_size;
+  float neck_scale;
+  float neck_cut;
+  float gb_offset;
+
   // clash damping of a launch (softened Coulomb and Lennard-Jones cores): clash distance (A) and
   // sigma ratio, off when both are 0.  With clash_cycle set (a minimization), system s uses them
   // scaled by (clash_cycles - c) / clash_cycles in its cycle c = clash_cycle[s], and not at all
@@ -162,6 +172,11 @@ struct DevPrecise {
   const double2* dihe_attn;      // 1 / scee, 1 / scnb of the attached 1-4 pair (0: none)
   double kappa;                  // Debye-Hueckel screening (1/A)
   double inv_dielectric;
+  const double* neck_sep;        // neck GB tables (DevSynthesis::neck_size entries squared)
+  const double* neck_val;
+  double neck_scale;
+  double neck_cut;
+  double gb_offset;
   double* radius;                // per padded atom: effective GB radius of the evaluation
   double* sde;                   // per padded atom: dE/dR after the chain-rule prefactor
 };

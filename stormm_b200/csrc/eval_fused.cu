@@ -62,6 +62,7 @@ kEvalFused(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
       const int k = findOwner(s.slot0, us.nsys, slot);
       const int a = slot - s.slot0[k];
       s.prm[slot] = slotParameters(d, s, k, a);
+      s.neck[slot] = slotNeck(d, s, k, a);
       const bool real = a < s.natom[k];
       const int gi = d.atom_start[s.sys[k]] + (real ? a : 0);
       placeSlot(d, s, slot, real, real ? d.xcrd[gi] : 0ll, real ? d.ycrd[gi] : 0ll,

@@ -43,6 +43,7 @@ constexpr double kNearToOne = 0.999999992549419403076171875;
 constexpr double kPi64 = 3.14159265358979323846;
 
 // A warp's staged tile: pa = (x, y, z, w1), pb = (w2, w3, -, -), code = Lennard-Jones type
+// (pass 2) or neck GB index (passes 1 and 3)
 struct Stage64 {
   double4* pa;
   double4* pb;
@@ -53,6 +54,26 @@ __device__ __forceinline__ Stage64 warpStage(double4* pa, double4* pb, int* code
   const int w = threadIdx.x >> 5;
   return Stage64{pa + w * kSlots64, pb + w * kSlots64, code + w * kSlots64};
 }
+
+// Neck GB terms in FP64 (nonbonded_potential.tpp:678-702, 1219-1245); size 0: not a neck model
+struct Neck64 {
+  const double* sep;
+  const double* val;
+  int size;
+  double scale;
+  double reach;    // 2 offset + cutoff
+  __device__ Neck64(const DevSynthesis &d, const DevPrecise &p) :
+      sep(p.neck_sep), val(p.neck_val), size(d.neck_size), scale(p.neck_scale),
+      reach(2.0 * p.gb_offset + p.neck_cut) {}
+  __device__ __forceinline__ double term(int ni, int nj, double r, double* deriv) const {
+    const int t = size * nj + ni;
+    const double m = r - sep[t];
+    const double m2 = m * m;
+    const double den = 1.0 + m2 + 0.3 * m2 * m2 * m2;
+    *deriv = ((2.0 * m + 1.8 * m2 * m2 * m) * val[t] * scale) / (den * den * r);
+    return scale * val[t] / den;
+  }
+};
 
 __device__ __forceinline__ void addFixed(long long* acc, double v) {
   atomicAdd(reinterpret_cast<unsigned long long*>(acc),
@@ -137,15 +158,18 @@ __device__ __forceinline__ double hctDerivative64(double r, double rho, double s
 // ------------------------------------------------------------------------------------------------
 // Pair functors for walkTile (lane l holds block I's atom, block J's atoms rotate)
 // ------------------------------------------------------------------------------------------------
-// Pass 1 payload: w1 = s * rho, w2 = rho
+// Pass 1 payload: w1 = s * rho, w2 = rho, code = neck index
 struct Radii64 {
   Stage64 v;
+  Neck64 neck;
   double4 ai, bi;
+  int ni;
   double psi_i, psi_j;
-  __device__ explicit Radii64(const Stage64 &v_in) : v(v_in) {}
+  __device__ Radii64(const Stage64 &v_in, const Neck64 &n) : v(v_in), neck(n) {}
   __device__ __forceinline__ void begin(int islot) {
     ai = v.pa[islot];
     bi = v.pb[islot];
+    ni = v.code[islot];
     psi_i = psi_j = 0.0;
   }
   __device__ __forceinline__ void pair(int jslot, int) {
@@ -155,6 +179,12 @@ struct Radii64 {
     const double r = sqrt(dx * dx + dy * dy + dz * dz);
     psi_i -= hctIntegral64(r, bi.x, aj.w);
     psi_j -= hctIntegral64(r, bj.x, ai.w);
+    if (neck.size > 0 && r < bi.x + bj.x + neck.reach) {
+      const int nj = v.code[jslot];
+      double unused;
+      psi_i -= neck.term(ni, nj, r, &unused);
+      psi_j -= neck.term(nj, ni, r, &unused);
+    }
   }
   __device__ __forceinline__ void rotate(int lane) {
     psi_j = __shfl_sync(0xffffffffu, psi_j, (lane + 1) & 31);
@@ -245,15 +275,19 @@ struct Pair64 {
   }
 };
 
-// Pass 3 payload: w1 = s * rho, w2 = rho, w3 = dE/dR after the chain-rule prefactor
+// Pass 3 payload: w1 = s * rho, w2 = rho, w3 = dE/dR after the chain-rule prefactor, code = neck
+// index
 struct Deriv64 {
   Stage64 v;
+  Neck64 neck;
   double4 ai, bi;
+  int ni;
   double fxi, fyi, fzi, fxj, fyj, fzj;
-  __device__ explicit Deriv64(const Stage64 &v_in) : v(v_in) {}
+  __device__ Deriv64(const Stage64 &v_in, const Neck64 &n) : v(v_in), neck(n) {}
   __device__ __forceinline__ void begin(int islot) {
     ai = v.pa[islot];
     bi = v.pb[islot];
+    ni = v.code[islot];
     fxi = fyi = fzi = fxj = fyj = fzj = 0.0;
   }
   __device__ __forceinline__ void pair(int jslot, int) {
@@ -261,7 +295,14 @@ struct Deriv64 {
     const double4 bj = v.pb[jslot];
     const double dx = aj.x - ai.x, dy = aj.y - ai.y, dz = aj.z - ai.z;
     const double r = sqrt(dx * dx + dy * dy + dz * dz);
-    const double fmag = hctDerivative64(r, bi.x, aj.w) * bi.y + hctDerivative64(r, bj.x, ai.w) * bj.y;
+    double fmag = hctDerivative64(r, bi.x, aj.w) * bi.y + hctDerivative64(r, bj.x, ai.w) * bj.y;
+    if (neck.size > 0 && r < bi.x + bj.x + neck.reach) {
+      const int nj = v.code[jslot];
+      double dij, dji;
+      neck.term(ni, nj, r, &dij);
+      neck.term(nj, ni, r, &dji);
+      fmag += dij * bi.y + dji * bj.y;
+    }
     fxi -= fmag * dx;
     fyi -= fmag * dy;
     fzi -= fmag * dz;
@@ -300,7 +341,7 @@ __device__ __forceinline__ void stageTile64(const DevSynthesis &d, const DevPrec
                         static_cast<double>(d.ycrd[gi]) * d.inv_gpos_scale,
                         static_cast<double>(d.zcrd[gi]) * d.inv_gpos_scale, 0.0);
       pb = make_double4(0.0, 0.0, 0.0, 0.0);
-      code = d.lj_idx[gi];
+      code = (PASS == 2) ? d.lj_idx[gi] : ((d.neck_size > 0) ? d.neck_idx[gi] : 0);
       if (PASS == 2) {
         pa.w = p.charge[gi];
         pb.x = p.radius[gi];
@@ -333,7 +374,7 @@ kRadii64(const DevSynthesis d, const DevPrecise p, const DevTiled t, int tile_be
   int first, last;
   warpTileRange(t, tile_begin, tile_end, &first, &last);
   const Stage64 v = warpStage(pa, pb, code);
-  Radii64 f(v);
+  Radii64 f(v, Neck64(d, p));
   for (int g = first; g < last; g++) {
     const int m = tiledOwner(t, g);
     const int sysid = t.systems[m];
@@ -427,7 +468,7 @@ kDeriv64(const DevSynthesis d, const DevPrecise p, const DevTiled t, int tile_be
   int first, last;
   warpTileRange(t, tile_begin, tile_end, &first, &last);
   const Stage64 v = warpStage(pa, pb, code);
-  Deriv64 f(v);
+  Deriv64 f(v, Neck64(d, p));
   for (int g = first; g < last; g++) {
     const int m = tiledOwner(t, g);
     const int sysid = t.systems[m];

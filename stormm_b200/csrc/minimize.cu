@@ -332,6 +332,7 @@ __device__ void minimizeUnit(const DevSynthesis &d, const DevMinimizer &m, const
   for (int slot = team.rank(); slot < us.nslots; slot += team.size()) {
     const int k = findOwner(s.slot0, us.nsys, slot);
     s.prm[slot] = slotParameters(d, s, k, slot - s.slot0[k]);
+    s.neck[slot] = slotNeck(d, s, k, slot - s.slot0[k]);
   }
   if (team.rank() < us.nsys) {
     const int k = team.rank();

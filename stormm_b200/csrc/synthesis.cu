@@ -75,12 +75,16 @@ void cudaCheck(cudaError_t err, const char* what) {
 namespace {
 
 double gbDefault(int igb, int which) {
-  // Constants/generalized_born.h:52-66 (OBC-I, OBC-II); HCT uses none of them
+  // Constants/generalized_born.h:52-75 (OBC-I, OBC-II, neck GB); HCT uses none of them, and neck
+  // GB II takes its element-specific values from the topology
   if (igb == SB_GB_OBC) {
     return (which == 0) ? 0.8 : (which == 1) ? 0.0 : 2.909125;
   }
   if (igb == SB_GB_OBC2) {
     return (which == 0) ? 1.0 : (which == 1) ? 0.8 : 4.85;
+  }
+  if (igb == SB_GB_NECK) {
+    return (which == 0) ? 1.09511284 : (which == 1) ? 1.90792938 : 2.50798245;
   }
   return 0.0;
 }
@@ -101,9 +105,16 @@ Synthesis::Synthesis(const sb_topology* tops, int ntop, const int* topology_inde
     throw Error(SB_ERR_ARGUMENT, "a synthesis needs at least one system and one topology");
   }
   if (opt.igb != SB_GB_NONE && opt.igb != SB_GB_HCT && opt.igb != SB_GB_OBC &&
-      opt.igb != SB_GB_OBC2) {
+      opt.igb != SB_GB_OBC2 && opt.igb != SB_GB_NECK && opt.igb != SB_GB_NECK2) {
     throw Error(SB_ERR_UNSUPPORTED, "implicit solvent model igb=" + std::to_string(opt.igb) +
-                " is not available on this path (supported: 0, 1, 2, 5)");
+                " is not available on this path (supported: 0, 1, 2, 5, 7, 8)");
+  }
+  // model constants of Potential/energy_abstracts.tpp:9-31
+  neck = (opt.igb == SB_GB_NECK || opt.igb == SB_GB_NECK2);
+  gb_offset = (opt.igb == SB_GB_NECK2) ? 0.195141 : 0.09;
+  if (neck && (opt.neck_max_separation == nullptr || opt.neck_max_value == nullptr ||
+               opt.neck_table_size < 1 || opt.neck_table_size > 64 || !(opt.neck_cut > 0.0))) {
+    throw Error(SB_ERR_ARGUMENT, "neck GB needs the neck tables (size 1-64) and a positive cutoff");
   }
   if (opt.gpos_bits < 24 || opt.gpos_bits > 40 || opt.frc_bits < 18 || opt.frc_bits > 40 ||
       opt.nrg_bits < 22 || opt.nrg_bits > 40) {
@@ -150,6 +161,9 @@ Synthesis::Synthesis(const sb_topology* tops, int ntop, const int* topology_inde
   buildLayout(tops, ntop);
   buildUnits();
   upload();
+  // the caller's tables were copied; keep no pointer to them
+  opt.neck_max_separation = nullptr;
+  opt.neck_max_value = nullptr;
 }
 
 void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
@@ -180,6 +194,14 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
   h_alpha.assign(np, 0.0f);
   h_beta.assign(np, 0.0f);
   h_gamma.assign(np, 0.0f);
+  if (neck) {
+    h_neck_idx.assign(np, 0);
+    const size_t nt2 = static_cast<size_t>(opt.neck_table_size) * opt.neck_table_size;
+    h64_neck_sep.assign(opt.neck_max_separation, opt.neck_max_separation + nt2);
+    h64_neck_val.assign(opt.neck_max_value, opt.neck_max_value + nt2);
+    h_neck_sep.assign(h64_neck_sep.begin(), h64_neck_sep.end());
+    h_neck_val.assign(h64_neck_val.begin(), h64_neck_val.end());
+  }
   if (fp64) {
     h64_charge.assign(np, 0.0);
     h64_rho.assign(np, 1.0);
@@ -286,7 +308,7 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
       }
       h_ljidx[base + i] = tp.lj_idx[i];
       if (opt.igb != SB_GB_NONE) {
-        const double rho = tp.pb_radii[i] - 0.09;
+        const double rho = tp.pb_radii[i] - gb_offset;
         h_rho[base + i] = static_cast<float>(rho);
         h_srho[base + i] = static_cast<float>(tp.gb_screen[i] * rho);
         h_pb[base + i] = static_cast<float>(tp.pb_radii[i]);
@@ -294,10 +316,24 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
         h_beta[base + i] = static_cast<float>(tp.gb_beta ? tp.gb_beta[i] : gbDefault(opt.igb, 1));
         h_gamma[base + i] = static_cast<float>(tp.gb_gamma ? tp.gb_gamma[i] : gbDefault(opt.igb, 2));
       }
+      if (neck) {
+        // AtomGraph::setImplicitSolventModel (Topology/atomgraph_setters.cpp:1088-1092)
+        const int idx = static_cast<int>(((tp.pb_radii[i] - 1.0) * 20.0) + 0.5);
+        if (idx < 0 || idx >= opt.neck_table_size) {
+          throw Error(SB_ERR_ARGUMENT, "neck GB needs intrinsic radii within the neck tables "
+                      "(1-2 A for STORMM's 21 x 21 tables)");
+        }
+        if (opt.igb == SB_GB_NECK2 && (tp.gb_alpha == nullptr || tp.gb_beta == nullptr ||
+                                        tp.gb_gamma == nullptr)) {
+          throw Error(SB_ERR_ARGUMENT, "neck GB II takes element-specific alpha, beta and gamma "
+                      "from the topology");
+        }
+        h_neck_idx[base + i] = idx;
+      }
       if (fp64) {
         h64_charge[base + i] = tp.charge[i] * sqrt_kc;
         if (opt.igb != SB_GB_NONE) {
-          const double rho = tp.pb_radii[i] - 0.09;
+          const double rho = tp.pb_radii[i] - gb_offset;
           h64_rho[base + i] = rho;
           h64_srho[base + i] = tp.gb_screen[i] * rho;
           h64_pb[base + i] = tp.pb_radii[i];
@@ -635,6 +671,15 @@ void Synthesis::upload() {
     dev64.inv_dielectric = 1.0 / opt.dielectric;
     dev64.radius = d64_radius.p;
     dev64.sde = d64_sde.p;
+    dev64.gb_offset = gb_offset;
+    if (neck) {
+      d64_neck_sep.upload(h64_neck_sep);
+      d64_neck_val.upload(h64_neck_val);
+      dev64.neck_sep = d64_neck_sep.p;
+      dev64.neck_val = d64_neck_val.p;
+      dev64.neck_scale = (opt.igb == SB_GB_NECK2) ? 0.826836 : 0.361825;
+      dev64.neck_cut = opt.neck_cut;
+    }
   }
   dev_tiled.nmol = static_cast<int>(h_tiled_systems.size());
   dev_tiled.ntiles = h_tile_prefix.back();
@@ -670,6 +715,11 @@ void Synthesis::upload() {
   d_status.zeros(1);
   // one tile beyond the last unit's, so no store or load of a tile walk can leave the buffer
   d_pair_deriv.zeros(static_cast<size_t>(fused_tiles + 1) * kPairDerivPerTile);
+  if (neck) {
+    d_neck_idx.upload(h_neck_idx);
+    d_neck_sep.upload(h_neck_sep);
+    d_neck_val.upload(h_neck_val);
+  }
 
   DevSynthesis &d = dev;
   std::memset(&d, 0, sizeof(DevSynthesis));
@@ -726,6 +776,15 @@ void Synthesis::upload() {
   d.unit_meta = eval_plan->d_meta.p;
   d.max_unit_slots = max_unit_slots;
   d.pair_deriv = d_pair_deriv.p;
+  d.gb_offset = static_cast<float>(gb_offset);
+  if (neck) {
+    d.neck_idx = d_neck_idx.p;
+    d.neck_sep = d_neck_sep.p;
+    d.neck_val = d_neck_val.p;
+    d.neck_size = opt.neck_table_size;
+    d.neck_scale = static_cast<float>((opt.igb == SB_GB_NECK2) ? 0.826836 : 0.361825);
+    d.neck_cut = static_cast<float>(opt.neck_cut);
+  }
   d.status = d_status.p;
 }
 

@@ -194,6 +194,14 @@ public:
   DeviceArray<int> d_psi_ovrf, d_sumdeijda_ovrf, d_status;
   DeviceArray<float> d_born_radii;
   DeviceArray<float2> d_pair_deriv;
+  std::vector<int> h_neck_idx;
+  std::vector<float> h_neck_sep, h_neck_val;
+  std::vector<double> h64_neck_sep, h64_neck_val;
+  DeviceArray<int> d_neck_idx;
+  DeviceArray<float> d_neck_sep, d_neck_val;
+  DeviceArray<double> d64_neck_sep, d64_neck_val;
+  double gb_offset = 0.09;       // baseline radius offset of the GB model
+  bool neck = false;
   int fused_tiles = 0;           // tiles of all molecules on the fused path
   DeviceArray<int> d_unpadded_map;
   DeviceArray<double> d_stage_xyz, d_stage_nrg;

@@ -177,18 +177,20 @@ __device__ __forceinline__ void stageTile(const DevSynthesis &d, const DevTiled 
     v.pb[slot] = pb;
     v.prm[slot] = prm;
     v.gbv[slot] = gbv;
+    v.neck[slot] = (d.neck_size > 0 && a < natom) ? d.neck_idx[base + a] : 0;
   }
   __syncwarp();
 }
 
 __device__ __forceinline__ UnitSmem warpView(float4* pa, float4* pb, float4* prm, float2* gbv,
-                                             const float2* lj) {
+                                             int* neck, const float2* lj) {
   UnitSmem v{};
   const int w = threadIdx.x >> 5;
   v.pa = pa + w * kStageSlots;
   v.pb = pb + w * kStageSlots;
   v.prm = prm + w * kStageSlots;
   v.gbv = gbv + w * kStageSlots;
+  v.neck = neck + w * kStageSlots;
   v.lj = const_cast<float2*>(lj);
   return v;
 }
@@ -199,17 +201,19 @@ __device__ __forceinline__ void addGlobal(long long* acc, float v) {
 }
 
 // GB pass 1 over tiles [tile_begin, tile_end)
+template <bool NECK>
 __global__ void __launch_bounds__(256, 4)
 kTiledRadii(const DevSynthesis d, const DevTiled t, int tile_begin, int tile_end) {
   __shared__ float4 pa[kTiledWarps * kStageSlots], pb[kTiledWarps * kStageSlots];
   __shared__ float4 prm[kTiledWarps * kStageSlots];
   __shared__ float2 gbv[kTiledWarps * kStageSlots];
+  __shared__ int neck[kTiledWarps * kStageSlots];
   const int lane = threadIdx.x & 31;
   const float ps = static_cast<float>(1 << kPsiBits);
   int first, last;
   warpTileRange(t, tile_begin, tile_end, &first, &last);
-  const UnitSmem v = warpView(pa, pb, prm, gbv, d.ljab);
-  RadiiPass2 p(v);
+  const UnitSmem v = warpView(pa, pb, prm, gbv, neck, d.ljab);
+  RadiiPass2<NECK> p(v, d);
   for (int g = first; g < last; g++) {
     const int m = tiledOwner(t, g);
     const int sysid = t.systems[m];
@@ -237,6 +241,7 @@ kTiledPair(const DevSynthesis d, const DevTiled t, int tile_begin, int tile_end)
   __shared__ float4 pa[kTiledWarps * kStageSlots], pb[kTiledWarps * kStageSlots];
   __shared__ float4 prm[kTiledWarps * kStageSlots];
   __shared__ float2 gbv[kTiledWarps * kStageSlots];
+  __shared__ int neck[kTiledWarps * kStageSlots];
   const int lane = threadIdx.x & 31;
   const float fs = d.frc_scale;
   const float es = d.nrg_scale;
@@ -267,7 +272,7 @@ kTiledPair(const DevSynthesis d, const DevTiled t, int tile_begin, int tile_end)
     }
     int I, J;
     const TileInfo ti = tiledTileInfo(d, sysid, g - t.tile_prefix[m], &I, &J);
-    const UnitSmem v = warpView(pa, pb, prm, gbv, d.ljab + d.lj_start[sysid]);
+    const UnitSmem v = warpView(pa, pb, prm, gbv, neck, d.ljab + d.lj_start[sysid]);
     stageTile<2, GB>(d, t, v, sysid, I, J, ti.diag, lane);
     unsigned mask = 0u;
     if (NB) {
@@ -319,17 +324,19 @@ kTiledPair(const DevSynthesis d, const DevTiled t, int tile_begin, int tile_end)
 }
 
 // Pass 3 (radius chain-rule forces) over tiles [tile_begin, tile_end)
+template <bool NECK>
 __global__ void __launch_bounds__(256, 4)
 kTiledDeriv(const DevSynthesis d, const DevTiled t, int tile_begin, int tile_end) {
   __shared__ float4 pa[kTiledWarps * kStageSlots], pb[kTiledWarps * kStageSlots];
   __shared__ float4 prm[kTiledWarps * kStageSlots];
   __shared__ float2 gbv[kTiledWarps * kStageSlots];
+  __shared__ int neck[kTiledWarps * kStageSlots];
   const int lane = threadIdx.x & 31;
   const float fs = d.frc_scale;
   int first, last;
   warpTileRange(t, tile_begin, tile_end, &first, &last);
-  const UnitSmem v = warpView(pa, pb, prm, gbv, d.ljab);
-  DerivPass p(v);
+  const UnitSmem v = warpView(pa, pb, prm, gbv, neck, d.ljab);
+  DerivPass<NECK> p(v, d);
   for (int g = first; g < last; g++) {
     const int m = tiledOwner(t, g);
     const int sysid = t.systems[m];
@@ -449,7 +456,8 @@ cudaError_t launchTiled(const DevSynthesis &d, const DevTiled &t, const int* h_t
 #undef SB_VALE
   }
   if (gb) {
-    kTiledRadii<<<tgrid, 256, 0, stream>>>(d, t, tb, te);
+    if (d.neck_size > 0) kTiledRadii<true><<<tgrid, 256, 0, stream>>>(d, t, tb, te);
+    else kTiledRadii<false><<<tgrid, 256, 0, stream>>>(d, t, tb, te);
 #define SB_ATOMS(F, E) \
     if (workspace) kTiledAtoms<F, E, true><<<agrid, 256, 0, stream>>>(d, t, ab, ae); \
     else kTiledAtoms<F, E, false><<<agrid, 256, 0, stream>>>(d, t, ab, ae);
@@ -478,7 +486,8 @@ cudaError_t launchTiled(const DevSynthesis &d, const DevTiled &t, const int* h_t
   if (gb && force) {
     if (workspace) kTiledChain<true><<<agrid, 256, 0, stream>>>(d, t, ab, ae);
     else kTiledChain<false><<<agrid, 256, 0, stream>>>(d, t, ab, ae);
-    kTiledDeriv<<<tgrid, 256, 0, stream>>>(d, t, tb, te);
+    if (d.neck_size > 0) kTiledDeriv<true><<<tgrid, 256, 0, stream>>>(d, t, tb, te);
+    else kTiledDeriv<false><<<tgrid, 256, 0, stream>>>(d, t, tb, te);
   }
   return cudaGetLastError();
 }

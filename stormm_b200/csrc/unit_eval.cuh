@@ -287,6 +287,37 @@ __device__ __forceinline__ void hctBoth2(float r, float r2, float invr, float2 r
   *deriv = f2(far_x ? vfd.x : vnd.x, far_y ? vfd.y : vnd.y);
 }
 
+// Neck GB (Mongan's neck between two spheres, nonbonded_potential.tpp:678-702, 1219-1245): pairs
+// closer than rho_i + rho_j + 2 offset + cutoff add scale * V / (1 + m^2 + 0.3 m^6), m = r - S,
+// to the descreening, with V and S looked up for the pair's neck indices
+struct NeckGb {
+  const float* sep;
+  const float* val;
+  int size;
+  float scale;
+  float reach;     // 2 offset + cutoff: the pair takes the neck term when r < rho_i + rho_j + reach
+  __device__ explicit NeckGb(const DevSynthesis &d) :
+      sep(d.neck_sep), val(d.neck_val), size(d.neck_size), scale(d.neck_scale),
+      reach(2.0f * d.gb_offset + d.neck_cut) {}
+  // the amount psi of the atom with index ni decreases by from the atom with index nj
+  __device__ __forceinline__ float integral(int ni, int nj, float r) const {
+    const int t = size * nj + ni;
+    const float m = r - __ldg(&sep[t]);
+    const float m2 = m * m;
+    return __fdividef(scale * __ldg(&val[t]), 1.0f + m2 + 0.3f * m2 * m2 * m2);
+  }
+  // the same and its radial derivative factor -(1/r) dI/dr, as hctDerivative
+  __device__ __forceinline__ float both(int ni, int nj, float r, float invr, float* deriv) const {
+    const int t = size * nj + ni;
+    const float m = r - __ldg(&sep[t]);
+    const float m2 = m * m;
+    const float v = scale * __ldg(&val[t]);
+    const float inv_den = __fdividef(1.0f, 1.0f + m2 + 0.3f * m2 * m2 * m2);
+    *deriv = (2.0f * m + 1.8f * m2 * m2 * m) * v * inv_den * inv_den * invr;
+    return v * inv_den;
+  }
+};
+
 // Shared-memory layout of one work unit
 struct UnitSmem {
   float4* pa;       // x_hi, y_hi, z_hi, pass payload w1
@@ -303,6 +334,7 @@ struct UnitSmem {
   int* psio;
   int* de;          // int63 dE/dR accumulator, 2^kDeijdaBits
   int* deo;
+  int* neck;        // neck GB table index of the atom
   float2* lj;       // Lennard-Jones tables of the unit's molecules (standard, then 1-4)
   unsigned long long* nrg;   // per unit molecule energies
   int* sys;         // molecule index
@@ -318,7 +350,7 @@ struct UnitSmem {
 
 __host__ __device__ inline size_t alignUp(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-constexpr int kSlotBytes = 3 * 16 + 8 + 10 * 4;
+constexpr int kSlotBytes = 3 * 16 + 8 + 11 * 4;
 
 // Dynamic shared memory of one work unit's evaluation: max_slots atom slots, max_lj table entries
 __host__ __device__ inline size_t unitSmemBytes(int max_slots, int max_lj,
@@ -352,7 +384,8 @@ __device__ UnitSmem carveSmem(char* base, int max_slots, int max_lj,
   s.psio = ip; ip += max_slots;
   s.de = ip; ip += max_slots;
   s.deo = ip; ip += max_slots;
-  off = alignUp(off + 10 * sizeof(int) * max_slots, 16);
+  s.neck = ip; ip += max_slots;
+  off = alignUp(off + 11 * sizeof(int) * max_slots, 16);
   s.lj = reinterpret_cast<float2*>(base + off); off += sizeof(float2) * max_lj;
   off = alignUp(off, 16);
   s.nrg = reinterpret_cast<unsigned long long*>(base + off);
@@ -834,16 +867,22 @@ __device__ __forceinline__ int traveledAtom(const TileInfo &ti, int lane) {
 
 // GB pass 1, two pairs per lane per step: psi_i -= H(r, rho_i, s_j rho_j) and
 // psi_j -= H(r, rho_j, s_i rho_i)
+template <bool NECK = false>
 struct RadiiPass2 {
   const UnitSmem &s;
+  NeckGb neck;
   float4 ai, bi;
+  int ni;           // neck index of atom i
   float2 psi_i2;    // i-side sums of the two pair streams
   float2 psi_j;     // traveling j-side sums: x for stream 1, y for stream 2
   float psi_i, psi_j1;
-  __device__ RadiiPass2(const UnitSmem &s_in) : s(s_in) {}
+  __device__ RadiiPass2(const UnitSmem &s_in, const DevSynthesis &d) : s(s_in), neck(d) {}
   __device__ __forceinline__ void begin(int islot) {
     ai = s.pa[islot];
     bi = s.pb[islot];
+    if (NECK) {
+      ni = s.neck[islot];
+    }
     psi_i2 = f2(0.0f);
     psi_j = f2(0.0f);
   }
@@ -858,8 +897,20 @@ struct RadiiPass2 {
     const float2 r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
     const float2 invr = f2(rsqrtf(r2.x), rsqrtf(r2.y));
     const float2 r = mul2(r2, invr);
-    const float2 hi = hctIntegral2(r, r2, invr, f2(bi.w), f2(aj1.w, aj2.w));
-    const float2 hj = hctIntegral2(r, r2, invr, f2(bj1.w, bj2.w), f2(ai.w));
+    float2 hi = hctIntegral2(r, r2, invr, f2(bi.w), f2(aj1.w, aj2.w));
+    float2 hj = hctIntegral2(r, r2, invr, f2(bj1.w, bj2.w), f2(ai.w));
+    if (NECK) {
+      if (r.x < bi.w + bj1.w + neck.reach) {
+        const int nj = s.neck[js1];
+        hi.x += neck.integral(ni, nj, r.x);
+        hj.x += neck.integral(nj, ni, r.x);
+      }
+      if (r.y < bi.w + bj2.w + neck.reach) {
+        const int nj = s.neck[js2];
+        hi.y += neck.integral(ni, nj, r.y);
+        hj.y += neck.integral(nj, ni, r.y);
+      }
+    }
     const float2 wneg = f2(-1.0f, -w2);
     psi_i2 = fma2(hi, wneg, psi_i2);
     psi_j = fma2(hj, wneg, psi_j);
@@ -995,15 +1046,21 @@ struct PairPass {
 };
 
 // Pass 3: radius chain-rule forces
+template <bool NECK = false>
 struct DerivPass {
   const UnitSmem &s;
+  NeckGb neck;
   float4 ai, bi;
+  int ni;
   float de_i;
   float fxi, fyi, fzi, fxj, fyj, fzj;
-  __device__ DerivPass(const UnitSmem &s_in) : s(s_in) {}
+  __device__ DerivPass(const UnitSmem &s_in, const DevSynthesis &d) : s(s_in), neck(d) {}
   __device__ __forceinline__ void begin(int islot) {
     ai = s.pa[islot];
     bi = s.pb[islot];
+    if (NECK) {
+      ni = s.neck[islot];
+    }
     de_i = s.gbv[islot].y;
     fxi = fyi = fzi = 0.0f;
     fxj = fyj = fzj = 0.0f;
@@ -1018,8 +1075,15 @@ struct DerivPass {
     const float r = r2 * invr;
     // scalar forms: on the long chains of the tiled path nearly every pair is far, and the
     // packed pair form measured slower there
-    const float fmag = hctDerivative(r, r2, invr, bi.w, aj.w) * de_i +
-                       hctDerivative(r, r2, invr, bj.w, ai.w) * de_j;
+    float fmag = hctDerivative(r, r2, invr, bi.w, aj.w) * de_i +
+                 hctDerivative(r, r2, invr, bj.w, ai.w) * de_j;
+    if (NECK && r < bi.w + bj.w + neck.reach) {
+      const int nj = s.neck[jslot];
+      float dij, dji;
+      neck.both(ni, nj, r, invr, &dij);
+      neck.both(nj, ni, r, invr, &dji);
+      fmag += dij * de_i + dji * de_j;
+    }
     fxi = fmaf(-fmag, dv.x, fxi);
     fyi = fmaf(-fmag, dv.y, fyi);
     fzi = fmaf(-fmag, dv.z, fzi);
@@ -1038,15 +1102,21 @@ struct DerivPass {
 // GB pass 1 of a force evaluation: psi_i -= H(r, rho_i, s_j rho_j), psi_j -= H(r, rho_j,
 // s_i rho_i), and the radial derivatives of both terms stored for pass 3 (one float2 per lane
 // and step of the tile walk, so the stores of a step are one coalesced 256-byte line)
+template <bool NECK = false>
 struct RadiiDerivPass {
   const UnitSmem &s;
+  NeckGb neck;
   float4 ai, bi;
+  int ni;
   float psi_i, psi_j;   // i-side sum, traveling j-side sum
   float2* out;          // this lane's entry for the current step
-  __device__ RadiiDerivPass(const UnitSmem &s_in) : s(s_in) {}
+  __device__ RadiiDerivPass(const UnitSmem &s_in, const DevSynthesis &d) : s(s_in), neck(d) {}
   __device__ __forceinline__ void begin(int islot, float2* tile_out) {
     ai = s.pa[islot];
     bi = s.pb[islot];
+    if (NECK) {
+      ni = s.neck[islot];
+    }
     psi_i = 0.0f;
     psi_j = 0.0f;
     out = tile_out;
@@ -1062,6 +1132,14 @@ struct RadiiDerivPass {
     const float r = r2 * invr;
     float2 h, hd;
     hctBoth2(r, r2, invr, f2(bi.w, bj.w), f2(aj.w, ai.w), &h, &hd);
+    if (NECK && r < bi.w + bj.w + neck.reach) {
+      const int nj = s.neck[jslot];
+      float dij, dji;
+      h.x += neck.both(ni, nj, r, invr, &dij);
+      h.y += neck.both(nj, ni, r, invr, &dji);
+      hd.x += dij;
+      hd.y += dji;
+    }
     psi_i -= h.x;
     psi_j -= h.y;
     __stcg(out, hd);
@@ -1118,13 +1196,13 @@ __device__ __forceinline__ size_t pairDerivOffset(int tile_base, int t) {
   return static_cast<size_t>(tile_base + t) * kPairDerivPerTile;
 }
 
-template <bool STORE>
+template <bool STORE, bool NECK>
 __device__ void gbRadiiTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u, int ntiles,
                              int tile_base, int first, int stride) {
   const int lane = threadIdx.x & 31;
   const float ps = static_cast<float>(1 << kPsiBits);
   if (STORE) {
-    RadiiDerivPass p(s);
+    RadiiDerivPass<NECK> p(s, d);
     for (int t = first; t < ntiles; t += stride) {
       const TileInfo ti = tileInfo(s, nsys_u, t);
       p.begin(ti.ibase + lane, d.pair_deriv + pairDerivOffset(tile_base, t) + lane);
@@ -1139,7 +1217,7 @@ __device__ void gbRadiiTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_
     }
     return;
   }
-  RadiiPass2 p(s);
+  RadiiPass2<NECK> p(s, d);
   for (int t = first; t < ntiles; t += stride) {
     const TileInfo ti = tileInfo(s, nsys_u, t);
     p.begin(ti.ibase + lane);
@@ -1369,6 +1447,11 @@ __device__ __forceinline__ float4 slotParameters(const DevSynthesis &d, const Un
   return make_float4(0.0f, __int_as_float(s.ljbase[k]), 1.0f, 0.0f);
 }
 
+// Neck GB table index of slot a of unit molecule k (0 for padding or other GB models)
+__device__ __forceinline__ int slotNeck(const DevSynthesis &d, const UnitSmem &s, int k, int a) {
+  return (d.neck_size > 0 && a < s.natom[k]) ? d.neck_idx[d.atom_start[s.sys[k]] + a] : 0;
+}
+
 // Place an atom (fixed-point coordinates c, real = true) or a padding slot (far from everything:
 // 16 A apart along x beyond 5000 A) and clear its accumulators for a new evaluation
 __device__ __forceinline__ void placeSlot(const DevSynthesis &d, const UnitSmem &s, int slot,
@@ -1431,7 +1514,12 @@ __device__ void evaluateStaged(const DevSynthesis &d, const UnitSmem &s, const U
     }
   }
   if (gb) {
-    gbRadiiTiles<FORCE>(d, s, nsys_u, ntiles, us.tile_base, team.warp(), team.warps());
+    if (d.neck_size > 0) {
+      gbRadiiTiles<FORCE, true>(d, s, nsys_u, ntiles, us.tile_base, team.warp(), team.warps());
+    }
+    else {
+      gbRadiiTiles<FORCE, false>(d, s, nsys_u, ntiles, us.tile_base, team.warp(), team.warps());
+    }
     team.sync();
     // effective radii, self terms (nonbonded_potential.tpp:730-805); a warp's 32 slots
     // belong to one molecule, so the self energies reduce across the warp

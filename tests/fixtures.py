@@ -68,7 +68,19 @@ def molecule_from_fixture(g):
 
 def igb_of_fixture(g):
     """Amber igb number of the fixture's implicit solvent model (STORMM enum order)."""
-    return {0: 0, 1: 1, 2: 2, 3: 5}[int(g["igb"][0])]
+    return {0: 0, 1: 1, 2: 2, 3: 5, 4: 7, 5: 8}[int(g["igb"][0])]
+
+
+def solvent_options(g):
+    """Synthesis options of the fixture's solvent model: igb, dielectric, salt and, for the neck
+    models, the neck tables STORMM used."""
+    opts = dict(igb=igb_of_fixture(g), dielectric=float(g["dielectric"][0]),
+                saltcon=float(g["saltcon"][0]))
+    if opts["igb"] in (7, 8):
+        opts.update(neck_max_separation=g["neck_max_sep"], neck_max_value=g["neck_max_val"],
+                    neck_table_size=int(g["neck_table_size"][0]),
+                    neck_cut=float(g["neck_cut"][0]))
+    return opts
 
 
 def reference_forces(g):

@@ -17,6 +17,9 @@ Fixtures written (numpy .npz, one per case):
   known-answer GB energies that test file asserts.
 * ``synthetic_{S64,H100,O100,V100}.npz``: solvent-model variants (salt 0.15 M with dielectric
   78.5; HCT; OBC-I with dielectric 40; vacuum), run with ``--variants-only`` on its own.
+* ``synthetic_N7.npz``, ``synthetic_N8.npz`` and ``reference_*_igb{7,8}.npz``
+  (``--neck-only``): the neck GB models (Mongan's GBn and GBn2) on an 80-atom molecule and the
+  reference systems, with the neck tables STORMM looked the pairs up in.
 * ``minimize_m0.npz``: STORMM's CPU line minimizer (MolecularMechanics/minimization.tpp) on the
   64-atom molecule, energy history and final coordinates.
 * ``synthetic_K64.npz`` and ``minimize_clash_k64.npz`` (``--clash-only``): a 64-atom molecule
@@ -96,10 +99,20 @@ def main():
                     help="write only the solvent-model variant fixtures")
     ap.add_argument("--clash-only", action="store_true",
                     help="write only the clash-damping fixtures")
+    ap.add_argument("--neck-only", action="store_true",
+                    help="write only the neck GB (igb 7, 8) fixtures")
     args = ap.parse_args()
     if not os.path.exists(DRIVER):
         raise SystemExit("build the reference driver first: make -C oracle/ref -j8")
     with tempfile.TemporaryDirectory() as tmp:
+        if args.neck_only:
+            for name, seed, n, igb in (("N7", 8820, 80, "7"), ("N8", 8821, 80, "8")):
+                mol = synthetic.make_molecule(seed, n, noise=0.1, name=name)
+                rec, _, _ = eval_molecule(mol, tmp, ["--igb", igb])
+                np.savez_compressed(os.path.join(HERE, f"synthetic_{name}.npz"), **rec)
+                print("wrote", name, rec["energy_terms"])
+            reference_systems(args.reference_root, tmp, ((7, "neck"), (8, "neck2")))
+            return
         if args.clash_only:
             mol = synthetic.make_molecule(8810, 64, noise=0.45, name="K64")
             rec, top, crd = eval_molecule(mol, tmp, ["--clash-r0", "1.5", "--clash-ratio", "0.9"])
@@ -145,22 +158,27 @@ def main():
                 print("wrote minimize_m0", mrec["min_potential_history"][[0, -1]])
 
         # 2. the reference's own GB test systems with its known answers
-        answers = gb_known_answers(args.reference_root)
-        tdir = os.path.join(args.reference_root, "test")
-        systems = {"trpcage": ("trpcage.top", "trpcage.inpcrd", 1.2, 2.0, 0),
-                   "ala_dipeptide": ("ala_dipeptide.top", "ala_dipeptide.inpcrd", 1.2, 2.0, 2)}
-        for sname, (tf, cf, scee, scnb, ans_idx) in systems.items():
-            for igb, key in ((1, "hct"), (2, "obc"), (5, "obc2")):
-                out = os.path.join(tmp, f"{sname}_{igb}.bin")
-                run_driver(["eval", os.path.join(tdir, "Topology", tf),
-                            os.path.join(tdir, "Trajectory", cf), out, "--igb", str(igb),
-                            "--diel", "78.5", "--qtol", "1e-10",
-                            "--qdisc", "9.31322574615478515625E-10",
-                            "--scee", str(scee), "--scnb", str(scnb)])
-                rec = read_records(out)
-                rec["known_answer_gb"] = np.array([answers[key][ans_idx]])
-                np.savez_compressed(os.path.join(HERE, f"reference_{sname}_igb{igb}.npz"), **rec)
-                print("wrote", sname, igb, rec["energy_terms"][-1], answers[key][ans_idx])
+        reference_systems(args.reference_root, tmp, ((1, "hct"), (2, "obc"), (5, "obc2")))
+
+
+def reference_systems(ref_root, tmp, models):
+    """Trp-cage and alanine dipeptide under the given (igb, known-answer key) models."""
+    answers = gb_known_answers(ref_root)
+    tdir = os.path.join(ref_root, "test")
+    systems = {"trpcage": ("trpcage.top", "trpcage.inpcrd", 1.2, 2.0, 0),
+               "ala_dipeptide": ("ala_dipeptide.top", "ala_dipeptide.inpcrd", 1.2, 2.0, 2)}
+    for sname, (tf, cf, scee, scnb, ans_idx) in systems.items():
+        for igb, key in models:
+            out = os.path.join(tmp, f"{sname}_{igb}.bin")
+            run_driver(["eval", os.path.join(tdir, "Topology", tf),
+                        os.path.join(tdir, "Trajectory", cf), out, "--igb", str(igb),
+                        "--diel", "78.5", "--qtol", "1e-10",
+                        "--qdisc", "9.31322574615478515625E-10",
+                        "--scee", str(scee), "--scnb", str(scnb)])
+            rec = read_records(out)
+            rec["known_answer_gb"] = np.array([answers[key][ans_idx]])
+            np.savez_compressed(os.path.join(HERE, f"reference_{sname}_igb{igb}.npz"), **rec)
+            print("wrote", sname, igb, rec["energy_terms"][-1], answers[key][ans_idx])
 
 
 if __name__ == "__main__":

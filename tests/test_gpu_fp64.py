@@ -13,21 +13,21 @@ import pytest
 import oracle
 import stormm_b200 as sb
 from stormm_b200 import synthetic
-from fixtures import (igb_of_fixture, load, molecule_from_fixture, reference_forces,
-                      reference_paths, rms_rel)
+from fixtures import (load, molecule_from_fixture, reference_forces, reference_paths, rms_rel,
+                      solvent_options)
 
 pytestmark = pytest.mark.gpu
 
 BITS = dict(frc_bits=36, nrg_bits=36)
 CASES = ["synthetic_M0.npz", "synthetic_E2.npz", "synthetic_E17.npz", "synthetic_E33.npz",
          "synthetic_E257.npz", "synthetic_C600.npz", "synthetic_S64.npz", "synthetic_H100.npz",
-         "synthetic_O100.npz", "synthetic_V100.npz", "synthetic_K64.npz"]
+         "synthetic_O100.npz", "synthetic_V100.npz", "synthetic_K64.npz", "synthetic_N7.npz",
+         "synthetic_N8.npz"]
 
 
 def _evaluate(g, precision, **extra):
     mol = molecule_from_fixture(g)
-    syn = sb.Synthesis([mol], igb=igb_of_fixture(g), dielectric=float(g["dielectric"][0]),
-                       saltcon=float(g["saltcon"][0]), precision=precision, **extra)
+    syn = sb.Synthesis([mol], precision=precision, **solvent_options(g), **extra)
     syn.set_coordinates(mol.coords)
     syn.initialize()
     syn.evaluate()

@@ -16,7 +16,8 @@ import pytest
 import oracle
 import stormm_b200 as sb
 from fixtures import (default_solvent_paths, igb_of_fixture, load, molecule_from_fixture,
-                      reference_forces, reference_paths, rms_rel, synthetic_paths)
+                      reference_forces, reference_paths, rms_rel, solvent_options,
+                      synthetic_paths)
 
 pytestmark = pytest.mark.gpu
 
@@ -45,8 +46,7 @@ def _check_energy(e_gpu, e_ref):
 def test_single_system_matches_stormm(path):
     g = load(os.path.basename(path))
     mol = molecule_from_fixture(g)
-    r = _run([mol], igb=igb_of_fixture(g), dielectric=float(g["dielectric"][0]),
-             saltcon=float(g["saltcon"][0]))
+    r = _run([mol], **solvent_options(g))
     _check_energy(r["energies"][0], g["energy_terms"])
     err = rms_rel(r["forces"], reference_forces(g))
     assert err <= FORCE_TOL, err
@@ -54,11 +54,12 @@ def test_single_system_matches_stormm(path):
 
 @pytest.mark.parametrize("path", reference_paths(), ids=os.path.basename)
 def test_reference_systems_known_answers(path):
-    """Trp-cage and alanine dipeptide under HCT, OBC and OBC-II, against STORMM's CPU results
-    and the known GB energies of test/Potential/test_generalized_born.cpp:296-300."""
+    """Trp-cage and alanine dipeptide under HCT, OBC, OBC-II and the two neck models, against
+    STORMM's CPU results and the known GB energies of
+    test/Potential/test_generalized_born.cpp:296-300."""
     g = load(os.path.basename(path))
     mol = molecule_from_fixture(g)
-    r = _run([mol], igb=igb_of_fixture(g), dielectric=float(g["dielectric"][0]))
+    r = _run([mol], **solvent_options(g))
     _check_energy(r["energies"][0], g["energy_terms"])
     assert abs(r["energies"][0][8] - g["known_answer_gb"][0]) < 1e-3
     assert rms_rel(r["forces"], reference_forces(g)) <= FORCE_TOL
@@ -199,3 +200,15 @@ def test_clash_mitigated_evaluation_matches_stormm():
     syn.initialize()
     syn.evaluate_clash(0.0, 0.0)
     assert np.array_equal(syn.forces_fixed()[0], f_plain)
+
+
+def test_neck_gb_on_the_tiled_path_and_without_tables():
+    """Neck GB II through the tile-by-tile kernels matches STORMM as the fused kernel does; a
+    neck model without its tables is refused."""
+    g = load("synthetic_N8.npz")
+    mol = molecule_from_fixture(g)
+    tiled = _run([mol], tiled_above_atoms=32, **solvent_options(g))
+    _check_energy(tiled["energies"][0], g["energy_terms"])
+    assert rms_rel(tiled["forces"], reference_forces(g)) <= FORCE_TOL
+    with pytest.raises(sb.StormmB200Error):
+        sb.Synthesis([mol], igb=8)
