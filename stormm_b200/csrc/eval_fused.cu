@@ -38,7 +38,7 @@ size_t fusedSmemBytes(int max_slots, int max_lj) { return unitSmemBytes(max_slot
 // ------------------------------------------------------------------------------------------------
 // The fused kernel: stage, evaluate, commit, one work unit at a time
 // ------------------------------------------------------------------------------------------------
-template <bool FORCE, bool ENERGY, int TERMS, bool CLASH>
+template <bool FORCE, bool ENERGY, int TERMS, bool CLASH, bool NECK>
 __global__ void __launch_bounds__(256, 4)
 kEvalFused(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
   extern __shared__ __align__(16) char smem_raw[];
@@ -62,14 +62,16 @@ kEvalFused(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
       const int k = findOwner(s.slot0, us.nsys, slot);
       const int a = slot - s.slot0[k];
       s.prm[slot] = slotParameters(d, s, k, a);
-      s.neck[slot] = slotNeck(d, s, k, a);
+      if (NECK) {
+        s.neck[slot] = slotNeck(d, s, k, a);
+      }
       const bool real = a < s.natom[k];
       const int gi = d.atom_start[s.sys[k]] + (real ? a : 0);
       placeSlot(d, s, slot, real, real ? d.xcrd[gi] : 0ll, real ? d.ycrd[gi] : 0ll,
                 real ? d.zcrd[gi] : 0ll);
     }
     __syncthreads();
-    evaluateStaged<FORCE, ENERGY, TERMS, true, CLASH>(d, s, us, BlockTeam());
+    evaluateStaged<FORCE, ENERGY, TERMS, true, CLASH, NECK>(d, s, us, BlockTeam());
 
     // commit forces (each atom belongs to exactly one unit) and energies
     if (FORCE) {
@@ -100,11 +102,15 @@ cudaError_t launchEvalFused(const DevSynthesis &d, int unit_begin, int unit_end,
                             int terms, bool force, bool energy, int blocks, int threads,
                             cudaStream_t stream, bool clash) {
   const size_t smem = fusedSmemBytes(d.max_unit_slots, max_lj);
-  // softened cores change only Coulomb, Lennard-Jones and 1-4 terms
+  // softened cores change only Coulomb, Lennard-Jones and 1-4 terms, the neck term only GB
   clash = clash && (terms & 3) != 0;
+  const bool neck = d.neck_size > 0 && (terms & 4) != 0;
 #define SB_LAUNCH(F, E, T)                                                                      \
   {                                                                                             \
-    auto kern = clash ? kEvalFused<F, E, T, ((T) & 3) != 0> : kEvalFused<F, E, T, false>;      \
+    auto kern = neck ? (clash ? kEvalFused<F, E, T, ((T) & 3) != 0, ((T) & 4) != 0> :          \
+                                kEvalFused<F, E, T, false, ((T) & 4) != 0>) :                   \
+                       (clash ? kEvalFused<F, E, T, ((T) & 3) != 0, false> :                    \
+                                kEvalFused<F, E, T, false, false>);                             \
     cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
                                            static_cast<int>(smem));                             \
     if (err != cudaSuccess) return err;                                                         \

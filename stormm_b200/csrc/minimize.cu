@@ -25,6 +25,8 @@
 // trajectory is bit-identical whichever unit, launch or neighbours it has.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "line_search.cuh"
 #include "unit_eval.cuh"
 
@@ -132,7 +134,7 @@ __device__ void moveUnit(const DevSynthesis &d, const DevMinimizer &m, const Uni
 
 // One line-minimization cycle of every unit molecule that has not converged; with CLASH, the
 // four evaluations of a molecule still within m.clash_cycles use softened cores
-template <bool HIST, bool CLASH, class Team>
+template <bool HIST, bool CLASH, bool NECK, class Team>
 __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
                                   const UnitSmem &s, const MinSmem &ms, const UnitShape &us,
                                   const Team &team) {
@@ -146,7 +148,7 @@ __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
     s.clash[k] = clashScaled(m.clash_distance, m.clash_ratio, m.clash_cycles, ms.cyc[k]);
   }
   placeUnit(d, m, s, us, team);
-  evaluateStaged<true, true, 7, false, CLASH>(d, s, us, team);
+  evaluateStaged<true, true, 7, false, CLASH, NECK>(d, s, us, team);
 
   // 2. gg, dgg and |f|^2 per 32-slot chunk (a chunk never straddles two molecules)
   for (int slot = team.rank(); slot < us.nslots; slot += team.size()) {
@@ -257,7 +259,7 @@ __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
   team.sync();
   moveUnit(d, m, s, ms, us, team);
   placeUnit(d, m, s, us, team);
-  evaluateStaged<false, true, 7, false, CLASH>(d, s, us, team);
+  evaluateStaged<false, true, 7, false, CLASH, NECK>(d, s, us, team);
 
   // second trial move: 1.04 x after a decrease, else 0.8 x
   if (team.rank() < us.nsys) {
@@ -275,7 +277,7 @@ __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
   team.sync();
   moveUnit(d, m, s, ms, us, team);
   placeUnit(d, m, s, us, team);
-  evaluateStaged<false, true, 7, false, CLASH>(d, s, us, team);
+  evaluateStaged<false, true, 7, false, CLASH, NECK>(d, s, us, team);
 
   // third trial move: the last factor x 1.03 after a decrease, else x 0.85
   if (team.rank() < us.nsys) {
@@ -293,7 +295,7 @@ __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
   team.sync();
   moveUnit(d, m, s, ms, us, team);
   placeUnit(d, m, s, us, team);
-  evaluateStaged<false, true, 7, false, CLASH>(d, s, us, team);
+  evaluateStaged<false, true, 7, false, CLASH, NECK>(d, s, us, team);
 
   // 4. cubic fit and final placement
   if (team.rank() < us.nsys) {
@@ -321,7 +323,7 @@ __device__ void minimizationCycle(const DevSynthesis &d, const DevMinimizer &m,
 }
 
 // Every cycle of one work unit, then its final energies (undamped) and state
-template <bool HIST, bool CLASH, class Team>
+template <bool HIST, bool CLASH, bool NECK, class Team>
 __device__ void minimizeUnit(const DevSynthesis &d, const DevMinimizer &m, const UnitSmem &s,
                              const MinSmem &ms, int u, int max_lj, int max_sys, int cycles,
                              int final_energy, const Team &team) {
@@ -332,7 +334,9 @@ __device__ void minimizeUnit(const DevSynthesis &d, const DevMinimizer &m, const
   for (int slot = team.rank(); slot < us.nslots; slot += team.size()) {
     const int k = findOwner(s.slot0, us.nsys, slot);
     s.prm[slot] = slotParameters(d, s, k, slot - s.slot0[k]);
-    s.neck[slot] = slotNeck(d, s, k, slot - s.slot0[k]);
+    if (NECK) {
+      s.neck[slot] = slotNeck(d, s, k, slot - s.slot0[k]);
+    }
   }
   if (team.rank() < us.nsys) {
     const int k = team.rank();
@@ -352,12 +356,12 @@ __device__ void minimizeUnit(const DevSynthesis &d, const DevMinimizer &m, const
     if (!team.any(moving != 0)) {
       break;
     }
-    minimizationCycle<HIST, CLASH>(d, m, s, ms, us, team);
+    minimizationCycle<HIST, CLASH, NECK>(d, m, s, ms, us, team);
   }
   if (final_energy) {
     // one more energy evaluation at the final coordinates (hpc_minimization.cu:372-383)
     placeUnit(d, m, s, us, team);
-    evaluateStaged<false, true, 7, false>(d, s, us, team);
+    evaluateStaged<false, true, 7, false, false, NECK>(d, s, us, team);
     for (int e = team.rank(); e < us.nsys * kNrgStride; e += team.size()) {
       d.energies[s.sys[e / kNrgStride] * kNrgStride + (e % kNrgStride)] = s.nrg[e];
     }
@@ -382,7 +386,7 @@ __device__ void minimizeUnit(const DevSynthesis &d, const DevMinimizer &m, const
 // One thread block per work unit (molecules of up to 2,048 atoms).  The minimizer keeps more
 // state live than a single evaluation; two blocks per SM with up to 128 registers a thread run
 // faster than four with 64, where the pair loops spill.
-template <bool HIST, bool CLASH>
+template <bool HIST, bool CLASH, bool NECK>
 __global__ void __launch_bounds__(256, 2)
 kMinimize(const DevSynthesis d, const DevMinimizer m, int unit_begin, int unit_end, int max_lj,
           int cycles, int final_energy) {
@@ -394,8 +398,8 @@ kMinimize(const DevSynthesis d, const DevMinimizer m, int unit_begin, int unit_e
   const BlockTeam team;
   int u = unit_begin + blockIdx.x;
   while (u < unit_end) {
-    minimizeUnit<HIST, CLASH>(d, m, s, ms, u, max_lj, kMaxUnitSystems, cycles, final_energy,
-                              team);
+    minimizeUnit<HIST, CLASH, NECK>(d, m, s, ms, u, max_lj, kMaxUnitSystems, cycles,
+                                    final_energy, team);
     if (threadIdx.x == 0) {
       next_unit = unit_begin + static_cast<int>(gridDim.x) + atomicAdd(m.queue, 1);
     }
@@ -448,8 +452,13 @@ cudaError_t launchMinimize(const DevSynthesis &d, const DevMinimizer &m, int uni
   }
   const size_t smem = minimizeSmemBytes(d.max_unit_slots, max_lj);
   const bool clash = m.clash_cycles > 0 && (m.clash_distance > 0.0f || m.clash_ratio > 0.0f);
-  auto kern = (m.history != nullptr) ? (clash ? kMinimize<true, true> : kMinimize<true, false>) :
-                                       (clash ? kMinimize<false, true> : kMinimize<false, false>);
+  const bool neck = d.neck_size > 0;
+  auto pick = [&](auto hist) {
+    constexpr bool H = decltype(hist)::value;
+    return neck ? (clash ? kMinimize<H, true, true> : kMinimize<H, false, true>) :
+                  (clash ? kMinimize<H, true, false> : kMinimize<H, false, false>);
+  };
+  auto kern = (m.history != nullptr) ? pick(std::true_type()) : pick(std::false_type());
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
   if (err != cudaSuccess) return err;

@@ -1494,8 +1494,10 @@ __device__ __forceinline__ void placeSlot(const DevSynthesis &d, const UnitSmem 
 // shared memory on entry (and a barrier since); forces in s.fx.. and per-molecule energies in
 // s.nrg on exit, after a barrier.  WS: also write the GB workspace (psi, effective radii, dE/dR)
 // to global memory.  CLASH: Coulomb and Lennard-Jones pairs, 1-4 pairs included, take the
-// softened cores of s.clash (per unit molecule, zero for none, set before that barrier).
-template <bool FORCE, bool ENERGY, int TERMS, bool WS, bool CLASH = false, class Team>
+// softened cores of s.clash (per unit molecule, zero for none, set before that barrier).  NECK:
+// the neck GB term (s.neck holds the slots' neck indices).
+template <bool FORCE, bool ENERGY, int TERMS, bool WS, bool CLASH = false, bool NECK = false,
+          class Team>
 __device__ void evaluateStaged(const DevSynthesis &d, const UnitSmem &s, const UnitShape &us,
                                const Team &team) {
   constexpr bool VALE = (TERMS & 1) != 0;
@@ -1514,12 +1516,7 @@ __device__ void evaluateStaged(const DevSynthesis &d, const UnitSmem &s, const U
     }
   }
   if (gb) {
-    if (d.neck_size > 0) {
-      gbRadiiTiles<FORCE, true>(d, s, nsys_u, ntiles, us.tile_base, team.warp(), team.warps());
-    }
-    else {
-      gbRadiiTiles<FORCE, false>(d, s, nsys_u, ntiles, us.tile_base, team.warp(), team.warps());
-    }
+    gbRadiiTiles<FORCE, NECK>(d, s, nsys_u, ntiles, us.tile_base, team.warp(), team.warps());
     team.sync();
     // effective radii, self terms (nonbonded_potential.tpp:730-805); a warp's 32 slots
     // belong to one molecule, so the self energies reduce across the warp
