@@ -333,19 +333,30 @@ class Synthesis:
         _check(library().sb_set_coordinates(self.handle, a.ctypes.data, stream),
                "sb_set_coordinates")
 
-    def coordinates(self, stream=None):
-        out = np.zeros(3 * self.total_atoms)
+    @staticmethod
+    def _output(out, n):
+        """A float64 buffer of n values: a new array, or the caller's (reused, e.g. pinned)."""
+        if out is None:
+            return np.zeros(n)
+        if (not isinstance(out, np.ndarray) or out.dtype != np.float64 or out.size != n or
+                not out.flags["C_CONTIGUOUS"]):
+            raise ValueError(f"output buffer must be a contiguous float64 array of {n} values")
+        return out
+
+    def coordinates(self, stream=None, out=None):
+        out = self._output(out, 3 * self.total_atoms)
         _check(library().sb_get_coordinates(self.handle, out.ctypes.data, stream),
                "sb_get_coordinates")
         return out.reshape(-1, 3)
 
-    def forces(self, stream=None):
-        out = np.zeros(3 * self.total_atoms)
+    def forces(self, stream=None, out=None):
+        """Forces (kcal/mol/A, unpadded atoms); `out` may be a reused (pinned) buffer."""
+        out = self._output(out, 3 * self.total_atoms)
         _check(library().sb_get_forces(self.handle, out.ctypes.data, stream), "sb_get_forces")
         return out.reshape(-1, 3)
 
-    def energies(self, stream=None):
-        out = np.zeros(self.nsys * NRG_STRIDE)
+    def energies(self, stream=None, out=None):
+        out = self._output(out, self.nsys * NRG_STRIDE)
         _check(library().sb_get_energies(self.handle, out.ctypes.data, stream),
                "sb_get_energies")
         return out.reshape(self.nsys, NRG_STRIDE)
