@@ -362,6 +362,55 @@ int sb_static_exclusion_mask(const sb_topology* top, int* supertile_stride_count
                              long long* n_mask_data);
 
 /* ------------------------------------------------------------------------------------------ */
+/* Amber file intake                                                                           */
+/* ------------------------------------------------------------------------------------------ */
+/* An Amber topology (prmtop) read from disk: what STORMM's AtomGraph(file_name) reads
+ * (Topology/atomgraph.h:83,156, atomgraph_detailers.cpp:677-1120).  Host only, no device
+ * needed.  Charges come out in electrons, Lennard-Jones tables expanded to n_types^2, 1-2 / 1-3
+ * / 1-4 exclusions from the bond graph, GB radii and screening factors as the file holds them.
+ * Refused: periodic topologies (SB_ERR_UNSUPPORTED) and nonzero 10-12 hydrogen-bond terms.
+ * CHARMM Urey-Bradley, improper and CMAP terms are counted in the view but not evaluated. */
+typedef struct sb_amber_topology sb_amber_topology;
+
+typedef struct {
+  sb_topology topology;             /* ready for sb_synthesis_create; gb_alpha / beta / gamma
+                                       are NULL until sb_amber_set_implicit_solvent */
+  const int* atomic_numbers;        /* natom (inferred from masses when the file has none) */
+  const double* masses;             /* natom, daltons */
+  const int* exclusion_bounds[3];   /* natom + 1 each: CSR bounds of the 1-2, 1-3, 1-4 lists */
+  const int* exclusion_list[3];     /* partners one, two and three bonds away, ascending */
+  const char* radius_set;           /* RADIUS_SET text ("" when absent) */
+  const char* title;
+  int implicit_solvent;             /* SB_GB_* applied, -1 for none yet */
+  int cmap_count;                   /* CHARMM terms present in the file (not evaluated) */
+  int urey_bradley_count;
+  int charmm_improper_count;
+} sb_amber_view;
+
+int sb_read_amber_topology(const char* prmtop_path, sb_amber_topology** out);
+/* Pointers into the topology's own arrays, valid until sb_amber_topology_destroy or the next
+ * sb_amber_set_implicit_solvent */
+int sb_amber_topology_view(const sb_amber_topology* top, sb_amber_view* view);
+/* Radius sets (STORMM's AtomicRadiusSet, Topology/atomgraph_enumerators.h:150-152) */
+#define SB_RADII_NONE 0         /* keep the file's radii and screening factors */
+#define SB_RADII_BONDI 1
+#define SB_RADII_AMBER6 2
+#define SB_RADII_MBONDI 3
+#define SB_RADII_MBONDI2 4
+#define SB_RADII_MBONDI3 5
+#define SB_RADII_PARSE 6
+/* Per-atom GB parameters of a model as STORMM's AtomGraph::setImplicitSolventModel assigns them
+ * (Topology/atomgraph_setters.cpp:672-1060): the radius set's radii and screening factors (the
+ * neck models replace file radii outside [1, 2] A by Bondi or mBondi3 radii), then uniform
+ * alpha / beta / gamma for HCT, OBC and OBC-II, element screening factors for neck GB, element
+ * alpha / beta / gamma and screening factors for neck GB II */
+int sb_amber_set_implicit_solvent(sb_amber_topology* top, int igb, int radius_set);
+int sb_amber_topology_destroy(sb_amber_topology* top);
+/* Coordinates of an Amber ASCII coordinate or restart file (STORMM's PhaseSpace(file_name)):
+ * 3 * natom doubles, interlaced x, y, z; the file's atom count must equal natom */
+int sb_read_amber_coordinates(const char* inpcrd_path, int natom, double* xyz);
+
+/* ------------------------------------------------------------------------------------------ */
 /* Autotuning                                                                                  */
 /* ------------------------------------------------------------------------------------------ */
 #define SB_TUNE_EVALUATE 1

@@ -184,27 +184,41 @@ def from_fixture(g) -> OracleSystem:
 
 def from_molecule(m, igb: int = 5, dielectric: float = 80.0, saltcon: float = 0.0,
                   coulomb_constant: float = 332.0522172900000) -> OracleSystem:
-    """Oracle system from a synthetic Molecule (OBC-II alpha/beta/gamma = 1.0, 0.8, 4.85)."""
+    """Oracle system from a Molecule: a synthetic one (one scee / scnb, no impropers, OBC-II
+    alpha / beta / gamma = 1.0, 0.8, 4.85 by model) or one read from an Amber topology, whose
+    per-dihedral 1-4 factors, improper flags, 1-4 Lennard-Jones tables and per-atom GB
+    parameters are used when present."""
     if igb in (7, 8):
         raise ValueError("neck GB needs the neck tables: build the oracle system from a fixture")
     n = m.natom
     eb, el = _csr_from_sets(n, [m.excl12, m.excl13, m.excl14])
     ab = {1: (0.0, 0.0, 0.0), 2: (0.8, 0.0, 2.909125), 5: (1.0, 0.8, 4.85)}.get(igb, (0, 0, 0))
     has14 = np.asarray(m.dihe_has14, dtype=bool)
+    nd = m.dihedrals.shape[0]
+    scee = getattr(m, "dihe_scee_array", None)
+    scnb = getattr(m, "dihe_scnb_array", None)
+    improper = getattr(m, "dihe_improper", None)
+    alpha = getattr(m, "gb_alpha", None)
+    beta = getattr(m, "gb_beta", None)
+    gamma = getattr(m, "gb_gamma", None)
     return OracleSystem(
         natom=n, coulomb_constant=coulomb_constant, charge=m.charge, lj_idx=m.lj_idx,
-        n_lj_types=m.n_lj_types, lja=m.lja, ljb=m.ljb, lja14=m.lja, ljb14=m.ljb,
-        excl_bounds=eb, excl_list=el, igb=igb, dielectric=dielectric, saltcon=saltcon,
-        pb_radii=m.pb_radii, gb_screen=m.gb_screen, gb_alpha=np.full(n, ab[0]),
-        gb_beta=np.full(n, ab[1]), gb_gamma=np.full(n, ab[2]),
+        n_lj_types=m.n_lj_types, lja=m.lja, ljb=m.ljb, lja14=getattr(m, "lja14", m.lja),
+        ljb14=getattr(m, "ljb14", m.ljb), excl_bounds=eb, excl_list=el, igb=igb,
+        dielectric=dielectric, saltcon=saltcon, pb_radii=m.pb_radii, gb_screen=m.gb_screen,
+        gb_alpha=alpha if alpha is not None else np.full(n, ab[0]),
+        gb_beta=beta if beta is not None else np.full(n, ab[1]),
+        gb_gamma=gamma if gamma is not None else np.full(n, ab[2]),
         nbond=m.bonds.shape[0], bond_i=m.bonds[:, 0], bond_j=m.bonds[:, 1], bond_k=m.bond_k,
         bond_r0=m.bond_r0, nangl=m.angles.shape[0], angl_i=m.angles[:, 0],
         angl_j=m.angles[:, 1], angl_k=m.angles[:, 2], angl_keq=m.angl_k,
-        angl_theta0=m.angl_theta0, ndihe=m.dihedrals.shape[0], dihe_i=m.dihedrals[:, 0],
+        angl_theta0=m.angl_theta0, ndihe=nd, dihe_i=m.dihedrals[:, 0],
         dihe_j=m.dihedrals[:, 1], dihe_k=m.dihedrals[:, 2], dihe_l=m.dihedrals[:, 3],
         dihe_amp=m.dihe_amp, dihe_freq=m.dihe_freq, dihe_phase=m.dihe_phase,
-        dihe_scee=np.where(has14, m.scee, 0.0), dihe_scnb=np.where(has14, m.scnb, 0.0),
-        dihe_improper=np.zeros(m.dihedrals.shape[0], dtype=np.int32))
+        dihe_scee=scee if scee is not None else np.where(has14, m.scee, 0.0),
+        dihe_scnb=scnb if scnb is not None else np.where(has14, m.scnb, 0.0),
+        dihe_improper=(np.asarray(improper, dtype=np.int32) if improper is not None else
+                       np.zeros(nd, dtype=np.int32)))
 
 
 def float_to_int63(v: float):

@@ -20,6 +20,9 @@ TERM_VALENCE, TERM_NONBONDED, TERM_GB, TERM_ALL = 1, 2, 4, 7
 TUNE_EVALUATE, TUNE_MINIMIZE = 1, 2
 MIN_GRAPH, MIN_PERSISTENT = 0, 1
 PRECISION_SINGLE, PRECISION_DOUBLE = 0, 1
+# AtomicRadiusSet (STORMM Topology/atomgraph_enumerators.h:150-152)
+RADII_NONE, RADII_BONDI, RADII_AMBER6, RADII_MBONDI, RADII_MBONDI2, RADII_MBONDI3, RADII_PARSE = \
+    range(7)
 INIT_FORCES, INIT_ENERGIES, INIT_GB_WORKSPACE = 1, 2, 4
 NRG_STRIDE = 16
 # StateVariable slots (STORMM Potential/energy_enumerators.h:36-50)
@@ -93,6 +96,16 @@ class ServerStats(ctypes.Structure):
     ]
 
 
+class AmberView(ctypes.Structure):
+    _fields_ = [
+        ("topology", Topology), ("atomic_numbers", _P), ("masses", _P),
+        ("exclusion_bounds", _P * 3), ("exclusion_list", _P * 3), ("radius_set", ctypes.c_char_p),
+        ("title", ctypes.c_char_p), ("implicit_solvent", ctypes.c_int),
+        ("cmap_count", ctypes.c_int), ("urey_bradley_count", ctypes.c_int),
+        ("charmm_improper_count", ctypes.c_int),
+    ]
+
+
 class StormmB200Error(RuntimeError):
     pass
 
@@ -161,6 +174,11 @@ def library() -> ctypes.CDLL:
             "sb_server_destroy": (ctypes.c_int, [vp]),
             "sb_static_exclusion_mask": (ctypes.c_int, [ctypes.POINTER(Topology), vp, vp, vp, vp,
                                                         vp, vp, vp]),
+            "sb_read_amber_topology": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(vp)]),
+            "sb_amber_topology_view": (ctypes.c_int, [vp, ctypes.POINTER(AmberView)]),
+            "sb_amber_set_implicit_solvent": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
+            "sb_amber_topology_destroy": (ctypes.c_int, [vp]),
+            "sb_read_amber_coordinates": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, vp]),
             "sb_last_error": (ctypes.c_char_p, []),
             "sb_version": (ctypes.c_char_p, []),
         }
@@ -278,6 +296,92 @@ def static_exclusion_mask(molecule):
                                         ctypes.byref(n[2])), "sb_static_exclusion_mask")
     return {"supertile_stride_count": nst.value, "supertile_map_idx": sup,
             "tile_map_idx": til, "mask_data": msk}
+
+
+def _host_array(ptr, count, ctype, dtype):
+    """Copy of count values at a library-owned pointer (empty when count is 0)."""
+    if count == 0:
+        return np.zeros(0, dtype=dtype)
+    return np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ctype)),
+                                 shape=(count,)).astype(dtype, copy=True)
+
+
+def read_amber(prmtop, inpcrd=None, igb=None, radius_set=0):
+    """A molecule from an Amber topology file and, optionally, its coordinate file: what
+    STORMM's AtomGraph(file_name) and PhaseSpace(file_name) read (Topology/atomgraph.h:83,156).
+    With igb, the per-atom GB parameters of that model are assigned as STORMM's
+    AtomGraph::setImplicitSolventModel assigns them: radius_set (RADII_*, default the file's
+    radii) first, then element screening factors for the neck models.  Returns a synthetic.Molecule (coordinates zero without inpcrd) carrying, besides
+    the usual fields, the per-dihedral 1-4 factors, improper flags, the 1-4 Lennard-Jones
+    tables when the file has them, the GB parameters when igb is given, and the file's title,
+    radius set and CHARMM term counts."""
+    from .synthetic import Molecule
+    lib = library()
+    h = ctypes.c_void_p()
+    _check(lib.sb_read_amber_topology(os.fsencode(str(prmtop)), ctypes.byref(h)),
+           "sb_read_amber_topology")
+    try:
+        if igb is not None:
+            _check(lib.sb_amber_set_implicit_solvent(h, int(igb), int(radius_set)),
+                   "sb_amber_set_implicit_solvent")
+        v = AmberView()
+        _check(lib.sb_amber_topology_view(h, ctypes.byref(v)), "sb_amber_topology_view")
+        t = v.topology
+        n, nt = t.natom, t.n_lj_types
+        dbl, i32 = ctypes.c_double, ctypes.c_int
+
+        def d(p, c):
+            return _host_array(p, c, dbl, np.float64)
+
+        def i(p, c):
+            return _host_array(p, c, i32, np.int32)
+
+        excl = []
+        for lv in range(3):
+            b = i(v.exclusion_bounds[lv], n + 1)
+            x = i(v.exclusion_list[lv], int(b[-1]))
+            excl.append([list(x[b[a]:b[a + 1]]) for a in range(n)])
+        scee = d(t.dihe_scee, t.ndihe)
+        mol = Molecule(
+            natom=n, coords=np.zeros((n, 3)), charge=d(t.charge, n), lj_idx=i(t.lj_idx, n),
+            lja=d(t.lja, nt * nt).reshape(nt, nt), ljb=d(t.ljb, nt * nt).reshape(nt, nt),
+            z_numbers=i(v.atomic_numbers, n), mass=d(v.masses, n), pb_radii=d(t.pb_radii, n),
+            gb_screen=d(t.gb_screen, n), bonds=i(t.bond_atoms, 2 * t.nbond).reshape(-1, 2),
+            bond_k=d(t.bond_keq, t.nbond), bond_r0=d(t.bond_leq, t.nbond),
+            angles=i(t.angl_atoms, 3 * t.nangl).reshape(-1, 3),
+            angl_k=d(t.angl_keq, t.nangl), angl_theta0=d(t.angl_theta0, t.nangl),
+            dihedrals=i(t.dihe_atoms, 4 * t.ndihe).reshape(-1, 4),
+            dihe_amp=d(t.dihe_amp, t.ndihe), dihe_freq=d(t.dihe_freq, t.ndihe),
+            dihe_phase=d(t.dihe_phase, t.ndihe), dihe_has14=scee > 0.0,
+            name=(v.title or b"").decode(errors="replace").strip() or "MOL",
+            excl12=excl[0], excl13=excl[1], excl14=excl[2])
+        mol.dihe_scee_array = scee
+        mol.dihe_scnb_array = d(t.dihe_scnb, t.ndihe)
+        mol.dihe_improper = i(t.dihe_improper, t.ndihe)
+        if t.lja14:
+            mol.lja14 = d(t.lja14, nt * nt).reshape(nt, nt)
+            mol.ljb14 = d(t.ljb14, nt * nt).reshape(nt, nt)
+        if igb is not None:
+            mol.gb_alpha = d(t.gb_alpha, n)
+            mol.gb_beta = d(t.gb_beta, n)
+            mol.gb_gamma = d(t.gb_gamma, n)
+        mol.radius_set = (v.radius_set or b"").decode(errors="replace")
+        mol.cmap_count = v.cmap_count
+        mol.urey_bradley_count = v.urey_bradley_count
+        mol.charmm_improper_count = v.charmm_improper_count
+    finally:
+        lib.sb_amber_topology_destroy(h)
+    if inpcrd is not None:
+        mol.coords = read_amber_coordinates(inpcrd, mol.natom)
+    return mol
+
+
+def read_amber_coordinates(path, natom):
+    """(natom, 3) coordinates of an Amber ASCII coordinate / restart file."""
+    xyz = np.zeros(3 * natom)
+    _check(library().sb_read_amber_coordinates(os.fsencode(str(path)), int(natom),
+                                               xyz.ctypes.data), "sb_read_amber_coordinates")
+    return xyz.reshape(natom, 3)
 
 
 def minimize_controls(**overrides) -> MinimizeControls:
