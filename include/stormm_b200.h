@@ -302,12 +302,17 @@ typedef struct {
   int cycles_per_launch;             /* minimization cycles per launch of a batch */
 } sb_server_options;
 
+#define SB_REQUEST_MINIMIZE 0          /* run the minimization, return the final coordinates */
+#define SB_REQUEST_EVALUATE 1          /* one force + energy evaluation, return the forces */
+
 typedef struct {
   long long request_id;
   int natom;
+  int kind;                          /* SB_REQUEST_* */
   int cycles;                        /* line-minimization cycles run */
   int converged;                     /* nonzero: the RMS force met controls.convergence_rms */
-  double rms_force;                  /* kcal/mol/A at the start of the last cycle */
+  double rms_force;                  /* kcal/mol/A at the start of the last cycle (minimization),
+                                        at the given coordinates (evaluation) */
   double energy;                     /* total potential energy at the final coordinates */
   double energies[SB_NRG_STRIDE];    /* the terms, StateVariable order */
   double submit_time;                /* seconds since the server started */
@@ -332,12 +337,18 @@ typedef struct sb_server sb_server;
  * 512 molecules per batch, 16 batches, 50 cycles a launch */
 void sb_default_server_options(sb_server_options* opt);
 int sb_server_create(const sb_server_options* opt, sb_server** out);
-/* Queue one molecule (topology and coordinates are copied); thread-safe */
+/* Queue one molecule for minimization (topology and coordinates are copied); thread-safe */
 int sb_server_submit(sb_server* srv, const sb_topology* top, const double* xyz,
                      long long* request_id);
-/* Completed requests, oldest first: up to max_results, each with its final coordinates packed
- * into xyz (natom * 3 doubles per result, in result order) while xyz_capacity doubles last;
- * xyz may be NULL to take results without coordinates.  *count receives the number returned. */
+/* Queue one molecule for a force + energy evaluation at the given coordinates.  Evaluation
+ * requests are batched with each other (a batch holds one kind of request), admitted under the
+ * same HBM budget and overlap on the device with the minimization batches in flight. */
+int sb_server_submit_evaluation(sb_server* srv, const sb_topology* top, const double* xyz,
+                                long long* request_id);
+/* Completed requests, oldest first: up to max_results, each with its natom * 3 doubles packed
+ * into xyz (in result order) while xyz_capacity doubles last: the final coordinates of a
+ * minimization, the forces (kcal/mol/A) of an evaluation.  xyz may be NULL to take results
+ * without them.  *count receives the number returned. */
 int sb_server_poll(sb_server* srv, sb_served_result* results, int max_results, double* xyz,
                    long long xyz_capacity, int* count);
 /* Wait until nothing is queued or in flight: SB_OK, or SB_TIMEOUT after timeout_seconds */

@@ -24,6 +24,7 @@ PRECISION_SINGLE, PRECISION_DOUBLE = 0, 1
 RADII_NONE, RADII_BONDI, RADII_AMBER6, RADII_MBONDI, RADII_MBONDI2, RADII_MBONDI3, RADII_PARSE = \
     range(7)
 INIT_FORCES, INIT_ENERGIES, INIT_GB_WORKSPACE = 1, 2, 4
+SB_REQUEST_MINIMIZE, SB_REQUEST_EVALUATE = 0, 1
 NRG_STRIDE = 16
 # StateVariable slots (STORMM Potential/energy_enumerators.h:36-50)
 NRG_SLOTS = {"bond": 0, "angle": 1, "proper_dihedral": 2, "improper_dihedral": 3, "vdw": 7,
@@ -81,7 +82,8 @@ class ServerOptions(ctypes.Structure):
 
 class ServedResult(ctypes.Structure):
     _fields_ = [
-        ("request_id", ctypes.c_longlong), ("natom", ctypes.c_int), ("cycles", ctypes.c_int),
+        ("request_id", ctypes.c_longlong), ("natom", ctypes.c_int), ("kind", ctypes.c_int),
+        ("cycles", ctypes.c_int),
         ("converged", ctypes.c_int), ("rms_force", ctypes.c_double), ("energy", ctypes.c_double),
         ("energies", ctypes.c_double * 16), ("submit_time", ctypes.c_double),
         ("admit_time", ctypes.c_double), ("finish_time", ctypes.c_double),
@@ -167,6 +169,8 @@ def library() -> ctypes.CDLL:
                                                 ctypes.POINTER(vp)]),
             "sb_server_submit": (ctypes.c_int, [vp, ctypes.POINTER(Topology), vp,
                                                 ctypes.POINTER(ctypes.c_longlong)]),
+            "sb_server_submit_evaluation": (ctypes.c_int, [vp, ctypes.POINTER(Topology), vp,
+                                                           ctypes.POINTER(ctypes.c_longlong)]),
             "sb_server_poll": (ctypes.c_int, [vp, ctypes.POINTER(ServedResult), ctypes.c_int, vp,
                                               ctypes.c_longlong, ctypes.POINTER(ctypes.c_int)]),
             "sb_server_drain": (ctypes.c_int, [vp, ctypes.c_double]),
@@ -593,8 +597,9 @@ SB_TIMEOUT = 1
 
 
 class Server:
-    """Continuous-batching minimization server (sb_server_*).  Submit molecules at any time;
-    completed requests come back from poll() with their final coordinates."""
+    """Continuous-batching request server (sb_server_*): minimizations and force + energy
+    evaluations.  Submit molecules at any time; completed requests come back from poll() with
+    their final coordinates (minimization) or forces (evaluation)."""
 
     def __init__(self, budget_bytes=2.0e9, max_batch_molecules=512, max_batches=16,
                  cycles_per_launch=50, options: Options | None = None, **controls):
@@ -619,18 +624,22 @@ class Server:
         """Topology arrays of a molecule, reusable for many submissions."""
         return _TopologyArrays(molecule)
 
-    def submit(self, molecule, coords=None, prepared=None):
+    def submit(self, molecule, coords=None, prepared=None, evaluate=False):
+        """Queue a minimization, or with evaluate=True a force + energy evaluation (its result
+        carries the forces where a minimization's carries the final coordinates)."""
         t = prepared if prepared is not None else _TopologyArrays(molecule)
         xyz = np.ascontiguousarray(np.asarray(molecule.coords if coords is None else coords,
                                               dtype=np.float64).reshape(-1))
         rid = ctypes.c_longlong()
-        _check(library().sb_server_submit(self.handle, ctypes.byref(t.struct), xyz.ctypes.data,
-                                          ctypes.byref(rid)), "sb_server_submit")
+        fn = library().sb_server_submit_evaluation if evaluate else library().sb_server_submit
+        _check(fn(self.handle, ctypes.byref(t.struct), xyz.ctypes.data, ctypes.byref(rid)),
+               "sb_server_submit")
         self._natom[rid.value] = molecule.natom
         return rid.value
 
     def poll(self, max_results=4096, coordinates=True):
-        """List of (result dict, coordinates or None) for the requests completed so far."""
+        """List of (result dict, array or None) for the requests completed so far: final
+        coordinates of a minimization, forces of an evaluation (dict key "kind")."""
         res = (ServedResult * max_results)()
         cap = 3 * sum(self._natom.values()) if coordinates else 0
         buf = np.zeros(max(cap, 1)) if coordinates else None
@@ -642,7 +651,9 @@ class Server:
         off = 0
         for k in range(n.value):
             r = res[k]
-            d = {"request_id": r.request_id, "natom": r.natom, "cycles": r.cycles,
+            d = {"request_id": r.request_id, "natom": r.natom,
+                 "kind": "evaluate" if r.kind == SB_REQUEST_EVALUATE else "minimize",
+                 "cycles": r.cycles,
                  "converged": bool(r.converged), "rms_force": r.rms_force, "energy": r.energy,
                  "energies": np.array(r.energies[:]), "submit_time": r.submit_time,
                  "admit_time": r.admit_time, "finish_time": r.finish_time}

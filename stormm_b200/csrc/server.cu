@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -61,6 +62,7 @@ struct Request {
   double bytes = 0.0;
   double t_submit = 0.0;
   double t_admit = 0.0;
+  int kind = SB_REQUEST_MINIMIZE;
 
   Request(const sb_topology &t, const double* coords) {
     natom = t.natom;
@@ -150,8 +152,10 @@ struct Result {
   std::vector<double> xyz;
 };
 
-// Admitted requests minimizing together on one stream
+// Admitted requests of one kind running together on one stream: minimizations, or energy and
+// force evaluations (one launch)
 struct Batch {
+  int kind = SB_REQUEST_MINIMIZE;
   std::vector<Request> reqs;
   std::vector<char> finished;
   int remaining = 0;
@@ -194,11 +198,20 @@ public:
     }
   }
 
-  long long submit(const sb_topology* top, const double* xyz) {
+  long long submit(const sb_topology* top, const double* xyz, int kind) {
     if (top == nullptr || xyz == nullptr || top->natom <= 0) {
       throw Error(SB_ERR_ARGUMENT, "a request needs a topology with atoms and coordinates");
     }
+    if (kind != SB_REQUEST_MINIMIZE && kind != SB_REQUEST_EVALUATE) {
+      throw Error(SB_ERR_ARGUMENT, "unknown request kind " + std::to_string(kind));
+    }
+    const int on_chip = (opt_.options.tiled_above_atoms > 0) ? opt_.options.tiled_above_atoms : 2048;
+    if (kind == SB_REQUEST_MINIMIZE && top->natom > on_chip) {
+      throw Error(SB_ERR_UNSUPPORTED, "molecules above " + std::to_string(on_chip) +
+                  " atoms are evaluated tile by tile and cannot be minimized");
+    }
     Request req(*top, xyz);
+    req.kind = kind;
     if (req.bytes > opt_.hbm_budget_bytes) {
       throw Error(SB_ERR_ARGUMENT, "the molecule alone exceeds the server's HBM budget");
     }
@@ -300,14 +313,23 @@ private:
           if (stop_) {
             break;
           }
-          if (static_cast<int>(batches.size()) < opt_.max_batches) {
+          if (static_cast<int>(batches.size()) < opt_.max_batches && !pending_.empty()) {
+            // a batch holds one kind of request: the oldest pending one's, taken in arrival
+            // order until the batch or the memory budget is full
+            const int kind = pending_.front().kind;
             double bytes = bytes_in_flight_;
-            while (!pending_.empty() &&
-                   static_cast<int>(take.size()) < opt_.max_batch_molecules &&
-                   bytes + pending_.front().bytes <= opt_.hbm_budget_bytes) {
-              bytes += pending_.front().bytes;
-              take.push_back(std::move(pending_.front()));
-              pending_.pop_front();
+            for (auto it = pending_.begin(); it != pending_.end() &&
+                 static_cast<int>(take.size()) < opt_.max_batch_molecules;) {
+              if (it->kind != kind) {
+                ++it;
+                continue;
+              }
+              if (bytes + it->bytes > opt_.hbm_budget_bytes) {
+                break;
+              }
+              bytes += it->bytes;
+              take.push_back(std::move(*it));
+              it = pending_.erase(it);
             }
             if (!take.empty()) {
               bytes_in_flight_ = bytes;
@@ -342,6 +364,7 @@ private:
   // Build, upload and start a batch on a stream of its own
   std::unique_ptr<Batch> admit(std::vector<Request> take) {
     auto b = std::make_unique<Batch>();
+    b->kind = take.front().kind;
     b->reqs = std::move(take);
     b->finished.assign(b->reqs.size(), 0);
     b->remaining = static_cast<int>(b->reqs.size());
@@ -365,16 +388,76 @@ private:
                                            index.data(), static_cast<int>(tops.size()),
                                            opt_.options);
       b->syn->setCoordinates(xyz.data(), b->stream);
-      b->syn->minimizeBegin(opt_.controls, b->stream);
+      if (b->kind == SB_REQUEST_MINIMIZE) {
+        b->syn->minimizeBegin(opt_.controls, b->stream);
+      }
     }
-    b->syn->minimizeAdvance(opt_.cycles_per_launch, true, b->stream);
+    if (b->kind == SB_REQUEST_MINIMIZE) {
+      b->syn->minimizeAdvance(opt_.cycles_per_launch, true, b->stream);
+    }
+    else {
+      b->syn->initialize(SB_INIT_FORCES | SB_INIT_ENERGIES | SB_INIT_GB_WORKSPACE, b->stream);
+      b->syn->evaluate(SB_TERM_ALL, true, true, b->stream);
+    }
     cudaCheck(cudaEventRecord(b->event, b->stream), "cudaEventRecord");
     return b;
+  }
+
+  // Results of an evaluation batch (all of it completes with its one launch)
+  void serviceEvaluation(Batch* b) {
+    const int n = static_cast<int>(b->reqs.size());
+    std::vector<double> nrg(static_cast<size_t>(n) * SB_NRG_STRIDE);
+    std::vector<double> frc(3 * static_cast<size_t>(b->syn->natom_total));
+    b->syn->getEnergies(nrg.data(), b->stream);
+    b->syn->getForces(frc.data(), b->stream);
+    const double t = now();
+    std::vector<Result> out;
+    size_t off = 0;
+    for (int k = 0; k < n; k++) {
+      const Request &r = b->reqs[k];
+      Result res;
+      std::memset(&res.r, 0, sizeof(sb_served_result));
+      res.r.request_id = r.id;
+      res.r.natom = r.natom;
+      res.r.kind = SB_REQUEST_EVALUATE;
+      double total = 0.0, f2 = 0.0;
+      for (int q = 0; q < SB_NRG_STRIDE; q++) {
+        res.r.energies[q] = nrg[static_cast<size_t>(k) * SB_NRG_STRIDE + q];
+        total += res.r.energies[q];
+      }
+      const size_t len = 3 * static_cast<size_t>(r.natom);
+      for (size_t q = 0; q < len; q++) {
+        f2 += frc[off + q] * frc[off + q];
+      }
+      res.r.energy = total;
+      res.r.rms_force = std::sqrt(f2 / static_cast<double>(len));
+      res.r.submit_time = r.t_submit;
+      res.r.admit_time = r.t_admit;
+      res.r.finish_time = t;
+      res.xyz.assign(frc.begin() + off, frc.begin() + off + len);
+      off += len;
+      out.push_back(std::move(res));
+      b->finished[k] = 1;
+    }
+    b->remaining = 0;
+    std::lock_guard<std::mutex> lock(mu_);
+    for (auto &res : out) {
+      results_.push_back(std::move(res));
+    }
+    in_flight_ -= n;
+    completed_ += n;
+    if (pending_.empty() && in_flight_ == 0) {
+      idle_cv_.notify_all();
+    }
   }
 
   // After a launch of the batch finished: retire what is done, relaunch the rest.  Returns true
   // when every molecule of the batch has retired.
   bool service(Batch* b) {
+    if (b->kind == SB_REQUEST_EVALUATE) {
+      serviceEvaluation(b);
+      return true;
+    }
     const int n = static_cast<int>(b->reqs.size());
     std::vector<int> cycles(n), done(n);
     std::vector<double> rms(n);
@@ -405,6 +488,7 @@ private:
         res.r.cycles = cycles[k];
         res.r.converged = done[k];
         res.r.rms_force = rms[k];
+        res.r.kind = SB_REQUEST_MINIMIZE;
         double total = 0.0;
         for (int q = 0; q < SB_NRG_STRIDE; q++) {
           res.r.energies[q] = nrg[static_cast<size_t>(k) * SB_NRG_STRIDE + q];
@@ -545,7 +629,15 @@ int sb_server_create(const sb_server_options* opt, sb_server** out) {
 int sb_server_submit(sb_server* srv, const sb_topology* top, const double* xyz,
                      long long* request_id) {
   return serverGuarded([&]() {
-    const long long id = needServer(srv)->submit(top, xyz);
+    const long long id = needServer(srv)->submit(top, xyz, SB_REQUEST_MINIMIZE);
+    if (request_id) *request_id = id;
+  });
+}
+
+int sb_server_submit_evaluation(sb_server* srv, const sb_topology* top, const double* xyz,
+                                long long* request_id) {
+  return serverGuarded([&]() {
+    const long long id = needServer(srv)->submit(top, xyz, SB_REQUEST_EVALUATE);
     if (request_id) *request_id = id;
   });
 }

@@ -79,3 +79,72 @@ def test_budget_bounds_the_molecules_in_flight():
     with pytest.raises(sb.StormmB200Error):
         srv.submit(big)
     srv.close()
+
+
+def _evaluated_alone(mol):
+    syn = sb.Synthesis([mol])
+    syn.set_coordinates(mol.coords)
+    syn.initialize()
+    syn.evaluate()
+    out = (syn.forces().copy(), syn.energies()[0].copy())
+    syn.close()
+    return out
+
+
+def test_evaluation_requests_mixed_with_minimizations():
+    """Force + energy requests share the server with minimizations: they batch with each other,
+    overlap with the minimization batches in flight, and each comes back exactly as a direct
+    evaluation of the molecule alone (and within the oracle's tolerance), as does each
+    minimization."""
+    import oracle
+    sizes = [16, 40, 64, 100, 23, 180, 2600, 48]      # 2,600 atoms goes to the tiled path
+    mols = [synthetic.make_molecule(synthetic._seed(7070, k), n, 0.3)
+            for k, n in enumerate(sizes[:-2])]
+    mols.append(synthetic.make_chain(synthetic._seed(7070, 6), sizes[6]))
+    mols.append(synthetic.make_molecule(synthetic._seed(7070, 7), sizes[7], 0.3))
+    srv = sb.Server(max_batch_molecules=3, max_batches=4, cycles_per_launch=20, **CONTROLS)
+    kinds = {}
+    for k, m in enumerate(mols):
+        if m.natom <= 2048:
+            kinds[srv.submit(m)] = ("minimize", m)
+        kinds[srv.submit(m, evaluate=True)] = ("evaluate", m)
+        if k == 3:
+            time.sleep(0.05)
+    assert srv.drain(120.0)
+    results = srv.poll()
+    srv.close()
+    assert len(results) == len(kinds)
+    seen = {"minimize": 0, "evaluate": 0}
+    for r, arr in results:
+        kind, m = kinds[r["request_id"]]
+        assert r["kind"] == kind
+        seen[kind] += 1
+        if kind == "minimize":
+            c_alone, e_alone, cyc_alone, _ = _alone(m)
+            assert np.array_equal(arr, c_alone) and np.array_equal(r["energies"], e_alone)
+            assert r["cycles"] == cyc_alone
+            continue
+        f_alone, e_alone = _evaluated_alone(m)
+        assert np.array_equal(arr, f_alone)
+        assert np.array_equal(r["energies"], e_alone)
+        assert r["cycles"] == 0
+        assert r["rms_force"] == pytest.approx(np.sqrt((f_alone ** 2).mean()), rel=1e-12)
+        o = oracle.from_molecule(m).evaluate(m.coords)
+        got = np.array([r["energies"][sb.NRG_SLOTS[t]] for t in sb.TERM_ORDER])
+        scale = max(np.abs(o["energies"]).sum(), 10.0)
+        assert np.all(np.abs(got - o["energies"]) <= 1e-6 * scale)
+        err = np.sqrt(((arr - o["forces"]) ** 2).sum() / (o["forces"] ** 2).sum())
+        assert err <= 5e-6, (m.natom, err)
+    assert seen == {"minimize": len(mols) - 1, "evaluate": len(mols)}
+
+
+def test_minimization_of_a_large_molecule_is_refused_at_submit():
+    big = synthetic.make_chain(synthetic._seed(7171, 0), 2600)
+    srv = sb.Server(**CONTROLS)
+    with pytest.raises(sb.StormmB200Error, match="cannot be minimized"):
+        srv.submit(big)
+    rid = srv.submit(big, evaluate=True)          # an evaluation of it is served
+    assert srv.drain(60.0)
+    (r, f), = srv.poll()
+    assert r["request_id"] == rid and f.shape == (2600, 3)
+    srv.close()
