@@ -372,6 +372,33 @@ int sb_static_exclusion_mask(const sb_topology* top, int* supertile_stride_count
                              int* tile_map_idx, long long* n_tile_map, uint32_t* mask_data,
                              long long* n_mask_data);
 
+/* STORMM's StaticExclusionMaskSynthesis tables for nsys systems (system k uses
+ * tops[topology_index[k]]), built as Synthesis/static_mask_synthesis.cpp:84-200 combines the
+ * per-topology tables: supertile_map_bounds (nsys + 1 ints, caller-sized), supertile_map_idx,
+ * tile_map_idx and mask_data with the sizing protocol of sb_static_exclusion_mask.  Host only. */
+int sb_static_exclusion_mask_synthesis(const sb_topology* tops, int ntop,
+                                       const int* topology_index, int nsys,
+                                       int* supertile_map_bounds, int* supertile_map_idx,
+                                       long long* n_supertile_map, int* tile_map_idx,
+                                       long long* n_tile_map, uint32_t* mask_data,
+                                       long long* n_mask_data);
+
+/* STORMM's nonbonded work units for the same synthesis, as buildNonbondedWorkUnits and
+ * AtomGraphSynthesis::loadNonbondedWorkUnits lay them out (Synthesis/nonbonded_workunit.cpp:
+ * 454-755, nonbonded_workunit.tpp:8-150, ag_synthesis_mechanics.cpp:2668-2730): 64-int
+ * abstracts per unit (import count, up to 20 import starts, packed import sizes, instruction
+ * range, import systems, initialization mask, refresh start and code) and the tile
+ * instructions, two words (x: import slots, y: mask offset in the synthesis tables) per tile,
+ * each unit's list padded with zeros to a multiple of 32.  init_task is STORMM's
+ * InitializationTask (0 GENERAL_DYNAMICS ... 3 GB_MINIMIZATION ... 6 NONE); refresh work is
+ * assigned as with no GPU given.  The kernels of this library use their own work units; these
+ * tables are for callers that keep STORMM's.  Syntheses large enough for STORMM's 256-tile
+ * units return SB_ERR_UNSUPPORTED.  Sizing as sb_static_exclusion_mask. */
+int sb_nonbonded_work_units(const sb_topology* tops, int ntop, const int* topology_index,
+                            int nsys, int init_task, int random_cache_depth, int* abstracts,
+                            long long* n_abstracts, uint32_t* instructions,
+                            long long* n_instructions);
+
 /* ------------------------------------------------------------------------------------------ */
 /* Amber file intake                                                                           */
 /* ------------------------------------------------------------------------------------------ */

@@ -19,6 +19,13 @@
 //       prints "evals=<n> seconds=<t>".  With --minimize N it instead runs N-cycle minimizations
 //       and prints "minimizations=<n> seconds=<t>".
 //
+//   nbwu <list-file> <out.bin> [--init-task N]
+//       STORMM's nonbonded work units (Synthesis/nonbonded_workunit.cpp) for a synthesis: each
+//       line of <list-file> is "<prmtop> <system count>", the systems laid out topology by
+//       topology; writes the StaticExclusionMaskSynthesis tables and the abstracts and tile
+//       instructions AtomGraphSynthesis::loadNonbondedWorkUnits stores (InitializationTask N,
+//       default 3 = GB_MINIMIZATION).
+//
 // Options: --igb {0,1,2,5,7,8} (default 5 = OBC-II), --diel X (80), --salt X (0),
 //          --qtol X --qdisc X (charge smoothing, STORMM defaults), --scee X --scnb X,
 //          --quantize (round coordinates to the 2^-32 Angstrom fixed-point grid first).
@@ -44,6 +51,9 @@
 #include "Potential/static_exclusionmask.h"
 #include "Potential/valence_potential.h"
 #include "Restraints/restraint_apparatus.h"
+#include "Synthesis/atomgraph_synthesis.h"
+#include "Synthesis/static_mask_synthesis.h"
+#include "Synthesis/synthesis_abstracts.h"
 #include "Topology/atomgraph.h"
 #include "Trajectory/phasespace.h"
 
@@ -483,6 +493,61 @@ int runTime(const std::string &list_file, double seconds, const Options &opt) {
   return 0;
 }
 
+int runNbwu(const std::string &list_file, const std::string &out, const Options &opt,
+             int init_task) {
+  std::ifstream lst(list_file);
+  std::vector<std::string> tops;
+  std::vector<int> counts;
+  std::string top;
+  int count = 0;
+  while (lst >> top >> count) {
+    tops.push_back(top);
+    counts.push_back(count);
+  }
+  std::vector<AtomGraph> ags;
+  ags.reserve(tops.size());
+  for (const std::string &t : tops) {
+    ags.push_back(loadTopology(t, opt));
+  }
+  std::vector<AtomGraph*> ag_ptrs;
+  std::vector<int> index;
+  for (size_t k = 0; k < ags.size(); k++) {
+    ag_ptrs.push_back(&ags[k]);
+    for (int c = 0; c < counts[k]; c++) {
+      index.push_back(static_cast<int>(k));
+    }
+  }
+  synthesis::AtomGraphSynthesis poly_ag(ag_ptrs, index);
+  const synthesis::StaticExclusionMaskSynthesis poly_se(ag_ptrs, index);
+  poly_ag.loadNonbondedWorkUnits(poly_se, static_cast<synthesis::InitializationTask>(init_task),
+                                 0, card::GpuDetails());
+  const synthesis::SyNonbondedKit<double, double2> nbk = poly_ag.getDoublePrecisionNonbondedKit();
+  const synthesis::SeMaskSynthesisReader ser = poly_se.data();
+  RecordWriter rw(out);
+  rw.i("index", index);
+  rw.i("se_atom_counts", ser.atom_counts, ser.nsys);
+  rw.i("se_atom_offsets", ser.atom_offsets, ser.nsys);
+  rw.i("se_supertile_map_bounds", ser.supertile_map_bounds, ser.nsys + 1);
+  rw.i("se_supertile_map_idx", ser.supertile_map_idx, ser.supertile_map_bounds[ser.nsys]);
+  rw.i("se_tile_map_idx", ser.tile_map_idx, 256 * static_cast<size_t>(ser.nsupertile));
+  rw.u("se_mask_data", ser.mask_data, 32 * static_cast<size_t>(ser.ntile));
+  const size_t abs_len = 64;
+  rw.i("nbwu_abstracts", nbk.nbwu_abstracts, abs_len * nbk.nnbwu);
+  int insr_end = 0;
+  for (int w = 0; w < nbk.nnbwu; w++) {
+    insr_end = std::max(insr_end, nbk.nbwu_abstracts[abs_len * w + 27]);
+  }
+  const int insr_count = ((insr_end + 31) / 32) * 32;
+  std::vector<uint> insr(2 * static_cast<size_t>(insr_count));
+  for (int k = 0; k < insr_count; k++) {
+    insr[2 * k] = nbk.nbwu_insr[k].x;
+    insr[2 * k + 1] = nbk.nbwu_insr[k].y;
+  }
+  rw.u("nbwu_insr", insr.data(), insr.size());
+  std::printf("work units %d, instructions %d\n", nbk.nnbwu, insr_count);
+  return 0;
+}
+
 } // namespace
 
 int main(int argc, char* argv[]) {
@@ -493,6 +558,7 @@ int main(int argc, char* argv[]) {
   const std::string mode(argv[1]);
   std::vector<std::string> pos;
   Options opt;
+  int init_task = 3;
   for (int i = 2; i < argc; i++) {
     const std::string a(argv[i]);
     auto next = [&]() -> double {
@@ -517,6 +583,7 @@ int main(int argc, char* argv[]) {
     else if (a == "--clash-r0") opt.clash_r0 = next();
     else if (a == "--clash-ratio") opt.clash_ratio = next();
     else if (a == "--quantize") opt.quantize = true;
+    else if (a == "--init-task") init_task = static_cast<int>(next());
     else pos.push_back(a);
   }
   if (mode == "eval" && pos.size() == 3) {
@@ -524,6 +591,9 @@ int main(int argc, char* argv[]) {
   }
   if (mode == "minimize" && pos.size() == 3) {
     return runMinimize(pos[0], pos[1], pos[2], opt);
+  }
+  if (mode == "nbwu" && pos.size() == 2) {
+    return runNbwu(pos[0], pos[1], opt, init_task);
   }
   if (mode == "time" && pos.size() == 2) {
     return runTime(pos[0], std::atof(pos[1].c_str()), opt);

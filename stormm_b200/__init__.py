@@ -183,6 +183,12 @@ def library() -> ctypes.CDLL:
             "sb_amber_set_implicit_solvent": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
             "sb_amber_topology_destroy": (ctypes.c_int, [vp]),
             "sb_read_amber_coordinates": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, vp]),
+            "sb_static_exclusion_mask_synthesis": (ctypes.c_int, [ctypes.POINTER(Topology),
+                                                                  ctypes.c_int, vp, ctypes.c_int,
+                                                                  vp, vp, vp, vp, vp, vp, vp]),
+            "sb_nonbonded_work_units": (ctypes.c_int, [ctypes.POINTER(Topology), ctypes.c_int, vp,
+                                                       ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                       vp, vp, vp, vp]),
             "sb_last_error": (ctypes.c_char_p, []),
             "sb_version": (ctypes.c_char_p, []),
         }
@@ -300,6 +306,57 @@ def static_exclusion_mask(molecule):
                                         ctypes.byref(n[2])), "sb_static_exclusion_mask")
     return {"supertile_stride_count": nst.value, "supertile_map_idx": sup,
             "tile_map_idx": til, "mask_data": msk}
+
+
+def _synthesis_topologies(molecules, topology_index):
+    mols = list(molecules)
+    if topology_index is None:
+        topology_index = np.arange(len(mols), dtype=np.int32)
+    index = np.ascontiguousarray(topology_index, dtype=np.int32)
+    tops = [_TopologyArrays(m) for m in mols]
+    arr = (Topology * len(mols))(*[t.struct for t in tops])
+    return tops, arr, index
+
+
+def static_exclusion_mask_synthesis(molecules, topology_index=None):
+    """STORMM's StaticExclusionMaskSynthesis tables (host only): a dict with
+    supertile_map_bounds, supertile_map_idx, tile_map_idx and mask_data."""
+    lib = library()
+    tops, arr, index = _synthesis_topologies(molecules, topology_index)
+    bounds = np.zeros(index.size + 1, dtype=np.int32)
+    n = [ctypes.c_longlong(0) for _ in range(3)]
+    args = (arr, len(tops), index.ctypes.data, index.size)
+    _check(lib.sb_static_exclusion_mask_synthesis(*args, None, None, ctypes.byref(n[0]), None,
+                                                  ctypes.byref(n[1]), None, ctypes.byref(n[2])),
+           "sb_static_exclusion_mask_synthesis")
+    sup = np.zeros(n[0].value, dtype=np.int32)
+    til = np.zeros(n[1].value, dtype=np.int32)
+    msk = np.zeros(n[2].value, dtype=np.uint32)
+    _check(lib.sb_static_exclusion_mask_synthesis(*args, bounds.ctypes.data, sup.ctypes.data,
+                                                  ctypes.byref(n[0]), til.ctypes.data,
+                                                  ctypes.byref(n[1]), msk.ctypes.data,
+                                                  ctypes.byref(n[2])),
+           "sb_static_exclusion_mask_synthesis")
+    return {"supertile_map_bounds": bounds, "supertile_map_idx": sup, "tile_map_idx": til,
+            "mask_data": msk}
+
+
+def nonbonded_work_units(molecules, topology_index=None, init_task=3, random_cache_depth=0):
+    """STORMM's nonbonded work units for a synthesis (host only): (abstracts as an
+    (n_units, 64) int32 array, tile instructions as an (n, 2) uint32 array).  init_task is
+    STORMM's InitializationTask (3 = GB_MINIMIZATION)."""
+    lib = library()
+    tops, arr, index = _synthesis_topologies(molecules, topology_index)
+    na, ni = ctypes.c_longlong(0), ctypes.c_longlong(0)
+    args = (arr, len(tops), index.ctypes.data, index.size, int(init_task),
+            int(random_cache_depth))
+    _check(lib.sb_nonbonded_work_units(*args, None, ctypes.byref(na), None, ctypes.byref(ni)),
+           "sb_nonbonded_work_units")
+    a = np.zeros(na.value, dtype=np.int32)
+    ins = np.zeros(ni.value, dtype=np.uint32)
+    _check(lib.sb_nonbonded_work_units(*args, a.ctypes.data, ctypes.byref(na), ins.ctypes.data,
+                                       ctypes.byref(ni)), "sb_nonbonded_work_units")
+    return a.reshape(-1, 64), ins.reshape(-1, 2)
 
 
 def _host_array(ptr, count, ctype, dtype):

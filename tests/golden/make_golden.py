@@ -22,6 +22,11 @@ Fixtures written (numpy .npz, one per case):
   reference systems, with the neck tables STORMM looked the pairs up in.
 * ``minimize_m0.npz``: STORMM's CPU line minimizer (MolecularMechanics/minimization.tpp) on the
   64-atom molecule, energy history and final coordinates.
+* ``nbwu_<case>.npz`` (``--nbwu-only``): STORMM's StaticExclusionMaskSynthesis tables and
+  nonbonded work units (AtomGraphSynthesis::loadNonbondedWorkUnits) for syntheses of synthetic
+  molecules; each case names its molecules by generator, seed and size, the systems per
+  topology and the InitializationTask.  Small cases hold the arrays, large ones their SHA-256
+  digests and sizes.
 * ``synthetic_K64.npz`` and ``minimize_clash_k64.npz`` (``--clash-only``): a 64-atom molecule
   with close contacts (0.45 A start noise), its clash-mitigated evaluation (softened cores below
   1.5 A and below 0.9 of the pair's sigma) beside the plain one, and a minimization whose first
@@ -101,10 +106,15 @@ def main():
                     help="write only the clash-damping fixtures")
     ap.add_argument("--neck-only", action="store_true",
                     help="write only the neck GB (igb 7, 8) fixtures")
+    ap.add_argument("--nbwu-only", action="store_true",
+                    help="write only the nonbonded work-unit fixtures")
     args = ap.parse_args()
     if not os.path.exists(DRIVER):
         raise SystemExit("build the reference driver first: make -C oracle/ref -j8")
     with tempfile.TemporaryDirectory() as tmp:
+        if args.nbwu_only:
+            nbwu_cases(tmp)
+            return
         if args.neck_only:
             for name, seed, n, igb in (("N7", 8820, 80, "7"), ("N8", 8821, 80, "8")):
                 mol = synthetic.make_molecule(seed, n, noise=0.1, name=name)
@@ -179,6 +189,52 @@ def reference_systems(ref_root, tmp, models):
             rec["known_answer_gb"] = np.array([answers[key][ans_idx]])
             np.savez_compressed(os.path.join(HERE, f"reference_{sname}_igb{igb}.npz"), **rec)
             print("wrote", sname, igb, rec["energy_terms"][-1], answers[key][ans_idx])
+
+
+# (name, [(generator, seed, natom, systems)], InitializationTask, store arrays in full)
+NBWU_CASES = [
+    ("mixed", [("molecule", 4101, 24, 1), ("molecule", 4102, 70, 2),
+               ("molecule", 4103, 300, 3)], 3, True),
+    ("edges", [("molecule", 4201, 16, 3), ("molecule", 4202, 17, 1), ("molecule", 4203, 33, 2),
+               ("molecule", 4204, 64, 5), ("molecule", 4205, 250, 1)], 1, True),
+    ("pair1000", [("molecule", 4301, 1000, 2)], 0, True),
+    ("chains32", [("chain", 4401, 3000, 4), ("chain", 4402, 700, 3)], 5, False),
+    ("chains64", [("chain", 4501, 5000, 12), ("chain", 4502, 2600, 6)], 3, False),
+]
+
+
+def nbwu_molecule(gen, seed, natom):
+    return (synthetic.make_chain if gen == "chain" else synthetic.make_molecule)(seed, natom)
+
+
+def nbwu_cases(tmp):
+    import hashlib
+    for name, spec, task, full in NBWU_CASES:
+        lines = []
+        for k, (gen, seed, natom, count) in enumerate(spec):
+            top = os.path.join(tmp, f"{name}_{k}.top")
+            prmtop.write_prmtop(nbwu_molecule(gen, seed, natom), top)
+            lines.append(f"{top} {count}")
+        lst = os.path.join(tmp, f"{name}.txt")
+        with open(lst, "w") as f:
+            f.write("\n".join(lines) + "\n")
+        out = os.path.join(tmp, f"{name}.bin")
+        run_driver(["nbwu", lst, out, "--init-task", str(task)])
+        rec = read_records(out)
+        keep = {"generators": np.array([s[0] for s in spec]),
+                "seeds": np.array([s[1] for s in spec]), "natoms": np.array([s[2] for s in spec]),
+                "counts": np.array([s[3] for s in spec]), "init_task": np.array([task]),
+                "index": rec["index"]}
+        for key in ("se_supertile_map_bounds", "se_supertile_map_idx", "se_tile_map_idx",
+                    "se_mask_data", "nbwu_abstracts", "nbwu_insr"):
+            arr = rec[key]
+            if full:
+                keep[key] = arr
+            else:
+                keep[key + "_sha256"] = np.array([hashlib.sha256(arr.tobytes()).hexdigest()])
+                keep[key + "_size"] = np.array([arr.size])
+        np.savez_compressed(os.path.join(HERE, f"nbwu_{name}.npz"), **keep)
+        print("wrote nbwu", name, rec["nbwu_abstracts"].size // 64, "units")
 
 
 if __name__ == "__main__":

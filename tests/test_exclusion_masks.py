@@ -1,11 +1,13 @@
 """STORMM's StaticExclusionMask tables from sb_static_exclusion_mask, bit for bit against the
 tables STORMM built for every fixture (host code: runs without a GPU)."""
+import glob
 import os
 
 import numpy as np
 import pytest
 
 import stormm_b200 as sb
+from conftest import GOLDEN
 from fixtures import load, molecule_from_fixture, reference_paths, synthetic_paths
 
 
@@ -37,3 +39,57 @@ def test_static_exclusion_mask_rejects_small_outputs():
                                                sup.ctypes.data, ctypes.byref(n[0]), None,
                                                ctypes.byref(n[1]), None, ctypes.byref(n[2]))
     assert rc == -1
+
+
+def _nbwu_case(path):
+    from stormm_b200 import synthetic
+    g = load(os.path.basename(path))
+    mols = []
+    for gen, seed, n in zip(g["generators"], g["seeds"], g["natoms"]):
+        make = synthetic.make_chain if str(gen) == "chain" else synthetic.make_molecule
+        mols.append(make(int(seed), int(n)))
+    return g, mols
+
+
+def _same(g, key, got):
+    import hashlib
+    if key in g:
+        return np.array_equal(got, g[key].astype(got.dtype))
+    return (got.size == int(g[key + "_size"][0]) and
+            hashlib.sha256(np.ascontiguousarray(got).tobytes()).hexdigest() ==
+            str(g[key + "_sha256"][0]))
+
+
+NBWU_PATHS = sorted(glob.glob(os.path.join(GOLDEN, "nbwu_*.npz")))
+
+
+@pytest.mark.parametrize("path", NBWU_PATHS, ids=os.path.basename)
+def test_static_exclusion_mask_synthesis_is_bit_exact(path):
+    """The synthesis-level mask tables (topologies shared by several systems, indices shifted
+    past earlier topologies' tables) equal STORMM's StaticExclusionMaskSynthesis."""
+    g, mols = _nbwu_case(path)
+    ms = sb.static_exclusion_mask_synthesis(mols, g["index"])
+    for key in ("supertile_map_bounds", "supertile_map_idx", "tile_map_idx", "mask_data"):
+        assert _same(g, "se_" + key, ms[key]), key
+
+
+@pytest.mark.parametrize("path", NBWU_PATHS, ids=os.path.basename)
+def test_nonbonded_work_units_are_bit_exact(path):
+    """STORMM's nonbonded work units (8-, 16-, 32- and 64-tile targets, the import-limit
+    backtracking, initialization masks and refresh ranges of several InitializationTasks):
+    abstracts and tile instructions equal AtomGraphSynthesis::loadNonbondedWorkUnits'."""
+    g, mols = _nbwu_case(path)
+    abstracts, insr = sb.nonbonded_work_units(mols, g["index"], init_task=int(g["init_task"][0]))
+    assert _same(g, "nbwu_abstracts", abstracts.reshape(-1))
+    assert _same(g, "nbwu_insr", insr.reshape(-1))
+    # every tile of every system appears once
+    n_tiles = sum(((int(n) + 15) // 16) * ((int(n) + 15) // 16 + 1) // 2 * int(c)
+                  for n, c in zip(g["natoms"], g["counts"]))
+    assert int((abstracts[:, 27] - abstracts[:, 26]).sum()) == n_tiles
+
+
+def test_nonbonded_work_units_refuse_huge_syntheses():
+    from stormm_b200 import synthetic
+    big = synthetic.make_chain(4601, 5000)
+    with pytest.raises(sb.StormmB200Error, match="256-tile"):
+        sb.nonbonded_work_units([big], np.zeros(200, dtype=np.int32))
