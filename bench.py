@@ -408,7 +408,7 @@ def bench_minimization(args, world, rank, local, flush):
         "persistent_kernel_value": persistent,
         "gpu_launches_per_step": 1 + 8 * MIN_CYCLES + 2,
         "unit_packing": {"atoms_per_unit": tuned[0], "tiles_per_unit": tuned[1],
-                         "chosen_by": "sb_autotune of the evaluation over 9 packings"},
+                         "chosen_by": "sb_autotune of the evaluation over the fixed and wave-sized packings"},
         "l2": "flushed (256 MB write) before every timed step",
     }
 
