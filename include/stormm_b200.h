@@ -137,7 +137,8 @@ typedef struct {
   int device;                  /* CUDA device ordinal */
   int tiled_above_atoms;       /* molecules with more atoms are evaluated tile by tile from global
                                   memory, spread over the whole GPU (0: 2048, the on-chip limit;
-                                  32-2048); they cannot be minimized */
+                                  32-2048); the graph minimizer minimizes them, the persistent
+                                  one refuses them */
   int precision;               /* SB_PRECISION_SINGLE (default): FP32 arithmetic with fixed-point
                                   accumulation; SB_PRECISION_DOUBLE: FP64 arithmetic from double
                                   parameters (STORMM's PrecisionModel::DOUBLE), every molecule tile

@@ -862,13 +862,14 @@ Clash Synthesis::minimizerClash() const {
   return c;
 }
 
-void Synthesis::rejectTiledMinimization() const {
+void Synthesis::rejectTiledMinimization(int kernel) const {
   if (fp64) {
     throw Error(SB_ERR_UNSUPPORTED, "the FP64 mode evaluates; minimization runs in FP32");
   }
-  if (!h_tiled_systems.empty()) {
+  if (!h_tiled_systems.empty() && kernel != SB_MIN_GRAPH) {
     throw Error(SB_ERR_UNSUPPORTED, "molecules above " + std::to_string(tiled_threshold) +
-                " atoms are evaluated tile by tile and cannot be minimized on chip");
+                " atoms are evaluated tile by tile and cannot be minimized on chip by the "
+                "persistent kernel; the graph minimizer (SB_MIN_GRAPH) minimizes them");
   }
 }
 
@@ -1022,7 +1023,7 @@ int Synthesis::checkStatus(cudaStream_t stream) {
 // Line minimization (MolecularMechanics/hpc_minimization.cu:129-600)
 // ------------------------------------------------------------------------------------------------
 void Synthesis::minimizeBegin(const sb_minimize_controls &ctl, cudaStream_t stream) {
-  rejectTiledMinimization();
+  rejectTiledMinimization(ctl.kernel);
   if (ctl.total_cycles < 0 || ctl.sd_cycles < 0) {
     throw Error(SB_ERR_ARGUMENT, "cycle counts must not be negative");
   }
@@ -1103,11 +1104,13 @@ Synthesis::~Synthesis() {
 }
 
 // One batched evaluation of all systems (single = false) or of systems [first, first + count)
-// one launch each (single = true)
+// one launch each (single = true); molecules above the on-chip limit go tile by tile
 void Synthesis::evaluateFor(int first, int count, bool single, bool force, cudaStream_t stream,
                             const Clash &clash) {
   if (!single) {
     launchPlan(*eval_plan, SB_TERM_ALL, force, true, stream, clash);
+    launchTiledRange(0, static_cast<int>(h_tiled_systems.size()), SB_TERM_ALL, force, true,
+                     stream, clash);
     return;
   }
   DevSynthesis d = dev;
@@ -1117,6 +1120,11 @@ void Synthesis::evaluateFor(int first, int count, bool single, bool force, cudaS
   d.max_unit_slots = single_slots;
   clash.apply(&d);
   for (int s = first; s < first + count; s++) {
+    if (tiled_index[s] >= 0) {
+      launchTiledRange(tiled_index[s], tiled_index[s] + 1, SB_TERM_ALL, force, true, stream,
+                       clash);
+      continue;
+    }
     cudaCheck(launchEvalFused(d, s, s + 1, single_lj, SB_TERM_ALL, force, true, 1, threads,
                               stream, clash.on()), "per-system evaluation launch");
   }

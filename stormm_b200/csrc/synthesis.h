@@ -255,7 +255,7 @@ private:
   void launchTiledRange(int mol_begin, int mol_end, int terms, bool force, bool energy,
                         cudaStream_t stream, const Clash &clash = Clash());
   Clash minimizerClash() const;
-  void rejectTiledMinimization() const;
+  void rejectTiledMinimization(int kernel) const;
   void graphCycle(int first, int count, bool single, cudaStream_t stream);
   void graphFinalEnergy(int first, int count, bool single, cudaStream_t stream);
   void evaluateFor(int first, int count, bool single, bool force, cudaStream_t stream,

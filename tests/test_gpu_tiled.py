@@ -95,7 +95,7 @@ def test_large_chains_against_oracle():
         assert rms_rel(forces[k], ref["forces"]) <= FORCE_TOL, k
 
 
-def test_tiled_per_system_launches_equal_batched_and_minimization_is_rejected():
+def test_tiled_per_system_launches_equal_batched_and_persistent_minimization_is_rejected():
     mols = [synthetic.make_chain(synthetic._seed(7171, 0), 2200),
             synthetic.make_molecule(synthetic._seed(7171, 1), 90, 0.1),
             synthetic.make_chain(synthetic._seed(7171, 2), 2050)]
@@ -106,5 +106,56 @@ def test_tiled_per_system_launches_equal_batched_and_minimization_is_rejected():
     syn.evaluate_range(0, len(mols))
     assert np.array_equal(syn.forces_fixed()[0], f_b[0])
     assert np.array_equal(syn.energies_fixed(), e_b)
-    with pytest.raises(sb.StormmB200Error):
-        syn.minimize(total_cycles=2)
+    with pytest.raises(sb.StormmB200Error, match="graph minimizer"):
+        syn.minimize(total_cycles=2, kernel=sb.MIN_PERSISTENT)
+
+
+def _graph_minimize(mols, cycles, **opts):
+    syn = sb.Synthesis(mols, **opts)
+    syn.set_coordinates(np.concatenate([m.coords for m in mols]))
+    syn.minimize(total_cycles=cycles, sd_cycles=10, clash_cycles=4, kernel=sb.MIN_GRAPH,
+                 record_history=True)
+    assert syn.status() == 0
+    return syn
+
+
+def test_graph_minimization_of_tiled_molecules_follows_the_oracle():
+    """Molecules on the tiled path minimize with the graph minimizer: the tiled evaluations take
+    the place of the fused ones in each cycle's graph.  Small molecules routed there
+    (tiled_above_atoms=32) follow the FP64 oracle's minimizer as the fused path does: the first
+    trial energies to 1e-5 relative, the final energy within 1 % of the drop."""
+    mols = [synthetic.make_molecule(synthetic._seed(7272, k), n, 0.3)
+            for k, n in enumerate([40, 64, 96])]
+    cycles = 40
+    syn = _graph_minimize(mols, cycles, tiled_above_atoms=32)
+    hist = syn.minimize_history()
+    for k, m in enumerate(mols):
+        _, h_ref = oracle.from_molecule(m).minimize(m.coords, cycles, 10, clash_cycles=4)
+        np.testing.assert_allclose(hist[k, :3], h_ref[:3], rtol=1e-5, err_msg=f"molecule {k}")
+        drop = h_ref[0] - h_ref[-1]
+        assert abs(hist[k, -1] - h_ref[-1]) <= 0.01 * drop + 1e-3, (k, hist[k, -1], h_ref[-1])
+
+
+def test_graph_minimization_mixes_tiled_and_fused_molecules():
+    """A 2,200-atom chain beside small molecules: the small ones minimize exactly as without
+    the chain, the chain exactly as alone and as in the per-system launch sequence, and its
+    energy falls."""
+    chain = synthetic.make_chain(synthetic._seed(7373, 0), 2200, 0.2)
+    small = [synthetic.make_molecule(synthetic._seed(7373, k), n, 0.3)
+             for k, n in enumerate([30, 75, 120], start=1)]
+    cycles = 25
+    mixed = _graph_minimize(small + [chain], cycles)
+    only_small = _graph_minimize(small, cycles)
+    alone = _graph_minimize([chain], cycles)
+    n_small = sum(m.natom for m in small)
+    assert np.array_equal(mixed.coordinates()[:n_small], only_small.coordinates())
+    assert np.array_equal(mixed.energies_fixed()[:3], only_small.energies_fixed())
+    assert np.array_equal(mixed.coordinates()[n_small:], alone.coordinates())
+    assert np.array_equal(mixed.energies_fixed()[3], alone.energies_fixed()[0])
+    h = mixed.minimize_history()[3]
+    assert h[-1] < h[0]
+    per_system = sb.Synthesis([chain])
+    per_system.set_coordinates(chain.coords)
+    per_system.minimize_range(0, 1, total_cycles=cycles, sd_cycles=10, clash_cycles=4,
+                              kernel=sb.MIN_GRAPH)
+    assert np.array_equal(per_system.coordinates(), alone.coordinates())
