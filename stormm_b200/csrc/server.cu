@@ -206,9 +206,11 @@ public:
       throw Error(SB_ERR_ARGUMENT, "unknown request kind " + std::to_string(kind));
     }
     const int on_chip = (opt_.options.tiled_above_atoms > 0) ? opt_.options.tiled_above_atoms : 2048;
-    if (kind == SB_REQUEST_MINIMIZE && top->natom > on_chip) {
+    if (kind == SB_REQUEST_MINIMIZE && top->natom > on_chip &&
+        opt_.controls.kernel != SB_MIN_GRAPH) {
       throw Error(SB_ERR_UNSUPPORTED, "molecules above " + std::to_string(on_chip) +
-                  " atoms are evaluated tile by tile and cannot be minimized");
+                  " atoms are evaluated tile by tile and cannot be minimized by the persistent "
+                  "kernel; a server whose controls select SB_MIN_GRAPH minimizes them");
     }
     Request req(*top, xyz);
     req.kind = kind;

@@ -141,10 +141,30 @@ def test_evaluation_requests_mixed_with_minimizations():
 def test_minimization_of_a_large_molecule_is_refused_at_submit():
     big = synthetic.make_chain(synthetic._seed(7171, 0), 2600)
     srv = sb.Server(**CONTROLS)
-    with pytest.raises(sb.StormmB200Error, match="cannot be minimized"):
+    with pytest.raises(sb.StormmB200Error, match="cannot be minimized by the persistent"):
         srv.submit(big)
     rid = srv.submit(big, evaluate=True)          # an evaluation of it is served
     assert srv.drain(60.0)
     (r, f), = srv.poll()
     assert r["request_id"] == rid and f.shape == (2600, 3)
     srv.close()
+
+
+def test_graph_kernel_server_minimizes_a_large_molecule():
+    big = synthetic.make_chain(synthetic._seed(7171, 1), 2300, 0.2)
+    small = synthetic.make_molecule(synthetic._seed(7171, 2), 60, 0.3)
+    controls = dict(total_cycles=30, sd_cycles=10, convergence_rms=0.0, kernel=sb.MIN_GRAPH)
+    srv = sb.Server(cycles_per_launch=10, **controls)
+    ids = {srv.submit(big): big, srv.submit(small): small}
+    assert srv.drain(120.0)
+    results = srv.poll()
+    srv.close()
+    assert len(results) == 2
+    for r, xyz in results:
+        m = ids[r["request_id"]]
+        alone = sb.Synthesis([m])
+        alone.set_coordinates(m.coords)
+        alone.minimize(**controls)
+        assert r["cycles"] == 30
+        assert np.array_equal(xyz, alone.coordinates())
+        assert np.array_equal(r["energies"], alone.energies()[0])
