@@ -194,6 +194,9 @@ struct DevMinimizer {
   float* xcg;                    // conjugate-gradient direction (kcal/mol/A, not normalized)
   float* ycg;
   float* zcg;
+  double* xcg64;                 // the direction in FP64 (FP64 mode only, else null)
+  double* ycg64;
+  double* zcg64;
   double* l_move;                // per system: baseline move length (A)
   int* cycle;                    // per system: completed line-minimization cycles
   int* done;                     // per system: nonzero once the RMS force met the target

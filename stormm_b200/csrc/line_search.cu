@@ -44,7 +44,9 @@ __device__ __forceinline__ int firstWarp() {
 
 __device__ __forceinline__ int warpStride() { return (gridDim.x * blockDim.x) >> 5; }
 
-// Move every atom of a system by step (fixed-point units per unit of direction)
+// Move every atom of a system by step (fixed-point units per unit of direction); DBL: the FP64
+// mode's direction
+template <bool DBL>
 __device__ __forceinline__ void moveSystem(const DevSynthesis &d, const DevMinimizer &m, int sys,
                                            double step, int lane) {
   if (step == 0.0) {
@@ -54,13 +56,20 @@ __device__ __forceinline__ void moveSystem(const DevSynthesis &d, const DevMinim
   const int base = d.atom_start[sys];
   for (int a = lane; a < natom; a += 32) {
     const int gi = base + a;
-    m.xcrd[gi] += __double2ll_rn(static_cast<double>(m.xcg[gi]) * step);
-    m.ycrd[gi] += __double2ll_rn(static_cast<double>(m.ycg[gi]) * step);
-    m.zcrd[gi] += __double2ll_rn(static_cast<double>(m.zcg[gi]) * step);
+    if (DBL) {
+      m.xcrd[gi] += __double2ll_rn(m.xcg64[gi] * step);
+      m.ycrd[gi] += __double2ll_rn(m.ycg64[gi] * step);
+      m.zcrd[gi] += __double2ll_rn(m.zcg64[gi] * step);
+    }
+    else {
+      m.xcrd[gi] += __double2ll_rn(static_cast<double>(m.xcg[gi]) * step);
+      m.ycrd[gi] += __double2ll_rn(static_cast<double>(m.ycg[gi]) * step);
+      m.zcrd[gi] += __double2ll_rn(static_cast<double>(m.zcg[gi]) * step);
+    }
   }
 }
 
-template <bool HIST>
+template <bool HIST, bool DBL>
 __global__ void __launch_bounds__(kLineThreads)
 kLineStart(const DevSynthesis d, const DevMinimizer m, int first, int count) {
   const int lane = threadIdx.x & 31;
@@ -124,23 +133,39 @@ kLineStart(const DevSynthesis d, const DevMinimizer m, int first, int count) {
         const long long ix = d.xfrc[gi];
         const long long iy = d.yfrc[gi];
         const long long iz = d.zfrc[gi];
-        float cx = static_cast<float>(static_cast<double>(ix) * inv_fs);
-        float cy = static_cast<float>(static_cast<double>(iy) * inv_fs);
-        float cz = static_cast<float>(static_cast<double>(iz) * inv_fs);
-        if (fabs(gam) > kVeryTiny) {
-          const float gf = static_cast<float>(gam);
-          cx = fmaf(gf, m.xcg[gi], cx);
-          cy = fmaf(gf, m.ycg[gi], cy);
-          cz = fmaf(gf, m.zcg[gi], cz);
+        if (DBL) {
+          double cx = static_cast<double>(ix) * inv_fs;
+          double cy = static_cast<double>(iy) * inv_fs;
+          double cz = static_cast<double>(iz) * inv_fs;
+          if (fabs(gam) > kVeryTiny) {
+            cx = fma(gam, m.xcg64[gi], cx);
+            cy = fma(gam, m.ycg64[gi], cy);
+            cz = fma(gam, m.zcg64[gi], cz);
+          }
+          m.xcg64[gi] = cx;
+          m.ycg64[gi] = cy;
+          m.zcg64[gi] = cz;
+          ms = cx * cx + cy * cy + cz * cz;
         }
-        m.xcg[gi] = cx;
-        m.ycg[gi] = cy;
-        m.zcg[gi] = cz;
+        else {
+          float cx = static_cast<float>(static_cast<double>(ix) * inv_fs);
+          float cy = static_cast<float>(static_cast<double>(iy) * inv_fs);
+          float cz = static_cast<float>(static_cast<double>(iz) * inv_fs);
+          if (fabs(gam) > kVeryTiny) {
+            const float gf = static_cast<float>(gam);
+            cx = fmaf(gf, m.xcg[gi], cx);
+            cy = fmaf(gf, m.ycg[gi], cy);
+            cz = fmaf(gf, m.zcg[gi], cz);
+          }
+          m.xcg[gi] = cx;
+          m.ycg[gi] = cy;
+          m.zcg[gi] = cz;
+          ms = static_cast<double>(cx) * cx + static_cast<double>(cy) * cy +
+               static_cast<double>(cz) * cz;
+        }
         m.xprv[gi] = ix;
         m.yprv[gi] = iy;
         m.zprv[gi] = iz;
-        ms = static_cast<double>(cx) * cx + static_cast<double>(cy) * cy +
-             static_cast<double>(cz) * cz;
       }
       msum += warpSumDouble(ms);
     }
@@ -155,11 +180,12 @@ kLineStart(const DevSynthesis d, const DevMinimizer m, int first, int count) {
       line[kLineAct] = 1.0;
     }
     __syncwarp();
-    moveSystem(d, m, sys, inv_norm * s_move * gpos_scale, lane);
+    moveSystem<DBL>(d, m, sys, inv_norm * s_move * gpos_scale, lane);
   }
 }
 
 // Second (move 1) or third (move 2) trial point
+template <bool DBL>
 __global__ void __launch_bounds__(kLineThreads)
 kLineMove(const DevSynthesis d, const DevMinimizer m, int first, int count, int move) {
   const int lane = threadIdx.x & 31;
@@ -185,11 +211,12 @@ kLineMove(const DevSynthesis d, const DevMinimizer m, int first, int count, int 
       line[kLineMfac] = mfac;
       line[(move == 1) ? kLineMv2 : kLineMv3] = mv_prev + mfac;
     }
-    moveSystem(d, m, sys, step, lane);
+    moveSystem<DBL>(d, m, sys, step, lane);
   }
 }
 
 // Cubic placement after the third trial point
+template <bool DBL>
 __global__ void __launch_bounds__(kLineThreads)
 kLineFinish(const DevSynthesis d, const DevMinimizer m, int first, int count) {
   const int lane = threadIdx.x & 31;
@@ -212,7 +239,7 @@ kLineFinish(const DevSynthesis d, const DevMinimizer m, int first, int count) {
       m.l_move[sys] = s_move * new_base;
       m.cycle[sys] += 1;
     }
-    moveSystem(d, m, sys, step, lane);
+    moveSystem<DBL>(d, m, sys, step, lane);
   }
 }
 
@@ -244,21 +271,40 @@ cudaError_t launchLineStep(const DevSynthesis &d, const DevMinimizer &m, int fir
     return cudaSuccess;
   }
   const int grid = lineGrid(count);
+  const bool dbl = (m.xcg64 != nullptr);
   switch (step) {
     case 0:
       if (m.history != nullptr) {
-        kLineStart<true><<<grid, kLineThreads, 0, stream>>>(d, m, first, count);
+        if (dbl) {
+          kLineStart<true, true><<<grid, kLineThreads, 0, stream>>>(d, m, first, count);
+        }
+        else {
+          kLineStart<true, false><<<grid, kLineThreads, 0, stream>>>(d, m, first, count);
+        }
+      }
+      else if (dbl) {
+        kLineStart<false, true><<<grid, kLineThreads, 0, stream>>>(d, m, first, count);
       }
       else {
-        kLineStart<false><<<grid, kLineThreads, 0, stream>>>(d, m, first, count);
+        kLineStart<false, false><<<grid, kLineThreads, 0, stream>>>(d, m, first, count);
       }
       break;
     case 1:
     case 2:
-      kLineMove<<<grid, kLineThreads, 0, stream>>>(d, m, first, count, step);
+      if (dbl) {
+        kLineMove<true><<<grid, kLineThreads, 0, stream>>>(d, m, first, count, step);
+      }
+      else {
+        kLineMove<false><<<grid, kLineThreads, 0, stream>>>(d, m, first, count, step);
+      }
       break;
     case 3:
-      kLineFinish<<<grid, kLineThreads, 0, stream>>>(d, m, first, count);
+      if (dbl) {
+        kLineFinish<true><<<grid, kLineThreads, 0, stream>>>(d, m, first, count);
+      }
+      else {
+        kLineFinish<false><<<grid, kLineThreads, 0, stream>>>(d, m, first, count);
+      }
       break;
     case 4:
       if (m.history != nullptr) {

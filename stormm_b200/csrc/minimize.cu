@@ -417,6 +417,11 @@ __global__ void kMinimizerReset(DevMinimizer m, int nsys, int natom_padded, doub
     m.xcg[i] = 0.0f;
     m.ycg[i] = 0.0f;
     m.zcg[i] = 0.0f;
+    if (m.xcg64 != nullptr) {
+      m.xcg64[i] = 0.0;
+      m.ycg64[i] = 0.0;
+      m.zcg64[i] = 0.0;
+    }
   }
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nsys; i += stride) {
     m.l_move[i] = dx0;

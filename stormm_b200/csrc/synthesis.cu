@@ -863,8 +863,9 @@ Clash Synthesis::minimizerClash() const {
 }
 
 void Synthesis::rejectTiledMinimization(int kernel) const {
-  if (fp64) {
-    throw Error(SB_ERR_UNSUPPORTED, "the FP64 mode evaluates; minimization runs in FP32");
+  if (fp64 && kernel != SB_MIN_GRAPH) {
+    throw Error(SB_ERR_UNSUPPORTED, "the FP64 mode minimizes with the graph minimizer "
+                "(SB_MIN_GRAPH) only");
   }
   if (!h_tiled_systems.empty() && kernel != SB_MIN_GRAPH) {
     throw Error(SB_ERR_UNSUPPORTED, "molecules above " + std::to_string(tiled_threshold) +
@@ -1024,6 +1025,9 @@ int Synthesis::checkStatus(cudaStream_t stream) {
 // ------------------------------------------------------------------------------------------------
 void Synthesis::minimizeBegin(const sb_minimize_controls &ctl, cudaStream_t stream) {
   rejectTiledMinimization(ctl.kernel);
+  if (fp64 && ctl.clash_cycles > 0 && (ctl.clash_distance > 0.0 || ctl.clash_ratio > 0.0)) {
+    throw Error(SB_ERR_UNSUPPORTED, "softened cores are not provided in the FP64 mode");
+  }
   if (ctl.total_cycles < 0 || ctl.sd_cycles < 0) {
     throw Error(SB_ERR_ARGUMENT, "cycle counts must not be negative");
   }
@@ -1048,6 +1052,11 @@ void Synthesis::minimizeBegin(const sb_minimize_controls &ctl, cudaStream_t stre
     d_mdone.allocate(nsys);
     d_line.allocate(static_cast<size_t>(nsys) * kLineFields);
     d_queue.allocate(2);
+    if (fp64) {
+      d_xcg64.allocate(np);
+      d_ycg64.allocate(np);
+      d_zcg64.allocate(np);
+    }
   }
   history_stride = 0;
   if (ctl.record_history) {
@@ -1069,6 +1078,11 @@ void Synthesis::minimizeBegin(const sb_minimize_controls &ctl, cudaStream_t stre
   m.xcg = d_xcg.p;
   m.ycg = d_ycg.p;
   m.zcg = d_zcg.p;
+  if (fp64) {
+    m.xcg64 = d_xcg64.p;
+    m.ycg64 = d_ycg64.p;
+    m.zcg64 = d_zcg64.p;
+  }
   m.l_move = d_lmove.p;
   m.cycle = d_mcycle.p;
   m.done = d_mdone.p;

@@ -227,6 +227,7 @@ public:
   // line-minimization state, allocated by the first minimization
   DeviceArray<long long> d_xprv, d_yprv, d_zprv;
   DeviceArray<float> d_xcg, d_ycg, d_zcg;
+  DeviceArray<double> d_xcg64, d_ycg64, d_zcg64;   // FP64 mode: the direction in double
   DeviceArray<double> d_lmove, d_rmsf, d_history;
   DeviceArray<int> d_mcycle, d_mdone, d_queue;
   int history_stride = 0;
