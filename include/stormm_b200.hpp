@@ -75,6 +75,10 @@ enum class ImplicitSolventModel {                                  // Topology/a
 enum class AtomicRadiusSet {                                       // Topology/atomgraph_enumerators.h:150
   NONE, BONDI, AMBER6, MBONDI, MBONDI2, MBONDI3, PARSE
 };
+enum class InitializationTask {                                    // Synthesis/synthesis_enumerators.h:109
+  GENERAL_DYNAMICS, GB_DYNAMICS, GENERAL_MINIMIZATION, GB_MINIMIZATION, LANGEVIN_DYNAMICS,
+  GB_LANGEVIN_DYNAMICS, NONE
+};
 enum class TrajectoryKind { POSITIONS, VELOCITIES, FORCES };      // Trajectory/trajectory_enumerators.h
 enum class StateVariable {                                         // Potential/energy_enumerators.h:36-68
   BOND = 0, ANGLE, PROPER_DIHEDRAL, IMPROPER_DIHEDRAL, UREY_BRADLEY, CHARMM_IMPROPER, CMAP, VDW,
@@ -459,6 +463,39 @@ public:
   bool isUploaded() const { return syn != nullptr; }
   PrecisionModel getPrecisionModel() const { return precision; }
 
+  /* STORMM's AtomGraphSynthesis::loadNonbondedWorkUnits (atomgraph_synthesis.h:429-431): the
+   * nonbonded work units exactly as STORMM builds them, for callers that keep STORMM's launch
+   * data (the kernels here use their own).  The mask synthesis argument stands for the
+   * exclusions of this synthesis' topologies. */
+  void loadNonbondedWorkUnits(const class StaticExclusionMaskSynthesis &,
+                              InitializationTask init_request = InitializationTask::NONE,
+                              int random_cache_depth = 0, const GpuDetails & = GpuDetails()) {
+    std::vector<sb_topology> tops;
+    for (AtomGraph* ag : topologies) {
+      tops.push_back(ag->abi());
+    }
+    long long na = 0, ni = 0;
+    const int task = static_cast<int>(init_request);
+    detail::check(sb_nonbonded_work_units(tops.data(), static_cast<int>(tops.size()),
+                                          indices.data(), static_cast<int>(indices.size()), task,
+                                          random_cache_depth, nullptr, &na, nullptr, &ni),
+                  "AtomGraphSynthesis::loadNonbondedWorkUnits");
+    nbwu_abstracts.assign(static_cast<size_t>(na), 0);
+    nbwu_instructions.assign(static_cast<size_t>(ni), 0u);
+    detail::check(sb_nonbonded_work_units(tops.data(), static_cast<int>(tops.size()),
+                                          indices.data(), static_cast<int>(indices.size()), task,
+                                          random_cache_depth, nbwu_abstracts.data(), &na,
+                                          nbwu_instructions.data(), &ni),
+                  "AtomGraphSynthesis::loadNonbondedWorkUnits");
+  }
+  int getNonbondedWorkUnitCount() const { return static_cast<int>(nbwu_abstracts.size() / 64); }
+  /* 64 ints per work unit, STORMM's TILE_GROUPS abstract layout */
+  const std::vector<int> &getNonbondedWorkUnitAbstracts() const { return nbwu_abstracts; }
+  /* (x, y) words of each tile instruction, each unit's list padded to a multiple of 32 */
+  const std::vector<uint32_t> &getNonbondedWorkUnitInstructions() const {
+    return nbwu_instructions;
+  }
+
   /* The device synthesis (throws before upload) */
   sb_synthesis* handle() const {
     if (syn == nullptr) {
@@ -477,6 +514,8 @@ private:
   PrecisionModel precision = PrecisionModel::SINGLE;
   sb_synthesis* syn = nullptr;
   mutable const void* bound_coordinates = nullptr;
+  std::vector<int> nbwu_abstracts;
+  std::vector<uint32_t> nbwu_instructions;
 
   static std::vector<int> identity(size_t n) {
     std::vector<int> v(n);

@@ -50,6 +50,12 @@ int hostChecks(FILE* out, const std::string &top, const std::string &crd) {
   poly_ag.setImplicitSolventModel(ImplicitSolventModel::OBC_GB_II);
   PhaseSpaceSynthesis poly_ps({ps, ps}, {&ag, &ag});
   std::fprintf(out, "systems 1 %d\n", poly_ps.getSystemCount());
+  StaticExclusionMaskSynthesis poly_se(poly_ag);
+  poly_ag.loadNonbondedWorkUnits(poly_se, InitializationTask::GB_MINIMIZATION);
+  const std::vector<int> &abstracts = poly_ag.getNonbondedWorkUnitAbstracts();
+  const std::vector<uint32_t> &insr = poly_ag.getNonbondedWorkUnitInstructions();
+  put(out, "nbwu_abstracts", std::vector<double>(abstracts.begin(), abstracts.end()));
+  put(out, "nbwu_insr", std::vector<double>(insr.begin(), insr.end()));
   bool ok = true;
   ok &= throwsRuntimeError([&]() { AtomGraph missing(top + ".absent"); }, "cannot open", out,
                            "missing_file");

@@ -76,6 +76,9 @@ def test_header_compiles_and_host_paths_work(tmp_path):
     assert int(out["atoms"][0]) == 30 and int(out["systems"][0]) == 2
     np.testing.assert_allclose(out["coords"].reshape(-1, 3),
                                sb.read_amber_coordinates(files[1], 30), rtol=0, atol=0)
+    abstracts, insr = sb.nonbonded_work_units([mol], np.array([0, 0]), init_task=3)
+    np.testing.assert_array_equal(out["nbwu_abstracts"], abstracts.reshape(-1))
+    np.testing.assert_array_equal(out["nbwu_insr"], insr.reshape(-1))
     for label, (ok, msg) in out["errors"].items():
         assert ok, (label, msg)
     assert set(out["errors"]) == {"missing_file", "empty_scorecard", "topology_index",
