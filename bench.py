@@ -556,10 +556,32 @@ def bench_served(local):
             "mean_cycles": float(np.mean([r["cycles"] for r in res])),
             "converged_fraction": float(np.mean([r["converged"] for r in res])),
         })
+    # A mixed stream: every other request a force + energy evaluation, the rest minimizations
+    rate = 1000.0
+    srv = sb.Server(options=sb.default_options(device=local), cycles_per_launch=50)
+    rng = np.random.default_rng(4242)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=int(rate * SERVED_WINDOW_S * 2) + 8))
+    arrivals = arrivals[arrivals < SERVED_WINDOW_S]
+    start = time.perf_counter()
+    for k, ta in enumerate(arrivals):
+        while time.perf_counter() - start < ta:
+            pass
+        srv.submit(mols[k % len(mols)], prepared=prepared[k % len(mols)], evaluate=(k % 2 == 1))
+    drained = srv.drain(600.0)
+    res = [r for r, _ in srv.poll(max_results=len(arrivals) + 16, coordinates=False)]
+    srv.close()
+    mixed = {"offered_per_s": rate, "evaluation_share": 0.5, "requests": len(arrivals),
+             "completed": len(res), "drained": bool(drained)}
+    for kind in ("evaluate", "minimize"):
+        lat = np.array([r["finish_time"] - r["submit_time"] for r in res if r["kind"] == kind])
+        if lat.size:
+            mixed[kind] = {"completed": int(lat.size),
+                           "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                           "p99_ms": float(np.percentile(lat, 99) * 1e3)}
     return {"workload": SERVED_WORKLOAD, "unit": "requests/s, latency ms (submit to result)",
             "arrival_window_s": SERVED_WINDOW_S, "cycles_per_launch": 50,
             "throughput_note": "completions over first submit to last result, drain tail included",
-            "sweep": sweeps}
+            "sweep": sweeps, "mixed_with_evaluations": mixed}
 
 
 def main():
