@@ -142,8 +142,7 @@ typedef struct {
   int precision;               /* SB_PRECISION_SINGLE (default): FP32 arithmetic with fixed-point
                                   accumulation; SB_PRECISION_DOUBLE: FP64 arithmetic from double
                                   parameters (STORMM's PrecisionModel::DOUBLE), every molecule tile
-                                  by tile; minimized by the graph minimizer with an FP64 direction,
-                                  without softened cores */
+                                  by tile; minimized by the graph minimizer with an FP64 direction */
   /* Neck GB (igb 7, 8): STORMM's NeckGeneralizedBornTable, neck_table_size^2 maximum
    * separations and values indexed [j_index * size + i_index], with the per-atom index
    * round(20 (r_pb - 1)) (radii must lie in [1, 2] A); read by sb_synthesis_create */

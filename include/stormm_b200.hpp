@@ -34,7 +34,7 @@
  *     over the first one's.
  *   - The precision model is chosen at upload (FP32 arithmetic with fixed-point accumulation,
  *     or FP64 arithmetic); a launch with the other model throws.  FP64 minimization runs the
- *     graph minimizer with the direction in FP64 and takes no clash damping.
+ *     graph minimizer with the direction in FP64.
  *   - The GB model, dielectric and salt concentration are one per synthesis.
  *   - MolecularMechanicsControls, CacheResource, Thermostat, ReductionBridge, LineMinimization,
  *     StopWatch and the AccumulationMethod argument are accepted and have nothing to carry: a
@@ -1104,7 +1104,7 @@ inline void minimize(PrecisionModel prec, const AtomGraphSynthesis &poly_ag,
  * getClashDampingCycles() cycles; coordinates move in place on the device (download the
  * PhaseSpaceSynthesis to read them) and the ScoreCard receives the final energies and the
  * total energy every getDiagnosticPrintFrequency() cycles.  With PrecisionModel::DOUBLE the
- * synthesis must have been uploaded for FP64 and the clash-damping cycles set to zero. */
+ * synthesis must have been uploaded for FP64. */
 inline void launchMinimization(PrecisionModel prec, const AtomGraphSynthesis &poly_ag,
                                const StaticExclusionMaskSynthesis &, PhaseSpaceSynthesis *poly_ps,
                                const MinimizeControls &mincon, MolecularMechanicsControls *,

@@ -179,6 +179,10 @@ struct DevPrecise {
   double gb_offset;
   double* radius;                // per padded atom: effective GB radius of the evaluation
   double* sde;                   // per padded atom: dE/dR after the chain-rule prefactor
+  double clash_distance;         // softened cores, as DevSynthesis' clash fields, in double
+  double clash_ratio;
+  int clash_cycles;
+  const int* clash_cycle;
 };
 
 // Line-minimization state (MolecularMechanics/line_minimization.h:15-221 and the conjugate

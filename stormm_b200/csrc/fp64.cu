@@ -192,12 +192,80 @@ struct Radii64 {
 };
 
 // Pass 2 payload: w1 = charge x sqrt(Coulomb constant), w2 = effective radius
-template <bool FORCE, bool ENERGY, bool NB, bool GB>
+// Softened cores in FP64 (STORMM's Potential/soft_core_potentials.tpp, the FP32 path's
+// softCorePair in double): the clash distance and sigma ratio of a system, scaled by its
+// minimization progress when a cycle count is given
+__device__ __forceinline__ double2 clashScaled64(const DevPrecise &p, int sysid) {
+  const int cycle = (p.clash_cycle != nullptr) ? p.clash_cycle[sysid] : -1;
+  if (cycle < 0) {
+    return make_double2(p.clash_distance, p.clash_ratio);
+  }
+  if (cycle >= p.clash_cycles) {
+    return make_double2(0.0, 0.0);
+  }
+  const double progress = static_cast<double>(p.clash_cycles - cycle) /
+                          static_cast<double>(p.clash_cycles);
+  return make_double2(p.clash_distance * progress, p.clash_ratio * progress);
+}
+
+// Quadratic Coulomb core below cd: qiqj (a (r + 1)^2 + b), continuous in value and slope
+__device__ __forceinline__ double2 quadraticCore64(double cd) {
+  if (cd <= 0.0) {
+    return make_double2(0.0, 0.0);
+  }
+  const double a = -0.5 / (cd * cd * (cd + 1.0));
+  return make_double2(a, 1.0 / cd - a * (cd + 1.0) * (cd + 1.0));
+}
+
+// Coulomb and Lennard-Jones energies of one pair with softened cores added to *e_elec, *e_vdw;
+// returns the force factor (force on j = factor x (r_j - r_i))
+__device__ __forceinline__ double softCorePair64(double r, double invr, double qiqj, double lja,
+                                                 double ljb, double cd, double2 qc, double ratio,
+                                                 double* e_elec, double* e_vdw) {
+  double fmag;
+  if (r < cd) {
+    const double rp = r + 1.0;
+    *e_elec += qiqj * (qc.x * rp * rp + qc.y);
+    fmag = (r > 1.0e-10) ? qiqj * (2.0 * qc.x + 2.0 * qc.x * invr) : 0.0;
+  }
+  else {
+    *e_elec += qiqj * invr;
+    fmag = -(qiqj * invr * invr * invr);
+  }
+  const double rl = (ljb > 1.0e-6) ? ratio * pow(lja / ljb, 1.0 / 6.0) : 0.0;
+  if (r < rl) {
+    const double il = 1.0 / rl;
+    const double il2 = il * il;
+    const double il6 = il2 * il2 * il2;
+    const double a = ((6.0 * ljb - 12.0 * lja * il6) * il * il6) /
+                     (((4.0 * rl + 12.0) * rl + 12.0) * rl + 4.0);
+    const double rlp = rl + 1.0;
+    const double rlp2 = rlp * rlp;
+    const double b = (lja * il6 - ljb) * il6 - a * rlp2 * rlp2;
+    const double rp = r + 1.0;
+    const double a3 = a * rp * rp * rp;
+    *e_vdw += a3 * rp + b;
+    if (r > 1.0e-10) {
+      fmag += 4.0 * a3 * invr;
+    }
+  }
+  else {
+    const double invr2 = invr * invr;
+    const double invr4 = invr2 * invr2;
+    *e_vdw += (lja * invr4 * invr4 - ljb * invr2) * invr4;
+    fmag += (6.0 * ljb - 12.0 * lja * invr4 * invr2) * invr4 * invr4;
+  }
+  return fmag;
+}
+
+template <bool FORCE, bool ENERGY, bool NB, bool GB, bool CLASH>
 struct Pair64 {
   Stage64 v;
   const double2* lj;   // the molecule's Lennard-Jones table
   int nt;
   double kappa, inv_diel;
+  double2 cl = make_double2(0.0, 0.0);   // the system's clash distance and sigma ratio
+  double2 qc = make_double2(0.0, 0.0);   // its quadratic Coulomb core
   double4 ai, bi;
   int code_i;
   unsigned mask;
@@ -221,7 +289,20 @@ struct Pair64 {
     const double r2 = dx * dx + dy * dy + dz * dz;
     const double qiqj = ai.w * aj.w;
     double fmag = 0.0;
-    if (NB && ((mask >> jl) & 1u) == 0u) {
+    if (NB && CLASH && ((mask >> jl) & 1u) == 0u && (cl.x > 0.0 || cl.y > 0.0)) {
+      const double invr = 1.0 / sqrt(r2);
+      const double2 ab = lj[code_i + v.code[jslot]];
+      double ee = 0.0, ev = 0.0;
+      fmag = softCorePair64(r2 * invr, invr, qiqj, ab.x, ab.y, cl.x, qc, cl.y, &ee, &ev);
+      if (ENERGY) {
+        e_elec += ee;
+        e_vdw += ev;
+      }
+      if (!FORCE) {
+        fmag = 0.0;
+      }
+    }
+    else if (NB && ((mask >> jl) & 1u) == 0u) {
       const double invr2 = 1.0 / r2;
       const double invr = sqrt(invr2);
       const double invr4 = invr2 * invr2;
@@ -395,7 +476,7 @@ kRadii64(const DevSynthesis d, const DevPrecise p, const DevTiled t, int tile_be
   }
 }
 
-template <bool FORCE, bool ENERGY, bool NB, bool GB>
+template <bool FORCE, bool ENERGY, bool NB, bool GB, bool CLASH>
 __global__ void __launch_bounds__(256)
 kPair64(const DevSynthesis d, const DevPrecise p, const DevTiled t, int tile_begin,
         int tile_end) {
@@ -419,8 +500,12 @@ kPair64(const DevSynthesis d, const DevPrecise p, const DevTiled t, int tile_beg
         mask = __ldg(&d.mask_pool[static_cast<size_t>(midx) * 32 + lane]);
       }
     }
-    Pair64<FORCE, ENERGY, NB, GB> f(v, p.ljab + d.lj_start[sysid], d.lj_ntypes[sysid],
-                                    p.kappa, p.inv_dielectric);
+    Pair64<FORCE, ENERGY, NB, GB, CLASH> f(v, p.ljab + d.lj_start[sysid], d.lj_ntypes[sysid],
+                                           p.kappa, p.inv_dielectric);
+    if (CLASH) {
+      f.cl = clashScaled64(p, sysid);
+      f.qc = quadraticCore64(f.cl.x);
+    }
     f.begin(lane, mask);
     walkTile(f, ti, lane);
     const int base = d.atom_start[sysid];
@@ -629,7 +714,7 @@ __device__ __forceinline__ void energyAdd(const DevSynthesis &d, int sysid, int 
 
 // Terms of the systems of tiled molecules [mol_begin, mol_end): the FP64 mode routes every
 // system to the tiled path in system order, so those molecules are consecutive systems
-template <bool FORCE, bool ENERGY>
+template <bool FORCE, bool ENERGY, bool CLASH>
 __global__ void __launch_bounds__(256)
 kValence64(const DevSynthesis d, const DevPrecise p, const DevTiled t, int mol_begin,
            int mol_end) {
@@ -770,15 +855,32 @@ kValence64(const DevSynthesis d, const DevPrecise p, const DevTiled t, int mol_b
       const double invr2 = 1.0 / dot3(dv, dv);
       const double invr = sqrt(invr2);
       const double invr4 = invr2 * invr2;
-      if (FORCE) {
-        const double fmag = -(qiqj * invr * invr2) +
-                            (6.0 * ljb - 12.0 * lja * invr4 * invr2) * invr4 * invr4;
-        at.force(ijkl.x, fmag * dv.x, fmag * dv.y, fmag * dv.z);
-        at.force(ijkl.w, -fmag * dv.x, -fmag * dv.y, -fmag * dv.z);
+      const double2 cl = CLASH ? clashScaled64(p, sysid) : make_double2(0.0, 0.0);
+      if (CLASH && (cl.x > 0.0 || cl.y > 0.0)) {
+        // clash-softened 1-4 pair (valence_potential.tpp:1337-1357)
+        double ee = 0.0, ev = 0.0;
+        const double fmag = softCorePair64(1.0 / invr, invr, qiqj, lja, ljb, cl.x,
+                                           quadraticCore64(cl.x), cl.y, &ee, &ev);
+        if (FORCE) {
+          at.force(ijkl.x, fmag * dv.x, fmag * dv.y, fmag * dv.z);
+          at.force(ijkl.w, -fmag * dv.x, -fmag * dv.y, -fmag * dv.z);
+        }
+        if (ENERGY) {
+          energyAdd(d, sysid, kElec14, ee);
+          energyAdd(d, sysid, kVdw14, ev);
+        }
       }
-      if (ENERGY) {
-        energyAdd(d, sysid, kElec14, qiqj * invr);
-        energyAdd(d, sysid, kVdw14, lja * invr4 * invr4 * invr4 - ljb * invr4 * invr2);
+      else {
+        if (FORCE) {
+          const double fmag = -(qiqj * invr * invr2) +
+                              (6.0 * ljb - 12.0 * lja * invr4 * invr2) * invr4 * invr4;
+          at.force(ijkl.x, fmag * dv.x, fmag * dv.y, fmag * dv.z);
+          at.force(ijkl.w, -fmag * dv.x, -fmag * dv.y, -fmag * dv.z);
+        }
+        if (ENERGY) {
+          energyAdd(d, sysid, kElec14, qiqj * invr);
+          energyAdd(d, sysid, kVdw14, lja * invr4 * invr4 * invr4 - ljb * invr4 * invr2);
+        }
       }
     }
   }
@@ -791,7 +893,7 @@ kValence64(const DevSynthesis d, const DevPrecise p, const DevTiled t, int mol_b
 cudaError_t launchTiled64(const DevSynthesis &d, const DevPrecise &p, const DevTiled &t,
                           const int* h_tile_prefix, const int* h_atom_prefix, int mol_begin,
                           int mol_end, int terms, bool force, bool energy, bool workspace,
-                          int sm_count, cudaStream_t stream) {
+                          int sm_count, cudaStream_t stream, bool clash) {
   if (mol_end <= mol_begin) {
     return cudaSuccess;
   }
@@ -804,9 +906,13 @@ cudaError_t launchTiled64(const DevSynthesis &d, const DevPrecise &p, const DevT
   const int agrid = atomGrid(ae - ab, sm_count);
   if (vale) {
     const int vgrid = sm_count * 4;
-    if (force && energy) kValence64<true, true><<<vgrid, 256, 0, stream>>>(d, p, t, mol_begin, mol_end);
-    else if (force) kValence64<true, false><<<vgrid, 256, 0, stream>>>(d, p, t, mol_begin, mol_end);
-    else kValence64<false, true><<<vgrid, 256, 0, stream>>>(d, p, t, mol_begin, mol_end);
+#define SB_VALE64(C)                                                                            \
+    if (force && energy) kValence64<true, true, C><<<vgrid, 256, 0, stream>>>(d, p, t, mol_begin, mol_end); \
+    else if (force) kValence64<true, false, C><<<vgrid, 256, 0, stream>>>(d, p, t, mol_begin, mol_end);    \
+    else kValence64<false, true, C><<<vgrid, 256, 0, stream>>>(d, p, t, mol_begin, mol_end);
+    if (clash) { SB_VALE64(true) }
+    else { SB_VALE64(false) }
+#undef SB_VALE64
   }
   if (gb) {
     kRadii64<<<tgrid, 256, 0, stream>>>(d, p, t, tb, te);
@@ -820,9 +926,11 @@ cudaError_t launchTiled64(const DevSynthesis &d, const DevPrecise &p, const DevT
   }
   if (nb || gb) {
 #define SB_PAIR(F, E)                                                                       \
-    if (nb && gb) kPair64<F, E, true, true><<<tgrid, 256, 0, stream>>>(d, p, t, tb, te);     \
-    else if (nb) kPair64<F, E, true, false><<<tgrid, 256, 0, stream>>>(d, p, t, tb, te);    \
-    else kPair64<F, E, false, true><<<tgrid, 256, 0, stream>>>(d, p, t, tb, te);
+    if (nb && gb && clash) kPair64<F, E, true, true, true><<<tgrid, 256, 0, stream>>>(d, p, t, tb, te); \
+    else if (nb && gb) kPair64<F, E, true, true, false><<<tgrid, 256, 0, stream>>>(d, p, t, tb, te);    \
+    else if (nb && clash) kPair64<F, E, true, false, true><<<tgrid, 256, 0, stream>>>(d, p, t, tb, te); \
+    else if (nb) kPair64<F, E, true, false, false><<<tgrid, 256, 0, stream>>>(d, p, t, tb, te);         \
+    else kPair64<F, E, false, true, false><<<tgrid, 256, 0, stream>>>(d, p, t, tb, te);
     if (force && energy) { SB_PAIR(true, true) }
     else if (force) { SB_PAIR(true, false) }
     else { SB_PAIR(false, true) }

@@ -40,7 +40,7 @@ cudaError_t launchTiled(const DevSynthesis &d, const DevTiled &t, const int* h_t
 cudaError_t launchTiled64(const DevSynthesis &d, const DevPrecise &p, const DevTiled &t,
                           const int* h_tile_prefix, const int* h_atom_prefix, int mol_begin,
                           int mol_end, int terms, bool force, bool energy, bool workspace,
-                          int sm_count, cudaStream_t stream);
+                          int sm_count, cudaStream_t stream, bool clash);
 cudaError_t launchImportCoordinates(const double* d_xyz, const int* d_map, int natom,
                                     double scale, long long* xcrd, long long* ycrd,
                                     long long* zcrd, int* xo, int* yo, int* zo, int* status,
@@ -835,11 +835,14 @@ void Synthesis::launchTiledRange(int mol_begin, int mol_end, int terms, bool for
   cudaCheck(cudaMemsetAsync(d_tiled_psi.p, 0, np * sizeof(long long), stream), "memset");
   cudaCheck(cudaMemsetAsync(d_tiled_de.p, 0, np * sizeof(long long), stream), "memset");
   if (fp64) {
-    if (clash.on()) {
-      throw Error(SB_ERR_UNSUPPORTED, "softened cores are not provided in the FP64 mode");
-    }
-    cudaCheck(launchTiled64(dev, dev64, dev_tiled, h_tile_prefix.data(), h_atom_prefix.data(),
-                            mol_begin, mol_end, terms, force, energy, true, sm_count, stream),
+    DevPrecise p = dev64;
+    p.clash_distance = clash.on() ? clash.distance64 : 0.0;
+    p.clash_ratio = clash.on() ? clash.ratio64 : 0.0;
+    p.clash_cycles = clash.cycles;
+    p.clash_cycle = clash.cycle;
+    cudaCheck(launchTiled64(dev, p, dev_tiled, h_tile_prefix.data(), h_atom_prefix.data(),
+                            mol_begin, mol_end, terms, force, energy, true, sm_count, stream,
+                            clash.on()),
               "FP64 evaluation launch");
     return;
   }
@@ -856,6 +859,8 @@ Clash Synthesis::minimizerClash() const {
   if (dev_min.clash_cycles > 0) {
     c.distance = dev_min.clash_distance;
     c.ratio = dev_min.clash_ratio;
+    c.distance64 = min_clash_distance;
+    c.ratio64 = min_clash_ratio;
     c.cycles = dev_min.clash_cycles;
     c.cycle = dev_min.cycle;
   }
@@ -1025,9 +1030,6 @@ int Synthesis::checkStatus(cudaStream_t stream) {
 // ------------------------------------------------------------------------------------------------
 void Synthesis::minimizeBegin(const sb_minimize_controls &ctl, cudaStream_t stream) {
   rejectTiledMinimization(ctl.kernel);
-  if (fp64 && ctl.clash_cycles > 0 && (ctl.clash_distance > 0.0 || ctl.clash_ratio > 0.0)) {
-    throw Error(SB_ERR_UNSUPPORTED, "softened cores are not provided in the FP64 mode");
-  }
   if (ctl.total_cycles < 0 || ctl.sd_cycles < 0) {
     throw Error(SB_ERR_ARGUMENT, "cycle counts must not be negative");
   }
@@ -1092,9 +1094,13 @@ void Synthesis::minimizeBegin(const sb_minimize_controls &ctl, cudaStream_t stre
   m.sd_cycles = ctl.sd_cycles;
   m.max_cycles = ctl.total_cycles;
   m.drms = ctl.convergence_rms;
+  min_clash_distance = 0.0;
+  min_clash_ratio = 0.0;
   if (ctl.clash_cycles > 0 && (ctl.clash_distance > 0.0 || ctl.clash_ratio > 0.0)) {
     m.clash_cycles = ctl.clash_cycles;
     m.clash_distance = static_cast<float>(ctl.clash_distance);
+    min_clash_distance = ctl.clash_distance;
+    min_clash_ratio = ctl.clash_ratio;
     m.clash_ratio = static_cast<float>(ctl.clash_ratio);
   }
   m.queue = d_queue.p;
@@ -1593,6 +1599,8 @@ int sb_evaluate_clash(sb_synthesis* syn, int terms, int eval_force, int eval_ene
     sb::Clash clash;
     clash.distance = static_cast<float>(clash_distance);
     clash.ratio = static_cast<float>(clash_ratio);
+    clash.distance64 = clash_distance;
+    clash.ratio64 = clash_ratio;
     need(syn)->evaluate(terms, eval_force != 0, eval_energy != 0, asStream(stream), clash);
   });
 }

@@ -112,6 +112,8 @@ struct UnitPlan {
 struct Clash {
   float distance = 0.0f;
   float ratio = 0.0f;
+  double distance64 = 0.0;        // the same in double, for the FP64 mode
+  double ratio64 = 0.0;
   int cycles = 0;
   const int* cycle = nullptr;
   bool on() const { return distance > 0.0f || ratio > 0.0f; }
@@ -228,6 +230,7 @@ public:
   DeviceArray<long long> d_xprv, d_yprv, d_zprv;
   DeviceArray<float> d_xcg, d_ycg, d_zcg;
   DeviceArray<double> d_xcg64, d_ycg64, d_zcg64;   // FP64 mode: the direction in double
+  double min_clash_distance = 0.0, min_clash_ratio = 0.0;   // the minimizer's, in double
   DeviceArray<double> d_lmove, d_rmsf, d_history;
   DeviceArray<int> d_mcycle, d_mdone, d_queue;
   int history_stride = 0;

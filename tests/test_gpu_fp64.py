@@ -105,17 +105,39 @@ def test_fp64_mode_limits():
     syn.set_coordinates(mol.coords)
     with pytest.raises(sb.StormmB200Error, match="graph minimizer"):
         syn.minimize(total_cycles=3, kernel=sb.MIN_PERSISTENT)
-    with pytest.raises(sb.StormmB200Error, match="softened cores"):
-        syn.minimize(total_cycles=3, clash_cycles=2, kernel=sb.MIN_GRAPH)
-    with pytest.raises(sb.StormmB200Error):
-        syn.evaluate_clash(0.2, 0.5)
     with pytest.raises(sb.StormmB200Error):
         sb.Synthesis([mol], precision=7)
 
 
-def test_fp64_mode_minimization_follows_the_oracle():
+def test_fp64_mode_clash_mitigated_evaluation_matches_stormm():
+    """Softened Coulomb and Lennard-Jones cores (1-4 pairs included) in FP64 against STORMM's
+    clash-mitigated FP64 evaluation of the same molecule, to the FP64 mode's tolerances."""
+    g = load("synthetic_K64.npz")
+    mol = molecule_from_fixture(g)
+    syn = sb.Synthesis([mol], precision=sb.PRECISION_DOUBLE, **solvent_options(g), **BITS)
+    syn.set_coordinates(mol.coords)
+    syn.initialize()
+    syn.evaluate_clash(float(g["clash_r0"][0]), float(g["clash_ratio"][0]))
+    assert syn.status() == 0
+    r = oracle.from_fixture(g).evaluate(_on_grid(mol.coords),
+                                        clash_distance=float(g["clash_r0"][0]),
+                                        clash_ratio=float(g["clash_ratio"][0]))
+    scale = max(np.abs(r["energies"]).sum(), 10.0)
+    assert np.all(np.abs(syn.energy_terms()[0] - r["energies"]) <= 1e-10 * scale)
+    assert rms_rel(syn.forces(), r["forces"]) <= 1e-10
+    # and against STORMM's own results at the unrounded coordinates, as the FP32 path
+    scale = max(np.abs(g["clash_energy_terms"]).sum(), 10.0)
+    assert np.all(np.abs(syn.energy_terms()[0] - g["clash_energy_terms"]) <= 1e-7 * scale)
+    assert rms_rel(syn.forces(), g["clash_frc_total"].reshape(-1, 3)) <= 1e-7
+
+
+@pytest.mark.parametrize("clash_cycles", [0, 4])
+def test_fp64_mode_minimization_follows_the_oracle(clash_cycles):
+    # wide softened cores (1 A, 0.9 sigma) so that the damped cycles change the trajectory
+    soft = dict(clash_distance=1.0, clash_ratio=0.9)
     """STORMM's launchMinimization with PrecisionModel::DOUBLE: the graph minimizer over the
-    FP64 evaluations with the conjugate direction kept in FP64.  Against the oracle's FP64
+    FP64 evaluations with the conjugate direction kept in FP64, with and without clash-damped
+    leading cycles.  Against the oracle's FP64
     minimizer (pinned to STORMM's CPU minimizer) from the same grid coordinates: the first ten
     cycles' energies to 1e-8 relative (1e-9 to 1e-10 measured) and the final energy within 1e-6
     of the energy drop (1e-9 to 1e-12 measured), and always closer than the FP32 path, which
@@ -127,15 +149,18 @@ def test_fp64_mode_minimization_follows_the_oracle():
     cycles, sd = 60, 20
     syn = sb.Synthesis(mols, precision=sb.PRECISION_DOUBLE, **BITS)
     syn.set_coordinates(np.concatenate([m.coords for m in mols]))
-    syn.minimize(total_cycles=cycles, sd_cycles=sd, kernel=sb.MIN_GRAPH, record_history=True)
+    syn.minimize(total_cycles=cycles, sd_cycles=sd, clash_cycles=clash_cycles,
+                 kernel=sb.MIN_GRAPH, record_history=True, **soft)
     assert syn.status() == 0
     hist = syn.minimize_history()
     f32 = sb.Synthesis(mols)
     f32.set_coordinates(np.concatenate([m.coords for m in mols]))
-    f32.minimize(total_cycles=cycles, sd_cycles=sd, kernel=sb.MIN_GRAPH, record_history=True)
+    f32.minimize(total_cycles=cycles, sd_cycles=sd, clash_cycles=clash_cycles,
+                 kernel=sb.MIN_GRAPH, record_history=True, **soft)
     hist32 = f32.minimize_history()
     for k, m in enumerate(mols):
-        _, h_ref = oracle.from_molecule(m).minimize(_on_grid(m.coords), cycles, sd)
+        _, h_ref = oracle.from_molecule(m).minimize(_on_grid(m.coords), cycles, sd,
+                                                    clash_cycles=clash_cycles, **soft)
         rel64 = np.abs(hist[k] - h_ref) / np.abs(h_ref)
         rel32 = np.abs(hist32[k] - h_ref) / np.abs(h_ref)
         drop = h_ref[0] - h_ref[-1]
