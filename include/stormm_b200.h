@@ -407,8 +407,10 @@ int sb_nonbonded_work_units(const sb_topology* tops, int ntop, const int* topolo
  * (Topology/atomgraph.h:83,156, atomgraph_detailers.cpp:677-1120).  Host only, no device
  * needed.  Charges come out in electrons, Lennard-Jones tables expanded to n_types^2, 1-2 / 1-3
  * / 1-4 exclusions from the bond graph, GB radii and screening factors as the file holds them.
- * Refused: periodic topologies (SB_ERR_UNSUPPORTED) and nonzero 10-12 hydrogen-bond terms.
- * CHARMM Urey-Bradley, improper and CMAP terms are counted in the view but not evaluated. */
+ * Refused: nonzero 10-12 hydrogen-bond terms and massless particles (virtual sites,
+ * SB_ERR_UNSUPPORTED).  A unit cell is reported in the view and not
+ * applied (this path evaluates in isolated boundary conditions); CHARMM Urey-Bradley, improper
+ * and CMAP terms are counted in the view but not evaluated. */
 typedef struct sb_amber_topology sb_amber_topology;
 
 typedef struct {
@@ -424,6 +426,7 @@ typedef struct {
   int cmap_count;                   /* CHARMM terms present in the file (not evaluated) */
   int urey_bradley_count;
   int charmm_improper_count;
+  int unit_cell;                    /* the file's IFBOX (0: none); recorded, not applied */
 } sb_amber_view;
 
 int sb_read_amber_topology(const char* prmtop_path, sb_amber_topology** out);

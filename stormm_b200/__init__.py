@@ -104,7 +104,7 @@ class AmberView(ctypes.Structure):
         ("exclusion_bounds", _P * 3), ("exclusion_list", _P * 3), ("radius_set", ctypes.c_char_p),
         ("title", ctypes.c_char_p), ("implicit_solvent", ctypes.c_int),
         ("cmap_count", ctypes.c_int), ("urey_bradley_count", ctypes.c_int),
-        ("charmm_improper_count", ctypes.c_int),
+        ("charmm_improper_count", ctypes.c_int), ("unit_cell", ctypes.c_int),
     ]
 
 
@@ -430,6 +430,7 @@ def read_amber(prmtop, inpcrd=None, igb=None, radius_set=0):
         mol.cmap_count = v.cmap_count
         mol.urey_bradley_count = v.urey_bradley_count
         mol.charmm_improper_count = v.charmm_improper_count
+        mol.unit_cell = v.unit_cell
     finally:
         lib.sb_amber_topology_destroy(h)
     if inpcrd is not None:

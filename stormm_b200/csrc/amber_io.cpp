@@ -22,9 +22,10 @@
 // negative is improper (Amber's convention, followed by atomgraph_detailers.cpp).  1-2, 1-3 and
 // 1-4 exclusions are the atoms one, two and three bonds away in the bond graph, as STORMM's
 // mapExclusions (Topology/atomgraph_refinement.cpp:2735-2935) derives them; the file's
-// EXCLUDED_ATOMS_LIST is not used.  Periodic topologies (IFBOX > 0) are refused: this path is
-// non-periodic.  CHARMM terms (Urey-Bradley, CHARMM impropers, CMAP) are counted and reported
-// but not evaluated by this library.
+// EXCLUDED_ATOMS_LIST is not used.  A topology's unit cell (IFBOX > 0) is reported, not
+// applied: this path evaluates in isolated boundary conditions.  Massless particles (virtual
+// sites) are refused.  CHARMM terms (Urey-Bradley, CHARMM impropers, CMAP) are counted and
+// reported but not evaluated by this library.
 //
 // sb_amber_set_implicit_solvent assigns the per-atom GB parameters the way STORMM's
 // AtomGraph::setImplicitSolventModel does (Topology/atomgraph_setters.cpp:672-1060): first an
@@ -65,6 +66,7 @@ struct sb_amber_topology {
   std::string radius_set, title;
   int igb = -1;                                  // model applied by sb_amber_set_implicit_solvent
   int cmap_count = 0, urey_bradley_count = 0, charmm_improper_count = 0;
+  int ifbox = 0;
 };
 
 namespace sb {
@@ -120,6 +122,9 @@ std::map<std::string, Section> readSections(const std::string &path) {
       p++;
       while (p < line.size() && std::isdigit(static_cast<unsigned char>(line[p]))) {
         p++;
+      }
+      if (p < line.size() && line[p] == '(') {
+        p++;                                    // nested form, e.g. %FORMAT(8(F9.5))
       }
       if (p >= line.size()) {
         throw Error(SB_ERR_ARGUMENT, "malformed %FORMAT line in " + path + ": " + line);
@@ -342,10 +347,9 @@ sb_amber_topology* readTopology(const std::string &path) {
     if (n <= 0 || ntypes <= 0) {
       throw Error(SB_ERR_ARGUMENT, "topology " + path + " declares no atoms or no atom types");
     }
-    if (ptr.size() > 27 && ptr[27] > 0) {
-      throw Error(SB_ERR_UNSUPPORTED, "topology " + path + " is periodic (IFBOX " +
-                  std::to_string(ptr[27]) + "); this path evaluates non-periodic systems");
-    }
+    // a unit cell (IFBOX > 0) is recorded, not applied: this path evaluates every system in
+    // isolated boundary conditions, as STORMM's GB evaluation of such a topology does
+    t->ifbox = (ptr.size() > 27) ? ptr[27] : 0;
     t->natom = n;
     t->ntypes = ntypes;
     t->title = text(secs, "TITLE");
@@ -360,6 +364,12 @@ sb_amber_topology* readTopology(const std::string &path) {
     t->mass = numbers<double>(secs, "MASS", true, path);
     needCount(t->mass.size(), n, "MASS", path);
     t->mass.resize(n);
+    for (int i = 0; i < n; i++) {
+      if (!(t->mass[i] > 1.0e-6)) {
+        throw Error(SB_ERR_UNSUPPORTED, "topology " + path + " holds massless particles "
+                    "(virtual sites), which this path does not evaluate");
+      }
+    }
     t->z_numbers = numbers<int>(secs, "ATOMIC_NUMBER", false, path);
     if (t->z_numbers.empty()) {
       t->z_numbers.resize(n);
@@ -759,6 +769,7 @@ void fillView(const sb_amber_topology* t, sb_amber_view* v) {
   v->cmap_count = t->cmap_count;
   v->urey_bradley_count = t->urey_bradley_count;
   v->charmm_improper_count = t->charmm_improper_count;
+  v->unit_cell = t->ifbox;
 }
 
 // ASCII restart / inpcrd: title, "natom [time]", then 3 natom coordinates in 12-column fields
