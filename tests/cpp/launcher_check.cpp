@@ -181,6 +181,24 @@ int deviceChecks(FILE* out, const std::vector<std::string> &files) {
   }
   put(out, "min_history", hist);
   put(out, "min_coords", xyz);
+
+  // The same minimization with PrecisionModel::DOUBLE on a synthesis uploaded for FP64
+  AtomGraphSynthesis poly_ag64(ag_list, systems);
+  poly_ag64.setImplicitSolventModel(ImplicitSolventModel::OBC_GB_II);
+  PhaseSpaceSynthesis poly_ps64(coords, ag_list, systems);
+  StaticExclusionMaskSynthesis poly_se64(poly_ag64);
+  poly_ag64.upload(PrecisionModel::DOUBLE);
+  poly_ps64.upload();
+  ScoreCard result64 = launchMinimization(poly_ag64, poly_se64, &poly_ps64, mincon, gpu,
+                                          PrecisionModel::DOUBLE);
+  poly_ps64.download();
+  std::vector<double> xyz64;
+  for (int s = 0; s < nsys; s++) {
+    const std::vector<double> c = poly_ps64.getInterlacedCoordinates(s);
+    xyz64.insert(xyz64.end(), c.begin(), c.end());
+  }
+  put(out, "min64_potential", result64.reportPotentialEnergies());
+  put(out, "min64_coords", xyz64);
   return 0;
 }
 

@@ -149,3 +149,14 @@ def test_launchers_match_python_path_and_oracle(tmp_path):
     samples = np.concatenate([np.append(hist[s, 0:40:10], hist[s, 40]) for s in range(nsys)])
     np.testing.assert_array_equal(cpp["min_history"], samples)
     assert np.all(cpp["min_potential"] < cpp["potential"])
+
+    # PrecisionModel::DOUBLE: the same minimization on a synthesis uploaded for FP64
+    syn64 = sb.Synthesis(mols, topology_index=index, igb=sb.SB_GB_OBC2,
+                         precision=sb.PRECISION_DOUBLE)
+    syn64.set_coordinates(xyz)
+    syn64.minimize(total_cycles=40, sd_cycles=10, clash_cycles=5, clash_distance=0.2,
+                   clash_ratio=0.5, convergence_rms=0.0, kernel=sb.MIN_GRAPH)
+    np.testing.assert_array_equal(cpp["min64_coords"], syn64.coordinates().reshape(-1))
+    fin64 = syn64.energies().reshape(nsys, -1)
+    np.testing.assert_allclose(cpp["min64_potential"], fin64[:, :13].sum(axis=1), rtol=1e-14,
+                               atol=1e-9)
