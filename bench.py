@@ -389,6 +389,30 @@ def bench_minimization(args, world, rank, local, flush):
     persistent = MIN_NSYS / (ev0.elapsed_time(ev1) / 1000.0)
     assert syn.status() == 0
     syn.close()
+    # FP64 mode (PrecisionModel::DOUBLE) on the first 256 molecules, one timed run after a short
+    # warm-up, and its final energies against the FP32 graph minimizer's
+    n64 = 256
+    m64 = mols[:n64]
+    x64 = np.concatenate([m.coords for m in m64])
+    s64 = sb.Synthesis(m64, device=local, precision=sb.PRECISION_DOUBLE)
+    s64.set_coordinates(x64)
+    s64.minimize(total_cycles=5, sd_cycles=2, kernel=sb.MIN_GRAPH)
+    s64.set_coordinates(x64)
+    torch.cuda.synchronize()
+    ev0, ev1 = _event_pair()
+    ev0.record()
+    s64.minimize(total_cycles=MIN_CYCLES, sd_cycles=MIN_SD_CYCLES, kernel=sb.MIN_GRAPH)
+    ev1.record()
+    torch.cuda.synchronize()
+    fp64_value = n64 / (ev0.elapsed_time(ev1) / 1000.0)
+    e64 = s64.energy_terms().sum(axis=1)
+    assert s64.status() == 0
+    s64.close()
+    fp64_mode = {"value": fp64_value, "unit": "minimizations/s", "molecules": n64,
+                 "cycles": MIN_CYCLES,
+                 "fp32_final_energy_rel_vs_fp64_median": float(np.median(
+                     np.abs(e_final[:n64] - e64) / np.maximum(np.abs(e64), 1.0))),
+                 "note": "graph minimizer over the FP64 evaluations, conjugate direction in FP64"}
     evals = MIN_NSYS * (4 * MIN_CYCLES + 1)
     return {
         "value": value, "unit": "minimizations/s", "workload": MIN_WORKLOAD,
@@ -406,6 +430,7 @@ def bench_minimization(args, world, rank, local, flush):
         "mean_energy_drop": (float(np.mean(e_start - e_final)) if e_start is not None else None),
         "kernel": "graph (one CUDA graph per cycle: 4 batched evaluations + 4 line-search kernels)",
         "persistent_kernel_value": persistent,
+        "fp64_mode": fp64_mode,
         "gpu_launches_per_step": 1 + 8 * MIN_CYCLES + 2,
         "unit_packing": {"atoms_per_unit": tuned[0], "tiles_per_unit": tuned[1],
                          "chosen_by": "sb_autotune of the evaluation over the fixed and wave-sized packings"},
