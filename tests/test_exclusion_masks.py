@@ -93,3 +93,20 @@ def test_nonbonded_work_units_refuse_huge_syntheses():
     big = synthetic.make_chain(4601, 5000)
     with pytest.raises(sb.StormmB200Error, match="256-tile"):
         sb.nonbonded_work_units([big], np.zeros(200, dtype=np.int32))
+
+
+def test_work_unit_and_mask_synthesis_argument_checks():
+    from stormm_b200 import synthetic
+    m = synthetic.make_molecule(4701, 40)
+    with pytest.raises(sb.StormmB200Error, match="initialization task"):
+        sb.nonbonded_work_units([m], [0], init_task=9)
+    with pytest.raises(sb.StormmB200Error, match="out of range"):
+        sb.nonbonded_work_units([m], [1])
+    with pytest.raises(sb.StormmB200Error, match="out of range"):
+        sb.static_exclusion_mask_synthesis([m], [0, 2])
+    # a synthesis of one system reproduces the single-topology tables
+    one = sb.static_exclusion_mask(m)
+    syn = sb.static_exclusion_mask_synthesis([m], [0])
+    assert np.array_equal(syn["supertile_map_idx"], one["supertile_map_idx"])
+    assert np.array_equal(syn["tile_map_idx"], one["tile_map_idx"])
+    assert np.array_equal(syn["mask_data"], one["mask_data"])
