@@ -3,6 +3,7 @@
   python -m stormm_b200.profile_case [--molecules 256] [--evals 4] [--energy-only]
   python -m stormm_b200.profile_case --workload minimization --molecules 4096 --minimize 20
   python -m stormm_b200.profile_case --workload chains --molecules 16 --evals 3
+  python -m stormm_b200.profile_case --workload chains --molecules 16 --evals 3 --precision double
 
 The first form builds the first molecules of the batched single-point workload (16-256 atoms),
 uploads them and runs a few force + energy evaluations; the second builds the first molecules
@@ -25,6 +26,7 @@ def main():
     ap.add_argument("--evals", type=int, default=4)
     ap.add_argument("--energy-only", action="store_true")
     ap.add_argument("--minimize", type=int, default=0, help="minimization cycles")
+    ap.add_argument("--precision", default="single", choices=["single", "double"])
     args = ap.parse_args()
     import stormm_b200 as sb
     from stormm_b200 import synthetic
@@ -34,7 +36,8 @@ def main():
         mols = synthetic.workload_chains(args.molecules)
     else:
         mols = synthetic.workload_batched_single_point(args.molecules)
-    syn = sb.Synthesis(mols)
+    syn = sb.Synthesis(mols, precision=(sb.PRECISION_DOUBLE if args.precision == "double"
+                                        else sb.PRECISION_SINGLE))
     syn.set_coordinates(np.concatenate([m.coords for m in mols]))
     if args.minimize > 0:
         syn.minimize(total_cycles=args.minimize, sd_cycles=min(50, args.minimize))
