@@ -477,7 +477,7 @@ kRadii64(const DevSynthesis d, const DevPrecise p, const DevTiled t, int tile_be
 }
 
 template <bool FORCE, bool ENERGY, bool NB, bool GB, bool CLASH>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
 kPair64(const DevSynthesis d, const DevPrecise p, const DevTiled t, int tile_begin,
         int tile_end) {
   __shared__ double4 pa[kTiledWarps * kSlots64], pb[kTiledWarps * kSlots64];
