@@ -73,6 +73,7 @@ def _lib():
                                             ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                             ctypes.c_double, ctypes.c_void_p,
                                             ctypes.POINTER(ctypes.c_int)]
+        _LIB.orc_energy_magnitudes.argtypes = [ctypes.POINTER(_System)] + [ctypes.c_void_p] * 3
         _LIB.orc_float_to_int63.argtypes = [ctypes.c_float, ctypes.POINTER(ctypes.c_int32),
                                             ctypes.POINTER(ctypes.c_int32)]
         _LIB.orc_double_to_int95.argtypes = [ctypes.c_double, ctypes.POINTER(ctypes.c_int64),
@@ -119,6 +120,19 @@ class OracleSystem:
                                clash_distance, clash_ratio)
         return {"energies": e, "forces": None if f is None else f.reshape(-1, 3), "psi": psi,
                 "radii": rad, "sumdeijda": sde}
+
+    def magnitudes(self, coords, radii=None):
+        """Per-term sum of the absolute values of the contributions (orc_energy_magnitudes);
+        radii: the effective GB radii of these coordinates (evaluated here when omitted)."""
+        lib = _lib()
+        c = np.ascontiguousarray(np.asarray(coords, dtype=np.float64).reshape(-1))
+        if radii is None:
+            radii = self.evaluate(coords, forces=False)["radii"]
+        rad = np.ascontiguousarray(np.asarray(radii, dtype=np.float64))
+        m = np.zeros(NTERMS)
+        lib.orc_energy_magnitudes(ctypes.byref(self.struct), c.ctypes.data, rad.ctypes.data,
+                                  m.ctypes.data)
+        return m
 
     def minimize(self, coords, maxcyc, sd_cycles, dx0=0.01, drms=0.0, with_cycles=False,
                  clash_cycles=0, clash_distance=0.2, clash_ratio=0.5):

@@ -564,6 +564,80 @@ void orc_evaluate_clash(const orc_system* s, const double* coords, double* force
   }
 }
 
+static double sq(double x) { return x * x; }
+
+/* Root-sum-square of the contributions per term (test infrastructure: the scale of the rounding
+ * error of a sum of independently rounded FP32 contributions).  Same loops as the evaluators
+ * above; squares are summed here and square-rooted at the end. */
+void orc_energy_magnitudes(const orc_system* s, const double* c, const double* radii,
+                           double* mags) {
+  for (int t = 0; t < ORC_NTERMS; t++) mags[t] = 0.0;
+  const int n = s->natom;
+  for (int t = 0; t < s->nbond; t++) {
+    mags[ORC_BOND] += sq(bond_term(c, NULL, s->bond_i[t], s->bond_j[t], s->bond_k[t],
+                                   s->bond_r0[t]));
+  }
+  for (int t = 0; t < s->nangl; t++) {
+    mags[ORC_ANGLE] += sq(angle_term(c, NULL, s->angl_i[t], s->angl_j[t], s->angl_k[t],
+                                     s->angl_keq[t], s->angl_theta0[t]));
+  }
+  for (int t = 0; t < s->ndihe; t++) {
+    const double e = dihedral_term(c, NULL, s->dihe_i[t], s->dihe_j[t], s->dihe_k[t],
+                                   s->dihe_l[t], s->dihe_amp[t], s->dihe_phase[t],
+                                   s->dihe_freq[t]);
+    mags[(s->dihe_improper && s->dihe_improper[t]) ? ORC_IMPROPER_DIHEDRAL :
+                                                    ORC_PROPER_DIHEDRAL] += sq(e);
+    if (s->dihe_scee[t] > 0.0) {
+      const int i = s->dihe_i[t], l = s->dihe_l[t];
+      double d[3];
+      for (int a = 0; a < 3; a++) d[a] = c[3 * l + a] - c[3 * i + a];
+      const double invr2 = 1.0 / dot3(d, d);
+      const double invr6 = invr2 * invr2 * invr2;
+      const int ty = s->lj_idx[i] * s->n_lj_types + s->lj_idx[l];
+      mags[ORC_ELEC_ONE_FOUR] += sq(s->coulomb_constant * s->charge[i] * s->charge[l] /
+                                    s->dihe_scee[t] * sqrt(invr2));
+      mags[ORC_VDW_ONE_FOUR] += sq((fabs(s->lja14[ty]) * invr6 + fabs(s->ljb14[ty])) * invr6 /
+                                   s->dihe_scnb[t]);
+    }
+  }
+  char* excl = (char*)calloc((size_t)n, 1);
+  for (int i = 0; i < n; i++) {
+    for (int e = s->excl_bounds[i]; e < s->excl_bounds[i + 1]; e++) excl[s->excl_list[e]] = 1;
+    for (int j = i + 1; j < n; j++) {
+      if (excl[j]) continue;
+      double d[3];
+      for (int a = 0; a < 3; a++) d[a] = c[3 * j + a] - c[3 * i + a];
+      const double invr2 = 1.0 / dot3(d, d);
+      const double invr6 = invr2 * invr2 * invr2;
+      const int ty = s->lj_idx[j] * s->n_lj_types + s->lj_idx[i];
+      mags[ORC_ELECTROSTATIC] += sq(s->coulomb_constant * s->charge[i] * s->charge[j] *
+                                    sqrt(invr2));
+      mags[ORC_VDW] += sq((fabs(s->lja[ty]) * invr6 + fabs(s->ljb[ty])) * invr6);
+    }
+    for (int e = s->excl_bounds[i]; e < s->excl_bounds[i + 1]; e++) excl[s->excl_list[e]] = 0;
+  }
+  free(excl);
+  if (s->igb != ORC_GB_NONE && radii) {
+    const double kappa = (s->saltcon > 1.0e-8) ? sqrt(GB_SALT_KAPPA * s->saltcon) : 0.0;
+    for (int i = 0; i < n; i++) {
+      const double expmkf = exp(-GB_KSCALE * kappa * radii[i]) / s->dielectric;
+      mags[ORC_GENERALIZED_BORN] += sq(0.5 * s->charge[i] * s->charge[i] *
+                                       s->coulomb_constant * (1.0 - expmkf) / radii[i]);
+      for (int j = i + 1; j < n; j++) {
+        double d[3];
+        for (int a = 0; a < 3; a++) d[a] = c[3 * j + a] - c[3 * i + a];
+        const double r2 = dot3(d, d);
+        const double ijb = radii[i] * radii[j];
+        const double fgbi = 1.0 / sqrt(r2 + ijb * exp(-r2 / (4.0 * ijb)));
+        const double expm = exp(-kappa * GB_KSCALE / fgbi) / s->dielectric;
+        mags[ORC_GENERALIZED_BORN] += sq(s->coulomb_constant * s->charge[i] * s->charge[j] *
+                                         (1.0 - expm) * fgbi);
+      }
+    }
+  }
+  for (int t = 0; t < ORC_NTERMS; t++) mags[t] = sqrt(mags[t]);
+}
+
 /* ---------------------------------------------------------------------------------------------
  * Line minimization following the batched GPU driver
  * ------------------------------------------------------------------------------------------- */

@@ -43,6 +43,24 @@ __device__ __forceinline__ void atomicAddInt63(float v, int* primary, int* overf
   }
 }
 
+// A fixed-point coordinate (already scaled to Angstroms) as an FP32 pair hi + lo with hi on a
+// 2^-10 A grid.  For |x| < 8192 A and a coordinate grid of up to 2^-35 A, hi + lo == x exactly,
+// and for two atoms both hi_j - hi_i and lo_j - lo_i are exact in FP32 (hi differences are below
+// 2^24 units of 2^-10, lo differences below 2^22 units of 2^-32), so their sum rounds the exact
+// separation once and that rounding's error is lo_d - (d - hi_d), recoverable in two additions
+// (separationError).  An unconstrained hi = (float)x loses both properties.
+__device__ __forceinline__ void splitCoordinate(double x, float* hi, float* lo) {
+  const double h = rint(x * 1024.0) * 0.0009765625;
+  *hi = static_cast<float>(h);
+  *lo = static_cast<float>(x - h);
+}
+
+// Rounding error of d = hd + ld, where hd and ld are separations of hi and lo parts from
+// splitCoordinate: the exact separation is d + separationError(hd, ld, d)
+__device__ __forceinline__ float separationError(float hd, float ld, float d) {
+  return __fsub_rn(ld, __fsub_rn(d, hd));
+}
+
 // int63 pair -> int64
 __device__ __forceinline__ long long int63ToLong(int primary, int overflow) {
   return static_cast<long long>(overflow) * 2147483648LL + static_cast<long long>(primary);

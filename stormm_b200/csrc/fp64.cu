@@ -35,10 +35,7 @@ constexpr double kTaylorG64 = 24.0 / 7.0;
 constexpr double kTaylorH64 = 40.0 / 9.0;
 constexpr double kTaylorHH64 = 60.0 / 11.0;
 constexpr double kGbKscale64 = 0.73;
-// valence_potential.tpp (asymptotes of the dihedral force near collinear atoms) and
 // Math/rounding.tpp (the arcsine route of a dihedral near 0 or pi)
-constexpr double kAsymptoticToOne = 0.99999904632568359375;
-constexpr double kInvOneMinusAsymptote = 1048576.0;
 constexpr double kNearToOne = 0.999999992549419403076171875;
 constexpr double kPi64 = 3.14159265358979323846;
 
@@ -206,56 +203,6 @@ __device__ __forceinline__ double2 clashScaled64(const DevPrecise &p, int sysid)
   const double progress = static_cast<double>(p.clash_cycles - cycle) /
                           static_cast<double>(p.clash_cycles);
   return make_double2(p.clash_distance * progress, p.clash_ratio * progress);
-}
-
-// Quadratic Coulomb core below cd: qiqj (a (r + 1)^2 + b), continuous in value and slope
-__device__ __forceinline__ double2 quadraticCore64(double cd) {
-  if (cd <= 0.0) {
-    return make_double2(0.0, 0.0);
-  }
-  const double a = -0.5 / (cd * cd * (cd + 1.0));
-  return make_double2(a, 1.0 / cd - a * (cd + 1.0) * (cd + 1.0));
-}
-
-// Coulomb and Lennard-Jones energies of one pair with softened cores added to *e_elec, *e_vdw;
-// returns the force factor (force on j = factor x (r_j - r_i))
-__device__ __forceinline__ double softCorePair64(double r, double invr, double qiqj, double lja,
-                                                 double ljb, double cd, double2 qc, double ratio,
-                                                 double* e_elec, double* e_vdw) {
-  double fmag;
-  if (r < cd) {
-    const double rp = r + 1.0;
-    *e_elec += qiqj * (qc.x * rp * rp + qc.y);
-    fmag = (r > 1.0e-10) ? qiqj * (2.0 * qc.x + 2.0 * qc.x * invr) : 0.0;
-  }
-  else {
-    *e_elec += qiqj * invr;
-    fmag = -(qiqj * invr * invr * invr);
-  }
-  const double rl = (ljb > 1.0e-6) ? ratio * pow(lja / ljb, 1.0 / 6.0) : 0.0;
-  if (r < rl) {
-    const double il = 1.0 / rl;
-    const double il2 = il * il;
-    const double il6 = il2 * il2 * il2;
-    const double a = ((6.0 * ljb - 12.0 * lja * il6) * il * il6) /
-                     (((4.0 * rl + 12.0) * rl + 12.0) * rl + 4.0);
-    const double rlp = rl + 1.0;
-    const double rlp2 = rlp * rlp;
-    const double b = (lja * il6 - ljb) * il6 - a * rlp2 * rlp2;
-    const double rp = r + 1.0;
-    const double a3 = a * rp * rp * rp;
-    *e_vdw += a3 * rp + b;
-    if (r > 1.0e-10) {
-      fmag += 4.0 * a3 * invr;
-    }
-  }
-  else {
-    const double invr2 = invr * invr;
-    const double invr4 = invr2 * invr2;
-    *e_vdw += (lja * invr4 * invr4 - ljb * invr2) * invr4;
-    fmag += (6.0 * ljb - 12.0 * lja * invr4 * invr2) * invr4 * invr4;
-  }
-  return fmag;
 }
 
 template <bool FORCE, bool ENERGY, bool NB, bool GB, bool CLASH>

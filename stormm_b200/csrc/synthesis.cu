@@ -202,8 +202,8 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
     h_neck_sep.assign(h64_neck_sep.begin(), h64_neck_sep.end());
     h_neck_val.assign(h64_neck_val.begin(), h64_neck_val.end());
   }
+  h64_charge.assign(np, 0.0);
   if (fp64) {
-    h64_charge.assign(np, 0.0);
     h64_rho.assign(np, 1.0);
     h64_srho.assign(np, 0.0);
     h64_pb.assign(np, 1.09);
@@ -224,9 +224,9 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
       const double a14 = (tp.lja14 != nullptr) ? tp.lja14[e] : tp.lja[e];
       const double b14 = (tp.ljb14 != nullptr) ? tp.ljb14[e] : tp.ljb[e];
       h_ljab14.push_back(make_float2(static_cast<float>(a14), static_cast<float>(b14)));
+      h64_ljab14.push_back(make_double2(a14, b14));
       if (fp64) {
         h64_ljab.push_back(make_double2(tp.lja[e], tp.ljb[e]));
-        h64_ljab14.push_back(make_double2(a14, b14));
       }
     }
     // exclusions as a symmetric set of pairs
@@ -330,8 +330,8 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
         }
         h_neck_idx[base + i] = idx;
       }
+      h64_charge[base + i] = tp.charge[i] * sqrt_kc;
       if (fp64) {
-        h64_charge[base + i] = tp.charge[i] * sqrt_kc;
         if (opt.igb != SB_GB_NONE) {
           const double rho = tp.pb_radii[i] - gb_offset;
           h64_rho[base + i] = rho;
@@ -368,6 +368,8 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
       const uint32_t k = check_atom(tp.angl_atoms[3 * a + 2]);
       h_angles.push_back(make_uint4(i | (j << 16), k, fbits(tp.angl_keq[a]),
                                     fbits(std::cos(tp.angl_theta0[a]))));
+      h_angl64.push_back(make_double4(tp.angl_keq[a], std::cos(tp.angl_theta0[a]),
+                                      std::sin(tp.angl_theta0[a]), tp.angl_theta0[a]));
       if (fp64) {
         h64_angl_atoms.push_back(make_int4(i, j, k, 0));
         h64_angl_prm.push_back(make_double2(tp.angl_keq[a], tp.angl_theta0[a]));
@@ -392,6 +394,10 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
                                     fbits(std::sin(tp.dihe_phase[d])),
                                     fbits(scee > 0.0 ? 1.0 / scee : 0.0),
                                     fbits((scee > 0.0 && scnb > 0.0) ? 1.0 / scnb : 0.0)));
+      h_dihe64.push_back(make_double4(tp.dihe_amp[d], std::cos(tp.dihe_phase[d]),
+                                      std::sin(tp.dihe_phase[d]), tp.dihe_freq[d]));
+      h_dihe14_64.push_back(make_double2(scee > 0.0 ? 1.0 / scee : 0.0,
+                                         (scee > 0.0 && scnb > 0.0) ? 1.0 / scnb : 0.0));
       if (fp64) {
         h64_dihe_atoms.push_back(make_int4(i, j, k, l));
         h64_dihe_prm.push_back(make_double4(tp.dihe_amp[d], tp.dihe_freq[d], tp.dihe_phase[d],
@@ -623,6 +629,11 @@ void Synthesis::upload() {
   d_angles.upload(h_angles);
   d_dihe_a.upload(h_dihe_a);
   d_dihe_b.upload(h_dihe_b);
+  d_angl64.upload(h_angl64);
+  d_dihe64.upload(h_dihe64);
+  d_dihe14_64.upload(h_dihe14_64);
+  d64_charge.upload(h64_charge);
+  d64_ljab14.upload(h64_ljab14);
   d_tile_mask_idx.upload(h_tile_mask_idx);
   d_mask_pool.upload(h_mask_pool);
   finalizePlan(single_plan.get());
@@ -636,7 +647,6 @@ void Synthesis::upload() {
     d_tiled_sde.zeros(natom_padded);
   }
   if (fp64) {
-    d64_charge.upload(h64_charge);
     d64_rho.upload(h64_rho);
     d64_srho.upload(h64_srho);
     d64_pb.upload(h64_pb);
@@ -644,7 +654,6 @@ void Synthesis::upload() {
     d64_beta.upload(h64_beta);
     d64_gamma.upload(h64_gamma);
     d64_ljab.upload(h64_ljab);
-    d64_ljab14.upload(h64_ljab14);
     d64_bond_atoms.upload(h64_bond_atoms);
     d64_bond_prm.upload(h64_bond_prm);
     d64_angl_atoms.upload(h64_angl_atoms);
@@ -766,6 +775,11 @@ void Synthesis::upload() {
   d.angles = d_angles.p;
   d.dihe_a = d_dihe_a.p;
   d.dihe_b = d_dihe_b.p;
+  d.angl64 = d_angl64.p;
+  d.dihe64 = d_dihe64.p;
+  d.dihe14_64 = d_dihe14_64.p;
+  d.charge64 = d64_charge.p;
+  d.ljab14_64 = d64_ljab14.p;
   d.tile_mask_idx = d_tile_mask_idx.p;
   d.mask_pool = d_mask_pool.p;
   d.energies = d_energies.p;

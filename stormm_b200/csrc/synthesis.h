@@ -178,6 +178,8 @@ public:
   std::vector<int> h_bond_start, h_angl_start, h_dihe_start;
   std::vector<float2> h_ljab, h_ljab14;
   std::vector<uint4> h_bonds, h_angles, h_dihe_a, h_dihe_b;
+  std::vector<double4> h_angl64, h_dihe64;
+  std::vector<double2> h_dihe14_64;
   std::vector<unsigned int> h_mask_pool;
   std::vector<long long> h_stage_ll;
   std::vector<int> h_unpadded_map;   // padded index of each unpadded atom
@@ -188,6 +190,8 @@ public:
   DeviceArray<float> d_charge, d_rho, d_srho, d_pb, d_alpha, d_beta, d_gamma;
   DeviceArray<float2> d_ljab, d_ljab14;
   DeviceArray<uint4> d_bonds, d_angles, d_dihe_a, d_dihe_b;
+  DeviceArray<double4> d_angl64, d_dihe64;
+  DeviceArray<double2> d_dihe14_64;
   DeviceArray<unsigned int> d_mask_pool;
   DeviceArray<long long> d_xcrd, d_ycrd, d_zcrd, d_xfrc, d_yfrc, d_zfrc;
   DeviceArray<int> d_xcrd_ovrf, d_ycrd_ovrf, d_zcrd_ovrf, d_xfrc_ovrf, d_yfrc_ovrf, d_zfrc_ovrf;
@@ -212,6 +216,7 @@ public:
   DeviceArray<float> d_tiled_radius, d_tiled_sde;
   DevTiled dev_tiled{};
   // FP64 mode (opt.precision == SB_PRECISION_DOUBLE): double parameters and per-atom GB state
+  // (charges and 1-4 tables in double are built in both modes: FP32 valence uses them too)
   bool fp64 = false;
   std::vector<double> h64_charge, h64_rho, h64_srho, h64_pb, h64_alpha, h64_beta, h64_gamma;
   std::vector<double2> h64_ljab, h64_ljab14, h64_bond_prm, h64_angl_prm, h64_dihe_attn;

@@ -42,16 +42,10 @@ struct GlobalValence {
   }
   __device__ __forceinline__ int chunkStride() const { return (blockDim.x >> 5) * gridDim.y; }
   __device__ __forceinline__ void hilo(int i, float4* a, float4* b) const {
-    const double x = static_cast<double>(d.xcrd[i]) * d.inv_gpos_scale;
-    const double y = static_cast<double>(d.ycrd[i]) * d.inv_gpos_scale;
-    const double z = static_cast<double>(d.zcrd[i]) * d.inv_gpos_scale;
-    a->x = static_cast<float>(x);
-    a->y = static_cast<float>(y);
-    a->z = static_cast<float>(z);
+    splitCoordinate(static_cast<double>(d.xcrd[i]) * d.inv_gpos_scale, &a->x, &b->x);
+    splitCoordinate(static_cast<double>(d.ycrd[i]) * d.inv_gpos_scale, &a->y, &b->y);
+    splitCoordinate(static_cast<double>(d.zcrd[i]) * d.inv_gpos_scale, &a->z, &b->z);
     a->w = 0.0f;
-    b->x = static_cast<float>(x - static_cast<double>(a->x));
-    b->y = static_cast<float>(y - static_cast<double>(a->y));
-    b->z = static_cast<float>(z - static_cast<double>(a->z));
     b->w = 0.0f;
   }
   __device__ __forceinline__ float4 pa(int i) const {
@@ -90,6 +84,27 @@ struct GlobalValence {
   }
   __device__ __forceinline__ float2 lj14(int code_i, int code_l, int) const {
     return lj14tab[(code_i & 0xffff) + (code_l >> 16)];
+  }
+  __device__ __forceinline__ double3 pos64(int i) const {
+    return make_double3(static_cast<double>(d.xcrd[i]) * d.inv_gpos_scale,
+                        static_cast<double>(d.ycrd[i]) * d.inv_gpos_scale,
+                        static_cast<double>(d.zcrd[i]) * d.inv_gpos_scale);
+  }
+  __device__ __forceinline__ void force64(int i, double fx, double fy, double fz,
+                                          float scale) const {
+    const double s = static_cast<double>(scale);
+    atomicAdd(reinterpret_cast<unsigned long long*>(&d.xfrc[i]),
+              static_cast<unsigned long long>(__double2ll_rn(fx * s)));
+    atomicAdd(reinterpret_cast<unsigned long long*>(&d.yfrc[i]),
+              static_cast<unsigned long long>(__double2ll_rn(fy * s)));
+    atomicAdd(reinterpret_cast<unsigned long long*>(&d.zfrc[i]),
+              static_cast<unsigned long long>(__double2ll_rn(fz * s)));
+  }
+  __device__ __forceinline__ void energy64(int k, int slot, double e, float scale) const {
+    const long long v = warpSum(__double2ll_rn(e * static_cast<double>(scale)));
+    if ((threadIdx.x & 31) == 0 && v != 0) {
+      atomicAdd(&d.energies[sys[k] * kNrgStride + slot], static_cast<unsigned long long>(v));
+    }
   }
   __device__ __forceinline__ float2 clash(int k) const {
     const int cycle = (d.clash_cycle != nullptr) ? d.clash_cycle[sys[k]] : -1;
@@ -139,13 +154,11 @@ __device__ __forceinline__ void stageTile(const DevSynthesis &d, const DevTiled 
     float2 gbv = make_float2(1.0f, 0.0f);
     if (a < natom) {
       const int gi = base + a;
-      const double x = static_cast<double>(d.xcrd[gi]) * d.inv_gpos_scale;
-      const double y = static_cast<double>(d.ycrd[gi]) * d.inv_gpos_scale;
-      const double z = static_cast<double>(d.zcrd[gi]) * d.inv_gpos_scale;
-      pa = make_float4(static_cast<float>(x), static_cast<float>(y), static_cast<float>(z), 0.0f);
-      pb = make_float4(static_cast<float>(x - static_cast<double>(pa.x)),
-                       static_cast<float>(y - static_cast<double>(pa.y)),
-                       static_cast<float>(z - static_cast<double>(pa.z)), 0.0f);
+      pa.w = 0.0f;
+      pb.w = 0.0f;
+      splitCoordinate(static_cast<double>(d.xcrd[gi]) * d.inv_gpos_scale, &pa.x, &pb.x);
+      splitCoordinate(static_cast<double>(d.ycrd[gi]) * d.inv_gpos_scale, &pa.y, &pb.y);
+      splitCoordinate(static_cast<double>(d.zcrd[gi]) * d.inv_gpos_scale, &pa.z, &pb.z);
       const int ty = d.lj_idx[gi];
       prm = make_float4(d.charge[gi], __int_as_float((ty * nt) | (ty << 16)), d.rho[gi],
                         d.srho[gi]);
@@ -251,14 +264,16 @@ kTiledPair(const DevSynthesis d, const DevTiled t, int tile_begin, int tile_end)
   long long acc_elec = 0, acc_vdw = 0, acc_gb = 0;
   int acc_sys = -1;
   auto flush = [&]() {
-    const long long se = warpSum(acc_elec), sv = warpSum(acc_vdw), sg = warpSum(acc_gb);
+    // per-tile energies rounded to the output grid (tileEnergy), the same value in every lane
     if (lane == 0 && acc_sys >= 0) {
       if (NB) {
-        atomicAdd(&d.energies[acc_sys * kNrgStride + kElec], static_cast<unsigned long long>(se));
-        atomicAdd(&d.energies[acc_sys * kNrgStride + kVdw], static_cast<unsigned long long>(sv));
+        atomicAdd(&d.energies[acc_sys * kNrgStride + kElec],
+                  static_cast<unsigned long long>(acc_elec));
+        atomicAdd(&d.energies[acc_sys * kNrgStride + kVdw],
+                  static_cast<unsigned long long>(acc_vdw));
       }
       if (GB) {
-        atomicAdd(&d.energies[acc_sys * kNrgStride + kGb], static_cast<unsigned long long>(sg));
+        atomicAdd(&d.energies[acc_sys * kNrgStride + kGb], static_cast<unsigned long long>(acc_gb));
       }
     }
     acc_elec = acc_vdw = acc_gb = 0;
@@ -312,9 +327,13 @@ kTiledPair(const DevSynthesis d, const DevTiled t, int tile_begin, int tile_end)
       }
     }
     if (ENERGY) {
-      acc_elec += __float2ll_rn(p.e_elec * es);
-      acc_vdw += __float2ll_rn(p.e_vdw * es);
-      acc_gb += __float2ll_rn(p.e_gb * es);
+      if (NB) {
+        acc_elec += tileEnergy(p.t_elec, es);
+        acc_vdw += tileEnergy(p.t_vdw, es);
+      }
+      if (GB) {
+        acc_gb += tileEnergy(p.t_gb, es);
+      }
     }
     __syncwarp();
   }

@@ -128,6 +128,75 @@ __device__ __forceinline__ float softCorePair(float r, float invr, float qiqj, f
   return fmag;
 }
 
+// Valence geometry in FP64 (the angle, dihedral and 1-4 terms of both precision modes)
+__device__ __forceinline__ double3 sub3d(double3 a, double3 b) {
+  return make_double3(a.x - b.x, a.y - b.y, a.z - b.z);
+}
+__device__ __forceinline__ double dot3d(double3 a, double3 b) {
+  return fma(a.x, b.x, fma(a.y, b.y, a.z * b.z));
+}
+__device__ __forceinline__ double3 cross3d(double3 a, double3 b) {
+  return make_double3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+
+// valence_potential.tpp: below this squared cosine between consecutive dihedral bonds the force
+// divides by the sine squared; above it (near-collinear atoms) it takes the fixed reciprocal
+constexpr double kAsymptoticToOne = 0.99999904632568359375;
+constexpr double kInvOneMinusAsymptote = 1048576.0;
+
+// Softened cores in FP64 (Potential/soft_core_potentials.tpp:30-52, 140-180; softCorePair in
+// double)
+// Quadratic Coulomb core below cd: qiqj (a (r + 1)^2 + b), continuous in value and slope
+__device__ __forceinline__ double2 quadraticCore64(double cd) {
+  if (cd <= 0.0) {
+    return make_double2(0.0, 0.0);
+  }
+  const double a = -0.5 / (cd * cd * (cd + 1.0));
+  return make_double2(a, 1.0 / cd - a * (cd + 1.0) * (cd + 1.0));
+}
+
+// Coulomb and Lennard-Jones energies of one pair with softened cores added to *e_elec, *e_vdw;
+// returns the force factor (force on j = factor x (r_j - r_i))
+__device__ __forceinline__ double softCorePair64(double r, double invr, double qiqj, double lja,
+                                                 double ljb, double cd, double2 qc, double ratio,
+                                                 double* e_elec, double* e_vdw) {
+  double fmag;
+  if (r < cd) {
+    const double rp = r + 1.0;
+    *e_elec += qiqj * (qc.x * rp * rp + qc.y);
+    fmag = (r > 1.0e-10) ? qiqj * (2.0 * qc.x + 2.0 * qc.x * invr) : 0.0;
+  }
+  else {
+    *e_elec += qiqj * invr;
+    fmag = -(qiqj * invr * invr * invr);
+  }
+  const double rl = (ljb > 1.0e-6) ? ratio * pow(lja / ljb, 1.0 / 6.0) : 0.0;
+  if (r < rl) {
+    const double il = 1.0 / rl;
+    const double il2 = il * il;
+    const double il6 = il2 * il2 * il2;
+    const double a = ((6.0 * ljb - 12.0 * lja * il6) * il * il6) /
+                     (((4.0 * rl + 12.0) * rl + 12.0) * rl + 4.0);
+    const double rlp = rl + 1.0;
+    const double rlp2 = rlp * rlp;
+    const double b = (lja * il6 - ljb) * il6 - a * rlp2 * rlp2;
+    const double rp = r + 1.0;
+    const double a3 = a * rp * rp * rp;
+    *e_vdw += a3 * rp + b;
+    if (r > 1.0e-10) {
+      fmag += 4.0 * a3 * invr;
+    }
+  }
+  else {
+    const double invr2 = invr * invr;
+    const double invr4 = invr2 * invr2;
+    *e_vdw += (lja * invr4 * invr4 - ljb * invr2) * invr4;
+    fmag += (6.0 * ljb - 12.0 * lja * invr4 * invr2) * invr4 * invr4;
+  }
+  return fmag;
+}
+
+
 // Packed FP32 pairs (Blackwell FFMA2 / FADD2 / FMUL2): two pairs of one lane in one instruction
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
@@ -148,7 +217,11 @@ __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __
 //   I = 1/2 [1/L - 1/U + (sj^2 - r^2)/(4r) (1/L^2 - 1/U^2) + ln(L/U) / (2r)]
 //       + (1/rho - 1/L) when rho < sj - r,
 // and I = 0 when rho >= U.  One formula instead of four keeps a warp on at most two paths; the
-// inside case is rare, so a branch there beats a reciprocal per pair.
+// inside case is rare, so a branch there beats a reciprocal per pair.  The closed form cancels
+// to a small remainder near r = 4 sj, so ln(L / U) needs an accurate absolute value: the fast
+// hardware logarithm (__logf) errs by about 1e-7 absolute with a consistent sign, which biased
+// every atom's psi by -6.5e-7 relative and the GB energy by +1.1e-6 relative (1,024 molecules
+// of 16-256 atoms); logf removes the bias (psi -7.6e-8, GB energy 1.0e-7).
 __device__ __forceinline__ float2 hctIntegral2(float2 r, float2 r2, float2 invr, float2 rho,
                                                float2 sj) {
   const bool far_x = r.x > 4.0f * sj.x;
@@ -174,7 +247,7 @@ __device__ __forceinline__ float2 hctIntegral2(float2 r, float2 r2, float2 invr,
     const float2 iu = mul2(l, inv_lu);
     const float2 dlu = sub2(il, iu);
     const float2 liu = mul2(l, iu);
-    const float2 lg = f2(__logf(liu.x), __logf(liu.y));
+    const float2 lg = f2(logf(liu.x), logf(liu.y));
     const float2 q = mul2(mul2(mul2(f2(0.25f), sub2(mul2(sj, sj), r2)), invr), dlu);
     float2 v = add2(fma2(q, add2(il, iu), dlu), mul2(mul2(f2(0.5f), invr), lg));
     if (rho.x < -rms.x) {
@@ -214,7 +287,7 @@ __device__ __forceinline__ float hctDerivative(float r, float r2, float invr, fl
   const float q = 0.25f * (sj * sj - r2) * invr;
   const float dq = -0.25f * fmaf(sj * sj, invr2, 1.0f);
   float di = -lam * il2 + iu2 + dq * (il2 - iu2) + 2.0f * q * (iu2 * iu - lam * il2 * il) +
-             0.5f * invr * (lam * il - iu - invr * __logf(l * iu));
+             0.5f * invr * (lam * il - iu - invr * logf(l * iu));
   di = 0.5f * di - ((-rms > rho) ? il2 : 0.0f);
   return (rho < u) ? -di * invr : 0.0f;
 }
@@ -254,7 +327,7 @@ __device__ __forceinline__ void hctBoth2(float r, float r2, float invr, float2 r
     const float2 il = mul2(u, inv_lu);
     const float2 iu = mul2(l, inv_lu);
     const float2 liu = mul2(l, iu);
-    const float2 lg = f2(__logf(liu.x), __logf(liu.y));
+    const float2 lg = f2(logf(liu.x), logf(liu.y));
     const float2 s2mr2 = sub2(sj2, f2(r2));
     // the integral
     const float2 dlu = sub2(il, iu);
@@ -463,6 +536,19 @@ __device__ __forceinline__ long long warpSum(long long v) {
   return v;
 }
 
+// A tile's energy in the output fixed-point format: the lanes' FP64 sums added by an xor
+// butterfly (every lane adds the same two values at every level, so all lanes hold the same bits
+// and the total does not depend on which warp ran the tile), then rounded once.  Rounding each
+// lane's share instead loses the pairs of distant tiles, whose per-lane sums fall below one unit
+// of 2^-26 kcal/mol (1.6e-6 of the Lennard-Jones energy of a 2,100-atom chain), and an integer
+// accumulator finer than the output overflows on clashing starting structures (1.6e7 kcal/mol).
+__device__ __forceinline__ long long tileEnergy(double v, float nrg_scale) {
+  for (int o = 16; o > 0; o >>= 1) {
+    v += __shfl_xor_sync(kFullMask, v, o);
+  }
+  return __double2ll_rn(v * static_cast<double>(nrg_scale));
+}
+
 // Warp-reduce one scaled energy per lane (all lanes in one molecule) into its slot
 __device__ __forceinline__ void warpEnergy(const UnitSmem &s, int k, int slot, float e,
                                            float scale) {
@@ -505,6 +591,25 @@ struct SmemValence {
   }
   __device__ __forceinline__ void energy(int k, int slot, float e, float scale) const {
     warpEnergy(s, k, slot, e, scale);
+  }
+  // exact coordinates of a slot: the hi + lo float pair summed in double
+  __device__ __forceinline__ double3 pos64(int i) const {
+    const float4 a = s.pa[i];
+    const float4 b = s.pb[i];
+    return make_double3(static_cast<double>(a.x) + static_cast<double>(b.x),
+                        static_cast<double>(a.y) + static_cast<double>(b.y),
+                        static_cast<double>(a.z) + static_cast<double>(b.z));
+  }
+  __device__ __forceinline__ void force64(int i, double fx, double fy, double fz,
+                                          float scale) const {
+    addForce(s, i, static_cast<float>(fx), static_cast<float>(fy), static_cast<float>(fz),
+             scale);
+  }
+  __device__ __forceinline__ void energy64(int k, int slot, double e, float scale) const {
+    const long long v = warpSum(__double2ll_rn(e * static_cast<double>(scale)));
+    if ((threadIdx.x & 31) == 0 && v != 0) {
+      atomicAdd(&s.nrg[k * kNrgStride + slot], static_cast<unsigned long long>(v));
+    }
   }
   __device__ __forceinline__ float2 clash(int k) const { return s.clash[k]; }
   // the molecule's 1-4 table follows its standard table in shared memory
@@ -575,197 +680,190 @@ __device__ void valenceTerms(const DevSynthesis &d, const V &v, int nsys_u) {
     }
   }
 
-  // angles, valence_potential.tpp:170-288.  theta - theta0 comes from rotating (cos, sin) of
-  // theta, taken from the dot and cross products, by theta0: well conditioned everywhere.
+  // angles, valence_potential.tpp:170-288, in FP64 from the exact coordinates: a near-linear
+  // angle's force divides by sin(theta), which FP32 deltas and cross products only give to
+  // about 1e-7 absolute.  theta - theta0 comes from rotating (cos, sin) of theta, taken from the
+  // dot and cross products, by theta0: well conditioned everywhere.
   for (int c = v.chunkBegin(); c < v.achunk0[nsys_u]; c += v.chunkStride()) {
     const int k = findOwner(v.achunk0, nsys_u, c);
     const int sysid = v.sys[k];
     const int t = (c - v.achunk0[k]) * 32 + lane;
     const int nterm = d.angl_start[sysid + 1] - d.angl_start[sysid];
-    float e = 0.0f;
+    double e = 0.0;
     if (t < nterm) {
       const uint4 rec = d.angles[d.angl_start[sysid] + t];
+      const double4 prm = d.angl64[d.angl_start[sysid] + t];   // k, cos, sin, theta0
       const int ia = v.slot0[k] + static_cast<int>(rec.x & 0xffffu);
       const int ja = v.slot0[k] + static_cast<int>(rec.x >> 16);
       const int ka = v.slot0[k] + static_cast<int>(rec.y);
-      const float keq = __uint_as_float(rec.z);
-      const float cth0 = __uint_as_float(rec.w);
-      const float sth0 = sqrtf(fmaxf(0.0f, fmaf(-cth0, cth0, 1.0f)));
-      const float3 ba = v.delta(ja, ia);
-      const float3 bc = v.delta(ja, ka);
-      const float mgba = ba.x * ba.x + ba.y * ba.y + ba.z * ba.z;
-      const float mgbc = bc.x * bc.x + bc.y * bc.y + bc.z * bc.z;
-      const float invbabc = rsqrtf(mgba * mgbc);
-      const float dotp = ba.x * bc.x + ba.y * bc.y + ba.z * bc.z;
-      const float cx = ba.y * bc.z - ba.z * bc.y;
-      const float cy = ba.z * bc.x - ba.x * bc.z;
-      const float cz = ba.x * bc.y - ba.y * bc.x;
-      const float crs = sqrtf(cx * cx + cy * cy + cz * cz);
-      const float sth = crs * invbabc;
-      const float cth = dotp * invbabc;
-      const float dtheta = atan2f(fmaf(sth, cth0, -cth * sth0), fmaf(cth, cth0, sth * sth0));
+      const double3 pj = v.pos64(ja);
+      const double3 ba = sub3d(v.pos64(ia), pj);
+      const double3 bc = sub3d(v.pos64(ka), pj);
+      const double mgba = dot3d(ba, ba);
+      const double mgbc = dot3d(bc, bc);
+      const double invbabc = rsqrt(mgba * mgbc);
+      const double3 cr = cross3d(ba, bc);
+      const double sth = sqrt(dot3d(cr, cr)) * invbabc;
+      const double cth = dot3d(ba, bc) * invbabc;
+      const double dtheta = atan2(fma(sth, prm.y, -cth * prm.z), fma(cth, prm.y, sth * prm.z));
       if (FORCE) {
-        const float dA = -2.0f * keq * dtheta / sth;
-        const float sqba = dA / mgba;
-        const float sqbc = dA / mgbc;
-        const float mbabc = dA * invbabc;
-        const float adx = bc.x * mbabc - cth * ba.x * sqba;
-        const float ady = bc.y * mbabc - cth * ba.y * sqba;
-        const float adz = bc.z * mbabc - cth * ba.z * sqba;
-        const float cdx = ba.x * mbabc - cth * bc.x * sqbc;
-        const float cdy = ba.y * mbabc - cth * bc.y * sqbc;
-        const float cdz = ba.z * mbabc - cth * bc.z * sqbc;
-        v.force(ia, -adx, -ady, -adz, fs);
-        v.force(ja, adx + cdx, ady + cdy, adz + cdz, fs);
-        v.force(ka, -cdx, -cdy, -cdz, fs);
+        const double dA = -2.0 * prm.x * dtheta / sth;
+        const double sqba = dA / mgba;
+        const double sqbc = dA / mgbc;
+        const double mbabc = dA * invbabc;
+        const double adx = bc.x * mbabc - cth * ba.x * sqba;
+        const double ady = bc.y * mbabc - cth * ba.y * sqba;
+        const double adz = bc.z * mbabc - cth * ba.z * sqba;
+        const double cdx = ba.x * mbabc - cth * bc.x * sqbc;
+        const double cdy = ba.y * mbabc - cth * bc.y * sqbc;
+        const double cdz = ba.z * mbabc - cth * bc.z * sqbc;
+        v.force64(ia, -adx, -ady, -adz, fs);
+        v.force64(ja, adx + cdx, ady + cdy, adz + cdz, fs);
+        v.force64(ka, -cdx, -cdy, -cdz, fs);
       }
-      e = __fmul_rn(__fmul_rn(keq, dtheta), dtheta);
+      e = prm.x * dtheta * dtheta;
     }
     if (ENERGY) {
-      v.energy(k, kAngle, e, es);
+      v.energy64(k, kAngle, e, es);
     }
   }
 
-  // dihedrals with attached 1-4 pairs, valence_potential.tpp:359-578, 1288-1420.  The signed
-  // angle is carried as (cos, sin) from x = (ab x bc) . (bc x cd) and y = |bc| ab . (bc x cd),
-  // the angle STORMM's acos / arcsine route gives (Math/rounding.tpp:25-80) without its ill
-  // conditioning near 0 and pi; cos(n theta - phase) and sin(n theta - phase) follow from the
-  // multiple-angle recurrence for integer periodicities.
+  // dihedrals with attached 1-4 pairs, valence_potential.tpp:359-578, 1288-1420, in FP64 from
+  // the exact coordinates.  The signed angle is carried as (cos, sin) from x = (ab x bc) .
+  // (bc x cd) and y = |bc| ab . (bc x cd), the angle STORMM's acos / arcsine route gives
+  // (Math/rounding.tpp:25-80) without its ill conditioning near 0 and pi; cos(n theta - phase)
+  // and sin(n theta - phase) follow from the multiple-angle recurrence for integer
+  // periodicities.  1 + cos(psi) cancels near psi = pi (impropers, and propers near their
+  // minimum); there sin^2(psi) / (1 - cos(psi)) gives the same value without the cancellation.
   for (int c = v.chunkBegin(); c < v.dchunk0[nsys_u]; c += v.chunkStride()) {
     const int k = findOwner(v.dchunk0, nsys_u, c);
     const int sysid = v.sys[k];
     const int t = (c - v.dchunk0[k]) * 32 + lane;
     const int nterm = d.dihe_start[sysid + 1] - d.dihe_start[sysid];
-    float e_prop = 0.0f, e_impr = 0.0f, e_el14 = 0.0f, e_lj14 = 0.0f;
+    double e_prop = 0.0, e_impr = 0.0, e_el14 = 0.0, e_lj14 = 0.0;
     if (t < nterm) {
       const int pos = d.dihe_start[sysid] + t;
       const uint4 ra = d.dihe_a[pos];
-      const uint4 rb = d.dihe_b[pos];
-      const int ia = v.slot0[k] + static_cast<int>(ra.x & 0xffffu);
+      const double4 prm = d.dihe64[pos];     // amplitude, cos(phase), sin(phase), periodicity
+      const int li = static_cast<int>(ra.x & 0xffffu);
+      const int ll = static_cast<int>((ra.y >> 16) & 0x7fffu);
+      const int ia = v.slot0[k] + li;
       const int ja = v.slot0[k] + static_cast<int>(ra.x >> 16);
       const int ka = v.slot0[k] + static_cast<int>(ra.y & 0xffffu);
-      const int la = v.slot0[k] + static_cast<int>((ra.y >> 16) & 0x7fffu);
+      const int la = v.slot0[k] + ll;
       const bool improper = (ra.y & 0x80000000u) != 0u;
-      const float amp = __uint_as_float(ra.z);
-      const float freq = __uint_as_float(ra.w);
-      const float cphase = __uint_as_float(rb.x);
-      const float sphase = __uint_as_float(rb.y);
-      const float3 ab = v.delta(ia, ja);
-      const float3 bc = v.delta(ja, ka);
-      const float3 cd = v.delta(ka, la);
-      float3 crabbc = make_float3(ab.y * bc.z - ab.z * bc.y, ab.z * bc.x - ab.x * bc.z,
-                                  ab.x * bc.y - ab.y * bc.x);
-      float3 crbccd = make_float3(bc.y * cd.z - bc.z * cd.y, bc.z * cd.x - bc.x * cd.z,
-                                  bc.x * cd.y - bc.y * cd.x);
-      const float mgbc = sqrtf(bc.x * bc.x + bc.y * bc.y + bc.z * bc.z);
-      const float xx = crabbc.x * crbccd.x + crabbc.y * crbccd.y + crabbc.z * crbccd.z;
-      const float yy = mgbc * (ab.x * crbccd.x + ab.y * crbccd.y + ab.z * crbccd.z);
-      const float inv_rr = rsqrtf(fmaf(xx, xx, yy * yy));
-      const float c1 = xx * inv_rr;
-      const float s1 = yy * inv_rr;
-      float cn, sn;
+      const double3 pi = v.pos64(ia);
+      const double3 pj = v.pos64(ja);
+      const double3 pk = v.pos64(ka);
+      const double3 pl = v.pos64(la);
+      const double3 ab = sub3d(pj, pi);
+      const double3 bc = sub3d(pk, pj);
+      const double3 cd = sub3d(pl, pk);
+      double3 crabbc = cross3d(ab, bc);
+      double3 crbccd = cross3d(bc, cd);
+      const double mgbc = sqrt(dot3d(bc, bc));
+      const double xx = dot3d(crabbc, crbccd);
+      const double yy = mgbc * dot3d(ab, crbccd);
+      const double inv_rr = rsqrt(fma(xx, xx, yy * yy));
+      const double c1 = xx * inv_rr;
+      const double s1 = yy * inv_rr;
+      double cn, sn;
+      const double freq = prm.w;
       const int nint = static_cast<int>(freq);
-      if (static_cast<float>(nint) == freq && nint >= 1 && nint <= 6) {
+      if (static_cast<double>(nint) == freq && nint >= 1 && nint <= 6) {
         cn = c1;
         sn = s1;
         for (int m = 1; m < nint; m++) {
-          const float cnew = cn * c1 - sn * s1;
+          const double cnew = cn * c1 - sn * s1;
           sn = sn * c1 + cn * s1;
           cn = cnew;
         }
       }
       else {
-        sincosf(freq * atan2f(yy, xx), &sn, &cn);
+        sincos(freq * atan2(yy, xx), &sn, &cn);
       }
-      const float cos_sangle = cn * cphase + sn * sphase;
-      const float sin_sangle = sn * cphase - cn * sphase;
+      const double cos_sangle = cn * prm.y + sn * prm.z;
+      const double sin_sangle = sn * prm.y - cn * prm.z;
       if (FORCE) {
-        const float fr = amp * freq * sin_sangle;
-        const float mgab = sqrtf(ab.x * ab.x + ab.y * ab.y + ab.z * ab.z);
-        const float mgcd = sqrtf(cd.x * cd.x + cd.y * cd.y + cd.z * cd.z);
-        const float invab = 1.0f / mgab;
-        const float invbc = 1.0f / mgbc;
-        const float invcd = 1.0f / mgcd;
-        const float cosb = -(ab.x * bc.x + ab.y * bc.y + ab.z * bc.z) * invab * invbc;
-        const float cosc = -(bc.x * cd.x + bc.y * cd.y + bc.z * cd.z) * invbc * invcd;
-        const float isinb2 = (cosb * cosb < 0.99999904632568359375f) ? fr / (1.0f - cosb * cosb) :
-                                                                        fr * 1048576.0f;
-        const float isinc2 = (cosc * cosc < 0.99999904632568359375f) ? fr / (1.0f - cosc * cosc) :
-                                                                        fr * 1048576.0f;
-        const float invabc = invab * invbc;
-        const float invbcd = invbc * invcd;
-        crabbc.x *= invabc;
-        crabbc.y *= invabc;
-        crabbc.z *= invabc;
-        crbccd.x *= invbcd;
-        crbccd.y *= invbcd;
-        crbccd.z *= invbcd;
-        const float fa = -invab * isinb2;
-        const float fb1 = (mgbc - mgab * cosb) * invabc * isinb2;
-        const float fb2 = cosc * invbc * isinc2;
-        const float fd = -invcd * isinc2;
-        const float fix = crabbc.x * fa, fiy = crabbc.y * fa, fiz = crabbc.z * fa;
-        const float fjx = fb1 * crabbc.x - fb2 * crbccd.x;
-        const float fjy = fb1 * crabbc.y - fb2 * crbccd.y;
-        const float fjz = fb1 * crabbc.z - fb2 * crbccd.z;
-        const float flx = -fd * crbccd.x, fly = -fd * crbccd.y, flz = -fd * crbccd.z;
-        v.force(ia, fix, fiy, fiz, fs);
-        v.force(ja, fjx, fjy, fjz, fs);
-        v.force(ka, -(fix + fjx + flx), -(fiy + fjy + fly), -(fiz + fjz + flz), fs);
-        v.force(la, flx, fly, flz, fs);
+        const double fr = prm.x * freq * sin_sangle;
+        const double mgab = sqrt(dot3d(ab, ab));
+        const double mgcd = sqrt(dot3d(cd, cd));
+        const double invab = 1.0 / mgab;
+        const double invbc = 1.0 / mgbc;
+        const double invcd = 1.0 / mgcd;
+        const double cosb = -dot3d(ab, bc) * invab * invbc;
+        const double cosc = -dot3d(bc, cd) * invbc * invcd;
+        const double isinb2 = (cosb * cosb < kAsymptoticToOne) ? fr / (1.0 - cosb * cosb) :
+                                                                  fr * kInvOneMinusAsymptote;
+        const double isinc2 = (cosc * cosc < kAsymptoticToOne) ? fr / (1.0 - cosc * cosc) :
+                                                                  fr * kInvOneMinusAsymptote;
+        const double invabc = invab * invbc;
+        const double invbcd = invbc * invcd;
+        crabbc = make_double3(crabbc.x * invabc, crabbc.y * invabc, crabbc.z * invabc);
+        crbccd = make_double3(crbccd.x * invbcd, crbccd.y * invbcd, crbccd.z * invbcd);
+        const double fa = -invab * isinb2;
+        const double fb1 = (mgbc - mgab * cosb) * invabc * isinb2;
+        const double fb2 = cosc * invbc * isinc2;
+        const double fd = -invcd * isinc2;
+        const double fix = crabbc.x * fa, fiy = crabbc.y * fa, fiz = crabbc.z * fa;
+        const double fjx = fb1 * crabbc.x - fb2 * crbccd.x;
+        const double fjy = fb1 * crabbc.y - fb2 * crbccd.y;
+        const double fjz = fb1 * crabbc.z - fb2 * crbccd.z;
+        const double flx = -fd * crbccd.x, fly = -fd * crbccd.y, flz = -fd * crbccd.z;
+        v.force64(ia, fix, fiy, fiz, fs);
+        v.force64(ja, fjx, fjy, fjz, fs);
+        v.force64(ka, -(fix + fjx + flx), -(fiy + fjy + fly), -(fiz + fjz + flz), fs);
+        v.force64(la, flx, fly, flz, fs);
       }
-      const float edih = __fmul_rn(amp, __fadd_rn(1.0f, cos_sangle));
+      const double opc = (cos_sangle >= 0.0) ? 1.0 + cos_sangle :
+                                               sin_sangle * sin_sangle / (1.0 - cos_sangle);
       if (improper) {
-        e_impr = edih;
+        e_impr = prm.x * opc;
       }
       else {
-        e_prop = edih;
+        e_prop = prm.x * opc;
       }
-      // attached 1-4 pair between atoms i and l
-      const float inv_scee = __uint_as_float(rb.z);
-      if (inv_scee > 0.0f) {
-        const float inv_scnb = __uint_as_float(rb.w);
-        const float3 dv = v.delta(ia, la);
-        const float4 pi = v.prm(ia);
-        const float4 pl = v.prm(la);
-        const int code_i = __float_as_int(pi.y);
-        const int code_l = __float_as_int(pl.y);
+      // attached 1-4 pair between atoms i and l, FP64 charges and 1-4 Lennard-Jones tables
+      const double2 att = d.dihe14_64[pos];   // 1 / scee, 1 / scnb
+      if (att.x > 0.0) {
+        const int gi = d.atom_start[sysid] + li;
+        const int gl = d.atom_start[sysid] + ll;
+        const double3 dv = sub3d(pl, pi);
         const int nt = d.lj_ntypes[sysid];
-        const float2 ab14 = v.lj14(code_i, code_l, nt);
-        const float lja = ab14.x * inv_scnb;
-        const float ljb = ab14.y * inv_scnb;
-        const float qiqj = pi.x * pl.x * inv_scee;
-        const float invr2 = 1.0f / (dv.x * dv.x + dv.y * dv.y + dv.z * dv.z);
-        const float invr = sqrtf(invr2);
-        const float invr4 = invr2 * invr2;
+        const double2 ab14 = d.ljab14_64[d.lj_start[sysid] + d.lj_idx[gi] * nt + d.lj_idx[gl]];
+        const double lja = ab14.x * att.y;
+        const double ljb = ab14.y * att.y;
+        const double qiqj = d.charge64[gi] * d.charge64[gl] * att.x;
+        const double invr2 = 1.0 / dot3d(dv, dv);
+        const double invr = sqrt(invr2);
+        const double invr6 = invr2 * invr2 * invr2;
         const float2 cl = CLASH ? v.clash(k) : make_float2(0.0f, 0.0f);
         if (CLASH && (cl.x > 0.0f || cl.y > 0.0f)) {
           // clash-softened 1-4 pair (valence_potential.tpp:1337-1357)
-          const float fmag = softCorePair(1.0f / invr, invr, qiqj, lja, ljb, cl.x,
-                                          quadraticCore(cl.x), cl.y, &e_el14, &e_lj14);
+          const double fmag = softCorePair64(1.0 / invr, invr, qiqj, lja, ljb, cl.x,
+                                             quadraticCore64(cl.x), cl.y, &e_el14, &e_lj14);
           if (FORCE) {
-            v.force(ia, fmag * dv.x, fmag * dv.y, fmag * dv.z, fs);
-            v.force(la, -fmag * dv.x, -fmag * dv.y, -fmag * dv.z, fs);
+            v.force64(ia, fmag * dv.x, fmag * dv.y, fmag * dv.z, fs);
+            v.force64(la, -fmag * dv.x, -fmag * dv.y, -fmag * dv.z, fs);
           }
         }
         else {
           if (FORCE) {
-            const float fmag = -(qiqj * invr * invr2) +
-                               (6.0f * ljb - 12.0f * lja * invr4 * invr2) * invr4 * invr4;
-            v.force(ia, fmag * dv.x, fmag * dv.y, fmag * dv.z, fs);
-            v.force(la, -fmag * dv.x, -fmag * dv.y, -fmag * dv.z, fs);
+            const double fmag = -(qiqj * invr * invr2) +
+                                (6.0 * ljb - 12.0 * lja * invr6) * invr6 * invr2;
+            v.force64(ia, fmag * dv.x, fmag * dv.y, fmag * dv.z, fs);
+            v.force64(la, -fmag * dv.x, -fmag * dv.y, -fmag * dv.z, fs);
           }
-          e_el14 = __fmul_rn(qiqj, invr);
-          e_lj14 = __fsub_rn(__fmul_rn(__fmul_rn(__fmul_rn(lja, invr4), invr4), invr4),
-                             __fmul_rn(__fmul_rn(ljb, invr4), invr2));
+          e_el14 = qiqj * invr;
+          e_lj14 = (lja * invr6 - ljb) * invr6;
         }
       }
     }
     if (ENERGY) {
-      v.energy(k, kProperDihedral, e_prop, es);
-      v.energy(k, kImproperDihedral, e_impr, es);
-      v.energy(k, kElec14, e_el14, es);
-      v.energy(k, kVdw14, e_lj14, es);
+      v.energy64(k, kProperDihedral, e_prop, es);
+      v.energy64(k, kImproperDihedral, e_impr, es);
+      v.energy64(k, kElec14, e_el14, es);
+      v.energy64(k, kVdw14, e_lj14, es);
     }
   }
 }
@@ -803,14 +901,25 @@ __device__ __forceinline__ TileInfo tileInfo(const UnitSmem &s, int nsys_u, int 
 // zero (no charge, zero screened radius and dE/dR, masked Lennard-Jones, far-away coordinates),
 // so partial tiles run the same branch-free loop; only the last step of a diagonal tile, where
 // lanes l and l + 16 would meet the same pair, runs on half the lanes.
+//
+// tileFlush(p) runs after every eighth step and at the end of the tile: passes that sum energies
+// in FP32 move their partial sums into integer accumulators there, so no FP32 running sum spans
+// more than eight pairs (the generic overload does nothing).
+template <class P>
+__device__ __forceinline__ void tileFlush(P &) {}
+
 template <class P>
 __device__ __forceinline__ void walkTile(P &p, const TileInfo &ti, int lane) {
   if (!ti.diag) {
+#pragma unroll 1
+    for (int k0 = 0; k0 < kTile; k0 += 8) {
 #pragma unroll 2
-    for (int k = 0; k < kTile; k++) {
-      const int jl = (lane + k) & 31;
-      p.pair(ti.jbase + jl, jl);
-      p.rotate(lane);
+      for (int k = k0; k < k0 + 8; k++) {
+        const int jl = (lane + k) & 31;
+        p.pair(ti.jbase + jl, jl);
+        p.rotate(lane);
+      }
+      tileFlush(p);
     }
   }
   else {
@@ -819,11 +928,15 @@ __device__ __forceinline__ void walkTile(P &p, const TileInfo &ti, int lane) {
       const int jl = (lane + k) & 31;
       p.pair(ti.jbase + jl, jl);
       p.rotate(lane);
+      if (k == 8) {
+        tileFlush(p);
+      }
     }
     if (lane < 16) {
       p.pair(ti.jbase + lane + 16, lane + 16);
     }
     p.rotate(lane);
+    tileFlush(p);
   }
 }
 
@@ -941,9 +1054,18 @@ struct PairPass {
   float clash_d, clash_r;
   float2 qcore;
   float fxi, fyi, fzi, dei, fxj, fyj, fzj, dej;
-  float e_elec, e_vdw, e_gb;
+  float e_elec, e_vdw, e_gb;        // FP32 sums of at most eight pairs (see tileFlush)
+  double t_elec, t_vdw, t_gb;       // this lane's FP64 sums over the tile (see tileEnergy)
   __device__ PairPass(const UnitSmem &s_in, float kappa, float inv_dielectric) :
       s(s_in), kk(-kappa * kGbKscale), inv_diel(inv_dielectric), salt(kappa > 0.0f) {}
+  __device__ __forceinline__ void flush() {
+    if (ENERGY) {
+      t_elec += static_cast<double>(e_elec);
+      t_vdw += static_cast<double>(e_vdw);
+      t_gb += static_cast<double>(e_gb);
+      e_elec = e_vdw = e_gb = 0.0f;
+    }
+  }
   __device__ __forceinline__ void begin(int islot, unsigned mask_in,
                                         float2 clash = make_float2(0.0f, 0.0f)) {
     ai = s.pa[islot];
@@ -960,22 +1082,35 @@ struct PairPass {
     fxi = fyi = fzi = dei = 0.0f;
     fxj = fyj = fzj = dej = 0.0f;
     e_elec = e_vdw = e_gb = 0.0f;
+    t_elec = t_vdw = t_gb = 0.0;
   }
   __device__ __forceinline__ void pair(int jslot, int jl) {
     const float4 aj = s.pa[jslot];
     const float4 bj = s.pb[jslot];
-    const float3 dv = pairDelta(ai, bi, aj, bj);
+    const float hx = aj.x - ai.x, hy = aj.y - ai.y, hz = aj.z - ai.z;
+    const float lx = bj.x - bi.x, ly = bj.y - bi.y, lz = bj.z - bi.z;
+    const float3 dv = make_float3(hx + lx, hy + ly, hz + lz);
     const float r2 = fmaf(dv.x, dv.x, fmaf(dv.y, dv.y, dv.z * dv.z));
     const float qiqj_all = ai.w * aj.w;
     float fmag = 0.0f;
     if (NB) {
       // excluded and padding pairs take the same path with zero parameters
       const float incl = ((mask >> jl) & 1u) ? 0.0f : 1.0f;
-      // one Newton step on rsqrt keeps r^-12 within a few ulp
+      // 1/r from rsqrt with one Newton step (Coulomb), and 1/r^2 as its own reciprocal: r^-6
+      // and r^-12 multiply the relative error of 1/r^2 by 3 and 6, so squaring 1/r (twice its
+      // error) would double the rounding of the repulsive wall, and the Newton step of 1/r^2
+      // takes the exact r^2 = r2 + 2 (dx ex + dy ey + dz ez) + O(e^2), the e the separations'
+      // recovered rounding errors (separationError): without it the Lennard-Jones energy of a
+      // molecule with close contacts errs by up to 1.5e-6 of the root-sum-square of its pair
+      // terms.  r2 >= 256 on padding slots, never zero.
       float invr = rsqrtf(r2);
       invr = invr * fmaf(-0.5f * r2 * invr, invr, 1.5f);
-      const float invr2 = invr * invr;
-      const float invr4 = invr2 * invr2;
+      const float r2c = fmaf(dv.x, separationError(hx, lx, dv.x),
+                             fmaf(dv.y, separationError(hy, ly, dv.y),
+                                  dv.z * separationError(hz, lz, dv.z)));
+      float invr2 = __fdividef(1.0f, r2);
+      invr2 = fmaf(invr2, fmaf(-2.0f * r2c, invr2, fmaf(-r2, invr2, 1.0f)), invr2);
+      const float invr6 = invr2 * invr2 * invr2;
       float2 ab = s.lj[code_i + (__float_as_int(s.prm[jslot].y) >> 16)];
       ab.x *= incl;
       ab.y *= incl;
@@ -987,12 +1122,10 @@ struct PairPass {
       else {
         if (ENERGY) {
           e_elec = __fadd_rn(e_elec, __fmul_rn(qiqj, invr));
-          e_vdw = __fadd_rn(e_vdw, __fmul_rn(__fsub_rn(__fmul_rn(__fmul_rn(ab.x, invr4), invr4),
-                                                       __fmul_rn(ab.y, invr2)), invr4));
+          e_vdw = __fadd_rn(e_vdw, __fmul_rn(__fsub_rn(__fmul_rn(ab.x, invr6), ab.y), invr6));
         }
         if (FORCE) {
-          fmag = -(qiqj * invr * invr2) +
-                 (6.0f * ab.y - 12.0f * ab.x * invr4 * invr2) * invr4 * invr4;
+          fmag = -(qiqj * invr * invr2) + (6.0f * ab.y - 12.0f * ab.x * invr6) * invr6 * invr2;
         }
       }
     }
@@ -1044,6 +1177,11 @@ struct PairPass {
     }
   }
 };
+
+template <bool FORCE, bool ENERGY, bool NB, bool GB, bool CLASH>
+__device__ __forceinline__ void tileFlush(PairPass<FORCE, ENERGY, NB, GB, CLASH> &p) {
+  p.flush();
+}
 
 // Pass 3: radius chain-rule forces
 template <bool NECK = false>
@@ -1240,24 +1378,26 @@ __device__ void pairTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u, 
   const float es = d.nrg_scale;
   const float ds = static_cast<float>(1 << kDeijdaBits);
   PairPass<FORCE, ENERGY, NB, GB, CLASH> p(s, d.kappa, d.inv_dielectric);
+  // a molecule's energies over this warp's tiles, each tile rounded to the output grid
+  // (tileEnergy), the same value in every lane
   long long acc_elec = 0, acc_vdw = 0, acc_gb = 0;
   int acc_k = -1;
+  auto commit = [&]() {
+    if (lane == 0 && acc_k >= 0) {
+      if (NB) {
+        atomicAdd(&s.nrg[acc_k * kNrgStride + kElec], static_cast<unsigned long long>(acc_elec));
+        atomicAdd(&s.nrg[acc_k * kNrgStride + kVdw], static_cast<unsigned long long>(acc_vdw));
+      }
+      if (GB) {
+        atomicAdd(&s.nrg[acc_k * kNrgStride + kGb], static_cast<unsigned long long>(acc_gb));
+      }
+    }
+    acc_elec = acc_vdw = acc_gb = 0;
+  };
   for (int t = first; t < ntiles; t += stride) {
     const TileInfo ti = tileInfo(s, nsys_u, t);
     if (ENERGY && ti.k != acc_k) {
-      if (acc_k >= 0) {
-        const long long se = warpSum(acc_elec), sv = warpSum(acc_vdw), sg = warpSum(acc_gb);
-        if (lane == 0) {
-          if (NB) {
-            atomicAdd(&s.nrg[acc_k * kNrgStride + kElec], static_cast<unsigned long long>(se));
-            atomicAdd(&s.nrg[acc_k * kNrgStride + kVdw], static_cast<unsigned long long>(sv));
-          }
-          if (GB) {
-            atomicAdd(&s.nrg[acc_k * kNrgStride + kGb], static_cast<unsigned long long>(sg));
-          }
-        }
-      }
-      acc_elec = acc_vdw = acc_gb = 0;
+      commit();
       acc_k = ti.k;
     }
     unsigned mask = 0u;
@@ -1287,22 +1427,17 @@ __device__ void pairTiles(const DevSynthesis &d, const UnitSmem &s, int nsys_u, 
       }
     }
     if (ENERGY) {
-      acc_elec += __float2ll_rn(p.e_elec * es);
-      acc_vdw += __float2ll_rn(p.e_vdw * es);
-      acc_gb += __float2ll_rn(p.e_gb * es);
+      if (NB) {
+        acc_elec += tileEnergy(p.t_elec, es);
+        acc_vdw += tileEnergy(p.t_vdw, es);
+      }
+      if (GB) {
+        acc_gb += tileEnergy(p.t_gb, es);
+      }
     }
   }
   if (ENERGY) {
-    const long long se = warpSum(acc_elec), sv = warpSum(acc_vdw), sg = warpSum(acc_gb);
-    if (lane == 0 && acc_k >= 0) {
-      if (NB) {
-        atomicAdd(&s.nrg[acc_k * kNrgStride + kElec], static_cast<unsigned long long>(se));
-        atomicAdd(&s.nrg[acc_k * kNrgStride + kVdw], static_cast<unsigned long long>(sv));
-      }
-      if (GB) {
-        atomicAdd(&s.nrg[acc_k * kNrgStride + kGb], static_cast<unsigned long long>(sg));
-      }
-    }
+    commit();
   }
 }
 
@@ -1459,15 +1594,9 @@ __device__ __forceinline__ void placeSlot(const DevSynthesis &d, const UnitSmem 
   const float4 prm = s.prm[slot];
   float4 pa, pb;
   if (real) {
-    const double x = static_cast<double>(cx) * d.inv_gpos_scale;
-    const double y = static_cast<double>(cy) * d.inv_gpos_scale;
-    const double z = static_cast<double>(cz) * d.inv_gpos_scale;
-    pa.x = static_cast<float>(x);
-    pa.y = static_cast<float>(y);
-    pa.z = static_cast<float>(z);
-    pb.x = static_cast<float>(x - static_cast<double>(pa.x));
-    pb.y = static_cast<float>(y - static_cast<double>(pa.y));
-    pb.z = static_cast<float>(z - static_cast<double>(pa.z));
+    splitCoordinate(static_cast<double>(cx) * d.inv_gpos_scale, &pa.x, &pb.x);
+    splitCoordinate(static_cast<double>(cy) * d.inv_gpos_scale, &pa.y, &pb.y);
+    splitCoordinate(static_cast<double>(cz) * d.inv_gpos_scale, &pa.z, &pb.z);
   }
   else {
     pa = make_float4(5000.0f + 16.0f * static_cast<float>(slot), 0.0f, 0.0f, 0.0f);

@@ -1,9 +1,32 @@
-"""Helpers that turn golden fixtures into molecule objects for the library and the oracle."""
+"""Helpers that turn golden fixtures into molecule objects for the library and the oracle, and
+the energy and force tolerances every GPU test applies.
+
+Tolerances of the FP32 path (FP32 arithmetic, fixed-point accumulation) against FP64 results
+(STORMM's CPU build or the FP64 oracle):
+
+* every energy term of every molecule: |E_gpu - E_ref| <= 1e-6 x max(|E_ref|, 1 kcal/mol, R),
+  R the root-sum-square of the term's contributions (oracle ``magnitudes``: each bond, angle,
+  dihedral, pair or GB self term; a Lennard-Jones pair counts |A|/r^12 + |B|/r^6).  For a term
+  whose contributions share a sign R <= |E| and the bound is plain 1e-6 relative (with an
+  absolute floor below 1 kcal/mol).  R matters for the Coulomb and Lennard-Jones pair sums and
+  GB, differences of large positive and negative parts: on the 1,024-molecule workload one
+  241-atom molecule's Coulomb total is -1.6 kcal/mol out of pair terms with R = 620 kcal/mol.
+  Each pair evaluated in FP32 is rounded independently (relative 1e-7 or so; r^-12 multiplies
+  the rounding of r^2 by six), so the error of the sum grows like R, and 1e-6 of R is what an
+  FP32 evaluation of each pair can meet.  The FP64 mode meets the bound without R on every term
+  (tests/test_gpu_workloads.py);
+* the total energy: within the sum of the per-term bounds;
+* forces: RMS relative error at most 5e-6 against FP64.
+"""
 import glob
 import os
 from types import SimpleNamespace
 
 import numpy as np
+
+ENERGY_REL_TOL = 1.0e-6
+ENERGY_FLOOR = 1.0               # kcal/mol: terms smaller than this are held to 1e-6 kcal/mol
+FORCE_TOL = 5.0e-6
 
 from conftest import GOLDEN
 
@@ -90,3 +113,44 @@ def reference_forces(g):
 
 def rms_rel(a, b):
     return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
+
+
+def energy_tolerances(e_ref, rss=None, rel=ENERGY_REL_TOL):
+    """Per-term bounds (see the module docstring); rss: the oracle's per-term root-sum-squares
+    of the contributions, or None for the plain bound rel x max(|E|, 1 kcal/mol)."""
+    e_ref = np.asarray(e_ref, dtype=np.float64)
+    scale = np.maximum(np.abs(e_ref), ENERGY_FLOOR)
+    if rss is not None:
+        scale = np.maximum(scale, np.asarray(rss, dtype=np.float64))
+    return rel * scale
+
+
+def energy_excess(e_gpu, e_ref, rss=None, **kw):
+    """Error over bound per term (a value above 1 fails)."""
+    return np.abs(np.asarray(e_gpu) - np.asarray(e_ref)) / energy_tolerances(e_ref, rss, **kw)
+
+
+def check_energies(e_gpu, e_ref, rss=None, what="", **kw):
+    """Assert every term and the total against the per-term bounds."""
+    tol = energy_tolerances(e_ref, rss, **kw)
+    err = np.abs(np.asarray(e_gpu) - np.asarray(e_ref))
+    assert np.all(err <= tol), (what, err / tol, e_gpu, e_ref)
+    assert abs(float(np.sum(e_gpu)) - float(np.sum(e_ref))) <= tol.sum(), what
+
+
+def total_tolerance(e_ref_terms, rss=None, **kw):
+    """Bound on a total energy: the sum of its terms' bounds."""
+    return float(energy_tolerances(e_ref_terms, rss, **kw).sum())
+
+
+def oracle_magnitudes(mol, coords=None):
+    """Per-term root-sum-squares of a molecule object at its (or the given) coordinates."""
+    import oracle
+    return oracle.from_molecule(mol).magnitudes(mol.coords if coords is None else coords)
+
+
+def fixture_magnitudes(g):
+    """Per-term root-sum-squares of a fixture at its coordinates, with STORMM's GB radii."""
+    import oracle
+    radii = g["gb_radii"] if "gb_radii" in g else None
+    return oracle.from_fixture(g).magnitudes(g["coords"], radii)

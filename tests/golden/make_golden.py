@@ -3,7 +3,9 @@
 Requires the reference sources and the reference CPU build (oracle/ref/Makefile, which puts
 libstormm_ref.so and stormm_ref_driver under oracle/_ref/).  Run from the repository root:
 
-    python tests/golden/make_golden.py [--reference-root /root/reference]
+    python tests/golden/make_golden.py [--reference-root DIR]
+
+(DIR defaults to $STORMM_REFERENCE_ROOT, else /root/reference.)
 
 Fixtures written (numpy .npz, one per case):
 
@@ -99,7 +101,8 @@ def gb_known_answers(ref_root):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference-root", default="/root/reference")
+    ap.add_argument("--reference-root",
+                    default=os.environ.get("STORMM_REFERENCE_ROOT", "/root/reference"))
     ap.add_argument("--variants-only", action="store_true",
                     help="write only the solvent-model variant fixtures")
     ap.add_argument("--clash-only", action="store_true",

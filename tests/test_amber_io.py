@@ -18,7 +18,7 @@ from stormm_b200.synthetic import make_chain, make_molecule
 
 from fixtures import igb_of_fixture, load, molecule_from_fixture, reference_paths
 
-REFERENCE_TEST = "/root/reference/test"
+REFERENCE_TEST = os.path.join(os.environ.get("STORMM_REFERENCE_ROOT", "/root/reference"), "test")
 FILES = {"trpcage": ("trpcage.top", "trpcage.inpcrd"),
          "ala_dipeptide": ("ala_dipeptide.top", "ala_dipeptide.inpcrd")}
 

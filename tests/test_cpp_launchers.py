@@ -21,7 +21,7 @@ from stormm_b200 import prmtop as amber_writer
 from stormm_b200 import synthetic
 
 from conftest import ROOT
-from fixtures import rms_rel
+from fixtures import check_energies, oracle_magnitudes, rms_rel
 
 SOURCE = os.path.join(ROOT, "tests", "cpp", "launcher_check.cpp")
 LIBDIR = os.path.join(ROOT, "stormm_b200")
@@ -127,8 +127,7 @@ def test_launchers_match_python_path_and_oracle(tmp_path):
         m = mols[t]
         o = oracle.from_molecule(m, igb=sb.SB_GB_OBC2).evaluate(m.coords)
         got = np.array([e[s, sb.NRG_SLOTS[k]] for k in sb.TERM_ORDER])
-        scale = max(np.abs(o["energies"]).sum(), 10.0)
-        assert np.all(np.abs(got - o["energies"]) <= 1e-6 * scale), (s, got, o["energies"])
+        check_energies(got, o["energies"], oracle_magnitudes(m), s)
         assert rms_rel(f[off:off + m.natom], o["forces"]) <= 5e-6
         off += m.natom
 

@@ -1,9 +1,9 @@
 """CUDA path against the FP64 oracle and STORMM's own CPU results, through the C ABI.
 
-Tolerances (FP32 arithmetic with fixed-point accumulation against FP64):
-* energies: each term and the total within 1e-6 of the system's summed absolute energy (with a
-  floor of 10 kcal/mol for molecules of a few atoms, whose FP32 bond energies carry an absolute
-  error of a few 1e-6 kcal/mol);
+Tolerances (FP32 arithmetic with fixed-point accumulation against FP64), as tests/fixtures.py
+states them:
+* energies: each term within 1e-6 of the largest of |E_term|, 1 kcal/mol and the root-sum-square
+  of the term's contributions;
 * forces: RMS relative error at most 5e-6 against FP64;
 * fixed-point sums: bit-identical across runs, across batch compositions and between the batched
   and the per-system launches.
@@ -15,14 +15,11 @@ import pytest
 
 import oracle
 import stormm_b200 as sb
-from fixtures import (default_solvent_paths, igb_of_fixture, load, molecule_from_fixture,
-                      reference_forces, reference_paths, rms_rel, solvent_options,
-                      synthetic_paths)
+from fixtures import (FORCE_TOL, check_energies, default_solvent_paths, fixture_magnitudes,
+                      load, molecule_from_fixture, oracle_magnitudes, reference_forces,
+                      reference_paths, rms_rel, solvent_options, synthetic_paths)
 
 pytestmark = pytest.mark.gpu
-
-ENERGY_TOL = 1.0e-6
-FORCE_TOL = 5.0e-6
 
 
 def _run(mols, igb=5, dielectric=80.0, terms=sb.TERM_ALL, coords=None, **opts):
@@ -36,18 +33,12 @@ def _run(mols, igb=5, dielectric=80.0, terms=sb.TERM_ALL, coords=None, **opts):
     return out
 
 
-def _check_energy(e_gpu, e_ref):
-    scale = max(np.abs(e_ref).sum(), 10.0)
-    assert np.all(np.abs(e_gpu - e_ref) <= ENERGY_TOL * scale), (e_gpu, e_ref)
-    assert abs(e_gpu.sum() - e_ref.sum()) <= ENERGY_TOL * scale
-
-
 @pytest.mark.parametrize("path", synthetic_paths(), ids=os.path.basename)
 def test_single_system_matches_stormm(path):
     g = load(os.path.basename(path))
     mol = molecule_from_fixture(g)
     r = _run([mol], **solvent_options(g))
-    _check_energy(r["energies"][0], g["energy_terms"])
+    check_energies(r["energies"][0], g["energy_terms"], fixture_magnitudes(g), path)
     err = rms_rel(r["forces"], reference_forces(g))
     assert err <= FORCE_TOL, err
 
@@ -60,7 +51,7 @@ def test_reference_systems_known_answers(path):
     g = load(os.path.basename(path))
     mol = molecule_from_fixture(g)
     r = _run([mol], **solvent_options(g))
-    _check_energy(r["energies"][0], g["energy_terms"])
+    check_energies(r["energies"][0], g["energy_terms"], fixture_magnitudes(g), path)
     assert abs(r["energies"][0][8] - g["known_answer_gb"][0]) < 1e-3
     assert rms_rel(r["forces"], reference_forces(g)) <= FORCE_TOL
 
@@ -93,7 +84,7 @@ def test_batch_of_mixed_sizes_is_bit_identical_to_single_runs():
     # and each system still matches STORMM
     for k, p in enumerate(paths):
         g = load(os.path.basename(p))
-        _check_energy(batch["energies"][k], g["energy_terms"])
+        check_energies(batch["energies"][k], g["energy_terms"], fixture_magnitudes(g), p)
 
 
 def _system_layout(syn, k):
@@ -143,7 +134,7 @@ def test_separate_launchers_sum_to_fused():
     syn.launch_nonbonded()
     syn.launch_valence()
     for k in range(len(mols)):
-        _check_energy(syn.energy_terms()[k], fused_e[k])
+        check_energies(syn.energy_terms()[k], fused_e[k], oracle_magnitudes(mols[k]))
     assert rms_rel(syn.forces(), fused_f) < 1e-6
 
 
@@ -153,7 +144,7 @@ def test_energy_only_matches_force_energy():
     e_fe = syn.energy_terms()
     syn.initialize()
     syn.evaluate(force=False, energy=True)
-    _check_energy(syn.energy_terms()[0], e_fe[0])
+    check_energies(syn.energy_terms()[0], e_fe[0], oracle_magnitudes(mols[0]))
     assert not syn.forces().any()
 
 
@@ -167,7 +158,7 @@ def test_synthetic_batch_against_oracle():
     off = 0
     for k, m in enumerate(mols):
         o = oracle.from_molecule(m).evaluate(m.coords)
-        _check_energy(r["energies"][k], o["energies"])
+        check_energies(r["energies"][k], o["energies"], oracle_magnitudes(m), m.natom)
         err = rms_rel(f_all[off:off + m.natom], o["forces"])
         assert err <= FORCE_TOL, (m.natom, err)
         off += m.natom
@@ -190,11 +181,12 @@ def test_clash_mitigated_evaluation_matches_stormm():
     syn.initialize()
     syn.evaluate_clash(float(g["clash_r0"][0]), float(g["clash_ratio"][0]))
     assert syn.status() == 0
-    _check_energy(syn.energy_terms()[0], g["clash_energy_terms"])
+    rss = fixture_magnitudes(g)
+    check_energies(syn.energy_terms()[0], g["clash_energy_terms"], rss)
     assert rms_rel(syn.forces(), g["clash_frc_total"].reshape(-1, 3)) <= FORCE_TOL
     syn.initialize()
     syn.evaluate()
-    _check_energy(syn.energy_terms()[0], g["energy_terms_mm"])
+    check_energies(syn.energy_terms()[0], g["energy_terms_mm"], rss)
     # zero distance and ratio is the plain evaluation, bit for bit
     f_plain = syn.forces_fixed()[0].copy()
     syn.initialize()
@@ -208,7 +200,7 @@ def test_neck_gb_on_the_tiled_path_and_without_tables():
     g = load("synthetic_N8.npz")
     mol = molecule_from_fixture(g)
     tiled = _run([mol], tiled_above_atoms=32, **solvent_options(g))
-    _check_energy(tiled["energies"][0], g["energy_terms"])
+    check_energies(tiled["energies"][0], g["energy_terms"], fixture_magnitudes(g))
     assert rms_rel(tiled["forces"], reference_forces(g)) <= FORCE_TOL
     with pytest.raises(sb.StormmB200Error):
         sb.Synthesis([mol], igb=8)

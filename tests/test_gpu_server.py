@@ -11,6 +11,7 @@ import pytest
 
 import stormm_b200 as sb
 from stormm_b200 import synthetic
+from fixtures import check_energies, oracle_magnitudes
 
 pytestmark = pytest.mark.gpu
 
@@ -131,8 +132,7 @@ def test_evaluation_requests_mixed_with_minimizations():
         assert r["rms_force"] == pytest.approx(np.sqrt((f_alone ** 2).mean()), rel=1e-12)
         o = oracle.from_molecule(m).evaluate(m.coords)
         got = np.array([r["energies"][sb.NRG_SLOTS[t]] for t in sb.TERM_ORDER])
-        scale = max(np.abs(o["energies"]).sum(), 10.0)
-        assert np.all(np.abs(got - o["energies"]) <= 1e-6 * scale)
+        check_energies(got, o["energies"], oracle_magnitudes(m), m.natom)
         err = np.sqrt(((arr - o["forces"]) ** 2).sum() / (o["forces"] ** 2).sum())
         assert err <= 5e-6, (m.natom, err)
     assert seen == {"minimize": len(mols) - 1, "evaluate": len(mols)}

@@ -16,12 +16,11 @@ import pytest
 import oracle
 import stormm_b200 as sb
 from stormm_b200 import synthetic
-from fixtures import load, molecule_from_fixture, reference_forces, rms_rel
+from fixtures import (FORCE_TOL, check_energies, fixture_magnitudes, load,
+                      molecule_from_fixture, oracle_magnitudes, reference_forces, rms_rel)
 
 pytestmark = pytest.mark.gpu
 
-ENERGY_TOL = 1.0e-6
-FORCE_TOL = 5.0e-6
 
 
 def _evaluate(mols, **opts):
@@ -33,10 +32,11 @@ def _evaluate(mols, **opts):
     return syn
 
 
-def _close(fused, tiled):
+def _close(fused, tiled, rss):
+    """The two FP32 paths sum in different orders: per-term bounds against each other."""
     e_f, e_t = fused.energy_terms(), tiled.energy_terms()
-    scale = np.maximum(np.abs(e_f).sum(axis=1), 10.0)[:, None]
-    assert np.all(np.abs(e_f - e_t) <= 1e-7 * scale)
+    for k in range(len(rss)):
+        check_energies(e_t[k], e_f[k], rss[k], k)
     assert rms_rel(tiled.forces(), fused.forces()) <= 1e-6
 
 
@@ -46,7 +46,8 @@ def test_tiled_path_agrees_with_fused_and_repeats_exactly():
     mols.append(molecule_from_fixture(load("synthetic_C600.npz")))
     fused = _evaluate(mols)
     tiled = _evaluate(mols, tiled_above_atoms=32)
-    _close(fused, tiled)
+    rss = [oracle_magnitudes(m) for m in mols]
+    _close(fused, tiled, rss)
     fp, _ = fused.forces_fixed()
     tp, _ = tiled.forces_fixed()
     assert np.abs(fp - tp).max() <= 2.0e-7 * np.abs(fp).max()
@@ -66,20 +67,19 @@ def test_tiled_path_agrees_with_fused_and_repeats_exactly():
         syn.initialize()
         syn.evaluate(force=False, energy=True)
     e_f, e_t = fused.energy_terms(), tiled.energy_terms()
-    assert np.all(np.abs(e_f - e_t) <= 1e-7 * np.maximum(np.abs(e_f).sum(axis=1), 10.0)[:, None])
+    for k in range(len(mols)):
+        check_energies(e_t[k], e_f[k], rss[k], k)
     for syn in (fused, tiled):
         syn.initialize()
         syn.launch_valence()
         syn.launch_nonbonded()
-    _close(fused, tiled)
+    _close(fused, tiled, rss)
 
 
 def test_tiled_chain_fixture_matches_stormm():
     g = load("synthetic_C600.npz")
     syn = _evaluate([molecule_from_fixture(g)], tiled_above_atoms=256)
-    e = syn.energy_terms()[0]
-    scale = max(np.abs(g["energy_terms"]).sum(), 10.0)
-    assert np.all(np.abs(e - g["energy_terms"]) <= ENERGY_TOL * scale)
+    check_energies(syn.energy_terms()[0], g["energy_terms"], fixture_magnitudes(g))
     assert rms_rel(syn.forces(), reference_forces(g)) <= FORCE_TOL
 
 
@@ -90,8 +90,7 @@ def test_large_chains_against_oracle():
     forces = syn.split(syn.forces())
     for k, m in enumerate(mols):
         ref = oracle.from_molecule(m).evaluate(m.coords)
-        scale = max(np.abs(ref["energies"]).sum(), 10.0)
-        assert np.all(np.abs(energies[k] - ref["energies"]) <= ENERGY_TOL * scale), k
+        check_energies(energies[k], ref["energies"], oracle_magnitudes(m), k)
         assert rms_rel(forces[k], ref["forces"]) <= FORCE_TOL, k
 
 

@@ -122,3 +122,19 @@ def test_clash_damped_minimization_reaches_reference_basin():
     ref_hist = m["min_potential_history"]
     assert abs(hist[0] - ref_hist[0]) < 1e-9 * abs(ref_hist[0])
     assert abs(hist[-1] - ref_hist[-1]) < 0.02 * abs(ref_hist[-1])
+
+
+def test_oracle_matches_stormm_on_the_single_point_workload_sample():
+    """The FP64 restatement against STORMM's own CPU build on 64 molecules of the 1,024-molecule
+    workload (tests/golden/workload_single_point_sample.npz)."""
+    from stormm_b200 import synthetic
+    g = dict(np.load(os.path.join(GOLDEN, "workload_single_point_sample.npz")))
+    mols = synthetic.workload_batched_single_point(1024, seed=synthetic.SEED_BASE + 1)
+    offs = np.concatenate([[0], np.cumsum(g["natom"])])
+    for j, k in enumerate(g["index"]):
+        m = mols[k]
+        c = g["coords"][offs[j]:offs[j + 1]]
+        r = oracle.from_molecule(m).evaluate(c)
+        np.testing.assert_allclose(r["energies"], g["energy_terms"][j], rtol=1e-11, atol=1e-10)
+        f = g["forces"][offs[j]:offs[j + 1]]
+        assert np.sqrt(((r["forces"] - f) ** 2).sum() / (f ** 2).sum()) < 1e-11
