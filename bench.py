@@ -13,9 +13,12 @@ trial points; one step is one whole minimization of every molecule.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-N > 1 runs under torchrun, one process per GPU; each rank works on its own molecules (weak
-scaling, no collective on the data path; the only collective is the max-over-ranks of the
-timing).  Rank 0 prints one JSON line.
+With N > 1 the benchmark runs one process per GPU: under torchrun (RANK / WORLD_SIZE set) or,
+without it, by spawning N ranks itself.  The ranks take disjoint shards of one seeded workload
+of N x 1,024 (and N x 4,096) molecules, partitioned by pair count largest first
+(stormm_b200.sharding.partition_lpt): weak scaling with no collective on the data path; the
+only collectives are the barriers around timed regions and the max over ranks of the timing.
+Rank 0 prints the details of every leg on one line and the summary on the last line.
 """
 from __future__ import annotations
 
@@ -49,6 +52,10 @@ SERVED_WINDOW_S = 1.0
 SERVED_WORKLOAD = ("served minimization stream: Poisson arrivals, lognormal sizes (median 48 atoms, "
                    "sigma 0.6, clipped 12-512), 0.3 A start noise, each to RMS force <= 0.01 "
                    "kcal/mol/A or 2000 cycles")
+TERMS = ["bond", "angle", "proper_dihedral", "improper_dihedral", "vdw", "vdw_14", "elec",
+         "elec_14", "gb"]
+ENERGY_BOUND = ("each term: |E - E_fp64| <= 1e-6 x max(|E_fp64|, 1 kcal/mol, root-sum-square of "
+                "the term's contributions); forces: RMS relative error <= 5e-6")
 
 
 def _args():
@@ -63,6 +70,7 @@ def _args():
     ap.add_argument("--min-steps", type=int, default=2)
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--no-large", action="store_true")
+    ap.add_argument("--no-errors", action="store_true")
     return ap.parse_args()
 
 
@@ -125,88 +133,118 @@ def _dist():
     return world, rank, local
 
 
-def _seed_single(rank: int) -> int:
+# ------------------------------------------------------------------------------------------------
+# Workloads: one seeded set of world x n molecules, an LPT shard per rank
+# ------------------------------------------------------------------------------------------------
+def _shard(sizes, world, rank):
+    from stormm_b200 import sharding
+    if world == 1:
+        return np.arange(len(sizes))
+    return sharding.partition_lpt(sizes, world)[rank]
+
+
+def single_point_molecules(world, rank):
     from stormm_b200 import synthetic
-    return synthetic.SEED_BASE + 1 + 1000 * rank
+    seed = synthetic.SEED_BASE + 1
+    sizes = synthetic.batched_sizes(world * NSYS, seed=seed)
+    idx = _shard(sizes, world, rank)
+    return [synthetic.make_molecule(synthetic._seed(seed, int(k)), int(sizes[k]), noise=0.1,
+                                    name=f"S{k}") for k in idx]
 
 
-def _seed_min(rank: int) -> int:
+def minimization_molecules(world, rank):
     from stormm_b200 import synthetic
-    return synthetic.SEED_BASE + 2 + 1000 * rank
+    seed = synthetic.SEED_BASE + 2
+    sizes = np.random.default_rng(seed).integers(24, 97, size=world * MIN_NSYS)
+    idx = _shard(sizes, world, rank)
+    return [synthetic.make_molecule(synthetic._seed(seed, int(k)), int(sizes[k]), noise=0.3,
+                                    name=f"N{k}") for k in idx]
 
 
-def _sample_seeds(seed: int, sizes, count: int, noise: float):
+def large_molecules(world, rank):
     from stormm_b200 import synthetic
-    return [(synthetic._seed(seed, k), int(sizes[k]), noise) for k in range(count)]
+    seed = synthetic.SEED_BASE + 4
+    sizes = np.random.default_rng(seed).integers(2000, 5001, size=world * LARGE_NSYS)
+    idx = _shard(sizes, world, rank)
+    return [synthetic.make_chain(synthetic._seed(seed, int(k)), int(sizes[k]), name=f"C{k}")
+            for k in idx]
 
 
-def _cpu_single_point(seconds: float):
-    """STORMM's CPU evaluator on this host's cores over the first 256 molecules."""
-    import oracle.cpu_baseline as cpub
-    from stormm_b200 import synthetic
-    seed = _seed_single(0)
-    sizes = synthetic.batched_sizes(NSYS, seed=seed)
-    n = 256
-    seeds = _sample_seeds(seed, sizes, n, 0.1)
-    mols = [synthetic.make_molecule(s, k, noise=z) for (s, k, z) in seeds]
-    r = cpub.run(mols, seconds=seconds, molecule_seeds=seeds)
-    r["sample"] = (f"first {n} molecules of the workload, {seconds:.0f} s, one single-threaded "
-                   f"FP64 process per core")
-    return r
-
-
-def _cpu_minimization(seconds: float):
-    """STORMM's CPU minimizer on this host's cores over the first 128 molecules."""
-    import oracle.cpu_baseline as cpub
-    from stormm_b200 import synthetic
-    seed = _seed_min(0)
-    sizes = np.random.default_rng(seed).integers(24, 97, size=MIN_NSYS)
-    n = 128
-    seeds = _sample_seeds(seed, sizes, n, 0.3)
-    mols = [synthetic.make_molecule(s, k, noise=z) for (s, k, z) in seeds]
-    r = cpub.run(mols, seconds=seconds, minimize_cycles=MIN_CYCLES, molecule_seeds=seeds,
-                 sd_cycles=MIN_SD_CYCLES)
-    r["sample"] = (f"first {n} molecules of the workload, {MIN_CYCLES} cycles each, "
-                   f"{seconds:.0f} s, one single-threaded FP64 process per core")
-    return r
-
-
+# ------------------------------------------------------------------------------------------------
+# Reference arm: STORMM's own CPU build on this host's cores
+# ------------------------------------------------------------------------------------------------
 def run_reference(args):
-    """Reference arm: STORMM's own CPU code on this host's cores, same metric and workloads."""
+    """STORMM's own CPU code (oracle/_ref, built from the reference sources) on this host's
+    cores over prebuilt Amber inputs of the workload's leading molecules."""
     world, rank, _ = _dist()
     if rank != 0:
         return
+    import oracle.cpu_baseline as cpub
     step_seconds = max(1.0, min(4.0, 60.0 / max(1, args.steps + args.warmup)))
     values = []
     info = None
     for s in range(args.warmup + args.steps):
-        info = _cpu_single_point(step_seconds)
+        info = cpub.run_sample("single_point", step_seconds)
         if s >= args.warmup:
             values.append(info["value"])
     value = float(np.mean(values))
-    ms = float(NSYS / value * 1000.0)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "force-evals/s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded), first 256 molecules of the workload as the bounded sample",
-        "config": {"workload": WORKLOAD, "molecules": NSYS, "atoms": "16-256",
-                   "gb": "OBC-II", "sample_molecules": 256},
+        "n_gpus": max(world, args.gpus), "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": float(NSYS / value * 1000.0), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded), the workload's first 256 molecules as the bounded sample",
+        "config": {"workload": WORKLOAD, "molecules": NSYS, "atoms": "16-256", "gb": "OBC-II",
+                   "sample_molecules": info["molecules"], "hardware": "host CPU cores"},
         "cpu_baseline": {"value": value, "unit": "force-evals/s", "cores": info["cores"],
                          "kind": info["kind"],
-                         "sample": f"256 molecules, {step_seconds:.1f} s per step, "
-                                   f"one single-threaded FP64 process per core"},
+                         "sample": f"{info['molecules']} molecules, {step_seconds:.1f} s per "
+                                   f"step, one single-threaded FP64 process per core"},
         "e2e": {"value": value, "unit": "force-evals/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     if not args.no_minimization:
-        m = _cpu_minimization(max(4.0, args.cpu_seconds))
+        m = cpub.run_sample("minimization", max(4.0, args.cpu_seconds))
         line["minimization"] = {"value": m["value"], "unit": "minimizations/s",
-                                "workload": MIN_WORKLOAD, "cores": m["cores"],
-                                "kind": m["kind"], "sample": m["sample"]}
+                                "workload": MIN_WORKLOAD, "cores": m["cores"], "kind": m["kind"],
+                                "sample": f"{m['molecules']} molecules, {MIN_CYCLES} cycles each"}
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------------------------------------
+# Accuracy against the FP64 oracle (outside every timed region)
+# ------------------------------------------------------------------------------------------------
+def fp64_errors(mols, energies, forces, coords=None):
+    """Largest per-term energy error relative to max(|E|, 1 kcal/mol), the largest ratio of error
+    to the tests' bound (ENERGY_BOUND), and the largest force RMS relative error, over molecules
+    evaluated by the FP64 oracle at the same coordinates."""
+    import oracle
+    rel = np.zeros(len(TERMS))
+    ratio = np.zeros(len(TERMS))
+    frel = 0.0
+    fabs = 0.0
+    for k, m in enumerate(mols):
+        c = m.coords if coords is None else coords[k]
+        osys = oracle.from_molecule(m)
+        r = osys.evaluate(c)
+        rss = osys.magnitudes(c, r["radii"])
+        err = np.abs(np.asarray(energies[k]) - r["energies"])
+        scale = np.maximum(np.abs(r["energies"]), 1.0)
+        rel = np.maximum(rel, err / scale)
+        ratio = np.maximum(ratio, err / (1e-6 * np.maximum(scale, rss)))
+        f = np.asarray(forces[k])
+        frel = max(frel, float(np.sqrt(((f - r["forces"]) ** 2).sum() /
+                                       (r["forces"] ** 2).sum())))
+        fabs = max(fabs, float(np.sqrt(((f - r["forces"]) ** 2).mean())))
+    return {"molecules": len(mols), "bound": ENERGY_BOUND,
+            "bound_ratio_max": float(ratio.max()),
+            "energy_rel_max": {t: float(v) for t, v in zip(TERMS, rel)},
+            "force_rms_rel_max": frel, "force_rms_abs_max_kcal_mol_A": fabs}
+
+
+# ------------------------------------------------------------------------------------------------
+# GPU legs
+# ------------------------------------------------------------------------------------------------
 def _event_pair():
     import torch
     return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -228,9 +266,9 @@ def _barrier(world: int):
 def bench_single_point(args, world, rank, local, flush):
     import torch
     import stormm_b200 as sb
-    from stormm_b200 import roofline, synthetic
+    from stormm_b200 import roofline
 
-    mols = synthetic.workload_batched_single_point(NSYS, seed=_seed_single(rank))
+    mols = single_point_molecules(world, rank)
     natoms = np.array([m.natom for m in mols])
     syn = sb.Synthesis(mols, device=local)
     xyz = np.concatenate([m.coords for m in mols])
@@ -264,13 +302,16 @@ def bench_single_point(args, world, rank, local, flush):
     kern_ms = np.array([s.elapsed_time(e) for s, e in zip(kbeg, ends)])
     total_ms = _max_over_ranks(float(step_ms.sum()), world)
     value = world * NSYS * args.steps / (total_ms / 1000.0)
+    errors = None
+    if rank == 0 and not args.no_errors:
+        errors = fp64_errors(mols, syn.energy_terms(), syn.split(syn.forces()))
 
     # end to end through the C ABI with host buffers: upload coordinates, evaluate, read back
-    # forces and energies every step
-    # (pinned host buffers, allocated once and reused, as a serving loop would)
+    # forces and energies every step (pinned host buffers, allocated once and reused, as a
+    # serving loop would)
     pinned_xyz = torch.from_numpy(xyz.copy()).pin_memory().numpy()
     pinned_f = torch.zeros(xyz.size, dtype=torch.float64).pin_memory().numpy()
-    pinned_e = torch.zeros(NSYS * sb.NRG_STRIDE, dtype=torch.float64).pin_memory().numpy()
+    pinned_e = torch.zeros(len(mols) * sb.NRG_STRIDE, dtype=torch.float64).pin_memory().numpy()
     for _ in range(2):
         syn.set_coordinates(pinned_xyz)
         step()
@@ -294,36 +335,36 @@ def bench_single_point(args, world, rank, local, flush):
     # per-system drop-in: one launch per molecule (same kernel, one molecule each)
     per_sys = None
     if rank == 0:
+        n = len(mols)
         syn.initialize()
-        syn.evaluate_range(0, NSYS)
+        syn.evaluate_range(0, n)
         torch.cuda.synchronize()
         ev0, ev1 = _event_pair()
         reps = 3
         ev0.record()
         for _ in range(reps):
             syn.initialize(sb.INIT_FORCES | sb.INIT_ENERGIES)
-            syn.evaluate_range(0, NSYS)
+            syn.evaluate_range(0, n)
         ev1.record()
         torch.cuda.synchronize()
-        per_sys = NSYS * reps / (ev0.elapsed_time(ev1) / 1000.0)
+        per_sys = n * reps / (ev0.elapsed_time(ev1) / 1000.0)
     syn.close()
 
     flops = roofline.flops_per_evaluation(natoms, force=True)
-    kern_avg_s = float(kern_ms.mean()) / 1000.0
     return {
         "value": value, "total_ms": total_ms, "step_ms": step_ms, "natoms": natoms,
         "info": info, "per_sys": per_sys, "e2e_value": e2e_value, "lat": lat,
         "h2d": int(xyz.size * 8), "d2h": int(f.size * 8 + e.size * 8),
-        "flops": flops, "kern_avg_s": kern_avg_s,
+        "flops": flops, "kern_avg_s": float(kern_ms.mean()) / 1000.0, "errors": errors,
     }
 
 
 def bench_minimization(args, world, rank, local, flush):
     import torch
+    import oracle
     import stormm_b200 as sb
-    from stormm_b200 import synthetic
 
-    mols = synthetic.workload_minimization(MIN_NSYS, seed=_seed_min(rank))
+    mols = minimization_molecules(world, rank)
     syn = sb.Synthesis(mols, device=local)
     xyz = np.concatenate([m.coords for m in mols])
     ctl = dict(total_cycles=MIN_CYCLES, sd_cycles=MIN_SD_CYCLES, kernel=sb.MIN_GRAPH)
@@ -349,12 +390,32 @@ def bench_minimization(args, world, rank, local, flush):
     _barrier(world)
     total_ms = _max_over_ranks(float(np.sum(times)), world)
     value = world * MIN_NSYS * args.min_steps / (total_ms / 1000.0)
-    e_final = syn.energy_terms().sum(axis=1)
-    e_start = None
+    e_final_terms = syn.energy_terms()
+    e_final = e_final_terms.sum(axis=1)
+    errors = None
+    if rank == 0 and not args.no_errors:
+        # accuracy at the minimized coordinates: an untimed force + energy evaluation there
+        # against the oracle, and the trajectory of the first 8 molecules against the oracle's
+        # restatement of STORMM's GPU line search over all 500 cycles
+        final_xyz = syn.split(syn.coordinates())
+        syn.initialize()
+        syn.evaluate()
+        errors = fp64_errors(mols, syn.energy_terms(), syn.split(syn.forces()), final_xyz)
+        errors["note"] = ("at minimized coordinates the forces approach zero, so their relative "
+                          "error is large by construction; the absolute RMS error is the measure")
+        traj = []
+        for k in range(8):
+            _, hist = oracle.from_molecule(mols[k]).minimize(mols[k].coords, MIN_CYCLES,
+                                                             MIN_SD_CYCLES)
+            drop = hist[0] - hist[-1]
+            traj.append(abs(e_final[k] - hist[-1]) / max(abs(drop), 1e-12))
+        errors["final_energy_vs_oracle_trajectory"] = {
+            "molecules": 8, "max_abs_diff_over_energy_drop": float(np.max(traj)),
+            "median": float(np.median(traj))}
     # end to end: pinned host coordinates in, minimize, coordinates and energies out
     pinned_xyz = torch.from_numpy(xyz.copy()).pin_memory().numpy()
     pinned_c = torch.zeros(xyz.size, dtype=torch.float64).pin_memory().numpy()
-    pinned_e = torch.zeros(MIN_NSYS * sb.NRG_STRIDE, dtype=torch.float64).pin_memory().numpy()
+    pinned_e = torch.zeros(len(mols) * sb.NRG_STRIDE, dtype=torch.float64).pin_memory().numpy()
     torch.cuda.synchronize()
     _barrier(world)
     t0 = time.perf_counter()
@@ -363,8 +424,9 @@ def bench_minimization(args, world, rank, local, flush):
     c = syn.coordinates(out=pinned_c)
     e = syn.energies(out=pinned_e)
     e2e_s = _max_over_ranks(time.perf_counter() - t0, world)
-    # per-system drop-in: one launch per molecule for the first 16 molecules
+    # per-system drop-in: one launch sequence per molecule for the first 16 molecules
     per_sys = None
+    e_start = None
     if rank == 0:
         syn.set_coordinates(xyz)
         ev0, ev1 = _event_pair()
@@ -386,33 +448,12 @@ def bench_minimization(args, world, rank, local, flush):
     syn.minimize(total_cycles=MIN_CYCLES, sd_cycles=MIN_SD_CYCLES, kernel=sb.MIN_PERSISTENT)
     ev1.record()
     torch.cuda.synchronize()
-    persistent = MIN_NSYS / (ev0.elapsed_time(ev1) / 1000.0)
+    persistent = len(mols) / (ev0.elapsed_time(ev1) / 1000.0)
     assert syn.status() == 0
     syn.close()
-    # FP64 mode (PrecisionModel::DOUBLE) on the first 256 molecules, one timed run after a short
-    # warm-up, and its final energies against the FP32 graph minimizer's
-    n64 = 256
-    m64 = mols[:n64]
-    x64 = np.concatenate([m.coords for m in m64])
-    s64 = sb.Synthesis(m64, device=local, precision=sb.PRECISION_DOUBLE)
-    s64.set_coordinates(x64)
-    s64.minimize(total_cycles=5, sd_cycles=2, kernel=sb.MIN_GRAPH)
-    s64.set_coordinates(x64)
-    torch.cuda.synchronize()
-    ev0, ev1 = _event_pair()
-    ev0.record()
-    s64.minimize(total_cycles=MIN_CYCLES, sd_cycles=MIN_SD_CYCLES, kernel=sb.MIN_GRAPH)
-    ev1.record()
-    torch.cuda.synchronize()
-    fp64_value = n64 / (ev0.elapsed_time(ev1) / 1000.0)
-    e64 = s64.energy_terms().sum(axis=1)
-    assert s64.status() == 0
-    s64.close()
-    fp64_mode = {"value": fp64_value, "unit": "minimizations/s", "molecules": n64,
-                 "cycles": MIN_CYCLES,
-                 "fp32_final_energy_rel_vs_fp64_median": float(np.median(
-                     np.abs(e_final[:n64] - e64) / np.maximum(np.abs(e64), 1.0))),
-                 "note": "graph minimizer over the FP64 evaluations, conjugate direction in FP64"}
+    fp64_mode = None
+    if rank == 0:
+        fp64_mode = _minimization_fp64(mols[:256], e_final[:256], local)
     evals = MIN_NSYS * (4 * MIN_CYCLES + 1)
     return {
         "value": value, "unit": "minimizations/s", "workload": MIN_WORKLOAD,
@@ -422,8 +463,8 @@ def bench_minimization(args, world, rank, local, flush):
         "evals_per_s": world * evals * args.min_steps / (total_ms / 1000.0),
         "evals_per_minimization": 4 * MIN_CYCLES + 1,
         "per_system_dropin": {"value": per_sys, "unit": "minimizations/s",
-                              "sample": "first 16 molecules, one launch each",
-                              "batched_speedup": (value / world / per_sys) if per_sys else None},
+                              "sample": "first 16 molecules, one launch sequence each"},
+        "batched_speedup": (value / world / per_sys) if per_sys else None,
         "e2e": {"value": world * MIN_NSYS / e2e_s, "unit": "minimizations/s",
                 "h2d_bytes_per_step": int(xyz.size * 8),
                 "d2h_bytes_per_step": int(c.size * 8 + e.size * 8)},
@@ -433,31 +474,45 @@ def bench_minimization(args, world, rank, local, flush):
         "fp64_mode": fp64_mode,
         "gpu_launches_per_step": 1 + 8 * MIN_CYCLES + 2,
         "unit_packing": {"atoms_per_unit": tuned[0], "tiles_per_unit": tuned[1],
-                         "chosen_by": "sb_autotune of the evaluation over the fixed and wave-sized packings"},
+                         "chosen_by": "sb_autotune of the evaluation"},
         "l2": "flushed (256 MB write) before every timed step",
+        "errors": errors,
     }
 
 
-def _cpu_large(seconds: float):
-    """STORMM's CPU evaluator on this host's cores over the first 32 chains."""
-    import oracle.cpu_baseline as cpub
-    from stormm_b200 import synthetic
-    seed = synthetic.SEED_BASE + 4
-    sizes = np.random.default_rng(seed).integers(2000, 5001, size=LARGE_NSYS)
-    n = 32
-    mols = [synthetic.make_chain(synthetic._seed(seed, k), int(sizes[k])) for k in range(n)]
-    r = cpub.run(mols, seconds=seconds)
-    r["sample"] = (f"first {n} chains of the workload, {seconds:.0f} s, one single-threaded FP64 "
-                   f"process per core")
-    return r
+def _minimization_fp64(mols, e_fp32_final, local):
+    """The FP64 mode (PrecisionModel::DOUBLE) on the first 256 molecules: one timed run after a
+    short warm-up, and the FP32 path's final energies against its own."""
+    import torch
+    import stormm_b200 as sb
+    x64 = np.concatenate([m.coords for m in mols])
+    s64 = sb.Synthesis(mols, device=local, precision=sb.PRECISION_DOUBLE)
+    s64.set_coordinates(x64)
+    s64.minimize(total_cycles=5, sd_cycles=2, kernel=sb.MIN_GRAPH)
+    s64.set_coordinates(x64)
+    torch.cuda.synchronize()
+    ev0, ev1 = _event_pair()
+    ev0.record()
+    s64.minimize(total_cycles=MIN_CYCLES, sd_cycles=MIN_SD_CYCLES, kernel=sb.MIN_GRAPH)
+    ev1.record()
+    torch.cuda.synchronize()
+    value = len(mols) / (ev0.elapsed_time(ev1) / 1000.0)
+    e64 = s64.energy_terms().sum(axis=1)
+    assert s64.status() == 0
+    s64.close()
+    return {"value": value, "unit": "minimizations/s", "molecules": len(mols),
+            "cycles": MIN_CYCLES,
+            "fp32_final_energy_rel_vs_fp64_median": float(np.median(
+                np.abs(e_fp32_final - e64) / np.maximum(np.abs(e64), 1.0))),
+            "note": "graph minimizer over the FP64 evaluations, conjugate direction in FP64"}
 
 
 def bench_large(args, world, rank, local, flush):
-    """Config of 256 chains of 2,000-5,000 atoms through the tiled path."""
+    """256 chains of 2,000-5,000 atoms through the tiled path."""
     import torch
     import stormm_b200 as sb
-    from stormm_b200 import roofline, synthetic
-    mols = synthetic.workload_chains(LARGE_NSYS, seed=synthetic.SEED_BASE + 4 + 1000 * rank)
+    from stormm_b200 import roofline
+    mols = large_molecules(world, rank)
     natoms = np.array([m.natom for m in mols])
     syn = sb.Synthesis(mols, device=local)
     syn.set_coordinates(np.concatenate([m.coords for m in mols]))
@@ -481,10 +536,9 @@ def bench_large(args, world, rank, local, flush):
     total_ms = _max_over_ranks(float(np.sum(times)), world)
     value = world * LARGE_NSYS * len(times) / (total_ms / 1000.0)
     fp64 = None
-    if rank == 0:
-        fp64 = _large_fp64(mols, local, syn.forces(), syn.energy_terms(), flush)
     per_sys = None
     if rank == 0:
+        fp64 = _large_fp64(mols, local, syn.forces(), syn.energy_terms(), flush)
         ev0, ev1 = _event_pair()
         ev0.record()
         syn.initialize(sb.INIT_FORCES | sb.INIT_ENERGIES)
@@ -496,23 +550,22 @@ def bench_large(args, world, rank, local, flush):
     flops = roofline.flops_per_evaluation(natoms, force=True)
     achieved = flops / (float(np.mean(times)) / 1000.0) / 1.0e12
     peak = roofline.fp32_peak_tflops(1965.0)
-    out = {"workload": LARGE_WORKLOAD, "value": value, "unit": "force-evals/s",
-           "molecules_per_gpu": LARGE_NSYS, "atoms_total_per_gpu": int(natoms.sum()),
-           "pairs_per_pass": roofline.pair_count(natoms), "steps": len(times),
-           "ms_per_step": total_ms / len(times),
-           "p50_ms": float(np.percentile(times, 50)), "p99_ms": float(np.percentile(times, 99)),
-           "per_system_dropin": {"value": per_sys, "unit": "force-evals/s",
-                                 "sample": "first 16 chains, one launch sequence each"},
-           "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                        "frac": achieved / peak, "flops_per_step": flops},
-           "l2": "flushed (256 MB write) before every timed step",
-           "fp64_gpu_mode": fp64}
-    return out
+    return {"workload": LARGE_WORKLOAD, "value": value, "unit": "force-evals/s",
+            "molecules_per_gpu": LARGE_NSYS, "atoms_total_per_gpu": int(natoms.sum()),
+            "pairs_per_pass": roofline.pair_count(natoms), "steps": len(times),
+            "ms_per_step": total_ms / len(times),
+            "p50_ms": float(np.percentile(times, 50)), "p99_ms": float(np.percentile(times, 99)),
+            "per_system_dropin": {"value": per_sys, "unit": "force-evals/s",
+                                  "sample": "first 16 chains, one launch sequence each"},
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "flops_per_step": flops},
+            "l2": "flushed (256 MB write) before every timed step",
+            "fp64_gpu_mode": fp64}
 
 
 def _large_fp64(mols, local, f32, e32, flush, steps=3):
-    """The same chains in the FP64-arithmetic mode (precision = SB_PRECISION_DOUBLE): its
-    throughput on one GPU, and how far the FP32 path's forces and energies lie from it."""
+    """The same chains in the FP64-arithmetic mode: its throughput on one GPU, and how far the
+    FP32 path's forces and energies lie from it."""
     import torch
     import stormm_b200 as sb
     syn = sb.Synthesis(mols, device=local, precision=sb.PRECISION_DOUBLE)
@@ -535,15 +588,11 @@ def _large_fp64(mols, local, f32, e32, flush, steps=3):
     e64 = syn.energy_terms()
     syn.close()
     frel = float(np.sqrt(((f32 - f64) ** 2).sum() / (f64 ** 2).sum()))
-    escale = np.maximum(np.abs(e64).sum(axis=1), 10.0)
-    erel = float(np.max(np.abs(e32.sum(axis=1) - e64.sum(axis=1)) / escale))
+    rel = np.max(np.abs(e32 - e64) / np.maximum(np.abs(e64), 1.0), axis=0)
     return {"value": len(mols) * steps / (float(np.sum(times)) / 1000.0),
             "unit": "force-evals/s", "steps": steps, "ms_per_step": float(np.mean(times)),
             "n_gpus": 1, "fp32_force_rms_rel_vs_fp64": frel,
-            "fp32_energy_rel_vs_fp64_max": erel,
-            "note": "FP64 arithmetic from double parameters, every chain tile by tile, integer "
-                    "accumulation; matches STORMM's FP64 CPU results to 1e-10 "
-                    "(tests/test_gpu_fp64.py)"}
+            "fp32_energy_rel_vs_fp64_max": {t: float(v) for t, v in zip(TERMS, rel)}}
 
 
 def bench_served(local):
@@ -575,7 +624,8 @@ def bench_served(local):
         sweeps.append({
             "offered_per_s": rate, "requests": len(arrivals), "completed": len(res),
             "drained": bool(drained),
-            "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+            "p50_ms": float(np.percentile(lat, 50) * 1e3),
+            "p99_ms": float(np.percentile(lat, 99) * 1e3),
             "admission_wait_p50_ms": float(np.percentile(wait, 50) * 1e3),
             "throughput_per_s": len(res) / (last - first),
             "mean_cycles": float(np.mean([r["cycles"] for r in res])),
@@ -609,18 +659,28 @@ def bench_served(local):
             "sweep": sweeps, "mixed_with_evaluations": mixed}
 
 
-def main():
-    args = _args()
-    if args.impl == "reference":
-        run_reference(args)
-        return
+def _cpu_leg(name, seconds):
+    """STORMM's CPU build on this host's cores over the named sample (oracle.cpu_baseline)."""
+    import oracle.cpu_baseline as cpub
+    try:
+        r = cpub.run_sample(name, seconds)
+        return {"value": r["value"], "unit": r["unit"], "cores": r["cores"], "kind": r["kind"],
+                "sample": f"the workload's first {r['molecules']} molecules, {seconds:.0f} s, "
+                          f"one single-threaded FP64 process per core"}
+    except Exception as exc:  # reported, not fatal
+        return {"value": None, "unit": None, "cores": 0, "kind": "unavailable",
+                "sample": str(exc)[:200]}
+
+
+def main_rank(args):
     world, rank, local = _dist()
     import torch
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
     from stormm_b200 import roofline
 
     # L2 flush buffer (> 126 MB L2), written between timed steps outside the timed events
@@ -637,31 +697,18 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        try:
-            r = _cpu_single_point(args.cpu_seconds)
-            cpu = {"value": r["value"], "unit": "force-evals/s", "cores": r["cores"],
-                   "kind": r["kind"], "sample": r["sample"]}
-            if mn is not None:
-                rm = _cpu_minimization(args.cpu_seconds)
-                mn["cpu_baseline"] = {"value": rm["value"], "unit": "minimizations/s",
-                                      "cores": rm["cores"], "kind": rm["kind"],
-                                      "sample": rm["sample"]}
-            if large is not None:
-                try:
-                    rl = _cpu_large(args.cpu_seconds)
-                    large["cpu_baseline"] = {"value": rl["value"], "unit": "force-evals/s",
-                                             "cores": rl["cores"], "kind": rl["kind"],
-                                             "sample": rl["sample"]}
-                except Exception as exc:  # reported, not fatal
-                    large["cpu_baseline"] = {"value": None, "kind": "unavailable",
-                                             "sample": str(exc)[:200]}
-        except Exception as exc:  # reported, not fatal
-            cpu = {"value": None, "unit": "force-evals/s", "cores": 0, "kind": "unavailable",
-                   "sample": str(exc)[:200]}
+        cpu = _cpu_leg("single_point", args.cpu_seconds)
+        if mn is not None:
+            mn["cpu_baseline"] = _cpu_leg("minimization", args.cpu_seconds)
+        if large is not None:
+            large["cpu_baseline"] = _cpu_leg("large", args.cpu_seconds)
 
     if rank == 0:
         info = sp["info"]
         natoms = sp["natoms"]
+        detail = {"detail": "bench legs in full (the summary line follows)",
+                  "minimization": mn, "served": served, "large": large}
+        print(json.dumps(detail, default=float), flush=True)
         line = {
             "metric": METRIC, "value": sp["value"], "unit": "force-evals/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
@@ -670,15 +717,15 @@ def main():
             "dtype": "f32 (int64 fixed-point accumulation)",
             "data": "synthetic (seeded generator, no dataset)",
             "config": {"workload": WORKLOAD, "molecules_per_gpu": NSYS,
-                       "atoms_total_per_gpu": int(natoms.sum()),
-                       "pairs_per_pass": roofline.pair_count(natoms), "gb": "OBC-II",
-                       "dielectric": 80.0, "parallelism": f"weak x{world} (independent shards)",
+                       "atoms_per_gpu_rank0": int(natoms.sum()),
+                       "pairs_per_pass_rank0": roofline.pair_count(natoms), "gb": "OBC-II",
+                       "parallelism": (f"{world} ranks, LPT shards of one {world * NSYS}-molecule "
+                                       f"workload" if world > 1 else "one GPU"),
                        "l2": "flushed (256 MB write) before every timed step",
                        "work_units": info["work_units"], "threads_per_block": info["threads"]},
             "p50_ms": float(np.percentile(sp["step_ms"], 50)),
             "p99_ms": float(np.percentile(sp["step_ms"], 99)),
             "per_system_dropin": {"value": sp["per_sys"], "unit": "force-evals/s",
-                                  "launches_per_step": NSYS,
                                   "batched_speedup": (sp["value"] / world / sp["per_sys"])
                                   if sp["per_sys"] else None},
             "e2e": {"value": sp["e2e_value"], "unit": "force-evals/s",
@@ -692,15 +739,38 @@ def main():
                          "kernel_ms": sp["kern_avg_s"] * 1000.0,
                          "peak_source": "nominal FP32 FMA pipe: 148 SM x 128 lanes x 2 x "
                                         "1965 MHz (no measured FP32 figure on this pool)"},
+            "errors_vs_fp64": sp["errors"],
             "clocks": csum,
             "cpu_baseline": cpu,
-            "minimization": mn,
-            "served": served,
-            "large": large,
         }
-        print(json.dumps(line), flush=True)
+        if mn is not None:
+            line["minimization"] = {
+                "value": mn["value"], "unit": "minimizations/s", "workload": MIN_WORKLOAD,
+                "evals_per_s": mn["evals_per_s"],
+                "per_system_dropin": mn["per_system_dropin"]["value"],
+                "batched_speedup": mn["batched_speedup"],
+                "errors_vs_fp64": mn["errors"],
+                "cpu_baseline": (mn.get("cpu_baseline") or {}).get("value")}
+        print(json.dumps(line, default=float), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+def _rank_main(args):
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        main_rank(args)
+
+
+def main():
+    args = _args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU without torchrun
+        from stormm_b200 import sharding
+        sharding.spawn_ranks(_rank_main, args.gpus, args)
+        return
+    _rank_main(args)
 
 
 if __name__ == "__main__":

@@ -1,9 +1,9 @@
 """Small, fixed profiling cases for the evaluation and minimization kernels.
 
-  python -m stormm_b200.profile_case [--molecules 256] [--evals 4] [--energy-only]
-  python -m stormm_b200.profile_case --workload minimization --molecules 4096 --minimize 20
-  python -m stormm_b200.profile_case --workload chains --molecules 16 --evals 3
-  python -m stormm_b200.profile_case --workload chains --molecules 16 --evals 3 --precision double
+  python profile_case.py [--molecules 256] [--evals 4] [--energy-only]
+  python profile_case.py --workload minimization --molecules 4096 --minimize 20
+  python profile_case.py --workload chains --molecules 16 --evals 3
+  python profile_case.py --workload chains --molecules 16 --evals 3 --precision double
 
 The first form builds the first molecules of the batched single-point workload (16-256 atoms),
 uploads them and runs a few force + energy evaluations; the second builds the first molecules

@@ -111,8 +111,7 @@ cudaError_t launchEvalFused(const DevSynthesis &d, int unit_begin, int unit_end,
                                 kEvalFused<F, E, T, false, ((T) & 4) != 0>) :                   \
                        (clash ? kEvalFused<F, E, T, ((T) & 3) != 0, false> :                    \
                                 kEvalFused<F, E, T, false, false>);                             \
-    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
-                                           static_cast<int>(smem));                             \
+    const cudaError_t err = allowLargeSmem(kern);                                               \
     if (err != cudaSuccess) return err;                                                         \
     kern<<<blocks, threads, smem, stream>>>(d, unit_begin, unit_end, max_lj);                   \
     return cudaGetLastError();                                                                  \

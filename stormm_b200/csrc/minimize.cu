@@ -464,8 +464,7 @@ cudaError_t launchMinimize(const DevSynthesis &d, const DevMinimizer &m, int uni
                   (clash ? kMinimize<H, true, false> : kMinimize<H, false, false>);
   };
   auto kern = (m.history != nullptr) ? pick(std::true_type()) : pick(std::false_type());
-  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
+  cudaError_t err = allowLargeSmem(kern);
   if (err != cudaSuccess) return err;
   int per_sm = 0;
   err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);

@@ -33,6 +33,10 @@
 
 #include <cuda_runtime.h>
 
+#include <mutex>
+#include <set>
+#include <utility>
+
 #include "device_kits.h"
 #include "fixed_point.cuh"
 
@@ -423,6 +427,37 @@ struct UnitSmem {
 
 __host__ __device__ inline size_t alignUp(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+// Raise a kernel's dynamic shared-memory limit to the device's opt-in maximum, once per kernel and
+// device (the attribute belongs to the function on the current device); launches then pass only
+// their own size, and the per-system drop-in, a launch per molecule, pays no attribute call
+template <class K>
+cudaError_t allowLargeSmem(K kern) {
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  int dev = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err != cudaSuccess) return err;
+  std::lock_guard<std::mutex> lock(mu);
+  const auto key = std::make_pair(reinterpret_cast<const void*>(kern), dev);
+  if (done.count(key) != 0) return cudaSuccess;
+  int optin = 0;
+  err = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (err != cudaSuccess) return err;
+  // static and dynamic shared memory together may not exceed the opt-in maximum
+  cudaFuncAttributes attr;
+  err = cudaFuncGetAttributes(&attr, kern);
+  if (err != cudaSuccess) return err;
+  err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             optin - static_cast<int>(attr.sharedSizeBytes));
+  if (err == cudaSuccess) {
+    done.insert(key);
+  }
+  else {
+    cudaGetLastError();   // reported here, not left for the next launch check to find
+  }
+  return err;
+}
+
 constexpr int kSlotBytes = 3 * 16 + 8 + 11 * 4;
 
 // Dynamic shared memory of one work unit's evaluation: max_slots atom slots, max_lj table entries
@@ -699,17 +734,23 @@ __device__ void valenceTerms(const DevSynthesis &d, const V &v, int nsys_u) {
       const double3 pj = v.pos64(ja);
       const double3 ba = sub3d(v.pos64(ia), pj);
       const double3 bc = sub3d(v.pos64(ka), pj);
+      // reciprocal square roots instead of divisions and square roots (FP64 divisions are long
+      // instruction sequences): 1 / sin(theta) = |ba| |bc| / |ba x bc|
       const double mgba = dot3d(ba, ba);
       const double mgbc = dot3d(bc, bc);
-      const double invbabc = rsqrt(mgba * mgbc);
+      const double inv_ba = rsqrt(mgba);
+      const double inv_bc = rsqrt(mgbc);
+      const double invbabc = inv_ba * inv_bc;
       const double3 cr = cross3d(ba, bc);
-      const double sth = sqrt(dot3d(cr, cr)) * invbabc;
+      const double cr2 = dot3d(cr, cr);
+      const double inv_cr = rsqrt(cr2);
+      const double sth = cr2 * inv_cr * invbabc;
       const double cth = dot3d(ba, bc) * invbabc;
       const double dtheta = atan2(fma(sth, prm.y, -cth * prm.z), fma(cth, prm.y, sth * prm.z));
       if (FORCE) {
-        const double dA = -2.0 * prm.x * dtheta / sth;
-        const double sqba = dA / mgba;
-        const double sqbc = dA / mgbc;
+        const double dA = -2.0 * prm.x * dtheta * inv_cr * ((mgba * inv_ba) * (mgbc * inv_bc));
+        const double sqba = dA * inv_ba * inv_ba;
+        const double sqbc = dA * inv_bc * inv_bc;
         const double mbabc = dA * invbabc;
         const double adx = bc.x * mbabc - cth * ba.x * sqba;
         const double ady = bc.y * mbabc - cth * ba.y * sqba;
@@ -761,7 +802,9 @@ __device__ void valenceTerms(const DevSynthesis &d, const V &v, int nsys_u) {
       const double3 cd = sub3d(pl, pk);
       double3 crabbc = cross3d(ab, bc);
       double3 crbccd = cross3d(bc, cd);
-      const double mgbc = sqrt(dot3d(bc, bc));
+      const double bc2 = dot3d(bc, bc);
+      const double invbc = rsqrt(bc2);
+      const double mgbc = bc2 * invbc;
       const double xx = dot3d(crabbc, crbccd);
       const double yy = mgbc * dot3d(ab, crbccd);
       const double inv_rr = rsqrt(fma(xx, xx, yy * yy));
@@ -786,17 +829,17 @@ __device__ void valenceTerms(const DevSynthesis &d, const V &v, int nsys_u) {
       const double sin_sangle = sn * prm.y - cn * prm.z;
       if (FORCE) {
         const double fr = prm.x * freq * sin_sangle;
-        const double mgab = sqrt(dot3d(ab, ab));
-        const double mgcd = sqrt(dot3d(cd, cd));
-        const double invab = 1.0 / mgab;
-        const double invbc = 1.0 / mgbc;
-        const double invcd = 1.0 / mgcd;
+        const double ab2 = dot3d(ab, ab);
+        const double cd2 = dot3d(cd, cd);
+        const double invab = rsqrt(ab2);
+        const double invcd = rsqrt(cd2);
+        const double mgab = ab2 * invab;
         const double cosb = -dot3d(ab, bc) * invab * invbc;
         const double cosc = -dot3d(bc, cd) * invbc * invcd;
-        const double isinb2 = (cosb * cosb < kAsymptoticToOne) ? fr / (1.0 - cosb * cosb) :
-                                                                  fr * kInvOneMinusAsymptote;
-        const double isinc2 = (cosc * cosc < kAsymptoticToOne) ? fr / (1.0 - cosc * cosc) :
-                                                                  fr * kInvOneMinusAsymptote;
+        const double isinb2 = (cosb * cosb < kAsymptoticToOne) ?
+                              fr * __drcp_rn(1.0 - cosb * cosb) : fr * kInvOneMinusAsymptote;
+        const double isinc2 = (cosc * cosc < kAsymptoticToOne) ?
+                              fr * __drcp_rn(1.0 - cosc * cosc) : fr * kInvOneMinusAsymptote;
         const double invabc = invab * invbc;
         const double invbcd = invbc * invcd;
         crabbc = make_double3(crabbc.x * invabc, crabbc.y * invabc, crabbc.z * invabc);
@@ -834,8 +877,8 @@ __device__ void valenceTerms(const DevSynthesis &d, const V &v, int nsys_u) {
         const double lja = ab14.x * att.y;
         const double ljb = ab14.y * att.y;
         const double qiqj = d.charge64[gi] * d.charge64[gl] * att.x;
-        const double invr2 = 1.0 / dot3d(dv, dv);
-        const double invr = sqrt(invr2);
+        const double invr = rsqrt(dot3d(dv, dv));
+        const double invr2 = invr * invr;
         const double invr6 = invr2 * invr2 * invr2;
         const float2 cl = CLASH ? v.clash(k) : make_float2(0.0f, 0.0f);
         if (CLASH && (cl.x > 0.0f || cl.y > 0.0f)) {

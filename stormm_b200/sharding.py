@@ -9,10 +9,14 @@ time (throughput = units on all ranks / slowest rank's time).
   ranks, balancing the pair count N(N-1)/2 that dominates the work.
 * ``max_over_ranks`` / ``sum_over_ranks``: the timing reductions, over whatever process group
   torch.distributed was initialised with (NCCL on GPUs; gloo works on CPU for tests).
+* ``spawn_ranks``: one process per rank without torchrun, with the rendezvous environment
+  (RANK, LOCAL_RANK, WORLD_SIZE, MASTER_ADDR = 127.0.0.1, a free MASTER_PORT) set in each.
 """
 from __future__ import annotations
 
 import heapq
+import os
+import socket
 
 import numpy as np
 
@@ -57,3 +61,24 @@ def max_over_ranks(value: float, device=None) -> float:
 def sum_over_ranks(value: float, device=None) -> float:
     import torch.distributed as dist
     return _reduce(value, dist.ReduceOp.SUM, device)
+
+
+def _free_port() -> int:
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as sock:
+        sock.bind(("127.0.0.1", 0))
+        return sock.getsockname()[1]
+
+
+def _rank_entry(rank, fn, nprocs, port, fn_args):
+    os.environ.update(RANK=str(rank), LOCAL_RANK=str(rank), WORLD_SIZE=str(nprocs),
+                      MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    fn(*fn_args)
+
+
+def spawn_ranks(fn, nprocs: int, *fn_args) -> None:
+    """Run fn(*fn_args) in nprocs spawned processes, one per rank, each with the rendezvous
+    environment torch.distributed reads; raises if any rank fails.  fn must be importable (a
+    module-level function)."""
+    import torch.multiprocessing as tmp
+    tmp.start_processes(_rank_entry, args=(fn, nprocs, _free_port(), fn_args), nprocs=nprocs,
+                        start_method="spawn", join=True)

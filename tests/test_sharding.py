@@ -63,3 +63,35 @@ def test_two_gloo_ranks_shard_and_reduce(tmp_path):
         assert float(tmax) == 2.5
         assert float(tsum) == 1024.0
         assert int(total) == 1024 and int(unique) == 1024
+
+
+def _spawned_rank_main(out_dir):
+    """Run by sharding.spawn_ranks: the bench's own shard selection on one rank, checked across
+    ranks with gloo collectives."""
+    import torch.distributed as dist
+    import bench
+    world = int(os.environ["WORLD_SIZE"])
+    rank = int(os.environ["RANK"])
+    dist.init_process_group("gloo")
+    try:
+        sizes = synthetic.batched_sizes(world * bench.NSYS, seed=synthetic.SEED_BASE + 1)
+        mine = bench._shard(sizes, world, rank)
+        gathered = [None] * world
+        dist.all_gather_object(gathered, mine.tolist())
+        t = sharding.max_over_ranks(float(rank))
+        with open(os.path.join(out_dir, f"spawn{rank}.txt"), "w") as f:
+            allidx = sorted(i for g in gathered for i in g)
+            f.write(f"{world} {t} {len(allidx)} {int(allidx == list(range(world * bench.NSYS)))}\n")
+    finally:
+        dist.destroy_process_group()
+
+
+def test_spawned_ranks_take_disjoint_lpt_shards_of_one_workload(tmp_path):
+    """bench.py --gpus N without torchrun: sharding.spawn_ranks starts one process per rank with
+    the rendezvous environment; the ranks' shards of the N x 1,024-molecule workload are
+    disjoint and cover it (two gloo ranks on CPU)."""
+    sharding.spawn_ranks(_spawned_rank_main, 2, str(tmp_path))
+    for rank in range(2):
+        world, tmax, total, covered = open(tmp_path / f"spawn{rank}.txt").read().split()
+        assert int(world) == 2 and float(tmax) == 1.0
+        assert int(total) == 2048 and int(covered) == 1
