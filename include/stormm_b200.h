@@ -272,6 +272,32 @@ int sb_minimize_range(sb_synthesis* syn, int first, int count, const sb_minimize
 int sb_minimize_begin(sb_synthesis* syn, const sb_minimize_controls* ctl, void* stream);
 int sb_minimize_advance(sb_synthesis* syn, int cycles, int final_energy, void* stream);
 
+/* The line-search steps one at a time, for a caller that runs its own evaluations in between, as
+ * STORMM's launchMinimization does with its kernels (hpc_minimization.cu:432-560).  Both need a
+ * minimization begun by sb_minimize_begin and act on every system of the synthesis.
+ *
+ * sb_conjugate_gradient replaces launchConjugateGradient (Math/hpc_reduction.h:55-63, kernels
+ * Math/conjugate_gradient.cui:8-140): from the forces and energies of a force + energy evaluation
+ * at the line start it records the energy in the history, takes gg, dgg and the RMS force per
+ * system (FP64, over 32-atom chunks in a fixed order), stops a system that met the RMS target
+ * or used up total_cycles, and sets the search direction to the forces plus gamma = dgg / gg
+ * times the previous direction (gamma = 0 for the first sd_cycles cycles).
+ *
+ * sb_line_advance replaces launchLineAdvance (MolecularMechanics/hpc_minimization.h:63-70,
+ * line_movement.cui:88-336) for move_number 0-3, after an energy evaluation at the current
+ * coordinates (move 0: the line-start evaluation itself): move 0 records the line-start energy
+ * and moves each active system along its normalized direction by its move length; moves 1 and 2
+ * read the trial energy and move on by factors of 1.04 / 0.8 and x1.03 / x0.85; move 3 reads
+ * the fourth energy, places the system at the minimum of the cubic through the four points,
+ * updates its move length and ends its cycle.
+ *
+ * Per cycle: clear forces and energies, force + energy evaluation, sb_conjugate_gradient,
+ * sb_line_advance(0), then three times: clear energies, energy evaluation, sb_line_advance(1, 2,
+ * 3).  With the evaluations of sb_evaluate this is, bit for bit, the cycle of sb_minimize with the
+ * graph kernel and no clash-damped cycles. */
+int sb_conjugate_gradient(sb_synthesis* syn, void* stream);
+int sb_line_advance(sb_synthesis* syn, int move_number, void* stream);
+
 /* Energy history of the last minimization that recorded one: nsys * (total_cycles + 1) doubles,
  * system-major.  Entry c is the energy at the start of cycle c; the entry after a system's last
  * cycle is its final energy (later entries stay 0 for a system that converged early). */

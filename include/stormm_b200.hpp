@@ -36,10 +36,11 @@
  *     or FP64 arithmetic); a launch with the other model throws.  FP64 minimization runs the
  *     graph minimizer with the direction in FP64.
  *   - The GB model, dielectric and salt concentration are one per synthesis.
- *   - MolecularMechanicsControls, CacheResource, Thermostat, ReductionBridge, LineMinimization,
- *     StopWatch and the AccumulationMethod argument are accepted and have nothing to carry: a
- *     thread block holds a whole work unit on chip, accumulation is always int64 + int32
- *     overflow, and the minimizer keeps its line-search state on the device.  CoreKlManager
+ *   - CacheResource, Thermostat, ReductionBridge, StopWatch and the AccumulationMethod argument
+ *     are accepted and have nothing to carry: a thread block holds a whole work unit on chip,
+ *     accumulation is always int64 + int32 overflow, and the minimizer keeps its line-search
+ *     state on the device.  MolecularMechanicsControls carries the minimizer's cycle counts and
+ *     move length to launchConjugateGradient; LineMinimization names the system count.  CoreKlManager
  *     carries the CUDA stream the launches go to (default stream unless set).
  *   - Streams are given as void* (cudaStream_t), so this header needs no CUDA header.
  */
@@ -133,11 +134,47 @@ private:
   int device;
 };
 
-class MolecularMechanicsControls {};                               // MolecularMechanics/mm_controls.h:100
+class MinimizeControls;
+/* MolecularMechanicsControls (MolecularMechanics/mm_controls.h:100-140): for a minimization it
+ * carries the cycle counts and the initial move length the line-search steps use
+ * (launchConjugateGradient begins the synthesis' minimizer state from them on its first call).
+ * STORMM's work-unit counters have no counterpart: a thread block holds a whole unit on chip. */
+class MolecularMechanicsControls {
+public:
+  explicit MolecularMechanicsControls(double initial_step_in = 0.01)
+      : initial_step(initial_step_in) {}
+  explicit MolecularMechanicsControls(const MinimizeControls &user_input);
+  int getTotalCycles() const { return total_cycles; }
+  int getSteepestDescentCycles() const { return sd_cycles; }
+  double getInitialStep() const { return initial_step; }
+  /* The synthesis whose minimizer these controls began (nullptr: none yet) */
+  const void* begunFor() const { return begun; }
+  void markBegun(const void* handle) { begun = handle; }
+
+private:
+  int total_cycles = 200, sd_cycles = 50;
+  double initial_step = 0.01;
+  const void* begun = nullptr;
+};
 class Thermostat {};                                               // Trajectory/thermostat.h
 class CacheResource {};                                            // Accelerator/cacheresource.h:63
-class ReductionBridge {};                                          // Math/reduction_bridge.h
-class LineMinimization {};                                         // MolecularMechanics/line_minimization.h:85
+class ReductionBridge {                                            // Math/reduction_bridge.h:24
+public:
+  explicit ReductionBridge(size_t = 0) {}
+};
+/* LineMinimization (MolecularMechanics/line_minimization.h:85-100): the per-system line-search
+ * record lives on the device with the synthesis; this object names the system count */
+class LineMinimization {
+public:
+  explicit LineMinimization(int system_count_in = 0, double dx0 = 0.0)
+      : system_count(system_count_in), initial_step(dx0) {}
+  int getSystemCount() const { return system_count; }
+  double getInitialStep() const { return initial_step; }
+
+private:
+  int system_count;
+  double initial_step;
+};
 class StopWatch {};                                                // UnitTesting/stopwatch.h
 
 /* ------------------------------------------------------------------------------------------ */
@@ -956,6 +993,11 @@ private:
   }
 };
 
+inline MolecularMechanicsControls::MolecularMechanicsControls(const MinimizeControls &user_input)
+    : total_cycles(user_input.getTotalCycles()),
+      sd_cycles(user_input.getSteepestDescentCycles()),
+      initial_step(user_input.getInitialStep()) {}
+
 /* ------------------------------------------------------------------------------------------ */
 /* Launchers                                                                                   */
 /* ------------------------------------------------------------------------------------------ */
@@ -1050,6 +1092,53 @@ inline void launchValence(PrecisionModel prec, const AtomGraphSynthesis &poly_ag
   launchValence(prec, poly_ag, mmctrl, poly_ps, heat_bath, sc, tb_space, eval_force,
                 eval_energy, purpose, AccumulationMethod::SPLIT, launcher, clash_distance,
                 clash_ratio);
+}
+
+/* launchConjugateGradient (Math/hpc_reduction.h:55-63): after a force + energy evaluation at the
+ * line start, one conjugate-gradient step of every system (sb_conjugate_gradient: gg, dgg, the
+ * steepest-descent / conjugate-gradient switch after mmctrl's steepest-descent cycles, the new
+ * search direction).  The first call with a given MolecularMechanicsControls begins the
+ * synthesis' minimizer state from it (move length, no previous direction, zero cycles). */
+inline void launchConjugateGradient(PrecisionModel prec, const AtomGraphSynthesis &poly_ag,
+                                    PhaseSpaceSynthesis *poly_ps, ReductionBridge *,
+                                    MolecularMechanicsControls *mmctrl,
+                                    const CoreKlManager &launcher) {
+  void* stream = launcher.getStream();
+  sb_synthesis* h = detail::prepare(prec, poly_ag, poly_ps, nullptr, nullptr, stream,
+                                    "launchConjugateGradient");
+  if (mmctrl == nullptr) {
+    throw std::runtime_error("launchConjugateGradient: MolecularMechanicsControls required");
+  }
+  if (mmctrl->begunFor() != h) {
+    sb_minimize_controls c;
+    sb_default_minimize_controls(&c);
+    c.total_cycles = mmctrl->getTotalCycles();
+    c.sd_cycles = mmctrl->getSteepestDescentCycles();
+    c.initial_step = mmctrl->getInitialStep();
+    c.clash_cycles = 0;
+    c.convergence_rms = 0.0;
+    c.kernel = SB_MIN_GRAPH;
+    detail::check(sb_minimize_begin(h, &c, stream), "launchConjugateGradient");
+    mmctrl->markBegun(h);
+  }
+  detail::check(sb_conjugate_gradient(h, stream), "launchConjugateGradient");
+}
+
+/* launchLineAdvance (MolecularMechanics/hpc_minimization.h:63-70): move 0-3 of the line search
+ * after an energy evaluation at the current coordinates (sb_line_advance); the energies are read
+ * on the device, so the ScoreCard is only bound */
+inline void launchLineAdvance(PrecisionModel prec, PhaseSpaceSynthesis *poly_ps,
+                              const AtomGraphSynthesis &poly_ag, ScoreCard *sc,
+                              LineMinimization *line_record, int move_number,
+                              const CoreKlManager &launcher) {
+  void* stream = launcher.getStream();
+  sb_synthesis* h = detail::prepare(prec, poly_ag, poly_ps, sc, nullptr, stream,
+                                    "launchLineAdvance");
+  if (line_record != nullptr && line_record->getSystemCount() != poly_ag.getSystemCount()) {
+    throw std::runtime_error("launchLineAdvance: the LineMinimization record is for another "
+                             "system count");
+  }
+  detail::check(sb_line_advance(h, move_number, stream), "launchLineAdvance");
 }
 
 namespace detail {

@@ -160,6 +160,8 @@ def library() -> ctypes.CDLL:
             "sb_get_minimize_history": (ctypes.c_int, [vp, vp, vp]),
             "sb_minimize_begin": (ctypes.c_int, [vp, ctypes.POINTER(MinimizeControls), vp]),
             "sb_minimize_advance": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, vp]),
+            "sb_conjugate_gradient": (ctypes.c_int, [vp, vp]),
+            "sb_line_advance": (ctypes.c_int, [vp, ctypes.c_int, vp]),
             "sb_autotune": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                            ctypes.POINTER(ctypes.c_int),
                                            ctypes.POINTER(ctypes.c_double), vp]),
@@ -600,6 +602,15 @@ class Synthesis:
         """Run up to `cycles` more cycles of every unfinished system (sb_minimize_advance)."""
         _check(library().sb_minimize_advance(self.handle, int(cycles), int(final_energy), stream),
                "sb_minimize_advance")
+
+    def conjugate_gradient(self, stream=None):
+        """One conjugate-gradient step of every system (sb_conjugate_gradient)."""
+        _check(library().sb_conjugate_gradient(self.handle, stream), "sb_conjugate_gradient")
+
+    def line_advance(self, move_number, stream=None):
+        """One line-search move 0-3 of every active system (sb_line_advance)."""
+        _check(library().sb_line_advance(self.handle, int(move_number), stream),
+               "sb_line_advance")
 
     def autotune(self, what=TUNE_EVALUATE, stream=None):
         """Pick the fastest work-unit packing; returns (atoms per unit, tiles per unit, ms)."""

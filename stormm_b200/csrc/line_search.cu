@@ -69,118 +69,170 @@ __device__ __forceinline__ void moveSystem(const DevSynthesis &d, const DevMinim
   }
 }
 
+// Conjugate-gradient step of one system at its line start (conjugate_gradient.cui:8-140):
+// energy E0 into the history, gg, dgg and |f|^2 over 32-atom chunks in a fixed order, the RMS
+// force and the convergence test, gamma (zero for the first sd_cycles cycles), the new direction
+// from the forces and its FP64 norm.  Returns false, with the system marked inactive for the
+// cycle, when it has converged or used up its cycles.
+template <bool HIST, bool DBL>
+__device__ __forceinline__ bool conjugateSystem(const DevSynthesis &d, const DevMinimizer &m,
+                                                int sys, double e0, int lane) {
+  const double inv_fs = 1.0 / static_cast<double>(d.frc_scale);
+  double* line = m.line + static_cast<size_t>(sys) * kLineFields;
+  const int cyc = m.cycle[sys];
+  if (m.done[sys] || cyc >= m.max_cycles) {
+    if (lane == 0) line[kLineAct] = 0.0;
+    return false;
+  }
+    const int natom = d.atom_count[sys];
+  const int base = d.atom_start[sys];
+  double gg = 0.0, dgg = 0.0, ff = 0.0;
+  for (int c = 0; c < natom; c += 32) {
+    const int a = c + lane;
+    double g = 0.0, dg = 0.0, f2s = 0.0;
+    if (a < natom) {
+      const int gi = base + a;
+      const double fx = int95ToDouble(d.xfrc[gi], d.xfrc_ovrf[gi]);
+      const double fy = int95ToDouble(d.yfrc[gi], d.yfrc_ovrf[gi]);
+      const double fz = int95ToDouble(d.zfrc[gi], d.zfrc_ovrf[gi]);
+      const double px = static_cast<double>(m.xprv[gi]);
+      const double py = static_cast<double>(m.yprv[gi]);
+      const double pz = static_cast<double>(m.zprv[gi]);
+      g = px * px + py * py + pz * pz;
+      dg = (fx - px) * fx + (fy - py) * fy + (fz - pz) * fz;
+      f2s = fx * fx + fy * fy + fz * fz;
+    }
+    gg += warpSumDouble(g);
+    dgg += warpSumDouble(dg);
+    ff += warpSumDouble(f2s);
+  }
+  gg *= inv_fs * inv_fs;
+  dgg *= inv_fs * inv_fs;
+  ff *= inv_fs * inv_fs;
+  const double rms = sqrt(ff / (3.0 * static_cast<double>(natom)));
+  if (lane == 0) {
+    m.rms_force[sys] = rms;
+    if (HIST && cyc < m.hist_stride) {
+      m.history[static_cast<size_t>(sys) * m.hist_stride + cyc] = e0;
+    }
+  }
+  if (m.drms > 0.0 && rms <= m.drms) {
+    if (lane == 0) {
+      m.done[sys] = 1;
+      line[kLineAct] = 0.0;
+    }
+    return false;
+  }
+  // the reference advances its step counter before the gather (hpc_minimization.cu:470)
+  const double gam = (cyc + 1 >= m.sd_cycles && gg > 0.0) ? dgg / gg : 0.0;
+  double msum = 0.0;
+  for (int c = 0; c < natom; c += 32) {
+    const int a = c + lane;
+    double ms = 0.0;
+    if (a < natom) {
+      const int gi = base + a;
+      const long long ix = d.xfrc[gi];
+      const long long iy = d.yfrc[gi];
+      const long long iz = d.zfrc[gi];
+      if (DBL) {
+        double cx = static_cast<double>(ix) * inv_fs;
+        double cy = static_cast<double>(iy) * inv_fs;
+        double cz = static_cast<double>(iz) * inv_fs;
+        if (fabs(gam) > kVeryTiny) {
+          cx = fma(gam, m.xcg64[gi], cx);
+          cy = fma(gam, m.ycg64[gi], cy);
+          cz = fma(gam, m.zcg64[gi], cz);
+        }
+        m.xcg64[gi] = cx;
+        m.ycg64[gi] = cy;
+        m.zcg64[gi] = cz;
+        ms = cx * cx + cy * cy + cz * cz;
+      }
+      else {
+        float cx = static_cast<float>(static_cast<double>(ix) * inv_fs);
+        float cy = static_cast<float>(static_cast<double>(iy) * inv_fs);
+        float cz = static_cast<float>(static_cast<double>(iz) * inv_fs);
+        if (fabs(gam) > kVeryTiny) {
+          const float gf = static_cast<float>(gam);
+          cx = fmaf(gf, m.xcg[gi], cx);
+          cy = fmaf(gf, m.ycg[gi], cy);
+          cz = fmaf(gf, m.zcg[gi], cz);
+        }
+        m.xcg[gi] = cx;
+        m.ycg[gi] = cy;
+        m.zcg[gi] = cz;
+        ms = static_cast<double>(cx) * cx + static_cast<double>(cy) * cy +
+             static_cast<double>(cz) * cz;
+      }
+      m.xprv[gi] = ix;
+      m.yprv[gi] = iy;
+      m.zprv[gi] = iz;
+    }
+    msum += warpSumDouble(ms);
+  }
+  const double inv_norm = (msum > 0.0) ? 1.0 / sqrt(msum) : 0.0;
+  if (lane == 0) {
+    line[kLineInvNorm] = inv_norm;
+    line[kLineAct] = 1.0;
+  }
+  return true;
+}
+
+// First move of a cycle (line_movement.cui:88-126): record E0 and move along the normalized
+// direction by the system's baseline move length
+template <bool DBL>
+__device__ __forceinline__ void firstMove(const DevSynthesis &d, const DevMinimizer &m, int sys,
+                                          double e0, double inv_norm, int lane) {
+  const double gpos_scale = 1.0 / d.inv_gpos_scale;
+  double* line = m.line + static_cast<size_t>(sys) * kLineFields;
+  const double s_move = m.l_move[sys];
+  if (lane == 0) {
+    line[kLineE0] = e0;
+    line[kLineSMove] = s_move;
+    line[kLineMfac] = 1.0;
+    line[kLineMv1] = 1.0;
+  }
+  __syncwarp();
+  moveSystem<DBL>(d, m, sys, inv_norm * s_move * gpos_scale, lane);
+}
+
+// Both at once, the graph minimizer's first line-search kernel of a cycle
 template <bool HIST, bool DBL>
 __global__ void __launch_bounds__(kLineThreads)
 kLineStart(const DevSynthesis d, const DevMinimizer m, int first, int count) {
   const int lane = threadIdx.x & 31;
-  const double inv_fs = 1.0 / static_cast<double>(d.frc_scale);
-  const double gpos_scale = 1.0 / d.inv_gpos_scale;
   for (int sys = first + firstWarp(); sys < first + count; sys += warpStride()) {
-    double* line = m.line + static_cast<size_t>(sys) * kLineFields;
     const double e0 = systemEnergy(d, sys, lane);
-    const int cyc = m.cycle[sys];
-    if (m.done[sys] || cyc >= m.max_cycles) {
-      if (lane == 0) line[kLineAct] = 0.0;
+    if (conjugateSystem<HIST, DBL>(d, m, sys, e0, lane)) {
+      __syncwarp();
+      const double inv_norm = m.line[static_cast<size_t>(sys) * kLineFields + kLineInvNorm];
+      firstMove<DBL>(d, m, sys, e0, inv_norm, lane);
+    }
+  }
+}
+
+// The conjugate-gradient step alone (STORMM's launchConjugateGradient)
+template <bool HIST, bool DBL>
+__global__ void __launch_bounds__(kLineThreads)
+kConjugateGradient(const DevSynthesis d, const DevMinimizer m, int first, int count) {
+  const int lane = threadIdx.x & 31;
+  for (int sys = first + firstWarp(); sys < first + count; sys += warpStride()) {
+    const double e0 = systemEnergy(d, sys, lane);
+    conjugateSystem<HIST, DBL>(d, m, sys, e0, lane);
+  }
+}
+
+// The first move alone (STORMM's launchLineAdvance with move 0), after kConjugateGradient
+template <bool DBL>
+__global__ void __launch_bounds__(kLineThreads)
+kLineFirstMove(const DevSynthesis d, const DevMinimizer m, int first, int count) {
+  const int lane = threadIdx.x & 31;
+  for (int sys = first + firstWarp(); sys < first + count; sys += warpStride()) {
+    const double* line = m.line + static_cast<size_t>(sys) * kLineFields;
+    if (line[kLineAct] == 0.0) {
       continue;
     }
-    const int natom = d.atom_count[sys];
-    const int base = d.atom_start[sys];
-    double gg = 0.0, dgg = 0.0, ff = 0.0;
-    for (int c = 0; c < natom; c += 32) {
-      const int a = c + lane;
-      double g = 0.0, dg = 0.0, f2s = 0.0;
-      if (a < natom) {
-        const int gi = base + a;
-        const double fx = int95ToDouble(d.xfrc[gi], d.xfrc_ovrf[gi]);
-        const double fy = int95ToDouble(d.yfrc[gi], d.yfrc_ovrf[gi]);
-        const double fz = int95ToDouble(d.zfrc[gi], d.zfrc_ovrf[gi]);
-        const double px = static_cast<double>(m.xprv[gi]);
-        const double py = static_cast<double>(m.yprv[gi]);
-        const double pz = static_cast<double>(m.zprv[gi]);
-        g = px * px + py * py + pz * pz;
-        dg = (fx - px) * fx + (fy - py) * fy + (fz - pz) * fz;
-        f2s = fx * fx + fy * fy + fz * fz;
-      }
-      gg += warpSumDouble(g);
-      dgg += warpSumDouble(dg);
-      ff += warpSumDouble(f2s);
-    }
-    gg *= inv_fs * inv_fs;
-    dgg *= inv_fs * inv_fs;
-    ff *= inv_fs * inv_fs;
-    const double rms = sqrt(ff / (3.0 * static_cast<double>(natom)));
-    if (lane == 0) {
-      m.rms_force[sys] = rms;
-      if (HIST && cyc < m.hist_stride) {
-        m.history[static_cast<size_t>(sys) * m.hist_stride + cyc] = e0;
-      }
-    }
-    if (m.drms > 0.0 && rms <= m.drms) {
-      if (lane == 0) {
-        m.done[sys] = 1;
-        line[kLineAct] = 0.0;
-      }
-      continue;
-    }
-    // the reference advances its step counter before the gather (hpc_minimization.cu:470)
-    const double gam = (cyc + 1 >= m.sd_cycles && gg > 0.0) ? dgg / gg : 0.0;
-    double msum = 0.0;
-    for (int c = 0; c < natom; c += 32) {
-      const int a = c + lane;
-      double ms = 0.0;
-      if (a < natom) {
-        const int gi = base + a;
-        const long long ix = d.xfrc[gi];
-        const long long iy = d.yfrc[gi];
-        const long long iz = d.zfrc[gi];
-        if (DBL) {
-          double cx = static_cast<double>(ix) * inv_fs;
-          double cy = static_cast<double>(iy) * inv_fs;
-          double cz = static_cast<double>(iz) * inv_fs;
-          if (fabs(gam) > kVeryTiny) {
-            cx = fma(gam, m.xcg64[gi], cx);
-            cy = fma(gam, m.ycg64[gi], cy);
-            cz = fma(gam, m.zcg64[gi], cz);
-          }
-          m.xcg64[gi] = cx;
-          m.ycg64[gi] = cy;
-          m.zcg64[gi] = cz;
-          ms = cx * cx + cy * cy + cz * cz;
-        }
-        else {
-          float cx = static_cast<float>(static_cast<double>(ix) * inv_fs);
-          float cy = static_cast<float>(static_cast<double>(iy) * inv_fs);
-          float cz = static_cast<float>(static_cast<double>(iz) * inv_fs);
-          if (fabs(gam) > kVeryTiny) {
-            const float gf = static_cast<float>(gam);
-            cx = fmaf(gf, m.xcg[gi], cx);
-            cy = fmaf(gf, m.ycg[gi], cy);
-            cz = fmaf(gf, m.zcg[gi], cz);
-          }
-          m.xcg[gi] = cx;
-          m.ycg[gi] = cy;
-          m.zcg[gi] = cz;
-          ms = static_cast<double>(cx) * cx + static_cast<double>(cy) * cy +
-               static_cast<double>(cz) * cz;
-        }
-        m.xprv[gi] = ix;
-        m.yprv[gi] = iy;
-        m.zprv[gi] = iz;
-      }
-      msum += warpSumDouble(ms);
-    }
-    const double inv_norm = (msum > 0.0) ? 1.0 / sqrt(msum) : 0.0;
-    const double s_move = m.l_move[sys];
-    if (lane == 0) {
-      line[kLineE0] = e0;
-      line[kLineInvNorm] = inv_norm;
-      line[kLineSMove] = s_move;
-      line[kLineMfac] = 1.0;
-      line[kLineMv1] = 1.0;
-      line[kLineAct] = 1.0;
-    }
-    __syncwarp();
-    moveSystem<DBL>(d, m, sys, inv_norm * s_move * gpos_scale, lane);
+    firstMove<DBL>(d, m, sys, systemEnergy(d, sys, lane), line[kLineInvNorm], lane);
   }
 }
 
@@ -264,7 +316,8 @@ int lineGrid(int count) {
 
 }  // namespace
 
-// step: 0 start, 1 and 2 trial moves, 3 finish, 4 history of the final energies
+// step: 0 start (conjugate gradient and first move), 1 and 2 trial moves, 3 finish, 4 history
+// of the final energies, 5 the conjugate-gradient step alone, 6 the first move alone
 cudaError_t launchLineStep(const DevSynthesis &d, const DevMinimizer &m, int first, int count,
                            int step, cudaStream_t stream) {
   if (count <= 0) {
@@ -309,6 +362,30 @@ cudaError_t launchLineStep(const DevSynthesis &d, const DevMinimizer &m, int fir
     case 4:
       if (m.history != nullptr) {
         kLineHistory<<<grid, kLineThreads, 0, stream>>>(d, m, first, count);
+      }
+      break;
+    case 5:
+      if (m.history != nullptr) {
+        if (dbl) {
+          kConjugateGradient<true, true><<<grid, kLineThreads, 0, stream>>>(d, m, first, count);
+        }
+        else {
+          kConjugateGradient<true, false><<<grid, kLineThreads, 0, stream>>>(d, m, first, count);
+        }
+      }
+      else if (dbl) {
+        kConjugateGradient<false, true><<<grid, kLineThreads, 0, stream>>>(d, m, first, count);
+      }
+      else {
+        kConjugateGradient<false, false><<<grid, kLineThreads, 0, stream>>>(d, m, first, count);
+      }
+      break;
+    case 6:
+      if (dbl) {
+        kLineFirstMove<true><<<grid, kLineThreads, 0, stream>>>(d, m, first, count);
+      }
+      else {
+        kLineFirstMove<false><<<grid, kLineThreads, 0, stream>>>(d, m, first, count);
       }
       break;
     default:

@@ -1213,6 +1213,26 @@ void Synthesis::launchMinPlan(const UnitPlan &plan, int cycles, bool final_energ
   }
 }
 
+// The line-search steps one at a time, for a caller that runs its own evaluations between them
+// (STORMM's launchConjugateGradient and launchLineAdvance): every system of the synthesis
+void Synthesis::conjugateGradient(cudaStream_t stream) {
+  if (!min_ready) {
+    throw Error(SB_ERR_ARGUMENT, "no minimization has begun on this synthesis");
+  }
+  cudaCheck(launchLineStep(dev, dev_min, 0, nsys, 5, stream), "conjugate gradient launch");
+}
+
+void Synthesis::lineAdvance(int move, cudaStream_t stream) {
+  if (!min_ready) {
+    throw Error(SB_ERR_ARGUMENT, "no minimization has begun on this synthesis");
+  }
+  if (move < 0 || move > 3) {
+    throw Error(SB_ERR_ARGUMENT, "line move number must be 0, 1, 2 or 3");
+  }
+  cudaCheck(launchLineStep(dev, dev_min, 0, nsys, (move == 0) ? 6 : move, stream),
+            "line advance launch");
+}
+
 void Synthesis::minimizeAdvance(int cycles, bool final_energy, cudaStream_t stream) {
   if (!min_ready) {
     throw Error(SB_ERR_ARGUMENT, "no minimization has begun on this synthesis");
@@ -1687,6 +1707,14 @@ int sb_minimize_advance(sb_synthesis* syn, int cycles, int final_energy, void* s
   return guarded([&]() {
     need(syn)->minimizeAdvance(cycles, final_energy != 0, asStream(stream));
   });
+}
+
+int sb_conjugate_gradient(sb_synthesis* syn, void* stream) {
+  return guarded([&]() { need(syn)->conjugateGradient(asStream(stream)); });
+}
+
+int sb_line_advance(sb_synthesis* syn, int move_number, void* stream) {
+  return guarded([&]() { need(syn)->lineAdvance(move_number, asStream(stream)); });
 }
 
 int sb_autotune(sb_synthesis* syn, int what, int* max_atoms_per_unit, int* max_tiles_per_unit,

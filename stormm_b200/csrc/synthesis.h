@@ -146,6 +146,8 @@ public:
   void minimize(const sb_minimize_controls &ctl, cudaStream_t stream);
   void minimizeBegin(const sb_minimize_controls &ctl, cudaStream_t stream);
   void minimizeAdvance(int cycles, bool final_energy, cudaStream_t stream);
+  void conjugateGradient(cudaStream_t stream);
+  void lineAdvance(int move, cudaStream_t stream);
   void autotune(int what, int* chosen_slots, int* chosen_tiles, double* best_ms,
                 cudaStream_t stream);
   void minimizeRange(int first, int count, const sb_minimize_controls &ctl, cudaStream_t stream);

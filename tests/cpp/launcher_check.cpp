@@ -182,6 +182,45 @@ int deviceChecks(FILE* out, const std::vector<std::string> &files) {
   put(out, "min_history", hist);
   put(out, "min_coords", xyz);
 
+  // A line search driven step by step, as STORMM's launchMinimization drives its kernels:
+  // evaluations by launchValence + launchNonbonded, launchConjugateGradient after the line-start
+  // evaluation, launchLineAdvance after each of the four evaluations (no clash-damped cycles)
+  poly_ps.upload();
+  MinimizeControls step_con;
+  step_con.setTotalCycles(12);
+  step_con.setSteepestDescentCycles(4);
+  step_con.setClashDampingCycles(0);
+  MolecularMechanicsControls step_ctrl(step_con);
+  LineMinimization line_record(nsys, step_con.getInitialStep());
+  ReductionBridge rbg(static_cast<size_t>(nsys));
+  ScoreCard sc_steps(nsys);
+  for (int cyc = 0; cyc < step_con.getTotalCycles(); cyc++) {
+    for (int move = 0; move < 4; move++) {
+      const EvaluateForce ef = (move == 0) ? EvaluateForce::YES : EvaluateForce::NO;
+      sc_steps.initialize();
+      if (move == 0) {
+        poly_ps.initializeForces();
+      }
+      launchValence(PrecisionModel::SINGLE, poly_ag, &step_ctrl, &poly_ps, &heat_bath, &sc_steps,
+                    &tb_space, ef, EvaluateEnergy::YES, VwuGoal::ACCUMULATE, launcher);
+      launchNonbonded(PrecisionModel::SINGLE, poly_ag, poly_se, &step_ctrl, &poly_ps, &heat_bath,
+                      &sc_steps, &tb_space, &ism_space, ef, EvaluateEnergy::YES, launcher);
+      if (move == 0) {
+        launchConjugateGradient(PrecisionModel::SINGLE, poly_ag, &poly_ps, &rbg, &step_ctrl,
+                                launcher);
+      }
+      launchLineAdvance(PrecisionModel::SINGLE, &poly_ps, poly_ag, &sc_steps, &line_record, move,
+                        launcher);
+    }
+  }
+  poly_ps.download();
+  std::vector<double> step_xyz;
+  for (int s = 0; s < nsys; s++) {
+    const std::vector<double> c = poly_ps.getInterlacedCoordinates(s);
+    step_xyz.insert(step_xyz.end(), c.begin(), c.end());
+  }
+  put(out, "steps_coords", step_xyz);
+
   // The same minimization with PrecisionModel::DOUBLE on a synthesis uploaded for FP64
   AtomGraphSynthesis poly_ag64(ag_list, systems);
   poly_ag64.setImplicitSolventModel(ImplicitSolventModel::OBC_GB_II);

@@ -149,6 +149,22 @@ def test_launchers_match_python_path_and_oracle(tmp_path):
     np.testing.assert_array_equal(cpp["min_history"], samples)
     assert np.all(cpp["min_potential"] < cpp["potential"])
 
+    # the line search step by step through launchConjugateGradient / launchLineAdvance, against
+    # the same steps through the C ABI from Python; the C++ caller starts from the coordinates its
+    # PhaseSpaceSynthesis downloaded after launchMinimization
+    syn.set_coordinates(cpp["min_coords"])
+    syn.minimize_begin(total_cycles=12, sd_cycles=4, clash_cycles=0, convergence_rms=0.0,
+                       kernel=sb.MIN_GRAPH)
+    for _ in range(12):
+        for move in range(4):
+            syn.initialize(sb.INIT_ENERGIES | (sb.INIT_FORCES if move == 0 else 0))
+            syn.launch_valence(force=(move == 0))
+            syn.launch_nonbonded(force=(move == 0))
+            if move == 0:
+                syn.conjugate_gradient()
+            syn.line_advance(move)
+    np.testing.assert_array_equal(cpp["steps_coords"], syn.coordinates().reshape(-1))
+
     # PrecisionModel::DOUBLE: the same minimization on a synthesis uploaded for FP64
     syn64 = sb.Synthesis(mols, topology_index=index, igb=sb.SB_GB_OBC2,
                          precision=sb.PRECISION_DOUBLE)

@@ -271,3 +271,46 @@ def test_graph_and_persistent_kernels_agree():
     np.testing.assert_allclose(h_g[:, :3], h_p[:, :3], rtol=1e-5)
     drop = h_p[:, 0] - h_p[:, -1]
     assert np.all(np.abs(h_g[:, -1] - h_p[:, -1]) <= 0.01 * drop + 1e-3)
+
+
+def test_line_search_steps_equal_the_graph_minimizer():
+    """sb_conjugate_gradient and sb_line_advance (STORMM's launchConjugateGradient and
+    launchLineAdvance) between evaluations run the graph minimizer's cycle: after 15 cycles the
+    coordinates and the energy history are bit-identical to sb_minimize's."""
+    mols = [synthetic.make_molecule(synthetic._seed(8181, k), n, 0.3)
+            for k, n in enumerate([24, 40, 63, 96, 130])]
+    xyz = np.concatenate([m.coords for m in mols])
+    ctl = dict(total_cycles=15, sd_cycles=5, clash_cycles=0, convergence_rms=0.0,
+               kernel=sb.MIN_GRAPH, record_history=True)
+    ref = sb.Synthesis(mols)
+    ref.set_coordinates(xyz)
+    ref.minimize(**ctl)
+    syn = sb.Synthesis(mols)
+    syn.set_coordinates(xyz)
+    syn.minimize_begin(**ctl)
+    for _ in range(15):
+        syn.initialize(sb.INIT_FORCES | sb.INIT_ENERGIES)
+        syn.evaluate()
+        syn.conjugate_gradient()
+        syn.line_advance(0)
+        for move in (1, 2, 3):
+            syn.initialize(sb.INIT_ENERGIES)
+            syn.evaluate(force=False, energy=True)
+            syn.line_advance(move)
+    assert syn.status() == 0 and ref.status() == 0
+    assert np.array_equal(syn.coordinates(), ref.coordinates())
+    np.testing.assert_array_equal(syn.minimize_history()[:, :15], ref.minimize_history()[:, :15])
+    cycles, _, _ = syn.minimize_progress()
+    assert np.all(cycles == 15)
+    with pytest.raises(sb.StormmB200Error):
+        syn.line_advance(4)
+
+
+def test_line_search_steps_need_a_begun_minimization():
+    mol = synthetic.make_molecule(synthetic._seed(8182, 0), 30, 0.3)
+    syn = sb.Synthesis([mol])
+    syn.set_coordinates(mol.coords)
+    with pytest.raises(sb.StormmB200Error):
+        syn.conjugate_gradient()
+    with pytest.raises(sb.StormmB200Error):
+        syn.line_advance(0)
