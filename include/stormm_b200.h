@@ -317,7 +317,15 @@ int sb_get_minimize_progress(sb_synthesis* syn, int* cycles_done, int* converged
  * launches of cycles_per_launch cycles on a stream of its own (batches overlap on the GPU),
  * retires every molecule that converged or reached total_cycles after each launch, and
  * backfills: new batches start while older ones are still running.  A molecule's result does
- * not depend on the batch it ran in. */
+ * not depend on the batch it ran in.
+ *
+ * Errors: submit checks the topology on the host (the checks the synthesis applies) and refuses
+ * a bad request with its error code; the server's controls are checked when it is created.  A
+ * batch that still fails to build is split and its requests are retried one per batch, so only
+ * the request that cannot be built fails; a request that fails is returned by poll with its
+ * error code in status.  Only a lost CUDA context stops the worker: the batches in flight are
+ * returned failed, and submit and drain then report the error (poll still hands out the
+ * results that were ready). */
 #define SB_TIMEOUT 1            /* sb_server_drain: work still in flight when time ran out */
 
 typedef struct {
@@ -338,6 +346,8 @@ typedef struct {
   int kind;                          /* SB_REQUEST_* */
   int cycles;                        /* line-minimization cycles run */
   int converged;                     /* nonzero: the RMS force met controls.convergence_rms */
+  int status;                        /* SB_OK, or the error code that failed the request (no
+                                        coordinates or forces are returned for it) */
   double rms_force;                  /* kcal/mol/A at the start of the last cycle (minimization),
                                         at the given coordinates (evaluation) */
   double energy;                     /* total potential energy at the final coordinates */
@@ -350,7 +360,8 @@ typedef struct {
 typedef struct {
   long long submitted;
   long long admitted;
-  long long completed;
+  long long completed;                /* results returned, the failed ones included */
+  long long failed;                   /* requests returned with an error status */
   int pending;                       /* queued, not yet admitted */
   int in_flight;                     /* admitted molecules still minimizing */
   int batches;

@@ -83,8 +83,8 @@ class ServerOptions(ctypes.Structure):
 class ServedResult(ctypes.Structure):
     _fields_ = [
         ("request_id", ctypes.c_longlong), ("natom", ctypes.c_int), ("kind", ctypes.c_int),
-        ("cycles", ctypes.c_int),
-        ("converged", ctypes.c_int), ("rms_force", ctypes.c_double), ("energy", ctypes.c_double),
+        ("cycles", ctypes.c_int), ("converged", ctypes.c_int), ("status", ctypes.c_int),
+        ("rms_force", ctypes.c_double), ("energy", ctypes.c_double),
         ("energies", ctypes.c_double * 16), ("submit_time", ctypes.c_double),
         ("admit_time", ctypes.c_double), ("finish_time", ctypes.c_double),
     ]
@@ -93,7 +93,8 @@ class ServedResult(ctypes.Structure):
 class ServerStats(ctypes.Structure):
     _fields_ = [
         ("submitted", ctypes.c_longlong), ("admitted", ctypes.c_longlong),
-        ("completed", ctypes.c_longlong), ("pending", ctypes.c_int), ("in_flight", ctypes.c_int),
+        ("completed", ctypes.c_longlong), ("failed", ctypes.c_longlong),
+        ("pending", ctypes.c_int), ("in_flight", ctypes.c_int),
         ("batches", ctypes.c_int), ("bytes_in_flight", ctypes.c_double),
     ]
 
@@ -708,7 +709,8 @@ class Server:
 
     def poll(self, max_results=4096, coordinates=True):
         """List of (result dict, array or None) for the requests completed so far: final
-        coordinates of a minimization, forces of an evaluation (dict key "kind")."""
+        coordinates of a minimization, forces of an evaluation (dict key "kind").  A request
+        that failed has a nonzero "status" (the library's error code) and no array."""
         res = (ServedResult * max_results)()
         cap = 3 * sum(self._natom.values()) if coordinates else 0
         buf = np.zeros(max(cap, 1)) if coordinates else None
@@ -722,12 +724,12 @@ class Server:
             r = res[k]
             d = {"request_id": r.request_id, "natom": r.natom,
                  "kind": "evaluate" if r.kind == SB_REQUEST_EVALUATE else "minimize",
-                 "cycles": r.cycles,
+                 "cycles": r.cycles, "status": r.status,
                  "converged": bool(r.converged), "rms_force": r.rms_force, "energy": r.energy,
                  "energies": np.array(r.energies[:]), "submit_time": r.submit_time,
                  "admit_time": r.admit_time, "finish_time": r.finish_time}
             xyz = None
-            if coordinates:
+            if coordinates and r.status == 0:
                 xyz = buf[off:off + 3 * r.natom].reshape(-1, 3).copy()
                 off += 3 * r.natom
             self._natom.pop(r.request_id, None)

@@ -13,6 +13,13 @@
 //             the rest; a batch whose molecules have all retired is freed on its stream
 // Batches overlap on the device, new batches start while older ones run (backfill), and a
 // molecule's trajectory is bit-identical whichever batch, unit or launch split it gets.
+//
+// Errors stay with the requests that cause them.  submit runs the synthesis's topology checks on
+// the host, so a malformed topology is refused before it is queued.  A batch that still fails
+// to build is released and its requests queued again to be admitted one per batch, so that only
+// the request that cannot be built fails; a batch whose launch or read-back fails returns its
+// unfinished requests with the error code.  Either way the worker goes on with the other
+// batches, unless the CUDA context itself is lost.
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -63,6 +70,7 @@ struct Request {
   double t_submit = 0.0;
   double t_admit = 0.0;
   int kind = SB_REQUEST_MINIMIZE;
+  bool solo = false;                  // retried alone after its batch failed to build
 
   Request(const sb_topology &t, const double* coords) {
     natom = t.natom;
@@ -170,13 +178,18 @@ struct Batch {
 class Server {
 public:
   explicit Server(const sb_server_options &o) : opt_(o), t0_(std::chrono::steady_clock::now()) {
-    if (o.hbm_budget_bytes <= 0.0 || o.max_batch_molecules < 1 || o.max_batches < 1 ||
+    if (!(o.hbm_budget_bytes > 0.0) || o.max_batch_molecules < 1 || o.max_batches < 1 ||
         o.cycles_per_launch < 1) {
       throw Error(SB_ERR_ARGUMENT, "server budget, batch limits and cycles per launch must be "
                   "positive");
     }
-    if (o.options.precision != SB_PRECISION_SINGLE) {
-      throw Error(SB_ERR_UNSUPPORTED, "the request server minimizes, which runs in FP32");
+    validateMinimizeControls(o.controls);
+    if (o.options.precision != SB_PRECISION_SINGLE && o.options.precision != SB_PRECISION_DOUBLE) {
+      throw Error(SB_ERR_ARGUMENT, "precision must be SB_PRECISION_SINGLE or SB_PRECISION_DOUBLE");
+    }
+    if (o.options.precision == SB_PRECISION_DOUBLE && o.controls.kernel != SB_MIN_GRAPH) {
+      throw Error(SB_ERR_UNSUPPORTED, "an FP64 server minimizes with the graph minimizer: set "
+                  "controls.kernel to SB_MIN_GRAPH");
     }
     int ndev = 0;
     cudaCheck(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
@@ -205,6 +218,7 @@ public:
     if (kind != SB_REQUEST_MINIMIZE && kind != SB_REQUEST_EVALUATE) {
       throw Error(SB_ERR_ARGUMENT, "unknown request kind " + std::to_string(kind));
     }
+    validateTopology(*top, opt_.options, -1);
     const int on_chip = (opt_.options.tiled_above_atoms > 0) ? opt_.options.tiled_above_atoms : 2048;
     if (kind == SB_REQUEST_MINIMIZE && top->natom > on_chip &&
         opt_.controls.kernel != SB_MIN_GRAPH) {
@@ -214,6 +228,9 @@ public:
     }
     Request req(*top, xyz);
     req.kind = kind;
+    if (opt_.options.precision == SB_PRECISION_DOUBLE) {
+      req.bytes *= 2.0;   // the FP64 mode's per-atom and per-term arrays are twice as wide
+    }
     if (req.bytes > opt_.hbm_budget_bytes) {
       throw Error(SB_ERR_ARGUMENT, "the molecule alone exceeds the server's HBM budget");
     }
@@ -230,7 +247,9 @@ public:
 
   int poll(sb_served_result* out, int max_results, double* xyz, long long cap) {
     std::lock_guard<std::mutex> lock(mu_);
-    failIfBroken();
+    if (results_.empty()) {
+      failIfBroken();
+    }
     int n = 0;
     long long used = 0;
     while (n < max_results && !results_.empty()) {
@@ -240,7 +259,9 @@ public:
         if (used + need > cap) {
           break;
         }
-        std::memcpy(xyz + used, r.xyz.data(), sizeof(double) * need);
+        if (need > 0) {
+          std::memcpy(xyz + used, r.xyz.data(), sizeof(double) * need);
+        }
         used += need;
       }
       out[n++] = r.r;
@@ -269,6 +290,7 @@ public:
     s.submitted = submitted_;
     s.admitted = admitted_;
     s.completed = completed_;
+    s.failed = failed_;
     s.pending = static_cast<int>(pending_.size());
     s.in_flight = in_flight_;
     s.batches = nbatches_;
@@ -287,10 +309,54 @@ private:
     }
   }
 
+  // After an error: clear it if it does not persist, and throw if the CUDA context is lost (an
+  // event that was never recorded queries as complete unless the context has failed)
+  void checkContext() {
+    cudaGetLastError();
+    const cudaError_t e = cudaEventQuery(probe_);
+    if (e != cudaSuccess) {
+      throw Error(SB_ERR_CUDA, std::string("CUDA context lost: ") + cudaGetErrorString(e));
+    }
+  }
+
+  // Requests admitted in arrival order while the batch and the memory budget allow: the oldest
+  // pending request's kind only; a request retried alone after a failed build forms a batch of
+  // its own.  Called with mu_ held.
+  std::vector<Request> takePending() {
+    std::vector<Request> take;
+    const int kind = pending_.front().kind;
+    double bytes = bytes_in_flight_;
+    for (auto it = pending_.begin(); it != pending_.end() &&
+         static_cast<int>(take.size()) < opt_.max_batch_molecules;) {
+      if (it->kind != kind) {
+        ++it;
+        continue;
+      }
+      if (bytes + it->bytes > opt_.hbm_budget_bytes || (it->solo && !take.empty())) {
+        break;
+      }
+      const bool solo = it->solo;
+      bytes += it->bytes;
+      take.push_back(std::move(*it));
+      it = pending_.erase(it);
+      if (solo) {
+        break;
+      }
+    }
+    if (!take.empty()) {
+      bytes_in_flight_ = bytes;
+      in_flight_ += static_cast<int>(take.size());
+      admitted_ += static_cast<long long>(take.size());
+      nbatches_++;
+    }
+    return take;
+  }
+
   void run() {
+    std::vector<std::unique_ptr<Batch>> batches;
     try {
       cudaCheck(cudaSetDevice(opt_.options.device), "cudaSetDevice");
-      std::vector<std::unique_ptr<Batch>> batches;
+      cudaCheck(cudaEventCreateWithFlags(&probe_, cudaEventDisableTiming), "cudaEventCreate");
       while (true) {
         bool progress = false;
         for (size_t b = 0; b < batches.size();) {
@@ -299,9 +365,21 @@ private:
             b++;
             continue;
           }
-          cudaCheck(q, "batch launch");
           progress = true;
-          if (service(batches[b].get())) {
+          bool finished = false;
+          try {
+            cudaCheck(q, "batch launch");
+            finished = service(batches[b].get());
+          }
+          catch (const Error &e) {
+            // this batch's requests fail; the other batches carry on unless the context is lost
+            std::unique_ptr<Batch> failed = std::move(batches[b]);
+            batches.erase(batches.begin() + b);
+            failBatch(std::move(failed), e.code);
+            checkContext();
+            continue;
+          }
+          if (finished) {
             retire(std::move(batches[b]));
             batches.erase(batches.begin() + b);
           }
@@ -316,29 +394,7 @@ private:
             break;
           }
           if (static_cast<int>(batches.size()) < opt_.max_batches && !pending_.empty()) {
-            // a batch holds one kind of request: the oldest pending one's, taken in arrival
-            // order until the batch or the memory budget is full
-            const int kind = pending_.front().kind;
-            double bytes = bytes_in_flight_;
-            for (auto it = pending_.begin(); it != pending_.end() &&
-                 static_cast<int>(take.size()) < opt_.max_batch_molecules;) {
-              if (it->kind != kind) {
-                ++it;
-                continue;
-              }
-              if (bytes + it->bytes > opt_.hbm_budget_bytes) {
-                break;
-              }
-              bytes += it->bytes;
-              take.push_back(std::move(*it));
-              it = pending_.erase(it);
-            }
-            if (!take.empty()) {
-              bytes_in_flight_ = bytes;
-              in_flight_ += static_cast<int>(take.size());
-              admitted_ += static_cast<long long>(take.size());
-              nbatches_++;
-            }
+            take = takePending();
           }
           if (take.empty() && !progress) {
             // nothing to launch or collect: sleep until a submission or a short timeout
@@ -347,7 +403,20 @@ private:
           }
         }
         if (!take.empty()) {
-          batches.push_back(admit(std::move(take)));
+          std::unique_ptr<Batch> b = makeBatch(std::move(take));
+          try {
+            start(b.get());
+            batches.push_back(std::move(b));
+          }
+          catch (const Error &e) {
+            if (b->reqs.size() > 1) {
+              requeueAlone(std::move(b));
+            }
+            else {
+              failBatch(std::move(b), e.code);
+            }
+            checkContext();
+          }
         }
       }
       // stop: let the launches in flight finish, then release every batch on its stream
@@ -357,19 +426,36 @@ private:
       }
     }
     catch (const std::exception &e) {
+      // the context is lost (or the worker could not start): return what is in flight as failed
+      for (auto &b : batches) {
+        if (b) {
+          failBatch(std::move(b), SB_ERR_CUDA);
+        }
+      }
       std::lock_guard<std::mutex> lock(mu_);
       error_ = e.what();
       idle_cv_.notify_all();
     }
+    if (probe_ != nullptr) {
+      cudaEventDestroy(probe_);
+      probe_ = nullptr;
+    }
   }
 
-  // Build, upload and start a batch on a stream of its own
-  std::unique_ptr<Batch> admit(std::vector<Request> take) {
+  std::unique_ptr<Batch> makeBatch(std::vector<Request> take) {
     auto b = std::make_unique<Batch>();
     b->kind = take.front().kind;
     b->reqs = std::move(take);
     b->finished.assign(b->reqs.size(), 0);
     b->remaining = static_cast<int>(b->reqs.size());
+    for (const Request &r : b->reqs) {
+      b->bytes += r.bytes;
+    }
+    return b;
+  }
+
+  // Build, upload and start a batch on a stream of its own
+  void start(Batch* b) {
     cudaCheck(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     cudaCheck(cudaEventCreateWithFlags(&b->event, cudaEventDisableTiming), "cudaEventCreate");
     const double t = now();
@@ -379,7 +465,6 @@ private:
     for (size_t k = 0; k < b->reqs.size(); k++) {
       Request &r = b->reqs[k];
       r.t_admit = t;
-      b->bytes += r.bytes;
       tops.push_back(r.view());
       index.push_back(static_cast<int>(k));
       xyz.insert(xyz.end(), r.xyz.begin(), r.xyz.end());
@@ -402,7 +487,59 @@ private:
       b->syn->evaluate(SB_TERM_ALL, true, true, b->stream);
     }
     cudaCheck(cudaEventRecord(b->event, b->stream), "cudaEventRecord");
-    return b;
+  }
+
+  // A batch that could not be built: release it and queue its requests again, at the front in
+  // their order, each to be admitted alone
+  void requeueAlone(std::unique_ptr<Batch> b) {
+    std::vector<Request> reqs = std::move(b->reqs);
+    b->reqs.clear();
+    retire(std::move(b));
+    std::lock_guard<std::mutex> lock(mu_);
+    in_flight_ -= static_cast<int>(reqs.size());
+    admitted_ -= static_cast<long long>(reqs.size());
+    for (auto it = reqs.rbegin(); it != reqs.rend(); ++it) {
+      it->solo = true;
+      pending_.push_front(std::move(*it));
+    }
+    cv_.notify_all();
+  }
+
+  // The unfinished requests of a batch are returned with the error code; the batch is released
+  void failBatch(std::unique_ptr<Batch> b, int code) {
+    const double t = now();
+    std::vector<Result> out;
+    for (size_t k = 0; k < b->reqs.size(); k++) {
+      if (b->finished[k]) {
+        continue;
+      }
+      const Request &r = b->reqs[k];
+      Result res;
+      std::memset(&res.r, 0, sizeof(sb_served_result));
+      res.r.request_id = r.id;
+      res.r.natom = r.natom;
+      res.r.kind = r.kind;
+      res.r.status = (code != SB_OK) ? code : SB_ERR_CUDA;
+      res.r.energy = std::nan("");
+      res.r.rms_force = std::nan("");
+      res.r.submit_time = r.t_submit;
+      res.r.admit_time = r.t_admit;
+      res.r.finish_time = t;
+      out.push_back(std::move(res));
+      b->finished[k] = 1;
+    }
+    b->remaining = 0;
+    retire(std::move(b));
+    std::lock_guard<std::mutex> lock(mu_);
+    for (auto &res : out) {
+      results_.push_back(std::move(res));
+    }
+    in_flight_ -= static_cast<int>(out.size());
+    completed_ += static_cast<long long>(out.size());
+    failed_ += static_cast<long long>(out.size());
+    if (pending_.empty() && in_flight_ == 0) {
+      idle_cv_.notify_all();
+    }
   }
 
   // Results of an evaluation batch (all of it completes with its one launch)
@@ -526,12 +663,19 @@ private:
 
   // Free a batch's device memory in its stream's order, then its stream
   void retire(std::unique_ptr<Batch> b) {
-    {
+    if (b->stream != nullptr) {
       AllocationStreamGuard guard(b->stream);
       b->syn.reset();
     }
-    cudaEventDestroy(b->event);
-    cudaStreamDestroy(b->stream);
+    else {
+      b->syn.reset();
+    }
+    if (b->event != nullptr) {
+      cudaEventDestroy(b->event);
+    }
+    if (b->stream != nullptr) {
+      cudaStreamDestroy(b->stream);
+    }
     std::lock_guard<std::mutex> lock(mu_);
     bytes_in_flight_ -= b->bytes;
     if (bytes_in_flight_ < 0.0) {
@@ -553,11 +697,13 @@ private:
   long long submitted_ = 0;
   long long admitted_ = 0;
   long long completed_ = 0;
+  long long failed_ = 0;
   int in_flight_ = 0;
   int nbatches_ = 0;
   double bytes_in_flight_ = 0.0;
   bool stop_ = false;
   std::string error_;
+  cudaEvent_t probe_ = nullptr;       // never recorded: queries fail only with a lost context
 };
 
 }  // namespace sb

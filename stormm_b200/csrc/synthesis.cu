@@ -98,6 +98,83 @@ uint32_t fbits(double v) {
 
 }  // namespace
 
+// Intrinsic radius -> row of the neck GB tables (Topology/atomgraph_setters.cpp:1088-1092)
+static int neckIndex(double pb_radius) {
+  return static_cast<int>(((pb_radius - 1.0) * 20.0) + 0.5);
+}
+
+void validateTopology(const sb_topology &tp, const sb_options &opt, int which) {
+  const std::string name = (which >= 0) ? "topology " + std::to_string(which) : "the topology";
+  if (tp.natom <= 0 || tp.natom > 65535 || tp.charge == nullptr || tp.lj_idx == nullptr ||
+      tp.lja == nullptr || tp.ljb == nullptr || tp.n_lj_types <= 0 || tp.n_lj_types > 64) {
+    throw Error(SB_ERR_ARGUMENT, name + " is incomplete or too large");
+  }
+  const int n = tp.natom;
+  if (tp.nbond < 0 || tp.nangl < 0 || tp.ndihe < 0 ||
+      (tp.nbond > 0 && (tp.bond_atoms == nullptr || tp.bond_keq == nullptr ||
+                        tp.bond_leq == nullptr)) ||
+      (tp.nangl > 0 && (tp.angl_atoms == nullptr || tp.angl_keq == nullptr ||
+                        tp.angl_theta0 == nullptr)) ||
+      (tp.ndihe > 0 && (tp.dihe_atoms == nullptr || tp.dihe_amp == nullptr ||
+                        tp.dihe_freq == nullptr || tp.dihe_phase == nullptr))) {
+    throw Error(SB_ERR_ARGUMENT, name + " has negative term counts or lacks term arrays");
+  }
+  for (int i = 0; i < n; i++) {
+    if (tp.lj_idx[i] < 0 || tp.lj_idx[i] >= tp.n_lj_types) {
+      throw Error(SB_ERR_ARGUMENT, name + ": Lennard-Jones type out of range");
+    }
+  }
+  if (tp.excl_bounds != nullptr) {
+    if (tp.excl_bounds[0] < 0 || (tp.excl_list == nullptr && tp.excl_bounds[n] > 0)) {
+      throw Error(SB_ERR_ARGUMENT, name + ": exclusion bounds without an exclusion list");
+    }
+    for (int i = 0; i < n; i++) {
+      if (tp.excl_bounds[i + 1] < tp.excl_bounds[i]) {
+        throw Error(SB_ERR_ARGUMENT, name + ": exclusion bounds must not decrease");
+      }
+      for (int e = tp.excl_bounds[i]; e < tp.excl_bounds[i + 1]; e++) {
+        if (tp.excl_list[e] < 0 || tp.excl_list[e] >= n) {
+          throw Error(SB_ERR_ARGUMENT, name + ": exclusion partner out of range");
+        }
+      }
+    }
+  }
+  if (opt.igb != SB_GB_NONE && (tp.pb_radii == nullptr || tp.gb_screen == nullptr)) {
+    throw Error(SB_ERR_ARGUMENT, name + " lacks GB radii");
+  }
+  if (opt.igb == SB_GB_NECK || opt.igb == SB_GB_NECK2) {
+    for (int i = 0; i < n; i++) {
+      const int idx = neckIndex(tp.pb_radii[i]);
+      if (idx < 0 || idx >= opt.neck_table_size) {
+        throw Error(SB_ERR_ARGUMENT, name + ": neck GB needs intrinsic radii within the neck "
+                    "tables (1-2 A for STORMM's 21 x 21 tables)");
+      }
+    }
+    if (opt.igb == SB_GB_NECK2 && (tp.gb_alpha == nullptr || tp.gb_beta == nullptr ||
+                                    tp.gb_gamma == nullptr)) {
+      throw Error(SB_ERR_ARGUMENT, name + ": neck GB II takes element-specific alpha, beta and "
+                  "gamma from the topology");
+    }
+  }
+  auto in_range = [n](const int* atoms, size_t count) {
+    for (size_t k = 0; k < count; k++) {
+      if (atoms[k] < 0 || atoms[k] >= n) return false;
+    }
+    return true;
+  };
+  if (!in_range(tp.bond_atoms, 2 * static_cast<size_t>(tp.nbond)) ||
+      !in_range(tp.angl_atoms, 3 * static_cast<size_t>(tp.nangl)) ||
+      !in_range(tp.dihe_atoms, 4 * static_cast<size_t>(tp.ndihe))) {
+    throw Error(SB_ERR_ARGUMENT, name + ": valence term atom index out of range");
+  }
+  // a dihedral's fourth atom shares its word with the improper flag
+  for (int d = 0; d < tp.ndihe; d++) {
+    if (tp.dihe_atoms[4 * d + 3] > 0x7fff) {
+      throw Error(SB_ERR_UNSUPPORTED, name + ": dihedral atom index above 32767");
+    }
+  }
+}
+
 Synthesis::Synthesis(const sb_topology* tops, int ntop, const int* topology_index, int nsys_in,
                      const sb_options &options) :
     opt(options), nsys(nsys_in) {
@@ -148,15 +225,7 @@ Synthesis::Synthesis(const sb_topology* tops, int ntop, const int* topology_inde
     }
   }
   for (int t = 0; t < ntop; t++) {
-    const sb_topology &tp = tops[t];
-    if (tp.natom <= 0 || tp.natom > 65535 || tp.charge == nullptr || tp.lj_idx == nullptr ||
-        tp.lja == nullptr || tp.ljb == nullptr || tp.n_lj_types <= 0 ||
-        tp.n_lj_types > 64) {
-      throw Error(SB_ERR_ARGUMENT, "topology " + std::to_string(t) + " is incomplete or too large");
-    }
-    if (opt.igb != SB_GB_NONE && (tp.pb_radii == nullptr || tp.gb_screen == nullptr)) {
-      throw Error(SB_ERR_ARGUMENT, "topology " + std::to_string(t) + " lacks GB radii");
-    }
+    validateTopology(tops[t], opt, t);
   }
   buildLayout(tops, ntop);
   buildUnits();
@@ -236,10 +305,6 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
       for (int i = 0; i < n; i++) {
         for (int e = tp.excl_bounds[i]; e < tp.excl_bounds[i + 1]; e++) {
           const int j = tp.excl_list[e];
-          if (j < 0 || j >= n) {
-            throw Error(SB_ERR_ARGUMENT, "exclusion partner out of range in topology " +
-                        std::to_string(t));
-          }
           if (j == i) continue;
           partners[i].push_back(j);
           partners[j].push_back(i);
@@ -303,9 +368,6 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
     const int base = atom_start[s];
     for (int i = 0; i < tp.natom; i++) {
       h_charge[base + i] = static_cast<float>(tp.charge[i] * sqrt_kc);
-      if (tp.lj_idx[i] < 0 || tp.lj_idx[i] >= tp.n_lj_types) {
-        throw Error(SB_ERR_ARGUMENT, "Lennard-Jones type out of range");
-      }
       h_ljidx[base + i] = tp.lj_idx[i];
       if (opt.igb != SB_GB_NONE) {
         const double rho = tp.pb_radii[i] - gb_offset;
@@ -318,17 +380,7 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
       }
       if (neck) {
         // AtomGraph::setImplicitSolventModel (Topology/atomgraph_setters.cpp:1088-1092)
-        const int idx = static_cast<int>(((tp.pb_radii[i] - 1.0) * 20.0) + 0.5);
-        if (idx < 0 || idx >= opt.neck_table_size) {
-          throw Error(SB_ERR_ARGUMENT, "neck GB needs intrinsic radii within the neck tables "
-                      "(1-2 A for STORMM's 21 x 21 tables)");
-        }
-        if (opt.igb == SB_GB_NECK2 && (tp.gb_alpha == nullptr || tp.gb_beta == nullptr ||
-                                        tp.gb_gamma == nullptr)) {
-          throw Error(SB_ERR_ARGUMENT, "neck GB II takes element-specific alpha, beta and gamma "
-                      "from the topology");
-        }
-        h_neck_idx[base + i] = idx;
+        h_neck_idx[base + i] = neckIndex(tp.pb_radii[i]);
       }
       h64_charge[base + i] = tp.charge[i] * sqrt_kc;
       if (fp64) {
@@ -343,13 +395,8 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
         }
       }
     }
-    auto check_atom = [&](int a) {
-      if (a < 0 || a >= tp.natom) {
-        throw Error(SB_ERR_ARGUMENT, "valence term atom index out of range in topology " +
-                    std::to_string(t));
-      }
-      return static_cast<uint32_t>(a);
-    };
+    // indices were range-checked by validateTopology
+    auto check_atom = [](int a) { return static_cast<uint32_t>(a); };
     for (int b = 0; b < tp.nbond; b++) {
       const uint32_t i = check_atom(tp.bond_atoms[2 * b]);
       const uint32_t j = check_atom(tp.bond_atoms[2 * b + 1]);
@@ -385,9 +432,6 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
       const double scnb = (tp.dihe_scnb != nullptr) ? tp.dihe_scnb[d] : 0.0;
       const uint32_t improper =
         (tp.dihe_improper != nullptr && tp.dihe_improper[d] != 0) ? 0x80000000u : 0u;
-      if (l > 0x7fffu) {
-        throw Error(SB_ERR_UNSUPPORTED, "dihedral atom index above 32767");
-      }
       h_dihe_a.push_back(make_uint4(i | (j << 16), k | (l << 16) | improper, fbits(tp.dihe_amp[d]),
                                     fbits(tp.dihe_freq[d])));
       h_dihe_b.push_back(make_uint4(fbits(std::cos(tp.dihe_phase[d])),
@@ -1042,8 +1086,7 @@ int Synthesis::checkStatus(cudaStream_t stream) {
 // ------------------------------------------------------------------------------------------------
 // Line minimization (MolecularMechanics/hpc_minimization.cu:129-600)
 // ------------------------------------------------------------------------------------------------
-void Synthesis::minimizeBegin(const sb_minimize_controls &ctl, cudaStream_t stream) {
-  rejectTiledMinimization(ctl.kernel);
+void validateMinimizeControls(const sb_minimize_controls &ctl) {
   if (ctl.total_cycles < 0 || ctl.sd_cycles < 0) {
     throw Error(SB_ERR_ARGUMENT, "cycle counts must not be negative");
   }
@@ -1051,9 +1094,18 @@ void Synthesis::minimizeBegin(const sb_minimize_controls &ctl, cudaStream_t stre
       !std::isfinite(ctl.clash_distance) || !std::isfinite(ctl.clash_ratio)) {
     throw Error(SB_ERR_ARGUMENT, "clash-damping cycles, distance and ratio must not be negative");
   }
-  if (!(ctl.initial_step > 0.0) || !(ctl.convergence_rms >= 0.0)) {
+  if (!(ctl.initial_step > 0.0) || !std::isfinite(ctl.initial_step) ||
+      !(ctl.convergence_rms >= 0.0)) {
     throw Error(SB_ERR_ARGUMENT, "initial step must be positive and the RMS target not negative");
   }
+  if (ctl.kernel != SB_MIN_GRAPH && ctl.kernel != SB_MIN_PERSISTENT) {
+    throw Error(SB_ERR_ARGUMENT, "unknown minimization kernel choice");
+  }
+}
+
+void Synthesis::minimizeBegin(const sb_minimize_controls &ctl, cudaStream_t stream) {
+  validateMinimizeControls(ctl);
+  rejectTiledMinimization(ctl.kernel);
   const size_t np = natom_padded;
   if (d_mcycle.p == nullptr) {
     d_xprv.allocate(np);
@@ -1119,9 +1171,6 @@ void Synthesis::minimizeBegin(const sb_minimize_controls &ctl, cudaStream_t stre
   }
   m.queue = d_queue.p;
   m.line = d_line.p;
-  if (ctl.kernel != SB_MIN_GRAPH && ctl.kernel != SB_MIN_PERSISTENT) {
-    throw Error(SB_ERR_ARGUMENT, "unknown minimization kernel choice");
-  }
   min_kernel = ctl.kernel;
   min_total_cycles = ctl.total_cycles;
   cudaCheck(launchMinimizerReset(m, dev, ctl.initial_step, stream), "minimizer reset");

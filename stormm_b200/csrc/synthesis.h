@@ -93,6 +93,15 @@ template <typename T> struct DeviceArray {
   }
 };
 
+// Host checks of a topology before anything is built from it (the constructor of Synthesis and
+// the request server's submit share them): sizes, required arrays, index ranges of
+// Lennard-Jones types, exclusion partners and valence atoms, and the GB and neck parameters the
+// options need.  Throws Error naming topology `which` (or "the topology" when it is negative).
+void validateTopology(const sb_topology &tp, const sb_options &opt, int which);
+
+// Host checks of minimization controls (minimizeBegin and the request server's constructor)
+void validateMinimizeControls(const sb_minimize_controls &ctl);
+
 // Packing of molecules into work units and the launch parameters of each size class
 struct UnitPlan {
   int max_slots_cap = 0;

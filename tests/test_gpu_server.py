@@ -4,6 +4,7 @@ Each served molecule must come back exactly as it does when minimized alone: tra
 per molecule, every sum is order-independent and the minimizer state persists between launches,
 so the coordinates, cycle counts and energies are bit-identical whatever batch, backfill or
 launch split a request gets."""
+import copy
 import time
 
 import numpy as np
@@ -168,3 +169,86 @@ def test_graph_kernel_server_minimizes_a_large_molecule():
         assert r["cycles"] == 30
         assert np.array_equal(xyz, alone.coordinates())
         assert np.array_equal(r["energies"], alone.energies()[0])
+
+
+def _widened_lj(mol, ntypes):
+    """The molecule with its Lennard-Jones tables padded to ntypes types (atoms keep theirs)."""
+    m = copy.deepcopy(mol)
+    nt = mol.lja.shape[0]
+    for name in ("lja", "ljb"):
+        t = np.full((ntypes, ntypes), 1.0)
+        t[:nt, :nt] = getattr(mol, name)
+        setattr(m, name, t)
+    return m
+
+
+def test_bad_requests_fail_alone():
+    """A malformed topology is refused at submit.  A molecule that passes the host checks but
+    cannot be built (its Lennard-Jones tables and atoms need more shared memory than a block
+    has) fails with its error code in the result, alone: the batch it was admitted with is
+    retried one request per batch, and every good request queued around it comes back exactly
+    as it does alone."""
+    good = [synthetic.make_molecule(synthetic._seed(6060, k), n, 0.3)
+            for k, n in enumerate([20, 44, 70, 33, 90])]
+    bad_type = copy.deepcopy(good[0])
+    bad_type.lj_idx = bad_type.lj_idx.copy()
+    bad_type.lj_idx[3] = bad_type.n_lj_types + 2
+    bad_excl = copy.deepcopy(good[1])
+    bad_excl.excl12 = [list(e) for e in bad_excl.excl12]
+    bad_excl.excl12[0].append(bad_excl.natom + 7)
+    unbuildable = _widened_lj(synthetic.make_molecule(synthetic._seed(6060, 9), 2048, 0.1), 64)
+    srv = sb.Server(max_batch_molecules=4, max_batches=2, cycles_per_launch=25, **CONTROLS)
+    ids = {}
+    for k, m in enumerate(good):
+        ids[srv.submit(m)] = ("minimize", m)
+        ids[srv.submit(m, evaluate=True)] = ("evaluate", m)
+        if k == 1:
+            with pytest.raises(sb.StormmB200Error, match="Lennard-Jones type out of range"):
+                srv.submit(bad_type)
+            with pytest.raises(sb.StormmB200Error, match="exclusion partner out of range"):
+                srv.submit(bad_excl, evaluate=True)
+            bad_id = srv.submit(unbuildable, evaluate=True)
+    assert srv.drain(120.0)
+    results = srv.poll()
+    st = srv.stats()
+    srv.close()
+    assert len(results) == len(ids) + 1
+    assert st["failed"] == 1 and st["completed"] == len(ids) + 1 and st["in_flight"] == 0
+    assert st["bytes_in_flight"] == 0.0 and st["batches"] == 0
+    for r, arr in results:
+        if r["request_id"] == bad_id:
+            assert r["status"] != 0 and arr is None and np.isnan(r["energy"])
+            continue
+        assert r["status"] == 0
+        kind, m = ids[r["request_id"]]
+        if kind == "minimize":
+            c_alone, e_alone, cyc_alone, _ = _alone(m)
+            assert np.array_equal(arr, c_alone) and np.array_equal(r["energies"], e_alone)
+            assert r["cycles"] == cyc_alone
+        else:
+            f_alone, e_alone = _evaluated_alone(m)
+            assert np.array_equal(arr, f_alone) and np.array_equal(r["energies"], e_alone)
+
+
+def test_fp64_server_minimizes_with_the_graph_kernel():
+    """An FP64 server runs with the graph minimizer, and each result equals the FP64
+    minimization of the molecule alone."""
+    mols = [synthetic.make_molecule(synthetic._seed(6161, k), n, 0.3)
+            for k, n in enumerate([24, 50, 81])]
+    controls = dict(total_cycles=40, sd_cycles=10, convergence_rms=0.0, kernel=sb.MIN_GRAPH)
+    opts = sb.default_options(precision=sb.PRECISION_DOUBLE)
+    srv = sb.Server(cycles_per_launch=10, options=opts, **controls)
+    ids = {srv.submit(m): m for m in mols}
+    assert srv.drain(120.0)
+    results = srv.poll()
+    srv.close()
+    assert len(results) == len(mols)
+    for r, xyz in results:
+        m = ids[r["request_id"]]
+        syn = sb.Synthesis([m], options=sb.default_options(precision=sb.PRECISION_DOUBLE))
+        syn.set_coordinates(m.coords)
+        syn.minimize(**controls)
+        assert r["status"] == 0
+        assert np.array_equal(xyz, syn.coordinates())
+        assert np.array_equal(r["energies"], syn.energies()[0])
+        syn.close()

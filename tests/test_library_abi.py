@@ -40,3 +40,23 @@ def test_null_handle_is_an_error():
     rc = lib.sb_evaluate(None, 7, 1, 1, None)
     assert rc == -1
     assert b"null" in lib.sb_last_error()
+
+
+def test_server_checks_its_controls_on_the_host():
+    """The request server refuses bad minimization controls and an FP64 server without the
+    graph minimizer when it is created, before any device is touched."""
+    with pytest.raises(stormm_b200.StormmB200Error, match="initial step"):
+        stormm_b200.Server(initial_step=-1.0)
+    with pytest.raises(stormm_b200.StormmB200Error, match="clash-damping"):
+        stormm_b200.Server(clash_cycles=5, clash_distance=-0.2)
+    with pytest.raises(stormm_b200.StormmB200Error, match="graph minimizer"):
+        stormm_b200.Server(options=stormm_b200.default_options(
+            precision=stormm_b200.PRECISION_DOUBLE), kernel=stormm_b200.MIN_PERSISTENT)
+
+
+def test_served_result_layout_matches_the_header():
+    """The Python mirror of sb_served_result and sb_server_stats has the C layout."""
+    r = stormm_b200.ServedResult
+    assert r.status.offset == 24 and r.rms_force.offset == 32
+    assert ctypes.sizeof(r) == 32 + 8 + 8 + 8 * 16 + 3 * 8
+    assert stormm_b200.ServerStats.failed.offset == 24
