@@ -514,7 +514,10 @@ int sb_autotune(sb_synthesis* syn, int what, int* max_atoms_per_unit, int* max_t
  * that has no synthesis handle and so no staging buffer.
  * Limit: nsys * stride <= 65,536 values (4,096 systems of 16 slots); larger requests return
  * SB_ERR_ARGUMENT.  The first call on each device (nsys = 0 does only this) looks up the
- * scratch address with that device current: make it before any stream capture begins.
+ * scratch address with that device current: make it before any stream capture begins.  The
+ * address is kept with its CUDA context; a call in another context (after cudaDeviceReset, or
+ * with a context of the caller's own current) looks it up again, so make a set-up call there
+ * too before a capture.
  * Nothing has to be zeroed first.  Calls on one device share the scratch: calls that overlap
  * in time race, so order them.  Synchronizes the stream before returning. */
 int sb_energies_to_host_static(const int64_t* d_energies, int nsys, int stride, int nrg_bits,

@@ -11,10 +11,14 @@
 // synthesis.
 //
 // The scratch holds kScratchValues doubles (512 KiB).  The first call on each device looks up
-// its address with cudaGetSymbolAddress while that device is current and keeps it for later
-// calls.  Nothing in the scratch needs to start at zero: every value a call reads back was
-// written by that call's kernel.  All calls on one device share the one array, so calls that
-// overlap in time (different streams or host threads) race on it; order them.
+// its address with cudaGetSymbolAddress while that device is current and keeps it, with the
+// CUDA context it belongs to, for later calls; a call made in another context (the device was
+// reset, or the caller made a context of its own current) looks the address up again, since
+// the module holding the array is loaded anew in every context.  Nothing in the scratch needs
+// to start at zero: every value a call reads back was written by that call's kernel.  All calls
+// on one device share the one array, so calls that overlap in time (different streams or host
+// threads) race on it; order them.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -38,14 +42,43 @@ static __device__ __align__(256) double g_energy_scratch[kScratchValues];
 
 std::mutex g_scratch_mutex;
 double* g_scratch_address[kMaxDevices] = {};
+CUcontext g_scratch_context[kMaxDevices] = {};
 
-// Address of this device's scratch; looked up once per device with that device current
+// The calling thread's current CUDA context (null before the runtime has made one current),
+// through the driver's cuCtxGetCurrent as the runtime hands it out, so that the library needs
+// no link to the driver library
+CUcontext currentContext() {
+  using CtxGetCurrent = CUresult (*)(CUcontext*);
+  static const CtxGetCurrent get = []() -> CtxGetCurrent {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult found = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &found) !=
+        cudaSuccess || found != cudaDriverEntryPointSuccess) {
+      return nullptr;
+    }
+    return reinterpret_cast<CtxGetCurrent>(fn);
+  }();
+  if (get == nullptr) {
+    throw Error(SB_ERR_CUDA, "cuCtxGetCurrent is not available from the CUDA runtime");
+  }
+  CUcontext ctx = nullptr;
+  if (get(&ctx) != CUDA_SUCCESS) {
+    throw Error(SB_ERR_CUDA, "cuCtxGetCurrent failed");
+  }
+  return ctx;
+}
+
+// Address of this device's scratch in the current context: looked up once per device and
+// context, with that device current
 double* scratchAddress(int device) {
   std::lock_guard<std::mutex> lock(g_scratch_mutex);
-  if (g_scratch_address[device] == nullptr) {
+  const CUcontext ctx = currentContext();
+  if (g_scratch_address[device] == nullptr || ctx == nullptr ||
+      ctx != g_scratch_context[device]) {
     void* p = nullptr;
     cudaCheck(cudaGetSymbolAddress(&p, g_energy_scratch), "cudaGetSymbolAddress(energy scratch)");
     g_scratch_address[device] = static_cast<double*>(p);
+    g_scratch_context[device] = currentContext();   // current now, if it was not before
   }
   return g_scratch_address[device];
 }
