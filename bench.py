@@ -19,14 +19,20 @@ of N x 1,024 (and N x 4,096) molecules, partitioned by pair count largest first
 (stormm_b200.sharding.partition_lpt): weak scaling with no collective on the data path; the
 only collectives are the barriers around timed regions and the max over ranks of the timing.
 Rank 0 prints the details of every leg on one line and the summary on the last line.
+
+Comparison points printed beside the numbers: STORMM's CPU build on the host cores
+(cpu_baseline, oracle/cpu_baseline.py) and, where oracle/ref_gpu/Makefile has built it,
+STORMM's own CUDA path on the same GPU and molecules (reference_gpu, oracle/gpu_reference.py).
 """
 from __future__ import annotations
 
 import argparse
+import functools
 import json
 import os
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 
@@ -71,6 +77,7 @@ def _args():
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--no-errors", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true")
     return ap.parse_args()
 
 
@@ -143,6 +150,7 @@ def _shard(sizes, world, rank):
     return sharding.partition_lpt(sizes, world)[rank]
 
 
+@functools.lru_cache(maxsize=None)
 def single_point_molecules(world, rank):
     from stormm_b200 import synthetic
     seed = synthetic.SEED_BASE + 1
@@ -152,6 +160,7 @@ def single_point_molecules(world, rank):
                                     name=f"S{k}") for k in idx]
 
 
+@functools.lru_cache(maxsize=None)
 def minimization_molecules(world, rank):
     from stormm_b200 import synthetic
     seed = synthetic.SEED_BASE + 2
@@ -469,6 +478,7 @@ def bench_minimization(args, world, rank, local, flush):
                 "h2d_bytes_per_step": int(xyz.size * 8),
                 "d2h_bytes_per_step": int(c.size * 8 + e.size * 8)},
         "mean_energy_drop": (float(np.mean(e_start - e_final)) if e_start is not None else None),
+        "mean_final_energy": float(np.mean(e_final)),
         "kernel": "graph (one CUDA graph per cycle: 4 batched evaluations + 4 line-search kernels)",
         "persistent_kernel_value": persistent,
         "fp64_mode": fp64_mode,
@@ -672,6 +682,46 @@ def _cpu_leg(name, seconds):
                 "sample": str(exc)[:200]}
 
 
+def _reference_gpu_leg(args, sp, mn):
+    """STORMM's own CUDA path (oracle/_ref_gpu, built from the reference sources by
+    oracle/ref_gpu/Makefile) on the same GPU and the same molecules: launchNonbonded +
+    launchValence over the batched single-point workload and launchMinimization over the
+    minimization workload, each in a subprocess that maps only STORMM's library and CUDA's.
+    Reported beside this path's numbers; a failure is reported, not fatal."""
+    from oracle import gpu_reference as gref
+    if not gref.available():
+        return {"available": False, "why": "reference CUDA build absent (oracle/ref_gpu/Makefile)"}
+    out = {"available": True,
+           "build": "STORMM's sources with its CUDA path, nvcc -O3 --use_fast_math sm_100",
+           "precision": "STORMM PrecisionModel::SINGLE (FP32, split fixed-point accumulation)"}
+    try:
+        lst = gref.write_inputs(f"single_point_{NSYS}", single_point_molecules(1, 0))
+        r = gref.time_evaluations(lst, max(20, args.steps))
+        out["single_point"] = {
+            "value": r["value"], "unit": "force-evals/s", "ms_per_eval": r["ms_per_eval"],
+            "systems": r["systems"], "atoms": r["atoms"], "evals": r["evals"],
+            "timing": "CUDA events over back-to-back evaluations, L2 not flushed (inputs fit "
+                      "in L2), the launches of the first stage of its minimizer's cycle",
+            "ratio_this_path": sp["value"] / r["value"]}
+    except Exception as exc:  # reported, not fatal
+        out["single_point"] = {"error": str(exc)[:300]}
+    if mn is not None:
+        try:
+            lst = gref.write_inputs(f"minimization_{MIN_NSYS}", minimization_molecules(1, 0))
+            with tempfile.TemporaryDirectory() as tmp:
+                r = gref.minimize(lst, os.path.join(tmp, "min.bin"), MIN_CYCLES, MIN_SD_CYCLES,
+                                  ntpr=MIN_CYCLES)
+            out["minimization"] = {
+                "value": r["value"], "unit": "minimizations/s", "ms": r["ms"],
+                "systems": r["systems"], "cycles": MIN_CYCLES, "sd_cycles": MIN_SD_CYCLES,
+                "timing": "wall time of one launchMinimization call (its set-up included)",
+                "mean_final_energy": float(np.mean(r["final_terms"].sum(axis=1))),
+                "ratio_this_path": mn["value"] / r["value"]}
+        except Exception as exc:  # reported, not fatal
+            out["minimization"] = {"error": str(exc)[:300]}
+    return out
+
+
 def main_rank(args):
     world, rank, local = _dist()
     import torch
@@ -702,12 +752,16 @@ def main_rank(args):
             mn["cpu_baseline"] = _cpu_leg("minimization", args.cpu_seconds)
         if large is not None:
             large["cpu_baseline"] = _cpu_leg("large", args.cpu_seconds)
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        ref_gpu = _reference_gpu_leg(args, sp, mn)
 
     if rank == 0:
         info = sp["info"]
         natoms = sp["natoms"]
         detail = {"detail": "bench legs in full (the summary line follows)",
-                  "minimization": mn, "served": served, "large": large}
+                  "minimization": mn, "served": served, "large": large,
+                  "reference_gpu": ref_gpu}
         print(json.dumps(detail, default=float), flush=True)
         line = {
             "metric": METRIC, "value": sp["value"], "unit": "force-evals/s", "n_gpus": world,
@@ -751,6 +805,10 @@ def main_rank(args):
                 "batched_speedup": mn["batched_speedup"],
                 "errors_vs_fp64": mn["errors"],
                 "cpu_baseline": (mn.get("cpu_baseline") or {}).get("value")}
+        if ref_gpu is not None and ref_gpu.get("available"):
+            line["reference_gpu"] = {
+                k: {f: v.get(f) for f in ("value", "ratio_this_path", "error") if f in v}
+                for k, v in ref_gpu.items() if isinstance(v, dict)}
         print(json.dumps(line, default=float), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
