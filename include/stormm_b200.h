@@ -389,7 +389,8 @@ int sb_server_submit_evaluation(sb_server* srv, const sb_topology* top, const do
  * without them.  *count receives the number returned. */
 int sb_server_poll(sb_server* srv, sb_served_result* results, int max_results, double* xyz,
                    long long xyz_capacity, int* count);
-/* Wait until nothing is queued or in flight: SB_OK, or SB_TIMEOUT after timeout_seconds */
+/* Wait until nothing is queued or in flight and every batch's device memory is released: SB_OK,
+ * or SB_TIMEOUT after timeout_seconds */
 int sb_server_drain(sb_server* srv, double timeout_seconds);
 int sb_server_get_stats(sb_server* srv, sb_server_stats* stats);
 /* Stops the worker after the launches in flight and releases everything */
@@ -488,6 +489,49 @@ int sb_amber_topology_destroy(sb_amber_topology* top);
 /* Coordinates of an Amber ASCII coordinate or restart file (STORMM's PhaseSpace(file_name)):
  * 3 * natom doubles, interlaced x, y, z; the file's atom count must equal natom */
 int sb_read_amber_coordinates(const char* inpcrd_path, int natom, double* xyz);
+/* Write coordinates (3 * natom doubles, interlaced) as an Amber input-coordinate file, the
+ * format STORMM's PhaseSpace::exportToFile writes for CoordinateFileKind::AMBER_INPCRD
+ * (Trajectory/write_frame.cpp:54-160): a title line, the atom count as %7d, then six %12.7f
+ * values a line; the checkpoint of a minimized structure.  title may be NULL. */
+int sb_write_amber_coordinates(const char* inpcrd_path, const char* title, int natom,
+                               const double* xyz);
+
+/* ------------------------------------------------------------------------------------------ */
+/* MDL MOL / SD files                                                                          */
+/* ------------------------------------------------------------------------------------------ */
+/* Compounds of an SD file (or one MOL file), V2000 format, as STORMM's MdlMol reads them
+ * (MoleculeFormat/mdlmol.cpp:47-324, readStructureDataFile at :1821-1880): coordinates, element
+ * symbols and atomic numbers, formal charges (atom-block codes, replaced by "M  CHG"
+ * properties), bonds with their MDL types, and the compound's data items.  V3000 compounds are
+ * refused (SB_ERR_UNSUPPORTED).  Host only. */
+typedef struct sb_sdf sb_sdf;
+
+typedef struct {
+  const char* title;
+  int natom;
+  const double* xyz;                 /* 3 * natom, interlaced, Angstrom */
+  const int* atomic_number;          /* natom (0 for a symbol that is no element) */
+  const int* formal_charge;          /* natom, electrons */
+  const char* symbols;               /* 4 characters per atom, NUL padded */
+  int nbond;
+  const int* bond_i;                 /* nbond, 0-based */
+  const int* bond_j;
+  const int* bond_order;             /* MDL bond type: 1-3 single to triple, 4 aromatic, ... */
+  int n_items;                       /* data items: "> <name>" and the lines that follow */
+  const char* const* item_names;
+  const char* const* item_contents;  /* lines joined by '\n' */
+} sb_sdf_view;
+
+int sb_read_sdf(const char* path, sb_sdf** out);
+int sb_sdf_compound_count(const sb_sdf* sdf, int* count);
+/* Pointers into the compound's own arrays, valid until sb_sdf_destroy */
+int sb_sdf_compound(const sb_sdf* sdf, int index, sb_sdf_view* view);
+int sb_sdf_destroy(sb_sdf* sdf);
+/* Write one compound in the V2000 format (coordinates %10.4f as STORMM's MdlMol writes them,
+ * charges as "M  CHG" properties, data items, closing "$$$$"), replacing the file or appended
+ * to it; the element symbols come from symbols, or from atomic_number when symbols is NULL.
+ * Up to 999 atoms and 999 bonds. */
+int sb_write_sdf_compound(const char* path, int append, const sb_sdf_view* compound);
 
 /* ------------------------------------------------------------------------------------------ */
 /* Autotuning                                                                                  */

@@ -275,13 +275,13 @@ public:
     const auto until = std::chrono::steady_clock::now() +
                        std::chrono::duration_cast<std::chrono::steady_clock::duration>(
                            std::chrono::duration<double>(timeout));
-    while (!(pending_.empty() && in_flight_ == 0) && error_.empty()) {
+    while (!idle() && error_.empty()) {
       if (idle_cv_.wait_until(lock, until) == std::cv_status::timeout) {
         break;
       }
     }
     failIfBroken();
-    return pending_.empty() && in_flight_ == 0;
+    return idle();
   }
 
   sb_server_stats stats() {
@@ -301,6 +301,11 @@ public:
 private:
   double now() const {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0_).count();
+  }
+
+  // Nothing queued, in flight or holding device memory (called with mu_ held)
+  bool idle() const {
+    return pending_.empty() && in_flight_ == 0 && nbatches_ == 0;
   }
 
   void failIfBroken() const {
@@ -537,7 +542,7 @@ private:
     in_flight_ -= static_cast<int>(out.size());
     completed_ += static_cast<long long>(out.size());
     failed_ += static_cast<long long>(out.size());
-    if (pending_.empty() && in_flight_ == 0) {
+    if (idle()) {
       idle_cv_.notify_all();
     }
   }
@@ -585,7 +590,7 @@ private:
     }
     in_flight_ -= n;
     completed_ += n;
-    if (pending_.empty() && in_flight_ == 0) {
+    if (idle()) {
       idle_cv_.notify_all();
     }
   }
@@ -683,6 +688,9 @@ private:
     }
     nbatches_--;
     cv_.notify_all();
+    if (idle()) {
+      idle_cv_.notify_all();
+    }
   }
 
   sb_server_options opt_;

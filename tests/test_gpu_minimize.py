@@ -314,3 +314,65 @@ def test_line_search_steps_need_a_begun_minimization():
         syn.conjugate_gradient()
     with pytest.raises(sb.StormmB200Error):
         syn.line_advance(0)
+
+
+def _stormm_gpu_case(case):
+    """Molecules, STORMM's starting coordinates and its launchMinimization histories
+    (tests/golden/gpu_minimize_<case>.npz, from STORMM's CUDA build on a B200)."""
+    g = load(f"gpu_minimize_{case}.npz")
+    mols = [synthetic.make_molecule(synthetic._seed(int(g["seed"]), k), int(n),
+                                    noise=float(g["noise"]))
+            for k, n in enumerate(g["sizes"])]
+    return g, mols
+
+
+def _minimize_like(g, mols, precision):
+    syn = sb.Synthesis(mols, precision=precision)
+    syn.set_coordinates(g["start_coords"])
+    clash = int(g["clash_cycles"]) > 0
+    syn.minimize(record_history=True, total_cycles=int(g["cycles"]), sd_cycles=int(g["sd_cycles"]),
+                 clash_cycles=int(g["clash_cycles"]),
+                 clash_distance=float(g["clash_distance"]) if clash else 0.0,
+                 clash_ratio=float(g["clash_ratio"]) if clash else 0.0, kernel=sb.MIN_GRAPH)
+    h = syn.minimize_history()
+    assert syn.status() == 0
+    syn.close()
+    return h
+
+
+@pytest.mark.parametrize("case", ["fp64", "fp64_clash"])
+def test_fp64_minimizer_follows_stormm_launch_minimization(case):
+    """The FP64 mode against STORMM's own launchMinimization in PrecisionModel::DOUBLE on a
+    B200, 12 molecules of 24-200 atoms over 200 cycles: the energy at the start of each of the
+    first 20 cycles within 1e-7 relative (both runs take the same line-search decisions there),
+    and the final energy within 1e-4 of the energy drop (rounding later steers the runs apart,
+    as it does STORMM's run and the FP64 oracle's)."""
+    g, mols = _stormm_gpu_case(case)
+    h = _minimize_like(g, mols, sb.PRECISION_DOUBLE)
+    s = g["history"]
+    rel = np.abs(h[:, :21] - s[:, :21]) / np.maximum(np.abs(s[:, :21]), 1.0)
+    assert rel.max() < 1e-7, (np.unravel_index(np.argmax(rel), rel.shape), rel.max())
+    drop = s[:, 0] - s[:, -1]
+    assert (np.abs(h[:, -1] - s[:, -1]) <= 1e-4 * drop).all(), np.abs(h[:, -1] - s[:, -1]) / drop
+
+
+@pytest.mark.parametrize("case", ["fp32", "fp32_clash"])
+def test_fp32_minimizer_follows_stormm_launch_minimization(case):
+    """The FP32 path against STORMM's launchMinimization in PrecisionModel::SINGLE on a B200:
+    each FP32 run starts within the single-point energy bound of the FP64 energy and follows
+    the FP64 trajectory (STORMM's own FP64 run, gpu_minimize_fp64*) to 1e-5 relative over the
+    first ten cycles, as STORMM's FP32 run does except where rounding flips an early
+    line-search decision (one molecule at cycle 2); after 200 cycles the final energies of the
+    two FP32 runs lie within 1e-3 of the energy drop."""
+    g, mols = _stormm_gpu_case(case)
+    g64 = load(f"gpu_minimize_{case.replace('fp32', 'fp64')}.npz")
+    h = _minimize_like(g, mols, sb.PRECISION_SINGLE)
+    s, s64 = g["history"], g64["history"]
+    ref = np.maximum(np.abs(s64[:, :11]), 1.0)
+    ours = np.abs(h[:, :11] - s64[:, :11]) / ref
+    theirs = np.abs(s[:, :11] - s64[:, :11]) / ref
+    follows = theirs.max(axis=1) < 1e-5          # molecules STORMM's FP32 run keeps on track
+    assert follows.sum() >= len(mols) - 1
+    assert ours[follows].max() < 1e-5, (ours.max(axis=1), theirs.max(axis=1))
+    drop = s[:, 0] - s[:, -1]
+    assert (np.abs(h[:, -1] - s[:, -1]) <= 1e-3 * drop).all(), np.abs(h[:, -1] - s[:, -1]) / drop

@@ -138,3 +138,40 @@ def test_oracle_matches_stormm_on_the_single_point_workload_sample():
         np.testing.assert_allclose(r["energies"], g["energy_terms"][j], rtol=1e-11, atol=1e-10)
         f = g["forces"][offs[j]:offs[j + 1]]
         assert np.sqrt(((r["forces"] - f) ** 2).sum() / (f ** 2).sum()) < 1e-11
+
+
+def _gpu_minimizer_case(case):
+    """Molecules, starting coordinates and STORMM's launchMinimization histories of one case of
+    tests/golden/gpu_minimize_<case>.npz (tests/golden/make_gpu_minimizer_golden.py)."""
+    from stormm_b200 import synthetic
+    g = _load(os.path.join(GOLDEN, f"gpu_minimize_{case}.npz"))
+    start = g["start_coords"].reshape(-1, 3)
+    mols, coords, off = [], [], 0
+    for k, n in enumerate(g["sizes"]):
+        mols.append(synthetic.make_molecule(synthetic._seed(int(g["seed"]), k), int(n),
+                                            noise=float(g["noise"])))
+        coords.append(start[off:off + n])
+        off += n
+    return g, mols, coords
+
+
+@pytest.mark.parametrize("case", ["fp64", "fp64_clash"])
+def test_minimizer_follows_stormm_gpu_minimizer(case):
+    """The oracle's FP64 restatement of STORMM's GPU line minimizer against STORMM's own
+    launchMinimization in PrecisionModel::DOUBLE on a B200 (12 molecules of 24-200 atoms, 200
+    cycles, 50 steepest descent; with 25 clash-damped cycles in the second case): the same
+    energy at the start of every one of the first 20 cycles to 1e-7 relative, while both take
+    the same line-search decisions, and final energies within 1e-4 of the energy drop once
+    rounding has steered the two runs apart."""
+    g, mols, coords = _gpu_minimizer_case(case)
+    cc = int(g["clash_cycles"])
+    for k, (m, c0) in enumerate(zip(mols, coords)):
+        _, h = oracle.from_molecule(m).minimize(c0, int(g["cycles"]), int(g["sd_cycles"]),
+                                                clash_cycles=cc,
+                                                clash_distance=float(g["clash_distance"]),
+                                                clash_ratio=float(g["clash_ratio"]))
+        s = g["history"][k]
+        rel = np.abs(h[:21] - s[:21]) / np.maximum(np.abs(s[:21]), 1.0)
+        assert rel.max() < 1e-7, (k, int(np.argmax(rel)), rel.max())
+        drop = s[0] - s[-1]
+        assert drop > 0 and abs(h[-1] - s[-1]) <= 1e-4 * drop, (k, h[-1], s[-1])
