@@ -19,6 +19,12 @@
 //       prints "evals=<n> seconds=<t>".  With --minimize N it instead runs N-cycle minimizations
 //       and prints "minimizations=<n> seconds=<t>".
 //
+//   sdf <file> <out.bin>
+//       STORMM's MdlMol parse of each compound of an SD / MOL file (readStructureDataFile).
+//   writecrd <in.inpcrd> <out.inpcrd>
+//       The coordinates of an Amber input-coordinate file written back by STORMM's
+//       PhaseSpace::exportToFile (CoordinateFileKind::AMBER_INPCRD).
+//
 //   nbwu <list-file> <out.bin> [--init-task N]
 //       STORMM's nonbonded work units (Synthesis/nonbonded_workunit.cpp) for a synthesis: each
 //       line of <list-file> is "<prmtop> <system count>", the systems laid out topology by
@@ -43,6 +49,7 @@
 #include "copyright.h"
 #include "Constants/generalized_born.h"
 #include "Constants/symbol_values.h"
+#include "MoleculeFormat/mdlmol.h"
 #include "MolecularMechanics/minimization.h"
 #include "MolecularMechanics/mm_evaluation.h"
 #include "Namelists/nml_minimize.h"
@@ -56,6 +63,7 @@
 #include "Synthesis/synthesis_abstracts.h"
 #include "Topology/atomgraph.h"
 #include "Trajectory/phasespace.h"
+#include "Trajectory/trajectory_enumerators.h"
 
 using namespace stormm;
 using namespace stormm::energy;
@@ -493,6 +501,82 @@ int runTime(const std::string &list_file, double seconds, const Options &opt) {
   return 0;
 }
 
+// STORMM's MdlMol parse of every compound of an SD / MOL file: per compound its atom and bond
+// counts, coordinates, atomic numbers, formal charges and element symbols, the bonds as
+// STORMM writes them back (writeMdl, V2000 bond lines: 1-based atoms and the bond type), and
+// the data items' names and lines
+int runSdf(const std::string &path, const std::string &out) {
+  const std::vector<structure::MdlMol> mols = structure::readStructureDataFile(path);
+  RecordWriter rw(out);
+  rw.iscalar("compounds", static_cast<int>(mols.size()));
+  for (size_t m = 0; m < mols.size(); m++) {
+    const std::string p = "c" + std::to_string(m) + "_";
+    const structure::MdlMol &mol = mols[m];
+    const int n = mol.getAtomCount();
+    rw.iscalar(p + "natom", n);
+    std::vector<double> xyz;
+    for (int i = 0; i < n; i++) {
+      const double3 c = mol.getCoordinates(i);
+      xyz.push_back(c.x);
+      xyz.push_back(c.y);
+      xyz.push_back(c.z);
+    }
+    rw.d(p + "xyz", xyz);
+    rw.i(p + "znum", mol.getAtomicNumbers());
+    rw.i(p + "charge", mol.getFormalCharges());
+    std::vector<int> sym;
+    for (int i = 0; i < n; i++) {
+      const char4 c = mol.getAtomSymbol(i);
+      sym.push_back(c.x);
+      sym.push_back(c.y);
+      sym.push_back(c.z);
+      sym.push_back(c.w);
+    }
+    rw.i(p + "symbols", sym);
+    // bond block of STORMM's own V2000 rendering: the fourth line after the atoms onward
+    const std::string text = mol.writeMdl(structure::MdlMolVersion::V2000);
+    std::vector<std::string> lines;
+    size_t a = 0;
+    while (a < text.size()) {
+      const size_t b = text.find('\n', a);
+      lines.push_back(text.substr(a, (b == std::string::npos ? text.size() : b) - a));
+      a = (b == std::string::npos) ? text.size() : b + 1;
+    }
+    std::vector<int> bonds;
+    for (int k = 0; k < mol.getBondCount(); k++) {
+      const std::string &ln = lines[4 + n + k];
+      bonds.push_back(std::atoi(ln.substr(0, 3).c_str()) - 1);
+      bonds.push_back(std::atoi(ln.substr(3, 3).c_str()) - 1);
+      bonds.push_back(std::atoi(ln.substr(6, 3).c_str()));
+    }
+    rw.i(p + "bonds", bonds);
+    rw.iscalar(p + "items", mol.getDataItemCount());
+    for (int k = 0; k < mol.getDataItemCount(); k++) {
+      const std::string q = p + "item" + std::to_string(k) + "_";
+      const std::string name = mol.getDataItemName(k);
+      std::vector<int> chars(name.begin(), name.end());
+      rw.i(q + "name", chars);
+      std::string content;
+      for (const std::string &line : mol.getDataItemContent(k)) {
+        if (!content.empty()) content += '\n';
+        content += line;
+      }
+      std::vector<int> cchars(content.begin(), content.end());
+      rw.i(q + "content", cchars);
+    }
+  }
+  return 0;
+}
+
+// An Amber input-coordinate file as STORMM writes it (PhaseSpace::exportToFile,
+// CoordinateFileKind::AMBER_INPCRD) after reading the coordinates of another one
+int runWriteCrd(const std::string &in, const std::string &out) {
+  PhaseSpace ps(in, CoordinateFileKind::AMBER_INPCRD);
+  ps.exportToFile(out, 0.0, TrajectoryKind::POSITIONS, CoordinateFileKind::AMBER_INPCRD,
+                  PrintSituation::OVERWRITE);
+  return 0;
+}
+
 int runNbwu(const std::string &list_file, const std::string &out, const Options &opt,
              int init_task) {
   std::ifstream lst(list_file);
@@ -594,6 +678,12 @@ int main(int argc, char* argv[]) {
   }
   if (mode == "nbwu" && pos.size() == 2) {
     return runNbwu(pos[0], pos[1], opt, init_task);
+  }
+  if (mode == "sdf" && pos.size() == 2) {
+    return runSdf(pos[0], pos[1]);
+  }
+  if (mode == "writecrd" && pos.size() == 2) {
+    return runWriteCrd(pos[0], pos[1]);
   }
   if (mode == "time" && pos.size() == 2) {
     return runTime(pos[0], std::atof(pos[1].c_str()), opt);

@@ -109,6 +109,17 @@ class AmberView(ctypes.Structure):
     ]
 
 
+class SdfView(ctypes.Structure):
+    _fields_ = [
+        ("title", ctypes.c_char_p), ("natom", ctypes.c_int), ("xyz", ctypes.c_void_p),
+        ("atomic_number", ctypes.c_void_p), ("formal_charge", ctypes.c_void_p),
+        ("symbols", ctypes.c_void_p), ("nbond", ctypes.c_int), ("bond_i", ctypes.c_void_p),
+        ("bond_j", ctypes.c_void_p), ("bond_order", ctypes.c_void_p), ("n_items", ctypes.c_int),
+        ("item_names", ctypes.POINTER(ctypes.c_char_p)),
+        ("item_contents", ctypes.POINTER(ctypes.c_char_p)),
+    ]
+
+
 class StormmB200Error(RuntimeError):
     pass
 
@@ -186,6 +197,14 @@ def library() -> ctypes.CDLL:
             "sb_amber_set_implicit_solvent": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
             "sb_amber_topology_destroy": (ctypes.c_int, [vp]),
             "sb_read_amber_coordinates": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, vp]),
+            "sb_write_amber_coordinates": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p,
+                                                          ctypes.c_int, vp]),
+            "sb_read_sdf": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(vp)]),
+            "sb_sdf_compound_count": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int)]),
+            "sb_sdf_compound": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(SdfView)]),
+            "sb_sdf_destroy": (ctypes.c_int, [vp]),
+            "sb_write_sdf_compound": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int,
+                                                     ctypes.POINTER(SdfView)]),
             "sb_static_exclusion_mask_synthesis": (ctypes.c_int, [ctypes.POINTER(Topology),
                                                                   ctypes.c_int, vp, ctypes.c_int,
                                                                   vp, vp, vp, vp, vp, vp, vp]),
@@ -447,6 +466,92 @@ def read_amber_coordinates(path, natom):
     _check(library().sb_read_amber_coordinates(os.fsencode(str(path)), int(natom),
                                                xyz.ctypes.data), "sb_read_amber_coordinates")
     return xyz.reshape(natom, 3)
+
+
+def write_amber_coordinates(path, xyz, title=""):
+    """Write (natom, 3) coordinates as an Amber input-coordinate file (STORMM's AMBER_INPCRD)."""
+    c = np.ascontiguousarray(np.asarray(xyz, dtype=np.float64).reshape(-1))
+    _check(library().sb_write_amber_coordinates(os.fsencode(str(path)), title.encode(),
+                                                c.size // 3, c.ctypes.data),
+           "sb_write_amber_coordinates")
+
+
+def read_sdf(path):
+    """Compounds of an SD / MOL file (V2000) as dicts: title, xyz (natom, 3), atomic_number,
+    formal_charge, symbols, bonds (nbond, 3: i, j, MDL type), items {name: text}."""
+    lib = library()
+    h = ctypes.c_void_p()
+    _check(lib.sb_read_sdf(os.fsencode(str(path)), ctypes.byref(h)), "sb_read_sdf")
+    try:
+        n = ctypes.c_int()
+        _check(lib.sb_sdf_compound_count(h, ctypes.byref(n)), "sb_sdf_compound_count")
+        out = []
+        for k in range(n.value):
+            v = SdfView()
+            _check(lib.sb_sdf_compound(h, k, ctypes.byref(v)), "sb_sdf_compound")
+            na, nb = v.natom, v.nbond
+
+            def arr(ptr, count, ct, dt):
+                if count == 0 or not ptr:
+                    return np.zeros(0, dtype=dt)
+                return np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ct)),
+                                             shape=(count,)).astype(dt)
+            sym = ctypes.string_at(v.symbols, 4 * na)
+            bonds = np.stack([arr(v.bond_i, nb, ctypes.c_int, np.int32),
+                              arr(v.bond_j, nb, ctypes.c_int, np.int32),
+                              arr(v.bond_order, nb, ctypes.c_int, np.int32)], axis=1)
+            out.append({
+                "title": v.title.decode(errors="replace"),
+                "xyz": arr(v.xyz, 3 * na, ctypes.c_double, np.float64).reshape(na, 3),
+                "atomic_number": arr(v.atomic_number, na, ctypes.c_int, np.int32),
+                "formal_charge": arr(v.formal_charge, na, ctypes.c_int, np.int32),
+                "symbols": [sym[4 * a:4 * a + 4].rstrip(b"\0").decode() for a in range(na)],
+                "bonds": bonds,
+                "items": {v.item_names[i].decode(): v.item_contents[i].decode()
+                          for i in range(v.n_items)},
+            })
+        return out
+    finally:
+        lib.sb_sdf_destroy(h)
+
+
+def write_sdf(path, compound, append=False):
+    """Write one compound (a dict as read_sdf returns; symbols or atomic_number, optional
+    formal_charge, bonds and items) as a V2000 SD entry."""
+    na = len(compound["xyz"])
+    xyz = np.ascontiguousarray(np.asarray(compound["xyz"], dtype=np.float64).reshape(-1))
+    keep = [xyz]
+    v = SdfView()
+    v.title = compound.get("title", "").encode()
+    v.natom = na
+    v.xyz = xyz.ctypes.data
+    if compound.get("symbols") is not None:
+        buf = ctypes.create_string_buffer(b"".join(s.encode()[:3].ljust(4, b"\0")
+                                                   for s in compound["symbols"]), 4 * na)
+        keep.append(buf)
+        v.symbols = ctypes.addressof(buf)
+    if compound.get("atomic_number") is not None:
+        z = np.ascontiguousarray(compound["atomic_number"], dtype=np.int32)
+        keep.append(z)
+        v.atomic_number = z.ctypes.data
+    if compound.get("formal_charge") is not None:
+        q = np.ascontiguousarray(compound["formal_charge"], dtype=np.int32)
+        keep.append(q)
+        v.formal_charge = q.ctypes.data
+    bonds = np.asarray(compound.get("bonds", np.zeros((0, 3))), dtype=np.int32).reshape(-1, 3)
+    v.nbond = len(bonds)
+    cols = [np.ascontiguousarray(bonds[:, c]) for c in range(3)]
+    keep.extend(cols)
+    if len(bonds):
+        v.bond_i, v.bond_j, v.bond_order = (c.ctypes.data for c in cols)
+    items = compound.get("items", {})
+    names = (ctypes.c_char_p * max(1, len(items)))(*[k.encode() for k in items])
+    texts = (ctypes.c_char_p * max(1, len(items)))(*[t.encode() for t in items.values()])
+    v.n_items = len(items)
+    v.item_names = names
+    v.item_contents = texts
+    _check(library().sb_write_sdf_compound(os.fsencode(str(path)), int(bool(append)),
+                                           ctypes.byref(v)), "sb_write_sdf_compound")
 
 
 def minimize_controls(**overrides) -> MinimizeControls:

@@ -40,7 +40,9 @@
 #include <cctype>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <fstream>
 #include <map>
 #include <sstream>
@@ -876,5 +878,48 @@ extern "C" int sb_read_amber_coordinates(const char* inpcrd_path, int natom, dou
                       "required");
     }
     sb::readCoordinates(inpcrd_path, natom, xyz);
+  });
+}
+
+extern "C" int sb_write_amber_coordinates(const char* inpcrd_path, const char* title, int natom,
+                                          const double* xyz) {
+  return sb::hostGuarded([&]() {
+    if (inpcrd_path == nullptr || xyz == nullptr || natom <= 0 || natom > 9999999) {
+      throw sb::Error(SB_ERR_ARGUMENT, "a file name, 1 to 9,999,999 atoms and their coordinates "
+                      "are required");
+    }
+    const size_t n = 3 * static_cast<size_t>(natom);
+    for (size_t k = 0; k < n; k++) {
+      // %12.7f keeps a value in its field below 1e4 in magnitude
+      if (!std::isfinite(xyz[k]) || std::fabs(xyz[k]) >= 9999.99999995) {
+        throw sb::Error(SB_ERR_ARGUMENT, "coordinates must be finite and below 1e4 A in "
+                        "magnitude to fit the Amber %12.7f fields");
+      }
+    }
+    std::string text = (title != nullptr) ? title : "";
+    if (text.find('\n') != std::string::npos) {
+      throw sb::Error(SB_ERR_ARGUMENT, "the title must be one line");
+    }
+    text += '\n';
+    char buf[32];
+    std::snprintf(buf, sizeof(buf), "%7d\n", natom);
+    text += buf;
+    for (size_t k = 0; k < n; k++) {
+      std::snprintf(buf, sizeof(buf), "%12.7f", xyz[k]);
+      // a value that rounds to zero prints unsigned, as STORMM's number formatting does
+      // (Parsing/ascii_numbers.cpp:10-420)
+      char* minus = std::strchr(buf, '-');
+      if (minus != nullptr && std::strtod(buf, nullptr) == 0.0) {
+        *minus = ' ';
+      }
+      text += buf;
+      if (k % 6 == 5 || k + 1 == n) {
+        text += '\n';
+      }
+    }
+    std::ofstream out(inpcrd_path, std::ios::trunc);
+    if (!out || !(out << text)) {
+      throw sb::Error(SB_ERR_ARGUMENT, std::string("cannot write ") + inpcrd_path);
+    }
   });
 }
