@@ -93,9 +93,8 @@ struct DevSynthesis {
   // close 1-4 pairs need more than FP32 deltas and cross products)
   const double4* angl64;         // per angle: k, cos(theta0), sin(theta0), theta0
   const double4* dihe64;         // per dihedral: amplitude, cos(phase), sin(phase), periodicity
-  const double2* dihe14_64;      // per dihedral: 1/scee, 1/scnb of the attached 1-4 pair (0: none)
-  const double* charge64;        // per padded atom: charge x sqrt(Coulomb constant)
-  const double2* ljab14_64;      // 1-4 (A, B) tables at lj_start offsets
+  const double4* dihe14_64;      // per dihedral: the attached 1-4 pair's q_i q_l / scee,
+                                 // A / scnb, B / scnb, and 1 (all 0: no 1-4 pair)
   const int* tile_mask_idx;      // per system tile, 0: no exclusions, else index into mask_pool
   const unsigned int* mask_pool; // 32 rows per mask: row = i lane, bit = j lane
 

@@ -271,8 +271,8 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
     h_neck_sep.assign(h64_neck_sep.begin(), h64_neck_sep.end());
     h_neck_val.assign(h64_neck_val.begin(), h64_neck_val.end());
   }
-  h64_charge.assign(np, 0.0);
   if (fp64) {
+    h64_charge.assign(np, 0.0);
     h64_rho.assign(np, 1.0);
     h64_srho.assign(np, 0.0);
     h64_pb.assign(np, 1.09);
@@ -293,8 +293,8 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
       const double a14 = (tp.lja14 != nullptr) ? tp.lja14[e] : tp.lja[e];
       const double b14 = (tp.ljb14 != nullptr) ? tp.ljb14[e] : tp.ljb[e];
       h_ljab14.push_back(make_float2(static_cast<float>(a14), static_cast<float>(b14)));
-      h64_ljab14.push_back(make_double2(a14, b14));
       if (fp64) {
+        h64_ljab14.push_back(make_double2(a14, b14));
         h64_ljab.push_back(make_double2(tp.lja[e], tp.ljb[e]));
       }
     }
@@ -382,8 +382,8 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
         // AtomGraph::setImplicitSolventModel (Topology/atomgraph_setters.cpp:1088-1092)
         h_neck_idx[base + i] = neckIndex(tp.pb_radii[i]);
       }
-      h64_charge[base + i] = tp.charge[i] * sqrt_kc;
       if (fp64) {
+        h64_charge[base + i] = tp.charge[i] * sqrt_kc;
         if (opt.igb != SB_GB_NONE) {
           const double rho = tp.pb_radii[i] - gb_offset;
           h64_rho[base + i] = rho;
@@ -440,8 +440,22 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
                                     fbits((scee > 0.0 && scnb > 0.0) ? 1.0 / scnb : 0.0)));
       h_dihe64.push_back(make_double4(tp.dihe_amp[d], std::cos(tp.dihe_phase[d]),
                                       std::sin(tp.dihe_phase[d]), tp.dihe_freq[d]));
-      h_dihe14_64.push_back(make_double2(scee > 0.0 ? 1.0 / scee : 0.0,
-                                         (scee > 0.0 && scnb > 0.0) ? 1.0 / scnb : 0.0));
+      // the attached 1-4 pair's attenuated parameters in FP64, so that the kernel reads them
+      // with the term instead of through a chain of dependent loads of charges, types and
+      // tables: the same products the kernel formed from those (q_i q_l / scee, A / scnb,
+      // B / scnb)
+      if (scee > 0.0) {
+        const double inv_scee = 1.0 / scee;
+        const double inv_scnb = (scnb > 0.0) ? 1.0 / scnb : 0.0;
+        const size_t e = static_cast<size_t>(tp.lj_idx[i]) * tp.n_lj_types + tp.lj_idx[l];
+        const double a14 = (tp.lja14 != nullptr) ? tp.lja14[e] : tp.lja[e];
+        const double b14 = (tp.ljb14 != nullptr) ? tp.ljb14[e] : tp.ljb[e];
+        h_dihe14_64.push_back(make_double4((tp.charge[i] * sqrt_kc) * (tp.charge[l] * sqrt_kc) *
+                                           inv_scee, a14 * inv_scnb, b14 * inv_scnb, 1.0));
+      }
+      else {
+        h_dihe14_64.push_back(make_double4(0.0, 0.0, 0.0, 0.0));
+      }
       if (fp64) {
         h64_dihe_atoms.push_back(make_int4(i, j, k, l));
         h64_dihe_prm.push_back(make_double4(tp.dihe_amp[d], tp.dihe_freq[d], tp.dihe_phase[d],
@@ -676,8 +690,10 @@ void Synthesis::upload() {
   d_angl64.upload(h_angl64);
   d_dihe64.upload(h_dihe64);
   d_dihe14_64.upload(h_dihe14_64);
-  d64_charge.upload(h64_charge);
-  d64_ljab14.upload(h64_ljab14);
+  if (fp64) {
+    d64_charge.upload(h64_charge);
+    d64_ljab14.upload(h64_ljab14);
+  }
   d_tile_mask_idx.upload(h_tile_mask_idx);
   d_mask_pool.upload(h_mask_pool);
   finalizePlan(single_plan.get());
@@ -822,8 +838,6 @@ void Synthesis::upload() {
   d.angl64 = d_angl64.p;
   d.dihe64 = d_dihe64.p;
   d.dihe14_64 = d_dihe14_64.p;
-  d.charge64 = d64_charge.p;
-  d.ljab14_64 = d64_ljab14.p;
   d.tile_mask_idx = d_tile_mask_idx.p;
   d.mask_pool = d_mask_pool.p;
   d.energies = d_energies.p;

@@ -190,7 +190,7 @@ public:
   std::vector<float2> h_ljab, h_ljab14;
   std::vector<uint4> h_bonds, h_angles, h_dihe_a, h_dihe_b;
   std::vector<double4> h_angl64, h_dihe64;
-  std::vector<double2> h_dihe14_64;
+  std::vector<double4> h_dihe14_64;
   std::vector<unsigned int> h_mask_pool;
   std::vector<long long> h_stage_ll;
   std::vector<int> h_unpadded_map;   // padded index of each unpadded atom
@@ -202,7 +202,7 @@ public:
   DeviceArray<float2> d_ljab, d_ljab14;
   DeviceArray<uint4> d_bonds, d_angles, d_dihe_a, d_dihe_b;
   DeviceArray<double4> d_angl64, d_dihe64;
-  DeviceArray<double2> d_dihe14_64;
+  DeviceArray<double4> d_dihe14_64;
   DeviceArray<unsigned int> d_mask_pool;
   DeviceArray<long long> d_xcrd, d_ycrd, d_zcrd, d_xfrc, d_yfrc, d_zfrc;
   DeviceArray<int> d_xcrd_ovrf, d_ycrd_ovrf, d_zcrd_ovrf, d_xfrc_ovrf, d_yfrc_ovrf, d_zfrc_ovrf;

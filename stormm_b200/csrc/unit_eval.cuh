@@ -786,6 +786,7 @@ __device__ void valenceTerms(const DevSynthesis &d, const V &v, int nsys_u) {
       const int pos = d.dihe_start[sysid] + t;
       const uint4 ra = d.dihe_a[pos];
       const double4 prm = d.dihe64[pos];     // amplitude, cos(phase), sin(phase), periodicity
+      const double4 p14 = d.dihe14_64[pos];  // the attached 1-4 pair: q q / scee, A, B, flag
       const int li = static_cast<int>(ra.x & 0xffffu);
       const int ll = static_cast<int>((ra.y >> 16) & 0x7fffu);
       const int ia = v.slot0[k] + li;
@@ -866,17 +867,13 @@ __device__ void valenceTerms(const DevSynthesis &d, const V &v, int nsys_u) {
       else {
         e_prop = prm.x * opc;
       }
-      // attached 1-4 pair between atoms i and l, FP64 charges and 1-4 Lennard-Jones tables
-      const double2 att = d.dihe14_64[pos];   // 1 / scee, 1 / scnb
-      if (att.x > 0.0) {
-        const int gi = d.atom_start[sysid] + li;
-        const int gl = d.atom_start[sysid] + ll;
+      // attached 1-4 pair between atoms i and l, its attenuated FP64 parameters stored with
+      // the term
+      if (p14.w != 0.0) {
         const double3 dv = sub3d(pl, pi);
-        const int nt = d.lj_ntypes[sysid];
-        const double2 ab14 = d.ljab14_64[d.lj_start[sysid] + d.lj_idx[gi] * nt + d.lj_idx[gl]];
-        const double lja = ab14.x * att.y;
-        const double ljb = ab14.y * att.y;
-        const double qiqj = d.charge64[gi] * d.charge64[gl] * att.x;
+        const double qiqj = p14.x;
+        const double lja = p14.y;
+        const double ljb = p14.z;
         const double invr = rsqrt(dot3d(dv, dv));
         const double invr2 = invr * invr;
         const double invr6 = invr2 * invr2 * invr2;
