@@ -18,6 +18,7 @@ from __future__ import annotations
 import multiprocessing as mp
 import os
 import subprocess
+import sys
 import tempfile
 import time
 
@@ -85,11 +86,15 @@ def prepare_samples(names=None) -> None:
 
 
 def _sample_files(name: str):
-    """(prmtop, inpcrd) paths of a prepared sample, preparing it first if needed."""
+    """(prmtop, inpcrd) paths of a prepared sample, preparing it first if needed: in a child
+    process, so that the process that times STORMM maps no library of the package under test."""
     d = _sample_dir(name)
     index = os.path.join(d, "index.txt")
     if not os.path.exists(index):
-        prepare_samples([name])
+        root = os.path.dirname(HERE)
+        subprocess.run([sys.executable, "-c",
+                        f"import sys; sys.path.insert(0, {root!r}); import oracle.cpu_baseline as c; "
+                        f"c.prepare_samples([{name!r}])"], check=True)
     with open(index) as f:
         return [tuple(os.path.join(d, p) for p in line.split()) for line in f if line.strip()]
 
