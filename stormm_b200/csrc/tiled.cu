@@ -164,6 +164,7 @@ __device__ __forceinline__ void stageTile(const DevSynthesis &d, const DevTiled 
                         d.srho[gi]);
       if (PASS == 2) {
         pa.w = prm.x;
+        gbv.y = prm.y;      // the Lennard-Jones code, where pass 2 reads it
         if (GB) {
           const float r = t.radius[gi];
           pb.w = r;

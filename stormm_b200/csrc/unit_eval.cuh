@@ -27,7 +27,8 @@
 // Shared memory per atom slot: pos_a = (x_hi, y_hi, z_hi, w1) and pos_b = (x_lo, y_lo, z_lo, w2)
 // feed the pair passes with two 16-byte loads per partner; w1 / w2 carry what the pass needs
 // (pass 1 and 3: s*rho and rho; pass 2: charge and effective radius).  prm holds the static
-// per-atom values, gbv the reciprocal effective radius and the chain-rule dE/dR.
+// per-atom values, gbv the reciprocal effective radius with the Lennard-Jones code (pass 2) and
+// then the chain-rule dE/dR (pass 3).
 #ifndef STORMM_B200_UNIT_EVAL_CUH
 #define STORMM_B200_UNIT_EVAL_CUH
 
@@ -400,7 +401,8 @@ struct UnitSmem {
   float4* pa;       // x_hi, y_hi, z_hi, pass payload w1
   float4* pb;       // x_lo, y_lo, z_lo, pass payload w2
   float4* prm;      // charge * sqrt(k_Coulomb), Lennard-Jones code (int bits), rho, s * rho
-  float2* gbv;      // 1 / effective radius, dE/dR after the chain rule
+  float2* gbv;      // 1 / effective radius; y: Lennard-Jones code bits in pass 2, dE/dR after
+                    // the chain rule
   int* fx;          // int63 force accumulators: primary
   int* fy;
   int* fz;
@@ -801,6 +803,35 @@ __device__ void valenceTerms(const DevSynthesis &d, const V &v, int nsys_u) {
       const double3 ab = sub3d(pj, pi);
       const double3 bc = sub3d(pk, pj);
       const double3 cd = sub3d(pl, pk);
+      // attached 1-4 pair between atoms i and l, its attenuated FP64 parameters stored with
+      // the term; evaluated first, so that the atoms' positions are no longer live in the
+      // torsion's force, and its force joins the torsion's on atoms i and l (one set of
+      // accumulator atomics for both)
+      double3 f14 = make_double3(0.0, 0.0, 0.0);
+      if (p14.w != 0.0) {
+        const double3 dv = sub3d(pl, pi);
+        const double qiqj = p14.x;
+        const double lja = p14.y;
+        const double ljb = p14.z;
+        const double invr = rsqrt(dot3d(dv, dv));
+        const double invr2 = invr * invr;
+        const double invr6 = invr2 * invr2 * invr2;
+        const float2 cl = CLASH ? v.clash(k) : make_float2(0.0f, 0.0f);
+        double fmag = 0.0;
+        if (CLASH && (cl.x > 0.0f || cl.y > 0.0f)) {
+          // clash-softened 1-4 pair (valence_potential.tpp:1337-1357)
+          fmag = softCorePair64(1.0 / invr, invr, qiqj, lja, ljb, cl.x, quadraticCore64(cl.x),
+                                cl.y, &e_el14, &e_lj14);
+        }
+        else {
+          if (FORCE) {
+            fmag = -(qiqj * invr * invr2) + (6.0 * ljb - 12.0 * lja * invr6) * invr6 * invr2;
+          }
+          e_el14 = qiqj * invr;
+          e_lj14 = (lja * invr6 - ljb) * invr6;
+        }
+        f14 = make_double3(fmag * dv.x, fmag * dv.y, fmag * dv.z);
+      }
       double3 crabbc = cross3d(ab, bc);
       double3 crbccd = cross3d(bc, cd);
       const double bc2 = dot3d(bc, bc);
@@ -828,6 +859,14 @@ __device__ void valenceTerms(const DevSynthesis &d, const V &v, int nsys_u) {
       }
       const double cos_sangle = cn * prm.y + sn * prm.z;
       const double sin_sangle = sn * prm.y - cn * prm.z;
+      const double opc = (cos_sangle >= 0.0) ? 1.0 + cos_sangle :
+                                               sin_sangle * sin_sangle / (1.0 - cos_sangle);
+      if (improper) {
+        e_impr = prm.x * opc;
+      }
+      else {
+        e_prop = prm.x * opc;
+      }
       if (FORCE) {
         const double fr = prm.x * freq * sin_sangle;
         const double ab2 = dot3d(ab, ab);
@@ -849,54 +888,17 @@ __device__ void valenceTerms(const DevSynthesis &d, const V &v, int nsys_u) {
         const double fb1 = (mgbc - mgab * cosb) * invabc * isinb2;
         const double fb2 = cosc * invbc * isinc2;
         const double fd = -invcd * isinc2;
-        const double fix = crabbc.x * fa, fiy = crabbc.y * fa, fiz = crabbc.z * fa;
-        const double fjx = fb1 * crabbc.x - fb2 * crbccd.x;
-        const double fjy = fb1 * crabbc.y - fb2 * crbccd.y;
-        const double fjz = fb1 * crabbc.z - fb2 * crbccd.z;
-        const double flx = -fd * crbccd.x, fly = -fd * crbccd.y, flz = -fd * crbccd.z;
-        v.force64(ia, fix, fiy, fiz, fs);
-        v.force64(ja, fjx, fjy, fjz, fs);
-        v.force64(ka, -(fix + fjx + flx), -(fiy + fjy + fly), -(fiz + fjz + flz), fs);
-        v.force64(la, flx, fly, flz, fs);
-      }
-      const double opc = (cos_sangle >= 0.0) ? 1.0 + cos_sangle :
-                                               sin_sangle * sin_sangle / (1.0 - cos_sangle);
-      if (improper) {
-        e_impr = prm.x * opc;
-      }
-      else {
-        e_prop = prm.x * opc;
-      }
-      // attached 1-4 pair between atoms i and l, its attenuated FP64 parameters stored with
-      // the term
-      if (p14.w != 0.0) {
-        const double3 dv = sub3d(pl, pi);
-        const double qiqj = p14.x;
-        const double lja = p14.y;
-        const double ljb = p14.z;
-        const double invr = rsqrt(dot3d(dv, dv));
-        const double invr2 = invr * invr;
-        const double invr6 = invr2 * invr2 * invr2;
-        const float2 cl = CLASH ? v.clash(k) : make_float2(0.0f, 0.0f);
-        if (CLASH && (cl.x > 0.0f || cl.y > 0.0f)) {
-          // clash-softened 1-4 pair (valence_potential.tpp:1337-1357)
-          const double fmag = softCorePair64(1.0 / invr, invr, qiqj, lja, ljb, cl.x,
-                                             quadraticCore64(cl.x), cl.y, &e_el14, &e_lj14);
-          if (FORCE) {
-            v.force64(ia, fmag * dv.x, fmag * dv.y, fmag * dv.z, fs);
-            v.force64(la, -fmag * dv.x, -fmag * dv.y, -fmag * dv.z, fs);
-          }
-        }
-        else {
-          if (FORCE) {
-            const double fmag = -(qiqj * invr * invr2) +
-                                (6.0 * ljb - 12.0 * lja * invr6) * invr6 * invr2;
-            v.force64(ia, fmag * dv.x, fmag * dv.y, fmag * dv.z, fs);
-            v.force64(la, -fmag * dv.x, -fmag * dv.y, -fmag * dv.z, fs);
-          }
-          e_el14 = qiqj * invr;
-          e_lj14 = (lja * invr6 - ljb) * invr6;
-        }
+        // each atom's force goes out as soon as it is formed (fewer doubles live at once); the
+        // third atom takes minus the sum of the torsion's other three, (fb2 + fd) cd' -
+        // (fa + fb1) ab'
+        v.force64(ia, crabbc.x * fa + f14.x, crabbc.y * fa + f14.y, crabbc.z * fa + f14.z, fs);
+        v.force64(la, -fd * crbccd.x - f14.x, -fd * crbccd.y - f14.y, -fd * crbccd.z - f14.z, fs);
+        v.force64(ja, fb1 * crabbc.x - fb2 * crbccd.x, fb1 * crabbc.y - fb2 * crbccd.y,
+                  fb1 * crabbc.z - fb2 * crbccd.z, fs);
+        const double gab = fa + fb1;
+        const double gcd = fb2 + fd;
+        v.force64(ka, gcd * crbccd.x - gab * crabbc.x, gcd * crbccd.y - gab * crabbc.y,
+                  gcd * crbccd.z - gab * crabbc.z, fs);
       }
     }
     if (ENERGY) {
@@ -1127,6 +1129,7 @@ struct PairPass {
   __device__ __forceinline__ void pair(int jslot, int jl) {
     const float4 aj = s.pa[jslot];
     const float4 bj = s.pb[jslot];
+    const float2 gj = s.gbv[jslot];    // pass 2: 1 / effective radius, Lennard-Jones code bits
     const float hx = aj.x - ai.x, hy = aj.y - ai.y, hz = aj.z - ai.z;
     const float lx = bj.x - bi.x, ly = bj.y - bi.y, lz = bj.z - bi.z;
     const float3 dv = make_float3(hx + lx, hy + ly, hz + lz);
@@ -1151,7 +1154,7 @@ struct PairPass {
       float invr2 = __fdividef(1.0f, r2);
       invr2 = fmaf(invr2, fmaf(-2.0f * r2c, invr2, fmaf(-r2, invr2, 1.0f)), invr2);
       const float invr6 = invr2 * invr2 * invr2;
-      float2 ab = s.lj[code_i + (__float_as_int(s.prm[jslot].y) >> 16)];
+      float2 ab = s.lj[code_i + (__float_as_int(gj.y) >> 16)];
       ab.x *= incl;
       ab.y *= incl;
       const float qiqj = qiqj_all * incl;
@@ -1172,7 +1175,7 @@ struct PairPass {
     if (GB) {
       const float qiqj = qiqj_all;
       const float ijb = bi.w * bj.w;
-      const float efac = __expf(-r2 * inv4ri * s.gbv[jslot].x);
+      const float efac = __expf(-r2 * inv4ri * gj.x);
       const float fgbi = rsqrtf(fmaf(ijb, efac, r2));
       float expmkf, fgbk;
       if (salt) {
@@ -1722,7 +1725,8 @@ __device__ void evaluateStaged(const DevSynthesis &d, const UnitSmem &s, const U
       }
       s.pa[slot] = pa;
       s.pb[slot] = pb;
-      s.gbv[slot].x = 1.0f / egbi;
+      // pass 2 reads a partner's reciprocal radius and Lennard-Jones code with one load
+      s.gbv[slot] = make_float2(1.0f / egbi, prm.y);
       if (ENERGY) {
         warpEnergy(s, k, kGb, e_self, d.nrg_scale);
       }
@@ -1733,7 +1737,9 @@ __device__ void evaluateStaged(const DevSynthesis &d, const UnitSmem &s, const U
     // pass 2 payload for Coulomb / Lennard-Jones alone: charge in w1
     for (int slot = team.rank(); slot < nslots; slot += team.size()) {
       float4 pa = s.pa[slot];
-      pa.w = s.prm[slot].x;
+      const float4 prm = s.prm[slot];
+      pa.w = prm.x;
+      s.gbv[slot].y = prm.y;     // the Lennard-Jones code, where pass 2 reads it
       s.pa[slot] = pa;
     }
     team.sync();
