@@ -44,6 +44,9 @@ sys.path.insert(0, ROOT)
 NSYS = 1024
 WORKLOAD = "batched single point: 1024 molecules, 16-256 atoms, OBC-II GB, valence + Coulomb/LJ"
 METRIC = "force-evals/s (batched single point, 1024 molecules of 16-256 atoms)"
+# dram__bytes_read.sum + dram__bytes_write.sum of one kEvalFused launch on the 1,024-molecule
+# single point, from the ncu capture summarized in profiles/ (the bench cannot profile itself)
+KEVALFUSED_TRAFFIC_BYTES = 85.669376e6 + 81.111296e6
 MIN_NSYS = 4096
 MIN_CYCLES = 500
 MIN_SD_CYCLES = 50
@@ -788,7 +791,12 @@ def main_rank(args):
                     "p99_ms": float(np.percentile(sp["lat"], 99)) * 1000.0},
             "gpu_launches": args.steps * (1 if info["work_units"] else 0),
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak,
-                         "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                         "unit": "TFLOP/s", "frac": achieved / peak,
+                         "traffic": KEVALFUSED_TRAFFIC_BYTES,
+                         "traffic_unit": "DRAM bytes read + written per launch",
+                         "traffic_source": "ncu capture of this launch shape "
+                                           "(profiles/kEvalFused_single_point_1024_molecules.md):"
+                                           " 35 MB of inputs, the rest the pair-derivative store",
                          "kernel": "kEvalFused", "flops_per_launch": sp["flops"],
                          "kernel_ms": sp["kern_avg_s"] * 1000.0,
                          "peak_source": "nominal FP32 FMA pipe: 148 SM x 128 lanes x 2 x "
