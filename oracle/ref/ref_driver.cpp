@@ -21,6 +21,9 @@
 //
 //   sdf <file> <out.bin>
 //       STORMM's MdlMol parse of each compound of an SD / MOL file (readStructureDataFile).
+//   geometry <prmtop> <list-file> <out.bin>
+//       STORMM's clash verdict (detectClash) for each coordinate file listed and its
+//       mass-weighted aligned RMSD (RMSDMethod::ALIGN_MASS) against the first.
 //   writecrd <in.inpcrd> <out.inpcrd>
 //       The coordinates of an Amber input-coordinate file written back by STORMM's
 //       PhaseSpace::exportToFile (CoordinateFileKind::AMBER_INPCRD).
@@ -58,6 +61,9 @@
 #include "Potential/static_exclusionmask.h"
 #include "Potential/valence_potential.h"
 #include "Restraints/restraint_apparatus.h"
+#include "Structure/clash_detection.h"
+#include "Structure/rmsd.h"
+#include "Trajectory/coordinateframe.h"
 #include "Synthesis/atomgraph_synthesis.h"
 #include "Synthesis/static_mask_synthesis.h"
 #include "Synthesis/synthesis_abstracts.h"
@@ -568,6 +574,32 @@ int runSdf(const std::string &path, const std::string &out) {
   return 0;
 }
 
+// STORMM's clash verdict (detectClash with its default clash distance and ratio) for each
+// coordinate file of <list-file> (one inpcrd per line) under one topology, and the
+// mass-weighted aligned RMSD (RMSDMethod::ALIGN_MASS) of each against the first
+int runGeometry(const std::string &prmtop, const std::string &list_file, const std::string &out,
+                const Options &opt) {
+  AtomGraph ag = loadTopology(prmtop, opt);
+  const StaticExclusionMask se(&ag);
+  std::ifstream lst(list_file);
+  std::string crd;
+  std::vector<CoordinateFrame> frames;
+  while (lst >> crd) {
+    frames.emplace_back(crd, CoordinateFileKind::AMBER_INPCRD);
+  }
+  std::vector<int> clash;
+  std::vector<double> rms;
+  for (const CoordinateFrame &cf : frames) {
+    clash.push_back(structure::detectClash(cf, ag, se, default_minimize_clash_r0,
+                                           default_minimize_clash_ratio) ? 1 : 0);
+    rms.push_back(structure::rmsd(frames[0], cf, ag, structure::RMSDMethod::ALIGN_MASS));
+  }
+  RecordWriter rw(out);
+  rw.i("clash", clash);
+  rw.d("rmsd_to_first", rms);
+  return 0;
+}
+
 // An Amber input-coordinate file as STORMM writes it (PhaseSpace::exportToFile,
 // CoordinateFileKind::AMBER_INPCRD) after reading the coordinates of another one
 int runWriteCrd(const std::string &in, const std::string &out) {
@@ -681,6 +713,9 @@ int main(int argc, char* argv[]) {
   }
   if (mode == "sdf" && pos.size() == 2) {
     return runSdf(pos[0], pos[1]);
+  }
+  if (mode == "geometry" && pos.size() == 3) {
+    return runGeometry(pos[0], pos[1], pos[2], opt);
   }
   if (mode == "writecrd" && pos.size() == 2) {
     return runWriteCrd(pos[0], pos[1]);
