@@ -316,8 +316,11 @@ int sb_get_minimize_progress(sb_synthesis* syn, int* cycles_done, int* converged
  * topology, coordinates and minimizer state resident on the device, runs its minimization in
  * launches of cycles_per_launch cycles on a stream of its own (batches overlap on the GPU),
  * retires every molecule that converged or reached total_cycles after each launch, and
- * backfills: new batches start while older ones are still running.  A molecule's result does
- * not depend on the batch it ran in.
+ * backfills: new batches start while older ones are still running, and when three quarters of a
+ * minimization batch have retired while minimizations wait, its remaining molecules move with
+ * their minimizer state into a new batch beside the waiting requests and the old batch's memory
+ * is released (persistent FP32 minimizer).  A molecule's result does not depend on the batch it
+ * ran in, nor on a move.
  *
  * Errors: submit checks the topology on the host (the checks the synthesis applies) and refuses
  * a bad request with its error code; the server's controls are checked when it is created.  A
@@ -362,6 +365,7 @@ typedef struct {
   long long admitted;
   long long completed;                /* results returned, the failed ones included */
   long long failed;                   /* requests returned with an error status */
+  long long migrated;                 /* molecule moves out of an emptying batch into a new one */
   int pending;                       /* queued, not yet admitted */
   int in_flight;                     /* admitted molecules still minimizing */
   int batches;

@@ -94,6 +94,7 @@ class ServerStats(ctypes.Structure):
     _fields_ = [
         ("submitted", ctypes.c_longlong), ("admitted", ctypes.c_longlong),
         ("completed", ctypes.c_longlong), ("failed", ctypes.c_longlong),
+        ("migrated", ctypes.c_longlong),
         ("pending", ctypes.c_int), ("in_flight", ctypes.c_int),
         ("batches", ctypes.c_int), ("bytes_in_flight", ctypes.c_double),
     ]

@@ -39,8 +39,8 @@ size_t fusedSmemBytes(int max_slots, int max_lj) { return unitSmemBytes(max_slot
 // The fused kernel: stage, evaluate, commit, one work unit at a time
 // ------------------------------------------------------------------------------------------------
 template <bool FORCE, bool ENERGY, int TERMS, bool CLASH, bool NECK>
-__global__ void __launch_bounds__(256, 4)
-kEvalFused(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
+__device__ __forceinline__ void evalFusedUnits(const DevSynthesis &d, int unit_begin,
+                                               int unit_end, int max_lj) {
   extern __shared__ __align__(16) char smem_raw[];
   const UnitSmem s = carveSmem(smem_raw, d.max_unit_slots, max_lj);
   for (int u = unit_begin + blockIdx.x; u < unit_end; u += gridDim.x) {
@@ -97,6 +97,20 @@ kEvalFused(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
   }
 }
 
+template <bool FORCE, bool ENERGY, int TERMS, bool CLASH, bool NECK>
+__global__ void __launch_bounds__(256, 4)
+kEvalFused(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
+  evalFusedUnits<FORCE, ENERGY, TERMS, CLASH, NECK>(d, unit_begin, unit_end, max_lj);
+}
+
+// The same with 512 threads a block: twice the warps per work unit, for launches of too few
+// units to fill the GPU with 256-thread blocks (a small batch, or its large molecules)
+template <bool FORCE, bool ENERGY, int TERMS, bool CLASH, bool NECK>
+__global__ void __launch_bounds__(512, 2)
+kEvalFusedWide(const DevSynthesis d, int unit_begin, int unit_end, int max_lj) {
+  evalFusedUnits<FORCE, ENERGY, TERMS, CLASH, NECK>(d, unit_begin, unit_end, max_lj);
+}
+
 // Host-side launcher (called from the C++ layer)
 cudaError_t launchEvalFused(const DevSynthesis &d, int unit_begin, int unit_end, int max_lj,
                             int terms, bool force, bool energy, int blocks, int threads,
@@ -105,16 +119,31 @@ cudaError_t launchEvalFused(const DevSynthesis &d, int unit_begin, int unit_end,
   // softened cores change only Coulomb, Lennard-Jones and 1-4 terms, the neck term only GB
   clash = clash && (terms & 3) != 0;
   const bool neck = d.neck_size > 0 && (terms & 4) != 0;
-#define SB_LAUNCH(F, E, T)                                                                      \
+  // 512-thread blocks exist for evaluations of all terms only
+  if (threads > 256 && terms != 7) {
+    threads = 256;
+  }
+  if (threads != 512 && (threads < 64 || threads > 256 || threads % 32 != 0)) {
+    return cudaErrorInvalidValue;
+  }
+#define SB_PICK(K, F, E, T)                                                                     \
+    (neck ? (clash ? K<F, E, T, ((T) & 3) != 0, ((T) & 4) != 0> :                               \
+                     K<F, E, T, false, ((T) & 4) != 0>) :                                       \
+            (clash ? K<F, E, T, ((T) & 3) != 0, false> : K<F, E, T, false, false>))
+#define SB_GO(KERN)                                                                             \
   {                                                                                             \
-    auto kern = neck ? (clash ? kEvalFused<F, E, T, ((T) & 3) != 0, ((T) & 4) != 0> :          \
-                                kEvalFused<F, E, T, false, ((T) & 4) != 0>) :                   \
-                       (clash ? kEvalFused<F, E, T, ((T) & 3) != 0, false> :                    \
-                                kEvalFused<F, E, T, false, false>);                             \
+    auto kern = KERN;                                                                           \
     const cudaError_t err = allowLargeSmem(kern);                                               \
     if (err != cudaSuccess) return err;                                                         \
     kern<<<blocks, threads, smem, stream>>>(d, unit_begin, unit_end, max_lj);                   \
     return cudaGetLastError();                                                                  \
+  }
+#define SB_LAUNCH(F, E, T)                                                                      \
+  {                                                                                             \
+    if constexpr ((T) == 7) {                                                                   \
+      if (threads > 256) SB_GO(SB_PICK(kEvalFusedWide, F, E, T))                                \
+    }                                                                                           \
+    SB_GO(SB_PICK(kEvalFused, F, E, T))                                                         \
   }
 #define SB_TERMS(F, E)                                  \
   switch (terms) {                                      \
@@ -139,6 +168,8 @@ cudaError_t launchEvalFused(const DevSynthesis &d, int unit_begin, int unit_end,
   return cudaErrorInvalidValue;
 #undef SB_TERMS
 #undef SB_LAUNCH
+#undef SB_GO
+#undef SB_PICK
 }
 
 }  // namespace sb

@@ -11,6 +11,10 @@
 //             molecule's progress, retire the molecules that converged or reached the cycle cap
 //             (final energies and coordinates are copied out), and launch the next cycles for
 //             the rest; a batch whose molecules have all retired is freed on its stream
+//   migrate   when at most a quarter of a minimization batch is still running and new
+//             minimizations wait, the running molecules' minimizer states are read out, they
+//             go back to the front of the queue and the batch is freed; admitted again with
+//             the waiting requests they continue from their states (slot backfill)
 // Batches overlap on the device, new batches start while older ones run (backfill), and a
 // molecule's trajectory is bit-identical whichever batch, unit or launch split it gets.
 //
@@ -71,6 +75,8 @@ struct Request {
   double t_admit = 0.0;
   int kind = SB_REQUEST_MINIMIZE;
   bool solo = false;                  // retried alone after its batch failed to build
+  // minimizer state carried over from the batch the request ran in before (null: fresh)
+  std::shared_ptr<MinimizerState> state;
 
   Request(const sb_topology &t, const double* coords) {
     natom = t.natom;
@@ -291,6 +297,7 @@ public:
     s.admitted = admitted_;
     s.completed = completed_;
     s.failed = failed_;
+    s.migrated = migrated_;
     s.pending = static_cast<int>(pending_.size());
     s.in_flight = in_flight_;
     s.batches = nbatches_;
@@ -469,7 +476,9 @@ private:
     std::vector<double> xyz;
     for (size_t k = 0; k < b->reqs.size(); k++) {
       Request &r = b->reqs[k];
-      r.t_admit = t;
+      if (r.state == nullptr) {
+        r.t_admit = t;
+      }
       tops.push_back(r.view());
       index.push_back(static_cast<int>(k));
       xyz.insert(xyz.end(), r.xyz.begin(), r.xyz.end());
@@ -482,6 +491,13 @@ private:
       b->syn->setCoordinates(xyz.data(), b->stream);
       if (b->kind == SB_REQUEST_MINIMIZE) {
         b->syn->minimizeBegin(opt_.controls, b->stream);
+        // molecules moved here from an emptying batch continue from their own state
+        for (size_t k = 0; k < b->reqs.size(); k++) {
+          if (b->reqs[k].state != nullptr) {
+            b->syn->importMinimizerState(static_cast<int>(k), *b->reqs[k].state, b->stream);
+            b->reqs[k].state.reset();
+          }
+        }
       }
     }
     if (b->kind == SB_REQUEST_MINIMIZE) {
@@ -661,9 +677,58 @@ private:
     if (b->remaining == 0) {
       return true;
     }
+    if (shouldMigrate(b)) {
+      migrate(b);
+      return true;
+    }
     b->syn->minimizeAdvance(opt_.cycles_per_launch, true, b->stream);
     cudaCheck(cudaEventRecord(b->event, b->stream), "cudaEventRecord");
     return false;
+  }
+
+  // A minimization batch whose molecules have mostly retired holds its whole memory budget and
+  // a launch per round for the few left.  When minimizations are waiting, those few move to
+  // the front of the queue with their minimizer state, the batch is released, and they are
+  // admitted again beside the waiting requests: their slots are backfilled.  Each moved
+  // molecule continues exactly where it was (state at a cycle boundary, the persistent FP32
+  // minimizer, whose per-molecule arithmetic does not depend on the batch).
+  bool shouldMigrate(const Batch* b) {
+    if (opt_.controls.kernel != SB_MIN_PERSISTENT ||
+        opt_.options.precision != SB_PRECISION_SINGLE || b->reqs.size() < 2 ||
+        4 * b->remaining > static_cast<int>(b->reqs.size())) {
+      return false;
+    }
+    std::lock_guard<std::mutex> lock(mu_);
+    for (const Request &r : pending_) {
+      if (r.kind == SB_REQUEST_MINIMIZE && r.state == nullptr) {
+        return true;
+      }
+    }
+    return false;
+  }
+
+  void migrate(Batch* b) {
+    std::vector<Request> moving;
+    for (size_t k = 0; k < b->reqs.size(); k++) {
+      if (b->finished[k]) {
+        continue;
+      }
+      auto st = std::make_shared<MinimizerState>();
+      b->syn->exportMinimizerState(static_cast<int>(k), st.get(), b->stream);
+      Request r = std::move(b->reqs[k]);
+      r.state = std::move(st);
+      moving.push_back(std::move(r));
+      b->finished[k] = 1;
+    }
+    b->remaining = 0;
+    std::lock_guard<std::mutex> lock(mu_);
+    in_flight_ -= static_cast<int>(moving.size());
+    admitted_ -= static_cast<long long>(moving.size());
+    migrated_ += static_cast<long long>(moving.size());
+    for (auto it = moving.rbegin(); it != moving.rend(); ++it) {
+      pending_.push_front(std::move(*it));
+    }
+    cv_.notify_all();
   }
 
   // Free a batch's device memory in its stream's order, then its stream
@@ -706,6 +771,7 @@ private:
   long long admitted_ = 0;
   long long completed_ = 0;
   long long failed_ = 0;
+  long long migrated_ = 0;
   int in_flight_ = 0;
   int nbatches_ = 0;
   double bytes_in_flight_ = 0.0;

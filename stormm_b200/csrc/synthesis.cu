@@ -874,15 +874,27 @@ void Synthesis::launchPlan(const UnitPlan &plan, int terms, bool force, bool ene
   if (plan.n_big > 0) {
     d.max_unit_slots = plan.big_slots;
     cudaCheck(launchEvalFused(d, 0, plan.n_big, plan.big_lj, terms, force, energy, plan.n_big,
-                              threads, stream, clash.on()),
+                              launchThreads(plan.n_big, terms), stream, clash.on()),
               "fused evaluation launch (large molecules)");
   }
   if (nunit > plan.n_big) {
     d.max_unit_slots = plan.small_slots;
     cudaCheck(launchEvalFused(d, plan.n_big, nunit, plan.small_lj, terms, force, energy,
-                              nunit - plan.n_big, threads, stream, clash.on()),
+                              nunit - plan.n_big, launchThreads(nunit - plan.n_big, terms),
+                              stream, clash.on()),
               "fused evaluation launch");
   }
+}
+
+// Threads a block for an evaluation launch of `units` work units: the configured count, or
+// 512 when the default 256 would leave the SMs short of warps (fewer units than two blocks an
+// SM) and the launch evaluates every term.  Sums are fixed-point, so the block size changes
+// no result bit.
+int Synthesis::launchThreads(int units, int terms) const {
+  if (opt.threads_per_block > 0 || terms != SB_TERM_ALL || units >= 2 * sm_count) {
+    return threads;
+  }
+  return 512;
 }
 
 void Synthesis::evaluate(int terms, bool force, bool energy, cudaStream_t stream,
@@ -1532,6 +1544,77 @@ void Synthesis::getMinimizeProgress(int* cycles, int* converged, double* rms,
                               stream), "progress download");
   }
   cudaCheck(cudaStreamSynchronize(stream), "progress download");
+}
+
+void Synthesis::exportMinimizerState(int system, MinimizerState* st, cudaStream_t stream) {
+  if (!min_ready || fp64 || system < 0 || system >= nsys) {
+    throw Error(SB_ERR_ARGUMENT, "minimizer state export needs a begun FP32 minimization and a "
+                "system in range");
+  }
+  const int n = atom_count[system];
+  const size_t a0 = atom_start[system];
+  st->natom = n;
+  const long long* crd[3] = {d_xcrd.p, d_ycrd.p, d_zcrd.p};
+  const int* ovrf[3] = {d_xcrd_ovrf.p, d_ycrd_ovrf.p, d_zcrd_ovrf.p};
+  const long long* prv[3] = {d_xprv.p, d_yprv.p, d_zprv.p};
+  const float* cg[3] = {d_xcg.p, d_ycg.p, d_zcg.p};
+  for (int c = 0; c < 3; c++) {
+    st->crd[c].resize(n);
+    st->crd_ovrf[c].resize(n);
+    st->prv[c].resize(n);
+    st->cg[c].resize(n);
+    cudaCheck(cudaMemcpyAsync(st->crd[c].data(), crd[c] + a0, sizeof(long long) * n,
+                              cudaMemcpyDeviceToHost, stream), "state export");
+    cudaCheck(cudaMemcpyAsync(st->crd_ovrf[c].data(), ovrf[c] + a0, sizeof(int) * n,
+                              cudaMemcpyDeviceToHost, stream), "state export");
+    cudaCheck(cudaMemcpyAsync(st->prv[c].data(), prv[c] + a0, sizeof(long long) * n,
+                              cudaMemcpyDeviceToHost, stream), "state export");
+    cudaCheck(cudaMemcpyAsync(st->cg[c].data(), cg[c] + a0, sizeof(float) * n,
+                              cudaMemcpyDeviceToHost, stream), "state export");
+  }
+  cudaCheck(cudaMemcpyAsync(&st->l_move, d_lmove.p + system, sizeof(double),
+                            cudaMemcpyDeviceToHost, stream), "state export");
+  cudaCheck(cudaMemcpyAsync(&st->rms_force, d_rmsf.p + system, sizeof(double),
+                            cudaMemcpyDeviceToHost, stream), "state export");
+  cudaCheck(cudaMemcpyAsync(&st->cycle, d_mcycle.p + system, sizeof(int),
+                            cudaMemcpyDeviceToHost, stream), "state export");
+  cudaCheck(cudaMemcpyAsync(&st->done, d_mdone.p + system, sizeof(int), cudaMemcpyDeviceToHost,
+                            stream), "state export");
+  cudaCheck(cudaStreamSynchronize(stream), "state export");
+}
+
+void Synthesis::importMinimizerState(int system, const MinimizerState &st,
+                                     cudaStream_t stream) {
+  if (!min_ready || fp64 || system < 0 || system >= nsys || st.natom != atom_count[system]) {
+    throw Error(SB_ERR_ARGUMENT, "minimizer state import needs a begun FP32 minimization and a "
+                "system of the same atom count");
+  }
+  const int n = st.natom;
+  const size_t a0 = atom_start[system];
+  long long* crd[3] = {d_xcrd.p, d_ycrd.p, d_zcrd.p};
+  int* ovrf[3] = {d_xcrd_ovrf.p, d_ycrd_ovrf.p, d_zcrd_ovrf.p};
+  long long* prv[3] = {d_xprv.p, d_yprv.p, d_zprv.p};
+  float* cg[3] = {d_xcg.p, d_ycg.p, d_zcg.p};
+  for (int c = 0; c < 3; c++) {
+    cudaCheck(cudaMemcpyAsync(crd[c] + a0, st.crd[c].data(), sizeof(long long) * n,
+                              cudaMemcpyHostToDevice, stream), "state import");
+    cudaCheck(cudaMemcpyAsync(ovrf[c] + a0, st.crd_ovrf[c].data(), sizeof(int) * n,
+                              cudaMemcpyHostToDevice, stream), "state import");
+    cudaCheck(cudaMemcpyAsync(prv[c] + a0, st.prv[c].data(), sizeof(long long) * n,
+                              cudaMemcpyHostToDevice, stream), "state import");
+    cudaCheck(cudaMemcpyAsync(cg[c] + a0, st.cg[c].data(), sizeof(float) * n,
+                              cudaMemcpyHostToDevice, stream), "state import");
+  }
+  cudaCheck(cudaMemcpyAsync(d_lmove.p + system, &st.l_move, sizeof(double),
+                            cudaMemcpyHostToDevice, stream), "state import");
+  cudaCheck(cudaMemcpyAsync(d_rmsf.p + system, &st.rms_force, sizeof(double),
+                            cudaMemcpyHostToDevice, stream), "state import");
+  cudaCheck(cudaMemcpyAsync(d_mcycle.p + system, &st.cycle, sizeof(int),
+                            cudaMemcpyHostToDevice, stream), "state import");
+  cudaCheck(cudaMemcpyAsync(d_mdone.p + system, &st.done, sizeof(int), cudaMemcpyHostToDevice,
+                            stream), "state import");
+  // the host copies are the caller's: wait until they have been read
+  cudaCheck(cudaStreamSynchronize(stream), "state import");
 }
 
 }  // namespace sb

@@ -102,6 +102,18 @@ void validateTopology(const sb_topology &tp, const sb_options &opt, int which);
 // Host checks of minimization controls (minimizeBegin and the request server's constructor)
 void validateMinimizeControls(const sb_minimize_controls &ctl);
 
+// A system's line-minimization state at a cycle boundary (FP32 path), on the host
+struct MinimizerState {
+  int natom = 0;
+  std::vector<long long> crd[3], prv[3];
+  std::vector<int> crd_ovrf[3];
+  std::vector<float> cg[3];
+  double l_move = 0.0;
+  double rms_force = 0.0;
+  int cycle = 0;
+  int done = 0;
+};
+
 // Packing of molecules into work units and the launch parameters of each size class
 struct UnitPlan {
   int max_slots_cap = 0;
@@ -162,6 +174,12 @@ public:
   void minimizeRange(int first, int count, const sb_minimize_controls &ctl, cudaStream_t stream);
   void getMinimizeHistory(double* out, cudaStream_t stream);
   void getMinimizeProgress(int* cycles, int* converged, double* rms, cudaStream_t stream);
+  // One system's minimizer state between cycles (coordinates, previous forces, conjugate
+  // direction, move length, cycle count, convergence flag, RMS force), read out of this
+  // synthesis or written into another one whose system has the same topology: the system then
+  // continues exactly as it would have where it was
+  void exportMinimizerState(int system, MinimizerState* state, cudaStream_t stream);
+  void importMinimizerState(int system, const MinimizerState &state, cudaStream_t stream);
 
   sb_options opt;
   int nsys = 0;
@@ -269,6 +287,7 @@ private:
   void buildLayout(const sb_topology* tops, int ntop);
   std::unique_ptr<UnitPlan> makePlan(int max_slots_cap, int max_tiles_cap) const;
   void finalizePlan(UnitPlan* plan) const;
+  int launchThreads(int units, int terms) const;
   void launchPlan(const UnitPlan &plan, int terms, bool force, bool energy, cudaStream_t stream,
                   const Clash &clash = Clash());
   void launchMinPlan(const UnitPlan &plan, int cycles, bool final_energy, cudaStream_t stream);

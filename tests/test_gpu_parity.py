@@ -108,6 +108,28 @@ def test_run_to_run_bit_identical():
         assert np.array_equal(first_e, a.energies_fixed())
 
 
+def test_block_size_changes_no_bit():
+    """A launch of few work units runs 512-thread blocks; 256 threads (set explicitly) give the
+    same fixed-point forces and energies, force+energy and energy-only."""
+    mols = [molecule_from_fixture(load(os.path.basename(p))) for p in default_solvent_paths()]
+    wide = _run(mols)["syn"]
+    narrow = _run(mols, threads_per_block=256)["syn"]
+    units = wide.launch_info()["work_units"]
+    assert units < 2 * 148
+    for syn in (wide, narrow):
+        syn.initialize()
+        syn.evaluate()
+    a, b = wide.forces_fixed(), narrow.forces_fixed()
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    assert np.array_equal(wide.energies_fixed(), narrow.energies_fixed())
+    for syn in (wide, narrow):
+        syn.initialize()
+        syn.evaluate(force=False)
+    assert np.array_equal(wide.energies_fixed(), narrow.energies_fixed())
+    wide.close()
+    narrow.close()
+
+
 def test_per_system_launches_match_batched():
     mols = [molecule_from_fixture(load(os.path.basename(p)))
             for p in default_solvent_paths()[:6]]

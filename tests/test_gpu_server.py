@@ -252,3 +252,36 @@ def test_fp64_server_minimizes_with_the_graph_kernel():
         assert np.array_equal(xyz, syn.coordinates())
         assert np.array_equal(r["energies"], syn.energies()[0])
         syn.close()
+
+
+def test_emptying_batch_moves_its_molecules_to_waiting_requests():
+    """Slot backfill: one batch at a time, four molecules a batch.  Three small molecules near
+    a minimum converge within a few launches while a large, rough one keeps going; once they
+    have retired, the large one moves with its minimizer state into a new batch beside the
+    waiting requests and the first batch is released.  Every result is bit-identical to
+    minimizing the molecule alone."""
+    controls = dict(total_cycles=150, sd_cycles=30, convergence_rms=3.0, kernel=sb.MIN_PERSISTENT)
+    mols = [synthetic.make_molecule(synthetic._seed(5150 + n, 0), n, 0.02) for n in (12, 14, 16)]
+    mols.append(synthetic.make_molecule(synthetic._seed(5199, 0), 257, 0.5))
+    mols += [synthetic.make_molecule(synthetic._seed(5151, k), n, 0.3)
+             for k, n in enumerate([40, 48, 56, 64])]
+    srv = sb.Server(max_batch_molecules=4, max_batches=1, cycles_per_launch=10, **controls)
+    ids = {srv.submit(m): m for m in mols}
+    assert srv.drain(120.0)
+    results = srv.poll()
+    st = srv.stats()
+    srv.close()
+    assert len(results) == len(mols) and st["failed"] == 0
+    assert st["migrated"] >= 1
+    assert st["admitted"] == len(mols) and st["bytes_in_flight"] == 0.0
+    for r, xyz in results:
+        m = ids[r["request_id"]]
+        syn = sb.Synthesis([m])
+        syn.set_coordinates(m.coords)
+        syn.minimize(**controls)
+        cycles, conv, _ = syn.minimize_progress()
+        assert r["cycles"] == int(cycles[0]) and r["converged"] == bool(conv[0])
+        assert np.array_equal(xyz, syn.coordinates().reshape(-1, 3))
+        assert np.array_equal(r["energies"], syn.energies()[0])
+        assert r["submit_time"] <= r["admit_time"] <= r["finish_time"]
+        syn.close()
