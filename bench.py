@@ -81,6 +81,8 @@ def _args():
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--no-errors", action="store_true")
     ap.add_argument("--no-reference-gpu", action="store_true")
+    ap.add_argument("--reference-gpu-full", action="store_true",
+                    help="compare with STORMM's CUDA path on the whole workloads (slow set-up)")
     return ap.parse_args()
 
 
@@ -629,6 +631,7 @@ def bench_served(local):
             srv.submit(mols[k % len(mols)], prepared=prepared[k % len(mols)])
         drained = srv.drain(600.0)
         res = [r for r, _ in srv.poll(max_results=len(arrivals) + 16, coordinates=False)]
+        moved = srv.stats()["migrated"]
         srv.close()
         lat = np.array([r["finish_time"] - r["submit_time"] for r in res])
         wait = np.array([r["admit_time"] - r["submit_time"] for r in res])
@@ -643,6 +646,7 @@ def bench_served(local):
             "throughput_per_s": len(res) / (last - first),
             "mean_cycles": float(np.mean([r["cycles"] for r in res])),
             "converged_fraction": float(np.mean([r["converged"] for r in res])),
+            "migrated": int(moved),
         })
     # A mixed stream: every other request a force + energy evaluation, the rest minimizations
     rate = 1000.0
@@ -685,41 +689,98 @@ def _cpu_leg(name, seconds):
                 "sample": str(exc)[:200]}
 
 
-def _reference_gpu_leg(args, sp, mn):
+REF_GPU_SP_SAMPLE = 256       # molecules of each workload the reference CUDA leg compares on
+REF_GPU_MIN_SAMPLE = 512
+
+
+def _this_path_on(mols, local, evals, minimize_cycles=0, sd_cycles=0):
+    """This path on the comparison sample, timed the way the reference CUDA leg times STORMM:
+    back-to-back force + energy evaluations (CUDA events, no L2 flush), or the wall time of one
+    minimization call after an untimed one with the same controls."""
+    import torch
+    import stormm_b200 as sb
+    syn = sb.Synthesis(mols, device=local)
+    xyz = np.concatenate([m.coords for m in mols])
+    syn.set_coordinates(xyz)
+    try:
+        if minimize_cycles == 0:
+            for _ in range(3):
+                syn.initialize(sb.INIT_FORCES | sb.INIT_ENERGIES)
+                syn.evaluate()
+            torch.cuda.synchronize()
+            e0, e1 = _event_pair()
+            e0.record()
+            for _ in range(evals):
+                syn.initialize(sb.INIT_FORCES | sb.INIT_ENERGIES)
+                syn.evaluate()
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            return {"value": len(mols) * evals / (ms / 1000.0), "ms_per_eval": ms / evals}
+        ctl = dict(total_cycles=minimize_cycles, sd_cycles=sd_cycles, kernel=sb.MIN_GRAPH)
+        syn.minimize(**ctl)
+        syn.set_coordinates(xyz)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        syn.minimize(**ctl)
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - t0) * 1000.0
+        return {"value": len(mols) / (ms / 1000.0), "ms": ms}
+    finally:
+        syn.close()
+
+
+def _reference_gpu_leg(args, local):
     """STORMM's own CUDA path (oracle/_ref_gpu, built from the reference sources by
-    oracle/ref_gpu/Makefile) on the same GPU and the same molecules: launchNonbonded +
-    launchValence over the batched single-point workload and launchMinimization over the
-    minimization workload, each in a subprocess that maps only STORMM's library and CUDA's.
-    Reported beside this path's numbers; a failure is reported, not fatal."""
+    oracle/ref_gpu/Makefile) against this path on the same GPU and the same molecules:
+    launchNonbonded + launchValence against the fused evaluation, launchMinimization against
+    the graph minimizer, STORMM's in a subprocess that maps only STORMM's library and CUDA's.
+    STORMM's host set-up of a synthesis grows steeply with the number of distinct topologies
+    (about 4 minutes for the 1,024 molecules of the single point, 13 for the 4,096 of the
+    minimization batch, measured on the B200 host), so by default both run on the workloads'
+    leading molecules (REF_GPU_SP_SAMPLE, REF_GPU_MIN_SAMPLE) and --reference-gpu-full runs the
+    whole workloads.  A failure is reported, not fatal."""
     from oracle import gpu_reference as gref
     if not gref.available():
         return {"available": False, "why": "reference CUDA build absent (oracle/ref_gpu/Makefile)"}
     out = {"available": True,
            "build": "STORMM's sources with its CUDA path, nvcc -O3 --use_fast_math sm_100",
            "precision": "STORMM PrecisionModel::SINGLE (FP32, split fixed-point accumulation)"}
+    full = args.reference_gpu_full
+    evals = max(20, args.steps)
     try:
-        lst = gref.write_inputs(f"single_point_{NSYS}", single_point_molecules(1, 0))
-        r = gref.time_evaluations(lst, max(20, args.steps))
+        mols = single_point_molecules(1, 0)
+        mols = mols if full else mols[:REF_GPU_SP_SAMPLE]
+        lst = gref.write_inputs(f"single_point_{len(mols)}", mols)
+        r = gref.time_evaluations(lst, evals)
+        ours = _this_path_on(mols, local, evals)
         out["single_point"] = {
             "value": r["value"], "unit": "force-evals/s", "ms_per_eval": r["ms_per_eval"],
-            "systems": r["systems"], "atoms": r["atoms"], "evals": r["evals"],
-            "timing": "CUDA events over back-to-back evaluations, L2 not flushed (inputs fit "
-                      "in L2), the launches of the first stage of its minimizer's cycle",
-            "ratio_this_path": sp["value"] / r["value"]}
+            "this_path_value": ours["value"], "this_path_ms_per_eval": ours["ms_per_eval"],
+            "ratio_this_path": ours["value"] / r["value"],
+            "molecules": len(mols), "atoms": r["atoms"], "evals": r["evals"],
+            "timing": "both: CUDA events over back-to-back force + energy evaluations (clear the "
+                      "accumulators, evaluate), L2 not flushed"}
     except Exception as exc:  # reported, not fatal
         out["single_point"] = {"error": str(exc)[:300]}
-    if mn is not None:
+    if not args.no_minimization:
         try:
-            lst = gref.write_inputs(f"minimization_{MIN_NSYS}", minimization_molecules(1, 0))
+            mols = minimization_molecules(1, 0)
+            mols = mols if full else mols[:REF_GPU_MIN_SAMPLE]
+            lst = gref.write_inputs(f"minimization_{len(mols)}", mols)
             with tempfile.TemporaryDirectory() as tmp:
                 r = gref.minimize(lst, os.path.join(tmp, "min.bin"), MIN_CYCLES, MIN_SD_CYCLES,
                                   ntpr=MIN_CYCLES)
+            ours = _this_path_on(mols, local, 0, MIN_CYCLES, MIN_SD_CYCLES)
             out["minimization"] = {
                 "value": r["value"], "unit": "minimizations/s", "ms": r["ms"],
-                "systems": r["systems"], "cycles": MIN_CYCLES, "sd_cycles": MIN_SD_CYCLES,
-                "timing": "wall time of one launchMinimization call (its set-up included)",
-                "mean_final_energy": float(np.mean(r["final_terms"].sum(axis=1))),
-                "ratio_this_path": mn["value"] / r["value"]}
+                "this_path_value": ours["value"], "this_path_ms": ours["ms"],
+                "ratio_this_path": ours["value"] / r["value"],
+                "molecules": r["systems"], "cycles": MIN_CYCLES, "sd_cycles": MIN_SD_CYCLES,
+                "timing": "wall time of one minimization call: STORMM's launchMinimization (its "
+                          "launch set-up included), this path's graph minimizer (its cycle graph "
+                          "captured by an untimed call)",
+                "mean_final_energy": float(np.mean(r["final_terms"].sum(axis=1)))}
         except Exception as exc:  # reported, not fatal
             out["minimization"] = {"error": str(exc)[:300]}
     return out
@@ -757,7 +818,7 @@ def main_rank(args):
             large["cpu_baseline"] = _cpu_leg("large", args.cpu_seconds)
     ref_gpu = None
     if rank == 0 and world == 1 and not args.no_reference_gpu:
-        ref_gpu = _reference_gpu_leg(args, sp, mn)
+        ref_gpu = _reference_gpu_leg(args, local)
 
     if rank == 0:
         info = sp["info"]
@@ -815,7 +876,8 @@ def main_rank(args):
                 "cpu_baseline": (mn.get("cpu_baseline") or {}).get("value")}
         if ref_gpu is not None and ref_gpu.get("available"):
             line["reference_gpu"] = {
-                k: {f: v.get(f) for f in ("value", "ratio_this_path", "error") if f in v}
+                k: {f: v.get(f) for f in ("value", "this_path_value", "ratio_this_path",
+                                          "molecules", "error") if f in v}
                 for k, v in ref_gpu.items() if isinstance(v, dict)}
         print(json.dumps(line, default=float), flush=True)
     if world > 1:

@@ -316,8 +316,9 @@ int sb_get_minimize_progress(sb_synthesis* syn, int* cycles_done, int* converged
  * topology, coordinates and minimizer state resident on the device, runs its minimization in
  * launches of cycles_per_launch cycles on a stream of its own (batches overlap on the GPU),
  * retires every molecule that converged or reached total_cycles after each launch, and
- * backfills: new batches start while older ones are still running, and when three quarters of a
- * minimization batch have retired while minimizations wait, its remaining molecules move with
+ * backfills: new batches start while older ones are still running, and when all but
+ * migrate_fraction of a minimization batch have retired while minimizations wait, its remaining
+ * molecules move with
  * their minimizer state into a new batch beside the waiting requests and the old batch's memory
  * is released (persistent FP32 minimizer).  A molecule's result does not depend on the batch it
  * ran in, nor on a move.
@@ -338,6 +339,9 @@ typedef struct {
   int max_batch_molecules;           /* most molecules admitted into one batch */
   int max_batches;                   /* batches in flight at once, one CUDA stream each */
   int cycles_per_launch;             /* minimization cycles per launch of a batch */
+  double migrate_fraction;           /* move a minimization batch's remaining molecules into a
+                                        new batch once this fraction of it or less remains and
+                                        minimizations wait, in [0, 1); 0: never (default 0.25) */
 } sb_server_options;
 
 #define SB_REQUEST_MINIMIZE 0          /* run the minimization, return the final coordinates */

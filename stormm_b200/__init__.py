@@ -77,6 +77,7 @@ class ServerOptions(ctypes.Structure):
         ("options", Options), ("controls", MinimizeControls),
         ("hbm_budget_bytes", ctypes.c_double), ("max_batch_molecules", ctypes.c_int),
         ("max_batches", ctypes.c_int), ("cycles_per_launch", ctypes.c_int),
+        ("migrate_fraction", ctypes.c_double),
     ]
 
 
@@ -778,7 +779,8 @@ class Server:
     their final coordinates (minimization) or forces (evaluation)."""
 
     def __init__(self, budget_bytes=2.0e9, max_batch_molecules=512, max_batches=16,
-                 cycles_per_launch=50, options: Options | None = None, **controls):
+                 cycles_per_launch=50, options: Options | None = None, migrate_fraction=None,
+                 **controls):
         lib = library()
         o = ServerOptions()
         lib.sb_default_server_options(ctypes.byref(o))
@@ -790,6 +792,8 @@ class Server:
         o.max_batch_molecules = int(max_batch_molecules)
         o.max_batches = int(max_batches)
         o.cycles_per_launch = int(cycles_per_launch)
+        if migrate_fraction is not None:
+            o.migrate_fraction = float(migrate_fraction)
         self.options = o
         handle = ctypes.c_void_p()
         _check(lib.sb_server_create(ctypes.byref(o), ctypes.byref(handle)), "sb_server_create")

@@ -189,6 +189,9 @@ public:
       throw Error(SB_ERR_ARGUMENT, "server budget, batch limits and cycles per launch must be "
                   "positive");
     }
+    if (!(o.migrate_fraction >= 0.0 && o.migrate_fraction < 1.0)) {
+      throw Error(SB_ERR_ARGUMENT, "migrate_fraction must lie in [0, 1)");
+    }
     validateMinimizeControls(o.controls);
     if (o.options.precision != SB_PRECISION_SINGLE && o.options.precision != SB_PRECISION_DOUBLE) {
       throw Error(SB_ERR_ARGUMENT, "precision must be SB_PRECISION_SINGLE or SB_PRECISION_DOUBLE");
@@ -695,7 +698,8 @@ private:
   bool shouldMigrate(const Batch* b) {
     if (opt_.controls.kernel != SB_MIN_PERSISTENT ||
         opt_.options.precision != SB_PRECISION_SINGLE || b->reqs.size() < 2 ||
-        4 * b->remaining > static_cast<int>(b->reqs.size())) {
+        static_cast<double>(b->remaining) >
+            opt_.migrate_fraction * static_cast<double>(b->reqs.size())) {
       return false;
     }
     std::lock_guard<std::mutex> lock(mu_);
@@ -829,6 +833,7 @@ void sb_default_server_options(sb_server_options* opt) {
   opt->max_batch_molecules = 512;
   opt->max_batches = 16;
   opt->cycles_per_launch = 50;
+  opt->migrate_fraction = 0.25;
 }
 
 int sb_server_create(const sb_server_options* opt, sb_server** out) {

@@ -115,7 +115,7 @@ def test_block_size_changes_no_bit():
     wide = _run(mols)["syn"]
     narrow = _run(mols, threads_per_block=256)["syn"]
     units = wide.launch_info()["work_units"]
-    assert units < 2 * 148
+    assert units < 4 * 148
     for syn in (wide, narrow):
         syn.initialize()
         syn.evaluate()

@@ -60,3 +60,17 @@ def test_served_result_layout_matches_the_header():
     assert r.status.offset == 24 and r.rms_force.offset == 32
     assert ctypes.sizeof(r) == 32 + 8 + 8 + 8 * 16 + 3 * 8
     assert stormm_b200.ServerStats.failed.offset == 24
+    assert stormm_b200.ServerStats.migrated.offset == 32
+
+
+def test_server_options_default_and_checks():
+    """sb_default_server_options sets every field (the migration threshold included), and the
+    server refuses a migration threshold outside [0, 1)."""
+    o = stormm_b200.ServerOptions()
+    stormm_b200.library().sb_default_server_options(ctypes.byref(o))
+    assert o.migrate_fraction == 0.25 and o.cycles_per_launch == 50
+    assert stormm_b200.ServerOptions.migrate_fraction.offset == (
+        stormm_b200.ServerOptions.cycles_per_launch.offset + 8)
+    for bad in (-0.1, 1.0):
+        with pytest.raises(stormm_b200.StormmB200Error, match="migrate_fraction"):
+            stormm_b200.Server(migrate_fraction=bad)
