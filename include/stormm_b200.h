@@ -447,6 +447,118 @@ int sb_nonbonded_work_units(const sb_topology* tops, int ntop, const int* topolo
                             long long* n_instructions);
 
 /* ------------------------------------------------------------------------------------------ */
+/* STORMM's valence work units                                                                 */
+/* ------------------------------------------------------------------------------------------ */
+/* The valence terms and constraint groups of one topology in STORMM's own order and indexing:
+ * the fields of its ValenceKit, ConstraintKit and NonbondedKit (Topology/atomgraph_abstracts.h)
+ * that buildValenceWorkUnits reads.  Parameter indices are the topology's.  dihe_kind is
+ * STORMM's TorsionKind (0 PROPER, 1 PROPER_NO_14, 2 IMPROPER, 3 IMPROPER_NO_14).  The
+ * relevance arrays are STORMM's bit masks (bit k of word k / 32 set: term k is evaluated); NULL
+ * marks a term relevant when none of its atoms has atomic number 0 (STORMM's rule without
+ * SHAKE / SETTLE).  solvent flags the atoms whose molecule is a single atom or a water (NULL:
+ * single-atom molecules, found from the 1-2 lists).  Urey-Bradley, CHARMM improper and CMAP
+ * terms, restraints and virtual sites are not represented; atoms of atomic number 0 are
+ * refused. */
+typedef struct {
+  int natom;
+  const int* z_numbers;          /* natom atomic numbers (NULL: all nonzero) */
+  const int* nb12_bounds;        /* natom + 1, CSR bounds of each atom's 1-2 partners */
+  const int* nb12_list;
+  const int* solvent;            /* natom flags (NULL: from the 1-2 lists) */
+  int nbond;
+  const int* bond_i;
+  const int* bond_j;
+  const int* bond_param;
+  const uint32_t* bond_relevance;
+  int nangl;
+  const int* angl_i;
+  const int* angl_j;
+  const int* angl_k;
+  const int* angl_param;
+  const uint32_t* angl_relevance;
+  int ndihe;
+  const int* dihe_i;
+  const int* dihe_j;
+  const int* dihe_k;
+  const int* dihe_l;
+  const int* dihe_param;
+  const int* dihe14_param;       /* 1-4 scaling-factor pair of each dihedral */
+  const int* dihe_kind;
+  int ninfr14;                   /* inferred 1-4 pairs (not carried by a dihedral) */
+  const int* infr14_i;
+  const int* infr14_l;
+  const int* infr14_param;
+  int nsettle;                   /* SETTLE groups (rigid waters) */
+  const int* settle_ox;
+  const int* settle_h1;
+  const int* settle_h2;
+  const int* settle_param;
+  int ngroup;                    /* hub-and-spoke constraint groups, central atom first */
+  const int* group_bounds;       /* ngroup + 1 */
+  const int* group_list;
+  const int* group_param;
+  const int* group_param_bounds; /* offsets of each group parameter set's bond lengths */
+} sb_valence_topology;
+
+typedef struct sb_valence_units sb_valence_units;
+
+/* STORMM's valence work units of one topology (Synthesis/valence_workunit.cpp:
+ * ValenceDelegator, ValenceWorkUnit, buildValenceWorkUnits with a blank RestraintApparatus):
+ * units grown from the first unassigned atom through the 1-2 graph up to atom_limit imported
+ * atoms (solvent_atom_limit for a unit seeded on a solvent atom), each atom updated by exactly
+ * one unit, each term's energy accumulated by the first unit that evaluates it, and the
+ * instructions STORMM stores against the topology's own parameter indices.  Limits lie in
+ * [32, 512].  Host only.  Release with sb_valence_units_destroy. */
+int sb_valence_work_units(const sb_valence_topology* top, int atom_limit, int solvent_atom_limit,
+                          sb_valence_units** out);
+int sb_valence_units_destroy(sb_valence_units* units);
+int sb_valence_unit_count(const sb_valence_units* units, int* count);
+
+#define SB_VWU_TASKS 16          /* STORMM's VwuTask order: BOND ANGL DIHE UBRD CBND CIMP CDHE
+                                    CMAP INFR14 RPOSN RBOND RANGL RDIHE VSITE SETTLE CGROUP */
+
+/* One unit, pointers into the set's storage (valid until it is destroyed).  Counts of the term
+ * lists and instruction arrays are the task counts; each acc_* mask has (count + 31) / 32 words,
+ * bit k set when the unit accumulates the energy of its k-th term of that kind. */
+typedef struct {
+  int imported_atoms;            /* getImportedAtomCount */
+  int moved_atoms;               /* getMovedAtomCount */
+  int updated_atoms;             /* getUpdatedAtomCount */
+  int task_counts[SB_VWU_TASKS]; /* getTaskCounts */
+  int n_manip;                   /* manipulation-mask entries (a multiple of 32) */
+  const int* imports;            /* imported atoms, ascending topology indices */
+  const uint32_t* manip;         /* n_manip (x, y) pairs: import mask, update mask */
+  const uint32_t* update_flags;  /* (imported_atoms + 31) / 32 words: getAtomUpdateFlags */
+  const int* bond_terms;         /* topology term indices, ascending */
+  const int* angl_terms;
+  const int* dihe_terms;
+  const int* infr14_terms;
+  const int* cbnd_terms;         /* composite bonds: the bonds (no Urey-Bradley terms) */
+  const int* cdhe_terms;         /* composite dihedrals: (first, second or -1) pairs */
+  const uint32_t* acc_bond;
+  const uint32_t* acc_angl;
+  const uint32_t* acc_dihe;
+  const uint32_t* acc_cbnd;
+  const uint32_t* acc_cdhe;
+  const uint32_t* acc_infr14;
+  const uint32_t* cbnd_insr;     /* 2 words per composite bond */
+  const uint32_t* angl_insr;     /* 2 words per angle */
+  const uint32_t* cdhe_insr;     /* 3 words per composite dihedral */
+  const uint32_t* infr14_insr;   /* 1 word per inferred 1-4 pair */
+  const uint32_t* settle_insr;   /* 2 words per SETTLE group */
+  const uint32_t* cgroup_insr;   /* 2 words per constraint slot (task_counts[15], padded) */
+} sb_valence_unit_view;
+
+int sb_valence_unit(const sb_valence_units* units, int unit, sb_valence_unit_view* view);
+
+/* calculateValenceWorkUnitSize (Synthesis/valence_workunit.cpp, the overload with an SM count)
+ * for a synthesis of nsys systems in isolated boundary conditions: the atom limit and STORMM's
+ * ValenceKernelSize (0 XL, 1 LG, 2 MD, 3 SM) it picks.  With sm_count <= 0 the overload without
+ * one: the size of least padding, kernel width not set. */
+int sb_valence_work_unit_size(const int* atom_counts, int nsys, int sm_count, int* atom_limit,
+                              int* kernel_width);
+
+/* ------------------------------------------------------------------------------------------ */
 /* Amber file intake                                                                           */
 /* ------------------------------------------------------------------------------------------ */
 /* An Amber topology (prmtop) read from disk: what STORMM's AtomGraph(file_name) reads

@@ -28,6 +28,17 @@
 //       The coordinates of an Amber input-coordinate file written back by STORMM's
 //       PhaseSpace::exportToFile (CoordinateFileKind::AMBER_INPCRD).
 //
+//   vwu <prmtop> <out.bin> [--vwu-atoms N]
+//       STORMM's valence work units of one topology (Synthesis/valence_workunit.cpp,
+//       buildValenceWorkUnits with a blank RestraintApparatus and an atom limit of N, default
+//       the synthesis sizing for one copy on 148 SMs): the ValenceKit arrays they are built from
+//       and, per unit, the import / update lists, manipulation masks, task counts, term lists,
+//       energy-accumulation masks and the instructions stored against the topology's own
+//       parameter indices.
+//   vwusize <counts-file> <sm-count> <out.bin>
+//       calculateValenceWorkUnitSize over each line of atom counts (one synthesis per line):
+//       the atom limit and kernel width it picks for that many SMs (sm-count 0: the overload
+//       without an SM count).
 //   nbwu <list-file> <out.bin> [--init-task N]
 //       STORMM's nonbonded work units (Synthesis/nonbonded_workunit.cpp) for a synthesis: each
 //       line of <list-file> is "<prmtop> <system count>", the systems laid out topology by
@@ -67,6 +78,7 @@
 #include "Synthesis/atomgraph_synthesis.h"
 #include "Synthesis/static_mask_synthesis.h"
 #include "Synthesis/synthesis_abstracts.h"
+#include "Synthesis/valence_workunit.h"
 #include "Topology/atomgraph.h"
 #include "Trajectory/phasespace.h"
 #include "Trajectory/trajectory_enumerators.h"
@@ -664,6 +676,218 @@ int runNbwu(const std::string &list_file, const std::string &out, const Options 
   return 0;
 }
 
+// Valence work units of one topology, with the inputs they are built from
+int runVwu(const std::string &prmtop, const std::string &out, const Options &opt, int atoms) {
+  const AtomGraph ag = loadTopology(prmtop, opt);
+  const ValenceKit<double> vk = ag.getDoublePrecisionValenceKit();
+  const NonbondedKit<double> nbk = ag.getDoublePrecisionNonbondedKit();
+  const ChemicalDetailsKit cdk = ag.getChemicalDetailsKit();
+  if (atoms <= 0) {
+    energy::ValenceKernelSize kw;
+    atoms = synthesis::calculateValenceWorkUnitSize(std::vector<int>(1, ag.getAtomCount()), 148,
+                                                    &kw).x;
+  }
+  const RestraintApparatus ra(&ag);
+  const std::vector<synthesis::ValenceWorkUnit> units =
+      synthesis::buildValenceWorkUnits(&ag, &ra, {atoms, atoms});
+  RecordWriter rw(out);
+  rw.iscalar("natom", ag.getAtomCount());
+  rw.iscalar("atom_limit", atoms);
+  rw.i("z_numbers", cdk.z_numbers, cdk.natom);
+  rw.i("nb12_bounds", nbk.nb12_bounds, nbk.natom + 1);
+  rw.i("nb12x", nbk.nb12x, nbk.nb12_bounds[nbk.natom]);
+  // the decision buildValenceWorkUnits makes for a unit seeded on each atom
+  const int water_natom = ag.getWaterResidueSize();
+  const std::string water_name = ag.getWaterResidueName();
+  std::vector<int> solvent(cdk.natom);
+  for (int a = 0; a < cdk.natom; a++) {
+    const int m = cdk.mol_home[a];
+    const int mn = cdk.mol_limits[m + 1] - cdk.mol_limits[m];
+    const char4 rn = cdk.res_names[ag.getResidueIndex(a)];
+    const std::string rns = {rn.x, rn.y, rn.z, rn.w};
+    solvent[a] = (mn == 1) ||
+                 (mn == water_natom && rns.substr(0, water_name.size()) == water_name &&
+                  rns.find_first_not_of(' ', water_name.size()) == std::string::npos);
+  }
+  rw.i("solvent", solvent);
+  rw.i("counts_ub_cimp_cmap", std::vector<int>{vk.nubrd, vk.ncimp, vk.ncmap});
+  rw.u("bond_relevance", vk.bond_relevance, (vk.nbond + 31) / 32);
+  rw.u("angl_relevance", vk.angl_relevance, (vk.nangl + 31) / 32);
+  {
+    const ConstraintKit<double> cnk = ag.getDoublePrecisionConstraintKit();
+    const VirtualSiteKit<double> vsk = ag.getDoublePrecisionVirtualSiteKit();
+    rw.i("counts_settle_cgroup_vsite", std::vector<int>{cnk.nsettle, cnk.ngroup, vsk.nsite});
+    rw.i("settle_ox", cnk.settle_ox_atoms, cnk.nsettle);
+    rw.i("settle_h1", cnk.settle_h1_atoms, cnk.nsettle);
+    rw.i("settle_h2", cnk.settle_h2_atoms, cnk.nsettle);
+    rw.i("settle_param", cnk.settle_param_idx, cnk.nsettle);
+    rw.i("group_bounds", cnk.group_bounds, cnk.ngroup + 1);
+    rw.i("group_list", cnk.group_list, cnk.group_bounds[cnk.ngroup]);
+    rw.i("group_param", cnk.group_param_idx, cnk.ngroup);
+    rw.i("group_param_bounds", cnk.group_param_bounds, cnk.ncnst_param + 1);
+  }
+  rw.i("bond_i", vk.bond_i_atoms, vk.nbond);
+  rw.i("bond_j", vk.bond_j_atoms, vk.nbond);
+  rw.i("bond_param", vk.bond_param_idx, vk.nbond);
+  rw.i("angl_i", vk.angl_i_atoms, vk.nangl);
+  rw.i("angl_j", vk.angl_j_atoms, vk.nangl);
+  rw.i("angl_k", vk.angl_k_atoms, vk.nangl);
+  rw.i("angl_param", vk.angl_param_idx, vk.nangl);
+  rw.i("dihe_i", vk.dihe_i_atoms, vk.ndihe);
+  rw.i("dihe_j", vk.dihe_j_atoms, vk.ndihe);
+  rw.i("dihe_k", vk.dihe_k_atoms, vk.ndihe);
+  rw.i("dihe_l", vk.dihe_l_atoms, vk.ndihe);
+  rw.i("dihe_param", vk.dihe_param_idx, vk.ndihe);
+  rw.i("dihe14_param", vk.dihe14_param_idx, vk.ndihe);
+  std::vector<int> kind(vk.ndihe);
+  for (int k = 0; k < vk.ndihe; k++) {
+    kind[k] = static_cast<int>(vk.dihe_modifiers[k].w);
+  }
+  rw.i("dihe_kind", kind);
+  rw.i("infr14_i", vk.infr14_i_atoms, vk.ninfr14);
+  rw.i("infr14_l", vk.infr14_l_atoms, vk.ninfr14);
+  rw.i("infr14_param", vk.infr14_param_idx, vk.ninfr14);
+  // per unit, concatenated: bounds arrays give each unit's range
+  std::vector<int> imp, imp_b{0}, upd_flags, upd_b{0}, manip, manip_b{0}, tasks;
+  std::vector<int> lists[4], list_b[4], cbnd_list, cbnd_b{0}, cdhe_list, cdhe_b{0};
+  std::vector<uint> acc[6], cbnd_insr, angl_insr, cdhe_insr, infr_insr, sett_insr, cnst_insr;
+  std::vector<int> moved, sett_b{0}, cnst_b{0};
+  std::vector<int> acc_b[6];
+  for (int t = 0; t < 6; t++) acc_b[t].push_back(0);
+  for (int t = 0; t < 4; t++) list_b[t].push_back(0);
+  const synthesis::VwuTask simple[4] = {synthesis::VwuTask::BOND, synthesis::VwuTask::ANGL,
+                                        synthesis::VwuTask::DIHE, synthesis::VwuTask::INFR14};
+  const synthesis::VwuTask acc_tasks[6] = {synthesis::VwuTask::BOND, synthesis::VwuTask::ANGL,
+                                           synthesis::VwuTask::DIHE, synthesis::VwuTask::CBND,
+                                           synthesis::VwuTask::CDHE, synthesis::VwuTask::INFR14};
+  for (const synthesis::ValenceWorkUnit &u : units) {
+    const std::vector<int> il = u.getAtomImportList();
+    imp.insert(imp.end(), il.begin(), il.end());
+    imp_b.push_back(imp.size());
+    const std::vector<uint> uf = u.getAtomUpdateFlags();
+    for (uint w : uf) upd_flags.push_back(static_cast<int>(w));
+    upd_b.push_back(upd_flags.size());
+    for (const uint2 m : u.getAtomManipulationMasks()) {
+      manip.push_back(static_cast<int>(m.x));
+      manip.push_back(static_cast<int>(m.y));
+    }
+    manip_b.push_back(manip.size());
+    const std::vector<int> tc = u.getTaskCounts();
+    tasks.insert(tasks.end(), tc.begin(), tc.end());
+    for (int t = 0; t < 4; t++) {
+      const std::vector<int> &l = u.getSimpleTaskList(simple[t]);
+      lists[t].insert(lists[t].end(), l.begin(), l.end());
+      list_b[t].push_back(lists[t].size());
+    }
+    const std::vector<int> &cb = u.getCompositeBondTaskList();
+    cbnd_list.insert(cbnd_list.end(), cb.begin(), cb.end());
+    cbnd_b.push_back(cbnd_list.size());
+    for (const int2 c : u.getCompositeDihedralTaskList()) {
+      cdhe_list.push_back(c.x);
+      cdhe_list.push_back(c.y);
+    }
+    cdhe_b.push_back(cdhe_list.size());
+    for (int t = 0; t < 6; t++) {
+      const std::vector<uint> &a = u.getAccumulationFlags(acc_tasks[t]);
+      acc[t].insert(acc[t].end(), a.begin(), a.end());
+      acc_b[t].push_back(acc[t].size());
+    }
+    for (const uint2 v : u.getCompositeBondInstructions()) {
+      cbnd_insr.push_back(v.x);
+      cbnd_insr.push_back(v.y);
+    }
+    for (const uint2 v : u.getAngleInstructions()) {
+      angl_insr.push_back(v.x);
+      angl_insr.push_back(v.y);
+    }
+    for (const uint3 v : u.getCompositeDihedralInstructions()) {
+      cdhe_insr.push_back(v.x);
+      cdhe_insr.push_back(v.y);
+      cdhe_insr.push_back(v.z);
+    }
+    for (const uint v : u.getInferred14Instructions()) {
+      infr_insr.push_back(v);
+    }
+    for (const uint2 v : u.getSettleGroupInstructions()) {
+      sett_insr.push_back(v.x);
+      sett_insr.push_back(v.y);
+    }
+    sett_b.push_back(sett_insr.size());
+    for (const uint2 v : u.getConstraintGroupInstructions()) {
+      cnst_insr.push_back(v.x);
+      cnst_insr.push_back(v.y);
+    }
+    cnst_b.push_back(cnst_insr.size());
+    moved.push_back(u.getMovedAtomCount());
+  }
+  rw.iscalar("nunit", units.size());
+  rw.i("imports", imp);
+  rw.i("imports_bounds", imp_b);
+  rw.i("update_flags", upd_flags);
+  rw.i("update_flags_bounds", upd_b);
+  rw.i("manip", manip);
+  rw.i("manip_bounds", manip_b);
+  rw.i("task_counts", tasks);
+  const char* lnames[4] = {"bond", "angl", "dihe", "infr14"};
+  for (int t = 0; t < 4; t++) {
+    rw.i(std::string(lnames[t]) + "_terms", lists[t]);
+    rw.i(std::string(lnames[t]) + "_terms_bounds", list_b[t]);
+  }
+  rw.i("cbnd_terms", cbnd_list);
+  rw.i("cbnd_terms_bounds", cbnd_b);
+  rw.i("cdhe_terms", cdhe_list);
+  rw.i("cdhe_terms_bounds", cdhe_b);
+  const char* anames[6] = {"bond", "angl", "dihe", "cbnd", "cdhe", "infr14"};
+  for (int t = 0; t < 6; t++) {
+    rw.u(std::string("acc_") + anames[t], acc[t].data(), acc[t].size());
+    rw.i(std::string("acc_") + anames[t] + "_bounds", acc_b[t]);
+  }
+  rw.u("cbnd_insr", cbnd_insr.data(), cbnd_insr.size());
+  rw.u("angl_insr", angl_insr.data(), angl_insr.size());
+  rw.u("cdhe_insr", cdhe_insr.data(), cdhe_insr.size());
+  rw.u("infr14_insr", infr_insr.data(), infr_insr.size());
+  rw.u("settle_insr", sett_insr.data(), sett_insr.size());
+  rw.i("settle_insr_bounds", sett_b);
+  rw.u("cgroup_insr", cnst_insr.data(), cnst_insr.size());
+  rw.i("cgroup_insr_bounds", cnst_b);
+  rw.i("moved_counts", moved);
+  std::printf("atoms %d, limit %d, units %zu\n", ag.getAtomCount(), atoms, units.size());
+  return 0;
+}
+
+// calculateValenceWorkUnitSize over syntheses given as lines of atom counts
+int runVwuSize(const std::string &counts_file, int sm_count, const std::string &out) {
+  std::ifstream in(counts_file);
+  std::string line;
+  std::vector<int> sizes, widths;
+  while (std::getline(in, line)) {
+    std::vector<int> counts;
+    size_t p = 0;
+    while (p < line.size()) {
+      size_t q = line.find(' ', p);
+      if (q == std::string::npos) q = line.size();
+      if (q > p) counts.push_back(std::atoi(line.substr(p, q - p).c_str()));
+      p = q + 1;
+    }
+    if (counts.empty()) continue;
+    if (sm_count > 0) {
+      energy::ValenceKernelSize kw;
+      const int2 sz = synthesis::calculateValenceWorkUnitSize(counts, sm_count, &kw);
+      sizes.push_back(sz.x);
+      widths.push_back(static_cast<int>(kw));
+    }
+    else {
+      const int2 sz = synthesis::calculateValenceWorkUnitSize(counts);
+      sizes.push_back(sz.x);
+      widths.push_back(-1);
+    }
+  }
+  RecordWriter rw(out);
+  rw.i("sizes", sizes);
+  rw.i("widths", widths);
+  return 0;
+}
+
 } // namespace
 
 int main(int argc, char* argv[]) {
@@ -675,6 +899,7 @@ int main(int argc, char* argv[]) {
   std::vector<std::string> pos;
   Options opt;
   int init_task = 3;
+  int vwu_atoms = 0;
   for (int i = 2; i < argc; i++) {
     const std::string a(argv[i]);
     auto next = [&]() -> double {
@@ -700,6 +925,7 @@ int main(int argc, char* argv[]) {
     else if (a == "--clash-ratio") opt.clash_ratio = next();
     else if (a == "--quantize") opt.quantize = true;
     else if (a == "--init-task") init_task = static_cast<int>(next());
+    else if (a == "--vwu-atoms") vwu_atoms = static_cast<int>(next());
     else pos.push_back(a);
   }
   if (mode == "eval" && pos.size() == 3) {
@@ -716,6 +942,12 @@ int main(int argc, char* argv[]) {
   }
   if (mode == "geometry" && pos.size() == 3) {
     return runGeometry(pos[0], pos[1], pos[2], opt);
+  }
+  if (mode == "vwu" && pos.size() == 2) {
+    return runVwu(pos[0], pos[1], opt, vwu_atoms);
+  }
+  if (mode == "vwusize" && pos.size() == 3) {
+    return runVwuSize(pos[0], std::atoi(pos[1].c_str()), pos[2]);
   }
   if (mode == "writecrd" && pos.size() == 2) {
     return runWriteCrd(pos[0], pos[1]);

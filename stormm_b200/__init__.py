@@ -62,6 +62,43 @@ class Options(ctypes.Structure):
     ]
 
 
+VWU_TASKS = ["BOND", "ANGL", "DIHE", "UBRD", "CBND", "CIMP", "CDHE", "CMAP", "INFR14", "RPOSN",
+             "RBOND", "RANGL", "RDIHE", "VSITE", "SETTLE", "CGROUP"]
+
+
+class ValenceTopology(ctypes.Structure):
+    _fields_ = [
+        ("natom", ctypes.c_int), ("z_numbers", _P), ("nb12_bounds", _P), ("nb12_list", _P),
+        ("solvent", _P),
+        ("nbond", ctypes.c_int), ("bond_i", _P), ("bond_j", _P), ("bond_param", _P),
+        ("bond_relevance", _P),
+        ("nangl", ctypes.c_int), ("angl_i", _P), ("angl_j", _P), ("angl_k", _P),
+        ("angl_param", _P), ("angl_relevance", _P),
+        ("ndihe", ctypes.c_int), ("dihe_i", _P), ("dihe_j", _P), ("dihe_k", _P), ("dihe_l", _P),
+        ("dihe_param", _P), ("dihe14_param", _P), ("dihe_kind", _P),
+        ("ninfr14", ctypes.c_int), ("infr14_i", _P), ("infr14_l", _P), ("infr14_param", _P),
+        ("nsettle", ctypes.c_int), ("settle_ox", _P), ("settle_h1", _P), ("settle_h2", _P),
+        ("settle_param", _P),
+        ("ngroup", ctypes.c_int), ("group_bounds", _P), ("group_list", _P), ("group_param", _P),
+        ("group_param_bounds", _P),
+    ]
+
+
+class ValenceUnitView(ctypes.Structure):
+    _fields_ = [
+        ("imported_atoms", ctypes.c_int), ("moved_atoms", ctypes.c_int),
+        ("updated_atoms", ctypes.c_int), ("task_counts", ctypes.c_int * 16),
+        ("n_manip", ctypes.c_int),
+        ("imports", _P), ("manip", _P), ("update_flags", _P),
+        ("bond_terms", _P), ("angl_terms", _P), ("dihe_terms", _P), ("infr14_terms", _P),
+        ("cbnd_terms", _P), ("cdhe_terms", _P),
+        ("acc_bond", _P), ("acc_angl", _P), ("acc_dihe", _P), ("acc_cbnd", _P),
+        ("acc_cdhe", _P), ("acc_infr14", _P),
+        ("cbnd_insr", _P), ("angl_insr", _P), ("cdhe_insr", _P), ("infr14_insr", _P),
+        ("settle_insr", _P), ("cgroup_insr", _P),
+    ]
+
+
 class MinimizeControls(ctypes.Structure):
     _fields_ = [
         ("total_cycles", ctypes.c_int), ("sd_cycles", ctypes.c_int),
@@ -213,6 +250,16 @@ def library() -> ctypes.CDLL:
             "sb_nonbonded_work_units": (ctypes.c_int, [ctypes.POINTER(Topology), ctypes.c_int, vp,
                                                        ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                        vp, vp, vp, vp]),
+            "sb_valence_work_units": (ctypes.c_int, [ctypes.POINTER(ValenceTopology),
+                                                     ctypes.c_int, ctypes.c_int,
+                                                     ctypes.POINTER(vp)]),
+            "sb_valence_units_destroy": (ctypes.c_int, [vp]),
+            "sb_valence_unit_count": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int)]),
+            "sb_valence_unit": (ctypes.c_int, [vp, ctypes.c_int,
+                                               ctypes.POINTER(ValenceUnitView)]),
+            "sb_valence_work_unit_size": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int,
+                                                         ctypes.POINTER(ctypes.c_int),
+                                                         ctypes.POINTER(ctypes.c_int)]),
             "sb_last_error": (ctypes.c_char_p, []),
             "sb_version": (ctypes.c_char_p, []),
         }
@@ -381,6 +428,95 @@ def nonbonded_work_units(molecules, topology_index=None, init_task=3, random_cac
     _check(lib.sb_nonbonded_work_units(*args, a.ctypes.data, ctypes.byref(na), ins.ctypes.data,
                                        ctypes.byref(ni)), "sb_nonbonded_work_units")
     return a.reshape(-1, 64), ins.reshape(-1, 2)
+
+
+_VWU_COUNTS = {"bond": "nbond", "angl": "nangl", "dihe": "ndihe", "infr14": "ninfr14",
+               "settle": "nsettle"}
+
+
+def valence_work_units(top, atom_limit, solvent_atom_limit=None):
+    """STORMM's valence work units of one topology (host only), from a dict of its ValenceKit /
+    ConstraintKit / NonbondedKit arrays in STORMM's order (keys as the fields of
+    sb_valence_topology; a missing optional array is NULL).  Returns one dict per unit: counts,
+    imports, manipulation masks ((n, 2) uint32), task counts (VWU_TASKS order), term lists,
+    energy-accumulation masks and instructions ((n, words) uint32)."""
+    lib = library()
+    keep = []
+
+    def arr(key, dtype=np.int32):
+        v = top.get(key)
+        if v is None:
+            return None
+        a = np.ascontiguousarray(np.asarray(v), dtype=dtype)
+        keep.append(a)
+        return a.ctypes.data
+
+    t = ValenceTopology()
+    t.natom = int(top["natom"])
+    for f, _ in ValenceTopology._fields_:
+        if f == "natom":
+            continue
+        if f.startswith("n") and f not in ("nb12_bounds", "nb12_list"):
+            continue
+        setattr(t, f, arr(f, np.uint32 if f.endswith("relevance") else np.int32))
+    for stem, count in _VWU_COUNTS.items():
+        first = {"bond": "bond_i", "angl": "angl_i", "dihe": "dihe_i", "infr14": "infr14_i",
+                 "settle": "settle_ox"}[stem]
+        setattr(t, count, 0 if top.get(first) is None else len(top[first]))
+    t.ngroup = 0 if top.get("group_bounds") is None else len(top["group_bounds"]) - 1
+    h = ctypes.c_void_p()
+    lim = int(atom_limit)
+    slim = lim if solvent_atom_limit is None else int(solvent_atom_limit)
+    _check(lib.sb_valence_work_units(ctypes.byref(t), lim, slim, ctypes.byref(h)),
+           "sb_valence_work_units")
+    try:
+        n = ctypes.c_int()
+        _check(lib.sb_valence_unit_count(h, ctypes.byref(n)), "sb_valence_unit_count")
+        out = []
+        for k in range(n.value):
+            v = ValenceUnitView()
+            _check(lib.sb_valence_unit(h, k, ctypes.byref(v)), "sb_valence_unit")
+            tc = list(v.task_counts)
+            u32 = lambda p, c: _host_array(p, c, ctypes.c_uint32, np.uint32)
+            i32 = lambda p, c: _host_array(p, c, ctypes.c_int, np.int32)
+            words = lambda c: (c + 31) // 32
+            nb, na, nd, ncb, ncd, nin, nst, ncg = (tc[0], tc[1], tc[2], tc[4], tc[6], tc[8],
+                                                   tc[14], tc[15])
+            out.append({
+                "imported": v.imported_atoms, "moved": v.moved_atoms, "updated": v.updated_atoms,
+                "task_counts": np.array(tc, dtype=np.int32),
+                "imports": i32(v.imports, v.imported_atoms),
+                "manip": u32(v.manip, 2 * v.n_manip).reshape(-1, 2),
+                "update_flags": u32(v.update_flags, words(v.imported_atoms)),
+                "bond_terms": i32(v.bond_terms, nb), "angl_terms": i32(v.angl_terms, na),
+                "dihe_terms": i32(v.dihe_terms, nd), "infr14_terms": i32(v.infr14_terms, nin),
+                "cbnd_terms": i32(v.cbnd_terms, ncb),
+                "cdhe_terms": i32(v.cdhe_terms, 2 * ncd).reshape(-1, 2),
+                "acc_bond": u32(v.acc_bond, words(nb)), "acc_angl": u32(v.acc_angl, words(na)),
+                "acc_dihe": u32(v.acc_dihe, words(nd)), "acc_cbnd": u32(v.acc_cbnd, words(ncb)),
+                "acc_cdhe": u32(v.acc_cdhe, words(ncd)),
+                "acc_infr14": u32(v.acc_infr14, words(nin)),
+                "cbnd_insr": u32(v.cbnd_insr, 2 * ncb).reshape(-1, 2),
+                "angl_insr": u32(v.angl_insr, 2 * na).reshape(-1, 2),
+                "cdhe_insr": u32(v.cdhe_insr, 3 * ncd).reshape(-1, 3),
+                "infr14_insr": u32(v.infr14_insr, nin),
+                "settle_insr": u32(v.settle_insr, 2 * nst).reshape(-1, 2),
+                "cgroup_insr": u32(v.cgroup_insr, 2 * ncg).reshape(-1, 2),
+            })
+        return out
+    finally:
+        lib.sb_valence_units_destroy(h)
+
+
+def valence_work_unit_size(atom_counts, sm_count):
+    """STORMM's calculateValenceWorkUnitSize for isolated systems: (atom limit, kernel width
+    0-3 = XL/LG/MD/SM, or None without an SM count)."""
+    c = np.ascontiguousarray(atom_counts, dtype=np.int32)
+    lim, width = ctypes.c_int(), ctypes.c_int(-1)
+    _check(library().sb_valence_work_unit_size(c.ctypes.data, c.size, int(sm_count),
+                                                ctypes.byref(lim), ctypes.byref(width)),
+           "sb_valence_work_unit_size")
+    return lim.value, (width.value if sm_count > 0 else None)
 
 
 def _host_array(ptr, count, ctype, dtype):

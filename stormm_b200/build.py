@@ -24,7 +24,7 @@ SYNTH_LIB = os.path.join(PKG, "libstormm_b200_synth.so")
 
 CUDA_SOURCES = ["eval_fused.cu", "minimize.cu", "synthesis.cu", "transfers.cu",
                 "static_scratch.cu", "server.cu", "tiled.cu", "fp64.cu", "line_search.cu",
-                "exclusion_mask.cpp", "amber_io.cpp", "sdf_io.cpp"]
+                "exclusion_mask.cpp", "valence_units.cpp", "amber_io.cpp", "sdf_io.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-ftz=true"]
 
