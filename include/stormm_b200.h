@@ -185,6 +185,12 @@ int sb_get_coordinates(sb_synthesis* syn, double* xyz, void* stream);
 int sb_get_forces(sb_synthesis* syn, double* xyz, void* stream);
 /* energies: nsys * SB_NRG_STRIDE doubles, kcal/mol, STORMM's slot order */
 int sb_get_energies(sb_synthesis* syn, double* energies, void* stream);
+/* No counterpart in the reference (PhaseSpaceSynthesis::download and ScoreCard::download wait):
+ * the forces and energies of sb_get_forces / sb_get_energies enqueued on the stream without
+ * waiting, into page-locked host buffers (refused otherwise), complete once the stream reaches
+ * this point; either may be NULL.  A serving loop with two syntheses on two streams overlaps
+ * one batch's transfers with the other's evaluation. */
+int sb_download_results_async(sb_synthesis* syn, double* forces, double* energies, void* stream);
 /* GB intermediates per atom (unpadded): psi (A^-1), effective radii (A), sum of dE/dR
  * after the chain-rule prefactor, as STORMM's ImplicitSolventWorkspace holds them */
 int sb_get_gb_workspace(sb_synthesis* syn, double* psi, double* radii, double* sumdeijda,

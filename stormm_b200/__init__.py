@@ -189,6 +189,7 @@ def library() -> ctypes.CDLL:
             "sb_get_coordinates": (ctypes.c_int, [vp, vp, vp]),
             "sb_get_forces": (ctypes.c_int, [vp, vp, vp]),
             "sb_get_energies": (ctypes.c_int, [vp, vp, vp]),
+            "sb_download_results_async": (ctypes.c_int, [vp, vp, vp, vp]),
             "sb_get_gb_workspace": (ctypes.c_int, [vp, vp, vp, vp, vp]),
             "sb_get_forces_fixed": (ctypes.c_int, [vp, vp, vp, vp]),
             "sb_get_energies_fixed": (ctypes.c_int, [vp, vp, vp]),
@@ -772,6 +773,15 @@ class Synthesis:
         _check(library().sb_get_energies(self.handle, out.ctypes.data, stream),
                "sb_get_energies")
         return out.reshape(self.nsys, NRG_STRIDE)
+
+    def download_async(self, forces=None, energies=None, stream=None):
+        """Enqueue the forces (3 per atom) and energies (nsys x NRG_STRIDE) into page-locked
+        float64 buffers on the stream without waiting (sb_download_results_async)."""
+        f = None if forces is None else self._output(forces, 3 * self.total_atoms)
+        e = None if energies is None else self._output(energies, self.nsys * NRG_STRIDE)
+        _check(library().sb_download_results_async(
+            self.handle, None if f is None else f.ctypes.data,
+            None if e is None else e.ctypes.data, stream), "sb_download_results_async")
 
     def energy_terms(self, stream=None):
         """Per system, the nine terms in TERM_ORDER."""

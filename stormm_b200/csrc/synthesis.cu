@@ -1077,6 +1077,34 @@ void Synthesis::getEnergies(double* out, cudaStream_t stream) {
   cudaCheck(cudaStreamSynchronize(stream), "energy download");
 }
 
+// Forces and energies exported and copied into the caller's page-locked buffers on the stream,
+// without waiting: a serving loop overlaps one batch's copies with another's evaluation
+void Synthesis::downloadResults(double* forces, double* energies, cudaStream_t stream) {
+  for (const double* p : {static_cast<const double*>(forces), static_cast<const double*>(energies)}) {
+    if (p == nullptr) continue;
+    cudaPointerAttributes attr;
+    cudaCheck(cudaPointerGetAttributes(&attr, p), "cudaPointerGetAttributes");
+    if (attr.type != cudaMemoryTypeHost) {
+      throw Error(SB_ERR_ARGUMENT, "asynchronous downloads need page-locked host buffers");
+    }
+  }
+  if (forces != nullptr) {
+    cudaCheck(launchExportForces(d_xfrc.p, d_yfrc.p, d_zfrc.p, d_xfrc_ovrf.p, d_yfrc_ovrf.p,
+                                 d_zfrc_ovrf.p, d_unpadded_map.p, natom_total,
+                                 std::ldexp(1.0, -opt.frc_bits), d_stage_xyz.p, stream),
+              "force export");
+    cudaCheck(cudaMemcpyAsync(forces, d_stage_xyz.p, sizeof(double) * 3 * natom_total,
+                              cudaMemcpyDeviceToHost, stream), "force download");
+  }
+  if (energies != nullptr) {
+    const int n = nsys * kNrgStride;
+    cudaCheck(launchExportEnergies(d_energies.p, n, std::ldexp(1.0, -opt.nrg_bits),
+                                   d_stage_nrg.p, stream), "energy export");
+    cudaCheck(cudaMemcpyAsync(energies, d_stage_nrg.p, sizeof(double) * n,
+                              cudaMemcpyDeviceToHost, stream), "energy download");
+  }
+}
+
 void Synthesis::getGbWorkspace(double* psi, double* radii, double* sde, cudaStream_t stream) {
   const size_t np = natom_padded;
   std::vector<long long> p(np), q(np);
@@ -1731,6 +1759,11 @@ int sb_get_forces(sb_synthesis* syn, double* xyz, void* stream) {
 
 int sb_get_energies(sb_synthesis* syn, double* energies, void* stream) {
   return guarded([&]() { need(syn)->getEnergies(energies, asStream(stream)); });
+}
+
+int sb_download_results_async(sb_synthesis* syn, double* forces, double* energies,
+                              void* stream) {
+  return guarded([&]() { need(syn)->downloadResults(forces, energies, asStream(stream)); });
 }
 
 int sb_get_gb_workspace(sb_synthesis* syn, double* psi, double* radii, double* sumdeijda,

@@ -161,6 +161,7 @@ public:
   void getForces(double* xyz, cudaStream_t stream);
   void getForcesFixed(long long* prim, int* ovrf, cudaStream_t stream);
   void getEnergies(double* out, cudaStream_t stream);
+  void downloadResults(double* forces, double* energies, cudaStream_t stream);
   void getEnergiesFixed(long long* out, cudaStream_t stream);
   void getGbWorkspace(double* psi, double* radii, double* sde, cudaStream_t stream);
   int checkStatus(cudaStream_t stream);

@@ -130,6 +130,34 @@ def test_block_size_changes_no_bit():
     narrow.close()
 
 
+def test_asynchronous_download_matches_the_getters():
+    """Two syntheses on two streams, results read back with sb_download_results_async into
+    page-locked buffers: equal to the synchronous getters; pageable buffers are refused."""
+    import torch
+    mols = [molecule_from_fixture(load(os.path.basename(p))) for p in default_solvent_paths()]
+    syns = [sb.Synthesis(mols), sb.Synthesis(mols)]
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    xyz = np.concatenate([m.coords for m in mols])
+    n = xyz.size
+    pf = [torch.zeros(n, dtype=torch.float64).pin_memory().numpy() for _ in range(2)]
+    pe = [torch.zeros(len(mols) * sb.NRG_STRIDE, dtype=torch.float64).pin_memory().numpy()
+          for _ in range(2)]
+    for b in range(2):
+        h = streams[b].cuda_stream
+        syns[b].set_coordinates(xyz, stream=h)
+        syns[b].initialize(stream=h)
+        syns[b].evaluate(stream=h)
+        syns[b].download_async(pf[b], pe[b], stream=h)
+    torch.cuda.synchronize()
+    for b in range(2):
+        np.testing.assert_array_equal(pf[b], syns[b].forces().reshape(-1))
+        np.testing.assert_array_equal(pe[b], syns[b].energies().reshape(-1))
+    with pytest.raises(sb.StormmB200Error, match="page-locked"):
+        syns[0].download_async(np.zeros(n), None)
+    for s in syns:
+        s.close()
+
+
 def test_per_system_launches_match_batched():
     mols = [molecule_from_fixture(load(os.path.basename(p)))
             for p in default_solvent_paths()[:6]]
