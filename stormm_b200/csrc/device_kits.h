@@ -230,6 +230,13 @@ enum LineField : int {
   kLineInvNorm, kLineAct, kLineFields
 };
 
+// Arrays zeroed by one launch of launchClear: 16-byte aligned bases, lengths in 16-byte words
+struct ClearList {
+  void* ptr[8];
+  size_t words[8];
+  int count = 0;
+};
+
 }  // namespace sb
 
 #endif

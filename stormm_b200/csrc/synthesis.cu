@@ -53,6 +53,7 @@ cudaError_t launchExportForces(const long long* xf, const long long* yf, const l
                                int natom, double inv_scale, double* d_xyz, cudaStream_t stream);
 cudaError_t launchExportEnergies(const unsigned long long* nrg, int n, double inv_scale,
                                  double* d_out, cudaStream_t stream);
+cudaError_t launchClear(const ClearList &list, int sm_count, cudaStream_t stream);
 
 namespace {
 thread_local std::string g_last_error;
@@ -993,25 +994,43 @@ void Synthesis::evaluateRange(int first, int count, int terms, bool force, bool 
 }
 
 void Synthesis::initialize(int what, cudaStream_t stream) {
+  // every array to clear in one launch (all are multiples of 16 bytes: padded atom counts are
+  // multiples of 32 and systems carry 16 energy slots); anything else falls back to a memset
   const size_t np = natom_padded;
+  ClearList list;
+  auto add = [&](void* p, size_t bytes) {
+    if (bytes % 16 == 0 && list.count < 8) {
+      list.ptr[list.count] = p;
+      list.words[list.count] = bytes / 16;
+      list.count++;
+    }
+    else {
+      cudaCheck(cudaMemsetAsync(p, 0, bytes, stream), "memset");
+    }
+  };
   if (what & SB_INIT_FORCES) {
-    cudaCheck(cudaMemsetAsync(d_xfrc.p, 0, np * sizeof(long long), stream), "memset");
-    cudaCheck(cudaMemsetAsync(d_yfrc.p, 0, np * sizeof(long long), stream), "memset");
-    cudaCheck(cudaMemsetAsync(d_zfrc.p, 0, np * sizeof(long long), stream), "memset");
-    cudaCheck(cudaMemsetAsync(d_xfrc_ovrf.p, 0, np * sizeof(int), stream), "memset");
-    cudaCheck(cudaMemsetAsync(d_yfrc_ovrf.p, 0, np * sizeof(int), stream), "memset");
-    cudaCheck(cudaMemsetAsync(d_zfrc_ovrf.p, 0, np * sizeof(int), stream), "memset");
+    add(d_xfrc.p, np * sizeof(long long));
+    add(d_yfrc.p, np * sizeof(long long));
+    add(d_zfrc.p, np * sizeof(long long));
+    add(d_xfrc_ovrf.p, np * sizeof(int));
+    add(d_yfrc_ovrf.p, np * sizeof(int));
+    add(d_zfrc_ovrf.p, np * sizeof(int));
   }
   if (what & SB_INIT_ENERGIES) {
-    cudaCheck(cudaMemsetAsync(d_energies.p, 0, d_energies.n * sizeof(unsigned long long), stream),
-              "memset");
+    add(d_energies.p, d_energies.n * sizeof(unsigned long long));
   }
   if (what & SB_INIT_GB_WORKSPACE) {
-    cudaCheck(cudaMemsetAsync(d_psi.p, 0, np * sizeof(long long), stream), "memset");
-    cudaCheck(cudaMemsetAsync(d_psi_ovrf.p, 0, np * sizeof(int), stream), "memset");
-    cudaCheck(cudaMemsetAsync(d_sumdeijda.p, 0, np * sizeof(long long), stream), "memset");
-    cudaCheck(cudaMemsetAsync(d_sumdeijda_ovrf.p, 0, np * sizeof(int), stream), "memset");
+    ClearList first = list;
+    if (list.count > 4) {
+      cudaCheck(launchClear(first, sm_count, stream), "accumulator clear");
+      list.count = 0;
+    }
+    add(d_psi.p, np * sizeof(long long));
+    add(d_psi_ovrf.p, np * sizeof(int));
+    add(d_sumdeijda.p, np * sizeof(long long));
+    add(d_sumdeijda_ovrf.p, np * sizeof(int));
   }
+  cudaCheck(launchClear(list, sm_count, stream), "accumulator clear");
 }
 
 void Synthesis::setCoordinates(const double* xyz, cudaStream_t stream) {

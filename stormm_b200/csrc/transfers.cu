@@ -71,6 +71,20 @@ __global__ void kExportEnergies(const unsigned long long* __restrict__ nrg, int 
   }
 }
 
+// Zero several arrays in one launch: each block walks every array in 16-byte words
+__global__ void kClear(ClearList list) {
+  const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+  const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+  for (int a = 0; a < list.count; a++) {
+    uint4* p = reinterpret_cast<uint4*>(list.ptr[a]);
+    const size_t n = list.words[a];
+    for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += stride) {
+      p[i] = zero;
+    }
+  }
+}
+
 int gridFor(int n) {
   const int b = (n + 255) / 256;
   return b < 1 ? 1 : (b > 4096 ? 4096 : b);
@@ -100,6 +114,20 @@ cudaError_t launchExportForces(const long long* xf, const long long* yf, const l
                                int natom, double inv_scale, double* d_xyz, cudaStream_t stream) {
   kExportForces<<<gridFor(natom), 256, 0, stream>>>(xf, yf, zf, xo, yo, zo, d_map, natom,
                                                     inv_scale, d_xyz);
+  return cudaGetLastError();
+}
+
+cudaError_t launchClear(const ClearList &list, int sm_count, cudaStream_t stream) {
+  size_t most = 0;
+  for (int a = 0; a < list.count; a++) {
+    if (reinterpret_cast<uintptr_t>(list.ptr[a]) % 16 != 0) return cudaErrorInvalidValue;
+    most = (list.words[a] > most) ? list.words[a] : most;
+  }
+  if (list.count == 0 || most == 0) return cudaSuccess;
+  size_t blocks = (most + 255) / 256;
+  const size_t cap = static_cast<size_t>(sm_count > 0 ? sm_count : 148) * 8;
+  blocks = (blocks > cap) ? cap : blocks;
+  kClear<<<static_cast<int>(blocks), 256, 0, stream>>>(list);
   return cudaGetLastError();
 }
 
