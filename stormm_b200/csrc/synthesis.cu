@@ -176,6 +176,37 @@ void validateTopology(const sb_topology &tp, const sb_options &opt, int which) {
   }
 }
 
+void UploadArena::commit(DeviceArray<unsigned char>* block) {
+  auto align = [](size_t x) { return (x + 255) / 256 * 256; };
+  std::vector<size_t> up_at(up_.size()), zero_at(zero_.size());
+  size_t up_bytes = 0;
+  for (size_t k = 0; k < up_.size(); k++) {
+    up_at[k] = up_bytes;
+    up_bytes = align(up_bytes + up_[k].bytes);
+  }
+  size_t total = up_bytes;
+  for (size_t k = 0; k < zero_.size(); k++) {
+    zero_at[k] = total;
+    total = align(total + zero_[k].bytes);
+  }
+  block->allocate(total > 0 ? total : 1);
+  unsigned char* base = block->p;
+  if (up_bytes > 0) {
+    std::vector<unsigned char> host(up_bytes, 0);
+    for (size_t k = 0; k < up_.size(); k++) {
+      if (up_[k].src != nullptr) std::memcpy(host.data() + up_at[k], up_[k].src, up_[k].bytes);
+    }
+    cudaCheck(cudaMemcpy(base, host.data(), up_bytes, cudaMemcpyHostToDevice), "cudaMemcpy");
+  }
+  if (total > up_bytes) {
+    cudaCheck(cudaMemset(base + up_bytes, 0, total - up_bytes), "cudaMemset");
+  }
+  for (size_t k = 0; k < up_.size(); k++) up_[k].bind(base + up_at[k]);
+  for (size_t k = 0; k < zero_.size(); k++) zero_[k].bind(base + zero_at[k]);
+  up_.clear();
+  zero_.clear();
+}
+
 Synthesis::Synthesis(const sb_topology* tops, int ntop, const int* topology_index, int nsys_in,
                      const sb_options &options) :
     opt(options), nsys(nsys_in) {
@@ -469,7 +500,8 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
   }
 }
 
-std::unique_ptr<UnitPlan> Synthesis::makePlan(int max_slots_cap, int max_tiles_cap) const {
+std::unique_ptr<UnitPlan> Synthesis::makePlan(int max_slots_cap, int max_tiles_cap,
+                                              bool defer) const {
   if (max_slots_cap < kTile || max_slots_cap % kTile != 0 || max_slots_cap > kMaxFusedAtoms ||
       max_tiles_cap < 1) {
     throw Error(SB_ERR_ARGUMENT, "work-unit caps must be a multiple of 32 atoms in [32, 2048] "
@@ -542,14 +574,15 @@ std::unique_ptr<UnitPlan> Synthesis::makePlan(int max_slots_cap, int max_tiles_c
     throw Error(SB_ERR_ARGUMENT, "work units need " + std::to_string(smem) +
                 " bytes of shared memory, above the device limit");
   }
-  finalizePlan(plan.get());
+  finalizePlan(plan.get(), defer);
   return plan;
 }
 
 // Molecule table of every unit (what each block would otherwise rebuild serially) and the
 // device descriptors pointing into it
-void Synthesis::finalizePlan(UnitPlan* plan) const {
-  std::vector<int4> desc = plan->units;
+void Synthesis::finalizePlan(UnitPlan* plan, bool defer) const {
+  std::vector<int4> &desc = plan->desc;
+  desc = plan->units;
   plan->meta.clear();
   int tile_base = 0;   // first tile of the unit in the pair-derivative store
   for (size_t u = 0; u < plan->units.size(); u++) {
@@ -585,8 +618,10 @@ void Synthesis::finalizePlan(UnitPlan* plan) const {
   if (tile_base > fused_tiles) {
     throw Error(SB_ERR_ARGUMENT, "work units hold more tiles than the molecules");
   }
-  plan->d_units.upload(desc);
-  plan->d_meta.upload(plan->meta);
+  if (!defer) {
+    plan->d_units.upload(desc);
+    plan->d_meta.upload(plan->meta);
+  }
 }
 
 void Synthesis::buildUnits() {
@@ -635,10 +670,10 @@ void Synthesis::buildUnits() {
   // (measured on 1,024 molecules of 16-256 atoms: 213 us against 238 us for units packed up to
   // 36 tiles, which leave a sliver of a second wave)
   const int tiles_cap = (opt.max_tiles_per_unit > 0) ? opt.max_tiles_per_unit : 4;
-  eval_plan = makePlan(slots_cap, tiles_cap);
+  eval_plan = makePlan(slots_cap, tiles_cap, true);
   // minimization keeps whole molecules on chip for hundreds of cycles: smaller units balance
   // the persistent grid better (sb_autotune can choose another packing)
-  min_plan = makePlan(128, 16);
+  min_plan = makePlan(128, 16, true);
   // one unit per system, in system order, for the per-system launches
   auto slots_of = [&](int s) { return (atom_count[s] + kTile - 1) / kTile * kTile; };
   auto tiles_of = [&](int s) {
@@ -666,64 +701,106 @@ void Synthesis::buildUnits() {
 }
 
 void Synthesis::upload() {
-  d_atom_start.upload(atom_start);
-  d_atom_count.upload(atom_count);
-  d_bond_start.upload(h_bond_start);
-  d_angl_start.upload(h_angl_start);
-  d_dihe_start.upload(h_dihe_start);
-  d_lj_start.upload(h_lj_start);
-  d_lj_ntypes.upload(h_lj_ntypes);
-  d_tile_start.upload(h_tile_start);
-  d_charge.upload(h_charge);
-  d_ljidx.upload(h_ljidx);
-  d_rho.upload(h_rho);
-  d_srho.upload(h_srho);
-  d_pb.upload(h_pb);
-  d_alpha.upload(h_alpha);
-  d_beta.upload(h_beta);
-  d_gamma.upload(h_gamma);
-  d_ljab.upload(h_ljab);
-  d_ljab14.upload(h_ljab14);
-  d_bonds.upload(h_bonds);
-  d_angles.upload(h_angles);
-  d_dihe_a.upload(h_dihe_a);
-  d_dihe_b.upload(h_dihe_b);
-  d_angl64.upload(h_angl64);
-  d_dihe64.upload(h_dihe64);
-  d_dihe14_64.upload(h_dihe14_64);
-  if (fp64) {
-    d64_charge.upload(h64_charge);
-    d64_ljab14.upload(h64_ljab14);
+  // every array of the synthesis in one device block: one copy, one memset (UploadArena)
+  UploadArena arena;
+  finalizePlan(single_plan.get(), true);
+  for (UnitPlan* plan : {eval_plan.get(), min_plan.get(), single_plan.get()}) {
+    arena.put(&plan->d_units, plan->desc);
+    arena.put(&plan->d_meta, plan->meta);
   }
-  d_tile_mask_idx.upload(h_tile_mask_idx);
-  d_mask_pool.upload(h_mask_pool);
-  finalizePlan(single_plan.get());
-  d_tiled_systems.upload(h_tiled_systems);
-  d_tile_prefix.upload(h_tile_prefix);
-  d_atom_prefix.upload(h_atom_prefix);
+  arena.put(&d_atom_start, atom_start);
+  arena.put(&d_atom_count, atom_count);
+  arena.put(&d_bond_start, h_bond_start);
+  arena.put(&d_angl_start, h_angl_start);
+  arena.put(&d_dihe_start, h_dihe_start);
+  arena.put(&d_lj_start, h_lj_start);
+  arena.put(&d_lj_ntypes, h_lj_ntypes);
+  arena.put(&d_tile_start, h_tile_start);
+  arena.put(&d_charge, h_charge);
+  arena.put(&d_ljidx, h_ljidx);
+  arena.put(&d_rho, h_rho);
+  arena.put(&d_srho, h_srho);
+  arena.put(&d_pb, h_pb);
+  arena.put(&d_alpha, h_alpha);
+  arena.put(&d_beta, h_beta);
+  arena.put(&d_gamma, h_gamma);
+  arena.put(&d_ljab, h_ljab);
+  arena.put(&d_ljab14, h_ljab14);
+  arena.put(&d_bonds, h_bonds);
+  arena.put(&d_angles, h_angles);
+  arena.put(&d_dihe_a, h_dihe_a);
+  arena.put(&d_dihe_b, h_dihe_b);
+  arena.put(&d_angl64, h_angl64);
+  arena.put(&d_dihe64, h_dihe64);
+  arena.put(&d_dihe14_64, h_dihe14_64);
+  arena.put(&d_tile_mask_idx, h_tile_mask_idx);
+  arena.put(&d_mask_pool, h_mask_pool);
+  arena.put(&d_tiled_systems, h_tiled_systems);
+  arena.put(&d_tile_prefix, h_tile_prefix);
+  arena.put(&d_atom_prefix, h_atom_prefix);
+  arena.put(&d_unpadded_map, h_unpadded_map);
   if (!h_tiled_systems.empty()) {
-    d_tiled_psi.zeros(natom_padded);
-    d_tiled_de.zeros(natom_padded);
-    d_tiled_radius.zeros(natom_padded);
-    d_tiled_sde.zeros(natom_padded);
+    arena.zero(&d_tiled_psi, natom_padded);
+    arena.zero(&d_tiled_de, natom_padded);
+    arena.zero(&d_tiled_radius, natom_padded);
+    arena.zero(&d_tiled_sde, natom_padded);
   }
   if (fp64) {
-    d64_rho.upload(h64_rho);
-    d64_srho.upload(h64_srho);
-    d64_pb.upload(h64_pb);
-    d64_alpha.upload(h64_alpha);
-    d64_beta.upload(h64_beta);
-    d64_gamma.upload(h64_gamma);
-    d64_ljab.upload(h64_ljab);
-    d64_bond_atoms.upload(h64_bond_atoms);
-    d64_bond_prm.upload(h64_bond_prm);
-    d64_angl_atoms.upload(h64_angl_atoms);
-    d64_angl_prm.upload(h64_angl_prm);
-    d64_dihe_atoms.upload(h64_dihe_atoms);
-    d64_dihe_prm.upload(h64_dihe_prm);
-    d64_dihe_attn.upload(h64_dihe_attn);
-    d64_radius.zeros(natom_padded);
-    d64_sde.zeros(natom_padded);
+    arena.put(&d64_charge, h64_charge);
+    arena.put(&d64_ljab14, h64_ljab14);
+    arena.put(&d64_rho, h64_rho);
+    arena.put(&d64_srho, h64_srho);
+    arena.put(&d64_pb, h64_pb);
+    arena.put(&d64_alpha, h64_alpha);
+    arena.put(&d64_beta, h64_beta);
+    arena.put(&d64_gamma, h64_gamma);
+    arena.put(&d64_ljab, h64_ljab);
+    arena.put(&d64_bond_atoms, h64_bond_atoms);
+    arena.put(&d64_bond_prm, h64_bond_prm);
+    arena.put(&d64_angl_atoms, h64_angl_atoms);
+    arena.put(&d64_angl_prm, h64_angl_prm);
+    arena.put(&d64_dihe_atoms, h64_dihe_atoms);
+    arena.put(&d64_dihe_prm, h64_dihe_prm);
+    arena.put(&d64_dihe_attn, h64_dihe_attn);
+    arena.zero(&d64_radius, natom_padded);
+    arena.zero(&d64_sde, natom_padded);
+    if (neck) {
+      arena.put(&d64_neck_sep, h64_neck_sep);
+      arena.put(&d64_neck_val, h64_neck_val);
+    }
+  }
+  if (neck) {
+    arena.put(&d_neck_idx, h_neck_idx);
+    arena.put(&d_neck_sep, h_neck_sep);
+    arena.put(&d_neck_val, h_neck_val);
+  }
+  const size_t np = natom_padded;
+  arena.zero(&d_stage_xyz, static_cast<size_t>(3) * natom_total);
+  arena.zero(&d_stage_nrg, static_cast<size_t>(nsys) * kNrgStride);
+  arena.zero(&d_xcrd, np);
+  arena.zero(&d_ycrd, np);
+  arena.zero(&d_zcrd, np);
+  arena.zero(&d_xcrd_ovrf, np);
+  arena.zero(&d_ycrd_ovrf, np);
+  arena.zero(&d_zcrd_ovrf, np);
+  arena.zero(&d_xfrc, np);
+  arena.zero(&d_yfrc, np);
+  arena.zero(&d_zfrc, np);
+  arena.zero(&d_xfrc_ovrf, np);
+  arena.zero(&d_yfrc_ovrf, np);
+  arena.zero(&d_zfrc_ovrf, np);
+  arena.zero(&d_energies, static_cast<size_t>(nsys) * kNrgStride);
+  arena.zero(&d_psi, np);
+  arena.zero(&d_psi_ovrf, np);
+  arena.zero(&d_sumdeijda, np);
+  arena.zero(&d_sumdeijda_ovrf, np);
+  arena.zero(&d_born_radii, np);
+  arena.zero(&d_status, 1);
+  // one tile beyond the last unit's, so no store or load of a tile walk can leave the buffer
+  arena.zero(&d_pair_deriv, static_cast<size_t>(fused_tiles + 1) * kPairDerivPerTile);
+  arena.commit(&d_arena);
+
+  if (fp64) {
     dev64.charge = d64_charge.p;
     dev64.rho = d64_rho.p;
     dev64.srho = d64_srho.p;
@@ -746,8 +823,6 @@ void Synthesis::upload() {
     dev64.sde = d64_sde.p;
     dev64.gb_offset = gb_offset;
     if (neck) {
-      d64_neck_sep.upload(h64_neck_sep);
-      d64_neck_val.upload(h64_neck_val);
       dev64.neck_sep = d64_neck_sep.p;
       dev64.neck_val = d64_neck_val.p;
       dev64.neck_scale = (opt.igb == SB_GB_NECK2) ? 0.826836 : 0.361825;
@@ -763,36 +838,6 @@ void Synthesis::upload() {
   dev_tiled.de_acc = d_tiled_de.p;
   dev_tiled.radius = d_tiled_radius.p;
   dev_tiled.sde = d_tiled_sde.p;
-  d_unpadded_map.upload(h_unpadded_map);
-  d_stage_xyz.zeros(static_cast<size_t>(3) * natom_total);
-  d_stage_nrg.zeros(static_cast<size_t>(nsys) * kNrgStride);
-  const size_t np = natom_padded;
-  d_xcrd.zeros(np);
-  d_ycrd.zeros(np);
-  d_zcrd.zeros(np);
-  d_xcrd_ovrf.zeros(np);
-  d_ycrd_ovrf.zeros(np);
-  d_zcrd_ovrf.zeros(np);
-  d_xfrc.zeros(np);
-  d_yfrc.zeros(np);
-  d_zfrc.zeros(np);
-  d_xfrc_ovrf.zeros(np);
-  d_yfrc_ovrf.zeros(np);
-  d_zfrc_ovrf.zeros(np);
-  d_energies.zeros(static_cast<size_t>(nsys) * kNrgStride);
-  d_psi.zeros(np);
-  d_psi_ovrf.zeros(np);
-  d_sumdeijda.zeros(np);
-  d_sumdeijda_ovrf.zeros(np);
-  d_born_radii.zeros(np);
-  d_status.zeros(1);
-  // one tile beyond the last unit's, so no store or load of a tile walk can leave the buffer
-  d_pair_deriv.zeros(static_cast<size_t>(fused_tiles + 1) * kPairDerivPerTile);
-  if (neck) {
-    d_neck_idx.upload(h_neck_idx);
-    d_neck_sep.upload(h_neck_sep);
-    d_neck_val.upload(h_neck_val);
-  }
 
   DevSynthesis &d = dev;
   std::memset(&d, 0, sizeof(DevSynthesis));
@@ -1182,23 +1227,26 @@ void Synthesis::minimizeBegin(const sb_minimize_controls &ctl, cudaStream_t stre
   rejectTiledMinimization(ctl.kernel);
   const size_t np = natom_padded;
   if (d_mcycle.p == nullptr) {
-    d_xprv.allocate(np);
-    d_yprv.allocate(np);
-    d_zprv.allocate(np);
-    d_xcg.allocate(np);
-    d_ycg.allocate(np);
-    d_zcg.allocate(np);
-    d_lmove.allocate(nsys);
-    d_rmsf.allocate(nsys);
-    d_mcycle.allocate(nsys);
-    d_mdone.allocate(nsys);
-    d_line.allocate(static_cast<size_t>(nsys) * kLineFields);
-    d_queue.allocate(2);
+    // the minimizer's arrays in one block (every kernel that reads them writes them first)
+    UploadArena arena;
+    arena.zero(&d_xprv, np);
+    arena.zero(&d_yprv, np);
+    arena.zero(&d_zprv, np);
+    arena.zero(&d_xcg, np);
+    arena.zero(&d_ycg, np);
+    arena.zero(&d_zcg, np);
+    arena.zero(&d_lmove, nsys);
+    arena.zero(&d_rmsf, nsys);
+    arena.zero(&d_mcycle, nsys);
+    arena.zero(&d_mdone, nsys);
+    arena.zero(&d_line, static_cast<size_t>(nsys) * kLineFields);
+    arena.zero(&d_queue, 2);
     if (fp64) {
-      d_xcg64.allocate(np);
-      d_ycg64.allocate(np);
-      d_zcg64.allocate(np);
+      arena.zero(&d_xcg64, np);
+      arena.zero(&d_ycg64, np);
+      arena.zero(&d_zcg64, np);
     }
+    arena.commit(&d_min_arena);
   }
   history_stride = 0;
   if (ctl.record_history) {

@@ -11,6 +11,7 @@
 
 #include <cuda_runtime.h>
 
+#include <functional>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -51,20 +52,28 @@ template <typename T> struct DeviceArray {
   T* p = nullptr;
   size_t n = 0;
   cudaStream_t s = nullptr;      // stream of a stream-ordered allocation
+  bool owned = true;             // false: a view into another array's memory (UploadArena)
   DeviceArray() = default;
   DeviceArray(const DeviceArray &) = delete;
   DeviceArray& operator=(const DeviceArray &) = delete;
   ~DeviceArray() { release(); }
   void release() {
-    if (p != nullptr) {
+    if (p != nullptr && owned) {
       if (s != nullptr) {
         cudaFreeAsync(p, s);
       }
       else {
         cudaFree(p);
       }
-      p = nullptr;
     }
+    p = nullptr;
+    owned = true;
+  }
+  void view(T* ptr, size_t count) {
+    release();
+    p = ptr;
+    n = count;
+    owned = false;
   }
   void allocate(size_t count) {
     release();
@@ -91,6 +100,35 @@ template <typename T> struct DeviceArray {
                 "cudaMemcpy");
     }
   }
+};
+
+// Many device arrays built at once: one allocation holds them all (256-byte aligned), the
+// arrays with host contents arrive in one copy and the zeroed ones are cleared by one memset,
+// instead of an allocation, a synchronization and a copy or memset per array.  The arrays
+// become views into `block`, which owns the memory.
+class UploadArena {
+public:
+  template <typename T> void put(DeviceArray<T>* a, const std::vector<T> &v) {
+    add(&up_, v.empty() ? nullptr : v.data(), sizeof(T) * v.size(), sizeof(T),
+        [a, n = v.size()](unsigned char* at) { a->view(reinterpret_cast<T*>(at), n); });
+  }
+  template <typename T> void zero(DeviceArray<T>* a, size_t count) {
+    add(&zero_, nullptr, sizeof(T) * count, sizeof(T),
+        [a, count](unsigned char* at) { a->view(reinterpret_cast<T*>(at), count); });
+  }
+  void commit(DeviceArray<unsigned char>* block);
+private:
+  struct Item {
+    const void* src;
+    size_t bytes;
+    std::function<void(unsigned char*)> bind;
+  };
+  static void add(std::vector<Item>* list, const void* src, size_t bytes, size_t unit,
+                  std::function<void(unsigned char*)> bind) {
+    // an empty array still gets one element, as DeviceArray::allocate gives it
+    list->push_back({src, bytes > 0 ? bytes : unit, std::move(bind)});
+  }
+  std::vector<Item> up_, zero_;
 };
 
 // Host checks of a topology before anything is built from it (the constructor of Synthesis and
@@ -124,7 +162,8 @@ struct UnitPlan {
   int big_slots = 0, big_lj = 0;
   int small_slots = 0, small_lj = 0;
   std::vector<int> meta;         // kUnitMetaFields ints per molecule row, plus a closing row
-  DeviceArray<int4> d_units;     // as units, but x = first row of the unit in meta
+  std::vector<int4> desc;        // as units, but x = first row of the unit in meta
+  DeviceArray<int4> d_units;     // desc on the device
   DeviceArray<int> d_meta;
 };
 
@@ -215,6 +254,8 @@ public:
   std::vector<int> h_unpadded_map;   // padded index of each unpadded atom
 
   // device arrays
+  DeviceArray<unsigned char> d_arena;    // owns the memory of the arrays upload() builds
+  DeviceArray<unsigned char> d_min_arena;  // and of the minimizer's arrays
   DeviceArray<int> d_atom_start, d_atom_count, d_bond_start, d_angl_start, d_dihe_start;
   DeviceArray<int> d_lj_start, d_lj_ntypes, d_tile_start, d_ljidx, d_tile_mask_idx;
   DeviceArray<float> d_charge, d_rho, d_srho, d_pb, d_alpha, d_beta, d_gamma;
@@ -286,8 +327,10 @@ public:
 
 private:
   void buildLayout(const sb_topology* tops, int ntop);
-  std::unique_ptr<UnitPlan> makePlan(int max_slots_cap, int max_tiles_cap) const;
-  void finalizePlan(UnitPlan* plan) const;
+  // defer: leave the device copy of the plan to the caller (the constructor's UploadArena)
+  std::unique_ptr<UnitPlan> makePlan(int max_slots_cap, int max_tiles_cap,
+                                     bool defer = false) const;
+  void finalizePlan(UnitPlan* plan, bool defer = false) const;
   int launchThreads(int units, int terms) const;
   void launchPlan(const UnitPlan &plan, int terms, bool force, bool energy, cudaStream_t stream,
                   const Clash &clash = Clash());
