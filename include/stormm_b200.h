@@ -121,6 +121,24 @@ typedef struct {
   const double* dihe_scee;     /* 1-4 electrostatic attenuation, 0 when the term carries no 1-4 */
   const double* dihe_scnb;     /* 1-4 Lennard-Jones attenuation */
   const int* dihe_improper;    /* nonzero: energy is reported as improper (NULL: all proper) */
+  /* CHARMM terms (all zero / NULL for Amber force fields), evaluated in FP64 by a kernel of
+   * their own after the fused pass (Potential/valence_potential.tpp:659-1300) */
+  int nubrd;                   /* Urey-Bradley 1-3 harmonic stretches */
+  const int* ubrd_atoms;       /* 2 * nubrd (atoms i, k) */
+  const double* ubrd_keq;      /* kcal/mol A^2 */
+  const double* ubrd_leq;      /* A */
+  int ncimp;                   /* CHARMM harmonic impropers: k (theta - phase)^2 */
+  const int* cimp_atoms;       /* 4 * ncimp */
+  const double* cimp_keq;      /* kcal/mol rad^2 */
+  const double* cimp_phase;    /* rad */
+  int ncmap;                   /* CMAP terms: a bicubic spline surface over two dihedrals */
+  const int* cmap_atoms;       /* 5 * ncmap: phi is atoms 0-3, psi atoms 1-4 */
+  const int* cmap_surface;     /* ncmap surface indices */
+  int ncmap_surf;
+  const int* cmap_dims;        /* grid points per side of each surface */
+  const double* cmap_values;   /* surfaces back to back, kcal/mol: the value at phi index j and
+                                  psi index k is at j + k * dim, grid point j at -180 + j * 360 /
+                                  dim degrees */
 } sb_topology;
 
 typedef struct {

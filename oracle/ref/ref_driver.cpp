@@ -280,6 +280,43 @@ void putTopology(RecordWriter *rw, const AtomGraph &ag) {
   rw->i("dihe_kind", dkind);
   rw->iscalar("ninfr14", vk.ninfr14);
 
+  // CHARMM terms, expanded per term; CMAP surfaces as STORMM holds them (column-major: the
+  // value at phi index j and psi index k is at j + k * dim within the surface)
+  std::vector<int> ua(2 * vk.nubrd), ca(4 * vk.ncimp), ma(5 * vk.ncmap), ms(vk.ncmap);
+  std::vector<double> uk(vk.nubrd), ul(vk.nubrd), ck(vk.ncimp), cp(vk.ncimp);
+  for (int t = 0; t < vk.nubrd; t++) {
+    ua[2 * t] = vk.ubrd_i_atoms[t];
+    ua[2 * t + 1] = vk.ubrd_k_atoms[t];
+    uk[t] = vk.ubrd_keq[vk.ubrd_param_idx[t]];
+    ul[t] = vk.ubrd_leq[vk.ubrd_param_idx[t]];
+  }
+  for (int t = 0; t < vk.ncimp; t++) {
+    ca[4 * t] = vk.cimp_i_atoms[t];
+    ca[4 * t + 1] = vk.cimp_j_atoms[t];
+    ca[4 * t + 2] = vk.cimp_k_atoms[t];
+    ca[4 * t + 3] = vk.cimp_l_atoms[t];
+    ck[t] = vk.cimp_keq[vk.cimp_param_idx[t]];
+    cp[t] = vk.cimp_phi[vk.cimp_param_idx[t]];
+  }
+  for (int t = 0; t < vk.ncmap; t++) {
+    ma[5 * t] = vk.cmap_i_atoms[t];
+    ma[5 * t + 1] = vk.cmap_j_atoms[t];
+    ma[5 * t + 2] = vk.cmap_k_atoms[t];
+    ma[5 * t + 3] = vk.cmap_l_atoms[t];
+    ma[5 * t + 4] = vk.cmap_m_atoms[t];
+    ms[t] = vk.cmap_surf_idx[t];
+  }
+  rw->i("ubrd_atoms", ua);
+  rw->d("ubrd_keq", uk);
+  rw->d("ubrd_leq", ul);
+  rw->i("cimp_atoms", ca);
+  rw->d("cimp_keq", ck);
+  rw->d("cimp_phase", cp);
+  rw->i("cmap_atoms", ma);
+  rw->i("cmap_surface", ms);
+  rw->i("cmap_dims", vk.cmap_dim, vk.ncmap_surf);
+  rw->d("cmap_values", vk.cmap_surf, vk.ncmap_surf > 0 ? vk.cmap_surf_bounds[vk.ncmap_surf] : 0);
+
   // Implicit solvent parameters
   rw->iscalar("igb", static_cast<int>(isk.igb));
   rw->scalar("dielectric", isk.dielectric);
@@ -397,6 +434,28 @@ int runEval(const std::string &prmtop, const std::string &inpcrd, const std::str
   rw.d("energy_terms", esum);
   putScoreCard(&rw, "energy_terms_fixed", sc);
 
+  // CHARMM terms: FP64 energy of each kind (Urey-Bradley, CHARMM improper, CMAP), the
+  // ScoreCard's fixed-point sums of the same, and the forces of each kind
+  {
+    std::vector<double> ce, cf;
+    ScoreCard sc_ch(1, 1, 32);
+    zeroForces(psw);
+    ce.push_back(evaluateUreyBradleyTerms(vk, psw, &sc_ch, EvaluateForce::YES, 0));
+    putForces(&rw, "frc_ubrd", psw);
+    zeroForces(psw);
+    ce.push_back(evaluateCharmmImproperTerms(vk, psw, &sc_ch, EvaluateForce::YES, 0));
+    putForces(&rw, "frc_cimp", psw);
+    zeroForces(psw);
+    ce.push_back(evaluateCmapTerms(vk, psw, &sc_ch, EvaluateForce::YES, 0));
+    putForces(&rw, "frc_cmap", psw);
+    rw.d("charmm_terms", ce);
+    for (StateVariable sv : {StateVariable::UREY_BRADLEY, StateVariable::CHARMM_IMPROPER,
+                             StateVariable::CMAP}) {
+      cf.push_back(sc_ch.reportInstantaneousStates(sv, 0));
+    }
+    rw.d("charmm_terms_fixed", cf);
+  }
+
   // The complete evaluation through the MM driver STORMM uses for single points
   zeroForces(psw);
   ScoreCard sc_all(1, 1, 26);
@@ -404,6 +463,14 @@ int runEval(const std::string &prmtop, const std::string &inpcrd, const std::str
   evalRestrainedMMGB(&ps, &sc_all, ag, ngb_tab, se, ra, EvaluateForce::YES, 0);
   putForces(&rw, "frc_total", psw);
   putScoreCard(&rw, "energy_terms_mm", sc_all);
+  {
+    std::vector<double> cm;
+    for (StateVariable sv : {StateVariable::UREY_BRADLEY, StateVariable::CHARMM_IMPROPER,
+                             StateVariable::CMAP}) {
+      cm.push_back(sc_all.reportInstantaneousStates(sv, 0));
+    }
+    rw.d("charmm_terms_mm", cm);
+  }
   if (opt.clash_r0 >= 0.0 || opt.clash_ratio >= 0.0) {
     const double r0 = (opt.clash_r0 >= 0.0) ? opt.clash_r0 : 0.0;
     const double ratio = (opt.clash_ratio >= 0.0) ? opt.clash_ratio : 0.0;

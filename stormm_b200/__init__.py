@@ -27,8 +27,9 @@ INIT_FORCES, INIT_ENERGIES, INIT_GB_WORKSPACE = 1, 2, 4
 SB_REQUEST_MINIMIZE, SB_REQUEST_EVALUATE = 0, 1
 NRG_STRIDE = 16
 # StateVariable slots (STORMM Potential/energy_enumerators.h:36-50)
-NRG_SLOTS = {"bond": 0, "angle": 1, "proper_dihedral": 2, "improper_dihedral": 3, "vdw": 7,
-             "vdw_14": 8, "elec": 9, "elec_14": 10, "gb": 11}
+NRG_SLOTS = {"bond": 0, "angle": 1, "proper_dihedral": 2, "improper_dihedral": 3,
+             "urey_bradley": 4, "charmm_improper": 5, "cmap": 6, "vdw": 7, "vdw_14": 8,
+             "elec": 9, "elec_14": 10, "gb": 11}
 # order of the oracle's / reference driver's nine energy terms
 TERM_ORDER = ["bond", "angle", "proper_dihedral", "improper_dihedral", "vdw", "vdw_14", "elec",
               "elec_14", "gb"]
@@ -46,6 +47,10 @@ class Topology(ctypes.Structure):
         ("angl_keq", _P), ("angl_theta0", _P), ("ndihe", ctypes.c_int), ("dihe_atoms", _P),
         ("dihe_amp", _P), ("dihe_freq", _P), ("dihe_phase", _P), ("dihe_scee", _P),
         ("dihe_scnb", _P), ("dihe_improper", _P),
+        ("nubrd", ctypes.c_int), ("ubrd_atoms", _P), ("ubrd_keq", _P), ("ubrd_leq", _P),
+        ("ncimp", ctypes.c_int), ("cimp_atoms", _P), ("cimp_keq", _P), ("cimp_phase", _P),
+        ("ncmap", ctypes.c_int), ("cmap_atoms", _P), ("cmap_surface", _P),
+        ("ncmap_surf", ctypes.c_int), ("cmap_dims", _P), ("cmap_values", _P),
     ]
 
 
@@ -356,6 +361,27 @@ class _TopologyArrays:
         t.dihe_scnb = ptr(scnb, np.float64)
         impr = getattr(mol, "dihe_improper", None)
         t.dihe_improper = ptr(impr, np.int32) if impr is not None else None
+        # CHARMM terms, when the molecule carries them
+        ub = getattr(mol, "ubrd_atoms", None)
+        if ub is not None and len(ub) > 0:
+            t.nubrd = len(np.asarray(ub).reshape(-1, 2))
+            t.ubrd_atoms = ptr(ub, np.int32)
+            t.ubrd_keq = ptr(mol.ubrd_keq, np.float64)
+            t.ubrd_leq = ptr(mol.ubrd_leq, np.float64)
+        ci = getattr(mol, "cimp_atoms", None)
+        if ci is not None and len(ci) > 0:
+            t.ncimp = len(np.asarray(ci).reshape(-1, 4))
+            t.cimp_atoms = ptr(ci, np.int32)
+            t.cimp_keq = ptr(mol.cimp_keq, np.float64)
+            t.cimp_phase = ptr(mol.cimp_phase, np.float64)
+        cm = getattr(mol, "cmap_atoms", None)
+        if cm is not None and len(cm) > 0:
+            t.ncmap = len(np.asarray(cm).reshape(-1, 5))
+            t.cmap_atoms = ptr(cm, np.int32)
+            t.cmap_surface = ptr(mol.cmap_surface, np.int32)
+            t.ncmap_surf = len(mol.cmap_dims)
+            t.cmap_dims = ptr(mol.cmap_dims, np.int32)
+            t.cmap_values = ptr(mol.cmap_values, np.float64)
         self.struct = t
 
 
@@ -591,6 +617,19 @@ def read_amber(prmtop, inpcrd=None, igb=None, radius_set=0):
         mol.cmap_count = v.cmap_count
         mol.urey_bradley_count = v.urey_bradley_count
         mol.charmm_improper_count = v.charmm_improper_count
+        if t.nubrd > 0:
+            mol.ubrd_atoms = i(t.ubrd_atoms, 2 * t.nubrd).reshape(-1, 2)
+            mol.ubrd_keq = d(t.ubrd_keq, t.nubrd)
+            mol.ubrd_leq = d(t.ubrd_leq, t.nubrd)
+        if t.ncimp > 0:
+            mol.cimp_atoms = i(t.cimp_atoms, 4 * t.ncimp).reshape(-1, 4)
+            mol.cimp_keq = d(t.cimp_keq, t.ncimp)
+            mol.cimp_phase = d(t.cimp_phase, t.ncimp)
+        if t.ncmap > 0:
+            mol.cmap_atoms = i(t.cmap_atoms, 5 * t.ncmap).reshape(-1, 5)
+            mol.cmap_surface = i(t.cmap_surface, t.ncmap)
+            mol.cmap_dims = i(t.cmap_dims, t.ncmap_surf)
+            mol.cmap_values = d(t.cmap_values, int((mol.cmap_dims.astype(np.int64) ** 2).sum()))
         mol.unit_cell = v.unit_cell
     finally:
         lib.sb_amber_topology_destroy(h)

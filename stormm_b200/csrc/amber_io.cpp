@@ -24,8 +24,8 @@
 // mapExclusions (Topology/atomgraph_refinement.cpp:2735-2935) derives them; the file's
 // EXCLUDED_ATOMS_LIST is not used.  A topology's unit cell (IFBOX > 0) is reported, not
 // applied: this path evaluates in isolated boundary conditions.  Massless particles (virtual
-// sites) are refused.  CHARMM terms (Urey-Bradley, CHARMM impropers, CMAP) are counted and
-// reported but not evaluated by this library.
+// sites) are refused.  CHARMM terms (Urey-Bradley, CHARMM impropers, CMAP with its surfaces)
+// are read into the topology and evaluated by the CHARMM-term kernel.
 //
 // sb_amber_set_implicit_solvent assigns the per-atom GB parameters the way STORMM's
 // AtomGraph::setImplicitSolventModel does (Topology/atomgraph_setters.cpp:672-1060): first an
@@ -68,6 +68,9 @@ struct sb_amber_topology {
   std::string radius_set, title;
   int igb = -1;                                  // model applied by sb_amber_set_implicit_solvent
   int cmap_count = 0, urey_bradley_count = 0, charmm_improper_count = 0;
+  // CHARMM terms, 0-based atoms, parameters expanded per term; CMAP surfaces column-major
+  std::vector<int> ubrd_atoms, cimp_atoms, cmap_atoms, cmap_surface, cmap_dims;
+  std::vector<double> ubrd_keq, ubrd_leq, cimp_keq, cimp_phase, cmap_values;
   int ifbox = 0;
 };
 
@@ -515,13 +518,94 @@ sb_amber_topology* readTopology(const std::string &path) {
     t->pb_radii.resize(n, 0.0);
     t->gb_screen.resize(n, 0.0);
 
-    // CHARMM terms this library does not evaluate
+    // CHARMM terms (Topology/atomgraph_detailers.cpp:897-990, 1196-1240): 1-based atoms, each
+    // term's last entry its 1-based parameter set; CMAP surfaces are stored phi-major and kept
+    // here column-major (phi index fastest), as the evaluation indexes them
+    auto atom0 = [&](int v) {
+      if (v < 1 || v > n) throw Error(SB_ERR_ARGUMENT, path + ": CHARMM term atom out of range");
+      return v - 1;
+    };
     const std::vector<int> ub = numbers<int>(secs, "CHARMM_UREY_BRADLEY_COUNT", false, path);
-    const std::vector<int> ci = numbers<int>(secs, "CHARMM_NUM_IMPROPERS", false, path);
-    const std::vector<int> cm = numbers<int>(secs, "CMAP_COUNT", false, path);
     t->urey_bradley_count = ub.empty() ? 0 : ub[0];
+    if (t->urey_bradley_count > 0) {
+      const std::vector<int> a = numbers<int>(secs, "CHARMM_UREY_BRADLEY", true, path);
+      const std::vector<double> k = numbers<double>(secs, "CHARMM_UREY_BRADLEY_FORCE_CONSTANT",
+                                                    true, path);
+      const std::vector<double> r = numbers<double>(secs, "CHARMM_UREY_BRADLEY_EQUIL_VALUE",
+                                                    true, path);
+      if (a.size() < 3 * static_cast<size_t>(t->urey_bradley_count)) {
+        throw Error(SB_ERR_ARGUMENT, path + ": short CHARMM_UREY_BRADLEY section");
+      }
+      for (int q = 0; q < t->urey_bradley_count; q++) {
+        const int p = a[3 * q + 2] - 1;
+        if (p < 0 || p >= static_cast<int>(std::min(k.size(), r.size()))) {
+          throw Error(SB_ERR_ARGUMENT, path + ": Urey-Bradley parameter index out of range");
+        }
+        t->ubrd_atoms.push_back(atom0(a[3 * q]));
+        t->ubrd_atoms.push_back(atom0(a[3 * q + 1]));
+        t->ubrd_keq.push_back(k[p]);
+        t->ubrd_leq.push_back(r[p]);
+      }
+    }
+    const std::vector<int> ci = numbers<int>(secs, "CHARMM_NUM_IMPROPERS", false, path);
     t->charmm_improper_count = ci.empty() ? 0 : ci[0];
-    t->cmap_count = cm.empty() ? 0 : cm[0];
+    if (t->charmm_improper_count > 0) {
+      const std::vector<int> a = numbers<int>(secs, "CHARMM_IMPROPERS", true, path);
+      const std::vector<double> k = numbers<double>(secs, "CHARMM_IMPROPER_FORCE_CONSTANT", true,
+                                                    path);
+      const std::vector<double> ph = numbers<double>(secs, "CHARMM_IMPROPER_PHASE", true, path);
+      if (a.size() < 5 * static_cast<size_t>(t->charmm_improper_count)) {
+        throw Error(SB_ERR_ARGUMENT, path + ": short CHARMM_IMPROPERS section");
+      }
+      for (int q = 0; q < t->charmm_improper_count; q++) {
+        const int p = a[5 * q + 4] - 1;
+        if (p < 0 || p >= static_cast<int>(std::min(k.size(), ph.size()))) {
+          throw Error(SB_ERR_ARGUMENT, path + ": CHARMM improper parameter index out of range");
+        }
+        for (int m = 0; m < 4; m++) t->cimp_atoms.push_back(atom0(a[5 * q + m]));
+        t->cimp_keq.push_back(k[p]);
+        t->cimp_phase.push_back(ph[p]);
+      }
+    }
+    for (const std::string prefix : {"CHARMM_CMAP_", "CMAP_"}) {
+      const std::vector<int> cm = numbers<int>(secs, prefix + "COUNT", false, path);
+      if (cm.empty()) continue;
+      t->cmap_count = cm[0];
+      const int nsurf = (cm.size() > 1) ? cm[1] : 0;
+      if (t->cmap_count <= 0) break;
+      t->cmap_dims = numbers<int>(secs, prefix + "RESOLUTION", true, path);
+      if (nsurf <= 0 || static_cast<int>(t->cmap_dims.size()) < nsurf) {
+        throw Error(SB_ERR_ARGUMENT, path + ": CMAP surfaces without resolutions");
+      }
+      t->cmap_dims.resize(nsurf);
+      for (int sfc = 0; sfc < nsurf; sfc++) {
+        const int dim = t->cmap_dims[sfc];
+        const std::string flag = prefix + "PARAMETER_" + (sfc + 1 < 10 ? "0" : "") +
+                                 std::to_string(sfc + 1);
+        const std::vector<double> grid = numbers<double>(secs, flag, true, path);
+        if (dim < 1 || grid.size() < static_cast<size_t>(dim) * dim) {
+          throw Error(SB_ERR_ARGUMENT, path + ": short " + flag + " section");
+        }
+        for (int k = 0; k < dim; k++) {
+          for (int j = 0; j < dim; j++) {
+            t->cmap_values.push_back(grid[static_cast<size_t>(j) * dim + k]);
+          }
+        }
+      }
+      const std::vector<int> a = numbers<int>(secs, prefix + "INDEX", true, path);
+      if (a.size() < 6 * static_cast<size_t>(t->cmap_count)) {
+        throw Error(SB_ERR_ARGUMENT, path + ": short " + prefix + "INDEX section");
+      }
+      for (int q = 0; q < t->cmap_count; q++) {
+        for (int m = 0; m < 5; m++) t->cmap_atoms.push_back(atom0(a[6 * q + m]));
+        const int sfc = a[6 * q + 5] - 1;
+        if (sfc < 0 || sfc >= nsurf) {
+          throw Error(SB_ERR_ARGUMENT, path + ": CMAP surface index out of range");
+        }
+        t->cmap_surface.push_back(sfc);
+      }
+      break;
+    }
 
     bondGraphExclusions(t);
     return t;
@@ -759,6 +843,20 @@ void fillView(const sb_amber_topology* t, sb_amber_view* v) {
   s.dihe_scee = t->dihe_scee.data();
   s.dihe_scnb = t->dihe_scnb.data();
   s.dihe_improper = t->dihe_improper.data();
+  s.nubrd = static_cast<int>(t->ubrd_keq.size());
+  s.ubrd_atoms = t->ubrd_atoms.empty() ? nullptr : t->ubrd_atoms.data();
+  s.ubrd_keq = t->ubrd_keq.empty() ? nullptr : t->ubrd_keq.data();
+  s.ubrd_leq = t->ubrd_leq.empty() ? nullptr : t->ubrd_leq.data();
+  s.ncimp = static_cast<int>(t->cimp_keq.size());
+  s.cimp_atoms = t->cimp_atoms.empty() ? nullptr : t->cimp_atoms.data();
+  s.cimp_keq = t->cimp_keq.empty() ? nullptr : t->cimp_keq.data();
+  s.cimp_phase = t->cimp_phase.empty() ? nullptr : t->cimp_phase.data();
+  s.ncmap = static_cast<int>(t->cmap_surface.size());
+  s.cmap_atoms = t->cmap_atoms.empty() ? nullptr : t->cmap_atoms.data();
+  s.cmap_surface = t->cmap_surface.empty() ? nullptr : t->cmap_surface.data();
+  s.ncmap_surf = (s.ncmap > 0) ? static_cast<int>(t->cmap_dims.size()) : 0;
+  s.cmap_dims = (s.ncmap > 0) ? t->cmap_dims.data() : nullptr;
+  s.cmap_values = (s.ncmap > 0) ? t->cmap_values.data() : nullptr;
   v->atomic_numbers = t->z_numbers.data();
   v->masses = t->mass.data();
   for (int lv = 0; lv < 3; lv++) {

@@ -230,6 +230,28 @@ enum LineField : int {
   kLineInvNorm, kLineAct, kLineFields
 };
 
+// CHARMM terms of a synthesis (charmm.cu), atom indices in the padded layout, each term with
+// its system; terms are stored system by system
+struct DevCharmm {
+  const int4* ubrd = nullptr;          // x i, y k, z system
+  const double2* ubrd_prm = nullptr;   // keq, leq
+  const int4* cimp = nullptr;          // atoms i, j, k, l
+  const int* cimp_sys = nullptr;
+  const double2* cimp_prm = nullptr;   // keq, phase
+  const int4* cmap = nullptr;          // atoms 0-3
+  const int4* cmap_b = nullptr;        // x atom 4, y system, z surface
+  const int2* cmap_surf = nullptr;     // per surface: first patch (16 doubles each), grid points
+  const double* cmap_patch = nullptr;  // 16 bicubic coefficients per grid cell
+  const long long* xcrd = nullptr;
+  const long long* ycrd = nullptr;
+  const long long* zcrd = nullptr;
+  long long* xfrc = nullptr;
+  long long* yfrc = nullptr;
+  long long* zfrc = nullptr;
+  unsigned long long* energies = nullptr;
+  double inv_gpos_scale = 0.0, frc_scale = 0.0, nrg_scale = 0.0;
+};
+
 // Arrays zeroed by one launch of launchClear: 16-byte aligned bases, lengths in 16-byte words
 struct ClearList {
   void* ptr[8];

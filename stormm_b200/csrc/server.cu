@@ -70,6 +70,9 @@ struct Request {
   std::vector<double> dihe_phase, dihe_scee, dihe_scnb, xyz;
   std::vector<int> lj_idx, excl_bounds, excl_list, bond_atoms, angl_atoms, dihe_atoms;
   std::vector<int> dihe_improper;
+  int nubrd = 0, ncimp = 0, ncmap = 0, ncmap_surf = 0;
+  std::vector<int> ubrd_atoms, cimp_atoms, cmap_atoms, cmap_surface, cmap_dims;
+  std::vector<double> ubrd_keq, ubrd_leq, cimp_keq, cimp_phase, cmap_values;
   double bytes = 0.0;
   double t_submit = 0.0;
   double t_admit = 0.0;
@@ -113,6 +116,24 @@ struct Request {
     copyArray(&dihe_scee, t.dihe_scee, ndihe);
     copyArray(&dihe_scnb, t.dihe_scnb, ndihe);
     copyArray(&dihe_improper, t.dihe_improper, ndihe);
+    nubrd = t.nubrd;
+    ncimp = t.ncimp;
+    ncmap = t.ncmap;
+    ncmap_surf = (t.ncmap > 0) ? t.ncmap_surf : 0;
+    copyArray(&ubrd_atoms, t.ubrd_atoms, 2 * static_cast<size_t>(nubrd));
+    copyArray(&ubrd_keq, t.ubrd_keq, nubrd);
+    copyArray(&ubrd_leq, t.ubrd_leq, nubrd);
+    copyArray(&cimp_atoms, t.cimp_atoms, 4 * static_cast<size_t>(ncimp));
+    copyArray(&cimp_keq, t.cimp_keq, ncimp);
+    copyArray(&cimp_phase, t.cimp_phase, ncimp);
+    copyArray(&cmap_atoms, t.cmap_atoms, 5 * static_cast<size_t>(ncmap));
+    copyArray(&cmap_surface, t.cmap_surface, ncmap);
+    copyArray(&cmap_dims, t.cmap_dims, ncmap_surf);
+    size_t nvalues = 0;
+    for (int s = 0; s < ncmap_surf; s++) {
+      nvalues += static_cast<size_t>(t.cmap_dims[s]) * t.cmap_dims[s];
+    }
+    copyArray(&cmap_values, t.cmap_values, nvalues);
     copyArray(&xyz, coords, 3 * n);
     // device memory the molecule holds while in flight: per-atom arrays (coordinates, forces,
     // parameters, GB workspace, minimizer state) on the padded atom count, valence records,
@@ -157,6 +178,20 @@ struct Request {
     t.dihe_scee = ptrOrNull(dihe_scee);
     t.dihe_scnb = ptrOrNull(dihe_scnb);
     t.dihe_improper = ptrOrNull(dihe_improper);
+    t.nubrd = nubrd;
+    t.ubrd_atoms = ptrOrNull(ubrd_atoms);
+    t.ubrd_keq = ptrOrNull(ubrd_keq);
+    t.ubrd_leq = ptrOrNull(ubrd_leq);
+    t.ncimp = ncimp;
+    t.cimp_atoms = ptrOrNull(cimp_atoms);
+    t.cimp_keq = ptrOrNull(cimp_keq);
+    t.cimp_phase = ptrOrNull(cimp_phase);
+    t.ncmap = ncmap;
+    t.cmap_atoms = ptrOrNull(cmap_atoms);
+    t.cmap_surface = ptrOrNull(cmap_surface);
+    t.ncmap_surf = ncmap_surf;
+    t.cmap_dims = ptrOrNull(cmap_dims);
+    t.cmap_values = ptrOrNull(cmap_values);
     return t;
   }
 };
@@ -233,6 +268,11 @@ public:
         opt_.controls.kernel != SB_MIN_GRAPH) {
       throw Error(SB_ERR_UNSUPPORTED, "molecules above " + std::to_string(on_chip) +
                   " atoms are evaluated tile by tile and cannot be minimized by the persistent "
+                  "kernel; a server whose controls select SB_MIN_GRAPH minimizes them");
+    }
+    if (kind == SB_REQUEST_MINIMIZE && (top->nubrd > 0 || top->ncimp > 0 || top->ncmap > 0) &&
+        opt_.controls.kernel != SB_MIN_GRAPH) {
+      throw Error(SB_ERR_UNSUPPORTED, "CHARMM terms cannot be minimized by the persistent "
                   "kernel; a server whose controls select SB_MIN_GRAPH minimizes them");
     }
     Request req(*top, xyz);

@@ -54,6 +54,9 @@ cudaError_t launchExportForces(const long long* xf, const long long* yf, const l
 cudaError_t launchExportEnergies(const unsigned long long* nrg, int n, double inv_scale,
                                  double* d_out, cudaStream_t stream);
 cudaError_t launchClear(const ClearList &list, int sm_count, cudaStream_t stream);
+cudaError_t launchCharmmTerms(const DevCharmm &c, int ub0, int nub, int ci0, int nci, int cm0,
+                              int ncm, bool force, bool energy, int sm_count,
+                              cudaStream_t stream);
 
 namespace {
 thread_local std::string g_last_error;
@@ -174,6 +177,199 @@ void validateTopology(const sb_topology &tp, const sb_options &opt, int which) {
       throw Error(SB_ERR_UNSUPPORTED, name + ": dihedral atom index above 32767");
     }
   }
+  // CHARMM terms
+  if (tp.nubrd < 0 || tp.ncimp < 0 || tp.ncmap < 0 || tp.ncmap_surf < 0 ||
+      (tp.nubrd > 0 && (tp.ubrd_atoms == nullptr || tp.ubrd_keq == nullptr ||
+                        tp.ubrd_leq == nullptr)) ||
+      (tp.ncimp > 0 && (tp.cimp_atoms == nullptr || tp.cimp_keq == nullptr ||
+                        tp.cimp_phase == nullptr)) ||
+      (tp.ncmap > 0 && (tp.cmap_atoms == nullptr || tp.cmap_surface == nullptr ||
+                        tp.ncmap_surf <= 0 || tp.cmap_dims == nullptr ||
+                        tp.cmap_values == nullptr))) {
+    throw Error(SB_ERR_ARGUMENT, name + " has negative CHARMM term counts or lacks their arrays");
+  }
+  if (!in_range(tp.ubrd_atoms, 2 * static_cast<size_t>(tp.nubrd)) ||
+      !in_range(tp.cimp_atoms, 4 * static_cast<size_t>(tp.ncimp)) ||
+      !in_range(tp.cmap_atoms, 5 * static_cast<size_t>(tp.ncmap))) {
+    throw Error(SB_ERR_ARGUMENT, name + ": CHARMM term atom index out of range");
+  }
+  if (tp.ncmap > 0) {
+    for (int s = 0; s < tp.ncmap_surf; s++) {
+      if (tp.cmap_dims[s] < 4 || tp.cmap_dims[s] > 360) {
+        throw Error(SB_ERR_ARGUMENT, name + ": CMAP surface grids must have 4 to 360 points");
+      }
+    }
+    for (int t = 0; t < tp.ncmap; t++) {
+      if (tp.cmap_surface[t] < 0 || tp.cmap_surface[t] >= tp.ncmap_surf) {
+        throw Error(SB_ERR_ARGUMENT, name + ": CMAP surface index out of range");
+      }
+    }
+  }
+}
+
+namespace {
+
+// First derivatives, per grid spacing, of the periodic cubic spline through n equally spaced
+// values, as a stencil: the derivative at point i is sum_m w[m] y[(i + m) mod n].  The spline's
+// knot slopes solve m[i-1] + 4 m[i] + m[i+1] = 3 (y[i+1] - y[i-1]) (continuous first and second
+// derivatives, periodic), so w[m] = 3 (g[m-1] - g[m+1]) with g the first row of the inverse of
+// that circulant matrix, found here by Gaussian elimination with partial pivoting.
+std::vector<double> splineSlopeStencil(int n) {
+  std::vector<double> a(static_cast<size_t>(n) * n, 0.0), g(n, 0.0);
+  for (int i = 0; i < n; i++) {
+    a[static_cast<size_t>(i) * n + i] = 4.0;
+    a[static_cast<size_t>(i) * n + (i + 1) % n] += 1.0;
+    a[static_cast<size_t>(i) * n + (i + n - 1) % n] += 1.0;
+  }
+  g[0] = 1.0;
+  for (int c = 0; c < n; c++) {
+    int piv = c;
+    for (int r = c + 1; r < n; r++) {
+      if (std::fabs(a[static_cast<size_t>(r) * n + c]) > std::fabs(a[static_cast<size_t>(piv) * n + c])) piv = r;
+    }
+    if (piv != c) {
+      for (int k = 0; k < n; k++) std::swap(a[static_cast<size_t>(c) * n + k], a[static_cast<size_t>(piv) * n + k]);
+      std::swap(g[c], g[piv]);
+    }
+    for (int r = c + 1; r < n; r++) {
+      const double f = a[static_cast<size_t>(r) * n + c] / a[static_cast<size_t>(c) * n + c];
+      if (f == 0.0) continue;
+      for (int k = c; k < n; k++) a[static_cast<size_t>(r) * n + k] -= f * a[static_cast<size_t>(c) * n + k];
+      g[r] -= f * g[c];
+    }
+  }
+  for (int r = n - 1; r >= 0; r--) {
+    double v = g[r];
+    for (int k = r + 1; k < n; k++) v -= a[static_cast<size_t>(r) * n + k] * g[k];
+    g[r] = v / a[static_cast<size_t>(r) * n + r];
+  }
+  std::vector<double> w(n);
+  for (int m = 0; m < n; m++) {
+    w[m] = 3.0 * (g[(m + n - 1) % n] - g[(m + 1) % n]);
+  }
+  return w;
+}
+
+// The bicubic coefficients of every grid cell of one CMAP surface (value at phi index j, psi
+// index k at j + k * n), appended to `out` cell by cell in the order j + k * n: for the cell at
+// (j, k), with F the 4 x 4 matrix of values, phi slopes, psi slopes and cross slopes at its
+// corners (rows: value and phi slope at j and j + 1; columns: value and psi slope at k and
+// k + 1), the coefficients a[r + 4 s] of u^r v^s are M F M^T, M the cubic Hermite basis
+// matrix; slopes per grid spacing from the periodic spline (Topology/atomgraph_refinement.cpp:
+// 3307-3600 builds the same patches)
+void cmapPatches(int n, const double* val, std::vector<double>* out) {
+  const std::vector<double> w = splineSlopeStencil(n);
+  auto at = [n](int j, int k) { return ((j % n) + n) % n + (((k % n) + n) % n) * n; };
+  std::vector<double> dphi(static_cast<size_t>(n) * n), dpsi(dphi.size()), dcross(dphi.size());
+  for (int k = 0; k < n; k++) {
+    for (int j = 0; j < n; j++) {
+      double sp = 0.0, ss = 0.0, sc = 0.0;
+      for (int m = 0; m < n; m++) {
+        sp += w[m] * val[at(j + m, k)];
+        ss += w[m] * val[at(j, k + m)];
+        for (int q = 0; q < n; q++) {
+          sc += w[m] * w[q] * val[at(j + m, k + q)];
+        }
+      }
+      dphi[at(j, k)] = sp;
+      dpsi[at(j, k)] = ss;
+      dcross[at(j, k)] = sc;
+    }
+  }
+  static const double kM[4][4] = {{1.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 1.0, 0.0},
+                                  {-3.0, 3.0, -2.0, -1.0}, {2.0, -2.0, 1.0, 1.0}};
+  for (int k = 0; k < n; k++) {
+    for (int j = 0; j < n; j++) {
+      const int c00 = at(j, k), c10 = at(j + 1, k), c01 = at(j, k + 1), c11 = at(j + 1, k + 1);
+      const double f[4][4] = {{val[c00], val[c01], dpsi[c00], dpsi[c01]},
+                              {val[c10], val[c11], dpsi[c10], dpsi[c11]},
+                              {dphi[c00], dphi[c01], dcross[c00], dcross[c01]},
+                              {dphi[c10], dphi[c11], dcross[c10], dcross[c11]}};
+      double mf[4][4];
+      for (int r = 0; r < 4; r++) {
+        for (int c = 0; c < 4; c++) {
+          double v = 0.0;
+          for (int q = 0; q < 4; q++) v += kM[r][q] * f[q][c];
+          mf[r][c] = v;
+        }
+      }
+      double cell[16];
+      for (int r = 0; r < 4; r++) {
+        for (int s = 0; s < 4; s++) {
+          double v = 0.0;
+          for (int q = 0; q < 4; q++) v += mf[r][q] * kM[s][q];
+          cell[r + 4 * s] = v;
+        }
+      }
+      out->insert(out->end(), cell, cell + 16);
+    }
+  }
+}
+
+}  // namespace
+
+// CHARMM term records in the padded layout, system by system, and the CMAP surfaces of each
+// topology once
+void Synthesis::buildCharmm(const sb_topology* tops, int ntop) {
+  h_ubrd.clear();
+  h_ubrd_prm.clear();
+  h_cimp.clear();
+  h_cimp_sys.clear();
+  h_cimp_prm.clear();
+  h_cmap.clear();
+  h_cmap_b.clear();
+  h_cmap_surf.clear();
+  h_cmap_patch.clear();
+  h_ubrd_start.assign(nsys + 1, 0);
+  h_cimp_start.assign(nsys + 1, 0);
+  h_cmap_start.assign(nsys + 1, 0);
+  std::vector<int> surf_base(ntop, -1);
+  for (int s = 0; s < nsys; s++) {
+    const int t = topo[s];
+    const sb_topology &tp = tops[t];
+    const int base = atom_start[s];
+    for (int k = 0; k < tp.nubrd; k++) {
+      h_ubrd.push_back(make_int4(base + tp.ubrd_atoms[2 * k], base + tp.ubrd_atoms[2 * k + 1], s, 0));
+      h_ubrd_prm.push_back(make_double2(tp.ubrd_keq[k], tp.ubrd_leq[k]));
+    }
+    for (int k = 0; k < tp.ncimp; k++) {
+      const int* a = tp.cimp_atoms + 4 * k;
+      h_cimp.push_back(make_int4(base + a[0], base + a[1], base + a[2], base + a[3]));
+      h_cimp_sys.push_back(s);
+      h_cimp_prm.push_back(make_double2(tp.cimp_keq[k], tp.cimp_phase[k]));
+    }
+    if (tp.ncmap > 0 && surf_base[t] < 0) {
+      surf_base[t] = static_cast<int>(h_cmap_surf.size());
+      size_t vo = 0;
+      for (int q = 0; q < tp.ncmap_surf; q++) {
+        const int dim = tp.cmap_dims[q];
+        h_cmap_surf.push_back(make_int2(static_cast<int>(h_cmap_patch.size() / 16), dim));
+        cmapPatches(dim, tp.cmap_values + vo, &h_cmap_patch);
+        vo += static_cast<size_t>(dim) * dim;
+      }
+    }
+    for (int k = 0; k < tp.ncmap; k++) {
+      const int* a = tp.cmap_atoms + 5 * k;
+      h_cmap.push_back(make_int4(base + a[0], base + a[1], base + a[2], base + a[3]));
+      h_cmap_b.push_back(make_int4(base + a[4], s, surf_base[t] + tp.cmap_surface[k], 0));
+    }
+    h_ubrd_start[s + 1] = static_cast<int>(h_ubrd.size());
+    h_cimp_start[s + 1] = static_cast<int>(h_cimp.size());
+    h_cmap_start[s + 1] = static_cast<int>(h_cmap.size());
+  }
+  has_charmm = !(h_ubrd.empty() && h_cimp.empty() && h_cmap.empty());
+}
+
+// The CHARMM terms of systems [first, last)
+void Synthesis::launchCharmm(int first, int last, bool force, bool energy,
+                             cudaStream_t stream) {
+  if (!has_charmm) return;
+  DevCharmm c = dev_charmm;
+  cudaCheck(launchCharmmTerms(c, h_ubrd_start[first], h_ubrd_start[last] - h_ubrd_start[first],
+                              h_cimp_start[first], h_cimp_start[last] - h_cimp_start[first],
+                              h_cmap_start[first], h_cmap_start[last] - h_cmap_start[first],
+                              force, energy, sm_count, stream),
+            "CHARMM term launch");
 }
 
 void UploadArena::commit(DeviceArray<unsigned char>* block) {
@@ -191,16 +387,22 @@ void UploadArena::commit(DeviceArray<unsigned char>* block) {
   }
   block->allocate(total > 0 ? total : 1);
   unsigned char* base = block->p;
+  // the copy and the memset go on the block's allocation stream (the legacy default stream when
+  // there is none) and are waited for here: the arrays are used next on other streams,
+  // non-blocking ones among them, which do not order themselves after the default stream
+  const cudaStream_t s = block->s;
+  std::vector<unsigned char> host(up_bytes, 0);
   if (up_bytes > 0) {
-    std::vector<unsigned char> host(up_bytes, 0);
     for (size_t k = 0; k < up_.size(); k++) {
       if (up_[k].src != nullptr) std::memcpy(host.data() + up_at[k], up_[k].src, up_[k].bytes);
     }
-    cudaCheck(cudaMemcpy(base, host.data(), up_bytes, cudaMemcpyHostToDevice), "cudaMemcpy");
+    cudaCheck(cudaMemcpyAsync(base, host.data(), up_bytes, cudaMemcpyHostToDevice, s),
+              "cudaMemcpyAsync");
   }
   if (total > up_bytes) {
-    cudaCheck(cudaMemset(base + up_bytes, 0, total - up_bytes), "cudaMemset");
+    cudaCheck(cudaMemsetAsync(base + up_bytes, 0, total - up_bytes, s), "cudaMemsetAsync");
   }
+  cudaCheck(cudaStreamSynchronize(s), "cudaStreamSynchronize");
   for (size_t k = 0; k < up_.size(); k++) up_[k].bind(base + up_at[k]);
   for (size_t k = 0; k < zero_.size(); k++) zero_[k].bind(base + zero_at[k]);
   up_.clear();
@@ -260,6 +462,7 @@ Synthesis::Synthesis(const sb_topology* tops, int ntop, const int* topology_inde
     validateTopology(tops[t], opt, t);
   }
   buildLayout(tops, ntop);
+  buildCharmm(tops, ntop);
   buildUnits();
   upload();
   // the caller's tables were copied; keep no pointer to them
@@ -739,6 +942,17 @@ void Synthesis::upload() {
   arena.put(&d_tile_prefix, h_tile_prefix);
   arena.put(&d_atom_prefix, h_atom_prefix);
   arena.put(&d_unpadded_map, h_unpadded_map);
+  if (has_charmm) {
+    arena.put(&d_ubrd, h_ubrd);
+    arena.put(&d_ubrd_prm, h_ubrd_prm);
+    arena.put(&d_cimp, h_cimp);
+    arena.put(&d_cimp_sys, h_cimp_sys);
+    arena.put(&d_cimp_prm, h_cimp_prm);
+    arena.put(&d_cmap, h_cmap);
+    arena.put(&d_cmap_b, h_cmap_b);
+    arena.put(&d_cmap_surf, h_cmap_surf);
+    arena.put(&d_cmap_patch, h_cmap_patch);
+  }
   if (!h_tiled_systems.empty()) {
     arena.zero(&d_tiled_psi, natom_padded);
     arena.zero(&d_tiled_de, natom_padded);
@@ -828,6 +1042,28 @@ void Synthesis::upload() {
       dev64.neck_scale = (opt.igb == SB_GB_NECK2) ? 0.826836 : 0.361825;
       dev64.neck_cut = opt.neck_cut;
     }
+  }
+  dev_charmm = DevCharmm();
+  if (has_charmm) {
+    dev_charmm.ubrd = d_ubrd.p;
+    dev_charmm.ubrd_prm = d_ubrd_prm.p;
+    dev_charmm.cimp = d_cimp.p;
+    dev_charmm.cimp_sys = d_cimp_sys.p;
+    dev_charmm.cimp_prm = d_cimp_prm.p;
+    dev_charmm.cmap = d_cmap.p;
+    dev_charmm.cmap_b = d_cmap_b.p;
+    dev_charmm.cmap_surf = d_cmap_surf.p;
+    dev_charmm.cmap_patch = d_cmap_patch.p;
+    dev_charmm.xcrd = d_xcrd.p;
+    dev_charmm.ycrd = d_ycrd.p;
+    dev_charmm.zcrd = d_zcrd.p;
+    dev_charmm.xfrc = d_xfrc.p;
+    dev_charmm.yfrc = d_yfrc.p;
+    dev_charmm.zfrc = d_zfrc.p;
+    dev_charmm.energies = d_energies.p;
+    dev_charmm.inv_gpos_scale = std::ldexp(1.0, -opt.gpos_bits);
+    dev_charmm.frc_scale = std::ldexp(1.0, opt.frc_bits);
+    dev_charmm.nrg_scale = std::ldexp(1.0, opt.nrg_bits);
   }
   dev_tiled.nmol = static_cast<int>(h_tiled_systems.size());
   dev_tiled.ntiles = h_tile_prefix.back();
@@ -955,6 +1191,9 @@ void Synthesis::evaluate(int terms, bool force, bool energy, cudaStream_t stream
   launchPlan(*eval_plan, terms, force, energy, stream, clash);
   launchTiledRange(0, static_cast<int>(h_tiled_systems.size()), terms, force, energy, stream,
                    clash);
+  if (terms & SB_TERM_VALENCE) {
+    launchCharmm(0, nsys, force, energy, stream);
+  }
 }
 
 void Synthesis::launchTiledRange(int mol_begin, int mol_end, int terms, bool force, bool energy,
@@ -1003,6 +1242,11 @@ void Synthesis::rejectTiledMinimization(int kernel) const {
     throw Error(SB_ERR_UNSUPPORTED, "the FP64 mode minimizes with the graph minimizer "
                 "(SB_MIN_GRAPH) only");
   }
+  if (has_charmm && kernel != SB_MIN_GRAPH) {
+    throw Error(SB_ERR_UNSUPPORTED, "CHARMM terms are evaluated by a kernel of their own and "
+                "cannot be minimized on chip by the persistent kernel; the graph minimizer "
+                "(SB_MIN_GRAPH) minimizes them");
+  }
   if (!h_tiled_systems.empty() && kernel != SB_MIN_GRAPH) {
     throw Error(SB_ERR_UNSUPPORTED, "molecules above " + std::to_string(tiled_threshold) +
                 " atoms are evaluated tile by tile and cannot be minimized on chip by the "
@@ -1030,11 +1274,15 @@ void Synthesis::evaluateRange(int first, int count, int terms, bool force, bool 
   for (int s = first; s < first + count; s++) {
     if (tiled_index[s] >= 0) {
       launchTiledRange(tiled_index[s], tiled_index[s] + 1, terms, force, energy, stream, clash);
-      continue;
     }
-    cudaCheck(launchEvalFused(d, s, s + 1, single_lj, terms, force, energy, 1, threads, stream,
-                              clash.on()),
-              "per-system evaluation launch");
+    else {
+      cudaCheck(launchEvalFused(d, s, s + 1, single_lj, terms, force, energy, 1, threads, stream,
+                                clash.on()),
+                "per-system evaluation launch");
+    }
+    if (terms & SB_TERM_VALENCE) {
+      launchCharmm(s, s + 1, force, energy, stream);
+    }
   }
 }
 
@@ -1316,6 +1564,7 @@ void Synthesis::evaluateFor(int first, int count, bool single, bool force, cudaS
     launchPlan(*eval_plan, SB_TERM_ALL, force, true, stream, clash);
     launchTiledRange(0, static_cast<int>(h_tiled_systems.size()), SB_TERM_ALL, force, true,
                      stream, clash);
+    launchCharmm(0, nsys, force, true, stream);
     return;
   }
   DevSynthesis d = dev;
@@ -1328,10 +1577,12 @@ void Synthesis::evaluateFor(int first, int count, bool single, bool force, cudaS
     if (tiled_index[s] >= 0) {
       launchTiledRange(tiled_index[s], tiled_index[s] + 1, SB_TERM_ALL, force, true, stream,
                        clash);
-      continue;
     }
-    cudaCheck(launchEvalFused(d, s, s + 1, single_lj, SB_TERM_ALL, force, true, 1, threads,
-                              stream, clash.on()), "per-system evaluation launch");
+    else {
+      cudaCheck(launchEvalFused(d, s, s + 1, single_lj, SB_TERM_ALL, force, true, 1, threads,
+                                stream, clash.on()), "per-system evaluation launch");
+    }
+    launchCharmm(s, s + 1, force, true, stream);
   }
 }
 

@@ -91,7 +91,9 @@ template <typename T> struct DeviceArray {
   }
   void zeros(size_t count) {
     allocate(count);
-    cudaCheck(cudaMemset(p, 0, sizeof(T) * (count > 0 ? count : 1)), "cudaMemset");
+    // ordered on the allocation stream and waited for, as the next user may be another stream
+    cudaCheck(cudaMemsetAsync(p, 0, sizeof(T) * (count > 0 ? count : 1), s), "cudaMemsetAsync");
+    cudaCheck(cudaStreamSynchronize(s), "cudaStreamSynchronize");
   }
   void upload(const std::vector<T> &v) {
     allocate(v.size());
@@ -256,6 +258,19 @@ public:
   // device arrays
   DeviceArray<unsigned char> d_arena;    // owns the memory of the arrays upload() builds
   DeviceArray<unsigned char> d_min_arena;  // and of the minimizer's arrays
+  // CHARMM terms (charmm.cu): records in the padded layout, per-system ranges on the host
+  bool has_charmm = false;
+  std::vector<int4> h_ubrd, h_cimp, h_cmap, h_cmap_b;
+  std::vector<double2> h_ubrd_prm, h_cimp_prm;
+  std::vector<int> h_cimp_sys, h_ubrd_start, h_cimp_start, h_cmap_start;
+  std::vector<int2> h_cmap_surf;
+  std::vector<double> h_cmap_patch;
+  DeviceArray<int4> d_ubrd, d_cimp, d_cmap, d_cmap_b;
+  DeviceArray<double2> d_ubrd_prm, d_cimp_prm;
+  DeviceArray<int> d_cimp_sys;
+  DeviceArray<int2> d_cmap_surf;
+  DeviceArray<double> d_cmap_patch;
+  DevCharmm dev_charmm;
   DeviceArray<int> d_atom_start, d_atom_count, d_bond_start, d_angl_start, d_dihe_start;
   DeviceArray<int> d_lj_start, d_lj_ntypes, d_tile_start, d_ljidx, d_tile_mask_idx;
   DeviceArray<float> d_charge, d_rho, d_srho, d_pb, d_alpha, d_beta, d_gamma;
@@ -327,6 +342,8 @@ public:
 
 private:
   void buildLayout(const sb_topology* tops, int ntop);
+  void buildCharmm(const sb_topology* tops, int ntop);
+  void launchCharmm(int first, int last, bool force, bool energy, cudaStream_t stream);
   // defer: leave the device copy of the plan to the caller (the constructor's UploadArena)
   std::unique_ptr<UnitPlan> makePlan(int max_slots_cap, int max_tiles_cap,
                                      bool defer = false) const;

@@ -72,7 +72,15 @@ def molecule_from_fixture(g):
     for i in range(n):
         e12[i] |= e11[i]
     scee = np.asarray(g["dihe_scee"], dtype=np.float64)
-    return SimpleNamespace(
+    charmm = {}
+    if "ubrd_atoms" in g:
+        # CHARMM terms (empty for Amber force fields)
+        charmm = dict(ubrd_atoms=g["ubrd_atoms"].reshape(-1, 2), ubrd_keq=g["ubrd_keq"],
+                      ubrd_leq=g["ubrd_leq"], cimp_atoms=g["cimp_atoms"].reshape(-1, 4),
+                      cimp_keq=g["cimp_keq"], cimp_phase=g["cimp_phase"],
+                      cmap_atoms=g["cmap_atoms"].reshape(-1, 5), cmap_surface=g["cmap_surface"],
+                      cmap_dims=g["cmap_dims"], cmap_values=g["cmap_values"])
+    return SimpleNamespace(**charmm,
         natom=n, coords=g["coords"].reshape(n, 3), charge=g["charge"], lj_idx=g["lj_idx"],
         n_lj_types=nt, lja=g["lja"].reshape(nt, nt), ljb=g["ljb"].reshape(nt, nt),
         lja14=g["lja14"].reshape(nt, nt), ljb14=g["ljb14"].reshape(nt, nt),

@@ -29,6 +29,9 @@ Fixtures written (numpy .npz, one per case):
   molecules; each case names its molecules by generator, seed and size, the systems per
   topology and the InitializationTask.  Small cases hold the arrays, large ones their SHA-256
   digests and sizes.
+* ``charmm_ala_dipeptide.npz`` and ``charmm_dhfr.npz`` (``--charmm-only``):
+  systems with CHARMM terms (one CMAP term; 2,117 Urey-Bradley terms, 418 CHARMM impropers and
+  157 CMAP terms), with STORMM's energies and forces of each CHARMM term kind.
 * ``synthetic_K64.npz`` and ``minimize_clash_k64.npz`` (``--clash-only``): a 64-atom molecule
   with close contacts (0.45 A start noise), its clash-mitigated evaluation (softened cores below
   1.5 A and below 0.9 of the pair's sigma) beside the plain one, and a minimization whose first
@@ -111,12 +114,17 @@ def main():
                     help="write only the neck GB (igb 7, 8) fixtures")
     ap.add_argument("--nbwu-only", action="store_true",
                     help="write only the nonbonded work-unit fixtures")
+    ap.add_argument("--charmm-only", action="store_true",
+                    help="write only the CHARMM-term fixtures")
     args = ap.parse_args()
     if not os.path.exists(DRIVER):
         raise SystemExit("build the reference driver first: make -C oracle/ref -j8")
     with tempfile.TemporaryDirectory() as tmp:
         if args.nbwu_only:
             nbwu_cases(tmp)
+            return
+        if args.charmm_only:
+            charmm_systems(args.reference_root, tmp)
             return
         if args.neck_only:
             for name, seed, n, igb in (("N7", 8820, 80, "7"), ("N8", 8821, 80, "8")):
@@ -192,6 +200,24 @@ def reference_systems(ref_root, tmp, models):
             rec["known_answer_gb"] = np.array([answers[key][ans_idx]])
             np.savez_compressed(os.path.join(HERE, f"reference_{sname}_igb{igb}.npz"), **rec)
             print("wrote", sname, igb, rec["energy_terms"][-1], answers[key][ans_idx])
+
+
+def charmm_systems(ref_root, tmp):
+    """Systems with CHARMM terms: alanine dipeptide (one CMAP term) and dihydrofolate
+    reductase (Urey-Bradley, CHARMM impropers and CMAP), OBC-II GB."""
+    tdir = os.path.join(ref_root, "test")
+    systems = {"ala_dipeptide": (("Topology", "ala_dipeptide.top"),
+                                 ("Trajectory", "ala_dipeptide.inpcrd"),
+                                 ["--scee", "1.2", "--scnb", "2.0"]),
+               "dhfr": (("Topology", "dhfr_cmap.top"), ("Trajectory", "dhfr_cmap.inpcrd"), [])}
+    for sname, (tf, cf, extra) in systems.items():
+        out = os.path.join(tmp, f"{sname}.bin")
+        run_driver(["eval", os.path.join(tdir, *tf), os.path.join(tdir, *cf), out, "--igb", "5",
+                    "--diel", "78.5", "--qtol", "1e-10",
+                    "--qdisc", "9.31322574615478515625E-10"] + extra)
+        rec = read_records(out)
+        np.savez_compressed(os.path.join(HERE, f"charmm_{sname}.npz"), **rec)
+        print("wrote", sname, rec["natom"], rec["charmm_terms"], rec["charmm_terms_mm"])
 
 
 # (name, [(generator, seed, natom, systems)], InitializationTask, store arrays in full)

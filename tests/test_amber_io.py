@@ -138,6 +138,24 @@ def test_reader_reports_charmm_terms_and_radius_set():
     assert np.all(m.coords == 0.0)
 
 
+@pytest.mark.skipif(not os.path.isdir(REFERENCE_TEST), reason="reference test files absent")
+@pytest.mark.parametrize("top,fixture", [("ala_dipeptide.top", "charmm_ala_dipeptide.npz"),
+                                         ("dhfr_cmap.top", "charmm_dhfr.npz")])
+def test_reader_reads_charmm_terms_as_stormm(top, fixture):
+    """Urey-Bradley, CHARMM improper and CMAP terms read from the file equal STORMM's parse
+    (atoms exactly; parameters and CMAP surface values, column-major, to the last bit of the
+    decimal conversion)."""
+    m = sb.read_amber(os.path.join(REFERENCE_TEST, "Topology", top))
+    g = load(fixture)
+    empty = np.zeros(0)
+    for key in ("ubrd_atoms", "cimp_atoms", "cmap_atoms", "cmap_surface", "cmap_dims"):
+        np.testing.assert_array_equal(np.asarray(getattr(m, key, empty)).reshape(-1),
+                                      g[key].reshape(-1), err_msg=key)
+    for key in ("ubrd_keq", "ubrd_leq", "cimp_keq", "cimp_phase", "cmap_values"):
+        np.testing.assert_allclose(np.asarray(getattr(m, key, empty)), g[key], rtol=1e-15,
+                                   atol=0.0, err_msg=key)
+
+
 @pytest.mark.parametrize("natom,chain", [(2, False), (24, False), (64, True), (200, False)])
 def test_round_trip_through_writer(tmp_path, natom, chain):
     src = (make_chain if chain else make_molecule)(seed=1000 + natom, natom=natom)

