@@ -471,6 +471,34 @@ int sb_nonbonded_work_units(const sb_topology* tops, int ntop, const int* topolo
                             long long* n_instructions);
 
 /* ------------------------------------------------------------------------------------------ */
+/* Restraints                                                                                  */
+/* ------------------------------------------------------------------------------------------ */
+/* STORMM's flat-bottom restraints (Restraints/bounded_restraint.h, evaluated as
+ * Potential/valence_potential.tpp:1558-2050 and Restraints/restraint_util.tpp:9-46), constant
+ * (a restraint whose initial and final steps coincide): for the restrained value d (distance
+ * from the target point, distance between two atoms, angle, or dihedral angle in radians), the
+ * energy is k2 (d - r2)^2 between r1 and r2, zero between r2 and r3, k3 (d - r3)^2 between r3 and
+ * r4, and continues linearly below r1 and above r4.  A dihedral is taken within pi of
+ * (r2 + r3) / 2.  Energies go to slot SB_RESTRAINT. */
+#define SB_RESTRAINT_POSITION 1
+#define SB_RESTRAINT_DISTANCE 2
+#define SB_RESTRAINT_ANGLE 3
+#define SB_RESTRAINT_DIHEDRAL 4
+
+typedef struct {
+  int system;                  /* system of the synthesis */
+  int kind;                    /* SB_RESTRAINT_*: the restraint involves that many atoms */
+  int atoms[4];                /* atom indices within the system (unused ones ignored) */
+  double k2, k3;               /* stiffness of the lower and upper walls (kcal/mol per unit^2) */
+  double r1, r2, r3, r4;       /* bounds, ascending (A, or radians for angles and dihedrals) */
+  double target[3];            /* positional restraints: the reference point (A) */
+} sb_restraint;
+
+/* Replace the synthesis's restraints (count 0 removes them); evaluated with the valence terms
+ * and by the graph minimizer (the persistent minimizer refuses restrained syntheses). */
+int sb_set_restraints(sb_synthesis* syn, const sb_restraint* restraints, int count);
+
+/* ------------------------------------------------------------------------------------------ */
 /* STORMM's valence work units                                                                 */
 /* ------------------------------------------------------------------------------------------ */
 /* The valence terms and constraint groups of one topology in STORMM's own order and indexing:

@@ -39,6 +39,12 @@
 //       calculateValenceWorkUnitSize over each line of atom counts (one synthesis per line):
 //       the atom limit and kernel width it picks for that many SMs (sm-count 0: the overload
 //       without an SM count).
+//   restraint <prmtop> <inpcrd> <restraint-file> <out.bin>
+//       STORMM's restraint evaluation (evaluateRestraints, Potential/valence_potential.tpp:
+//       1558-2050) for constant restraints listed one a line: "kind i j k l k2 k3 r1 r2 r3 r4 x
+//       y z" (kind 1 positional, 2 distance, 3 angle, 4 dihedral; 0-based atoms, unused ones
+//       -1; the target x y z used by positional restraints); writes each restraint's energy,
+//       the total and the forces.
 //   nbwu <list-file> <out.bin> [--init-task N]
 //       STORMM's nonbonded work units (Synthesis/nonbonded_workunit.cpp) for a synthesis: each
 //       line of <list-file> is "<prmtop> <system count>", the systems laid out topology by
@@ -71,6 +77,7 @@
 #include "Potential/scorecard.h"
 #include "Potential/static_exclusionmask.h"
 #include "Potential/valence_potential.h"
+#include "Restraints/bounded_restraint.h"
 #include "Restraints/restraint_apparatus.h"
 #include "Structure/clash_detection.h"
 #include "Structure/rmsd.h"
@@ -743,6 +750,55 @@ int runNbwu(const std::string &list_file, const std::string &out, const Options 
   return 0;
 }
 
+// Constant restraints of several kinds on one structure, evaluated by STORMM's CPU code
+int runRestraint(const std::string &prmtop, const std::string &inpcrd, const std::string &list,
+                 const std::string &out, const Options &opt) {
+  AtomGraph ag = loadTopology(prmtop, opt);
+  PhaseSpace ps(inpcrd, CoordinateFileKind::AMBER_INPCRD);
+  if (opt.quantize) {
+    quantizeCoordinates(&ps);
+  }
+  std::ifstream in(list);
+  std::vector<BoundedRestraint> rs;
+  int kind, a[4];
+  double k2, k3, r1, r2, r3, r4, x, y, z;
+  while (in >> kind >> a[0] >> a[1] >> a[2] >> a[3] >> k2 >> k3 >> r1 >> r2 >> r3 >> r4 >> x >>
+         y >> z) {
+    switch (kind) {
+    case 1:
+      rs.emplace_back(a[0], &ag, k2, k3, r1, r2, r3, r4, double3{x, y, z});
+      break;
+    case 2:
+      rs.emplace_back(a[0], a[1], &ag, k2, k3, r1, r2, r3, r4);
+      break;
+    case 3:
+      rs.emplace_back(a[0], a[1], a[2], &ag, k2, k3, r1, r2, r3, r4);
+      break;
+    default:
+      rs.emplace_back(a[0], a[1], a[2], a[3], &ag, k2, k3, r1, r2, r3, r4);
+      break;
+    }
+  }
+  RecordWriter rw(out);
+  PhaseSpaceWriter psw = ps.data();
+  std::vector<double> each;
+  for (const BoundedRestraint &r : rs) {
+    const RestraintApparatus one(std::vector<BoundedRestraint>(1, r), &ag);
+    ScoreCard sc1(1, 1, 32);
+    each.push_back(evaluateRestraints(one, &ps, &sc1, EvaluateForce::NO, 0, 0));
+  }
+  const RestraintApparatus ra(rs, &ag);
+  ScoreCard sc(1, 1, 32);
+  zeroForces(psw);
+  const double total = evaluateRestraints(ra, &ps, &sc, EvaluateForce::YES, 0, 0);
+  putCoordinates(&rw, "coords", psw);
+  putForces(&rw, "frc_restraint", psw);
+  rw.d("restraint_energies", each);
+  rw.scalar("restraint_total", total);
+  std::printf("restraints %zu, energy %.10f\n", rs.size(), total);
+  return 0;
+}
+
 // Valence work units of one topology, with the inputs they are built from
 int runVwu(const std::string &prmtop, const std::string &out, const Options &opt, int atoms) {
   const AtomGraph ag = loadTopology(prmtop, opt);
@@ -1009,6 +1065,9 @@ int main(int argc, char* argv[]) {
   }
   if (mode == "geometry" && pos.size() == 3) {
     return runGeometry(pos[0], pos[1], pos[2], opt);
+  }
+  if (mode == "restraint" && pos.size() == 4) {
+    return runRestraint(pos[0], pos[1], pos[2], pos[3], opt);
   }
   if (mode == "vwu" && pos.size() == 2) {
     return runVwu(pos[0], pos[1], opt, vwu_atoms);

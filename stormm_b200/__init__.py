@@ -29,7 +29,7 @@ NRG_STRIDE = 16
 # StateVariable slots (STORMM Potential/energy_enumerators.h:36-50)
 NRG_SLOTS = {"bond": 0, "angle": 1, "proper_dihedral": 2, "improper_dihedral": 3,
              "urey_bradley": 4, "charmm_improper": 5, "cmap": 6, "vdw": 7, "vdw_14": 8,
-             "elec": 9, "elec_14": 10, "gb": 11}
+             "elec": 9, "elec_14": 10, "gb": 11, "restraint": 12}
 # order of the oracle's / reference driver's nine energy terms
 TERM_ORDER = ["bond", "angle", "proper_dihedral", "improper_dihedral", "vdw", "vdw_14", "elec",
               "elec_14", "gb"]
@@ -102,6 +102,18 @@ class ValenceUnitView(ctypes.Structure):
         ("cbnd_insr", _P), ("angl_insr", _P), ("cdhe_insr", _P), ("infr14_insr", _P),
         ("settle_insr", _P), ("cgroup_insr", _P),
     ]
+
+
+class Restraint(ctypes.Structure):
+    _fields_ = [
+        ("system", ctypes.c_int), ("kind", ctypes.c_int), ("atoms", ctypes.c_int * 4),
+        ("k2", ctypes.c_double), ("k3", ctypes.c_double), ("r1", ctypes.c_double),
+        ("r2", ctypes.c_double), ("r3", ctypes.c_double), ("r4", ctypes.c_double),
+        ("target", ctypes.c_double * 3),
+    ]
+
+
+RESTRAINT_POSITION, RESTRAINT_DISTANCE, RESTRAINT_ANGLE, RESTRAINT_DIHEDRAL = 1, 2, 3, 4
 
 
 class MinimizeControls(ctypes.Structure):
@@ -195,6 +207,7 @@ def library() -> ctypes.CDLL:
             "sb_get_forces": (ctypes.c_int, [vp, vp, vp]),
             "sb_get_energies": (ctypes.c_int, [vp, vp, vp]),
             "sb_download_results_async": (ctypes.c_int, [vp, vp, vp, vp]),
+            "sb_set_restraints": (ctypes.c_int, [vp, ctypes.POINTER(Restraint), ctypes.c_int]),
             "sb_get_gb_workspace": (ctypes.c_int, [vp, vp, vp, vp, vp]),
             "sb_get_forces_fixed": (ctypes.c_int, [vp, vp, vp, vp]),
             "sb_get_energies_fixed": (ctypes.c_int, [vp, vp, vp]),
@@ -812,6 +825,24 @@ class Synthesis:
         _check(library().sb_get_energies(self.handle, out.ctypes.data, stream),
                "sb_get_energies")
         return out.reshape(self.nsys, NRG_STRIDE)
+
+    def set_restraints(self, restraints):
+        """Replace the synthesis's restraints: an iterable of dicts with system, kind
+        (RESTRAINT_*), atoms, k2, k3, r1-r4 and, for positional ones, target."""
+        rs = list(restraints)
+        arr = (Restraint * max(1, len(rs)))()
+        for q, r in enumerate(rs):
+            a = list(r["atoms"]) + [0] * (4 - len(r["atoms"]))
+            arr[q].system = int(r.get("system", 0))
+            arr[q].kind = int(r["kind"])
+            for m in range(4):
+                arr[q].atoms[m] = int(a[m])
+            for f in ("k2", "k3", "r1", "r2", "r3", "r4"):
+                setattr(arr[q], f, float(r[f]))
+            t = r.get("target", (0.0, 0.0, 0.0))
+            for m in range(3):
+                arr[q].target[m] = float(t[m])
+        _check(library().sb_set_restraints(self.handle, arr, len(rs)), "sb_set_restraints")
 
     def download_async(self, forces=None, energies=None, stream=None):
         """Enqueue the forces (3 per atom) and energies (nsys x NRG_STRIDE) into page-locked

@@ -1,5 +1,6 @@
-// CHARMM terms of a synthesis, in FP64 from the exact fixed-point coordinates, one thread per
-// term, after the fused pass (or the tiled / FP64 path) has evaluated everything else:
+// CHARMM terms and restraints of a synthesis, in FP64 from the exact fixed-point coordinates,
+// one thread per term, after the fused pass (or the tiled / FP64 path) has evaluated everything
+// else:
 //
 //   Urey-Bradley     k (r_ik - r0)^2 between the outer atoms of an angle
 //                    (Potential/valence_potential.tpp:659-691 with evalHarmonicStretch)
@@ -10,6 +11,8 @@
 //                    shifted by pi into [0, 2 pi) and mapped onto the surface's grid cells
 //                    (valence_potential.tpp:789-1222); the 16 coefficients of each cell are
 //                    built on the host (cmapPatches in synthesis.cu)
+//   restraints       STORMM's flat-bottom positional, distance, angle and dihedral restraints
+//                    (valence_potential.tpp:1558-2050), constant ones
 //
 // Every force and energy enters the int64 accumulators through integer atomics of the term's
 // own contribution rounded to the fixed-point grid, so sums do not depend on scheduling; the
@@ -166,7 +169,138 @@ kCharmmTerms(const DevCharmm c, int ub0, int nub, int ci0, int nci, int cm0, int
   }
 }
 
+constexpr int kSlotRestraint = 12;       // StateVariable::RESTRAINT
+
+// The flat-bottom potential of a restrained value d (Restraints/restraint_util.tpp:9-46):
+// returns the energy and sets *g = -dE/dd
+__device__ __forceinline__ double flatBottom(double d, double2 k, double4 r, double* g) {
+  double keq, dl, e;
+  if (d < r.x) {
+    dl = r.x - r.y;
+    keq = k.x;
+    e = keq * (dl * dl + 2.0 * dl * (d - r.x));
+  }
+  else if (d < r.y) {
+    dl = d - r.y;
+    keq = k.x;
+    e = keq * dl * dl;
+  }
+  else if (d < r.z) {
+    dl = 0.0;
+    keq = 0.0;
+    e = 0.0;
+  }
+  else if (d < r.w) {
+    dl = d - r.z;
+    keq = k.y;
+    e = keq * dl * dl;
+  }
+  else {
+    dl = r.w - r.z;
+    keq = k.y;
+    e = keq * (dl * dl + 2.0 * dl * (d - r.w));
+  }
+  *g = -2.0 * keq * dl;
+  return e;
+}
+
+template <bool FORCE, bool ENERGY>
+__global__ void __launch_bounds__(128)
+kRestraints(const DevCharmm c, int first, int count) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
+    const int q = first + t;
+    const int4 a = c.rst_atoms[q];
+    const int2 meta = c.rst_meta[q];
+    const double2 k = c.rst_k[q];
+    const double4 r = c.rst_r[q];
+    double e = 0.0, g = 0.0;
+    if (meta.x == 1) {
+      // positional: distance of the atom from the target point
+      const double4 tg = c.rst_target[q];
+      const double3 d = make_double3(static_cast<double>(c.xcrd[a.x]) * c.inv_gpos_scale - tg.x,
+                                     static_cast<double>(c.ycrd[a.x]) * c.inv_gpos_scale - tg.y,
+                                     static_cast<double>(c.zcrd[a.x]) * c.inv_gpos_scale - tg.z);
+      const double dr = sqrt(dot3d(d, d));
+      e = flatBottom(dr, k, r, &g);
+      if (FORCE) {
+        if (dr < 1.0e-8) {
+          // at the target itself the direction is arbitrary: the force is split evenly over
+          // the three axes, as the reference does
+          const double f = g / sqrt(3.0);
+          addForce(c, a.x, f, f, f);
+        }
+        else {
+          const double f = g / dr;
+          addForce(c, a.x, f * d.x, f * d.y, f * d.z);
+        }
+      }
+    }
+    else if (meta.x == 2) {
+      const double3 d = displacement(c, a.x, a.y);
+      const double dr = sqrt(dot3d(d, d));
+      e = flatBottom(dr, k, r, &g);
+      if (FORCE) {
+        const double f = g / dr;
+        addForce(c, a.y, f * d.x, f * d.y, f * d.z);
+        addForce(c, a.x, -f * d.x, -f * d.y, -f * d.z);
+      }
+    }
+    else if (meta.x == 3) {
+      // angle at the second atom, from acos of the normalized dot product as the reference
+      // measures it
+      const double3 ba = displacement(c, a.y, a.x);
+      const double3 bc = displacement(c, a.y, a.z);
+      const double inv_ba = rsqrt(dot3d(ba, ba)), inv_bc = rsqrt(dot3d(bc, bc));
+      double cs = dot3d(ba, bc) * inv_ba * inv_bc;
+      cs = fmin(1.0, fmax(-1.0, cs));
+      e = flatBottom(acos(cs), k, r, &g);
+      if (FORCE) {
+        // dtheta/dr_i = -(bc / (|ba||bc|) - cos ba / |ba|^2) / sin
+        const double s = g / sqrt(fmax(1.0 - cs * cs, 1.0e-30));
+        const double3 fi = make_double3(-s * (bc.x * inv_ba * inv_bc - cs * ba.x * inv_ba * inv_ba),
+                                        -s * (bc.y * inv_ba * inv_bc - cs * ba.y * inv_ba * inv_ba),
+                                        -s * (bc.z * inv_ba * inv_bc - cs * ba.z * inv_ba * inv_ba));
+        const double3 fk = make_double3(-s * (ba.x * inv_ba * inv_bc - cs * bc.x * inv_bc * inv_bc),
+                                        -s * (ba.y * inv_ba * inv_bc - cs * bc.y * inv_bc * inv_bc),
+                                        -s * (ba.z * inv_ba * inv_bc - cs * bc.z * inv_bc * inv_bc));
+        addForce(c, a.x, fi.x, fi.y, fi.z);
+        addForce(c, a.z, fk.x, fk.y, fk.z);
+        addForce(c, a.y, -(fi.x + fk.x), -(fi.y + fk.y), -(fi.z + fk.z));
+      }
+    }
+    else {
+      const double3 ab = displacement(c, a.x, a.y);
+      const double3 bc = displacement(c, a.y, a.z);
+      const double3 cd = displacement(c, a.z, a.w);
+      const double mid = 0.5 * (r.y + r.z);
+      double th = dihedralAngle(ab, bc, cd) - mid;
+      th -= kTwoPi * rint(th / kTwoPi);       // within pi of the midpoint
+      e = flatBottom(mid + th, k, r, &g);
+      if (FORCE) dihedralForces(c, a.x, a.y, a.z, a.w, ab, bc, cd, g);
+    }
+    if (ENERGY) addEnergy(c, meta.y, kSlotRestraint, e);
+  }
+}
+
 }  // namespace
+
+cudaError_t launchRestraints(const DevCharmm &c, int first, int count, bool force, bool energy,
+                             int sm_count, cudaStream_t stream) {
+  if (count == 0 || (!force && !energy)) return cudaSuccess;
+  int blocks = (count + 127) / 128;
+  const int cap = 8 * (sm_count > 0 ? sm_count : 148);
+  blocks = blocks > cap ? cap : blocks;
+  if (force && energy) {
+    kRestraints<true, true><<<blocks, 128, 0, stream>>>(c, first, count);
+  }
+  else if (force) {
+    kRestraints<true, false><<<blocks, 128, 0, stream>>>(c, first, count);
+  }
+  else {
+    kRestraints<false, true><<<blocks, 128, 0, stream>>>(c, first, count);
+  }
+  return cudaGetLastError();
+}
 
 cudaError_t launchCharmmTerms(const DevCharmm &c, int ub0, int nub, int ci0, int nci, int cm0,
                               int ncm, bool force, bool energy, int sm_count,

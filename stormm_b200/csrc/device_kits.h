@@ -250,6 +250,13 @@ struct DevCharmm {
   long long* zfrc = nullptr;
   unsigned long long* energies = nullptr;
   double inv_gpos_scale = 0.0, frc_scale = 0.0, nrg_scale = 0.0;
+  // restraints: atoms in the padded layout (unused ones repeat the first), x kind y system,
+  // stiffnesses, bounds r1-r4, positional target
+  const int4* rst_atoms = nullptr;
+  const int2* rst_meta = nullptr;
+  const double2* rst_k = nullptr;
+  const double4* rst_r = nullptr;
+  const double4* rst_target = nullptr;
 };
 
 // Arrays zeroed by one launch of launchClear: 16-byte aligned bases, lengths in 16-byte words

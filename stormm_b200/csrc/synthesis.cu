@@ -57,6 +57,8 @@ cudaError_t launchClear(const ClearList &list, int sm_count, cudaStream_t stream
 cudaError_t launchCharmmTerms(const DevCharmm &c, int ub0, int nub, int ci0, int nci, int cm0,
                               int ncm, bool force, bool energy, int sm_count,
                               cudaStream_t stream);
+cudaError_t launchRestraints(const DevCharmm &c, int first, int count, bool force, bool energy,
+                             int sm_count, cudaStream_t stream);
 
 namespace {
 thread_local std::string g_last_error;
@@ -361,15 +363,97 @@ void Synthesis::buildCharmm(const sb_topology* tops, int ntop) {
 }
 
 // The CHARMM terms of systems [first, last)
-void Synthesis::launchCharmm(int first, int last, bool force, bool energy,
-                             cudaStream_t stream) {
-  if (!has_charmm) return;
-  DevCharmm c = dev_charmm;
-  cudaCheck(launchCharmmTerms(c, h_ubrd_start[first], h_ubrd_start[last] - h_ubrd_start[first],
-                              h_cimp_start[first], h_cimp_start[last] - h_cimp_start[first],
-                              h_cmap_start[first], h_cmap_start[last] - h_cmap_start[first],
-                              force, energy, sm_count, stream),
-            "CHARMM term launch");
+void Synthesis::launchExtraTerms(int first, int last, bool force, bool energy,
+                                 cudaStream_t stream) {
+  if (has_charmm) {
+    cudaCheck(launchCharmmTerms(dev_charmm, h_ubrd_start[first],
+                                h_ubrd_start[last] - h_ubrd_start[first], h_cimp_start[first],
+                                h_cimp_start[last] - h_cimp_start[first], h_cmap_start[first],
+                                h_cmap_start[last] - h_cmap_start[first], force, energy,
+                                sm_count, stream),
+              "CHARMM term launch");
+  }
+  if (!h_rst_start.empty() && h_rst_start[nsys] > 0) {
+    cudaCheck(launchRestraints(dev_charmm, h_rst_start[first],
+                               h_rst_start[last] - h_rst_start[first], force, energy, sm_count,
+                               stream),
+              "restraint launch");
+  }
+}
+
+// Restraints replace the previous set; records sorted by system so that a system's restraints
+// are one contiguous range
+void Synthesis::setRestraints(const sb_restraint* list, int count) {
+  if (count < 0 || (count > 0 && list == nullptr)) {
+    throw Error(SB_ERR_ARGUMENT, "restraints: negative count or no list");
+  }
+  std::vector<int> order(count);
+  for (int q = 0; q < count; q++) {
+    const sb_restraint &r = list[q];
+    if (r.system < 0 || r.system >= nsys) {
+      throw Error(SB_ERR_ARGUMENT, "restraint " + std::to_string(q) + ": system out of range");
+    }
+    if (r.kind < SB_RESTRAINT_POSITION || r.kind > SB_RESTRAINT_DIHEDRAL) {
+      throw Error(SB_ERR_ARGUMENT, "restraint " + std::to_string(q) + ": unknown kind");
+    }
+    for (int m = 0; m < r.kind; m++) {
+      if (r.atoms[m] < 0 || r.atoms[m] >= atom_count[r.system]) {
+        throw Error(SB_ERR_ARGUMENT, "restraint " + std::to_string(q) + ": atom out of range");
+      }
+    }
+    if (!(r.r1 <= r.r2 && r.r2 <= r.r3 && r.r3 <= r.r4) || !(r.k2 >= 0.0) || !(r.k3 >= 0.0) ||
+        !std::isfinite(r.r1) || !std::isfinite(r.r4) || !std::isfinite(r.k2) ||
+        !std::isfinite(r.k3)) {
+      throw Error(SB_ERR_ARGUMENT, "restraint " + std::to_string(q) + ": bounds must ascend and "
+                  "stiffnesses be finite and non-negative");
+    }
+    order[q] = q;
+  }
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return list[a].system < list[b].system; });
+  std::vector<int4> atoms(count);
+  std::vector<int2> meta(count);
+  std::vector<double2> kk(count);
+  std::vector<double4> rr(count), tg(count);
+  h_rst_start.assign(nsys + 1, 0);
+  for (int q = 0; q < count; q++) {
+    const sb_restraint &r = list[order[q]];
+    const int base = atom_start[r.system];
+    int a[4];
+    for (int m = 0; m < 4; m++) a[m] = base + ((m < r.kind) ? r.atoms[m] : r.atoms[0]);
+    atoms[q] = make_int4(a[0], a[1], a[2], a[3]);
+    meta[q] = make_int2(r.kind, r.system);
+    kk[q] = make_double2(r.k2, r.k3);
+    rr[q] = make_double4(r.r1, r.r2, r.r3, r.r4);
+    tg[q] = make_double4(r.target[0], r.target[1], r.target[2], 0.0);
+    h_rst_start[r.system + 1]++;
+  }
+  for (int s = 0; s < nsys; s++) h_rst_start[s + 1] += h_rst_start[s];
+  if (count > 0) {
+    UploadArena arena;
+    arena.put(&d_rst_atoms, atoms);
+    arena.put(&d_rst_meta, meta);
+    arena.put(&d_rst_k, kk);
+    arena.put(&d_rst_r, rr);
+    arena.put(&d_rst_target, tg);
+    arena.commit(&d_rst_arena);
+  }
+  dev_charmm.rst_atoms = d_rst_atoms.p;
+  dev_charmm.rst_meta = d_rst_meta.p;
+  dev_charmm.rst_k = d_rst_k.p;
+  dev_charmm.rst_r = d_rst_r.p;
+  dev_charmm.rst_target = d_rst_target.p;
+  dev_charmm.xcrd = d_xcrd.p;
+  dev_charmm.ycrd = d_ycrd.p;
+  dev_charmm.zcrd = d_zcrd.p;
+  dev_charmm.xfrc = d_xfrc.p;
+  dev_charmm.yfrc = d_yfrc.p;
+  dev_charmm.zfrc = d_zfrc.p;
+  dev_charmm.energies = d_energies.p;
+  dev_charmm.inv_gpos_scale = std::ldexp(1.0, -opt.gpos_bits);
+  dev_charmm.frc_scale = std::ldexp(1.0, opt.frc_bits);
+  dev_charmm.nrg_scale = std::ldexp(1.0, opt.nrg_bits);
+  restraint_version++;
 }
 
 void UploadArena::commit(DeviceArray<unsigned char>* block) {
@@ -1192,7 +1276,7 @@ void Synthesis::evaluate(int terms, bool force, bool energy, cudaStream_t stream
   launchTiledRange(0, static_cast<int>(h_tiled_systems.size()), terms, force, energy, stream,
                    clash);
   if (terms & SB_TERM_VALENCE) {
-    launchCharmm(0, nsys, force, energy, stream);
+    launchExtraTerms(0, nsys, force, energy, stream);
   }
 }
 
@@ -1242,6 +1326,11 @@ void Synthesis::rejectTiledMinimization(int kernel) const {
     throw Error(SB_ERR_UNSUPPORTED, "the FP64 mode minimizes with the graph minimizer "
                 "(SB_MIN_GRAPH) only");
   }
+  if (!h_rst_start.empty() && h_rst_start[nsys] > 0 && kernel != SB_MIN_GRAPH) {
+    throw Error(SB_ERR_UNSUPPORTED, "restraints are evaluated by a kernel of their own and "
+                "cannot be minimized on chip by the persistent kernel; the graph minimizer "
+                "(SB_MIN_GRAPH) minimizes them");
+  }
   if (has_charmm && kernel != SB_MIN_GRAPH) {
     throw Error(SB_ERR_UNSUPPORTED, "CHARMM terms are evaluated by a kernel of their own and "
                 "cannot be minimized on chip by the persistent kernel; the graph minimizer "
@@ -1281,7 +1370,7 @@ void Synthesis::evaluateRange(int first, int count, int terms, bool force, bool 
                 "per-system evaluation launch");
     }
     if (terms & SB_TERM_VALENCE) {
-      launchCharmm(s, s + 1, force, energy, stream);
+      launchExtraTerms(s, s + 1, force, energy, stream);
     }
   }
 }
@@ -1564,7 +1653,7 @@ void Synthesis::evaluateFor(int first, int count, bool single, bool force, cudaS
     launchPlan(*eval_plan, SB_TERM_ALL, force, true, stream, clash);
     launchTiledRange(0, static_cast<int>(h_tiled_systems.size()), SB_TERM_ALL, force, true,
                      stream, clash);
-    launchCharmm(0, nsys, force, true, stream);
+    launchExtraTerms(0, nsys, force, true, stream);
     return;
   }
   DevSynthesis d = dev;
@@ -1582,7 +1671,7 @@ void Synthesis::evaluateFor(int first, int count, bool single, bool force, cudaS
       cudaCheck(launchEvalFused(d, s, s + 1, single_lj, SB_TERM_ALL, force, true, 1, threads,
                                 stream, clash.on()), "per-system evaluation launch");
     }
-    launchCharmm(s, s + 1, force, true, stream);
+    launchExtraTerms(s, s + 1, force, true, stream);
   }
 }
 
@@ -1670,7 +1759,8 @@ void Synthesis::minimizeAdvance(int cycles, bool final_energy, cudaStream_t stre
     // the graph holds its kernels' arguments by value: capture again when any of them changed
     const bool stale = cycle_graph == nullptr || cycle_graph_plan != eval_plan.get() ||
                        std::memcmp(&cycle_graph_min, &dev_min, sizeof(DevMinimizer)) != 0 ||
-                       std::memcmp(&cycle_graph_dev, &dev, sizeof(DevSynthesis)) != 0;
+                       std::memcmp(&cycle_graph_dev, &dev, sizeof(DevSynthesis)) != 0 ||
+                       cycle_graph_restraints != restraint_version;
     if (stale) {
       // capture one cycle on a stream of the synthesis' own, then replay it on the caller's
       if (cycle_graph != nullptr) {
@@ -1699,6 +1789,7 @@ void Synthesis::minimizeAdvance(int cycles, bool final_energy, cudaStream_t stre
       cycle_graph_plan = eval_plan.get();
       cycle_graph_min = dev_min;
       cycle_graph_dev = dev;
+      cycle_graph_restraints = restraint_version;
     }
     for (int c = 0; c < cycles; c++) {
       cudaCheck(cudaGraphLaunch(cycle_graph, stream), "cudaGraphLaunch");
@@ -2077,6 +2168,10 @@ int sb_get_forces(sb_synthesis* syn, double* xyz, void* stream) {
 
 int sb_get_energies(sb_synthesis* syn, double* energies, void* stream) {
   return guarded([&]() { need(syn)->getEnergies(energies, asStream(stream)); });
+}
+
+int sb_set_restraints(sb_synthesis* syn, const sb_restraint* restraints, int count) {
+  return guarded([&]() { need(syn)->setRestraints(restraints, count); });
 }
 
 int sb_download_results_async(sb_synthesis* syn, double* forces, double* energies,

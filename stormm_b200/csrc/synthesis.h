@@ -203,6 +203,7 @@ public:
   void getForcesFixed(long long* prim, int* ovrf, cudaStream_t stream);
   void getEnergies(double* out, cudaStream_t stream);
   void downloadResults(double* forces, double* energies, cudaStream_t stream);
+  void setRestraints(const sb_restraint* list, int count);
   void getEnergiesFixed(long long* out, cudaStream_t stream);
   void getGbWorkspace(double* psi, double* radii, double* sde, cudaStream_t stream);
   int checkStatus(cudaStream_t stream);
@@ -271,6 +272,14 @@ public:
   DeviceArray<int2> d_cmap_surf;
   DeviceArray<double> d_cmap_patch;
   DevCharmm dev_charmm;
+  // restraints (sb_set_restraints): records sorted by system, per-system ranges on the host
+  std::vector<int> h_rst_start;
+  DeviceArray<unsigned char> d_rst_arena;
+  DeviceArray<int4> d_rst_atoms;
+  DeviceArray<int2> d_rst_meta;
+  DeviceArray<double2> d_rst_k;
+  DeviceArray<double4> d_rst_r, d_rst_target;
+  int restraint_version = 0;
   DeviceArray<int> d_atom_start, d_atom_count, d_bond_start, d_angl_start, d_dihe_start;
   DeviceArray<int> d_lj_start, d_lj_ntypes, d_tile_start, d_ljidx, d_tile_mask_idx;
   DeviceArray<float> d_charge, d_rho, d_srho, d_pb, d_alpha, d_beta, d_gamma;
@@ -335,6 +344,7 @@ public:
   const UnitPlan* cycle_graph_plan = nullptr;
   DevMinimizer cycle_graph_min{};   // kernel arguments the graph was captured with
   DevSynthesis cycle_graph_dev{};
+  int cycle_graph_restraints = 0;
   cudaStream_t capture_stream = nullptr;
   ~Synthesis();
 
@@ -343,7 +353,7 @@ public:
 private:
   void buildLayout(const sb_topology* tops, int ntop);
   void buildCharmm(const sb_topology* tops, int ntop);
-  void launchCharmm(int first, int last, bool force, bool energy, cudaStream_t stream);
+  void launchExtraTerms(int first, int last, bool force, bool energy, cudaStream_t stream);
   // defer: leave the device copy of the plan to the caller (the constructor's UploadArena)
   std::unique_ptr<UnitPlan> makePlan(int max_slots_cap, int max_tiles_cap,
                                      bool defer = false) const;

@@ -32,6 +32,9 @@ Fixtures written (numpy .npz, one per case):
 * ``charmm_ala_dipeptide.npz`` and ``charmm_dhfr.npz`` (``--charmm-only``):
   systems with CHARMM terms (one CMAP term; 2,117 Urey-Bradley terms, 418 CHARMM impropers and
   157 CMAP terms), with STORMM's energies and forces of each CHARMM term kind.
+* ``restraints_r60.npz`` (``--restraints-only``): 40 constant restraints (positional, distance,
+  angle and dihedral, the measured value in each region of the flat-bottom potential) on a
+  60-atom molecule, STORMM's energy of each, the total and the forces.
 * ``synthetic_K64.npz`` and ``minimize_clash_k64.npz`` (``--clash-only``): a 64-atom molecule
   with close contacts (0.45 A start noise), its clash-mitigated evaluation (softened cores below
   1.5 A and below 0.9 of the pair's sigma) beside the plain one, and a minimization whose first
@@ -116,6 +119,8 @@ def main():
                     help="write only the nonbonded work-unit fixtures")
     ap.add_argument("--charmm-only", action="store_true",
                     help="write only the CHARMM-term fixtures")
+    ap.add_argument("--restraints-only", action="store_true",
+                    help="write only the restraint fixture")
     args = ap.parse_args()
     if not os.path.exists(DRIVER):
         raise SystemExit("build the reference driver first: make -C oracle/ref -j8")
@@ -125,6 +130,9 @@ def main():
             return
         if args.charmm_only:
             charmm_systems(args.reference_root, tmp)
+            return
+        if args.restraints_only:
+            restraint_case(tmp)
             return
         if args.neck_only:
             for name, seed, n, igb in (("N7", 8820, 80, "7"), ("N8", 8821, 80, "8")):
@@ -200,6 +208,62 @@ def reference_systems(ref_root, tmp, models):
             rec["known_answer_gb"] = np.array([answers[key][ans_idx]])
             np.savez_compressed(os.path.join(HERE, f"reference_{sname}_igb{igb}.npz"), **rec)
             print("wrote", sname, igb, rec["energy_terms"][-1], answers[key][ans_idx])
+
+
+def _dihedral(p0, p1, p2, p3):
+    b0, b1, b2 = p1 - p0, p2 - p1, p3 - p2
+    n1, n2 = np.cross(b0, b1), np.cross(b1, b2)
+    return np.arctan2(np.linalg.norm(b1) * b0 @ n2, n1 @ n2)
+
+
+def restraint_case(tmp):
+    """Constant restraints of every kind on a 60-atom molecule, the measured value of each
+    placed in each region of the flat-bottom potential (below r1, r1-r2, r2-r3, r3-r4, above
+    r4), evaluated by STORMM's CPU code."""
+    mol = synthetic.make_molecule(8830, 60, noise=0.1, name="R60")
+    rec, top, crd = eval_molecule(mol, tmp)
+    x = rec["coords"].reshape(-1, 3)
+    rng = np.random.default_rng(8830)
+    # offsets of r1..r4 from the measured value that put it in region 0..4
+    regions = [(0.3, 0.5, 0.7, 0.9), (-0.1, 0.2, 0.4, 0.6), (-0.3, -0.1, 0.1, 0.3),
+               (-0.6, -0.4, -0.1, 0.2), (-0.9, -0.7, -0.5, -0.3)]
+    rows = []
+    for kind in (1, 2, 3, 4):
+        for reg, off in enumerate(regions):
+            for rep in range(2):
+                atoms = rng.choice(mol.natom, size=4, replace=False)
+                k2, k3 = rng.uniform(2.0, 30.0, size=2)
+                target = np.zeros(3)
+                if kind == 1:
+                    target = x[atoms[0]] + rng.normal(size=3) * 1.5
+                    value, scale = np.linalg.norm(x[atoms[0]] - target), 1.0
+                elif kind == 2:
+                    value, scale = np.linalg.norm(x[atoms[1]] - x[atoms[0]]), 1.0
+                elif kind == 3:
+                    ba, bc = x[atoms[0]] - x[atoms[1]], x[atoms[2]] - x[atoms[1]]
+                    value = np.arccos(ba @ bc / np.linalg.norm(ba) / np.linalg.norm(bc))
+                    scale = 0.5
+                else:
+                    value, scale = _dihedral(*x[atoms]), 0.8
+                r = [value + scale * o for o in off]
+                if kind in (1, 2):
+                    r = [max(v, 0.0) for v in r]      # distances are not negative
+                elif kind == 3:
+                    r = [min(max(v, 0.0), np.pi) for v in r]
+                used = list(atoms[:kind]) + [-1] * (4 - kind)
+                rows.append([kind] + used + [k2, k3] + r + list(target))
+    lst = os.path.join(tmp, "restraints.txt")
+    with open(lst, "w") as f:
+        for row in rows:
+            f.write(" ".join(repr(float(v)) if i > 4 else str(int(v)) for i, v in enumerate(row))
+                    + "\n")
+    out = os.path.join(tmp, "restraints.bin")
+    run_driver(["restraint", top, crd, lst, out, "--quantize"])
+    rrec = read_records(out)
+    rec.update({k: v for k, v in rrec.items() if k != "coords"})
+    rec["restraints"] = np.array(rows, dtype=np.float64)
+    np.savez_compressed(os.path.join(HERE, "restraints_r60.npz"), **rec)
+    print("wrote restraints_r60", len(rows), rrec["restraint_total"])
 
 
 def charmm_systems(ref_root, tmp):
