@@ -80,6 +80,10 @@ struct DevSynthesis {
   const float* gb_alpha;
   const float* gb_beta;
   const float* gb_gamma;
+  // the same GB radius parameters in FP64 (rho, intrinsic radius, alpha, beta; gamma), for the
+  // per-atom effective radius and chain-rule factor, whose OBC form cancels for buried atoms
+  const double4* gb_radius64;
+  const double* gb_gamma64;
 
   // tables
   const float2* ljab;            // (A, B) per type pair

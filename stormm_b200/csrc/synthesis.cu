@@ -582,6 +582,8 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
   h_alpha.assign(np, 0.0f);
   h_beta.assign(np, 0.0f);
   h_gamma.assign(np, 0.0f);
+  h_gb_radius64.assign(np, make_double4(1.0, 1.09, 0.0, 0.0));
+  h_gb_gamma64.assign(np, 0.0);
   if (neck) {
     h_neck_idx.assign(np, 0);
     const size_t nt2 = static_cast<size_t>(opt.neck_table_size) * opt.neck_table_size;
@@ -696,6 +698,10 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
         h_alpha[base + i] = static_cast<float>(tp.gb_alpha ? tp.gb_alpha[i] : gbDefault(opt.igb, 0));
         h_beta[base + i] = static_cast<float>(tp.gb_beta ? tp.gb_beta[i] : gbDefault(opt.igb, 1));
         h_gamma[base + i] = static_cast<float>(tp.gb_gamma ? tp.gb_gamma[i] : gbDefault(opt.igb, 2));
+        h_gb_radius64[base + i] = make_double4(
+            rho, tp.pb_radii[i], tp.gb_alpha ? tp.gb_alpha[i] : gbDefault(opt.igb, 0),
+            tp.gb_beta ? tp.gb_beta[i] : gbDefault(opt.igb, 1));
+        h_gb_gamma64[base + i] = tp.gb_gamma ? tp.gb_gamma[i] : gbDefault(opt.igb, 2);
       }
       if (neck) {
         // AtomGraph::setImplicitSolventModel (Topology/atomgraph_setters.cpp:1088-1092)
@@ -1011,6 +1017,8 @@ void Synthesis::upload() {
   arena.put(&d_alpha, h_alpha);
   arena.put(&d_beta, h_beta);
   arena.put(&d_gamma, h_gamma);
+  arena.put(&d_gb_radius64, h_gb_radius64);
+  arena.put(&d_gb_gamma64, h_gb_gamma64);
   arena.put(&d_ljab, h_ljab);
   arena.put(&d_ljab14, h_ljab14);
   arena.put(&d_bonds, h_bonds);
@@ -1195,6 +1203,8 @@ void Synthesis::upload() {
   d.gb_alpha = d_alpha.p;
   d.gb_beta = d_beta.p;
   d.gb_gamma = d_gamma.p;
+  d.gb_radius64 = d_gb_radius64.p;
+  d.gb_gamma64 = d_gb_gamma64.p;
   d.ljab = d_ljab.p;
   d.ljab14 = d_ljab14.p;
   d.bonds = d_bonds.p;

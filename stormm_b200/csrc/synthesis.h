@@ -246,6 +246,8 @@ public:
 
   // host staging of the packed layout
   std::vector<float> h_charge, h_rho, h_srho, h_pb, h_alpha, h_beta, h_gamma;
+  std::vector<double4> h_gb_radius64;
+  std::vector<double> h_gb_gamma64;
   std::vector<int> h_ljidx, h_lj_start, h_lj_ntypes, h_tile_start, h_tile_mask_idx;
   std::vector<int> h_bond_start, h_angl_start, h_dihe_start;
   std::vector<float2> h_ljab, h_ljab14;
@@ -283,6 +285,8 @@ public:
   DeviceArray<int> d_atom_start, d_atom_count, d_bond_start, d_angl_start, d_dihe_start;
   DeviceArray<int> d_lj_start, d_lj_ntypes, d_tile_start, d_ljidx, d_tile_mask_idx;
   DeviceArray<float> d_charge, d_rho, d_srho, d_pb, d_alpha, d_beta, d_gamma;
+  DeviceArray<double4> d_gb_radius64;
+  DeviceArray<double> d_gb_gamma64;
   DeviceArray<float2> d_ljab, d_ljab14;
   DeviceArray<uint4> d_bonds, d_angles, d_dihe_a, d_dihe_b;
   DeviceArray<double4> d_angl64, d_dihe64;

@@ -397,8 +397,8 @@ kTiledAtoms(const DevSynthesis d, const DevTiled t, int atom_begin, int atom_end
     float e_self = 0.0f;
     float egbi = 1.0f;
     if (a < d.atom_count[sysid]) {
-      const float psi = static_cast<float>(t.psi_acc[gi]) * inv_ps;
-      egbi = effectiveRadius(d, gi, psi, d.rho[gi]);
+      const double psi = static_cast<double>(t.psi_acc[gi]) * static_cast<double>(inv_ps);
+      egbi = effectiveRadius(d, gi, psi);
       float self_de;
       e_self = gbSelfTerm(d, d.charge[gi], egbi, &self_de);
       if (FORCE) {
@@ -434,8 +434,8 @@ kTiledChain(const DevSynthesis d, const DevTiled t, int atom_begin, int atom_end
     if (a < d.atom_count[sysid]) {
       sde = static_cast<float>(t.de_acc[gi]) * inv_ds;
       if (d.igb != 1) {
-        const float psi = static_cast<float>(t.psi_acc[gi]) * inv_ps;
-        sde *= obcChainFactor(d, gi, psi, d.rho[gi]);
+        const double psi = static_cast<double>(t.psi_acc[gi]) * static_cast<double>(inv_ps);
+        sde *= obcChainFactor(d, gi, psi);
       }
       if (WS) {
         d.sumdeijda[gi] = __double2ll_rn(static_cast<double>(sde) * d.psi_out_scale);

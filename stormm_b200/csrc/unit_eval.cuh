@@ -1506,20 +1506,24 @@ __device__ void gbDerivativeTiles(const DevSynthesis &d, const UnitSmem &s, int 
 // Per-atom GB steps between the pair passes (nonbonded_potential.tpp:730-805, 982-1021)
 // ------------------------------------------------------------------------------------------------
 // Effective radius of atom gi from its descreening sum psi (HCT, or OBC / OBC-II)
-__device__ __forceinline__ float effectiveRadius(const DevSynthesis &d, int gi, float psi,
-                                                 float rho) {
-  float egbi;
+// Effective GB radius of an atom from its descreening sum psi, in FP64 with the FP64
+// parameters: the OBC form 1 / (1 / rho - tanh(...) / r) cancels for buried atoms, where tanh
+// nears 1 and 1 / rho - 1 / r is a small difference, and FP32 there loses the 1e-6 relative
+// accuracy of the GB energy on compact proteins.  One evaluation per atom, so FP64 costs
+// nothing measurable.
+__device__ __forceinline__ float effectiveRadius(const DevSynthesis &d, int gi, double psi) {
+  const double4 p = d.gb_radius64[gi];   // rho, intrinsic radius, alpha, beta
+  double egbi;
   if (d.igb == 1) {
-    egbi = 1.0f / (1.0f / rho + psi);
-    if (egbi < 0.0f) egbi = 30.0f;
+    egbi = 1.0 / (1.0 / p.x + psi);
+    if (egbi < 0.0) egbi = 30.0;
   }
   else {
-    const float fipsi = psi * (-rho);
-    egbi = 1.0f / (1.0f / rho - tanhf((d.gb_alpha[gi] - d.gb_beta[gi] * fipsi +
-                                       d.gb_gamma[gi] * fipsi * fipsi) * fipsi) /
-                                d.pb_radii[gi]);
+    const double fipsi = psi * (-p.x);
+    egbi = 1.0 / (1.0 / p.x - tanh((p.z - p.w * fipsi + d.gb_gamma64[gi] * fipsi * fipsi) *
+                                   fipsi) / p.y);
   }
-  return egbi;
+  return static_cast<float>(egbi);
 }
 
 // GB self energy of a charge q (scaled by sqrt of the Coulomb constant) with effective radius
@@ -1536,13 +1540,15 @@ __device__ __forceinline__ float gbSelfTerm(const DevSynthesis &d, float q, floa
 }
 
 // OBC chain-rule factor dR/dpsi-type prefactor applied to the summed dE/dR
-__device__ __forceinline__ float obcChainFactor(const DevSynthesis &d, int gi, float psi,
-                                                float rho) {
-  const float fipsi = psi * (-rho);
-  const float al = d.gb_alpha[gi], be = d.gb_beta[gi], ga = d.gb_gamma[gi];
-  const float thi = tanhf((al - (be - ga * fipsi) * fipsi) * fipsi);
-  return (al - (2.0f * be - 3.0f * ga * fipsi) * fipsi) * (1.0f - thi * thi) * rho /
-         d.pb_radii[gi];
+// OBC chain-rule factor (the dR/dpsi-type prefactor applied to the summed dE/dR), in FP64 for
+// the same reason: 1 - tanh^2 cancels where tanh nears 1
+__device__ __forceinline__ float obcChainFactor(const DevSynthesis &d, int gi, double psi) {
+  const double4 p = d.gb_radius64[gi];
+  const double fipsi = psi * (-p.x);
+  const double ga = d.gb_gamma64[gi];
+  const double thi = tanh((p.z - (p.w - ga * fipsi) * fipsi) * fipsi);
+  return static_cast<float>((p.z - (2.0 * p.w - 3.0 * ga * fipsi) * fipsi) * (1.0 - thi * thi) *
+                            p.x / p.y);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -1704,8 +1710,9 @@ __device__ void evaluateStaged(const DevSynthesis &d, const UnitSmem &s, const U
       float egbi = 1.0f;
       if (a < s.natom[k]) {
         const int gi = d.atom_start[s.sys[k]] + a;
-        const float psi = static_cast<float>(int63ToLong(s.psi[slot], s.psio[slot])) * inv_ps;
-        egbi = effectiveRadius(d, gi, psi, prm.z);
+        const double psi = static_cast<double>(int63ToLong(s.psi[slot], s.psio[slot])) *
+                           static_cast<double>(inv_ps);
+        egbi = effectiveRadius(d, gi, psi);
         float self_de;
         e_self = gbSelfTerm(d, prm.x, egbi, &self_de);
         if (FORCE) {
@@ -1776,8 +1783,9 @@ __device__ void evaluateStaged(const DevSynthesis &d, const UnitSmem &s, const U
         const int gi = d.atom_start[s.sys[k]] + a;
         sde = static_cast<float>(int63ToLong(s.de[slot], s.deo[slot])) * inv_ds;
         if (d.igb != 1) {
-          const float psi = static_cast<float>(int63ToLong(s.psi[slot], s.psio[slot])) * inv_ps;
-          sde *= obcChainFactor(d, gi, psi, prm.z);
+          const double psi = static_cast<double>(int63ToLong(s.psi[slot], s.psio[slot])) *
+                             static_cast<double>(inv_ps);
+          sde *= obcChainFactor(d, gi, psi);
         }
         if (WS) {
           d.sumdeijda[gi] = __double2ll_rn(static_cast<double>(sde) * d.psi_out_scale);

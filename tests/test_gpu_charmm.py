@@ -45,8 +45,8 @@ def test_charmm_terms_match_stormm(name, precision):
     tol = 1e-9 * np.abs(g["charmm_terms"]) + counts * 2.0 ** -27
     assert np.all(np.abs(charmm - g["charmm_terms"]) <= tol), (charmm, g["charmm_terms"])
     if precision == sb.PRECISION_SINGLE and name == "charmm_dhfr.npz":
-        # the FP32 tiled path on this 2,489-atom protein: GB measured at 1.42 times its 1e-6
-        # per-term bound (FP32 Born radii summed over some 2,500 partners an atom), every other
+        # the FP32 tiled path on this 2,489-atom protein: GB measured at 1.36 times its 1e-6
+        # per-term bound (FP32 descreening sums over some 2,500 partners an atom), every other
         # term within its bound; the FP64 mode (the other parametrization) meets all bounds
         excess = energy_excess(syn.energy_terms()[0], g["energy_terms"], fixture_magnitudes(g))
         assert excess[:8].max() <= 1.0 and excess[8] <= 1.5, excess
