@@ -240,7 +240,10 @@ int sb_launch_valence(sb_synthesis* syn, int eval_force, int eval_energy, void* 
 int sb_evaluate_clash(sb_synthesis* syn, int terms, int eval_force, int eval_energy,
                       double clash_distance, double clash_ratio, void* stream);
 
-/* Number of work units the batched launches use, and the launch shape chosen */
+/* Number of work units the batched launches use, and the launch shape chosen: threads is the
+ * block size of the evaluation launch of packed units (512 when that launch holds fewer units
+ * than one wave of 256-thread blocks, unless sb_autotune found 256 faster or threads_per_block
+ * fixes it) */
 int sb_launch_info(const sb_synthesis* syn, int* work_units, int* blocks, int* threads);
 
 /* ------------------------------------------------------------------------------------------ */

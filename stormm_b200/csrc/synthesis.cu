@@ -1268,7 +1268,8 @@ void Synthesis::launchPlan(const UnitPlan &plan, int terms, bool force, bool ene
 // atoms: 141 us against 184); beyond one wave the 256-thread blocks are faster.  Sums are
 // fixed-point, so the block size changes no result bit.
 int Synthesis::launchThreads(int units, int terms) const {
-  if (opt.threads_per_block > 0 || terms != SB_TERM_ALL || units >= 4 * sm_count) {
+  if (opt.threads_per_block > 0 || !allow_wide || terms != SB_TERM_ALL ||
+      units >= 4 * sm_count) {
     return threads;
   }
   return 512;
@@ -1908,6 +1909,8 @@ void Synthesis::autotune(int what, int* chosen_slots, int* chosen_tiles, double*
   ctl.sd_cycles = 4;
   double best = 1.0e30;
   std::unique_ptr<UnitPlan> best_plan;
+  bool best_wide = allow_wide;
+  const bool keep_wide = allow_wide;
   for (const auto &c : candidates) {
     std::unique_ptr<UnitPlan> plan;
     try {
@@ -1916,27 +1919,41 @@ void Synthesis::autotune(int what, int* chosen_slots, int* chosen_tiles, double*
     catch (const Error &) {
       continue;   // a candidate that does not fit this synthesis
     }
-    float ms = 0.0f;
-    if (what == SB_TUNE_EVALUATE) {
-      launchPlan(*plan, SB_TERM_ALL, true, true, stream);
-      cudaCheck(cudaEventRecord(e0, stream), "cudaEventRecord");
-      for (int r = 0; r < 3; r++) {
+    // evaluation packings are timed with both block-size rules: 512-thread blocks for launches
+    // of fewer units than one wave of 256-thread blocks, or 256 threads throughout
+    const int modes = (what == SB_TUNE_EVALUATE && opt.threads_per_block <= 0) ? 2 : 1;
+    double plan_best = 1.0e30;
+    bool plan_wide = keep_wide;
+    for (int mode = 0; mode < modes; mode++) {
+      allow_wide = (modes == 2) ? (mode == 0) : keep_wide;
+      float ms = 0.0f;
+      if (what == SB_TUNE_EVALUATE) {
         launchPlan(*plan, SB_TERM_ALL, true, true, stream);
+        cudaCheck(cudaEventRecord(e0, stream), "cudaEventRecord");
+        for (int r = 0; r < 3; r++) {
+          launchPlan(*plan, SB_TERM_ALL, true, true, stream);
+        }
+        cudaCheck(cudaEventRecord(e1, stream), "cudaEventRecord");
       }
-      cudaCheck(cudaEventRecord(e1, stream), "cudaEventRecord");
+      else {
+        minimizeBegin(ctl, stream);
+        cudaCheck(cudaEventRecord(e0, stream), "cudaEventRecord");
+        launchMinPlan(*plan, ctl.total_cycles, false, stream);
+        cudaCheck(cudaEventRecord(e1, stream), "cudaEventRecord");
+        copy3(d_xcrd.p, d_ycrd.p, d_zcrd.p, keep.p, keep.p + np, keep.p + 2 * np);
+      }
+      cudaCheck(cudaEventSynchronize(e1), "cudaEventSynchronize");
+      cudaCheck(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+      if (ms < plan_best) {
+        plan_best = ms;
+        plan_wide = allow_wide;
+      }
     }
-    else {
-      minimizeBegin(ctl, stream);
-      cudaCheck(cudaEventRecord(e0, stream), "cudaEventRecord");
-      launchMinPlan(*plan, ctl.total_cycles, false, stream);
-      cudaCheck(cudaEventRecord(e1, stream), "cudaEventRecord");
-      copy3(d_xcrd.p, d_ycrd.p, d_zcrd.p, keep.p, keep.p + np, keep.p + 2 * np);
-    }
-    cudaCheck(cudaEventSynchronize(e1), "cudaEventSynchronize");
-    cudaCheck(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
-    if (ms < best) {
-      best = ms;
+    allow_wide = keep_wide;
+    if (plan_best < best) {
+      best = plan_best;
       best_plan = std::move(plan);
+      best_wide = plan_wide;
     }
   }
   cudaEventDestroy(e0);
@@ -1953,6 +1970,7 @@ void Synthesis::autotune(int what, int* chosen_slots, int* chosen_tiles, double*
   if (chosen_tiles) *chosen_tiles = best_plan->max_tiles_cap;
   if (best_ms) *best_ms = best;
   if (what == SB_TUNE_EVALUATE) {
+    allow_wide = best_wide;
     eval_plan = std::move(best_plan);
     dev.nunit = eval_plan->units.size();
     dev.unit_desc = eval_plan->d_units.p;
@@ -2260,7 +2278,12 @@ int sb_launch_info(const sb_synthesis* syn, int* work_units, int* blocks, int* t
     const sb::Synthesis* s = need(syn);
     if (work_units) *work_units = s->eval_plan->units.size();
     if (blocks) *blocks = s->eval_plan->units.size();
-    if (threads) *threads = s->threads;
+    if (threads) {
+      // block size of the batched evaluation's launch of packed units
+      const int n = static_cast<int>(s->eval_plan->units.size());
+      const int packed = n - s->eval_plan->n_big;
+      *threads = s->launchThreads(packed > 0 ? packed : n, SB_TERM_ALL);
+    }
   });
 }
 

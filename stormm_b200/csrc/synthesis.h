@@ -204,6 +204,7 @@ public:
   void getEnergies(double* out, cudaStream_t stream);
   void downloadResults(double* forces, double* energies, cudaStream_t stream);
   void setRestraints(const sb_restraint* list, int count);
+  int launchThreads(int units, int terms) const;
   void getEnergiesFixed(long long* out, cudaStream_t stream);
   void getGbWorkspace(double* psi, double* radii, double* sde, cudaStream_t stream);
   int checkStatus(cudaStream_t stream);
@@ -362,7 +363,7 @@ private:
   std::unique_ptr<UnitPlan> makePlan(int max_slots_cap, int max_tiles_cap,
                                      bool defer = false) const;
   void finalizePlan(UnitPlan* plan, bool defer = false) const;
-  int launchThreads(int units, int terms) const;
+  bool allow_wide = true;        // 512-thread blocks for small all-term launches (autotuned)
   void launchPlan(const UnitPlan &plan, int terms, bool force, bool energy, cudaStream_t stream,
                   const Clash &clash = Clash());
   void launchMinPlan(const UnitPlan &plan, int cycles, bool final_energy, cudaStream_t stream);

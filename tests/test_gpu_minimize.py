@@ -225,8 +225,11 @@ def test_autotune_keeps_results():
     e_ref = syn.energies_fixed().copy()
     syn.minimize(total_cycles=20, sd_cycles=5)
     c_min = syn.coordinates().copy()
+    assert syn.launch_info()["threads"] == 512      # eight molecules: far below one wave
     slots, tiles, ms = syn.autotune(sb.TUNE_EVALUATE)
     assert slots % 32 == 0 and tiles > 0 and ms > 0
+    # the tuner also chose the block-size rule; either way no result bit changes
+    assert syn.launch_info()["threads"] in (256, 512)
     syn.set_coordinates(xyz)
     syn.initialize()
     syn.evaluate()
