@@ -477,12 +477,21 @@ int sb_nonbonded_work_units(const sb_topology* tops, int ntop, const int* topolo
 /* Restraints                                                                                  */
 /* ------------------------------------------------------------------------------------------ */
 /* STORMM's flat-bottom restraints (Restraints/bounded_restraint.h, evaluated as
- * Potential/valence_potential.tpp:1558-2050 and Restraints/restraint_util.tpp:9-46), constant
- * (a restraint whose initial and final steps coincide): for the restrained value d (distance
- * from the target point, distance between two atoms, angle, or dihedral angle in radians), the
- * energy is k2 (d - r2)^2 between r1 and r2, zero between r2 and r3, k3 (d - r3)^2 between r3 and
- * r4, and continues linearly below r1 and above r4.  A dihedral is taken within pi of
- * (r2 + r3) / 2.  Energies go to slot SB_RESTRAINT. */
+ * Potential/valence_potential.tpp:1558-2050 and Restraints/restraint_util.tpp:9-77): for the
+ * restrained value d (distance from the target point, distance between two atoms, angle, or
+ * dihedral angle in radians), the energy is k2 (d - r2)^2 between r1 and r2, zero between r2 and
+ * r3, k3 (d - r3)^2 between r3 and r4, and continues linearly below r1 and above r4.  A dihedral
+ * is taken within pi of (r2 + r3) / 2.  Energies go to slot SB_RESTRAINT.
+ *
+ * Time dependence (computeRestraintMixture): at step s, a restraint is absent while
+ * s < init_step; with init_step == final_step it then holds its initial values (the final ones
+ * are ignored, so a zero-filled tail is a constant restraint from step 0); otherwise the
+ * stiffnesses, bounds and target are (1 - w) initial + w final with
+ * w = (s - init_step) / (final_step - init_step) up to final_step, and the final values after.
+ * The step is the synthesis's restraint step (sb_set_restraint_step, 0 by default) for
+ * evaluations, and each system's completed cycle count inside the graph minimizer (the cycle's
+ * four evaluations at its index, the final evaluation at the cycles run), as STORMM's
+ * minimizer hands its cycle counter to the restraints. */
 #define SB_RESTRAINT_POSITION 1
 #define SB_RESTRAINT_DISTANCE 2
 #define SB_RESTRAINT_ANGLE 3
@@ -495,11 +504,19 @@ typedef struct {
   double k2, k3;               /* stiffness of the lower and upper walls (kcal/mol per unit^2) */
   double r1, r2, r3, r4;       /* bounds, ascending (A, or radians for angles and dihedrals) */
   double target[3];            /* positional restraints: the reference point (A) */
+  int init_step, final_step;   /* steps at which the restraint engages and is complete */
+  double final_k2, final_k3;   /* values at final_step (used when final_step > init_step) */
+  double final_r1, final_r2, final_r3, final_r4;
+  double final_target[3];
 } sb_restraint;
 
 /* Replace the synthesis's restraints (count 0 removes them); evaluated with the valence terms
  * and by the graph minimizer (the persistent minimizer refuses restrained syntheses). */
 int sb_set_restraints(sb_synthesis* syn, const sb_restraint* restraints, int count);
+
+/* The step at which evaluations outside the minimizer take time-dependent restraints
+ * (non-negative; SB_ERR_ARGUMENT otherwise). */
+int sb_set_restraint_step(sb_synthesis* syn, int step);
 
 /* ------------------------------------------------------------------------------------------ */
 /* STORMM's valence work units                                                                 */

@@ -45,6 +45,12 @@
 //       y z" (kind 1 positional, 2 distance, 3 angle, 4 dihedral; 0-based atoms, unused ones
 //       -1; the target x y z used by positional restraints); writes each restraint's energy,
 //       the total and the forces.
+//   restraintramp <prmtop> <inpcrd> <restraint-file> <steps> <out.bin>
+//       The same for time-dependent restraints, one a line: "kind i j k l init_step final_step
+//       k2 k3 r1 r2 r3 r4 x y z k2' k3' r1' r2' r3' r4' x' y' z'" (initial values, then final
+//       ones), evaluated at each step of the comma-separated <steps>: each restraint's energy,
+//       the total and the forces at step s are written as restraint_energies_s,
+//       restraint_total_s and frc_restraint_s.
 //   nbwu <list-file> <out.bin> [--init-task N]
 //       STORMM's nonbonded work units (Synthesis/nonbonded_workunit.cpp) for a synthesis: each
 //       line of <list-file> is "<prmtop> <system count>", the systems laid out topology by
@@ -64,6 +70,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <sstream>
 #include <string>
 #include <vector>
 #include "copyright.h"
@@ -750,6 +757,69 @@ int runNbwu(const std::string &list_file, const std::string &out, const Options 
   return 0;
 }
 
+// Time-dependent restraints on one structure, evaluated by STORMM's CPU code at several steps
+int runRestraintRamp(const std::string &prmtop, const std::string &inpcrd,
+                     const std::string &list, const std::string &steps, const std::string &out,
+                     const Options &opt) {
+  AtomGraph ag = loadTopology(prmtop, opt);
+  PhaseSpace ps(inpcrd, CoordinateFileKind::AMBER_INPCRD);
+  if (opt.quantize) {
+    quantizeCoordinates(&ps);
+  }
+  std::ifstream in(list);
+  std::vector<BoundedRestraint> rs;
+  int kind, a[4], s0, s1;
+  double v[18];
+  while (in >> kind >> a[0] >> a[1] >> a[2] >> a[3] >> s0 >> s1) {
+    for (int m = 0; m < 18; m++) {
+      in >> v[m];
+    }
+    const double3 t0 = { v[6], v[7], v[8] };
+    const double3 t1 = { v[15], v[16], v[17] };
+    switch (kind) {
+    case 1:
+      rs.emplace_back(a[0], &ag, s0, s1, v[0], v[1], v[2], v[3], v[4], v[5], v[9], v[10], v[11],
+                      v[12], v[13], v[14], t0, t1);
+      break;
+    case 2:
+      rs.emplace_back(a[0], a[1], &ag, s0, s1, v[0], v[1], v[2], v[3], v[4], v[5], v[9], v[10],
+                      v[11], v[12], v[13], v[14]);
+      break;
+    case 3:
+      rs.emplace_back(a[0], a[1], a[2], &ag, s0, s1, v[0], v[1], v[2], v[3], v[4], v[5], v[9],
+                      v[10], v[11], v[12], v[13], v[14]);
+      break;
+    default:
+      rs.emplace_back(a[0], a[1], a[2], a[3], &ag, s0, s1, v[0], v[1], v[2], v[3], v[4], v[5],
+                      v[9], v[10], v[11], v[12], v[13], v[14]);
+      break;
+    }
+  }
+  RecordWriter rw(out);
+  PhaseSpaceWriter psw = ps.data();
+  putCoordinates(&rw, "coords", psw);
+  std::stringstream ss(steps);
+  std::string tok;
+  while (std::getline(ss, tok, ',')) {
+    const int step = std::atoi(tok.c_str());
+    std::vector<double> each;
+    for (const BoundedRestraint &r : rs) {
+      const RestraintApparatus one(std::vector<BoundedRestraint>(1, r), &ag);
+      ScoreCard sc1(1, 1, 32);
+      each.push_back(evaluateRestraints(one, &ps, &sc1, EvaluateForce::NO, 0, step));
+    }
+    const RestraintApparatus ra(rs, &ag);
+    ScoreCard sc(1, 1, 32);
+    zeroForces(psw);
+    const double total = evaluateRestraints(ra, &ps, &sc, EvaluateForce::YES, 0, step);
+    putForces(&rw, "frc_restraint_" + tok, psw);
+    rw.d("restraint_energies_" + tok, each);
+    rw.scalar("restraint_total_" + tok, total);
+    std::printf("step %d: restraints %zu, energy %.10f\n", step, rs.size(), total);
+  }
+  return 0;
+}
+
 // Constant restraints of several kinds on one structure, evaluated by STORMM's CPU code
 int runRestraint(const std::string &prmtop, const std::string &inpcrd, const std::string &list,
                  const std::string &out, const Options &opt) {
@@ -1068,6 +1138,9 @@ int main(int argc, char* argv[]) {
   }
   if (mode == "restraint" && pos.size() == 4) {
     return runRestraint(pos[0], pos[1], pos[2], pos[3], opt);
+  }
+  if (mode == "restraintramp" && pos.size() == 5) {
+    return runRestraintRamp(pos[0], pos[1], pos[2], pos[3], pos[4], opt);
   }
   if (mode == "vwu" && pos.size() == 2) {
     return runVwu(pos[0], pos[1], opt, vwu_atoms);

@@ -110,6 +110,11 @@ class Restraint(ctypes.Structure):
         ("k2", ctypes.c_double), ("k3", ctypes.c_double), ("r1", ctypes.c_double),
         ("r2", ctypes.c_double), ("r3", ctypes.c_double), ("r4", ctypes.c_double),
         ("target", ctypes.c_double * 3),
+        ("init_step", ctypes.c_int), ("final_step", ctypes.c_int),
+        ("final_k2", ctypes.c_double), ("final_k3", ctypes.c_double),
+        ("final_r1", ctypes.c_double), ("final_r2", ctypes.c_double),
+        ("final_r3", ctypes.c_double), ("final_r4", ctypes.c_double),
+        ("final_target", ctypes.c_double * 3),
     ]
 
 
@@ -208,6 +213,7 @@ def library() -> ctypes.CDLL:
             "sb_get_energies": (ctypes.c_int, [vp, vp, vp]),
             "sb_download_results_async": (ctypes.c_int, [vp, vp, vp, vp]),
             "sb_set_restraints": (ctypes.c_int, [vp, ctypes.POINTER(Restraint), ctypes.c_int]),
+            "sb_set_restraint_step": (ctypes.c_int, [vp, ctypes.c_int]),
             "sb_get_gb_workspace": (ctypes.c_int, [vp, vp, vp, vp, vp]),
             "sb_get_forces_fixed": (ctypes.c_int, [vp, vp, vp, vp]),
             "sb_get_energies_fixed": (ctypes.c_int, [vp, vp, vp]),
@@ -828,7 +834,9 @@ class Synthesis:
 
     def set_restraints(self, restraints):
         """Replace the synthesis's restraints: an iterable of dicts with system, kind
-        (RESTRAINT_*), atoms, k2, k3, r1-r4 and, for positional ones, target."""
+        (RESTRAINT_*), atoms, k2, k3, r1-r4 and, for positional ones, target; a time-dependent
+        restraint adds init_step, final_step and the final_* values (the same names with a
+        final_ prefix), which it reaches by a linear ramp between the two steps."""
         rs = list(restraints)
         arr = (Restraint * max(1, len(rs)))()
         for q, r in enumerate(rs):
@@ -842,7 +850,19 @@ class Synthesis:
             t = r.get("target", (0.0, 0.0, 0.0))
             for m in range(3):
                 arr[q].target[m] = float(t[m])
+            arr[q].init_step = int(r.get("init_step", 0))
+            arr[q].final_step = int(r.get("final_step", arr[q].init_step))
+            for f in ("k2", "k3", "r1", "r2", "r3", "r4"):
+                setattr(arr[q], "final_" + f, float(r.get("final_" + f, 0.0)))
+            t = r.get("final_target", (0.0, 0.0, 0.0))
+            for m in range(3):
+                arr[q].final_target[m] = float(t[m])
         _check(library().sb_set_restraints(self.handle, arr, len(rs)), "sb_set_restraints")
+
+    def set_restraint_step(self, step):
+        """The step at which evaluations take time-dependent restraints (sb_set_restraint_step;
+        the graph minimizer uses each system's cycle count instead)."""
+        _check(library().sb_set_restraint_step(self.handle, int(step)), "sb_set_restraint_step")
 
     def download_async(self, forces=None, energies=None, stream=None):
         """Enqueue the forces (3 per atom) and energies (nsys x NRG_STRIDE) into page-locked

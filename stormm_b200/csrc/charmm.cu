@@ -204,6 +204,22 @@ __device__ __forceinline__ double flatBottom(double d, double2 k, double4 r, dou
   return e;
 }
 
+// Weights of the initial and final values at a step (Restraints/restraint_util.tpp:48-75)
+__device__ __forceinline__ double2 restraintMixture(int step, int2 s) {
+  if (step < s.x) return make_double2(0.0, 0.0);
+  if (s.x == s.y) return make_double2(1.0, 0.0);
+  if (step < s.y) {
+    const double w = static_cast<double>(step - s.x) / static_cast<double>(s.y - s.x);
+    return make_double2(1.0 - w, w);
+  }
+  return make_double2(0.0, 1.0);
+}
+
+// w.x a + w.y b, each product rounded before the sum as the host code rounds it
+__device__ __forceinline__ double mix(double2 w, double a, double b) {
+  return __dadd_rn(__dmul_rn(w.x, a), __dmul_rn(w.y, b));
+}
+
 template <bool FORCE, bool ENERGY>
 __global__ void __launch_bounds__(128)
 kRestraints(const DevCharmm c, int first, int count) {
@@ -211,12 +227,19 @@ kRestraints(const DevCharmm c, int first, int count) {
     const int q = first + t;
     const int4 a = c.rst_atoms[q];
     const int2 meta = c.rst_meta[q];
-    const double2 k = c.rst_k[q];
-    const double4 r = c.rst_r[q];
+    const int step = (c.rst_cycle != nullptr) ? c.rst_cycle[meta.y] : c.rst_step;
+    const double2 w = restraintMixture(step, c.rst_steps[q]);
+    const double2 k0 = c.rst_k[q], k1 = c.rst_kf[q];
+    const double4 r0 = c.rst_r[q], r1 = c.rst_rf[q];
+    const double2 k = make_double2(mix(w, k0.x, k1.x), mix(w, k0.y, k1.y));
+    const double4 r = make_double4(mix(w, r0.x, r1.x), mix(w, r0.y, r1.y), mix(w, r0.z, r1.z),
+                                   mix(w, r0.w, r1.w));
     double e = 0.0, g = 0.0;
     if (meta.x == 1) {
       // positional: distance of the atom from the target point
-      const double4 tg = c.rst_target[q];
+      const double4 t0 = c.rst_target[q], t1 = c.rst_target_f[q];
+      const double3 tg = make_double3(mix(w, t0.x, t1.x), mix(w, t0.y, t1.y),
+                                      mix(w, t0.z, t1.z));
       const double3 d = make_double3(static_cast<double>(c.xcrd[a.x]) * c.inv_gpos_scale - tg.x,
                                      static_cast<double>(c.ycrd[a.x]) * c.inv_gpos_scale - tg.y,
                                      static_cast<double>(c.zcrd[a.x]) * c.inv_gpos_scale - tg.z);
@@ -272,7 +295,8 @@ kRestraints(const DevCharmm c, int first, int count) {
       const double3 ab = displacement(c, a.x, a.y);
       const double3 bc = displacement(c, a.y, a.z);
       const double3 cd = displacement(c, a.z, a.w);
-      const double mid = 0.5 * (r.y + r.z);
+      // the midpoint mixes the end points' sums (valence_potential.tpp:1954)
+      const double mid = 0.5 * mix(w, r0.y + r0.z, r1.y + r1.z);
       double th = dihedralAngle(ab, bc, cd) - mid;
       th -= kTwoPi * rint(th / kTwoPi);       // within pi of the midpoint
       e = flatBottom(mid + th, k, r, &g);

@@ -261,6 +261,14 @@ struct DevCharmm {
   const double2* rst_k = nullptr;
   const double4* rst_r = nullptr;
   const double4* rst_target = nullptr;
+  // time dependence: final stiffnesses, bounds and target, the steps at which the restraint
+  // engages and is complete, and the step (rst_cycle: per-system cycle counts that replace it)
+  const double2* rst_kf = nullptr;
+  const double4* rst_rf = nullptr;
+  const double4* rst_target_f = nullptr;
+  const int2* rst_steps = nullptr;
+  int rst_step = 0;
+  const int* rst_cycle = nullptr;
 };
 
 // Arrays zeroed by one launch of launchClear: 16-byte aligned bases, lengths in 16-byte words

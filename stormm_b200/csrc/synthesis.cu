@@ -362,9 +362,10 @@ void Synthesis::buildCharmm(const sb_topology* tops, int ntop) {
   has_charmm = !(h_ubrd.empty() && h_cimp.empty() && h_cmap.empty());
 }
 
-// The CHARMM terms of systems [first, last)
+// The CHARMM terms and restraints of systems [first, last); cycle: the minimizer's per-system
+// cycle counts, which then give the step of time-dependent restraints
 void Synthesis::launchExtraTerms(int first, int last, bool force, bool energy,
-                                 cudaStream_t stream) {
+                                 cudaStream_t stream, const int* cycle) {
   if (has_charmm) {
     cudaCheck(launchCharmmTerms(dev_charmm, h_ubrd_start[first],
                                 h_ubrd_start[last] - h_ubrd_start[first], h_cimp_start[first],
@@ -374,7 +375,9 @@ void Synthesis::launchExtraTerms(int first, int last, bool force, bool energy,
               "CHARMM term launch");
   }
   if (!h_rst_start.empty() && h_rst_start[nsys] > 0) {
-    cudaCheck(launchRestraints(dev_charmm, h_rst_start[first],
+    DevCharmm c = dev_charmm;
+    c.rst_cycle = cycle;
+    cudaCheck(launchRestraints(c, h_rst_start[first],
                                h_rst_start[last] - h_rst_start[first], force, energy, sm_count,
                                stream),
               "restraint launch");
@@ -401,11 +404,20 @@ void Synthesis::setRestraints(const sb_restraint* list, int count) {
         throw Error(SB_ERR_ARGUMENT, "restraint " + std::to_string(q) + ": atom out of range");
       }
     }
-    if (!(r.r1 <= r.r2 && r.r2 <= r.r3 && r.r3 <= r.r4) || !(r.k2 >= 0.0) || !(r.k3 >= 0.0) ||
-        !std::isfinite(r.r1) || !std::isfinite(r.r4) || !std::isfinite(r.k2) ||
-        !std::isfinite(r.k3)) {
+    auto sane = [](double k2, double k3, double r1, double r2, double r3, double r4) {
+      return r1 <= r2 && r2 <= r3 && r3 <= r4 && k2 >= 0.0 && k3 >= 0.0 && std::isfinite(r1) &&
+             std::isfinite(r4) && std::isfinite(k2) && std::isfinite(k3);
+    };
+    const bool ramp = r.final_step != r.init_step;
+    if (!sane(r.k2, r.k3, r.r1, r.r2, r.r3, r.r4) ||
+        (ramp && !sane(r.final_k2, r.final_k3, r.final_r1, r.final_r2, r.final_r3,
+                       r.final_r4))) {
       throw Error(SB_ERR_ARGUMENT, "restraint " + std::to_string(q) + ": bounds must ascend and "
                   "stiffnesses be finite and non-negative");
+    }
+    if (r.init_step < 0 || r.final_step < r.init_step) {
+      throw Error(SB_ERR_ARGUMENT, "restraint " + std::to_string(q) + ": steps must satisfy "
+                  "0 <= init_step <= final_step");
     }
     order[q] = q;
   }
@@ -413,8 +425,9 @@ void Synthesis::setRestraints(const sb_restraint* list, int count) {
                    [&](int a, int b) { return list[a].system < list[b].system; });
   std::vector<int4> atoms(count);
   std::vector<int2> meta(count);
-  std::vector<double2> kk(count);
-  std::vector<double4> rr(count), tg(count);
+  std::vector<double2> kk(count), kf(count);
+  std::vector<double4> rr(count), tg(count), rf(count), tf(count);
+  std::vector<int2> steps(count);
   h_rst_start.assign(nsys + 1, 0);
   for (int q = 0; q < count; q++) {
     const sb_restraint &r = list[order[q]];
@@ -426,6 +439,17 @@ void Synthesis::setRestraints(const sb_restraint* list, int count) {
     kk[q] = make_double2(r.k2, r.k3);
     rr[q] = make_double4(r.r1, r.r2, r.r3, r.r4);
     tg[q] = make_double4(r.target[0], r.target[1], r.target[2], 0.0);
+    steps[q] = make_int2(r.init_step, r.final_step);
+    if (r.final_step != r.init_step) {
+      kf[q] = make_double2(r.final_k2, r.final_k3);
+      rf[q] = make_double4(r.final_r1, r.final_r2, r.final_r3, r.final_r4);
+      tf[q] = make_double4(r.final_target[0], r.final_target[1], r.final_target[2], 0.0);
+    }
+    else {
+      kf[q] = kk[q];
+      rf[q] = rr[q];
+      tf[q] = tg[q];
+    }
     h_rst_start[r.system + 1]++;
   }
   for (int s = 0; s < nsys; s++) h_rst_start[s + 1] += h_rst_start[s];
@@ -436,6 +460,10 @@ void Synthesis::setRestraints(const sb_restraint* list, int count) {
     arena.put(&d_rst_k, kk);
     arena.put(&d_rst_r, rr);
     arena.put(&d_rst_target, tg);
+    arena.put(&d_rst_kf, kf);
+    arena.put(&d_rst_rf, rf);
+    arena.put(&d_rst_target_f, tf);
+    arena.put(&d_rst_steps, steps);
     arena.commit(&d_rst_arena);
   }
   dev_charmm.rst_atoms = d_rst_atoms.p;
@@ -443,6 +471,10 @@ void Synthesis::setRestraints(const sb_restraint* list, int count) {
   dev_charmm.rst_k = d_rst_k.p;
   dev_charmm.rst_r = d_rst_r.p;
   dev_charmm.rst_target = d_rst_target.p;
+  dev_charmm.rst_kf = d_rst_kf.p;
+  dev_charmm.rst_rf = d_rst_rf.p;
+  dev_charmm.rst_target_f = d_rst_target_f.p;
+  dev_charmm.rst_steps = d_rst_steps.p;
   dev_charmm.xcrd = d_xcrd.p;
   dev_charmm.ycrd = d_ycrd.p;
   dev_charmm.zcrd = d_zcrd.p;
@@ -1664,7 +1696,7 @@ void Synthesis::evaluateFor(int first, int count, bool single, bool force, cudaS
     launchPlan(*eval_plan, SB_TERM_ALL, force, true, stream, clash);
     launchTiledRange(0, static_cast<int>(h_tiled_systems.size()), SB_TERM_ALL, force, true,
                      stream, clash);
-    launchExtraTerms(0, nsys, force, true, stream);
+    launchExtraTerms(0, nsys, force, true, stream, dev_min.cycle);
     return;
   }
   DevSynthesis d = dev;
@@ -1682,7 +1714,7 @@ void Synthesis::evaluateFor(int first, int count, bool single, bool force, cudaS
       cudaCheck(launchEvalFused(d, s, s + 1, single_lj, SB_TERM_ALL, force, true, 1, threads,
                                 stream, clash.on()), "per-system evaluation launch");
     }
-    launchExtraTerms(s, s + 1, force, true, stream);
+    launchExtraTerms(s, s + 1, force, true, stream, dev_min.cycle);
   }
 }
 
@@ -2200,6 +2232,13 @@ int sb_get_energies(sb_synthesis* syn, double* energies, void* stream) {
 
 int sb_set_restraints(sb_synthesis* syn, const sb_restraint* restraints, int count) {
   return guarded([&]() { need(syn)->setRestraints(restraints, count); });
+}
+
+int sb_set_restraint_step(sb_synthesis* syn, int step) {
+  return guarded([&]() {
+    if (step < 0) throw sb::Error(SB_ERR_ARGUMENT, "restraint step must be non-negative");
+    need(syn)->dev_charmm.rst_step = step;
+  });
 }
 
 int sb_download_results_async(sb_synthesis* syn, double* forces, double* energies,

@@ -282,6 +282,9 @@ public:
   DeviceArray<int2> d_rst_meta;
   DeviceArray<double2> d_rst_k;
   DeviceArray<double4> d_rst_r, d_rst_target;
+  DeviceArray<double2> d_rst_kf;               // final stiffnesses, bounds and targets
+  DeviceArray<double4> d_rst_rf, d_rst_target_f;
+  DeviceArray<int2> d_rst_steps;               // initial and final steps
   int restraint_version = 0;
   DeviceArray<int> d_atom_start, d_atom_count, d_bond_start, d_angl_start, d_dihe_start;
   DeviceArray<int> d_lj_start, d_lj_ntypes, d_tile_start, d_ljidx, d_tile_mask_idx;
@@ -358,7 +361,8 @@ public:
 private:
   void buildLayout(const sb_topology* tops, int ntop);
   void buildCharmm(const sb_topology* tops, int ntop);
-  void launchExtraTerms(int first, int last, bool force, bool energy, cudaStream_t stream);
+  void launchExtraTerms(int first, int last, bool force, bool energy, cudaStream_t stream,
+                        const int* cycle = nullptr);
   // defer: leave the device copy of the plan to the caller (the constructor's UploadArena)
   std::unique_ptr<UnitPlan> makePlan(int max_slots_cap, int max_tiles_cap,
                                      bool defer = false) const;

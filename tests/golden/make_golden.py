@@ -35,6 +35,10 @@ Fixtures written (numpy .npz, one per case):
 * ``restraints_r60.npz`` (``--restraints-only``): 40 constant restraints (positional, distance,
   angle and dihedral, the measured value in each region of the flat-bottom potential) on a
   60-atom molecule, STORMM's energy of each, the total and the forces.
+* ``restraint_ramps_r60.npz`` (``--ramps-only``): 24 time-dependent restraints on the same
+  molecule (initial and final bounds, stiffnesses and targets, a ramp between two steps, or
+  both steps equal), STORMM's energies and forces at steps before, at, within and after the
+  ramps.
 * ``synthetic_K64.npz`` and ``minimize_clash_k64.npz`` (``--clash-only``): a 64-atom molecule
   with close contacts (0.45 A start noise), its clash-mitigated evaluation (softened cores below
   1.5 A and below 0.9 of the pair's sigma) beside the plain one, and a minimization whose first
@@ -121,6 +125,8 @@ def main():
                     help="write only the CHARMM-term fixtures")
     ap.add_argument("--restraints-only", action="store_true",
                     help="write only the restraint fixture")
+    ap.add_argument("--ramps-only", action="store_true",
+                    help="write only the time-dependent restraint fixture")
     args = ap.parse_args()
     if not os.path.exists(DRIVER):
         raise SystemExit("build the reference driver first: make -C oracle/ref -j8")
@@ -130,6 +136,9 @@ def main():
             return
         if args.charmm_only:
             charmm_systems(args.reference_root, tmp)
+            return
+        if args.ramps_only:
+            ramp_case(tmp)
             return
         if args.restraints_only:
             restraint_case(tmp)
@@ -214,6 +223,70 @@ def _dihedral(p0, p1, p2, p3):
     b0, b1, b2 = p1 - p0, p2 - p1, p3 - p2
     n1, n2 = np.cross(b0, b1), np.cross(b1, b2)
     return np.arctan2(np.linalg.norm(b1) * b0 @ n2, n1 @ n2)
+
+
+RAMP_STEPS = (0, 4, 5, 12, 17, 25, 30, 45)
+
+
+def ramp_case(tmp):
+    """Time-dependent restraints of every kind on the 60-atom molecule of the restraint case:
+    bounds, stiffnesses and positional targets that move from initial to final values between
+    two steps, plus restraints whose initial and final steps coincide (constant once engaged,
+    absent before), evaluated by STORMM's CPU code at steps before, at, within and after
+    every ramp."""
+    mol = synthetic.make_molecule(8830, 60, noise=0.1, name="R60")
+    rec, top, crd = eval_molecule(mol, tmp)
+    x = rec["coords"].reshape(-1, 3)
+    rng = np.random.default_rng(8831)
+    rows = []
+    for kind in (1, 2, 3, 4):
+        for rep in range(6):
+            atoms = rng.choice(mol.natom, size=4, replace=False)
+            if kind == 1:
+                t0 = x[atoms[0]] + rng.normal(size=3) * 1.5
+                t1 = x[atoms[0]] + rng.normal(size=3) * 1.5
+                value, scale = np.linalg.norm(x[atoms[0]] - t0), 1.0
+            else:
+                t0 = t1 = np.zeros(3)
+                if kind == 2:
+                    value, scale = np.linalg.norm(x[atoms[1]] - x[atoms[0]]), 1.0
+                elif kind == 3:
+                    ba, bc = x[atoms[0]] - x[atoms[1]], x[atoms[2]] - x[atoms[1]]
+                    value = np.arccos(ba @ bc / np.linalg.norm(ba) / np.linalg.norm(bc))
+                    scale = 0.5
+                else:
+                    value, scale = _dihedral(*x[atoms]), 0.8
+
+            def bounds():
+                off = np.sort(rng.uniform(-1.0, 1.0, size=4))
+                r = [value + scale * o for o in off]
+                if kind in (1, 2):
+                    r = [max(v, 0.0) for v in r]
+                elif kind == 3:
+                    r = [min(max(v, 0.0), np.pi) for v in r]
+                return r
+
+            s0 = int(rng.choice([0, 5, 12]))
+            s1 = s0 if rep == 5 else s0 + int(rng.choice([13, 18]))
+            k0, k1 = rng.uniform(2.0, 30.0, size=2), rng.uniform(2.0, 30.0, size=2)
+            used = list(atoms[:kind]) + [-1] * (4 - kind)
+            rows.append([kind] + used + [s0, s1] + list(k0) + bounds() + list(t0) + list(k1)
+                        + bounds() + list(t1))
+    lst = os.path.join(tmp, "ramps.txt")
+    with open(lst, "w") as f:
+        for row in rows:
+            f.write(" ".join(repr(float(v)) if i > 6 else str(int(v)) for i, v in enumerate(row))
+                    + "\n")
+    out = os.path.join(tmp, "ramps.bin")
+    run_driver(["restraintramp", top, crd, lst, ",".join(map(str, RAMP_STEPS)), out,
+                "--quantize"])
+    rrec = read_records(out)
+    rec.update({k: v for k, v in rrec.items() if k != "coords"})
+    rec["restraints"] = np.array(rows, dtype=np.float64)
+    rec["steps"] = np.array(RAMP_STEPS, dtype=np.int32)
+    np.savez_compressed(os.path.join(HERE, "restraint_ramps_r60.npz"), **rec)
+    print("wrote restraint_ramps_r60", len(rows), [float(rrec["restraint_total_%d" % s][0])
+                                                   for s in RAMP_STEPS])
 
 
 def restraint_case(tmp):
