@@ -514,6 +514,17 @@ typedef struct {
  * and by the graph minimizer (the persistent minimizer refuses restrained syntheses). */
 int sb_set_restraints(sb_synthesis* syn, const sb_restraint* restraints, int count);
 
+/* STORMM's sphere-point surface area of every system (Potential/surface_area.cpp:46-99 and
+ * surface_area.tpp:28-173, as apps/Gbsa/src/mmgbsa.cpp:248 calls it: every molecule, radii half
+ * the Lennard-Jones sigma of the (type 0, atom type) pair-table entry, double precision) at the
+ * synthesis's current coordinates: for each atom, n_points points (sphere_points, 3 doubles each,
+ * on the unit sphere) at its radius plus probe_radius; a point counts 4 pi (radius + probe)^2 /
+ * n_points unless it lies strictly inside another atom's enlarged sphere in the same or the
+ * next-lower cell along each axis of the reference's grid.  out[s] = area * weight (weight 1:
+ * A^2; STORMM's default 0.005 kcal/mol per A^2, probe 1.4 A).  Synchronous on the stream. */
+int sb_surface_area(sb_synthesis* syn, const double* sphere_points, int n_points,
+                    double probe_radius, double weight, double* out, void* stream);
+
 /* The step at which evaluations outside the minimizer take time-dependent restraints
  * (non-negative; SB_ERR_ARGUMENT otherwise). */
 int sb_set_restraint_step(sb_synthesis* syn, int step);

@@ -245,3 +245,43 @@ def double_to_int95(v: float):
     x, y = ctypes.c_int64(), ctypes.c_int32()
     _lib().orc_double_to_int95(v, ctypes.byref(x), ctypes.byref(y))
     return x.value, y.value
+
+
+def sasa_radii(m) -> np.ndarray:
+    """Per-atom surface-area radii as STORMM's surface area takes them
+    (Potential/surface_area.tpp:163-173): half the sigma of the first n_lj_types entries of the
+    pair table, i.e. of (type 0, atom type), sigma = sqrt(cbrt(A / B)) with B > 1e-6
+    (Topology/atomgraph_detailers.cpp:270-277)."""
+    a = np.asarray(m.lja, dtype=np.float64).reshape(-1)[np.asarray(m.lj_idx)]
+    b = np.asarray(m.ljb, dtype=np.float64).reshape(-1)[np.asarray(m.lj_idx)]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        return np.where(b > 1e-6, 0.5 * np.sqrt(np.cbrt(a / np.where(b > 0, b, 1.0))), 0.0)
+
+
+def surface_area(coords, radii, points, probe=1.4, weight=1.0) -> float:
+    """STORMM's sphere-point surface area (Potential/surface_area.tpp:28-161): cells of at least
+    twice the largest enlarged radius over the bounding box, a point of an atom in cell (i, j, k)
+    tested against atoms in cells i-1..i, j-1..j, k-1..k only, strict inequality, zero when an
+    axis has no extent."""
+    x = np.asarray(coords, dtype=np.float64)
+    pts = np.asarray(points, dtype=np.float64).reshape(-1, 3)
+    origin = x.min(axis=0)
+    length = x.max(axis=0) - origin
+    width_min = 2.0 * (radii.max() + probe)
+    count = np.ceil(length / width_min).astype(int)
+    if (count == 0).any():
+        return 0.0
+    width = length / count
+    cell = np.clip(((x - origin) / width).astype(int), 0, count - 1)
+    r_eff = radii + probe
+    patch = 4.0 * np.pi / len(pts)
+    total = 0.0
+    for m in range(len(x)):
+        near = np.all((cell <= cell[m]) & (cell >= cell[m] - 1), axis=1)
+        near[m] = False
+        p = x[m] + pts * r_eff[m]
+        d = p[:, None, :] - x[near][None, :, :]
+        d2 = (d[..., 0] * d[..., 0] + d[..., 1] * d[..., 1]) + d[..., 2] * d[..., 2]
+        buried = (d2 < r_eff[near][None, :] ** 2).any(axis=1)
+        total += np.count_nonzero(~buried) * (patch * r_eff[m] * r_eff[m])
+    return total * weight

@@ -51,6 +51,10 @@
 //       ones), evaluated at each step of the comma-separated <steps>: each restraint's energy,
 //       the total and the forces at step s are written as restraint_energies_s,
 //       restraint_total_s and frc_restraint_s.
+//   sasa <prmtop> <inpcrd> <n-points> <out.bin>
+//       STORMM's surface area (Potential/surface_area.cpp:46-99, LJ-sigma radii, every
+//       molecule, probe 1.4 A, double precision): the sphere points it places, the area
+//       (weight 1) and the energy at the default 0.005 kcal/mol per A^2.
 //   nbwu <list-file> <out.bin> [--init-task N]
 //       STORMM's nonbonded work units (Synthesis/nonbonded_workunit.cpp) for a synthesis: each
 //       line of <list-file> is "<prmtop> <system count>", the systems laid out topology by
@@ -84,6 +88,9 @@
 #include "Potential/scorecard.h"
 #include "Potential/static_exclusionmask.h"
 #include "Potential/valence_potential.h"
+#include "Potential/surface_area.h"
+#include "Math/geodesic.h"
+#include "Math/series_ops.h"
 #include "Restraints/bounded_restraint.h"
 #include "Restraints/restraint_apparatus.h"
 #include "Structure/clash_detection.h"
@@ -757,6 +764,38 @@ int runNbwu(const std::string &list_file, const std::string &out, const Options 
   return 0;
 }
 
+// Surface area of every molecule of one structure, by STORMM's CPU code
+int runSasa(const std::string &prmtop, const std::string &inpcrd, int npts,
+            const std::string &out, const Options &opt) {
+  AtomGraph ag = loadTopology(prmtop, opt);
+  PhaseSpace ps(inpcrd, CoordinateFileKind::AMBER_INPCRD);
+  if (opt.quantize) {
+    quantizeCoordinates(&ps);
+  }
+  const std::vector<int> mols = incrementingSeries<int>(0, ag.getMoleculeCount());
+  const std::vector<double3> pts = surfaceDistribution<double, double3>(npts);
+  std::vector<double> flat;
+  for (const double3 &p : pts) {
+    flat.push_back(p.x);
+    flat.push_back(p.y);
+    flat.push_back(p.z);
+  }
+  const double area = surfaceArea(&ps, &ag, mols, npts, default_sasa_probe_radius, 1.0,
+                                  EvaluateForce::NO, SasaReference::LENNARD_JONES_SIGMA,
+                                  PrecisionModel::DOUBLE);
+  const double energy = surfaceArea(&ps, &ag, mols, npts, default_sasa_probe_radius,
+                                    default_sasa_energy, EvaluateForce::NO,
+                                    SasaReference::LENNARD_JONES_SIGMA, PrecisionModel::DOUBLE);
+  RecordWriter rw(out);
+  PhaseSpaceWriter psw = ps.data();
+  putCoordinates(&rw, "coords", psw);
+  rw.d("sphere_points", flat);
+  rw.scalar("sasa_area", area);
+  rw.scalar("sasa_energy", energy);
+  std::printf("points %zu, area %.10f, energy %.10f\n", pts.size(), area, energy);
+  return 0;
+}
+
 // Time-dependent restraints on one structure, evaluated by STORMM's CPU code at several steps
 int runRestraintRamp(const std::string &prmtop, const std::string &inpcrd,
                      const std::string &list, const std::string &steps, const std::string &out,
@@ -1138,6 +1177,9 @@ int main(int argc, char* argv[]) {
   }
   if (mode == "restraint" && pos.size() == 4) {
     return runRestraint(pos[0], pos[1], pos[2], pos[3], opt);
+  }
+  if (mode == "sasa" && pos.size() == 4) {
+    return runSasa(pos[0], pos[1], std::atoi(pos[2].c_str()), pos[3], opt);
   }
   if (mode == "restraintramp" && pos.size() == 5) {
     return runRestraintRamp(pos[0], pos[1], pos[2], pos[3], pos[4], opt);

@@ -214,6 +214,8 @@ def library() -> ctypes.CDLL:
             "sb_download_results_async": (ctypes.c_int, [vp, vp, vp, vp]),
             "sb_set_restraints": (ctypes.c_int, [vp, ctypes.POINTER(Restraint), ctypes.c_int]),
             "sb_set_restraint_step": (ctypes.c_int, [vp, ctypes.c_int]),
+            "sb_surface_area": (ctypes.c_int, [vp, vp, ctypes.c_int, ctypes.c_double,
+                                               ctypes.c_double, vp, vp]),
             "sb_get_gb_workspace": (ctypes.c_int, [vp, vp, vp, vp, vp]),
             "sb_get_forces_fixed": (ctypes.c_int, [vp, vp, vp, vp]),
             "sb_get_energies_fixed": (ctypes.c_int, [vp, vp, vp]),
@@ -858,6 +860,17 @@ class Synthesis:
             for m in range(3):
                 arr[q].final_target[m] = float(t[m])
         _check(library().sb_set_restraints(self.handle, arr, len(rs)), "sb_set_restraints")
+
+    def surface_area(self, sphere_points, probe_radius=1.4, weight=1.0, stream=None):
+        """STORMM's sphere-point surface area of every system (sb_surface_area): sphere_points
+        is an (n, 3) array of unit vectors; weight 1 gives A^2, 0.005 STORMM's default energy
+        in kcal/mol."""
+        pts = np.ascontiguousarray(sphere_points, dtype=np.float64).reshape(-1, 3)
+        out = np.zeros(self.nsys)
+        _check(library().sb_surface_area(self.handle, pts.ctypes.data, len(pts),
+                                         float(probe_radius), float(weight), out.ctypes.data,
+                                         stream), "sb_surface_area")
+        return out
 
     def set_restraint_step(self, step):
         """The step at which evaluations take time-dependent restraints (sb_set_restraint_step;

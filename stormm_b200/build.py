@@ -23,7 +23,7 @@ LIB = os.path.join(PKG, "libstormm_b200.so")
 SYNTH_LIB = os.path.join(PKG, "libstormm_b200_synth.so")
 
 CUDA_SOURCES = ["eval_fused.cu", "minimize.cu", "synthesis.cu", "transfers.cu",
-                "static_scratch.cu", "server.cu", "tiled.cu", "fp64.cu", "line_search.cu", "charmm.cu",
+                "static_scratch.cu", "server.cu", "tiled.cu", "fp64.cu", "line_search.cu", "charmm.cu", "sasa.cu",
                 "exclusion_mask.cpp", "valence_units.cpp", "amber_io.cpp", "sdf_io.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-ftz=true"]

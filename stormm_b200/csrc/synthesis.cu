@@ -59,6 +59,11 @@ cudaError_t launchCharmmTerms(const DevCharmm &c, int ub0, int nub, int ci0, int
                               cudaStream_t stream);
 cudaError_t launchRestraints(const DevCharmm &c, int first, int count, bool force, bool energy,
                              int sm_count, cudaStream_t stream);
+cudaError_t launchSurfaceArea(const long long* xcrd, const long long* ycrd,
+                              const long long* zcrd, double inv_gpos_scale,
+                              const int* atom_start, const int* atom_count, int nsys,
+                              const double* radius, const double3* pts, int npts, double probe,
+                              double weight, int* cell, double* out, cudaStream_t stream);
 
 namespace {
 thread_local std::string g_last_error;
@@ -608,6 +613,7 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
   const size_t np = natom_padded;
   h_charge.assign(np, 0.0f);
   h_ljidx.assign(np, 0);
+  h_sasa_radius.assign(np, 0.0);
   h_rho.assign(np, 1.0f);
   h_srho.assign(np, 0.0f);
   h_pb.assign(np, 1.09f);
@@ -722,6 +728,12 @@ void Synthesis::buildLayout(const sb_topology* tops, int ntop) {
     for (int i = 0; i < tp.natom; i++) {
       h_charge[base + i] = static_cast<float>(tp.charge[i] * sqrt_kc);
       h_ljidx[base + i] = tp.lj_idx[i];
+      {
+        // surface-area radius: half the sigma of the (type 0, atom type) entry of the pair
+        // table, which is what STORMM's first n_lj_types sigma values hold
+        const double a = tp.lja[tp.lj_idx[i]], b = tp.ljb[tp.lj_idx[i]];
+        h_sasa_radius[base + i] = (b > 1.0e-6) ? 0.5 * std::sqrt(std::cbrt(a / b)) : 0.0;
+      }
       if (opt.igb != SB_GB_NONE) {
         const double rho = tp.pb_radii[i] - gb_offset;
         h_rho[base + i] = static_cast<float>(rho);
@@ -1512,6 +1524,36 @@ void Synthesis::getEnergiesFixed(long long* out, cudaStream_t stream) {
   cudaCheck(cudaStreamSynchronize(stream), "energy download");
 }
 
+void Synthesis::surfaceArea(const double* points, int npts, double probe, double weight,
+                            double* out, cudaStream_t stream) {
+  if (points == nullptr || out == nullptr || npts <= 0 || !(probe >= 0.0) ||
+      !std::isfinite(probe) || !std::isfinite(weight)) {
+    throw Error(SB_ERR_ARGUMENT, "surface area: points, a positive point count, a finite "
+                "non-negative probe and a finite weight are required");
+  }
+  std::vector<double3> pts(npts);
+  for (int p = 0; p < npts; p++) {
+    pts[p] = make_double3(points[3 * p], points[3 * p + 1], points[3 * p + 2]);
+  }
+  DeviceArray<double> radius, result;
+  DeviceArray<double3> d_pts;
+  DeviceArray<int> cell;
+  radius.allocate(h_sasa_radius.size());
+  d_pts.allocate(npts);
+  cell.allocate(h_sasa_radius.size());
+  result.allocate(nsys);
+  cudaCheck(cudaMemcpyAsync(radius.p, h_sasa_radius.data(), h_sasa_radius.size() * sizeof(double),
+                            cudaMemcpyHostToDevice, stream), "surface area upload");
+  cudaCheck(cudaMemcpyAsync(d_pts.p, pts.data(), npts * sizeof(double3), cudaMemcpyHostToDevice,
+                            stream), "surface area upload");
+  cudaCheck(launchSurfaceArea(d_xcrd.p, d_ycrd.p, d_zcrd.p, std::ldexp(1.0, -opt.gpos_bits),
+                              d_atom_start.p, d_atom_count.p, nsys, radius.p, d_pts.p, npts,
+                              probe, weight, cell.p, result.p, stream), "surface area launch");
+  cudaCheck(cudaMemcpyAsync(out, result.p, nsys * sizeof(double), cudaMemcpyDeviceToHost,
+                            stream), "surface area download");
+  cudaCheck(cudaStreamSynchronize(stream), "surface area");
+}
+
 void Synthesis::getEnergies(double* out, cudaStream_t stream) {
   const int n = nsys * kNrgStride;
   cudaCheck(launchExportEnergies(d_energies.p, n, std::ldexp(1.0, -opt.nrg_bits), d_stage_nrg.p,
@@ -2232,6 +2274,13 @@ int sb_get_energies(sb_synthesis* syn, double* energies, void* stream) {
 
 int sb_set_restraints(sb_synthesis* syn, const sb_restraint* restraints, int count) {
   return guarded([&]() { need(syn)->setRestraints(restraints, count); });
+}
+
+int sb_surface_area(sb_synthesis* syn, const double* sphere_points, int n_points,
+                    double probe_radius, double weight, double* out, void* stream) {
+  return guarded([&]() {
+    need(syn)->surfaceArea(sphere_points, n_points, probe_radius, weight, out, asStream(stream));
+  });
 }
 
 int sb_set_restraint_step(sb_synthesis* syn, int step) {

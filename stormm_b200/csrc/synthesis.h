@@ -202,6 +202,10 @@ public:
   void getForces(double* xyz, cudaStream_t stream);
   void getForcesFixed(long long* prim, int* ovrf, cudaStream_t stream);
   void getEnergies(double* out, cudaStream_t stream);
+  // STORMM's sphere-point surface area of every system (sasa.cu); out: nsys values on the host
+  void surfaceArea(const double* points, int npts, double probe, double weight, double* out,
+                   cudaStream_t stream);
+  std::vector<double> h_sasa_radius;   // per padded atom: half the LJ sigma of (type 0, type)
   void downloadResults(double* forces, double* energies, cudaStream_t stream);
   void setRestraints(const sb_restraint* list, int count);
   int launchThreads(int units, int terms) const;

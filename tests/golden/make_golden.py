@@ -35,6 +35,8 @@ Fixtures written (numpy .npz, one per case):
 * ``restraints_r60.npz`` (``--restraints-only``): 40 constant restraints (positional, distance,
   angle and dihedral, the measured value in each region of the flat-bottom potential) on a
   60-atom molecule, STORMM's energy of each, the total and the forces.
+* ``sasa_s60.npz``, ``sasa_s200.npz``, ``sasa_s33.npz`` (``--sasa-only``): STORMM's surface
+  area of three synthetic molecules (272, 272 and 100 sphere points), with the points.
 * ``restraint_ramps_r60.npz`` (``--ramps-only``): 24 time-dependent restraints on the same
   molecule (initial and final bounds, stiffnesses and targets, a ramp between two steps, or
   both steps equal), STORMM's energies and forces at steps before, at, within and after the
@@ -125,6 +127,8 @@ def main():
                     help="write only the CHARMM-term fixtures")
     ap.add_argument("--restraints-only", action="store_true",
                     help="write only the restraint fixture")
+    ap.add_argument("--sasa-only", action="store_true",
+                    help="write only the surface-area fixtures")
     ap.add_argument("--ramps-only", action="store_true",
                     help="write only the time-dependent restraint fixture")
     args = ap.parse_args()
@@ -139,6 +143,10 @@ def main():
             return
         if args.ramps_only:
             ramp_case(tmp)
+            return
+        if args.sasa_only:
+            for seed, n, npts in ((8830, 60, 272), (8840, 200, 272), (8850, 33, 100)):
+                sasa_case(tmp, seed, n, npts)
             return
         if args.restraints_only:
             restraint_case(tmp)
@@ -223,6 +231,19 @@ def _dihedral(p0, p1, p2, p3):
     b0, b1, b2 = p1 - p0, p2 - p1, p3 - p2
     n1, n2 = np.cross(b0, b1), np.cross(b1, b2)
     return np.arctan2(np.linalg.norm(b1) * b0 @ n2, n1 @ n2)
+
+
+def sasa_case(tmp, seed, n, npts):
+    """STORMM's surface area (LJ-sigma radii, probe 1.4 A) of a synthetic molecule: the sphere
+    points it places, the area and the energy at 0.005 kcal/mol per A^2."""
+    mol = synthetic.make_molecule(seed, n, noise=0.1, name="S%d" % n)
+    rec, top, crd = eval_molecule(mol, tmp)
+    out = os.path.join(tmp, "sasa.bin")
+    run_driver(["sasa", top, crd, str(npts), out, "--quantize"])
+    rrec = read_records(out)
+    rec.update({k: v for k, v in rrec.items() if k != "coords"})
+    np.savez_compressed(os.path.join(HERE, "sasa_s%d.npz" % n), **rec)
+    print("wrote sasa_s%d" % n, rrec["sasa_area"][0], len(rrec["sphere_points"]) // 3)
 
 
 RAMP_STEPS = (0, 4, 5, 12, 17, 25, 30, 45)
