@@ -14,8 +14,11 @@ exclusions side by side, and a Lennard-Jones table over both molecules' types wh
 each molecule are that molecule's own table and whose cross blocks follow the Lorentz-Berthelot
 rules from each type's sigma and epsilon (the rules of the force fields here; STORMM's
 combination of topologies infers the rule from the tables, Topology/combograph_ljmodel.cpp).
-Not computed here: the surface-area term the application adds with its own solver
-(surfaceArea, Potential/surface_area.h), and its carve-out of the binding site.
+The surface-area term (apps/Gbsa/src/mmgbsa.cpp:244-253: surfaceArea over every molecule,
+probe 1.4 A, 0.005 kcal/mol per A^2) is added when the caller passes the sphere points
+(sphere_points, unit vectors; STORMM's application places 272 by its geodesic polyhedron),
+computed on the GPU for every system of the batch at the final coordinates.
+Not computed here: the application's carve-out of the binding site.
 """
 from __future__ import annotations
 
@@ -103,9 +106,11 @@ class MMGBSA:
         self.ligand = ligand
         self.complex = combine(receptor, ligand)
 
-    def run(self, poses, minimize_cycles=0, options=None, **controls):
+    def run(self, poses, minimize_cycles=0, options=None, sphere_points=None,
+            probe_radius=1.4, sasa_weight=0.005, **controls):
         """Energies of the receptor, each ligand pose and each complex (after minimize_cycles
-        line-minimization cycles when positive), and the binding energy of each pose."""
+        line-minimization cycles when positive), and the binding energy of each pose; with
+        sphere_points, the surface-area energy of each system joins them."""
         import stormm_b200 as sb
         poses = np.asarray(poses, dtype=np.float64).reshape(-1, self.ligand.natom, 3)
         k = len(poses)
@@ -122,10 +127,18 @@ class MMGBSA:
             syn.evaluate()
             e = syn.energy_terms()
             coords = syn.split(syn.coordinates())
+            sa = None
+            if sphere_points is not None:
+                sa = syn.surface_area(sphere_points, probe_radius, sasa_weight)
         finally:
             syn.close()
         rec, lig, cpx = e[0], e[1:1 + k], e[1 + k:]
         binding_terms = cpx - rec[None, :] - lig
-        return {"receptor": rec, "ligand": lig, "complex": cpx,
-                "binding_terms": binding_terms, "binding": binding_terms.sum(axis=1),
-                "coordinates": coords}
+        out = {"receptor": rec, "ligand": lig, "complex": cpx,
+               "binding_terms": binding_terms, "binding": binding_terms.sum(axis=1),
+               "coordinates": coords}
+        if sa is not None:
+            out["surface_area"] = sa
+            out["binding_surface_area"] = sa[1 + k:] - sa[0] - sa[1:1 + k]
+            out["binding"] = out["binding"] + out["binding_surface_area"]
+        return out

@@ -52,3 +52,27 @@ def test_binding_energies():
     res_min = calc.run(poses, minimize_cycles=40, sd_cycles=10)
     assert (res_min["complex"].sum(axis=1) < res["complex"].sum(axis=1)).all()
     assert res_min["receptor"].sum() < res["receptor"].sum()
+
+
+def test_surface_area_term():
+    """With sphere points (STORMM's 272-point set from the surface-area fixture) every system's
+    surface-area energy equals the oracle's restatement of STORMM's surfaceArea at the same
+    coordinates, and the binding energy takes the complex's minus the parts'."""
+    from fixtures import load
+    pts = load("sasa_s60.npz")["sphere_points"]
+    r = synthetic.make_molecule(synthetic._seed(62, 0), 150, noise=0.1)
+    l = synthetic.make_molecule(synthetic._seed(62, 1), 32, noise=0.1)
+    calc = mmgbsa.MMGBSA(r, l)
+    poses = _poses(r, l, 3, np.random.default_rng(4))
+    plain = calc.run(poses)
+    res = calc.run(poses, sphere_points=pts)
+    # the oracle takes the synthesis's own (fixed-point) coordinates
+    parts = [r] + [l] * len(poses) + [calc.complex] * len(poses)
+    for k, m in enumerate(parts):
+        x = np.asarray(res["coordinates"][k]).reshape(-1, 3)
+        want = oracle.surface_area(x, oracle.sasa_radii(m), pts, weight=0.005)
+        assert abs(res["surface_area"][k] - want) <= 1e-10 * want, k
+    k = len(poses)
+    sa = res["surface_area"]
+    np.testing.assert_allclose(res["binding"] - plain["binding"],
+                               sa[1 + k:] - sa[0] - sa[1:1 + k], rtol=0, atol=1e-12)
